@@ -1,0 +1,264 @@
+/*
+ * tpicb200.h - C ABI of the B200-native single-GPU ECSIM particle cycle.
+ *
+ * TPIC exposes its hot path as stream-ordered C++ template "enqueue"
+ * functions that take LPFx owners, an executor (CUDA stream) and an
+ * `unsigned* invalid` device flag, return an lpfx::ErrorCode, allocate
+ * nothing and never synchronise (SURVEY boundary; e.g.
+ * include/tpic/ecsim/deposition/current_deposition_device.hpp:285-313).
+ * The reference promises no binary ABI (docs/developer/architecture.md:459-460),
+ * so this header is the plain-C form of those entry points: caller-owned
+ * device buffers in the layouts below, a cudaStream_t, an optional device
+ * `uint32_t* invalid` counter and an int status that mirrors lpfx::ErrorCode.
+ *
+ * Layouts (all device memory, all fully periodic grids of nx*ny*nz cells):
+ *   node field  : 3 components, component-major; each component has extent
+ *                 (nx+3)(ny+3)(nz+3): interior nodes 0..n plus a one-node
+ *                 halo, index (i+1) + (nx+3)*((j+1) + (ny+3)*(k+1)).
+ *                 Node n is the periodic duplicate of node 0 (TPIC keeps
+ *                 cells+1 nodes per axis, data/fields/grid_shape.hpp:25-50).
+ *   cell field  : 3 components, extent (nx+2)(ny+2)(nz+2) with a one-cell
+ *                 halo, index (i+1) + (nx+2)*((j+1) + (ny+2)*(k+1)).
+ *   mass records: 126 scalars per node-field vertex (same vertex index as a
+ *                 node field): 14 canonical stencils x 9 row-major tensor
+ *                 entries, TPIC's compact layout
+ *                 (data/mass_matrix/mass_matrix_layout.hpp:11-68).
+ *   particles   : SoA records of one species (data/particles/particle_schema.hpp:20-36):
+ *                 rx, ry, rz cell-relative fractions in [0,1), u, v, w,
+ *                 signed macro-charge q (double), int32 cell key
+ *                 (i+2) + (nx+4)*((j+2) + (ny+4)*(k+2))
+ *                 (data/particles/particle_cell.hpp:34-46), optional uint64 id.
+ *   bins        : counts[(nx+4)(ny+4)(nz+4)] and offsets[bins+1] (uint32),
+ *                 one bin per halo-2 cell key, as LPFx's direct-cell sort.
+ *   solver field: E_theta and the other solver vectors are node fields of
+ *                 double (TPIC's SolverStorage, ecsim/gmres/gmres.hpp:44-52).
+ *
+ * Precision modes (types of the stored quantities):
+ *   TPICB200_PRECISION_DOUBLE : everything double (TPIC's "double" level).
+ *   TPICB200_PRECISION_MIXED  : positions and charges double, velocities,
+ *                               E, B, J and mass float; mover, current and
+ *                               scalar mass arithmetic float; positions
+ *                               accumulated in double; GMRES Krylov basis
+ *                               float with double dots, Givens rotations,
+ *                               residuals and solution (refined cycles).
+ *
+ * Threading: a context is used by one host thread at a time; calls are
+ * stream-ordered and not re-entrant. No entry point allocates memory except
+ * tpicb200_create. The product fails loudly (TPICB200_BACKEND_FAILURE)
+ * without a usable sm_100 device; there is no CPU fallback.
+ */
+#ifndef TPICB200_H
+#define TPICB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* cudaStream_t-compatible handle (0 = legacy default stream). */
+typedef struct CUstream_st* tpicb200_stream;
+typedef struct tpicb200_context tpicb200_context;
+
+/* Status codes: 0-4 mirror lpfx::ErrorCode (success, invalid_argument,
+ * invalid_state, overflow, backend_failure); include/lpfx/core/error.hpp. */
+enum {
+  TPICB200_SUCCESS = 0,
+  TPICB200_INVALID_ARGUMENT = 1,
+  TPICB200_INVALID_STATE = 2,
+  TPICB200_OVERFLOW = 3,
+  TPICB200_BACKEND_FAILURE = 4,
+  TPICB200_NOT_CONVERGED = 5,     /* GMRES did not reach its tolerance */
+  TPICB200_CAPACITY_EXCEEDED = 6, /* a particle count above the context's capacity */
+  TPICB200_INVALID_DATA = 7       /* a cycle raised the device invalid flag */
+};
+
+enum { TPICB200_PRECISION_DOUBLE = 0, TPICB200_PRECISION_MIXED = 1 };
+
+/* Mass-matrix assembly forms, the extended `--mass-matrix` selection
+ * (TPIC: scalar | matrix-core, config/numerics_options.hpp:31-47). */
+enum {
+  TPICB200_MASS_SCALAR = 0,     /* CUDA cores, the precision mode's compute type */
+  TPICB200_MASS_SCALAR_F64 = 1, /* CUDA cores, FP64 cell sums, narrowed once at the flush */
+  TPICB200_MASS_TF32 = 2,       /* tcgen05 tensor cores, TF32 operands, FP32 accumulation */
+  TPICB200_MASS_BF16X3 = 3      /* tcgen05, BF16 hi/lo split products, FP32 accumulation */
+};
+
+typedef struct {
+  int nx, ny, nz;       /* cells per axis (fully periodic) */
+  double lx, ly, lz;    /* box lengths */
+} tpicb200_grid;
+
+typedef struct {
+  double dt, theta, c;      /* time step, implicitness, light speed (TPIC admits c = 1) */
+  double gmres_tol;         /* relative tolerance of the true residual */
+  int gmres_restart;        /* 30 in TPIC (config/physics.hpp:20) */
+  int gmres_max_iterations; /* 100 in TPIC (config/physics.hpp:21) */
+  int precision;            /* TPICB200_PRECISION_* */
+  uint32_t max_particles;   /* capacity of the sort scratch (largest species) */
+} tpicb200_options;
+
+typedef struct {
+  void* rx; void* ry; void* rz; /* double */
+  void* u; void* v; void* w;    /* double (DOUBLE) or float (MIXED) */
+  double* q;
+  int32_t* cell;
+  uint64_t* id;                 /* may be NULL */
+  uint32_t count;
+} tpicb200_particles;
+
+typedef struct {
+  int64_t node_count;     /* elements per node-field component */
+  int64_t cell_count;     /* elements per cell-field component */
+  int64_t bin_count;      /* halo-2 particle bins */
+  int64_t interior_nodes; /* (nx+1)(ny+1)(nz+1): GMRES vector length / 3 */
+  size_t field_scalar_bytes; /* sizeof E/B/J scalars: 8 (DOUBLE) or 4 (MIXED) */
+  size_t mass_scalar_bytes;  /* sizeof mass scalars */
+  size_t velocity_scalar_bytes;
+} tpicb200_layout;
+
+typedef struct {
+  int converged, iterations;
+  double initial_residual, residual, rhs_norm, relative_residual;
+} tpicb200_gmres_result;
+
+/* Whole-cycle state: every pointer is a caller-owned device buffer.
+ * Particles are double-buffered per species (slot[s][current] is live; the
+ * sort writes the other slot and flips current). */
+#define TPICB200_MAX_SPECIES 8
+typedef struct {
+  int ns;
+  double qom[TPICB200_MAX_SPECIES];
+  tpicb200_particles slot[TPICB200_MAX_SPECIES][2];
+  int current[TPICB200_MAX_SPECIES];
+  uint32_t* counts[TPICB200_MAX_SPECIES];  /* bins of the live slot */
+  uint32_t* offsets[TPICB200_MAX_SPECIES];
+  void* e;          /* node field, committed E^n */
+  void* b_cell;     /* cell field, committed B^n */
+  void* b_node;     /* node field, particle-facing B^n */
+  void* b_cell_next;
+  void* b_node_next;
+  void* j;          /* node field, assembled J-hat */
+  void* mass;       /* mass records */
+  double* e_theta;  /* solver node field */
+  int mass_kind;    /* TPICB200_MASS_* */
+} tpicb200_state;
+
+typedef struct {
+  tpicb200_gmres_result gmres;
+  double field_energy[2];               /* electric, magnetic after the cycle */
+  double species[TPICB200_MAX_SPECIES][5]; /* kinetic, charge, momentum x/y/z */
+  double total_energy;
+  float stage_ms[6]; /* solve, move, advance, sort, deposit, fold+diagnostics */
+} tpicb200_cycle_report;
+
+const char* tpicb200_version(void);
+/* Message of the last failure on the calling thread. */
+const char* tpicb200_last_error(void);
+
+/* Set up a context: geometry, constants and the solver/sort workspace.
+ * Replaces the owner construction of MaxwellOperator, Gmres and the sort
+ * workspace (ecsim/maxwell/maxwell_device.hpp:60-95,
+ * ecsim/gmres/gmres_device.hpp:316-336). The calling thread's current CUDA
+ * device is used. */
+int tpicb200_create(const tpicb200_grid* grid, const tpicb200_options* options,
+                    tpicb200_context** out);
+int tpicb200_destroy(tpicb200_context* ctx);
+int tpicb200_get_layout(const tpicb200_context* ctx, tpicb200_layout* out);
+
+/* Implicit theta-scheme mover of one species over `p->count` records:
+ * v_new = 2*(alpha v + beta alpha E_theta) - v, x += dt v_new, periodic wrap.
+ * Replaces enqueue_local_particle_mover (ecsim/particles/particle_mover_device.hpp:310-328).
+ * e_theta: solver node field; b_node: the old particle-facing B (node field).
+ * An invalid record keeps its attributes and increments *invalid. */
+int tpicb200_mover(tpicb200_context* ctx, double qom, tpicb200_particles* p,
+                   const double* e_theta, const void* b_node, uint32_t* invalid,
+                   tpicb200_stream stream);
+
+/* Stable counting sort by cell key: out receives the records of `in` in key
+ * order (equal keys keep their input order), counts/offsets the bins.
+ * Replaces FullParticleSort::enqueue (ecsim/particles/particle_sort_device.hpp:132-145)
+ * whose device sort is unstable within a bin; this one is bit-exact against
+ * the stable host sort (lpfx/algorithm/particle/host/sort.hpp:205-290).
+ * in and out must not alias; an out-of-range key increments *invalid and the
+ * call returns TPICB200_INVALID_DATA after synchronising. */
+int tpicb200_sort(tpicb200_context* ctx, const tpicb200_particles* in, tpicb200_particles* out,
+                  uint32_t* counts, uint32_t* offsets, uint32_t* invalid,
+                  tpicb200_stream stream);
+
+/* Zero J (node field) and the mass records. Replaces enqueue_clear_mass_matrix
+ * (ecsim/mass_matrix/mass_matrix_deposition_device.hpp:107-121) and the moment clear. */
+int tpicb200_clear_moments(tpicb200_context* ctx, void* j, void* mass, tpicb200_stream stream);
+
+/* Implicit current and mass-matrix deposition of one species, added into j
+ * and mass (either may be NULL) at the periodic unique nodes; call
+ * tpicb200_fold_periodic after the last species. With counts/offsets (the
+ * bins of p, from tpicb200_sort) the sorted cell-tile kernels run; with NULL
+ * bins the per-particle kernels run (scalar forms only). Replaces
+ * enqueue_sorted_current / enqueue_unsorted_current
+ * (ecsim/deposition/current_deposition_device.hpp:340-421) and
+ * enqueue_sorted_mass_matrix<Kernel> / enqueue_unsorted_mass_matrix
+ * (ecsim/mass_matrix/mass_matrix_deposition_device.hpp:124-182). */
+int tpicb200_deposit(tpicb200_context* ctx, double qom, const tpicb200_particles* p,
+                     const uint32_t* counts, const uint32_t* offsets, const void* b_node,
+                     void* j, void* mass, int mass_kind, uint32_t* invalid,
+                     tpicb200_stream stream);
+
+/* Periodic fold: the duplicate endpoint nodes and the one-node ghosts of j
+ * and of the mass records take the values of their periodic unique node.
+ * Replaces the self-periodic J.add/ghost exchange and the compact mass halo
+ * (ecsim/deposition/current_assembly_device.hpp:26-53,
+ * communication/mass_halo/mass_halo_device.hpp:91-160,350-364). */
+int tpicb200_fold_periodic(tpicb200_context* ctx, void* j, void* mass, tpicb200_stream stream);
+
+/* out = M * in / V at the interior nodes (double node fields, in with
+ * ghosts). Replaces enqueue_mass_matrix_apply (ecsim/mass_matrix/mass_matrix_apply_device.hpp:65-96). */
+int tpicb200_mass_apply(tpicb200_context* ctx, const void* mass, const double* in, double* out,
+                        tpicb200_stream stream);
+
+/* Field solve: rhs = E + delta curl_C2N(B) - k J; GMRES(restart) on
+ * A(v) = v + delta^2 curl_C2N curl_N2C v + k M v / V from the guess E; writes
+ * E_theta (interior nodes and ghosts) when converged. Host-blocking like
+ * Gmres::host_blocking_solve (ecsim/gmres/gmres_device.hpp:353-454):
+ * two scalars are read back per Arnoldi step. b_cell needs filled ghosts. */
+int tpicb200_field_solve(tpicb200_context* ctx, const void* e, const void* b_cell, const void* j,
+                         const void* mass, double* e_theta, tpicb200_gmres_result* result,
+                         tpicb200_stream stream);
+
+/* Field advance: e <- E_theta/theta - (1-theta)/theta e; b_cell_next <-
+ * b_cell - c dt curl_N2C(E_theta) with periodic ghosts; b_node_next <-
+ * cell_to_node(b_cell_next). Replaces MaxwellOperator::enqueue_next_e_and_cell
+ * and enqueue_next_cell_closure_and_node_interpolation (ecsim/maxwell/maxwell_device.hpp:234-252). */
+int tpicb200_field_advance(tpicb200_context* ctx, void* e, const void* b_cell,
+                           const double* e_theta, void* b_cell_next, void* b_node_next,
+                           tpicb200_stream stream);
+
+/* Particle-facing B: b_node <- cell_to_node(b_cell) (ghosts of b_cell are
+ * refreshed first). Startup form of complete_initial_magnetic_field. */
+int tpicb200_magnetic_to_nodes(tpicb200_context* ctx, void* b_cell, void* b_node,
+                               tpicb200_stream stream);
+
+/* Scalar diagnostics (diagnostics/scalar_diagnostics_device.hpp:49-133):
+ * out[0] = V/(8 pi) sum |E|^2 over unique nodes, out[1] = V/(8 pi) sum |B|^2
+ * over cells, then per species kinetic energy, charge, momentum x/y/z.
+ * Host-blocking (synchronises `stream`). */
+int tpicb200_energy(tpicb200_context* ctx, const void* e, const void* b_cell,
+                    const tpicb200_particles* species, const double* qom, int ns, double* out,
+                    tpicb200_stream stream);
+
+/* Startup: B nodes from cells, the first sort and the bootstrap deposition
+ * (docs/developer/architecture.md:161-171). */
+int tpicb200_prepare(tpicb200_context* ctx, tpicb200_state* state, tpicb200_stream stream);
+
+/* ncycles ECSIM cycles: solve, move (old B), field advance, sort, deposit
+ * (next B), fold, commit; reports (may be NULL) receive one entry per cycle
+ * with the energies of the committed state. Host-blocking. */
+int tpicb200_cycle(tpicb200_context* ctx, tpicb200_state* state, int ncycles,
+                   tpicb200_cycle_report* reports, tpicb200_stream stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TPICB200_H */

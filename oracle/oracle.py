@@ -1,0 +1,253 @@
+"""ctypes front end of the CPU oracle (oracle/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: the checker of the CUDA path. Only tests/,
+__graft_entry__.smoke() and bench.py's CPU-baseline leg use it; the product
+(tpic_b200/) never imports it.
+
+`OracleCycle` runs TPIC's one-rank cycle on the host in the layouts of
+include/tpicb200.h: solve, move (old B), advance, stable sort, deposit
+(next B), fold, commit (include/tpic/simulation/driver/pipeline.hpp:437-540).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIBRARY = HERE / "liboracle.so"
+REF_LIBRARY = HERE / "_ref" / "libtpicref.so"
+
+_lib = None
+_ref = None
+
+dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+
+
+class OGrid(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+                ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double)]
+
+
+class OGmres(C.Structure):
+    _fields_ = [("converged", C.c_int), ("iterations", C.c_int), ("initial_residual", C.c_double),
+                ("residual", C.c_double), ("rhs_norm", C.c_double), ("relative_residual", C.c_double)]
+
+
+def build() -> None:
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not LIBRARY.exists():
+            build()
+        lib = C.CDLL(str(LIBRARY))
+        vp = C.c_void_p
+        lib.oracle_mover.restype = C.c_long
+        lib.oracle_mover.argtypes = [C.c_int, C.POINTER(OGrid), C.c_double, C.c_double, C.c_double,
+                                     vp, vp, vp, vp, vp, vp, vp, vp, C.c_long, vp, vp]
+        lib.oracle_sort.restype = C.c_long
+        lib.oracle_sort.argtypes = [C.POINTER(OGrid), vp, C.c_long, vp, vp, vp]
+        lib.oracle_deposit.restype = C.c_long
+        lib.oracle_deposit.argtypes = [C.c_int, C.POINTER(OGrid), C.c_double, C.c_double, C.c_double,
+                                       vp, vp, vp, vp, vp, vp, vp, vp, C.c_long, vp, vp, vp]
+        lib.oracle_fold.argtypes = [C.POINTER(OGrid), vp, vp]
+        lib.oracle_mass_apply.argtypes = [C.c_int, C.POINTER(OGrid), vp, vp, vp]
+        for name in ("oracle_curl_n2c", "oracle_curl_c2n", "oracle_cell_to_node"):
+            getattr(lib, name).argtypes = [C.POINTER(OGrid), vp, vp]
+        lib.oracle_node_ghosts.argtypes = [C.POINTER(OGrid), vp]
+        lib.oracle_cell_ghosts.argtypes = [C.POINTER(OGrid), vp]
+        lib.oracle_field_solve.restype = C.c_int
+        lib.oracle_field_solve.argtypes = [C.POINTER(OGrid), C.c_double, C.c_double, C.c_double, vp, vp, vp, vp,
+                                           vp, C.c_int, C.c_int, C.c_double, C.POINTER(OGmres)]
+        lib.oracle_field_advance.argtypes = [C.POINTER(OGrid), C.c_double, C.c_double, C.c_double, vp, vp, vp,
+                                             vp, vp]
+        lib.oracle_field_energy.argtypes = [C.POINTER(OGrid), vp, vp, vp]
+        lib.oracle_species_scalars.argtypes = [C.c_int, C.c_double, vp, vp, vp, vp, C.c_long, vp]
+        lib.oracle_pair_stencil.restype = C.c_int
+        lib.oracle_pair_stencil.argtypes = [C.c_int, C.c_int]
+        lib.oracle_cic_weights_f64.argtypes = [C.c_double, C.c_double, C.c_double, vp]
+        lib.oracle_cic_weights_f32.argtypes = [C.c_float, C.c_float, C.c_float, vp]
+        lib.oracle_response_f64.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double, vp]
+        lib.oracle_response_f32.argtypes = [C.c_float, C.c_float, C.c_float, C.c_float, vp]
+        for name in ("oracle_node_count", "oracle_cell_count", "oracle_bin_count"):
+            getattr(lib, name).restype = C.c_long
+            getattr(lib, name).argtypes = [C.POINTER(OGrid)]
+        _lib = lib
+    return _lib
+
+
+def load_reference():
+    """The reference's own header numerics compiled by oracle/Makefile, or None."""
+    global _ref
+    if _ref is None and REF_LIBRARY.exists():
+        lib = C.CDLL(str(REF_LIBRARY))
+        vp = C.c_void_p
+        lib.ref_cic_weights_f64.argtypes = [C.c_double, C.c_double, C.c_double, vp]
+        lib.ref_cic_weights_f32.argtypes = [C.c_float, C.c_float, C.c_float, vp]
+        lib.ref_response_f64.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double, vp]
+        lib.ref_response_f32.argtypes = [C.c_float, C.c_float, C.c_float, C.c_float, vp]
+        lib.ref_pair_stencil.restype = C.c_int
+        lib.ref_pair_stencil.argtypes = [C.c_int, C.c_int]
+        lib.ref_stencil_offset.argtypes = [C.c_int, vp]
+        lib.ref_encode_key.restype = C.c_int
+        lib.ref_encode_key.argtypes = [C.c_int] * 6
+        lib.ref_decode_key.argtypes = [C.c_int] * 4 + [vp]
+        for name in ("ref_curl_n2c", "ref_curl_c2n"):
+            getattr(lib, name).argtypes = [C.c_int, C.c_int, C.c_int, vp, C.c_double, C.c_double, C.c_double,
+                                           C.c_int, C.c_int, C.c_int, vp]
+        lib.ref_cell_to_node.restype = C.c_double
+        lib.ref_cell_to_node.argtypes = [C.c_int, C.c_int, vp, C.c_int, C.c_int, C.c_int]
+        lib.ref_mass_apply_node.argtypes = [C.c_int, C.c_int, C.c_int, vp, vp, C.c_double, C.c_int, C.c_int,
+                                            C.c_int, vp]
+        _ref = lib
+    return _ref
+
+
+def ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+class OracleCycle:
+    """The ECSIM cycle on the host (FP64 fields and moments; the mover in the
+    storage/compute types of the selected precision, bit-identical to the GPU
+    mover)."""
+
+    def __init__(self, grid, species, dt, theta=0.5, c=1.0, gmres_tol=1e-8, precision=0,
+                 restart=30, max_iterations=100, e0=(0.0, 0.0, 0.0), b0=(0.0, 0.0, 0.0)):
+        self.lib = load()
+        self.og = OGrid(grid.nx, grid.ny, grid.nz, grid.lx / grid.nx, grid.ly / grid.ny, grid.lz / grid.nz)
+        self.grid = grid
+        self.dt, self.theta, self.c, self.tol = dt, theta, c, gmres_tol
+        self.restart, self.max_iterations = restart, max_iterations
+        self.precision = precision
+        self.vdt = np.float64 if precision == 0 else np.float32
+        self.fdt = np.float64 if precision == 0 else np.float32
+        og = C.byref(self.og)
+        self.nodes = self.lib.oracle_node_count(og)
+        self.cells = self.lib.oracle_cell_count(og)
+        self.nbins = self.lib.oracle_bin_count(og)
+        n, cl = self.nodes, self.cells
+        self.e = np.zeros(3 * n)
+        self.b = np.zeros(3 * cl)
+        for k in range(3):
+            self.e[k * n:(k + 1) * n] = e0[k]
+            self.b[k * cl:(k + 1) * cl] = b0[k]
+        # Fields are stored in the precision's storage type between stages.
+        self.e = self.e.astype(self.fdt).astype(np.float64)
+        self.b = self.b.astype(self.fdt).astype(np.float64)
+        self.bnode = np.zeros(3 * n)
+        self.j = np.zeros(3 * n)
+        self.m = np.zeros(126 * n)
+        self.theta_field = np.zeros(3 * n)
+        self.species = species  # list of (qom, dict of arrays)
+        self.gmres = []
+
+    def _ptrs(self, d):
+        return [ptr(d[k]) for k in ("rx", "ry", "rz", "u", "v", "w", "q", "cell")]
+
+    def sort(self):
+        for qom, d in self.species:
+            n = len(d["cell"])
+            perm = np.empty(n, dtype=np.uint32)
+            counts = np.empty(self.nbins, dtype=np.uint32)
+            offsets = np.empty(self.nbins + 1, dtype=np.uint32)
+            status = self.lib.oracle_sort(C.byref(self.og), ptr(d["cell"]), n, ptr(perm), ptr(counts),
+                                          ptr(offsets))
+            if status != 0:
+                raise ValueError("out-of-range cell key")
+            for k in [k for k in d if not k.startswith("_")]:
+                d[k] = np.ascontiguousarray(d[k][perm])
+            d["_counts"], d["_offsets"] = counts, offsets
+
+    def deposit(self, bnode):
+        self.j[:] = 0
+        self.m[:] = 0
+        bn = bnode.astype(self.fdt)
+        for qom, d in self.species:
+            bad = self.lib.oracle_deposit(self.precision, C.byref(self.og), qom, self.dt, self.c, *self._ptrs(d),
+                                          len(d["cell"]), ptr(bn), ptr(self.j), ptr(self.m))
+            if bad:
+                raise ValueError(f"{bad} invalid records in deposition")
+        self.lib.oracle_fold(C.byref(self.og), ptr(self.j), ptr(self.m))
+        # Moments are stored in the precision's storage type.
+        self.j = self.j.astype(self.fdt).astype(np.float64)
+        self.m = self.m.astype(self.fdt).astype(np.float64)
+
+    def prepare(self):
+        self.lib.oracle_cell_ghosts(C.byref(self.og), ptr(self.b))
+        self.lib.oracle_cell_to_node(C.byref(self.og), ptr(self.b), ptr(self.bnode))
+        self.bnode = self.bnode.astype(self.fdt).astype(np.float64)
+        self.sort()
+        self.deposit(self.bnode)
+
+    def solve(self):
+        res = OGmres()
+        status = self.lib.oracle_field_solve(C.byref(self.og), self.dt, self.theta, self.c, ptr(self.e), ptr(self.b),
+                                             ptr(self.j), ptr(self.m), ptr(self.theta_field), self.restart,
+                                             self.max_iterations, self.tol, C.byref(res))
+        self.gmres.append(res)
+        if status != 0:
+            raise RuntimeError("oracle GMRES did not converge")
+        return res
+
+    def move(self):
+        bn = self.bnode.astype(self.fdt)
+        for qom, d in self.species:
+            bad = self.lib.oracle_mover(self.precision, C.byref(self.og), qom, self.dt, self.c, *self._ptrs(d),
+                                        len(d["cell"]), ptr(self.theta_field), ptr(bn))
+            if bad:
+                raise ValueError(f"{bad} invalid records in the mover")
+
+    def advance(self):
+        bnext = np.zeros_like(self.b)
+        bnode_next = np.zeros_like(self.bnode)
+        self.lib.oracle_field_advance(C.byref(self.og), self.dt, self.theta, self.c, ptr(self.e), ptr(self.b),
+                                      ptr(self.theta_field), ptr(bnext), ptr(bnode_next))
+        self.e = self.e.astype(self.fdt).astype(np.float64)
+        self.bnext = bnext.astype(self.fdt).astype(np.float64)
+        self.bnode_next = bnode_next.astype(self.fdt).astype(np.float64)
+
+    def energy(self):
+        out = np.zeros(2)
+        self.lib.oracle_field_energy(C.byref(self.og), ptr(self.e), ptr(self.b), ptr(out))
+        res = [out[0], out[1]]
+        for qom, d in self.species:
+            s = np.zeros(5)
+            self.lib.oracle_species_scalars(self.precision, qom, ptr(d["u"]), ptr(d["v"]), ptr(d["w"]), ptr(d["q"]),
+                                            len(d["q"]), ptr(s))
+            res.extend(s)
+        return np.array(res)
+
+    def cycle(self):
+        self.solve()
+        self.move()
+        self.advance()
+        self.sort()
+        self.deposit(self.bnode_next)
+        self.b, self.bnode = self.bnext, self.bnode_next
+        return self.energy()
+
+
+def total_energy(scalars: np.ndarray, ns: int) -> float:
+    return float(scalars[0] + scalars[1] + sum(scalars[2 + 5 * s] for s in range(ns)))
+
+
+def case_species_arrays(case, precision: int, generate) -> list:
+    """(qom, arrays) per species in the storage types of `precision`."""
+    vdt = np.float64 if precision == 0 else np.float32
+    out = []
+    for s, sp in enumerate(case.species):
+        d = generate(case.grid, sp, s, seed=case.seed, velocity_dtype=vdt)
+        d.pop("id", None)
+        out.append((sp.qom, d))
+    return out
+
+
+__all__ = ["OracleCycle", "load", "load_reference", "build", "total_energy", "case_species_arrays", "OGrid", "ptr",
+           "math"]

@@ -1,0 +1,121 @@
+"""ctypes bindings of include/tpicb200.h (the library's C ABI).
+
+The library is the in-tree tpic_b200/libtpicb200.so built for sm_100a by
+tpic_b200/build.py. Loading fails loudly when it is missing: there is no
+Python or CPU fallback for any stage of the cycle.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIBRARY = Path(__file__).resolve().parent / "libtpicb200.so"
+
+SUCCESS, INVALID_ARGUMENT, INVALID_STATE, OVERFLOW, BACKEND_FAILURE = 0, 1, 2, 3, 4
+NOT_CONVERGED, CAPACITY_EXCEEDED, INVALID_DATA = 5, 6, 7
+PRECISION_DOUBLE, PRECISION_MIXED = 0, 1
+MASS_SCALAR, MASS_SCALAR_F64, MASS_TF32, MASS_BF16X3 = 0, 1, 2, 3
+MAX_SPECIES = 8
+
+MASS_KINDS = {"scalar": MASS_SCALAR, "scalar-f64": MASS_SCALAR_F64, "fp64": MASS_SCALAR_F64,
+              "tf32": MASS_TF32, "bf16x3": MASS_BF16X3, "matrix-core": MASS_TF32}
+PRECISIONS = {"double": PRECISION_DOUBLE, "mixed": PRECISION_MIXED}
+
+
+class Grid(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+                ("lx", C.c_double), ("ly", C.c_double), ("lz", C.c_double)]
+
+
+class Options(C.Structure):
+    _fields_ = [("dt", C.c_double), ("theta", C.c_double), ("c", C.c_double), ("gmres_tol", C.c_double),
+                ("gmres_restart", C.c_int), ("gmres_max_iterations", C.c_int), ("precision", C.c_int),
+                ("max_particles", C.c_uint32)]
+
+
+class Particles(C.Structure):
+    _fields_ = [("rx", C.c_void_p), ("ry", C.c_void_p), ("rz", C.c_void_p),
+                ("u", C.c_void_p), ("v", C.c_void_p), ("w", C.c_void_p),
+                ("q", C.c_void_p), ("cell", C.c_void_p), ("id", C.c_void_p), ("count", C.c_uint32)]
+
+
+class Layout(C.Structure):
+    _fields_ = [("node_count", C.c_int64), ("cell_count", C.c_int64), ("bin_count", C.c_int64),
+                ("interior_nodes", C.c_int64), ("field_scalar_bytes", C.c_size_t),
+                ("mass_scalar_bytes", C.c_size_t), ("velocity_scalar_bytes", C.c_size_t)]
+
+
+class GmresResult(C.Structure):
+    _fields_ = [("converged", C.c_int), ("iterations", C.c_int), ("initial_residual", C.c_double),
+                ("residual", C.c_double), ("rhs_norm", C.c_double), ("relative_residual", C.c_double)]
+
+
+class State(C.Structure):
+    _fields_ = [("ns", C.c_int), ("qom", C.c_double * MAX_SPECIES),
+                ("slot", (Particles * 2) * MAX_SPECIES), ("current", C.c_int * MAX_SPECIES),
+                ("counts", C.c_void_p * MAX_SPECIES), ("offsets", C.c_void_p * MAX_SPECIES),
+                ("e", C.c_void_p), ("b_cell", C.c_void_p), ("b_node", C.c_void_p),
+                ("b_cell_next", C.c_void_p), ("b_node_next", C.c_void_p), ("j", C.c_void_p),
+                ("mass", C.c_void_p), ("e_theta", C.c_void_p), ("mass_kind", C.c_int)]
+
+
+class CycleReport(C.Structure):
+    _fields_ = [("gmres", GmresResult), ("field_energy", C.c_double * 2),
+                ("species", (C.c_double * 5) * MAX_SPECIES), ("total_energy", C.c_double),
+                ("stage_ms", C.c_float * 6)]
+
+
+EXPORTS = {
+    "tpicb200_version": (C.c_char_p, []),
+    "tpicb200_last_error": (C.c_char_p, []),
+    "tpicb200_create": (C.c_int, [C.POINTER(Grid), C.POINTER(Options), C.POINTER(C.c_void_p)]),
+    "tpicb200_destroy": (C.c_int, [C.c_void_p]),
+    "tpicb200_get_layout": (C.c_int, [C.c_void_p, C.POINTER(Layout)]),
+    "tpicb200_mover": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(Particles), C.c_void_p, C.c_void_p,
+                                 C.c_void_p, C.c_void_p]),
+    "tpicb200_sort": (C.c_int, [C.c_void_p, C.POINTER(Particles), C.POINTER(Particles), C.c_void_p,
+                                C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tpicb200_clear_moments": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tpicb200_deposit": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(Particles), C.c_void_p, C.c_void_p,
+                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "tpicb200_fold_periodic": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tpicb200_mass_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tpicb200_field_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.c_void_p, C.POINTER(GmresResult), C.c_void_p]),
+    "tpicb200_field_advance": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.c_void_p, C.c_void_p]),
+    "tpicb200_magnetic_to_nodes": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tpicb200_energy": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(Particles),
+                                  C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_double), C.c_void_p]),
+    "tpicb200_prepare": (C.c_int, [C.c_void_p, C.POINTER(State), C.c_void_p]),
+    "tpicb200_cycle": (C.c_int, [C.c_void_p, C.POINTER(State), C.c_int, C.POINTER(CycleReport), C.c_void_p]),
+}
+
+_lib = None
+
+
+class TpicError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"tpicb200 status {status}: {message}")
+        self.status = status
+
+
+def load() -> C.CDLL:
+    """Loads the sm_100a library; raises when it has not been built."""
+    global _lib
+    if _lib is None:
+        if not LIBRARY.exists():
+            raise RuntimeError(f"{LIBRARY} is missing: run `python -m tpic_b200.build` (no CPU fallback exists)")
+        lib = C.CDLL(str(LIBRARY))
+        for name, (restype, argtypes) in EXPORTS.items():
+            fn = getattr(lib, name)
+            fn.restype = restype
+            fn.argtypes = argtypes
+        _lib = lib
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != SUCCESS:
+        message = load().tpicb200_last_error().decode()
+        raise TpicError(status, message)

@@ -1,0 +1,413 @@
+// The C ABI (include/tpicb200.h): context, argument checks, stage entry
+// points and the cycle driver. Every entry point validates its arguments,
+// enqueues on the caller's stream and maps CUDA failures to status codes.
+#include "kernels.cuh"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <utility>
+
+using namespace tpicb200;
+
+struct tpicb200_context {
+  int device = 0;
+  Geom g{};
+  tpicb200_options opt{};
+  SolverWorkspace* solver = nullptr;
+  uint32_t* cursor = nullptr;
+  uint32_t* perm = nullptr;
+  uint32_t* scan = nullptr;
+  uint32_t* invalid = nullptr;   // context's own invalid counter
+  double* partials = nullptr;    // energy reduction partials
+  double* reduced = nullptr;     // energy reduction results
+  double* pinned = nullptr;      // host mirror of `reduced` + invalid
+  int energy_blocks = 0;
+  cudaEvent_t events[8]{};
+};
+
+namespace {
+
+thread_local std::string last_error;
+
+int fail(int status, const std::string& message) {
+  last_error = message;
+  return status;
+}
+
+int cuda_status(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return TPICB200_SUCCESS;
+  return fail(TPICB200_BACKEND_FAILURE, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+int check_ctx(const tpicb200_context* ctx) {
+  if (!ctx) return fail(TPICB200_INVALID_ARGUMENT, "null context");
+  return TPICB200_SUCCESS;
+}
+
+int check_particles(const tpicb200_context* ctx, const tpicb200_particles* p) {
+  if (!p) return fail(TPICB200_INVALID_ARGUMENT, "null particle set");
+  if (p->count > ctx->opt.max_particles)
+    return fail(TPICB200_CAPACITY_EXCEEDED, "particle count above the context capacity");
+  if (p->count && (!p->rx || !p->ry || !p->rz || !p->u || !p->v || !p->w || !p->q || !p->cell))
+    return fail(TPICB200_INVALID_ARGUMENT, "null particle attribute");
+  return TPICB200_SUCCESS;
+}
+
+uint32_t* invalid_or_own(tpicb200_context* ctx, uint32_t* invalid) {
+  return invalid ? invalid : ctx->invalid;
+}
+
+}  // namespace
+
+namespace tpicb200 {
+Geom make_geom(const tpicb200_grid& grid) {
+  Geom g{};
+  g.nx = grid.nx; g.ny = grid.ny; g.nz = grid.nz;
+  g.NX = grid.nx + 3; g.NY = grid.ny + 3; g.NZ = grid.nz + 3;
+  g.CX = grid.nx + 2; g.CY = grid.ny + 2; g.CZ = grid.nz + 2;
+  g.ex = grid.nx + 4; g.ey = grid.ny + 4; g.ez = grid.nz + 4;
+  g.nodes = (long long)g.NX * g.NY * g.NZ;
+  g.cells = (long long)g.CX * g.CY * g.CZ;
+  g.bins = (long long)g.ex * g.ey * g.ez;
+  g.inx = grid.nx + 1; g.iny = grid.ny + 1; g.inz = grid.nz + 1;
+  g.interior = (long long)g.inx * g.iny * g.inz;
+  g.dx = grid.lx / grid.nx; g.dy = grid.ly / grid.ny; g.dz = grid.lz / grid.nz;
+  g.inv[0] = 1.0 / g.dx; g.inv[1] = 1.0 / g.dy; g.inv[2] = 1.0 / g.dz;
+  g.volume = (g.dx * g.dy) * g.dz;
+  g.inv_volume = 1.0 / g.volume;
+  return g;
+}
+}  // namespace tpicb200
+
+extern "C" {
+
+const char* tpicb200_version(void) { return "tpicb200 0.1 (sm_100a)"; }
+const char* tpicb200_last_error(void) { return last_error.c_str(); }
+
+int tpicb200_create(const tpicb200_grid* grid, const tpicb200_options* options, tpicb200_context** out) {
+  if (!grid || !options || !out) return fail(TPICB200_INVALID_ARGUMENT, "null create argument");
+  *out = nullptr;
+  if (grid->nx <= 0 || grid->ny <= 0 || grid->nz <= 0 || !(grid->lx > 0) || !(grid->ly > 0) ||
+      !(grid->lz > 0) || !std::isfinite(grid->lx) || !std::isfinite(grid->ly) || !std::isfinite(grid->lz))
+    return fail(TPICB200_INVALID_ARGUMENT, "grid extents must be positive and finite");
+  const long long bins = (grid->nx + 4LL) * (grid->ny + 4LL) * (grid->nz + 4LL);
+  const long long nodes = (grid->nx + 3LL) * (grid->ny + 3LL) * (grid->nz + 3LL);
+  if (bins > 0x7fffffffLL || nodes * 126 > (1LL << 40))
+    return fail(TPICB200_OVERFLOW, "grid too large for int32 cell keys");
+  if (!(options->dt > 0) || !std::isfinite(options->dt) || !(options->theta > 0) || options->theta > 1 ||
+      !(options->c > 0) || !std::isfinite(options->c) || !(options->gmres_tol >= 0) ||
+      options->gmres_restart <= 0 || options->gmres_restart > 1024 || options->gmres_max_iterations <= 0)
+    return fail(TPICB200_INVALID_ARGUMENT, "invalid time step, theta, c or GMRES parameters");
+  if (options->precision != TPICB200_PRECISION_DOUBLE && options->precision != TPICB200_PRECISION_MIXED)
+    return fail(TPICB200_INVALID_ARGUMENT, "unknown precision mode");
+  int device = 0, count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+    return fail(TPICB200_BACKEND_FAILURE, "no CUDA device: the ECSIM cycle has no CPU fallback");
+  cudaGetDevice(&device);
+  int major = 0;
+  cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device);
+  if (major != 10) return fail(TPICB200_BACKEND_FAILURE, "this build targets sm_100a (B200) only");
+  auto* ctx = new tpicb200_context();
+  ctx->device = device;
+  ctx->g = make_geom(*grid);
+  ctx->opt = *options;
+  cudaError_t e = cudaSuccess;
+  ctx->solver = solver_create(options->precision, ctx->g, options->gmres_restart, options->dt,
+                              options->theta, options->c, &e);
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  ctx->energy_blocks = 4 * sms;
+  auto alloc = [&](void** p, size_t bytes) {
+    if (e == cudaSuccess) e = cudaMalloc(p, bytes ? bytes : 4);
+  };
+  alloc((void**)&ctx->cursor, size_t(ctx->g.bins) * 4);
+  alloc((void**)&ctx->perm, size_t(options->max_particles) * 4);
+  alloc((void**)&ctx->scan, sort_scan_words(ctx->g.bins) * 4);
+  alloc((void**)&ctx->invalid, 4);
+  alloc((void**)&ctx->partials, size_t(ctx->energy_blocks) * (2 + 5 * TPICB200_MAX_SPECIES) * 8);
+  alloc((void**)&ctx->reduced, (2 + 5 * TPICB200_MAX_SPECIES + 2) * 8);
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&ctx->pinned, (2 + 5 * TPICB200_MAX_SPECIES + 2) * 8);
+  if (e == cudaSuccess) e = cudaMemset(ctx->invalid, 0, 4);
+  for (auto& ev : ctx->events)
+    if (e == cudaSuccess) e = cudaEventCreate(&ev);
+  if (e != cudaSuccess) {
+    tpicb200_destroy(ctx);
+    return cuda_status(e, "context allocation failed");
+  }
+  *out = ctx;
+  return TPICB200_SUCCESS;
+}
+
+int tpicb200_destroy(tpicb200_context* ctx) {
+  if (!ctx) return TPICB200_SUCCESS;
+  cudaDeviceSynchronize();
+  solver_destroy(ctx->solver);
+  cudaFree(ctx->cursor); cudaFree(ctx->perm); cudaFree(ctx->scan); cudaFree(ctx->invalid);
+  cudaFree(ctx->partials); cudaFree(ctx->reduced);
+  if (ctx->pinned) cudaFreeHost(ctx->pinned);
+  for (auto& ev : ctx->events)
+    if (ev) cudaEventDestroy(ev);
+  delete ctx;
+  return TPICB200_SUCCESS;
+}
+
+int tpicb200_get_layout(const tpicb200_context* ctx, tpicb200_layout* out) {
+  if (check_ctx(ctx) || !out) return fail(TPICB200_INVALID_ARGUMENT, "null layout argument");
+  out->node_count = ctx->g.nodes;
+  out->cell_count = ctx->g.cells;
+  out->bin_count = ctx->g.bins;
+  out->interior_nodes = ctx->g.interior;
+  const bool dbl = ctx->opt.precision == TPICB200_PRECISION_DOUBLE;
+  out->field_scalar_bytes = dbl ? 8 : 4;
+  out->mass_scalar_bytes = dbl ? 8 : 4;
+  out->velocity_scalar_bytes = dbl ? 8 : 4;
+  return TPICB200_SUCCESS;
+}
+
+int tpicb200_mover(tpicb200_context* ctx, double qom, tpicb200_particles* p, const double* e_theta,
+                   const void* b_node, uint32_t* invalid, tpicb200_stream stream) {
+  if (int s = check_ctx(ctx)) return s;
+  if (int s = check_particles(ctx, p)) return s;
+  if (!e_theta || !b_node || !std::isfinite(qom))
+    return fail(TPICB200_INVALID_ARGUMENT, "mover needs E_theta, B nodes and a finite q/m");
+  const double beta = qom * ctx->opt.dt / 2;
+  if (!std::isfinite(beta)) return fail(TPICB200_OVERFLOW, "q/m*dt/2 is not finite");
+  return cuda_status(launch_mover(ctx->opt.precision, ctx->g, qom, ctx->opt.dt, ctx->opt.c, p, e_theta,
+                                  b_node, invalid_or_own(ctx, invalid), (cudaStream_t)stream),
+                     "mover launch failed");
+}
+
+int tpicb200_sort(tpicb200_context* ctx, const tpicb200_particles* in, tpicb200_particles* out,
+                  uint32_t* counts, uint32_t* offsets, uint32_t* invalid, tpicb200_stream stream) {
+  if (int s = check_ctx(ctx)) return s;
+  if (int s = check_particles(ctx, in)) return s;
+  if (!out || !counts || !offsets) return fail(TPICB200_INVALID_ARGUMENT, "sort needs output records and bins");
+  if (in->count && (!out->rx || !out->ry || !out->rz || !out->u || !out->v || !out->w || !out->q ||
+                    !out->cell || (in->id && !out->id)))
+    return fail(TPICB200_INVALID_ARGUMENT, "null output attribute");
+  if (in->count && (in->rx == out->rx || in->cell == out->cell))
+    return fail(TPICB200_INVALID_ARGUMENT, "sort input and output alias");
+  return cuda_status(launch_sort(ctx->opt.precision, ctx->g, in, out, counts, offsets, ctx->cursor, ctx->perm,
+                                 ctx->scan, invalid_or_own(ctx, invalid), (cudaStream_t)stream),
+                     "sort launch failed");
+}
+
+int tpicb200_clear_moments(tpicb200_context* ctx, void* j, void* mass, tpicb200_stream stream) {
+  if (int s = check_ctx(ctx)) return s;
+  const size_t fb = ctx->opt.precision == TPICB200_PRECISION_DOUBLE ? 8 : 4;
+  cudaError_t e = cudaSuccess;
+  if (j) e = cudaMemsetAsync(j, 0, 3 * size_t(ctx->g.nodes) * fb, (cudaStream_t)stream);
+  if (mass && e == cudaSuccess) e = cudaMemsetAsync(mass, 0, 126 * size_t(ctx->g.nodes) * fb, (cudaStream_t)stream);
+  return cuda_status(e, "moment clear failed");
+}
+
+int tpicb200_deposit(tpicb200_context* ctx, double qom, const tpicb200_particles* p, const uint32_t* counts,
+                     const uint32_t* offsets, const void* b_node, void* j, void* mass, int mass_kind,
+                     uint32_t* invalid, tpicb200_stream stream) {
+  if (int s = check_ctx(ctx)) return s;
+  if (int s = check_particles(ctx, p)) return s;
+  if (!b_node || !std::isfinite(qom)) return fail(TPICB200_INVALID_ARGUMENT, "deposit needs B nodes and finite q/m");
+  if ((counts == nullptr) != (offsets == nullptr))
+    return fail(TPICB200_INVALID_ARGUMENT, "counts and offsets go together");
+  const bool dbl = ctx->opt.precision == TPICB200_PRECISION_DOUBLE;
+  if (mass_kind < TPICB200_MASS_SCALAR || mass_kind > TPICB200_MASS_BF16X3)
+    return fail(TPICB200_INVALID_ARGUMENT, "unknown mass kind");
+  if (dbl && mass_kind != TPICB200_MASS_SCALAR && mass_kind != TPICB200_MASS_SCALAR_F64)
+    return fail(TPICB200_INVALID_ARGUMENT, "tensor-core mass forms need the mixed precision mode");
+  const double boc = qom * ctx->opt.dt / 2 / ctx->opt.c;
+  if (!std::isfinite(boc)) return fail(TPICB200_OVERFLOW, "beta/c is not finite");
+  uint32_t* inv = invalid_or_own(ctx, invalid);
+  cudaStream_t s = (cudaStream_t)stream;
+  if (mass_kind == TPICB200_MASS_TF32 || mass_kind == TPICB200_MASS_BF16X3) {
+    if (!counts) return fail(TPICB200_INVALID_ARGUMENT, "tensor-core mass forms need sorted bins");
+    return cuda_status(launch_deposit_tc(mass_kind, ctx->g, qom, ctx->opt.dt, ctx->opt.c, p, counts, offsets,
+                                         b_node, j, mass, inv, s),
+                       "tensor-core deposition launch failed");
+  }
+  return cuda_status(launch_deposit(ctx->opt.precision, mass_kind, ctx->g, qom, ctx->opt.dt, ctx->opt.c, p,
+                                    counts, offsets, b_node, j, mass, inv, s),
+                     "deposition launch failed");
+}
+
+int tpicb200_fold_periodic(tpicb200_context* ctx, void* j, void* mass, tpicb200_stream stream) {
+  if (int s = check_ctx(ctx)) return s;
+  return cuda_status(launch_fold(ctx->opt.precision, ctx->g, j, mass, (cudaStream_t)stream), "fold launch failed");
+}
+
+int tpicb200_mass_apply(tpicb200_context* ctx, const void* mass, const double* in, double* out,
+                        tpicb200_stream stream) {
+  if (int s = check_ctx(ctx)) return s;
+  if (!mass || !in || !out || in == out) return fail(TPICB200_INVALID_ARGUMENT, "mass apply needs distinct fields");
+  return cuda_status(solver_mass_apply(ctx->solver, mass, in, out, (cudaStream_t)stream), "mass apply failed");
+}
+
+int tpicb200_field_solve(tpicb200_context* ctx, const void* e, const void* b_cell, const void* j,
+                         const void* mass, double* e_theta, tpicb200_gmres_result* result,
+                         tpicb200_stream stream) {
+  if (int s = check_ctx(ctx)) return s;
+  if (!e || !b_cell || !j || !mass || !e_theta) return fail(TPICB200_INVALID_ARGUMENT, "null field-solve argument");
+  cudaError_t err = cudaSuccess;
+  const int status = solver_solve(ctx->solver, e, b_cell, j, mass, e_theta, result, ctx->opt.gmres_max_iterations,
+                                  ctx->opt.gmres_tol, (cudaStream_t)stream, &err);
+  if (err != cudaSuccess) return cuda_status(err, "field solve failed");
+  if (status == TPICB200_NOT_CONVERGED) return fail(status, "GMRES did not converge");
+  if (status != TPICB200_SUCCESS) return fail(status, "field solve failed (non-finite residual)");
+  return status;
+}
+
+int tpicb200_field_advance(tpicb200_context* ctx, void* e, const void* b_cell, const double* e_theta,
+                           void* b_cell_next, void* b_node_next, tpicb200_stream stream) {
+  if (int s = check_ctx(ctx)) return s;
+  if (!e || !b_cell || !e_theta || !b_cell_next || !b_node_next || b_cell == b_cell_next)
+    return fail(TPICB200_INVALID_ARGUMENT, "null or aliased field-advance argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  const int p = ctx->opt.precision;
+  cudaError_t err = launch_field_advance(p, ctx->g, ctx->opt.theta, -ctx->opt.c * ctx->opt.dt, e, b_cell, e_theta,
+                                         b_cell_next, ctx->invalid, s);
+  if (err == cudaSuccess) err = launch_cell_ghosts(p, ctx->g, b_cell_next, s);
+  if (err == cudaSuccess) err = launch_cell_to_node(p, ctx->g, b_cell_next, b_node_next, s);
+  return cuda_status(err, "field advance failed");
+}
+
+int tpicb200_magnetic_to_nodes(tpicb200_context* ctx, void* b_cell, void* b_node, tpicb200_stream stream) {
+  if (int s = check_ctx(ctx)) return s;
+  if (!b_cell || !b_node) return fail(TPICB200_INVALID_ARGUMENT, "null magnetic field");
+  cudaError_t err = launch_cell_ghosts(ctx->opt.precision, ctx->g, b_cell, (cudaStream_t)stream);
+  if (err == cudaSuccess) err = launch_cell_to_node(ctx->opt.precision, ctx->g, b_cell, b_node, (cudaStream_t)stream);
+  return cuda_status(err, "cell-to-node failed");
+}
+
+int tpicb200_energy(tpicb200_context* ctx, const void* e, const void* b_cell, const tpicb200_particles* species,
+                    const double* qom, int ns, double* out, tpicb200_stream stream) {
+  if (int s = check_ctx(ctx)) return s;
+  if (!e || !b_cell || !out || ns < 0 || ns > TPICB200_MAX_SPECIES || (ns > 0 && (!species || !qom)))
+    return fail(TPICB200_INVALID_ARGUMENT, "invalid energy arguments");
+  cudaStream_t s = (cudaStream_t)stream;
+  const int blocks = ctx->energy_blocks;
+  cudaError_t err = launch_field_energy(ctx->opt.precision, ctx->g, e, b_cell, ctx->partials, blocks, s);
+  for (int sp = 0; sp < ns && err == cudaSuccess; ++sp)
+    err = launch_species_scalars(ctx->opt.precision, &species[sp], qom[sp],
+                                 ctx->partials + size_t(blocks) * (2 + 5 * sp), blocks, s);
+  const int rows = 2 + 5 * ns;
+  if (err == cudaSuccess) err = launch_reduce_rows(ctx->partials, ctx->reduced, rows, blocks, blocks, rows, s);
+  if (err == cudaSuccess) err = cudaMemcpyAsync(ctx->pinned, ctx->reduced, rows * 8, cudaMemcpyDeviceToHost, s);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+  if (err != cudaSuccess) return cuda_status(err, "energy reduction failed");
+  const double norm = ctx->g.volume / (8 * 3.14159265358979323846);
+  out[0] = norm * ctx->pinned[0];
+  out[1] = norm * ctx->pinned[1];
+  for (int r = 2; r < rows; ++r) out[r] = ctx->pinned[r];
+  return TPICB200_SUCCESS;
+}
+
+static int deposit_all(tpicb200_context* ctx, tpicb200_state* st, const void* b_node, cudaStream_t s) {
+  if (int r = tpicb200_clear_moments(ctx, st->j, st->mass, (tpicb200_stream)s)) return r;
+  for (int sp = 0; sp < st->ns; ++sp) {
+    const int cur = st->current[sp];
+    if (int r = tpicb200_deposit(ctx, st->qom[sp], &st->slot[sp][cur], st->counts[sp], st->offsets[sp], b_node,
+                                 st->j, st->mass, st->mass_kind, nullptr, (tpicb200_stream)s))
+      return r;
+  }
+  return tpicb200_fold_periodic(ctx, st->j, st->mass, (tpicb200_stream)s);
+}
+
+static int sort_all(tpicb200_context* ctx, tpicb200_state* st, cudaStream_t s) {
+  for (int sp = 0; sp < st->ns; ++sp) {
+    const int cur = st->current[sp];
+    tpicb200_particles* in = &st->slot[sp][cur];
+    tpicb200_particles* out = &st->slot[sp][1 - cur];
+    if (int r = tpicb200_sort(ctx, in, out, st->counts[sp], st->offsets[sp], nullptr, (tpicb200_stream)s)) return r;
+    st->current[sp] = 1 - cur;
+  }
+  return TPICB200_SUCCESS;
+}
+
+static int check_state(tpicb200_context* ctx, tpicb200_state* st) {
+  if (!st || st->ns <= 0 || st->ns > TPICB200_MAX_SPECIES)
+    return fail(TPICB200_INVALID_ARGUMENT, "invalid state or species count");
+  if (!st->e || !st->b_cell || !st->b_node || !st->b_cell_next || !st->b_node_next || !st->j || !st->mass ||
+      !st->e_theta)
+    return fail(TPICB200_INVALID_ARGUMENT, "null state field");
+  for (int sp = 0; sp < st->ns; ++sp) {
+    if (!st->counts[sp] || !st->offsets[sp] || (st->current[sp] != 0 && st->current[sp] != 1))
+      return fail(TPICB200_INVALID_ARGUMENT, "invalid species bins or slot");
+    if (int r = check_particles(ctx, &st->slot[sp][st->current[sp]])) return r;
+    st->slot[sp][1 - st->current[sp]].count = st->slot[sp][st->current[sp]].count;
+    if (int r = check_particles(ctx, &st->slot[sp][1 - st->current[sp]])) return r;
+  }
+  return TPICB200_SUCCESS;
+}
+
+int tpicb200_prepare(tpicb200_context* ctx, tpicb200_state* st, tpicb200_stream stream) {
+  if (int s = check_ctx(ctx)) return s;
+  if (int r = check_state(ctx, st)) return r;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (int r = tpicb200_magnetic_to_nodes(ctx, st->b_cell, st->b_node, stream)) return r;
+  if (int r = sort_all(ctx, st, s)) return r;
+  return deposit_all(ctx, st, st->b_node, s);
+}
+
+static int read_invalid(tpicb200_context* ctx, cudaStream_t s, uint32_t* value) {
+  cudaError_t err = cudaMemcpyAsync(ctx->pinned, ctx->invalid, 4, cudaMemcpyDeviceToHost, s);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+  if (err != cudaSuccess) return cuda_status(err, "invalid-flag readback failed");
+  std::memcpy(value, ctx->pinned, 4);
+  return TPICB200_SUCCESS;
+}
+
+int tpicb200_cycle(tpicb200_context* ctx, tpicb200_state* st, int ncycles, tpicb200_cycle_report* reports,
+                   tpicb200_stream stream) {
+  if (int s = check_ctx(ctx)) return s;
+  if (int r = check_state(ctx, st)) return r;
+  if (ncycles < 0) return fail(TPICB200_INVALID_ARGUMENT, "negative cycle count");
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaEvent_t* ev = ctx->events;
+  for (int cycle = 0; cycle < ncycles; ++cycle) {
+    tpicb200_cycle_report report{};
+    cudaEventRecord(ev[0], s);
+    // Field solve (reads the committed E^n, B^n and the assembled J-hat, M).
+    if (int r = tpicb200_field_solve(ctx, st->e, st->b_cell, st->j, st->mass, st->e_theta, &report.gmres, stream))
+      return r;
+    cudaEventRecord(ev[1], s);
+    // Movers gather the old B nodes and E_theta.
+    for (int sp = 0; sp < st->ns; ++sp)
+      if (int r = tpicb200_mover(ctx, st->qom[sp], &st->slot[sp][st->current[sp]], st->e_theta, st->b_node, nullptr,
+                                 stream))
+        return r;
+    cudaEventRecord(ev[2], s);
+    if (int r = tpicb200_field_advance(ctx, st->e, st->b_cell, st->e_theta, st->b_cell_next, st->b_node_next, stream))
+      return r;
+    cudaEventRecord(ev[3], s);
+    if (int r = sort_all(ctx, st, s)) return r;
+    cudaEventRecord(ev[4], s);
+    // Deposition of the moved records with the next B.
+    if (int r = deposit_all(ctx, st, st->b_node_next, s)) return r;
+    cudaEventRecord(ev[5], s);
+    std::swap(st->b_cell, st->b_cell_next);
+    std::swap(st->b_node, st->b_node_next);
+    if (reports) {
+      tpicb200_particles live[TPICB200_MAX_SPECIES];
+      for (int sp = 0; sp < st->ns; ++sp) live[sp] = st->slot[sp][st->current[sp]];
+      double out[2 + 5 * TPICB200_MAX_SPECIES];
+      if (int r = tpicb200_energy(ctx, st->e, st->b_cell, live, st->qom, st->ns, out, stream)) return r;
+      report.field_energy[0] = out[0];
+      report.field_energy[1] = out[1];
+      report.total_energy = out[0] + out[1];
+      for (int sp = 0; sp < st->ns; ++sp) {
+        for (int q = 0; q < 5; ++q) report.species[sp][q] = out[2 + 5 * sp + q];
+        report.total_energy += out[2 + 5 * sp];
+      }
+    }
+    cudaEventRecord(ev[6], s);
+    uint32_t bad = 0;
+    if (int r = read_invalid(ctx, s, &bad)) return r;
+    if (bad) return fail(TPICB200_INVALID_DATA, "the cycle raised the invalid-data flag");
+    for (int k = 0; k < 6; ++k) cudaEventElapsedTime(&report.stage_ms[k], ev[k], ev[k + 1]);
+    if (reports) reports[cycle] = report;
+  }
+  return TPICB200_SUCCESS;
+}
+
+}  // extern "C"

@@ -1,0 +1,64 @@
+// Host-side launch entry points of the kernel files (internal to the library).
+#pragma once
+
+#include "common.cuh"
+
+namespace tpicb200 {
+
+// mover.cu
+cudaError_t launch_mover(int precision, const Geom& g, double qom, double dt, double c,
+                         tpicb200_particles* p, const double* theta, const void* bnode,
+                         uint32_t* invalid, cudaStream_t s);
+
+// sort.cu: scratch needs `bins` cursor words, `capacity` permutation words and
+// the scan workspace returned by sort_scan_words().
+size_t sort_scan_words(long long bins);
+cudaError_t launch_sort(int precision, const Geom& g, const tpicb200_particles* in,
+                        tpicb200_particles* out, uint32_t* counts, uint32_t* offsets,
+                        uint32_t* cursor, uint32_t* perm, uint32_t* scan_scratch,
+                        uint32_t* invalid, cudaStream_t s);
+
+// deposit.cu
+cudaError_t launch_deposit(int precision, int mass_kind, const Geom& g, double qom, double dt,
+                           double c, const tpicb200_particles* p, const uint32_t* counts,
+                           const uint32_t* offsets, const void* bnode, void* j, void* mass,
+                           uint32_t* invalid, cudaStream_t s);
+cudaError_t launch_fold(int precision, const Geom& g, void* j, void* mass, cudaStream_t s);
+
+// mass_tc.cu (tcgen05 forms)
+cudaError_t launch_deposit_tc(int mass_kind, const Geom& g, double qom, double dt, double c,
+                              const tpicb200_particles* p, const uint32_t* counts,
+                              const uint32_t* offsets, const void* bnode, void* j, void* mass,
+                              uint32_t* invalid, cudaStream_t s);
+
+// fields.cu
+cudaError_t launch_node_ghosts(const Geom& g, double* f, int components, cudaStream_t s);
+cudaError_t launch_cell_ghosts(int precision, const Geom& g, void* f, cudaStream_t s);
+cudaError_t launch_cell_to_node(int precision, const Geom& g, const void* cellf, void* node,
+                                cudaStream_t s);
+cudaError_t launch_rhs(int precision, const Geom& g, double delta, double kfac, const void* e,
+                       const void* bcell, const void* j, double* rhs, cudaStream_t s);
+cudaError_t launch_field_advance(int precision, const Geom& g, double theta_value, double faraday,
+                                 void* e, const void* bcell, const double* etheta, void* bnext,
+                                 uint32_t* invalid, cudaStream_t s);
+cudaError_t launch_field_energy(int precision, const Geom& g, const void* e, const void* bcell,
+                                double* partials, int blocks, cudaStream_t s);
+cudaError_t launch_species_scalars(int precision, const tpicb200_particles* p, double qom,
+                                   double* partials, int blocks, cudaStream_t s);
+cudaError_t launch_reduce_rows(const double* partials, double* out, int rows, int row_stride,
+                               int count, int filled, cudaStream_t s);
+cudaError_t launch_copy_node_field(const Geom& g, const void* in, int in_double, double* out,
+                                   cudaStream_t s);
+
+// solver.cu
+struct SolverWorkspace;
+SolverWorkspace* solver_create(int precision, const Geom& g, int restart, double dt,
+                               double theta, double c, cudaError_t* err);
+void solver_destroy(SolverWorkspace* w);
+int solver_solve(SolverWorkspace* w, const void* e, const void* bcell, const void* j,
+                 const void* mass, double* etheta, tpicb200_gmres_result* result,
+                 int max_iterations, double tol, cudaStream_t s, cudaError_t* err);
+cudaError_t solver_mass_apply(SolverWorkspace* w, const void* mass, const double* in, double* out,
+                              cudaStream_t s);
+
+}  // namespace tpicb200

@@ -1,0 +1,573 @@
+// Matrix-free field solve: the implicit Maxwell operator
+//   A(v) = v + delta^2 curl_C2N(curl_N2C v) + k (M v)/V
+// fused into one kernel per interior node, and restarted GMRES with FP64
+// reductions, device-side Givens rotations and two scalars read back per
+// Arnoldi step, restating Gmres::host_blocking_solve
+// (ecsim/gmres/gmres_device.hpp:353-454) and its kernels (:137-292).
+//
+// The reference applies A in four launches with three intermediate fields
+// (N2C curl, C2N curl, M v, combination; ecsim/maxwell/maxwell_device.hpp:433-484).
+// Here one thread evaluates the eight cell curls around its node in
+// registers, the C2N curl of those, the 27-block mass product and the
+// combination ((1*v + delta^2*curl) + k*Mv) in the same arithmetic type and
+// order, and stores the image straight into the compact Krylov vector: the
+// M records (504 B/node FP32, 1008 B/node FP64) are the only HBM stream.
+#include "kernels.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <limits>
+#include <vector>
+
+namespace tpicb200 {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kDotTile = 4;
+
+__device__ __forceinline__ void compact_coordinates(const Geom& g, long long t, int& i, int& j, int& k) {
+  i = int(t % g.inx);
+  j = int((t / g.inx) % g.iny);
+  k = int(t / ((long long)g.inx * g.iny));
+}
+
+// curl_N2C at cell (i,j,k) of the double node field `v` in arithmetic C.
+template <class C>
+__device__ __forceinline__ void cell_curl(const Geom& g, const double* __restrict__ v, int i, int j, int k,
+                                          const C inv[3], C out[3]) {
+  const long long nn = g.nodes;
+  const long long b = g.node(i, j, k), sy = g.NX, sz = (long long)g.NX * g.NY;
+  C s[3][8];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const double* p = v + c * nn + b;
+    s[c][0] = C(p[0]); s[c][1] = C(p[1]); s[c][2] = C(p[sy]); s[c][3] = C(p[sz]);
+    s[c][4] = C(p[1 + sy]); s[c][5] = C(p[1 + sz]); s[c][6] = C(p[sy + sz]); s[c][7] = C(p[1 + sy + sz]);
+  }
+  auto dx = [&](const C* q) { return C(0.25) * inv[0] * (q[1] - q[0] + (q[5] - q[3]) + (q[4] - q[2]) + (q[7] - q[6])); };
+  auto dy = [&](const C* q) { return C(0.25) * inv[1] * (q[2] - q[0] + (q[6] - q[3]) + (q[4] - q[1]) + (q[7] - q[5])); };
+  auto dz = [&](const C* q) { return C(0.25) * inv[2] * (q[3] - q[0] + (q[5] - q[1]) + (q[6] - q[2]) + (q[7] - q[4])); };
+  out[0] = dy(s[2]) - dz(s[1]);
+  out[1] = dz(s[0]) - dx(s[2]);
+  out[2] = dx(s[1]) - dy(s[0]);
+}
+
+template <class C, class M>
+__device__ __forceinline__ void block_product(const M* __restrict__ b, C vx, C vy, C vz, C& x, C& y, C& z) {
+  x = vx * C(b[0]) + vy * C(b[1]) + vz * C(b[2]);
+  y = vx * C(b[3]) + vy * C(b[4]) + vz * C(b[5]);
+  z = vx * C(b[6]) + vy * C(b[7]) + vz * C(b[8]);
+}
+
+// (M v)_g before the row volume scale: centre, then per stencil the forward
+// neighbour with this vertex's block and the backward neighbour with the
+// neighbour vertex's block, untransposed (apply_mass_matrix_node,
+// ecsim/mass_matrix/mass_matrix_stencil.hpp:119-149).
+template <class C, class M>
+__device__ __forceinline__ void mass_product(const Geom& g, const M* __restrict__ mass,
+                                             const double* __restrict__ v, int i, int j, int k, C out[3]) {
+  const long long nn = g.nodes;
+  const long long at = g.node(i, j, k);
+  C x, y, z;
+  block_product<C>(mass + at * 126, C(v[at]), C(v[nn + at]), C(v[2 * nn + at]), x, y, z);
+#pragma unroll
+  for (int s = 1; s < 14; ++s) {
+    const long long d = stencil_offset(s, 0) + (long long)g.NX * (stencil_offset(s, 1) + (long long)g.NY * stencil_offset(s, 2));
+    C bx, by, bz;
+    const long long f = at + d, b = at - d;
+    block_product<C>(mass + at * 126 + s * 9, C(v[f]), C(v[nn + f]), C(v[2 * nn + f]), bx, by, bz);
+    x += bx; y += by; z += bz;
+    block_product<C>(mass + b * 126 + s * 9, C(v[b]), C(v[nn + b]), C(v[2 * nn + b]), bx, by, bz);
+    x += bx; y += by; z += bz;
+  }
+  out[0] = x; out[1] = y; out[2] = z;
+}
+
+template <class C, class M, class Out>
+__global__ void __launch_bounds__(kThreads) maxwell_apply_kernel(Geom g, C d2, C kfac, C inv_volume,
+                                                                 const M* __restrict__ mass,
+                                                                 const double* __restrict__ v,
+                                                                 Out* __restrict__ out) {
+  const C inv[3] = {C(g.inv[0]), C(g.inv[1]), C(g.inv[2])};
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < g.interior;
+       t += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    compact_coordinates(g, t, i, j, k);
+    // Cell curls: base (i,j,k), x (i-1), y (j-1), z (k-1), xy, xz, yz, xyz.
+    C cc[8][3];
+    cell_curl<C>(g, v, i, j, k, inv, cc[0]);
+    cell_curl<C>(g, v, i - 1, j, k, inv, cc[1]);
+    cell_curl<C>(g, v, i, j - 1, k, inv, cc[2]);
+    cell_curl<C>(g, v, i, j, k - 1, inv, cc[3]);
+    cell_curl<C>(g, v, i - 1, j - 1, k, inv, cc[4]);
+    cell_curl<C>(g, v, i - 1, j, k - 1, inv, cc[5]);
+    cell_curl<C>(g, v, i, j - 1, k - 1, inv, cc[6]);
+    cell_curl<C>(g, v, i - 1, j - 1, k - 1, inv, cc[7]);
+    // C2N curl of the cell curls (cell sources: anchor - neighbour).
+    auto dx = [&](int c) { return C(0.25) * inv[0] * (cc[0][c] - cc[1][c] + (cc[3][c] - cc[5][c]) + (cc[2][c] - cc[4][c]) + (cc[6][c] - cc[7][c])); };
+    auto dy = [&](int c) { return C(0.25) * inv[1] * (cc[0][c] - cc[2][c] + (cc[3][c] - cc[6][c]) + (cc[1][c] - cc[4][c]) + (cc[5][c] - cc[7][c])); };
+    auto dz = [&](int c) { return C(0.25) * inv[2] * (cc[0][c] - cc[3][c] + (cc[1][c] - cc[5][c]) + (cc[2][c] - cc[6][c]) + (cc[4][c] - cc[7][c])); };
+    const C curl2[3] = {dy(2) - dz(1), dz(0) - dx(2), dx(1) - dy(0)};
+    C mv[3];
+    mass_product<C>(g, mass, v, i, j, k, mv);
+    const long long at = g.node(i, j, k);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      // The mass image is narrowed to the solver storage (double) before the
+      // combination reads it back (maxwell_device.hpp:424-429,471-484).
+      const C m = C(double(mv[c] * inv_volume));
+      const C value = (C(1) * C(v[c * g.nodes + at]) + d2 * C(double(curl2[c]))) + kfac * m;
+      out[c * g.interior + t] = Out(value);
+    }
+  }
+}
+
+template <class M>
+__global__ void __launch_bounds__(kThreads) mass_apply_kernel(Geom g, double inv_volume, const M* __restrict__ mass,
+                                                              const double* __restrict__ v, double* __restrict__ out) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < g.interior;
+       t += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    compact_coordinates(g, t, i, j, k);
+    double mv[3];
+    mass_product<double>(g, mass, v, i, j, k, mv);
+    const long long at = g.node(i, j, k);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) out[c * g.nodes + at] = mv[c] * inv_volume;
+  }
+}
+
+// Compact vector <-> node field interiors (gmres_field_vector_transfer_kernel,
+// gmres_device.hpp:137-157).
+template <class V>
+__global__ void __launch_bounds__(kThreads) pack_kernel(Geom g, const double* __restrict__ f, V* __restrict__ vec) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < g.interior;
+       t += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    compact_coordinates(g, t, i, j, k);
+    const long long at = g.node(i, j, k);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) vec[c * g.interior + t] = V(f[c * g.nodes + at]);
+  }
+}
+template <class V>
+__global__ void __launch_bounds__(kThreads) unpack_kernel(Geom g, const V* __restrict__ vec, double* __restrict__ f) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < g.interior;
+       t += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    compact_coordinates(g, t, i, j, k);
+    const long long at = g.node(i, j, k);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) f[c * g.nodes + at] = double(vec[c * g.interior + t]);
+  }
+}
+template <class T>
+__global__ void __launch_bounds__(kThreads) pack_storage_kernel(Geom g, const T* __restrict__ f, double* __restrict__ vec) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < g.interior;
+       t += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    compact_coordinates(g, t, i, j, k);
+    const long long at = g.node(i, j, k);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) vec[c * g.interior + t] = double(f[c * g.nodes + at]);
+  }
+}
+
+// Dots of `image` with basis columns [first, first+4) per block row,
+// block partials per column (gmres_dot_batch_kernel, gmres_device.hpp:163-192).
+template <class S>
+__global__ void __launch_bounds__(kThreads) dot_batch_kernel(const S* __restrict__ basis, const S* __restrict__ image,
+                                                             double* __restrict__ partials, long long count,
+                                                             int columns) {
+  __shared__ double scratch[kDotTile][kThreads / 32];
+  for (int first = blockIdx.y * kDotTile; first < columns; first += gridDim.y * kDotTile) {
+    double sum[kDotTile] = {0, 0, 0, 0};
+    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < count;
+         n += (long long)gridDim.x * blockDim.x) {
+      const double value = double(image[n]);
+#pragma unroll
+      for (int r = 0; r < kDotTile; ++r)
+        if (first + r < columns) sum[r] += double(basis[(long long)(first + r) * count + n]) * value;
+    }
+#pragma unroll
+    for (int r = 0; r < kDotTile; ++r)
+      if (first + r < columns) {
+        const double total = block_sum<kThreads>(sum[r], scratch[r]);
+        if (threadIdx.x == 0) partials[(long long)(first + r) * gridDim.x + blockIdx.x] = total;
+      }
+    __syncthreads();
+  }
+}
+
+// r = b - image with block partials of |r|^2 (and |b|^2)
+// (gmres_residual_squared_norm_kernel, gmres_device.hpp:197-216).
+template <bool RhsNorm>
+__global__ void __launch_bounds__(kThreads) residual_kernel(const double* __restrict__ b, const double* __restrict__ image,
+                                                            double* __restrict__ r, double* __restrict__ partials,
+                                                            long long count) {
+  __shared__ double scratch[2][kThreads / 32];
+  double s0 = 0, s1 = 0;
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < count;
+       n += (long long)gridDim.x * blockDim.x) {
+    const double bv = b[n];
+    const double value = bv - image[n];
+    r[n] = value;
+    s0 += value * value;
+    if (RhsNorm) s1 += bv * bv;
+  }
+  s0 = block_sum<kThreads>(s0, scratch[0]);
+  if (RhsNorm) s1 = block_sum<kThreads>(s1, scratch[1]);
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x] = s0;
+    if (RhsNorm) partials[gridDim.x + blockIdx.x] = s1;
+  }
+}
+
+// Classical Gram-Schmidt with the reduced dots, squared-norm partials of the
+// stored result; block 0 copies the dots into the Hessenberg column
+// (gmres_orthogonalize_squared_norm_kernel, gmres_device.hpp:243-263).
+template <class S>
+__global__ void __launch_bounds__(kThreads) orthogonalize_kernel(const S* __restrict__ basis, const double* __restrict__ dots,
+                                                                 S* __restrict__ image, double* __restrict__ column,
+                                                                 double* __restrict__ partials, long long count,
+                                                                 int columns) {
+  __shared__ double scratch[kThreads / 32];
+  double norm2 = 0;
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < count;
+       n += (long long)gridDim.x * blockDim.x) {
+    double value = double(image[n]);
+    for (int c = 0; c < columns; ++c) value -= dots[c] * double(basis[(long long)c * count + n]);
+    const S stored = S(value);
+    image[n] = stored;
+    norm2 += double(stored) * double(stored);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0)
+    for (int row = 0; row < columns; ++row) column[row] = dots[row];
+  const double total = block_sum<kThreads>(norm2, scratch);
+  if (threadIdx.x == 0) partials[blockIdx.x] = total;
+}
+
+struct ArnoldiTail {
+  double* column;
+  double* cosine;
+  double* sine;
+  double* rhs;
+  double* status;
+  int step;  // -1: restart tail (rhs[0] = norm)
+};
+
+// Restart tail and Arnoldi least-squares update
+// (RestartRhsTail / ArnoldiLeastSquaresUpdate, gmres_device.hpp:52-98).
+__device__ void run_tail(const ArnoldiTail& t, double norm2) {
+  if (t.step < 0) {
+    t.rhs[0] = sqrt(norm2);
+    return;
+  }
+  const int step = t.step;
+  const double sub = sqrt(norm2);
+  double* column = t.column;
+  column[step + 1] = sub;
+  for (int row = 0; row < step; ++row) {
+    const double upper = column[row], lower = column[row + 1];
+    column[row] = t.cosine[row] * upper + t.sine[row] * lower;
+    column[row + 1] = -t.sine[row] * upper + t.cosine[row] * lower;
+  }
+  const double diagonal = column[step];
+  const double den = hypot(diagonal, sub);
+  const double c = den != 0.0 ? diagonal / den : 1.0;
+  const double s = den != 0.0 ? sub / den : 0.0;
+  t.cosine[step] = c;
+  t.sine[step] = s;
+  column[step] = c * diagonal + s * sub;
+  column[step + 1] = 0.0;
+  const double upper = t.rhs[step], lower = t.rhs[step + 1];
+  t.rhs[step] = c * upper + s * lower;
+  t.rhs[step + 1] = -s * upper + c * lower;
+  t.status[0] = fabs(t.rhs[step + 1]);
+  t.status[1] = sub == 0.0 ? 1.0 : 0.0;
+}
+
+// target = source / sqrt(norm2[0]) (zero for a zero norm), also stored into
+// the operator input field (gmres_normalize_kernel, gmres_device.hpp:224-237).
+template <class Src, class S>
+__global__ void __launch_bounds__(kThreads) normalize_kernel(Geom g, const Src* __restrict__ source,
+                                                             const double* __restrict__ norm2, S* __restrict__ target,
+                                                             double* __restrict__ input, ArnoldiTail tail) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) run_tail(tail, norm2[0]);
+  const double n2 = norm2[0];
+  const double scale = n2 > 0.0 ? 1.0 / sqrt(n2) : 0.0;
+  const long long count = 3 * g.interior;
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < count;
+       n += (long long)gridDim.x * blockDim.x) {
+    const S value = S(double(source[n]) * scale);
+    target[n] = value;
+    const long long c = n / g.interior, t = n - c * g.interior;
+    int i, j, k;
+    compact_coordinates(g, t, i, j, k);
+    input[c * g.nodes + g.node(i, j, k)] = double(value);
+  }
+}
+
+// gmres_back_substitute_kernel, gmres_device.hpp:267-277 (one thread).
+__global__ void back_substitute_kernel(const double* hessenberg, const double* rhs, double* coefficients,
+                                       int leading, int columns) {
+  for (int row = columns - 1; row >= 0; --row) {
+    double sum = 0;
+    for (int column = row + 1; column < columns; ++column)
+      sum += hessenberg[(long long)column * leading + row] * coefficients[column];
+    const double diagonal = hessenberg[(long long)row * leading + row];
+    coefficients[row] = diagonal != 0.0 ? (rhs[row] - sum) / diagonal : 0.0;
+  }
+}
+
+// x += sum of coefficient * basis column (gmres_update_solution_kernel, :281-292).
+template <class S>
+__global__ void __launch_bounds__(kThreads) update_solution_kernel(const S* __restrict__ basis,
+                                                                   const double* __restrict__ coefficients,
+                                                                   double* __restrict__ x, long long count,
+                                                                   int columns) {
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < count;
+       n += (long long)gridDim.x * blockDim.x) {
+    double value = x[n];
+    for (int c = 0; c < columns; ++c) value += coefficients[c] * double(basis[(long long)c * count + n]);
+    x[n] = value;
+  }
+}
+
+}  // namespace
+
+struct SolverWorkspace {
+  int precision;
+  Geom g;
+  int restart;
+  double dt, theta, c, delta, kfac;
+  long long count;  // 3 * interior
+  unsigned rblocks;
+  void* basis = nullptr;   // (restart+1) * count Scalar
+  void* image = nullptr;   // count Scalar
+  double* x = nullptr;
+  double* b = nullptr;
+  double* r = nullptr;
+  double* ximage = nullptr;
+  double* input = nullptr;  // node field (3 * nodes)
+  double* rhs = nullptr;    // node field
+  double* values = nullptr;
+  double* partials = nullptr;
+  double* state = nullptr;
+  double* pinned = nullptr;
+  int batch;
+  size_t scalar_bytes;
+
+  double* hessenberg() { return state; }
+  double* cosine() { return state + (size_t)restart * (restart + 1); }
+  double* sine() { return cosine() + restart; }
+  double* ls_rhs() { return sine() + restart; }
+  double* coefficients() { return ls_rhs() + restart + 1; }
+  double* status() { return coefficients() + restart; }
+  template <class S> S* basis_col(int c) { return (S*)basis + (size_t)c * count; }
+};
+
+SolverWorkspace* solver_create(int precision, const Geom& g, int restart, double dt, double theta,
+                               double c, cudaError_t* err) {
+  auto* w = new SolverWorkspace();
+  w->precision = precision;
+  w->g = g;
+  w->restart = restart;
+  w->dt = dt;
+  w->theta = theta;
+  w->c = c;
+  w->delta = c * theta * dt;
+  w->kfac = 4 * 3.14159265358979323846 * (theta * dt);
+  w->count = 3 * g.interior;
+  int device = 0, sms = 148;
+  cudaGetDevice(&device);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  w->rblocks = unsigned(std::min<long long>((w->count + kThreads - 1) / kThreads, 4LL * sms));
+  w->batch = std::max(restart, 2);
+  w->scalar_bytes = precision == TPICB200_PRECISION_DOUBLE ? 8 : 4;
+  cudaError_t e = cudaSuccess;
+  auto alloc = [&](void** p, size_t bytes) {
+    if (e == cudaSuccess) e = cudaMalloc(p, bytes);
+  };
+  alloc(&w->basis, (size_t)(restart + 1) * w->count * w->scalar_bytes);
+  alloc(&w->image, (size_t)w->count * w->scalar_bytes);
+  alloc((void**)&w->x, w->count * sizeof(double));
+  alloc((void**)&w->b, w->count * sizeof(double));
+  alloc((void**)&w->r, w->count * sizeof(double));
+  alloc((void**)&w->ximage, w->count * sizeof(double));
+  alloc((void**)&w->input, 3 * g.nodes * sizeof(double));
+  alloc((void**)&w->rhs, 3 * g.nodes * sizeof(double));
+  alloc((void**)&w->values, w->batch * sizeof(double));
+  alloc((void**)&w->partials, (size_t)w->batch * w->rblocks * sizeof(double));
+  alloc((void**)&w->state, ((size_t)restart * (restart + 1) + 4 * restart + 3) * sizeof(double));
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&w->pinned, 2 * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemset(w->input, 0, 3 * g.nodes * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemset(w->rhs, 0, 3 * g.nodes * sizeof(double));
+  *err = e;
+  if (e != cudaSuccess) {
+    solver_destroy(w);
+    return nullptr;
+  }
+  return w;
+}
+
+void solver_destroy(SolverWorkspace* w) {
+  if (!w) return;
+  cudaFree(w->basis); cudaFree(w->image); cudaFree(w->x); cudaFree(w->b); cudaFree(w->r);
+  cudaFree(w->ximage); cudaFree(w->input); cudaFree(w->rhs); cudaFree(w->values);
+  cudaFree(w->partials); cudaFree(w->state);
+  if (w->pinned) cudaFreeHost(w->pinned);
+  delete w;
+}
+
+namespace {
+
+template <class P>
+struct Solve {
+  using S = typename P::EC;     // Krylov basis and Arnoldi arithmetic
+  using Mass = typename P::Mass;
+  using Fld = typename P::Fld;
+  static constexpr bool refined = sizeof(S) < sizeof(double);
+
+  SolverWorkspace* w;
+  cudaStream_t s;
+  cudaError_t err = cudaSuccess;
+
+  unsigned blocks() const { return grid_for(w->g.interior, kThreads); }
+  void check() { if (err == cudaSuccess) err = cudaGetLastError(); }
+
+  template <class C, class Out> void apply(const Mass* mass, Out* out) {
+    launch_node_ghosts(w->g, w->input, 3, s);
+    const double iv = w->g.inv_volume;
+    maxwell_apply_kernel<C, Mass, Out><<<blocks(), kThreads, 0, s>>>(
+        w->g, C(w->delta * w->delta), C(w->kfac), C(iv), mass, w->input, out);
+    check();
+  }
+  void reduce(int filled) {
+    launch_reduce_rows(w->partials, w->values, w->batch, w->rblocks, w->rblocks, filled, s);
+  }
+  bool read_controls(const double* src, double out[2]) {
+    if (err != cudaSuccess) return false;
+    err = cudaMemcpyAsync(w->pinned, src, 2 * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+    out[0] = w->pinned[0];
+    out[1] = w->pinned[1];
+    return err == cudaSuccess;
+  }
+  void apply_solution(const Mass* mass) {
+    unpack_kernel<double><<<blocks(), kThreads, 0, s>>>(w->g, w->x, w->input);
+    apply<double, double>(mass, w->ximage);
+  }
+
+  int run(const void* e, const void* bcell, const void* j, const void* mass_v, double* etheta,
+          tpicb200_gmres_result* result, int max_iterations, double tolerance) {
+    const Geom& g = w->g;
+    const Mass* mass = (const Mass*)mass_v;
+    const long long N = w->count;
+    const int m = w->restart;
+    tpicb200_gmres_result res{};
+    // Initial guess E^n (the copy of E into theta, maxwell_device.hpp:134-147) and the RHS.
+    pack_storage_kernel<Fld><<<blocks(), kThreads, 0, s>>>(g, (const Fld*)e, w->x);
+    launch_rhs(P::id, g, w->delta, w->kfac, e, bcell, j, w->rhs, s);
+    pack_kernel<double><<<blocks(), kThreads, 0, s>>>(g, w->rhs, w->b);
+    check();
+    apply_solution(mass);
+    residual_kernel<true><<<w->rblocks, kThreads, 0, s>>>(w->b, w->ximage, w->r, w->partials, N);
+    reduce(2);
+    double controls[2];
+    if (!read_controls(w->values, controls)) return TPICB200_BACKEND_FAILURE;
+    if (!std::isfinite(controls[0]) || !std::isfinite(controls[1])) return TPICB200_OVERFLOW;
+    res.residual = res.initial_residual = std::sqrt(controls[0]);
+    res.rhs_norm = std::sqrt(controls[1]);
+    const double scale = res.rhs_norm == 0.0 ? 1.0 : res.rhs_norm;
+    const double atol = scale * tolerance;
+    auto converged = [&] {
+      res.relative_residual = res.residual / scale;
+      res.converged = res.residual <= atol;
+    };
+    converged();
+    while (!res.converged && res.iterations < max_iterations) {
+      cudaMemsetAsync(w->state, 0, ((size_t)m * (m + 1) + 4 * m + 3) * sizeof(double), s);
+      // values[0] holds |r|^2 of the residual just formed.
+      normalize_kernel<double, S><<<w->rblocks, kThreads, 0, s>>>(
+          g, w->r, w->values, w->template basis_col<S>(0), w->input,
+          ArnoldiTail{nullptr, nullptr, nullptr, w->ls_rhs(), nullptr, -1});
+      check();
+      const int columns = std::min(m, max_iterations - res.iterations);
+      const double cycle_tolerance =
+          refined ? std::max(atol, res.residual * 16.0 * double(std::numeric_limits<S>::epsilon())) : atol;
+      int completed = 0;
+      bool breakdown = false;
+      for (int col = 0; col < columns; ++col) {
+        S* image = (S*)w->image;
+        apply<S, S>(mass, image);
+        const dim3 grid(w->rblocks, (col + 1 + kDotTile - 1) / kDotTile);
+        dot_batch_kernel<S><<<grid, kThreads, 0, s>>>(w->template basis_col<S>(0), image, w->partials, N, col + 1);
+        reduce(col + 1);
+        double* h_column = w->hessenberg() + (size_t)col * (m + 1);
+        orthogonalize_kernel<S><<<w->rblocks, kThreads, 0, s>>>(w->template basis_col<S>(0), w->values, image,
+                                                               h_column, w->partials, N, col + 1);
+        reduce(1);
+        normalize_kernel<S, S><<<w->rblocks, kThreads, 0, s>>>(
+            g, image, w->values, w->template basis_col<S>(col + 1), w->input,
+            ArnoldiTail{h_column, w->cosine(), w->sine(), w->ls_rhs(), w->status(), col});
+        check();
+        double st[2];
+        if (!read_controls(w->status(), st)) return TPICB200_BACKEND_FAILURE;
+        if (!std::isfinite(st[0]) || !std::isfinite(st[1])) return TPICB200_OVERFLOW;
+        completed = col + 1;
+        breakdown = st[1] != 0.0;
+        if (st[0] <= cycle_tolerance || breakdown) break;
+      }
+      back_substitute_kernel<<<1, 1, 0, s>>>(w->hessenberg(), w->ls_rhs(), w->coefficients(), m + 1, completed);
+      update_solution_kernel<S><<<grid_for(N, kThreads), kThreads, 0, s>>>(w->template basis_col<S>(0),
+                                                                          w->coefficients(), w->x, N, completed);
+      check();
+      res.iterations += completed;
+      apply_solution(mass);
+      residual_kernel<false><<<w->rblocks, kThreads, 0, s>>>(w->b, w->ximage, w->r, w->partials, N);
+      reduce(1);
+      if (!read_controls(w->values, controls)) return TPICB200_BACKEND_FAILURE;
+      if (!std::isfinite(controls[0]) || controls[0] < 0) return TPICB200_OVERFLOW;
+      res.residual = std::sqrt(controls[0]);
+      converged();
+      if (breakdown && !res.converged) break;
+    }
+    if (result) *result = res;
+    if (!res.converged) return TPICB200_NOT_CONVERGED;
+    unpack_kernel<double><<<blocks(), kThreads, 0, s>>>(g, w->x, etheta);
+    launch_node_ghosts(g, etheta, 3, s);
+    check();
+    return err == cudaSuccess ? TPICB200_SUCCESS : TPICB200_BACKEND_FAILURE;
+  }
+};
+
+}  // namespace
+
+int solver_solve(SolverWorkspace* w, const void* e, const void* bcell, const void* j, const void* mass,
+                 double* etheta, tpicb200_gmres_result* result, int max_iterations, double tol,
+                 cudaStream_t s, cudaError_t* err) {
+  int status;
+  if (w->precision == TPICB200_PRECISION_DOUBLE) {
+    Solve<PDouble> solve{w, s};
+    status = solve.run(e, bcell, j, mass, etheta, result, max_iterations, tol);
+    *err = solve.err;
+  } else {
+    Solve<PMixed> solve{w, s};
+    status = solve.run(e, bcell, j, mass, etheta, result, max_iterations, tol);
+    *err = solve.err;
+  }
+  return status;
+}
+
+cudaError_t solver_mass_apply(SolverWorkspace* w, const void* mass, const double* in, double* out,
+                              cudaStream_t s) {
+  const unsigned blocks = grid_for(w->g.interior, kThreads);
+  if (w->precision == TPICB200_PRECISION_DOUBLE)
+    mass_apply_kernel<double><<<blocks, kThreads, 0, s>>>(w->g, w->g.inv_volume, (const double*)mass, in, out);
+  else
+    mass_apply_kernel<float><<<blocks, kThreads, 0, s>>>(w->g, w->g.inv_volume, (const float*)mass, in, out);
+  return cudaGetLastError();
+}
+
+}  // namespace tpicb200

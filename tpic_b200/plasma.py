@@ -1,0 +1,174 @@
+"""Seeded synthetic plasmas for the ECSIM cycle.
+
+TPIC loads particles with cuRAND's XORWOW stream
+(initialization/particles/particle_loading_device.hpp:32-53); that generator
+is not reproduced. This module defines its own counter-based stream,
+Philox-4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy
+as 1, 2, 3", SC'11), so that the same host arrays feed the CUDA path, the CPU
+oracle and every test, bit for bit.
+
+Per particle with global load index `n` of species `s`:
+  block A = philox((n_lo, n_hi, s, 0), seed) -> subcell offsets x, y, z and u1
+  block B = philox((n_lo, n_hi, s, 1), seed) -> u2, u3, u4
+  uniforms are (r + 0.5) * 2**-32, normals come from Box-Muller:
+  (n0, n1) from (u1, u2), n2 from (u3, u4).
+The load order follows TPIC's dense path (particle_loading_device.hpp:85-120):
+cell = n // ppc (x fastest), subcell = n % ppc (x fastest), fraction =
+(subcell + offset) / npcel on each axis, a stored fraction of exactly one
+carries into the next cell; velocity = drift + thermal * normal; macro-charge
+q = sign(qom) * V/ppc * rho/(4 pi) (src/initialization/prepared_initialization.cpp:36-70).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+M0, M1 = 0xD2511F53, 0xCD9E8D57
+W0, W1 = 0x9E3779B9, 0xBB67AE85
+MASK = 0xFFFFFFFF
+
+
+def philox4x32(c0, c1, c2, c3, k0: int, k1: int, xp=np):
+    """Philox-4x32-10 on int64 arrays holding 32-bit words (numpy or torch).
+
+    The 32x32-bit products may wrap in int64; their low 64 bits are exact, and
+    the arithmetic shift followed by the 32-bit mask recovers the high word."""
+    for _ in range(10):
+        p0 = c0 * M0
+        p1 = c2 * M1
+        hi0, lo0 = (p0 >> 32) & MASK, p0 & MASK
+        hi1, lo1 = (p1 >> 32) & MASK, p1 & MASK
+        c0, c1, c2, c3 = hi1 ^ c1 ^ k0, lo1, hi0 ^ c3 ^ k1, lo0
+        k0 = (k0 + W0) & MASK
+        k1 = (k1 + W1) & MASK
+    return c0, c1, c2, c3
+
+
+def _uniform(r, xp=np):
+    return (r.astype(xp.float64) if xp is np else r.to(dtype=xp.float64)) * 2.0**-32 + 2.0**-33
+
+
+@dataclass
+class SpeciesSpec:
+    qom: float
+    rho: float = 1.0
+    npcel: tuple = (2, 2, 2)
+    vth: tuple = (0.0, 0.0, 0.0)
+    drift: tuple = (0.0, 0.0, 0.0)
+
+    @property
+    def ppc(self) -> int:
+        return int(self.npcel[0] * self.npcel[1] * self.npcel[2])
+
+
+@dataclass
+class GridSpec:
+    nx: int
+    ny: int
+    nz: int
+    lx: float
+    ly: float
+    lz: float
+
+    @property
+    def spacing(self):
+        return (self.lx / self.nx, self.ly / self.ny, self.lz / self.nz)
+
+    @property
+    def cells(self) -> int:
+        return self.nx * self.ny * self.nz
+
+    def encode(self, i, j, k):
+        return (i + 2) + (self.nx + 4) * ((j + 2) + (self.ny + 4) * (k + 2))
+
+
+def generate_species(grid: GridSpec, sp: SpeciesSpec, species_index: int, seed: int = 0,
+                     velocity_dtype=np.float64, first: int = 0, count: int | None = None,
+                     xp=np, device=None) -> dict:
+    """Records [first, first+count) of one uniform species, in load order.
+
+    xp = numpy (host arrays) or torch (device arrays on `device`); both give
+    the same integer stream, and the same values up to the last bit of the
+    transcendental functions of Box-Muller.
+    """
+    ppc = sp.ppc
+    total = grid.cells * ppc
+    if count is None:
+        count = total - first
+    k0, k1 = seed & MASK, (seed >> 32) & MASK
+    if xp is np:
+        n = np.arange(first, first + count, dtype=np.int64)
+        zeros = np.zeros_like(n)
+        ones = np.ones_like(n)
+        sidx = np.full_like(n, species_index)
+    else:
+        n = xp.arange(first, first + count, dtype=xp.int64, device=device)
+        zeros = xp.zeros_like(n)
+        ones = xp.ones_like(n)
+        sidx = xp.full_like(n, species_index)
+    lo, hi = n & MASK, (n >> 32) & MASK
+    a = philox4x32(lo, hi, sidx, zeros, k0, k1, xp)
+    b = philox4x32(lo, hi, sidx, ones, k0, k1, xp)
+    cell = n // ppc
+    sub = n % ppc
+    npx, npy, npz = sp.npcel
+    sub_x, sub_y, sub_z = sub % npx, (sub // npx) % npy, sub // (npx * npy)
+    ci, cj, ck = cell % grid.nx, (cell // grid.nx) % grid.ny, cell // (grid.nx * grid.ny)
+    out = {}
+    cells = [ci, cj, ck]
+    fr = []
+    for axis, (s, r, npc) in enumerate(zip((sub_x, sub_y, sub_z), a[:3], (npx, npy, npz))):
+        off = _uniform(r, xp)
+        sf = s.astype(np.float64) if xp is np else s.to(xp.float64)
+        f = (sf + off) * (1.0 / npc)
+        carry = f >= 1.0
+        f = xp.where(carry, xp.zeros_like(f), f)
+        cells[axis] = cells[axis] + (carry.astype(np.int64) if xp is np else carry.to(xp.int64))
+        fr.append(f)
+    extents = (grid.nx, grid.ny, grid.nz)
+    for axis in range(3):
+        cells[axis] = cells[axis] % extents[axis]
+    u1, u2, u3, u4 = _uniform(a[3], xp), _uniform(b[0], xp), _uniform(b[1], xp), _uniform(b[2], xp)
+    r12 = xp.sqrt(-2.0 * xp.log(u1))
+    r34 = xp.sqrt(-2.0 * xp.log(u3))
+    normals = (r12 * xp.cos(2.0 * math.pi * u2), r12 * xp.sin(2.0 * math.pi * u2),
+               r34 * xp.cos(2.0 * math.pi * u4))
+    vel = []
+    for axis in range(3):
+        value = sp.drift[axis] + sp.vth[axis] * normals[axis]
+        vel.append(value.astype(velocity_dtype) if xp is np else value.to(velocity_dtype))
+    dx, dy, dz = grid.spacing
+    volume = (dx * dy) * dz
+    q = (1.0 if sp.qom > 0 else -1.0) * volume / ppc * (sp.rho / (4 * math.pi))
+    key = grid.encode(cells[0], cells[1], cells[2])
+    if xp is np:
+        out.update(rx=fr[0], ry=fr[1], rz=fr[2], u=vel[0], v=vel[1], w=vel[2],
+                   q=np.full(count, q, dtype=np.float64), cell=key.astype(np.int32),
+                   id=n.astype(np.uint64))
+    else:
+        out.update(rx=fr[0], ry=fr[1], rz=fr[2], u=vel[0], v=vel[1], w=vel[2],
+                   q=xp.full((count,), q, dtype=xp.float64, device=device), cell=key.to(xp.int32),
+                   id=n.clone())
+    return out
+
+
+@dataclass
+class FieldInit:
+    e0: tuple = (0.0, 0.0, 0.0)
+    b0: tuple = (0.0, 0.0, 0.0)
+
+
+@dataclass
+class Case:
+    """A periodic ECSIM run: grid, species, time integration and fields."""
+    grid: GridSpec
+    species: list
+    dt: float
+    theta: float = 0.5
+    c: float = 1.0
+    gmres_tol: float = 1e-8
+    ncycles: int = 1
+    fields: FieldInit = field(default_factory=FieldInit)
+    seed: int = 0
