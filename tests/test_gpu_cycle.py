@@ -1,0 +1,80 @@
+"""Whole-cycle parity: the CUDA cycle driver (tpicb200_prepare / tpicb200_cycle)
+against the oracle's cycle on the same seeded plasma, and energy conservation
+to the GMRES tolerance as the ECSIM method guarantees."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle as O
+from fieldutil import interior_nodes
+from tpic_b200.plasma import Case, FieldInit, GridSpec, SpeciesSpec, generate_species
+
+pytestmark = pytest.mark.gpu
+
+
+def c1_case(n=16, ncycles=3, npcel=(3, 3, 3)):
+    """Plain ECSIM FP64 uniform plasma: 16^3 cells, 10^3 d_i, electrons q/m=-64,
+    ions q/m=1, 27 ppc/species, vth_e=0.045, vth_i=0.0056, B0=(0,0,0.0195),
+    dt=0.15, theta=0.5, GMRES rtol 1e-8."""
+    g = GridSpec(n, n, n, 10.0, 10.0, 10.0)
+    sp = [SpeciesSpec(qom=-64.0, rho=1.0, npcel=npcel, vth=(0.045,) * 3),
+          SpeciesSpec(qom=1.0, rho=1.0, npcel=npcel, vth=(0.0056,) * 3)]
+    return Case(g, sp, dt=0.15, theta=0.5, gmres_tol=1e-8, ncycles=ncycles, fields=FieldInit(b0=(0.0, 0.0, 0.0195)))
+
+
+def run_both(case, precision, cycles, mass_kind="scalar"):
+    from tpic_b200.simulation import Simulation
+    sim = Simulation(case, precision={0: "double", 1: "mixed"}[precision], mass_kind=mass_kind)
+    sim.prepare()
+    reports = sim.run(cycles)
+    arrays = O.case_species_arrays(case, precision, generate_species)
+    oc = O.OracleCycle(case.grid, arrays, case.dt, case.theta, case.c, case.gmres_tol, precision, b0=case.fields.b0)
+    oc.prepare()
+    energies = [oc.cycle() for _ in range(cycles)]
+    return sim, reports, oc, energies
+
+
+def test_c1_cycle_matches_oracle_fp64():
+    case = c1_case(n=16)
+    sim, reports, oc, energies = run_both(case, 0, 3)
+    for r, e, og in zip(reports, energies, oc.gmres):
+        assert r.gmres_iterations == og.iterations
+        assert abs(r.total_energy - O.total_energy(e, 2)) <= 1e-10 * abs(O.total_energy(e, 2))
+        assert abs(r.field_energy[0] - e[0]) <= 1e-9 * abs(e[0]) + 1e-15
+    for s in range(2):
+        live = {k: v.cpu().numpy() for k, v in sim.live(s).items()}
+        want = oc.species[s][1]
+        assert np.array_equal(live["cell"], want["cell"])
+        assert np.allclose(live["rx"], want["rx"], rtol=0, atol=1e-11)
+        assert np.allclose(live["u"], want["u"], rtol=1e-9, atol=1e-13)
+    g = case.grid
+    e_gpu = interior_nodes(g, sim.field("e").cpu().numpy())
+    e_cpu = interior_nodes(g, oc.e)
+    assert np.abs(e_gpu - e_cpu).max() <= 3e-10 * np.abs(e_cpu).max() + 3e-12
+
+
+def test_c1_energy_conserved_fp64():
+    case = c1_case(n=16)
+    from tpic_b200.simulation import Simulation
+    sim = Simulation(case, precision="double")
+    sim.prepare()
+    w0 = sim.energy()
+    total0 = w0[0] + w0[1] + w0[2] + w0[7]
+    reports = sim.run(3)
+    for r in reports:
+        assert abs(r.total_energy - total0) <= 1e-9 * total0
+        assert r.gmres_relative_residual <= 1e-8
+
+
+@pytest.mark.parametrize("mass_kind", ["scalar", "scalar-f64"])
+def test_c1_mixed_precision_energy(mass_kind):
+    case = c1_case(n=16)
+    from tpic_b200.simulation import Simulation
+    sim = Simulation(case, precision="mixed", mass_kind=mass_kind)
+    sim.prepare()
+    w0 = sim.energy()
+    total0 = w0[0] + w0[1] + w0[2] + w0[7]
+    reports = sim.run(3)
+    for r in reports:
+        assert abs(r.total_energy - total0) <= 1e-6 * total0

@@ -1,0 +1,401 @@
+"""Stage-by-stage parity of the CUDA path (through the C ABI) with the CPU
+oracle on the same seeded inputs.
+
+Bars: mover cell keys, fractions and velocities bit-exact; sort permutation,
+counts and offsets bit-exact (stable order); current and mass within TPIC's
+sorted-mass tolerances (3e-12*max|coef| + 1e-15 FP64, 3e-5*max|coef| + 1e-15
+FP32, docs/developer/testing.md:255-260); fields within rtol 3e-10 / atol
+3e-12 (FP64 storage) and 3e-5 / 3e-7 (FP32), testing.md:262-273.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle as O
+from fieldutil import (bits, interior_nodes, interior_records, periodic_cell_field, periodic_node_field,
+                       smooth_random_unique)
+from tpic_b200.plasma import GridSpec, SpeciesSpec, generate_species
+
+pytestmark = pytest.mark.gpu
+
+GRID = GridSpec(6, 5, 4, 3.0, 2.5, 2.0)
+
+
+def ogrid(g):
+    return O.OGrid(g.nx, g.ny, g.nz, g.lx / g.nx, g.ly / g.ny, g.lz / g.nz)
+
+
+def species_arrays(g, precision, seed=3, vth=(0.6, 0.5, 0.4), npcel=(2, 2, 2), qom=-4.0):
+    vdt = np.float64 if precision == 0 else np.float32
+    d = generate_species(g, SpeciesSpec(qom=qom, npcel=npcel, vth=vth), 0, seed=seed, velocity_dtype=vdt)
+    return d
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    assert torch.cuda.is_available()
+    return torch
+
+
+def make_ctx(g, precision, **kw):
+    from gpu_helpers import StageContext
+    return StageContext(g, precision=precision, **kw)
+
+
+def oracle_mover(g, precision, qom, dt, d, etheta, bnode):
+    lib = O.load()
+    a = {k: np.ascontiguousarray(v.copy()) for k, v in d.items()}
+    bad = lib.oracle_mover(precision, C.byref(ogrid(g)), qom, dt, 1.0, *[O.ptr(a[k]) for k in
+                           ("rx", "ry", "rz", "u", "v", "w", "q", "cell")], len(a["cell"]), O.ptr(etheta),
+                           O.ptr(bnode))
+    return a, bad
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_mover_bit_exact(torch_cuda, precision):
+    g = GRID
+    rng = np.random.default_rng(11)
+    d = species_arrays(g, precision)
+    n = len(d["cell"])
+    ctx = make_ctx(g, precision, dt=0.3)
+    etheta = periodic_node_field(g, smooth_random_unique(g, rng, 0.4))
+    bnode = periodic_node_field(g, smooth_random_unique(g, rng, 0.9)).astype(ctx.np_fdt)
+    parts = ctx.upload_particles(d)
+    ctx.mover(-4.0, parts, n, ctx.field(etheta, np.float64), ctx.field(bnode))
+    got = ctx.download(parts, n)
+    want, bad = oracle_mover(g, precision, -4.0, 0.3, d, etheta, bnode)
+    assert bad == 0 and ctx.invalid_count() == 0
+    assert np.array_equal(got["cell"], want["cell"])
+    for k in ("rx", "ry", "rz", "u", "v", "w"):
+        assert np.array_equal(bits(got[k]), bits(want[k])), k
+    # The flight crossed cells and periodic boundaries.
+    assert np.mean(got["cell"] != d["cell"]) > 0.3
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_mover_edge_records(torch_cuda, precision):
+    """Endpoint fractions, sub-ULP negative crossings and invalid records
+    (which keep every attribute), as sorted_current_mover_device.cpp:126-140,241-259."""
+    g = GridSpec(3, 2, 2, 3.0, 2.0, 2.0)
+    vdt = np.float64 if precision == 0 else np.float32
+    n = 10
+    key = lambda i, j, k: g.encode(i, j, k)
+    d = {
+        "rx": np.array([0.0, 1 - 2**-53, 0.0, 2**-60, 0.25, 0.5, 0.5, 1.0, 0.5, 0.5]),
+        "ry": np.full(n, 0.5), "rz": np.full(n, 0.5),
+        "u": np.array([0.0, 0.0, -1e-17, -2**-70, 7.3, -9.1, 0.0, 0.0, np.nan, 0.0], dtype=vdt),
+        "v": np.array([0.0, 1e-3, 0.0, 0.0, -3.3, 2.2, 0.0, 0.0, 0.0, 0.0], dtype=vdt),
+        "w": np.zeros(n, dtype=vdt), "q": np.full(n, -0.1),
+        "cell": np.array([key(0, 0, 0), key(2, 1, 1), key(0, 0, 0), key(0, 1, 0), key(1, 1, 1), key(2, 0, 1),
+                          key(-1, 0, 0), key(1, 0, 0), key(1, 1, 0), 10**6], dtype=np.int32),
+    }
+    d["rx"][5] = 0.0
+    ctx = make_ctx(g, precision, dt=0.5)
+    etheta = np.zeros(3 * ctx.layout.node_count)
+    bnode = np.zeros(3 * ctx.layout.node_count, dtype=ctx.np_fdt)
+    parts = ctx.upload_particles(d)
+    ctx.mover(-1.0, parts, n, ctx.field(etheta, np.float64), ctx.field(bnode))
+    got = ctx.download(parts, n)
+    want, bad = oracle_mover(g, precision, -1.0, 0.5, d, etheta, bnode)
+    assert bad == 4 and ctx.invalid_count() == 4  # halo key, fraction 1, NaN velocity, key out of range
+    assert np.array_equal(got["cell"], want["cell"])
+    for k in ("rx", "ry", "rz", "u", "v", "w"):
+        assert np.array_equal(bits(got[k]), bits(want[k])), k
+    for r in (6, 7, 8, 9):  # invalid records are unchanged
+        assert got["cell"][r] == d["cell"][r] and bits(got["rx"])[r] == bits(d["rx"])[r]
+    assert ((got["rx"][:6] >= 0) & (got["rx"][:6] < 1)).all()
+
+
+def oracle_sort(g, keys):
+    lib = O.load()
+    n = len(keys)
+    nb = lib.oracle_bin_count(C.byref(ogrid(g)))
+    perm = np.empty(max(n, 1), np.uint32)
+    counts = np.empty(nb, np.uint32)
+    offsets = np.empty(nb + 1, np.uint32)
+    assert lib.oracle_sort(C.byref(ogrid(g)), O.ptr(np.ascontiguousarray(keys)), n, O.ptr(perm), O.ptr(counts),
+                           O.ptr(offsets)) == 0
+    return perm[:n], counts, offsets
+
+
+def run_sort_case(g, keys, precision=0):
+    n = len(keys)
+    vdt = np.float64 if precision == 0 else np.float32
+    idx = np.arange(n)
+    d = {"rx": idx * 0.125, "ry": idx * -0.25, "rz": idx * 0.5, "u": (idx * -0.5).astype(vdt),
+         "v": (idx * 0.25).astype(vdt), "w": (idx * -0.125).astype(vdt), "q": idx * 2.0,
+         "cell": np.asarray(keys, dtype=np.int32), "id": (idx + 100).astype(np.uint64)}
+    ctx = make_ctx(g, precision, max_particles=max(n, 1))
+    src = ctx.upload_particles(d) if n else ctx.empty_particles(0, True)
+    dst, counts, offsets = ctx.sort(src, n, with_id=True)
+    got = ctx.download(dst, n)
+    perm, wc, wo = oracle_sort(g, d["cell"])
+    assert ctx.invalid_count() == 0
+    assert np.array_equal(counts.cpu().numpy().view(np.uint32), wc)
+    assert np.array_equal(offsets.cpu().numpy().view(np.uint32), wo)
+    for k in ("rx", "ry", "rz", "u", "v", "w", "q", "cell", "id"):
+        assert np.array_equal(got[k], d[k][perm]), k
+    # The attribute mapping of particle_sort_device.cpp:96-131 holds.
+    ident = got["id"].astype(np.int64) - 100
+    assert np.array_equal(got["rx"], ident * 0.125) and np.array_equal(got["q"], ident * 2.0)
+    assert (np.diff(got["cell"]) >= 0).all()
+
+
+def test_sort_stable_random(torch_cuda):
+    g = GridSpec(8, 7, 6, 1.0, 1.0, 1.0)
+    rng = np.random.default_rng(5)
+    i, j, k = rng.integers(0, 8, 40000), rng.integers(0, 7, 40000), rng.integers(0, 6, 40000)
+    run_sort_case(g, g.encode(i, j, k))
+
+
+def test_sort_nearly_sorted_and_fixture_keys(torch_cuda):
+    g = GridSpec(16, 8, 8, 1.0, 1.0, 1.0)
+    rng = np.random.default_rng(9)
+    i = np.repeat(np.arange(16 * 8 * 8), 50)
+    keys = g.encode(i % 16, (i // 16) % 8, i // 128)
+    moved = rng.random(len(keys)) < 0.08
+    keys = np.where(moved, g.encode(rng.integers(0, 16, len(keys)), rng.integers(0, 8, len(keys)),
+                                    rng.integers(0, 8, len(keys))), keys)
+    run_sort_case(g, keys, precision=1)
+    # The reference fixture: key = (i*7+3) % 19 (particle_sort_device.cpp:67).
+    run_sort_case(GridSpec(2, 2, 2, 1.0, 1.0, 1.0), (np.arange(1000) * 7 + 3) % 19)
+
+
+@pytest.mark.parametrize("n", [0, 1, 33, 300, 9000, 20000])
+def test_sort_one_bin_and_empty(torch_cuda, n):
+    g = GridSpec(3, 3, 3, 1.0, 1.0, 1.0)
+    rng = np.random.default_rng(n)
+    keys = np.full(n, g.encode(1, 2, 0))
+    if n > 3:  # a few foreign keys interleaved so the big bin is not already in order after placement
+        keys[rng.integers(0, n, n // 10)] = g.encode(0, 0, 0)
+    run_sort_case(g, keys)
+
+
+def test_sort_rejects_out_of_range_key(torch_cuda):
+    g = GridSpec(3, 3, 3, 1.0, 1.0, 1.0)
+    ctx = make_ctx(g, 0, max_particles=10)
+    d = {k: np.zeros(4) for k in ("rx", "ry", "rz", "u", "v", "w", "q")}
+    d["cell"] = np.array([5, 6, -1, 7], dtype=np.int32)
+    src = ctx.upload_particles(d)
+    ctx.sort(src, 4)
+    assert ctx.invalid_count() == 1
+
+
+# --------------------------------------------------------------------------
+def oracle_moments(g, precision, qom, dt, d, bnode):
+    lib = O.load()
+    og = ogrid(g)
+    nodes = lib.oracle_node_count(C.byref(og))
+    j = np.zeros(3 * nodes)
+    m = np.zeros(126 * nodes)
+    bad = lib.oracle_deposit(precision, C.byref(og), qom, dt, 1.0, *[O.ptr(np.ascontiguousarray(d[k])) for k in
+                             ("rx", "ry", "rz", "u", "v", "w", "q", "cell")], len(d["cell"]),
+                             O.ptr(np.ascontiguousarray(bnode)), O.ptr(j), O.ptr(m))
+    lib.oracle_fold(C.byref(og), O.ptr(j), O.ptr(m))
+    return j, m, bad
+
+
+def assert_moments(g, jg, mg, jw, mw, rel):
+    jw_i, jg_i = interior_nodes(g, jw), interior_nodes(g, jg)
+    scale = np.abs(jw_i).max()
+    assert np.abs(jg_i - jw_i).max() <= rel * scale + 1e-15
+    mw_i, mg_i = interior_records(g, mw), interior_records(g, mg)
+    scale = np.abs(mw_i).max()
+    assert np.abs(mg_i - mw_i).max() <= rel * scale + 1e-15
+
+
+@pytest.mark.parametrize("precision,kind,sorted_bins", [(0, 0, True), (0, 0, False), (1, 0, True), (1, 0, False),
+                                                        (1, 1, True), (0, 1, True)])
+def test_deposit_matches_oracle(torch_cuda, precision, kind, sorted_bins):
+    g = GRID
+    rng = np.random.default_rng(21)
+    d = species_arrays(g, precision, vth=(0.2, 0.1, 0.3), npcel=(3, 3, 3))
+    n = len(d["cell"])
+    ctx = make_ctx(g, precision, dt=0.2)
+    bnode = periodic_node_field(g, smooth_random_unique(g, rng, 0.9)).astype(ctx.np_fdt)
+    parts = ctx.upload_particles(d)
+    bn = ctx.field(bnode)
+    j, m = ctx.moments()
+    if sorted_bins:
+        parts, counts, offsets = ctx.sort(parts, n)
+        ctx.deposit(-4.0, parts, n, bn, j, m, counts, offsets, kind=kind)
+    else:
+        ctx.deposit(-4.0, parts, n, bn, j, m, kind=kind)
+    ctx.fold(j, m)
+    jw, mw, bad = oracle_moments(g, precision, -4.0, 0.2, d, bnode)
+    assert bad == 0 and ctx.invalid_count() == 0
+    rel = 3e-12 if precision == 0 else 3e-5
+    assert_moments(g, j.cpu().numpy().astype(np.float64), m.cpu().numpy().astype(np.float64), jw, mw, rel)
+
+
+def reference_mass_fixture(precision):
+    """sorted_mass_device.cpp:190-297 ordinary case: a thin 4x2x2 grid, 16
+    cells with occupancies {0,1,3,4,5,31,32,33,65,129,257,64,127,128,130,19},
+    fractions (n%17)/17, (n%13)/13, (n%11)/11, charges, beta = -0.07 and
+    linear nodal B profiles."""
+    g = GridSpec(4, 2, 2, 4.0, 2.0, 2.0)
+    occupancy = [0, 1, 3, 4, 5, 31, 32, 33, 65, 129, 257, 64, 127, 128, 130, 19]
+    rx, ry, rz, q, keys = [], [], [], [], []
+    for compact, occ in enumerate(occupancy):
+        i, j, k = compact % 4, (compact // 4) % 2, compact // 8
+        for n in range(occ):
+            rx.append((n % 17) / 17.0)
+            ry.append((n % 13) / 13.0)
+            rz.append((n % 11) / 11.0)
+            q.append((-0.3 if n % 7 == 0 else 0.8) * (1 + 0.05 * compact))
+            keys.append(g.encode(i, j, k))
+    total = len(keys)
+    vdt = np.float64 if precision == 0 else np.float32
+    d = {"rx": np.array(rx), "ry": np.array(ry), "rz": np.array(rz), "u": np.zeros(total, vdt),
+         "v": np.zeros(total, vdt), "w": np.zeros(total, vdt), "q": np.array(q), "cell": np.array(keys, np.int32)}
+    nodes = (g.nz + 3) * (g.ny + 3) * (g.nx + 3)
+    b = np.zeros((3, g.nz + 3, g.ny + 3, g.nx + 3))
+    for k in range(3):
+        for j in range(3):
+            for i in range(5):
+                b[0, k + 1, j + 1, i + 1] = 0.2 + 0.07 * i - 0.03 * j + 0.01 * k
+                b[1, k + 1, j + 1, i + 1] = -0.4 + 0.02 * i + 0.05 * j - 0.04 * k
+                b[2, k + 1, j + 1, i + 1] = 0.7 - 0.01 * i + 0.03 * j + 0.02 * k
+    assert b.size == 3 * nodes
+    return g, d, b.ravel()
+
+
+def host_matrix_core_mass(g, d, bnode, beta):
+    """Restatement of the fixture oracle host_matrix_core_mass,
+    sorted_mass_device.cpp:111-182: an FP64 8x8x9 tensor per cell, flushed to
+    the canonical pairs, then summed over periodic copies (this build keeps
+    the reference's cell-local nodes only inside the fold)."""
+    nodes = (g.nz + 3) * (g.ny + 3) * (g.nx + 3)
+    b = bnode.reshape(3, g.nz + 3, g.ny + 3, g.nx + 3)
+    result = np.zeros(126 * nodes)
+    stencil = [[O.load().oracle_pair_stencil(a, bb) for bb in range(8)] for a in range(8)]
+    cells = {}
+    for n, key in enumerate(d["cell"]):
+        cells.setdefault(int(key), []).append(n)
+    for key, members in cells.items():
+        yz = key // (g.nx + 4)
+        i, j, k = key % (g.nx + 4) - 2, yz % (g.ny + 4) - 2, yz // (g.ny + 4) - 2
+        tensor = np.zeros((8, 8, 9))
+        for n in members:
+            x, y, z = d["rx"][n], d["ry"][n], d["rz"][n]
+            w = np.array([((x if a & 1 else 1.0 - x) * (y if a & 2 else 1.0 - y)) * (z if a & 4 else 1.0 - z)
+                          for a in range(8)])
+            field = np.zeros(3)
+            for a in range(8):
+                at = (k + ((a >> 2) & 1) + 1, j + ((a >> 1) & 1) + 1, i + (a & 1) + 1)
+                field += w[a] * b[:, at[0], at[1], at[2]]
+            x_, y_, z_ = beta * field
+            inv = 1.0 / (1.0 + (x_ * x_ + y_ * y_ + z_ * z_))
+            alpha = np.array([(1 + x_ * x_) * inv, x_ * y_ * inv + z_ * inv, x_ * z_ * inv - y_ * inv,
+                              x_ * y_ * inv - z_ * inv, (1 + y_ * y_) * inv, y_ * z_ * inv + x_ * inv,
+                              x_ * z_ * inv + y_ * inv, y_ * z_ * inv - x_ * inv, (1 + z_ * z_) * inv])
+            scale = beta * d["q"][n]
+            tensor += (alpha * scale)[None, None, :] * (w[:, None] * w[None, :])[:, :, None]
+        for a in range(8):
+            vertex = (i + (a & 1) + 1) + (g.nx + 3) * ((j + ((a >> 1) & 1) + 1) + (g.ny + 3) * (k + ((a >> 2) & 1) + 1))
+            for bb in range(8):
+                s = stencil[a][bb]
+                if s >= 0:
+                    result[vertex * 126 + s * 9: vertex * 126 + s * 9 + 9] += tensor[a, bb]
+    O.load().oracle_fold(C.byref(ogrid(g)), 0, O.ptr(result))
+    return result
+
+
+@pytest.mark.parametrize("precision,kind", [(0, 0), (1, 0), (1, 1)])
+def test_reference_mass_fixture(torch_cuda, precision, kind):
+    g, d, bnode = reference_mass_fixture(precision)
+    n = len(d["cell"])
+    ctx = make_ctx(g, precision, dt=0.14, max_particles=n)
+    parts = ctx.upload_particles(d)
+    parts, counts, offsets = ctx.sort(parts, n)  # the fixture is already in key order
+    _, m = ctx.moments()
+    ctx.deposit(-1.0, parts, n, ctx.field(bnode), None, m, counts, offsets, kind=kind)
+    ctx.fold(None, m)
+    want = host_matrix_core_mass(g, d, bnode, -0.07)
+    got = m.cpu().numpy().astype(np.float64)
+    wi, gi = interior_records(g, want), interior_records(g, got)
+    rel = 3e-12 if precision == 0 else 3e-5
+    assert ctx.invalid_count() == 0
+    assert np.abs(gi - wi).max() <= rel * np.abs(wi).max() + 1e-15
+
+
+def test_mass_apply_matches_oracle(torch_cuda):
+    g = GRID
+    rng = np.random.default_rng(2)
+    nodes = (g.nz + 3) * (g.ny + 3) * (g.nx + 3)
+    unique = rng.normal(size=(126, g.nz, g.ny, g.nx))
+    m = periodic_node_field_records(g, unique)
+    v = periodic_node_field(g, smooth_random_unique(g, rng, 1.0))
+    ctx = make_ctx(g, 0)
+    out = ctx.mass_apply(ctx.field(m), ctx.field(v, np.float64)).cpu().numpy()
+    want = np.zeros(3 * nodes)
+    O.load().oracle_mass_apply(0, C.byref(ogrid(g)), O.ptr(m), O.ptr(v), O.ptr(want))
+    assert np.allclose(interior_nodes(g, out), interior_nodes(g, want), rtol=1e-13, atol=1e-13)
+    ref = O.load_reference()
+    if ref is not None:  # the reference's own apply_mass_matrix_node at a few nodes
+        for (i, j, k) in [(0, 0, 0), (6, 5, 4), (3, 2, 1)]:
+            o = np.zeros(3)
+            ref.ref_mass_apply_node(g.nx, g.ny, g.nz, O.ptr(m), O.ptr(v), 1.0 / ((0.5 * 0.5) * 0.5), i, j, k, O.ptr(o))
+            assert np.allclose(interior_nodes(g, out)[:, k, j, i], o, rtol=1e-13, atol=1e-13)
+
+
+def periodic_node_field_records(g, unique):
+    k = (np.arange(-1, g.nz + 2) % g.nz)[:, None, None]
+    j = (np.arange(-1, g.ny + 2) % g.ny)[None, :, None]
+    i = (np.arange(-1, g.nx + 2) % g.nx)[None, None, :]
+    return np.stack([unique[e][k, j, i] for e in range(126)], axis=-1).ravel()
+
+
+# --------------------------------------------------------------------------
+def prepared_oracle(g, precision, seed=1):
+    from tpic_b200.plasma import generate_species as gen
+    species = [SpeciesSpec(qom=-16.0, npcel=(2, 2, 2), vth=(0.08,) * 3), SpeciesSpec(qom=1.0, npcel=(2, 2, 2),
+                                                                                      vth=(0.01,) * 3)]
+    arrays = []
+    for s, sp in enumerate(species):
+        dd = gen(g, sp, s, seed=seed, velocity_dtype=np.float64 if precision == 0 else np.float32)
+        dd.pop("id")
+        arrays.append((sp.qom, dd))
+    oc = O.OracleCycle(g, arrays, 0.2, 0.5, 1.0, 1e-10, precision, b0=(0.1, -0.05, 0.2))
+    oc.prepare()
+    return oc
+
+
+def test_field_solve_matches_oracle(torch_cuda):
+    g = GRID
+    oc = prepared_oracle(g, 0)
+    rng = np.random.default_rng(4)
+    oc.e = periodic_node_field(g, smooth_random_unique(g, rng, 0.01))
+    bcell = periodic_cell_field(g, smooth_random_unique(g, rng, 0.05))
+    oc.b = bcell
+    ctx = make_ctx(g, 0, dt=0.2, tol=1e-10)
+    et, res = ctx.field_solve(ctx.field(oc.e), ctx.field(bcell), ctx.field(oc.j), ctx.field(oc.m))
+    ores = oc.solve()
+    assert res.converged and res.relative_residual <= 1e-10
+    assert res.iterations == ores.iterations
+    got, want = interior_nodes(g, et.cpu().numpy()), interior_nodes(g, oc.theta_field)
+    assert np.abs(got - want).max() <= 3e-10 * np.abs(want).max() + 3e-12
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_field_advance_matches_oracle(torch_cuda, precision):
+    g = GRID
+    rng = np.random.default_rng(8)
+    ctx = make_ctx(g, precision, dt=0.2)
+    fdt = ctx.np_fdt
+    e = periodic_node_field(g, smooth_random_unique(g, rng, 0.3)).astype(fdt)
+    b = periodic_cell_field(g, smooth_random_unique(g, rng, 0.3)).astype(fdt)
+    th = periodic_node_field(g, smooth_random_unique(g, rng, 0.3))
+    et = ctx.field(e)
+    bnext, bnode = ctx.field_advance(et, ctx.field(b), ctx.field(th, np.float64))
+    we, wb, wbn = e.astype(np.float64), np.zeros(b.size), np.zeros(e.size)
+    O.load().oracle_field_advance(C.byref(ogrid(g)), 0.2, 0.5, 1.0, O.ptr(we), O.ptr(b.astype(np.float64)),
+                                  O.ptr(th), O.ptr(wb), O.ptr(wbn))
+    rtol, atol = (3e-10, 3e-12) if precision == 0 else (3e-5, 3e-7)
+    assert np.allclose(interior_nodes(g, et.cpu().numpy()), interior_nodes(g, we), rtol=rtol, atol=atol)
+    assert np.allclose(bnext.cpu().numpy(), wb, rtol=rtol, atol=atol)
+    assert np.allclose(bnode.cpu().numpy(), wbn, rtol=rtol, atol=atol)

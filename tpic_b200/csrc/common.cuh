@@ -120,8 +120,9 @@ __host__ __device__ constexpr int pair_stencil(int a, int b) {
 }
 
 __device__ __forceinline__ int wrap_index(int i, int n) {
-  // Periodic unique index in [0, n) for i in [-n, 2n).
-  return i < 0 ? i + n : (i >= n ? i - n : i);
+  // Periodic unique index in [0, n) (n = 1 maps the ghost n+1 = 2 to 0 too).
+  const int r = i % n;
+  return r < 0 ? r + n : r;
 }
 
 // The non-unique vertices of a node field: every vertex of the (n+3)^3 box
