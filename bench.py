@@ -1,0 +1,389 @@
+#!/usr/bin/env python
+"""Benchmark of the single-GPU ECSIM particle cycle (particles*cycles/s).
+
+Workload (default): the 3-D uniform thermal plasma at scale -- 128^3 cells,
+box 20^3 d_i, electrons (q/m = -64) and ions (q/m = 1), 64 particles per cell
+per species (268,435,456 particles), Maxwellian vth_e = 0.045c, vth_i =
+0.0056c, B0 = (0, 0, 0.0195), FP64 positions / FP32 velocities (mixed
+precision), dt = 0.15/omega_pi, theta = 0.5, GMRES rtol 1e-8 -- seeded
+synthetic inputs from tpic_b200.plasma (no dataset is involved).
+
+A step is one full ECSIM cycle (solve, move, field advance, stable sort,
+current + mass deposition, fold, commit, energy diagnostics) through the C
+ABI's tpicb200_cycle. Inputs stay resident in HBM (13 GB of particle
+records per slot, far larger than the 126 MB L2).
+
+  python bench.py [--gpus N --steps K --warmup W] [--mass-matrix scalar|scalar-f64|tf32|bf16x3]
+  python bench.py --impl reference ...   (the CPU implementation of the path)
+
+N > 1 runs N independent replicas (the path is timed on one GPU; the
+replicas share nothing), launched by torchrun; rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import multiprocessing as mp
+import os
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "particles*cycles/s on 1 B200, tensor-core vs plain FP32 assembly at equal energy error"
+UNIT = "particles*cycles/s"
+PEAKS = ROOT / "MEASURED_PEAKS.json"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def workload(scale: int = 128, ppc_axis: int = 4):
+    from tpic_b200.plasma import Case, FieldInit, GridSpec, SpeciesSpec
+    box = 20.0 * scale / 128
+    g = GridSpec(scale, scale, scale, box, box, box)
+    npcel = (ppc_axis,) * 3
+    species = [SpeciesSpec(qom=-64.0, rho=1.0, npcel=npcel, vth=(0.045,) * 3),
+               SpeciesSpec(qom=1.0, rho=1.0, npcel=npcel, vth=(0.0056,) * 3)]
+    return Case(g, species, dt=0.15, theta=0.5, gmres_tol=1e-8, fields=FieldInit(b0=(0.0, 0.0, 0.0195)))
+
+
+def peaks():
+    try:
+        data = json.loads(PEAKS.read_text())
+        return float(data["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.file,
+                                         stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait(timeout=10)
+
+    def summary(self):
+        self.file.flush()
+        rows = [r.split(", ") for r in Path(self.file.name).read_text().splitlines() if r.strip()]
+        rows = [r for r in rows if len(r) >= 9]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].strip() == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": float(rows[0][2]),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_oracle_rate(scale: int, ppc_axis: int, cycles: int, warmup: int, precision: int = 1) -> dict:
+    """The oracle cycle (the CPU restatement of the path) on a bounded sample
+    of the workload: `scale`^3 cells at the workload's cell size and loading."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    from tpic_b200.plasma import generate_species
+    case = workload(scale, ppc_axis)
+    oc = O.OracleCycle(case.grid, O.case_species_arrays(case, precision, generate_species), case.dt, case.theta,
+                       case.c, case.gmres_tol, precision, b0=case.fields.b0)
+    oc.prepare()
+    for _ in range(warmup):
+        oc.cycle()
+    n = sum(len(d["cell"]) for _, d in oc.species)
+    t0 = time.perf_counter()
+    for _ in range(cycles):
+        oc.cycle()
+    dt = time.perf_counter() - t0
+    return {"particles": n, "cycles": cycles, "seconds": dt}
+
+
+def _cpu_worker(args):
+    scale, ppc_axis, cycles, warmup = args
+    return cpu_oracle_rate(scale, ppc_axis, cycles, warmup)
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cores = os.cpu_count() or 1
+    scale = args.cpu_scale
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(cores) as pool:
+        results = pool.map(_cpu_worker, [(scale, 4, args.steps, args.warmup)] * cores)
+    wall = time.perf_counter() - t0
+    value = sum(r["particles"] * r["cycles"] for r in results) / max(r["seconds"] for r in results)
+    sample = (f"{cores} independent replicas of a {scale}^3-cell slice of the workload "
+              f"({results[0]['particles']} particles each, same cell size and loading), "
+              f"{args.steps} timed oracle cycles after {args.warmup} warm-up cycles")
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * max(r["seconds"] for r in results) / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64/f32 (host)",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": "3-D uniform thermal plasma, 128^3 cells, 2 species x 64 ppc (bounded CPU sample)",
+                       "sample_cells": scale ** 3, "precision": "mixed"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "wall_s": wall}
+    print(json.dumps(line), flush=True)
+
+
+def run_gpu(args) -> None:
+    import torch
+    from tpic_b200 import _lib
+    from tpic_b200.simulation import Simulation
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    case = workload(args.scale, 4)
+    t_gen = time.perf_counter()
+    sim = Simulation(case, precision=args.precision, mass_kind=args.mass_matrix, device=local,
+                     generate_on_device=True)
+    gen_s = time.perf_counter() - t_gen
+    nparticles = sum(case.grid.cells * sp.ppc for sp in case.species)
+    stream = torch.cuda.current_stream()
+    lib = sim.lib
+
+    sim.prepare()
+    w0 = sim.energy()
+    total0 = w0[0] + w0[1] + sum(w0[2 + 5 * s] for s in range(len(case.species)))
+    warm = sim.run(args.warmup)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device-resident timing -------------------------------------------------
+    launches0 = lib.tpicb200_launch_count()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        reports = sim.run(args.steps)
+        stop.record(stream)
+        barrier()
+    launches = lib.tpicb200_launch_count() - launches0
+    seconds = start.elapsed_time(stop) / 1e3
+    if dist is not None:
+        t = torch.tensor([seconds], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        seconds = float(t.item())
+    value = world * nparticles * args.steps / seconds
+    drift = max(abs(r.total_energy - total0) / abs(total0) for r in reports)
+    stage_names = ["solve", "move", "advance", "sort", "deposit", "fold_diagnostics"]
+    stages = {name: float(np.mean([r.stage_ms[k] for r in reports])) for k, name in enumerate(stage_names)}
+    gmres_it = float(np.mean([r.gmres_iterations for r in reports]))
+
+    # ---- dominant-kernel roofline: per-stage kernels timed alone -----------------
+    kernels = stage_kernel_times(sim, args, stream)
+    hbm, peak_kind = peaks()
+    dominant = max(kernels, key=lambda k: kernels[k]["ms"])
+    dk = kernels[dominant]
+    achieved = dk["bytes"] / (dk["ms"] / 1e3) / 1e9
+    traffic = load_traffic(dominant)
+    roofline = {"kernel": dominant, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "peak_source": peak_kind,
+                "traffic": traffic, "algorithmic_bytes": dk["bytes"],
+                "all_kernels": {k: {"ms": v["ms"], "GB/s": v["bytes"] / (v["ms"] / 1e3) / 1e9,
+                                    "frac": v["bytes"] / (v["ms"] / 1e3) / 1e9 / hbm} for k, v in kernels.items()}}
+
+    # ---- end to end through the public API with host buffers -----------------------
+    e2e = end_to_end(sim, args, stream, barrier, nparticles, world, dist)
+
+    sim.close()
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1e3 * seconds / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32" if args.precision == "mixed" else "f64", "data": "synthetic",
+                "config": {"workload": f"3-D uniform thermal plasma, {args.scale}^3 cells, box 20^3 d_i, "
+                                       f"2 species x 64 ppc, mass ratio 64", "particles": nparticles,
+                           "precision": args.precision, "mass_matrix": args.mass_matrix, "dt": case.dt,
+                           "theta": case.theta, "gmres_tol": case.gmres_tol, "l2": "inputs larger than L2",
+                           "parallelism": f"replicas x{world}"},
+                "energy_drift": drift, "gmres_iterations": gmres_it, "stages_ms": stages,
+                "clocks": clocks.summary(), "e2e": e2e, "gpu_launches": int(launches),
+                "roofline": roofline, "generation_s": gen_s}
+        if not args.no_cpu_baseline:
+            cb = cpu_oracle_rate(args.cpu_scale, 4, 2, 0)
+            line["cpu_baseline"] = {"value": cb["particles"] * cb["cycles"] / cb["seconds"], "unit": UNIT,
+                                    "cores": 1, "kind": "port",
+                                    "sample": f"oracle cycle on a {args.cpu_scale}^3-cell slice of the workload "
+                                              f"({cb['particles']} particles), {cb['cycles']} cycles, 1 thread"}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def stage_kernel_times(sim, args, stream, repeats: int = 5) -> dict:
+    """Average device time of each stage's kernels launched alone through the
+    C ABI, with the algorithmic bytes of one launch (HBM roofline)."""
+    import torch
+    from tpic_b200 import _lib
+    lib, st = sim.lib, sim.state
+    s_ = C.c_void_p(stream.cuda_stream)
+    g = sim.case.grid
+    ns = st.ns
+    vb = 4 if args.precision == "mixed" else 8
+    fb = vb
+    n_total = sum(st.slot[s][st.current[s]].count for s in range(ns))
+    nodes = sim.layout.node_count
+    out = {}
+
+    def timed(fn):
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        fn()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(repeats):
+            fn()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        return ev0.elapsed_time(ev1) / repeats
+
+    scratch_inv = torch.zeros(1, dtype=torch.int32, device="cuda")
+
+    # Deposition (current + mass) of all species from the sorted records.
+    def deposit():
+        lib.tpicb200_clear_moments(sim.ctx, st.j, st.mass, s_)
+        for s in range(ns):
+            p = st.slot[s][st.current[s]]
+            _lib.check(lib.tpicb200_deposit(sim.ctx, st.qom[s], C.byref(p), st.counts[s], st.offsets[s], st.b_node,
+                                            st.j, st.mass, st.mass_kind, scratch_inv.data_ptr(), s_))
+    out["deposit"] = {"ms": timed(deposit),
+                      "bytes": n_total * (24 + 3 * vb + 8 + 4) + nodes * (126 + 3) * fb}
+
+    # Sort of all species (ping-pong into the idle slot and back, one each way).
+    def sort_once():
+        for s in range(ns):
+            cur = st.current[s]
+            _lib.check(lib.tpicb200_sort(sim.ctx, C.byref(st.slot[s][cur]), C.byref(st.slot[s][1 - cur]),
+                                         st.counts[s], st.offsets[s], scratch_inv.data_ptr(), s_))
+            st.current[s] = 1 - cur
+    out["sort"] = {"ms": timed(sort_once), "bytes": n_total * (4 + 2 * (24 + 3 * vb + 8 + 4))}
+    # Make sure the live slot is the sorted one with valid bins (an even number of sorts ran).
+    if (repeats + 1) % 2:
+        sort_once()
+
+    # Mover of all species (E_theta and B as left by the last cycle).
+    saved = {}
+    for s in range(ns):
+        cur = st.current[s]
+        saved[s] = {k: v.clone() for k, v in sim.slots[s][cur].items()}
+
+    def move():
+        for s in range(ns):
+            p = st.slot[s][st.current[s]]
+            _lib.check(lib.tpicb200_mover(sim.ctx, st.qom[s], C.byref(p), st.e_theta, st.b_node,
+                                          scratch_inv.data_ptr(), s_))
+    out["mover"] = {"ms": timed(move), "bytes": n_total * ((24 + 3 * vb + 8 + 4) + (24 + 3 * vb + 4))}
+    for s in range(ns):
+        for k, v in saved[s].items():
+            sim.slots[s][st.current[s]][k].copy_(v)
+    del saved
+    torch.cuda.synchronize()
+    return out
+
+
+def load_traffic(kernel: str):
+    """DRAM bytes per launch from the committed ncu capture summary, if any."""
+    path = ROOT / "profiles" / "traffic.json"
+    try:
+        return json.loads(path.read_text()).get(kernel)
+    except Exception:
+        return None
+
+
+def end_to_end(sim, args, stream, barrier, nparticles, world, dist) -> dict:
+    """The metric through the public API from host buffers: every timed run
+    uploads the full state (particle records of the live slots and the
+    fields) from pinned host memory, prepares, runs the cycles and reads the
+    per-cycle energy reports back to the host."""
+    import torch
+    live = []
+    for s in range(sim.state.ns):
+        slot = sim.slots[s][sim.state.current[s]]
+        live.append({k: (v, v.cpu().pin_memory()) for k, v in slot.items()})
+    fields = [(t, t.cpu().pin_memory()) for t in (sim.field("e"), sim.field("b_cell"))]
+    h2d = sum(h.numel() * h.element_size() for d in live for _, h in d.values()) + \
+        sum(h.numel() * h.element_size() for _, h in fields)
+    steps = args.steps
+    barrier()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for d in live:
+        for dev, host in d.values():
+            dev.copy_(host, non_blocking=True)
+    for dev, host in fields:
+        dev.copy_(host, non_blocking=True)
+    sim.prepare()
+    reports = sim.run(steps)  # energy scalars read back to the host every cycle
+    stop.record(stream)
+    barrier()
+    seconds = start.elapsed_time(stop) / 1e3
+    if dist is not None:
+        t = torch.tensor([seconds], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        seconds = float(t.item())
+    d2h = (2 + 5 * sim.state.ns) * 8 + 4
+    return {"value": world * nparticles * steps / seconds, "unit": UNIT,
+            "h2d_bytes_per_step": int(h2d / steps), "d2h_bytes_per_step": d2h,
+            "seconds": seconds, "cycles": len(reports)}
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["tpic_b200", "reference"], default="tpic_b200")
+    ap.add_argument("--mass-matrix", default="scalar", choices=["scalar", "scalar-f64", "tf32", "bf16x3"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "double"])
+    ap.add_argument("--scale", type=int, default=128, help="cells per axis of the workload")
+    ap.add_argument("--cpu-scale", type=int, default=24, help="cells per axis of the CPU sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("at least 3 warm-up steps")
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

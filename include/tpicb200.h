@@ -156,6 +156,9 @@ typedef struct {
 const char* tpicb200_version(void);
 /* Message of the last failure on the calling thread. */
 const char* tpicb200_last_error(void);
+/* Number of kernels this library has launched since it was loaded (a
+ * host-side count kept by every launch site; for benchmarks and tests). */
+unsigned long long tpicb200_launch_count(void);
 
 /* Set up a context: geometry, constants and the solver/sort workspace.
  * Replaces the owner construction of MaxwellOperator, Gmres and the sort

@@ -90,8 +90,8 @@ class StageContext:
         _lib.check(self.lib.tpicb200_mover(self.ctx, qom, C.byref(p), etheta.data_ptr(), bnode.data_ptr(),
                                            self.invalid.data_ptr(), self.stream))
 
-    def sort(self, src: dict, n: int, with_id=False):
-        dst = self.empty_particles(n, with_id)
+    def sort(self, src: dict, n: int, with_id=None):
+        dst = self.empty_particles(n, ("id" in src) if with_id is None else with_id)
         counts = torch.zeros(self.layout.bin_count, dtype=torch.int32, device="cuda")
         offsets = torch.zeros(self.layout.bin_count + 1, dtype=torch.int32, device="cuda")
         pin, pout = self.struct(src, n), self.struct(dst, n)

@@ -68,6 +68,7 @@ class CycleReport(C.Structure):
 EXPORTS = {
     "tpicb200_version": (C.c_char_p, []),
     "tpicb200_last_error": (C.c_char_p, []),
+    "tpicb200_launch_count": (C.c_ulonglong, []),
     "tpicb200_create": (C.c_int, [C.POINTER(Grid), C.POINTER(Options), C.POINTER(C.c_void_p)]),
     "tpicb200_destroy": (C.c_int, [C.c_void_p]),
     "tpicb200_get_layout": (C.c_int, [C.c_void_p, C.POINTER(Layout)]),

@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <atomic>
 #include <utility>
 
 using namespace tpicb200;
@@ -62,6 +63,9 @@ uint32_t* invalid_or_own(tpicb200_context* ctx, uint32_t* invalid) {
 }  // namespace
 
 namespace tpicb200 {
+static std::atomic<unsigned long long> g_launches{0};
+void count_launches(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
 Geom make_geom(const tpicb200_grid& grid) {
   Geom g{};
   g.nx = grid.nx; g.ny = grid.ny; g.nz = grid.nz;
@@ -85,6 +89,7 @@ extern "C" {
 
 const char* tpicb200_version(void) { return "tpicb200 0.1 (sm_100a)"; }
 const char* tpicb200_last_error(void) { return last_error.c_str(); }
+unsigned long long tpicb200_launch_count(void) { return tpicb200::g_launches.load(); }
 
 int tpicb200_create(const tpicb200_grid* grid, const tpicb200_options* options, tpicb200_context** out) {
   if (!grid || !options || !out) return fail(TPICB200_INVALID_ARGUMENT, "null create argument");

@@ -374,11 +374,13 @@ cudaError_t launch_typed(bool mass_only_scalar, const Geom& g, DepositParams dp,
     sorted_deposit_kernel<P, MC><<<blocks, 128, 0, s>>>(g, dp, (const double*)p->rx, (const double*)p->ry,
         (const double*)p->rz, (const Vel*)p->u, (const Vel*)p->v, (const Vel*)p->w, p->q, p->cell,
         counts, offsets, (const Fld*)bnode, (Fld*)j, (Mass*)mass, invalid);
+    count_launches(1);
   } else if (p->count) {
     unsorted_deposit_kernel<P, MC><<<grid_for(p->count, 128, 148u * 16u), 128, 0, s>>>(g, dp,
         (const double*)p->rx, (const double*)p->ry, (const double*)p->rz, (const Vel*)p->u,
         (const Vel*)p->v, (const Vel*)p->w, p->q, p->cell, p->count, (const Fld*)bnode, (Fld*)j,
         (Mass*)mass, invalid);
+    count_launches(1);
   }
   return cudaGetLastError();
 }
@@ -402,11 +404,13 @@ cudaError_t launch_fold(int precision, const Geom& g, void* j, void* mass, cudaS
     const unsigned blocks = grid_for(3 * shell_count(g), 256, 148u * 8u);
     if (precision == TPICB200_PRECISION_DOUBLE) fold_field_kernel<double><<<blocks, 256, 0, s>>>(g, (double*)j);
     else fold_field_kernel<float><<<blocks, 256, 0, s>>>(g, (float*)j);
+    count_launches(1);
   }
   if (mass) {
     const unsigned blocks = grid_for(126 * shell_count(g), 256, 148u * 8u);
     if (precision == TPICB200_PRECISION_DOUBLE) fold_mass_kernel<double><<<blocks, 256, 0, s>>>(g, (double*)mass);
     else fold_mass_kernel<float><<<blocks, 256, 0, s>>>(g, (float*)mass);
+    count_launches(1);
   }
   return cudaGetLastError();
 }

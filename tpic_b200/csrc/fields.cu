@@ -268,6 +268,7 @@ __global__ void __launch_bounds__(256) copy_node_kernel(long long total, const T
 
 cudaError_t launch_node_ghosts(const Geom& g, double* f, int components, cudaStream_t s) {
   node_fill_kernel<double><<<grid_for(shell_count(g) * components, 256), 256, 0, s>>>(g, f, components);
+  count_launches(1);
   return cudaGetLastError();
 }
 
@@ -276,6 +277,7 @@ cudaError_t launch_cell_ghosts(int precision, const Geom& g, void* f, cudaStream
   const unsigned blocks = grid_for(3 * shell, 256);
   if (precision == TPICB200_PRECISION_DOUBLE) cell_fill_kernel<double><<<blocks, 256, 0, s>>>(g, (double*)f);
   else cell_fill_kernel<float><<<blocks, 256, 0, s>>>(g, (float*)f);
+  count_launches(1);
   return cudaGetLastError();
 }
 
@@ -288,6 +290,7 @@ cudaError_t launch_cell_to_node(int precision, const Geom& g, const void* cellf,
     cell_to_node_kernel<float, float><<<blocks, 256, 0, s>>>(g, (const float*)cellf, (float*)node);
     node_fill_kernel<float><<<grid_for(3 * shell_count(g), 256), 256, 0, s>>>(g, (float*)node, 3);
   }
+  count_launches(2);
   return cudaGetLastError();
 }
 
@@ -300,6 +303,7 @@ cudaError_t launch_rhs(int precision, const Geom& g, double delta, double kfac, 
   else
     rhs_kernel<float, float><<<blocks, 256, 0, s>>>(g, float(delta), float(kfac), (const float*)e,
                                                    (const float*)bcell, (const float*)j, rhs);
+  count_launches(1);
   return cudaGetLastError();
 }
 
@@ -321,6 +325,7 @@ cudaError_t launch_field_advance(int precision, const Geom& g, double theta_valu
     faraday_kernel<float, float><<<fb, 256, 0, s>>>(g, float(faraday), (const float*)bcell, etheta,
                                                    (float*)bnext, invalid);
   }
+  count_launches(2);
   return cudaGetLastError();
 }
 
@@ -330,6 +335,7 @@ cudaError_t launch_field_energy(int precision, const Geom& g, const void* e, con
     field_energy_kernel<double><<<blocks, 256, 0, s>>>(g, (const double*)e, (const double*)bcell, partials);
   else
     field_energy_kernel<float><<<blocks, 256, 0, s>>>(g, (const float*)e, (const float*)bcell, partials);
+  count_launches(1);
   return cudaGetLastError();
 }
 
@@ -341,12 +347,14 @@ cudaError_t launch_species_scalars(int precision, const tpicb200_particles* p, d
   else
     species_kernel<float><<<blocks, 256, 0, s>>>((const float*)p->u, (const float*)p->v,
                                                  (const float*)p->w, p->q, p->count, 1.0 / qom, partials);
+  count_launches(1);
   return cudaGetLastError();
 }
 
 cudaError_t launch_reduce_rows(const double* partials, double* out, int rows, int row_stride, int count,
                                int filled, cudaStream_t s) {
   reduce_rows_kernel<<<rows, 256, 0, s>>>(partials, out, row_stride, count, filled);
+  count_launches(1);
   return cudaGetLastError();
 }
 
@@ -354,6 +362,7 @@ cudaError_t launch_copy_node_field(const Geom& g, const void* in, int in_double,
   const long long total = 3 * g.nodes;
   if (in_double) copy_node_kernel<double><<<grid_for(total, 256), 256, 0, s>>>(total, (const double*)in, out);
   else copy_node_kernel<float><<<grid_for(total, 256), 256, 0, s>>>(total, (const float*)in, out);
+  count_launches(1);
   return cudaGetLastError();
 }
 

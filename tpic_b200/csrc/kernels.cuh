@@ -5,6 +5,9 @@
 
 namespace tpicb200 {
 
+// Host-side count of the kernels this library launched (tpicb200_launch_count).
+void count_launches(unsigned n);
+
 // mover.cu
 cudaError_t launch_mover(int precision, const Geom& g, double qom, double dt, double c,
                          tpicb200_particles* p, const double* theta, const void* bnode,

@@ -130,6 +130,7 @@ cudaError_t launch(const Geom& g, double qom, double dt, double c, tpicb200_part
       (typename P::Pos*)p->rz, (typename P::Vel*)p->u, (typename P::Vel*)p->v,
       (typename P::Vel*)p->w, p->q, p->cell, p->count, theta,
       (const typename P::Fld*)bnode, invalid);
+  count_launches(1);
   return cudaGetLastError();
 }
 

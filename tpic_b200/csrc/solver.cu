@@ -441,6 +441,7 @@ struct Solve {
     const double iv = w->g.inv_volume;
     maxwell_apply_kernel<C, Mass, Out><<<blocks(), kThreads, 0, s>>>(
         w->g, C(w->delta * w->delta), C(w->kfac), C(iv), mass, w->input, out);
+    count_launches(1);
     check();
   }
   void reduce(int filled) {
@@ -456,6 +457,7 @@ struct Solve {
   }
   void apply_solution(const Mass* mass) {
     unpack_kernel<double><<<blocks(), kThreads, 0, s>>>(w->g, w->x, w->input);
+    count_launches(1);
     apply<double, double>(mass, w->ximage);
   }
 
@@ -470,9 +472,11 @@ struct Solve {
     pack_storage_kernel<Fld><<<blocks(), kThreads, 0, s>>>(g, (const Fld*)e, w->x);
     launch_rhs(P::id, g, w->delta, w->kfac, e, bcell, j, w->rhs, s);
     pack_kernel<double><<<blocks(), kThreads, 0, s>>>(g, w->rhs, w->b);
+    count_launches(2);
     check();
     apply_solution(mass);
     residual_kernel<true><<<w->rblocks, kThreads, 0, s>>>(w->b, w->ximage, w->r, w->partials, N);
+    count_launches(1);
     reduce(2);
     double controls[2];
     if (!read_controls(w->values, controls)) return TPICB200_BACKEND_FAILURE;
@@ -492,6 +496,7 @@ struct Solve {
       normalize_kernel<double, S><<<w->rblocks, kThreads, 0, s>>>(
           g, w->r, w->values, w->template basis_col<S>(0), w->input,
           ArnoldiTail{nullptr, nullptr, nullptr, w->ls_rhs(), nullptr, -1});
+      count_launches(1);
       check();
       const int columns = std::min(m, max_iterations - res.iterations);
       const double cycle_tolerance =
@@ -511,6 +516,7 @@ struct Solve {
         normalize_kernel<S, S><<<w->rblocks, kThreads, 0, s>>>(
             g, image, w->values, w->template basis_col<S>(col + 1), w->input,
             ArnoldiTail{h_column, w->cosine(), w->sine(), w->ls_rhs(), w->status(), col});
+        count_launches(3);
         check();
         double st[2];
         if (!read_controls(w->status(), st)) return TPICB200_BACKEND_FAILURE;
@@ -522,10 +528,12 @@ struct Solve {
       back_substitute_kernel<<<1, 1, 0, s>>>(w->hessenberg(), w->ls_rhs(), w->coefficients(), m + 1, completed);
       update_solution_kernel<S><<<grid_for(N, kThreads), kThreads, 0, s>>>(w->template basis_col<S>(0),
                                                                           w->coefficients(), w->x, N, completed);
+      count_launches(2);
       check();
       res.iterations += completed;
       apply_solution(mass);
       residual_kernel<false><<<w->rblocks, kThreads, 0, s>>>(w->b, w->ximage, w->r, w->partials, N);
+      count_launches(1);
       reduce(1);
       if (!read_controls(w->values, controls)) return TPICB200_BACKEND_FAILURE;
       if (!std::isfinite(controls[0]) || controls[0] < 0) return TPICB200_OVERFLOW;
@@ -536,6 +544,7 @@ struct Solve {
     if (result) *result = res;
     if (!res.converged) return TPICB200_NOT_CONVERGED;
     unpack_kernel<double><<<blocks(), kThreads, 0, s>>>(g, w->x, etheta);
+    count_launches(1);
     launch_node_ghosts(g, etheta, 3, s);
     check();
     return err == cudaSuccess ? TPICB200_SUCCESS : TPICB200_BACKEND_FAILURE;
@@ -567,6 +576,7 @@ cudaError_t solver_mass_apply(SolverWorkspace* w, const void* mass, const double
     mass_apply_kernel<double><<<blocks, kThreads, 0, s>>>(w->g, w->g.inv_volume, (const double*)mass, in, out);
   else
     mass_apply_kernel<float><<<blocks, kThreads, 0, s>>>(w->g, w->g.inv_volume, (const float*)mass, in, out);
+  count_launches(1);
   return cudaGetLastError();
 }
 

@@ -361,6 +361,7 @@ cudaError_t launch_sort(int precision, const Geom& g, const tpicb200_particles* 
           in->id ? out->id : nullptr, sc.flag);
   }
   report_kernel<<<1, 1, 0, s>>>(sc.flag, invalid);
+  count_launches(n ? 9 : 4);
   out->count = n;
   return cudaGetLastError();
 }
