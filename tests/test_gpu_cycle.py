@@ -78,3 +78,16 @@ def test_c1_mixed_precision_energy(mass_kind):
     reports = sim.run(3)
     for r in reports:
         assert abs(r.total_energy - total0) <= 1e-6 * total0
+
+
+@pytest.mark.parametrize("mass_kind,bound", [("tf32", 1e-4), ("bf16x3", 1e-5)])
+def test_c1_tensor_core_energy(mass_kind, bound):
+    case = c1_case(n=16)
+    from tpic_b200.simulation import Simulation
+    sim = Simulation(case, precision="mixed", mass_kind=mass_kind)
+    sim.prepare()
+    w0 = sim.energy()
+    total0 = w0[0] + w0[1] + w0[2] + w0[7]
+    reports = sim.run(3)
+    for r in reports:
+        assert abs(r.total_energy - total0) <= bound * total0

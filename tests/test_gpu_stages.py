@@ -399,3 +399,59 @@ def test_field_advance_matches_oracle(torch_cuda, precision):
     assert np.allclose(interior_nodes(g, et.cpu().numpy()), interior_nodes(g, we), rtol=rtol, atol=atol)
     assert np.allclose(bnext.cpu().numpy(), wb, rtol=rtol, atol=atol)
     assert np.allclose(bnode.cpu().numpy(), wbn, rtol=rtol, atol=atol)
+
+
+# --------------------------------------------------------------------------
+# Tensor-core (tcgen05) mass assembly.
+@pytest.mark.parametrize("kind", [2, 3])
+def test_tc_exact_inputs(torch_cuda, kind):
+    """Inputs exactly representable in TF32 (fractions in {0, 1/4, 1/2, 3/4},
+    B = 0 so alpha = I, power-of-two charges): every product is exact, so the
+    tensor-core mass matrix must equal the FP64 oracle to FP32 accumulation
+    rounding. Checks the operand layouts, descriptors and the pair epilogue."""
+    g = GridSpec(5, 4, 3, 5.0, 4.0, 3.0)
+    rng = np.random.default_rng(17)
+    rows = []
+    for cell in range(g.cells):
+        i, j, k = cell % g.nx, (cell // g.nx) % g.ny, cell // (g.nx * g.ny)
+        for _ in range(int(rng.integers(0, 90))):
+            rows.append((g.encode(i, j, k), *(rng.integers(0, 4, 3) / 4.0), rng.choice([0.5, -0.25, 1.0])))
+    rows = np.array(rows)
+    n = len(rows)
+    d = {"cell": rows[:, 0].astype(np.int32), "rx": rows[:, 1].copy(), "ry": rows[:, 2].copy(), "rz": rows[:, 3].copy(),
+         "q": rows[:, 4].copy(), "u": np.zeros(n, np.float32), "v": np.zeros(n, np.float32), "w": np.zeros(n, np.float32)}
+    ctx = make_ctx(g, 1, dt=1.0, max_particles=n)
+    parts = ctx.upload_particles(d)
+    parts, counts, offsets = ctx.sort(parts, n)
+    bnode = np.zeros(3 * ctx.layout.node_count, np.float32)
+    j, m = ctx.moments()
+    ctx.deposit(1.0, parts, n, ctx.field(bnode), j, m, counts, offsets, kind=kind)
+    ctx.fold(j, m)
+    jw, mw, bad = oracle_moments(g, 1, 1.0, 1.0, d, bnode)
+    assert bad == 0 and ctx.invalid_count() == 0
+    got = interior_records(g, m.cpu().numpy().astype(np.float64))
+    want = interior_records(g, mw)
+    assert np.abs(got - want).max() <= 1e-6 * np.abs(want).max()
+
+
+@pytest.mark.parametrize("kind,rel", [(2, 3e-3), (3, 1e-4)])
+def test_tc_mass_matches_oracle(torch_cuda, kind, rel):
+    g = GRID
+    rng = np.random.default_rng(23)
+    d = species_arrays(g, 1, vth=(0.2, 0.1, 0.3), npcel=(4, 4, 4))
+    n = len(d["cell"])
+    ctx = make_ctx(g, 1, dt=0.2, max_particles=n)
+    bnode = periodic_node_field(g, smooth_random_unique(g, rng, 0.9)).astype(np.float32)
+    parts = ctx.upload_particles(d)
+    parts, counts, offsets = ctx.sort(parts, n)
+    j, m = ctx.moments()
+    ctx.deposit(-4.0, parts, n, ctx.field(bnode), j, m, counts, offsets, kind=kind)
+    ctx.fold(j, m)
+    jw, mw, bad = oracle_moments(g, 1, -4.0, 0.2, d, bnode)
+    assert bad == 0 and ctx.invalid_count() == 0
+    jg, mg = j.cpu().numpy().astype(np.float64), m.cpu().numpy().astype(np.float64)
+    jw_i, jg_i = interior_nodes(g, jw), interior_nodes(g, jg)
+    assert np.abs(jg_i - jw_i).max() <= 3e-5 * np.abs(jw_i).max() + 1e-15  # J-hat stays FP32
+    mw_i, mg_i = interior_records(g, mw), interior_records(g, mg)
+    err = np.abs(mg_i - mw_i).max() / np.abs(mw_i).max()
+    assert err <= rel, err

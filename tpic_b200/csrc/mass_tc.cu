@@ -1,13 +1,464 @@
-// Tensor-core (tcgen05) mass-matrix assembly forms. Placeholder until the
-// tcgen05 kernels land: the TF32 and BF16x3 selections are rejected.
+// Tensor-core (tcgen05) mass-matrix assembly with the implicit current on
+// CUDA cores, one species of sorted records per launch.
+//
+// The mass block of a corner pair is K_ab = sum_p s_p alpha_p W_pa W_pb with
+// s = (beta/c) q (ecsim/mass_matrix/mass_matrix_scalar_device.hpp:25-97). With
+// CIC weights W_pa = X_p(a_x) Y_p(a_y) Z_p(a_z), the pair weight factors per
+// axis into one of three products, (1-x)^2, x(1-x) or x^2, so W_pa W_pb is the
+// monomial m_pt of the per-axis class t = (a_x+b_x) + 3(a_y+b_y) + 9(a_z+b_z).
+// A cell's 36 canonical pair blocks are therefore 27 monomial moments
+//   G[t][c] = sum_p m_pt (s_p alpha_p[c]),  t < 27, c < 9,
+// a dense contraction over the cell's particles: D = A^T B with K = particles.
+//
+// Tensor-core mapping (one CTA of four warps works on four cells at once):
+//   A (tensor memory, M = 128 lanes x K columns): lane 32w + t holds m_pt of
+//     cell w's particles (rows 27..31 of each quadrant are zero);
+//   B (shared memory, K x N = 48, MN-major, no swizzle): columns 12w..12w+8
+//     hold s_p alpha_p of cell w's particle p (the rest zero);
+//   D (tensor memory, 128 x 48 FP32): D[32w + t][12w + c] = G_w[t][c]; the
+//     off-diagonal blocks are never read.
+// Each 32-particle chunk is four tcgen05.mma.kind::tf32 (K = 8) issued by one
+// thread; A and B are double-buffered so the next chunk is produced while the
+// tensor core consumes the previous one (tcgen05.commit -> mbarrier).
+// Operands are rounded to TF32 with round-to-nearest (cvt.rna) so the
+// rounding is unbiased; accumulation is FP32. The epilogue reads G with
+// tcgen05.ld and adds each monomial's 3x3 block to the 1, 2 or 4 canonical
+// pair records that share it (324 atomics per cell, as the reference's flush).
+// J-hat is accumulated in FP32 on the CUDA cores exactly as the scalar form.
+//
+// BF16x3 form: every operand v is split into hi = bf16(v) and lo = bf16(v - hi)
+// (round-to-nearest) and D accumulates A_hi B_hi + A_hi B_lo + A_lo B_hi with
+// tcgen05.mma.kind::f16 (BF16 inputs, FP32 accumulation, K = 16); B then has
+// 16 columns per cell (N = 64) so each cell's block is whole 16-byte core rows.
 #include "kernels.cuh"
+#include "tcgen05.cuh"
+
+#include <algorithm>
+
+#include <cuda_bf16.h>
 
 namespace tpicb200 {
+namespace {
 
-cudaError_t launch_deposit_tc(int, const Geom&, double, double, double, const tpicb200_particles*,
-                              const uint32_t*, const uint32_t*, const void*, void*, void*, uint32_t*,
-                              cudaStream_t) {
-  return cudaErrorNotSupported;
+constexpr int kCells = 4;          // cells per CTA group (one per warp)
+constexpr int kChunk = 32;         // particles per chunk (one per lane)
+constexpr int kFacStride = 36;     // floats per factor row (padded against bank conflicts)
+constexpr uint32_t kTmemCols = 128;
+constexpr uint32_t kDcol = 64;
+// Per form: B columns per cell, N, bytes of one B tile (N-chunks of 16 bytes,
+// each 4 K-groups x 128 bytes for a 32-particle chunk), B tiles per buffer.
+template <bool Bf16> struct Form {
+  static constexpr int cols = Bf16 ? 16 : 12;
+  static constexpr int n = kCells * cols;
+  static constexpr int per_chunk16 = Bf16 ? 8 : 4;   // values per 16-byte N-chunk
+  static constexpr uint32_t tile_bytes = uint32_t(n / per_chunk16) * 512u;
+  static constexpr int tiles = Bf16 ? 2 : 1;         // hi (+ lo)
+};
+
+// Canonical pairs sharing each monomial class: corner a and stencil s.
+struct MonomialPairs {
+  int count[27];
+  int corner[27][4];
+  int stencil[27][4];
+};
+constexpr MonomialPairs make_monomial_pairs() {
+  MonomialPairs r{};
+  for (int a = 0; a < 8; ++a)
+    for (int b = 0; b < 8; ++b) {
+      const int s = pair_stencil(a, b);
+      if (s < 0) continue;
+      const int t = ((a & 1) + (b & 1)) + 3 * (((a >> 1) & 1) + ((b >> 1) & 1)) + 9 * (((a >> 2) & 1) + ((b >> 2) & 1));
+      r.corner[t][r.count[t]] = a;
+      r.stencil[t][r.count[t]] = s;
+      ++r.count[t];
+    }
+  return r;
+}
+__constant__ MonomialPairs c_pairs = make_monomial_pairs();
+
+struct TcParams {
+  float beta_over_c;
+  float inv_volume;
+};
+
+template <bool Bf16> struct __align__(128) TcShared {
+  uint8_t btile[2][Form<Bf16>::tiles][Form<Bf16>::tile_bytes];
+  float fac[kCells][12][kFacStride];
+  float bcache[kCells][24];
+  uint64_t mbar[2];
+  uint32_t tmem_base;
+  uint32_t count[kCells];
+};
+
+__device__ __forceinline__ long long wrapped(const Geom& g, int i, int j, int k) {
+  return g.node(i == g.nx ? 0 : i, j == g.ny ? 0 : j, k == g.nz ? 0 : k);
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo_elem, float hi_elem) {
+  const __nv_bfloat162 v = __floats2bfloat162_rn(lo_elem, hi_elem);  // .x (low half) = first element
+  return *reinterpret_cast<const uint32_t*>(&v);
+}
+__device__ __forceinline__ void split_bf16(float v, float& hi, float& lo) {
+  hi = __bfloat162float(__float2bfloat16_rn(v));
+  lo = v - hi;
+}
+
+template <bool Bf16>
+__global__ void __launch_bounds__(128, 1) tc_deposit_kernel(Geom g, TcParams tp,
+    const double* __restrict__ rx, const double* __restrict__ ry, const double* __restrict__ rz,
+    const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w,
+    const double* __restrict__ q, const int32_t* __restrict__ key, const uint32_t* __restrict__ counts,
+    const uint32_t* __restrict__ offsets, const float* __restrict__ bnode, float* __restrict__ J,
+    float* __restrict__ M, uint32_t* invalid) {
+  using F = Form<Bf16>;
+  constexpr int kCols = F::cols;
+  constexpr int kN = F::n;
+  __shared__ TcShared<Bf16> sh;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const long long nn = g.nodes;
+  if (warp == 0) {
+    tc::tmem_alloc(&sh.tmem_base, kTmemCols);
+    tc::tmem_relinquish();
+  }
+  if (threadIdx.x == 0) {
+    tc::mbar_init(&sh.mbar[0], 1);
+    tc::mbar_init(&sh.mbar[1], 1);
+    tc::fence_mbar_init();
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = sh.tmem_base;
+  const uint32_t lane_base = uint32_t(32 * warp) << 16;
+  constexpr uint32_t idesc = tc::instr_desc(Bf16 ? 1u : 2u, 128, kN);
+  uint32_t phase[2] = {0, 0};
+  bool pending[2] = {false, false};
+  int buf = 0;
+  bool failed = false;
+
+  const long long cells = (long long)g.nx * g.ny * g.nz;
+  const long long groups = (cells + kCells - 1) / kCells;
+  // Monomial row of this thread in its warp's quadrant.
+  const int t_row = lane;
+  const int tx = t_row % 3, tyz = t_row / 3;
+
+  for (long long grp = blockIdx.x; grp < groups && !failed; grp += gridDim.x) {
+    const long long cell = grp * kCells + warp;
+    const bool live = cell < cells;
+    int ci = 0, cj = 0, ck = 0;
+    uint32_t count = 0, first = 0;
+    int32_t bin = -1;
+    if (live) {
+      ci = int(cell % g.nx); cj = int((cell / g.nx) % g.ny); ck = int(cell / ((long long)g.nx * g.ny));
+      bin = g.encode(ci, cj, ck);
+      count = counts[bin];
+      first = offsets[bin];
+      if (lane < 24) {
+        const int a = lane / 3, c = lane % 3;
+        sh.bcache[warp][lane] = bnode[c * nn + g.node(ci + (a & 1), cj + ((a >> 1) & 1), ck + ((a >> 2) & 1))];
+      }
+    }
+    if (lane == 0) sh.count[warp] = count;
+    __syncthreads();
+    uint32_t maxc = sh.count[0];
+#pragma unroll
+    for (int c = 1; c < kCells; ++c) maxc = max(maxc, sh.count[c]);
+    float jsum[24];
+#pragma unroll
+    for (int t = 0; t < 24; ++t) jsum[t] = 0.0f;
+
+    for (uint32_t chunk = 0; chunk < maxc; chunk += kChunk) {
+      // The buffer is free once the MMAs that read it have completed.
+      bool bad = false;
+      if (pending[buf]) {
+        bad = !tc::mbar_wait(&sh.mbar[buf], phase[buf]);
+        phase[buf] ^= 1u;
+        pending[buf] = false;
+      }
+      // Particle phase: one record per lane.
+      const uint32_t k = chunk + lane;
+      float bv[kCols];
+      float fac[12];
+#pragma unroll
+      for (int c = 0; c < kCols; ++c) bv[c] = 0.0f;
+#pragma unroll
+      for (int f = 0; f < 12; ++f) fac[f] = 0.0f;
+      if (k < count) {
+        const uint32_t n = first + k;
+        const double fx = rx[n], fy = ry[n], fz = rz[n];
+        if (key[n] == bin && fx >= 0 && fx < 1 && fy >= 0 && fy < 1 && fz >= 0 && fz < 1) {
+          const float x = float(fx), y = float(fy), z = float(fz);
+          float wt[8];
+          cic_weights<float>(x, y, z, wt);
+          float b[3];
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            float val = 0.0f;
+#pragma unroll
+            for (int a = 0; a < 8; ++a) val += wt[a] * sh.bcache[warp][a * 3 + c];
+            b[c] = val;
+          }
+          const Response<float> r(b[0], b[1], b[2], tp.beta_over_c);
+          const float charge = float(q[n]);
+          float hx, hy, hz;
+          r.apply(u[n], v[n], w[n], hx, hy, hz);
+          const float qv = charge * tp.inv_volume;
+          const float jc[3] = {qv * hx, qv * hy, qv * hz};
+          const float scale = tp.beta_over_c * charge;
+          if (isfinite(jc[0]) && isfinite(jc[1]) && isfinite(jc[2]) && isfinite(r.norm_square) && isfinite(scale)) {
+#pragma unroll
+            for (int a = 0; a < 8; ++a)
+#pragma unroll
+              for (int c = 0; c < 3; ++c) jsum[a * 3 + c] += __fmul_rn(jc[c], wt[a]);
+#pragma unroll
+            for (int e = 0; e < 9; ++e) bv[e] = r.a[e] * scale;
+            const float cx = 1.0f - x, cy = 1.0f - y, cz = 1.0f - z;
+            const float X[3] = {cx * cx, x * cx, x * x};
+            const float Y[3] = {cy * cy, y * cy, y * y};
+            const float Z[3] = {cz * cz, z * cz, z * z};
+            fac[0] = X[0]; fac[1] = X[1]; fac[2] = X[2];
+#pragma unroll
+            for (int tz = 0; tz < 3; ++tz)
+#pragma unroll
+              for (int ty = 0; ty < 3; ++ty) fac[3 + ty + 3 * tz] = Y[ty] * Z[tz];
+          } else {
+            atomicAdd(invalid, 1u);
+          }
+        } else {
+          atomicAdd(invalid, 1u);
+        }
+      }
+      // B tile (MN-major core matrices: 8 K-rows x 16 bytes of N-values,
+      // K-groups 128 B apart, 16-byte N-chunks 512 B apart).
+      if constexpr (!Bf16) {
+        uint8_t* bt = sh.btile[buf][0];
+#pragma unroll
+        for (int j = 0; j < kCols / 4; ++j) {
+          uint4 pack;
+          pack.x = tc::to_tf32(bv[4 * j + 0]);
+          pack.y = tc::to_tf32(bv[4 * j + 1]);
+          pack.z = tc::to_tf32(bv[4 * j + 2]);
+          pack.w = tc::to_tf32(bv[4 * j + 3]);
+          *reinterpret_cast<uint4*>(bt + (3 * warp + j) * 512 + (lane >> 3) * 128 + (lane & 7) * 16) = pack;
+        }
+      } else {
+        float hi[kCols], lo[kCols];
+#pragma unroll
+        for (int c = 0; c < kCols; ++c) split_bf16(bv[c], hi[c], lo[c]);
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          const uint4 ph = make_uint4(pack_bf16(hi[8 * j + 0], hi[8 * j + 1]), pack_bf16(hi[8 * j + 2], hi[8 * j + 3]),
+                                      pack_bf16(hi[8 * j + 4], hi[8 * j + 5]), pack_bf16(hi[8 * j + 6], hi[8 * j + 7]));
+          const uint4 pl = make_uint4(pack_bf16(lo[8 * j + 0], lo[8 * j + 1]), pack_bf16(lo[8 * j + 2], lo[8 * j + 3]),
+                                      pack_bf16(lo[8 * j + 4], lo[8 * j + 5]), pack_bf16(lo[8 * j + 6], lo[8 * j + 7]));
+          const int off = (2 * warp + j) * 512 + (lane >> 3) * 128 + (lane & 7) * 16;
+          *reinterpret_cast<uint4*>(sh.btile[buf][0] + off) = ph;
+          *reinterpret_cast<uint4*>(sh.btile[buf][1] + off) = pl;
+        }
+      }
+#pragma unroll
+      for (int f = 0; f < 12; ++f) sh.fac[warp][f][lane] = fac[f];
+      __syncwarp();
+      // A: lane t of warp w writes m_pt of the chunk's 32 particles into
+      // tensor-memory lane 32w + t (TF32: columns 32*buf .. +31; BF16: the
+      // hi pairs in columns 32*buf .. +15 and the lo pairs in +16 .. +31).
+      const bool row = t_row < 27;
+      const float* xrow = sh.fac[warp][row ? tx : 0];
+      const float* yzrow = sh.fac[warp][row ? 3 + tyz : 0];
+      if constexpr (!Bf16) {
+#pragma unroll
+        for (int q8 = 0; q8 < 4; ++q8) {
+          uint32_t m[8];
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const float4 xf = *reinterpret_cast<const float4*>(xrow + 8 * q8 + 4 * h);
+            const float4 yzf = *reinterpret_cast<const float4*>(yzrow + 8 * q8 + 4 * h);
+            m[4 * h + 0] = row ? tc::to_tf32(xf.x * yzf.x) : 0u;
+            m[4 * h + 1] = row ? tc::to_tf32(xf.y * yzf.y) : 0u;
+            m[4 * h + 2] = row ? tc::to_tf32(xf.z * yzf.z) : 0u;
+            m[4 * h + 3] = row ? tc::to_tf32(xf.w * yzf.w) : 0u;
+          }
+          tc::tmem_st8(tmem + lane_base + (buf ? 32u : 0u) + 8 * q8, m);
+        }
+      } else {
+#pragma unroll
+        for (int q16 = 0; q16 < 2; ++q16) {
+          uint32_t mh[8], ml[8];
+#pragma unroll
+          for (int h = 0; h < 4; ++h) {
+            const float4 xf = *reinterpret_cast<const float4*>(xrow + 16 * q16 + 4 * h);
+            const float4 yzf = *reinterpret_cast<const float4*>(yzrow + 16 * q16 + 4 * h);
+            float v4[4] = {xf.x * yzf.x, xf.y * yzf.y, xf.z * yzf.z, xf.w * yzf.w};
+            float hi4[4], lo4[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              split_bf16(row ? v4[e] : 0.0f, hi4[e], lo4[e]);
+            }
+            mh[2 * h + 0] = pack_bf16(hi4[0], hi4[1]);
+            mh[2 * h + 1] = pack_bf16(hi4[2], hi4[3]);
+            ml[2 * h + 0] = pack_bf16(lo4[0], lo4[1]);
+            ml[2 * h + 1] = pack_bf16(lo4[2], lo4[3]);
+          }
+          tc::tmem_st8(tmem + lane_base + (buf ? 32u : 0u) + 8 * q16, mh);
+          tc::tmem_st8(tmem + lane_base + (buf ? 32u : 0u) + 16 + 8 * q16, ml);
+        }
+      }
+      tc::tmem_wait_st();
+      tc::fence_proxy_async_smem();
+      tc::fence_before_sync();
+      if (__syncthreads_or(bad)) {
+        failed = true;
+        break;
+      }
+      if (threadIdx.x == 0) {
+        tc::fence_after_sync();
+        const uint32_t abase = tmem + (buf ? 32u : 0u);
+        if constexpr (!Bf16) {
+          const uint32_t bbase = tc::smem_u32(sh.btile[buf][0]);
+#pragma unroll
+          for (int s = 0; s < 4; ++s)
+            tc::mma_tf32_ts(tmem + kDcol, abase + 8 * s, tc::smem_desc(bbase + s * 128, 128, 512), idesc,
+                            (chunk > 0 || s > 0) ? 1u : 0u);
+        } else {
+          const uint32_t bhi = tc::smem_u32(sh.btile[buf][0]), blo = tc::smem_u32(sh.btile[buf][1]);
+#pragma unroll
+          for (int s = 0; s < 2; ++s) {
+            const uint32_t a_hi = abase + 8 * s, a_lo = abase + 16 + 8 * s;
+            tc::mma_f16_ts(tmem + kDcol, a_hi, tc::smem_desc(bhi + s * 256, 128, 512), idesc,
+                           (chunk > 0 || s > 0) ? 1u : 0u);
+            tc::mma_f16_ts(tmem + kDcol, a_hi, tc::smem_desc(blo + s * 256, 128, 512), idesc, 1u);
+            tc::mma_f16_ts(tmem + kDcol, a_lo, tc::smem_desc(bhi + s * 256, 128, 512), idesc, 1u);
+          }
+        }
+        tc::commit(&sh.mbar[buf]);
+      }
+      pending[buf] = true;
+      buf ^= 1;
+    }
+    if (failed) break;
+
+    // J-hat of this warp's cell: reduce-scatter of the 24 lane sums.
+    if (live) {
+      const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
+      float h12[12];
+#pragma unroll
+      for (int t = 0; t < 12; ++t) {
+        const float keep = b4 ? jsum[t + 12] : jsum[t];
+        const float send = b4 ? jsum[t] : jsum[t + 12];
+        h12[t] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+      }
+      float h6[6];
+#pragma unroll
+      for (int t = 0; t < 6; ++t) {
+        const float keep = b3 ? h12[t + 6] : h12[t];
+        const float send = b3 ? h12[t] : h12[t + 6];
+        h6[t] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+      }
+      float h3[3];
+#pragma unroll
+      for (int t = 0; t < 3; ++t) {
+        const float keep = b2 ? h6[t + 3] : h6[t];
+        const float send = b2 ? h6[t] : h6[t + 3];
+        h3[t] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+      }
+#pragma unroll
+      for (int t = 0; t < 3; ++t) {
+        h3[t] += __shfl_xor_sync(0xffffffffu, h3[t], 2);
+        h3[t] += __shfl_xor_sync(0xffffffffu, h3[t], 1);
+      }
+      if ((lane & 3) == 0) {
+        const int index0 = (b4 ? 12 : 0) + (b3 ? 6 : 0) + (b2 ? 3 : 0);
+#pragma unroll
+        for (int t = 0; t < 3; ++t) {
+          const int index = index0 + t, a = index / 3, c = index % 3;
+          const float value = h3[t];
+          if (!isfinite(value)) atomicAdd(invalid, 1u);
+          else if (value != 0.0f)
+            atomicAdd(J + c * nn + wrapped(g, ci + (a & 1), cj + ((a >> 1) & 1), ck + ((a >> 2) & 1)), value);
+        }
+      }
+    }
+
+    // Mass: wait for the group's last MMA, read G_w and flush its pairs.
+    if (maxc > 0) {
+      const int last = buf ^ 1;
+      const bool ok = tc::mbar_wait(&sh.mbar[last], phase[last]);
+      phase[last] ^= 1u;
+      pending[last] = false;
+      tc::fence_after_sync();
+      if (__syncthreads_or(!ok)) {
+        failed = true;
+        break;
+      }
+      uint32_t gbits[8], g8;
+      tc::tmem_ld8(tmem + lane_base + kDcol + kCols * warp, gbits);
+      tc::tmem_ld1(tmem + lane_base + kDcol + kCols * warp + 8, g8);
+      tc::tmem_wait_ld();
+      if (live && count > 0 && t_row < 27) {
+        float G[9];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) G[e] = __uint_as_float(gbits[e]);
+        G[8] = __uint_as_float(g8);
+        bool finite_block = true;
+#pragma unroll
+        for (int e = 0; e < 9; ++e) finite_block = finite_block && isfinite(G[e]);
+        if (!finite_block) {
+          atomicAdd(invalid, 1u);
+        } else {
+          const int np = c_pairs.count[t_row];
+          for (int p = 0; p < np; ++p) {
+            const int a = c_pairs.corner[t_row][p], s = c_pairs.stencil[t_row][p];
+            float* rec = M + wrapped(g, ci + (a & 1), cj + ((a >> 1) & 1), ck + ((a >> 2) & 1)) * 126 + s * 9;
+#pragma unroll
+            for (int e = 0; e < 9; ++e)
+              if (G[e] != 0.0f) atomicAdd(rec + e, G[e]);
+          }
+        }
+      }
+    }
+    // D is overwritten by the next group's first MMA only after every warp
+    // has read it.
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+  }
+
+  if (failed && threadIdx.x == 0) atomicAdd(invalid, 1u << 20);
+  // Retire in-flight MMAs (bounded) before freeing tensor memory.
+#pragma unroll
+  for (int b = 0; b < 2; ++b)
+    if (pending[b]) tc::mbar_wait(&sh.mbar[b], phase[b]);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  if (warp == 0) tc::tmem_dealloc(tmem, kTmemCols);
+}
+
+}  // namespace
+
+cudaError_t launch_deposit_tc(int mass_kind, const Geom& g, double qom, double dt, double c,
+                              const tpicb200_particles* p, const uint32_t* counts, const uint32_t* offsets,
+                              const void* bnode, void* j, void* mass, uint32_t* invalid, cudaStream_t s) {
+  if (mass_kind != TPICB200_MASS_TF32 && mass_kind != TPICB200_MASS_BF16X3) return cudaErrorNotSupported;
+  if (!j || !mass) return cudaErrorInvalidValue;
+  TcParams tp{float(qom * dt / 2 / c), float(g.inv_volume)};
+  int device = 0, sms = 148;
+  cudaGetDevice(&device);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  const long long cells = (long long)g.nx * g.ny * g.nz;
+  const long long groups = (cells + kCells - 1) / kCells;
+  const unsigned blocks = unsigned(std::min<long long>(groups, 4LL * sms));
+  // Dynamic shared-memory padding brings each CTA to ~47 KB, so at most four
+  // CTAs (4 x 128 tensor-memory columns = all 512) are resident per SM and
+  // no tcgen05.alloc ever waits for another CTA's columns.
+  const bool tf32 = mass_kind == TPICB200_MASS_TF32;
+  auto kernel = tf32 ? tc_deposit_kernel<false> : tc_deposit_kernel<true>;
+  const int pad = 47 * 1024 - int(tf32 ? sizeof(TcShared<false>) : sizeof(TcShared<true>));
+  kernel<<<blocks, 128, pad, s>>>(g, tp, (const double*)p->rx, (const double*)p->ry,
+      (const double*)p->rz, (const float*)p->u, (const float*)p->v, (const float*)p->w, p->q, p->cell, counts,
+      offsets, (const float*)bnode, (float*)j, (float*)mass, invalid);
+  count_launches(1);
+  return cudaGetLastError();
 }
 
 }  // namespace tpicb200
