@@ -22,7 +22,8 @@
  *   mass records: 126 scalars per node-field vertex (same vertex index as a
  *                 node field): 14 canonical stencils x 9 row-major tensor
  *                 entries, TPIC's compact layout
- *                 (data/mass_matrix/mass_matrix_layout.hpp:11-68).
+ *                 (data/mass_matrix/mass_matrix_layout.hpp:11-68), or the
+ *                 same entries stencil-major (tpicb200_options.mass_layout).
  *   particles   : SoA records of one species (data/particles/particle_schema.hpp:20-36):
  *                 rx, ry, rz cell-relative fractions in [0,1), u, v, w,
  *                 signed macro-charge q (double), int32 cell key
@@ -76,6 +77,15 @@ enum {
 
 enum { TPICB200_PRECISION_DOUBLE = 0, TPICB200_PRECISION_MIXED = 1 };
 
+/* Storage order of the mass coefficients (every call of a context uses its
+ * option). RECORDS is TPIC's compact layout: 126 consecutive scalars per
+ * vertex (data/mass_matrix/mass_matrix_layout.hpp:30-46). STENCIL_MAJOR keeps
+ * the same 126 entries as 126 arrays of node_count scalars, entry
+ * k = 9*stencil + component of vertex v at k*node_count + v, so a warp
+ * applying the matrix to 32 consecutive nodes reads each entry with one
+ * coalesced 128-byte request. */
+enum { TPICB200_MASS_LAYOUT_RECORDS = 0, TPICB200_MASS_LAYOUT_STENCIL_MAJOR = 1 };
+
 /* Mass-matrix assembly forms, the extended `--mass-matrix` selection
  * (TPIC: scalar | matrix-core, config/numerics_options.hpp:31-47). */
 enum {
@@ -97,6 +107,7 @@ typedef struct {
   int gmres_max_iterations; /* 100 in TPIC (config/physics.hpp:21) */
   int precision;            /* TPICB200_PRECISION_* */
   uint32_t max_particles;   /* capacity of the sort scratch (largest species) */
+  int mass_layout;          /* TPICB200_MASS_LAYOUT_* (0: TPIC records) */
 } tpicb200_options;
 
 typedef struct {

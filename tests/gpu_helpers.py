@@ -14,13 +14,14 @@ ATTRS = ("rx", "ry", "rz", "u", "v", "w", "q", "cell")
 
 class StageContext:
     def __init__(self, grid, precision=0, dt=0.15, theta=0.5, c=1.0, tol=1e-8, max_particles=1 << 20,
-                 restart=30, max_iterations=100):
+                 restart=30, max_iterations=100, mass_layout=0):
         self.lib = _lib.load()
         self.g = grid
         self.precision = precision
         self.fdt = torch.float64 if precision == 0 else torch.float32
         self.np_fdt = np.float64 if precision == 0 else np.float32
-        opts = _lib.Options(dt, theta, c, tol, restart, max_iterations, precision, max_particles)
+        opts = _lib.Options(dt, theta, c, tol, restart, max_iterations, precision, max_particles, mass_layout)
+        self.mass_layout = mass_layout
         gr = _lib.Grid(grid.nx, grid.ny, grid.nz, grid.lx, grid.ly, grid.lz)
         h = C.c_void_p()
         _lib.check(self.lib.tpicb200_create(C.byref(gr), C.byref(opts), C.byref(h)))
@@ -98,6 +99,19 @@ class StageContext:
         _lib.check(self.lib.tpicb200_sort(self.ctx, C.byref(pin), C.byref(pout), counts.data_ptr(),
                                           offsets.data_ptr(), self.invalid.data_ptr(), self.stream))
         return dst, counts, offsets
+
+    def records(self, m) -> np.ndarray:
+        """Mass coefficients of a device buffer in TPIC's record order (float64)."""
+        a = m.cpu().numpy().astype(np.float64)
+        if self.mass_layout == 1:
+            a = np.ascontiguousarray(a.reshape(126, -1).T).ravel()
+        return a
+
+    def mass_from_records(self, rec: np.ndarray):
+        a = rec.astype(self.np_fdt)
+        if self.mass_layout == 1:
+            a = np.ascontiguousarray(a.reshape(-1, 126).T).ravel()
+        return torch.from_numpy(a).cuda()
 
     def moments(self):
         nodes = self.layout.node_count

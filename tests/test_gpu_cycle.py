@@ -23,9 +23,10 @@ def c1_case(n=16, ncycles=3, npcel=(3, 3, 3)):
     return Case(g, sp, dt=0.15, theta=0.5, gmres_tol=1e-8, ncycles=ncycles, fields=FieldInit(b0=(0.0, 0.0, 0.0195)))
 
 
-def run_both(case, precision, cycles, mass_kind="scalar"):
+def run_both(case, precision, cycles, mass_kind="scalar", mass_layout="records"):
     from tpic_b200.simulation import Simulation
-    sim = Simulation(case, precision={0: "double", 1: "mixed"}[precision], mass_kind=mass_kind)
+    sim = Simulation(case, precision={0: "double", 1: "mixed"}[precision], mass_kind=mass_kind,
+                     mass_layout=mass_layout)
     sim.prepare()
     reports = sim.run(cycles)
     arrays = O.case_species_arrays(case, precision, generate_species)
@@ -35,9 +36,10 @@ def run_both(case, precision, cycles, mass_kind="scalar"):
     return sim, reports, oc, energies
 
 
-def test_c1_cycle_matches_oracle_fp64():
+@pytest.mark.parametrize("mass_layout", ["records", "stencil-major"])
+def test_c1_cycle_matches_oracle_fp64(mass_layout):
     case = c1_case(n=16)
-    sim, reports, oc, energies = run_both(case, 0, 3)
+    sim, reports, oc, energies = run_both(case, 0, 3, mass_layout=mass_layout)
     for r, e, og in zip(reports, energies, oc.gmres):
         assert r.gmres_iterations == og.iterations
         assert abs(r.total_energy - O.total_energy(e, 2)) <= 1e-10 * abs(O.total_energy(e, 2))

@@ -208,14 +208,15 @@ def assert_moments(g, jg, mg, jw, mw, rel):
     assert np.abs(mg_i - mw_i).max() <= rel * scale + 1e-15
 
 
-@pytest.mark.parametrize("precision,kind,sorted_bins", [(0, 0, True), (0, 0, False), (1, 0, True), (1, 0, False),
-                                                        (1, 1, True), (0, 1, True)])
-def test_deposit_matches_oracle(torch_cuda, precision, kind, sorted_bins):
+@pytest.mark.parametrize("precision,kind,sorted_bins,layout", [
+    (0, 0, True, 0), (0, 0, False, 0), (1, 0, True, 0), (1, 0, False, 0), (1, 1, True, 0), (0, 1, True, 0),
+    (0, 0, True, 1), (1, 0, False, 1), (1, 0, True, 1)])
+def test_deposit_matches_oracle(torch_cuda, precision, kind, sorted_bins, layout):
     g = GRID
     rng = np.random.default_rng(21)
     d = species_arrays(g, precision, vth=(0.2, 0.1, 0.3), npcel=(3, 3, 3))
     n = len(d["cell"])
-    ctx = make_ctx(g, precision, dt=0.2)
+    ctx = make_ctx(g, precision, dt=0.2, mass_layout=layout)
     bnode = periodic_node_field(g, smooth_random_unique(g, rng, 0.9)).astype(ctx.np_fdt)
     parts = ctx.upload_particles(d)
     bn = ctx.field(bnode)
@@ -229,7 +230,7 @@ def test_deposit_matches_oracle(torch_cuda, precision, kind, sorted_bins):
     jw, mw, bad = oracle_moments(g, precision, -4.0, 0.2, d, bnode)
     assert bad == 0 and ctx.invalid_count() == 0
     rel = 3e-12 if precision == 0 else 3e-5
-    assert_moments(g, j.cpu().numpy().astype(np.float64), m.cpu().numpy().astype(np.float64), jw, mw, rel)
+    assert_moments(g, j.cpu().numpy().astype(np.float64), ctx.records(m), jw, mw, rel)
 
 
 def reference_mass_fixture(precision):
@@ -323,15 +324,16 @@ def test_reference_mass_fixture(torch_cuda, precision, kind):
     assert np.abs(gi - wi).max() <= rel * np.abs(wi).max() + 1e-15
 
 
-def test_mass_apply_matches_oracle(torch_cuda):
+@pytest.mark.parametrize("layout", [0, 1])
+def test_mass_apply_matches_oracle(torch_cuda, layout):
     g = GRID
     rng = np.random.default_rng(2)
     nodes = (g.nz + 3) * (g.ny + 3) * (g.nx + 3)
     unique = rng.normal(size=(126, g.nz, g.ny, g.nx))
     m = periodic_node_field_records(g, unique)
     v = periodic_node_field(g, smooth_random_unique(g, rng, 1.0))
-    ctx = make_ctx(g, 0)
-    out = ctx.mass_apply(ctx.field(m), ctx.field(v, np.float64)).cpu().numpy()
+    ctx = make_ctx(g, 0, mass_layout=layout)
+    out = ctx.mass_apply(ctx.mass_from_records(m), ctx.field(v, np.float64)).cpu().numpy()
     want = np.zeros(3 * nodes)
     O.load().oracle_mass_apply(0, C.byref(ogrid(g)), O.ptr(m), O.ptr(v), O.ptr(want))
     assert np.allclose(interior_nodes(g, out), interior_nodes(g, want), rtol=1e-13, atol=1e-13)
@@ -365,15 +367,16 @@ def prepared_oracle(g, precision, seed=1):
     return oc
 
 
-def test_field_solve_matches_oracle(torch_cuda):
+@pytest.mark.parametrize("layout", [0, 1])
+def test_field_solve_matches_oracle(torch_cuda, layout):
     g = GRID
     oc = prepared_oracle(g, 0)
     rng = np.random.default_rng(4)
     oc.e = periodic_node_field(g, smooth_random_unique(g, rng, 0.01))
     bcell = periodic_cell_field(g, smooth_random_unique(g, rng, 0.05))
     oc.b = bcell
-    ctx = make_ctx(g, 0, dt=0.2, tol=1e-10)
-    et, res = ctx.field_solve(ctx.field(oc.e), ctx.field(bcell), ctx.field(oc.j), ctx.field(oc.m))
+    ctx = make_ctx(g, 0, dt=0.2, tol=1e-10, mass_layout=layout)
+    et, res = ctx.field_solve(ctx.field(oc.e), ctx.field(bcell), ctx.field(oc.j), ctx.mass_from_records(oc.m))
     ores = oc.solve()
     assert res.converged and res.relative_residual <= 1e-10
     assert res.iterations == ores.iterations
@@ -434,13 +437,13 @@ def test_tc_exact_inputs(torch_cuda, kind):
     assert np.abs(got - want).max() <= 1e-6 * np.abs(want).max()
 
 
-@pytest.mark.parametrize("kind,rel", [(2, 3e-3), (3, 1e-4)])
-def test_tc_mass_matches_oracle(torch_cuda, kind, rel):
+@pytest.mark.parametrize("kind,rel,layout", [(2, 3e-3, 0), (3, 1e-4, 0), (2, 3e-3, 1), (3, 1e-4, 1)])
+def test_tc_mass_matches_oracle(torch_cuda, kind, rel, layout):
     g = GRID
     rng = np.random.default_rng(23)
     d = species_arrays(g, 1, vth=(0.2, 0.1, 0.3), npcel=(4, 4, 4))
     n = len(d["cell"])
-    ctx = make_ctx(g, 1, dt=0.2, max_particles=n)
+    ctx = make_ctx(g, 1, dt=0.2, max_particles=n, mass_layout=layout)
     bnode = periodic_node_field(g, smooth_random_unique(g, rng, 0.9)).astype(np.float32)
     parts = ctx.upload_particles(d)
     parts, counts, offsets = ctx.sort(parts, n)
@@ -449,7 +452,7 @@ def test_tc_mass_matches_oracle(torch_cuda, kind, rel):
     ctx.fold(j, m)
     jw, mw, bad = oracle_moments(g, 1, -4.0, 0.2, d, bnode)
     assert bad == 0 and ctx.invalid_count() == 0
-    jg, mg = j.cpu().numpy().astype(np.float64), m.cpu().numpy().astype(np.float64)
+    jg, mg = j.cpu().numpy().astype(np.float64), ctx.records(m)
     jw_i, jg_i = interior_nodes(g, jw), interior_nodes(g, jg)
     assert np.abs(jg_i - jw_i).max() <= 3e-5 * np.abs(jw_i).max() + 1e-15  # J-hat stays FP32
     mw_i, mg_i = interior_records(g, mw), interior_records(g, mg)

@@ -15,6 +15,7 @@ SUCCESS, INVALID_ARGUMENT, INVALID_STATE, OVERFLOW, BACKEND_FAILURE = 0, 1, 2, 3
 NOT_CONVERGED, CAPACITY_EXCEEDED, INVALID_DATA = 5, 6, 7
 PRECISION_DOUBLE, PRECISION_MIXED = 0, 1
 MASS_SCALAR, MASS_SCALAR_F64, MASS_TF32, MASS_BF16X3 = 0, 1, 2, 3
+MASS_LAYOUT_RECORDS, MASS_LAYOUT_STENCIL_MAJOR = 0, 1
 MAX_SPECIES = 8
 
 MASS_KINDS = {"scalar": MASS_SCALAR, "scalar-f64": MASS_SCALAR_F64, "fp64": MASS_SCALAR_F64,
@@ -30,7 +31,7 @@ class Grid(C.Structure):
 class Options(C.Structure):
     _fields_ = [("dt", C.c_double), ("theta", C.c_double), ("c", C.c_double), ("gmres_tol", C.c_double),
                 ("gmres_restart", C.c_int), ("gmres_max_iterations", C.c_int), ("precision", C.c_int),
-                ("max_particles", C.c_uint32)]
+                ("max_particles", C.c_uint32), ("mass_layout", C.c_int)]
 
 
 class Particles(C.Structure):

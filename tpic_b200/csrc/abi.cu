@@ -81,6 +81,8 @@ Geom make_geom(const tpicb200_grid& grid) {
   g.inv[0] = 1.0 / g.dx; g.inv[1] = 1.0 / g.dy; g.inv[2] = 1.0 / g.dz;
   g.volume = (g.dx * g.dy) * g.dz;
   g.inv_volume = 1.0 / g.volume;
+  g.mvs = 126;
+  g.mes = 1;
   return g;
 }
 }  // namespace tpicb200
@@ -107,6 +109,9 @@ int tpicb200_create(const tpicb200_grid* grid, const tpicb200_options* options, 
     return fail(TPICB200_INVALID_ARGUMENT, "invalid time step, theta, c or GMRES parameters");
   if (options->precision != TPICB200_PRECISION_DOUBLE && options->precision != TPICB200_PRECISION_MIXED)
     return fail(TPICB200_INVALID_ARGUMENT, "unknown precision mode");
+  if (options->mass_layout != TPICB200_MASS_LAYOUT_RECORDS &&
+      options->mass_layout != TPICB200_MASS_LAYOUT_STENCIL_MAJOR)
+    return fail(TPICB200_INVALID_ARGUMENT, "unknown mass layout");
   int device = 0, count = 0;
   if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
     return fail(TPICB200_BACKEND_FAILURE, "no CUDA device: the ECSIM cycle has no CPU fallback");
@@ -117,6 +122,10 @@ int tpicb200_create(const tpicb200_grid* grid, const tpicb200_options* options, 
   auto* ctx = new tpicb200_context();
   ctx->device = device;
   ctx->g = make_geom(*grid);
+  if (options->mass_layout == TPICB200_MASS_LAYOUT_STENCIL_MAJOR) {
+    ctx->g.mvs = 1;
+    ctx->g.mes = ctx->g.nodes;
+  }
   ctx->opt = *options;
   cudaError_t e = cudaSuccess;
   ctx->solver = solver_create(options->precision, ctx->g, options->gmres_restart, options->dt,

@@ -25,6 +25,13 @@ struct Geom {
   double inv[3];       // 1/spacing
   double volume;       // (dx*dy)*dz
   double inv_volume;   // 1/volume
+  // Mass storage: entry k = 9*stencil + component of vertex v lives at
+  // v*mvs + k*mes: (126, 1) for TPIC's records, (1, nodes) stencil-major.
+  long long mvs, mes;
+
+  __host__ __device__ __forceinline__ long long mass_index(long long vertex, int k) const {
+    return vertex * mvs + (long long)k * mes;
+  }
 
   __host__ __device__ __forceinline__ long long node(int i, int j, int k) const {
     return (long long)(i + 1) + (long long)NX * ((j + 1) + (long long)NY * (k + 1));

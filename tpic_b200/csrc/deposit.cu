@@ -123,11 +123,10 @@ __global__ void __launch_bounds__(128) unsorted_deposit_kernel(Geom g, DepositPa
           if (s < 0) continue;
           const MC pw = wt[a] * wt[bb];
           if (pw == MC(0)) continue;
-          Mass* rec = M + nodes[a] * 126 + s * 9;
 #pragma unroll
           for (int e = 0; e < 9; ++e) {
             const Mass amount = Mass(as[e] * pw);
-            if (amount != Mass(0)) atomicAdd(rec + e, amount);
+            if (amount != Mass(0)) atomicAdd(M + g.mass_index(nodes[a], s * 9 + e), amount);
           }
         }
     }
@@ -318,12 +317,11 @@ __global__ void __launch_bounds__(128) sorted_deposit_kernel(Geom g, DepositPara
 #pragma unroll
       for (int slot = 0; slot < 2; ++slot) {
         if (stencil[slot] < 0) continue;
-        Mass* rec = M + vertex * 126 + stencil[slot] * 9;
 #pragma unroll
         for (int e = 0; e < 9; ++e) {
           const Mass amount = Mass(macc[slot][e]);
           if (!isfinite(amount)) atomicAdd(invalid, 1u);
-          else if (amount != Mass(0)) atomicAdd(rec + e, amount);
+          else if (amount != Mass(0)) atomicAdd(M + g.mass_index(vertex, stencil[slot] * 9 + e), amount);
         }
       }
     }
@@ -352,11 +350,16 @@ __global__ void __launch_bounds__(256) fold_mass_kernel(Geom g, T* __restrict__ 
   const long long total = shell_count(g) * 126;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
-    const long long sv = t / 126, e = t - sv * 126;
+    // Records: consecutive threads copy consecutive entries of one record;
+    // stencil-major: consecutive threads copy one entry of consecutive vertices.
+    const long long shell = shell_count(g);
+    long long sv, e;
+    if (g.mes == 1) { sv = t / 126; e = t - sv * 126; }
+    else { e = t / shell; sv = t - e * shell; }
     int i, j, k;
     shell_coordinates(g, sv, i, j, k);
-    m[g.node(i, j, k) * 126 + e] =
-        m[g.node(wrap_index(i, g.nx), wrap_index(j, g.ny), wrap_index(k, g.nz)) * 126 + e];
+    m[g.mass_index(g.node(i, j, k), int(e))] =
+        m[g.mass_index(g.node(wrap_index(i, g.nx), wrap_index(j, g.ny), wrap_index(k, g.nz)), int(e))];
   }
 }
 

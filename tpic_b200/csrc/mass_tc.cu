@@ -13,8 +13,10 @@
 // Tensor-core mapping (one CTA of four warps works on four cells at once):
 //   A (tensor memory, M = 128 lanes x K columns): lane 32w + t holds m_pt of
 //     cell w's particles (rows 27..31 of each quadrant are zero);
-//   B (shared memory, K x N = 48, MN-major, no swizzle): columns 12w..12w+8
-//     hold s_p alpha_p of cell w's particle p (the rest zero);
+//   B (shared memory, K x N, no swizzle): columns 12w..12w+8 (TF32, N = 48,
+//     K-major core matrices of 8 N-rows x 4 K-values) or 16w..16w+8 (BF16,
+//     N = 64, MN-major core matrices of 8 K-rows x 8 N-values) hold
+//     s_p alpha_p of cell w's particle p (the rest zero);
 //   D (tensor memory, 128 x 48 FP32): D[32w + t][12w + c] = G_w[t][c]; the
 //     off-diagonal blocks are never read.
 // Each 32-particle chunk is four tcgen05.mma.kind::tf32 (K = 8) issued by one
@@ -45,13 +47,16 @@ constexpr int kChunk = 32;         // particles per chunk (one per lane)
 constexpr int kFacStride = 36;     // floats per factor row (padded against bank conflicts)
 constexpr uint32_t kTmemCols = 128;
 constexpr uint32_t kDcol = 64;
-// Per form: B columns per cell, N, bytes of one B tile (N-chunks of 16 bytes,
-// each 4 K-groups x 128 bytes for a 32-particle chunk), B tiles per buffer.
+// Per form: B columns per cell, N, bytes of one B tile, B tiles per buffer.
+// TF32 (K-major): 8 K-chunks of 4 particles, each 6 N-groups x 128 bytes,
+// padded by 16 bytes (K-chunk stride 784 B) so the 32 lanes' 4-byte stores
+// of one column fall in 32 different banks.
+// BF16 (MN-major): 8 N-chunks of 8 values, each 4 K-groups x 128 bytes.
+constexpr uint32_t kTf32KChunk = 6 * 128 + 16;
 template <bool Bf16> struct Form {
   static constexpr int cols = Bf16 ? 16 : 12;
   static constexpr int n = kCells * cols;
-  static constexpr int per_chunk16 = Bf16 ? 8 : 4;   // values per 16-byte N-chunk
-  static constexpr uint32_t tile_bytes = uint32_t(n / per_chunk16) * 512u;
+  static constexpr uint32_t tile_bytes = Bf16 ? uint32_t(n / 8) * 512u : 8u * kTf32KChunk;
   static constexpr int tiles = Bf16 ? 2 : 1;         // hi (+ lo)
 };
 
@@ -130,7 +135,7 @@ __global__ void __launch_bounds__(128, 1) tc_deposit_kernel(Geom g, TcParams tp,
   tc::fence_after_sync();
   const uint32_t tmem = sh.tmem_base;
   const uint32_t lane_base = uint32_t(32 * warp) << 16;
-  constexpr uint32_t idesc = tc::instr_desc(Bf16 ? 1u : 2u, 128, kN);
+  constexpr uint32_t idesc = tc::instr_desc(Bf16 ? 1u : 2u, 128, kN, Bf16 ? 1u : 0u);
   uint32_t phase[2] = {0, 0};
   bool pending[2] = {false, false};
   int buf = 0;
@@ -142,22 +147,58 @@ __global__ void __launch_bounds__(128, 1) tc_deposit_kernel(Geom g, TcParams tp,
   const int t_row = lane;
   const int tx = t_row % 3, tyz = t_row / 3;
 
-  for (long long grp = blockIdx.x; grp < groups && !failed; grp += gridDim.x) {
-    const long long cell = grp * kCells + warp;
-    const bool live = cell < cells;
-    int ci = 0, cj = 0, ck = 0;
-    uint32_t count = 0, first = 0;
-    int32_t bin = -1;
-    if (live) {
-      ci = int(cell % g.nx); cj = int((cell / g.nx) % g.ny); ck = int(cell / ((long long)g.nx * g.ny));
-      bin = g.encode(ci, cj, ck);
-      count = counts[bin];
-      first = offsets[bin];
+  // Software pipeline: the metadata and B corners of the next group and the
+  // records of the next chunk (possibly the next group's first) are loaded
+  // while the current chunk is produced and consumed.
+  struct Meta {
+    int ci, cj, ck;
+    uint32_t count, first;
+    int32_t bin;
+    bool live;
+    float bval;  // lane < 24: B corner (lane / 3) component (lane % 3)
+  };
+  struct Rec {
+    double fx, fy, fz, q;
+    float u, v, w;
+    int32_t key;
+    bool present;
+  };
+  auto load_meta = [&](long long grp_) {
+    Meta m{0, 0, 0, 0u, 0u, -1, false, 0.0f};
+    const long long cell = grp_ * kCells + warp;
+    if (grp_ < groups && cell < cells) {
+      m.live = true;
+      m.ci = int(cell % g.nx); m.cj = int((cell / g.nx) % g.ny); m.ck = int(cell / ((long long)g.nx * g.ny));
+      m.bin = g.encode(m.ci, m.cj, m.ck);
+      m.count = counts[m.bin];
+      m.first = offsets[m.bin];
       if (lane < 24) {
         const int a = lane / 3, c = lane % 3;
-        sh.bcache[warp][lane] = bnode[c * nn + g.node(ci + (a & 1), cj + ((a >> 1) & 1), ck + ((a >> 2) & 1))];
+        m.bval = bnode[c * nn + g.node(m.ci + (a & 1), m.cj + ((a >> 1) & 1), m.ck + ((a >> 2) & 1))];
       }
     }
+    return m;
+  };
+  auto load_rec = [&](const Meta& m, uint32_t k) {
+    Rec r{0.0, 0.0, 0.0, 0.0, 0.0f, 0.0f, 0.0f, -1, false};
+    if (k < m.count) {
+      const uint32_t n = m.first + k;
+      r.present = true;
+      r.fx = rx[n]; r.fy = ry[n]; r.fz = rz[n]; r.q = q[n];
+      r.u = u[n]; r.v = v[n]; r.w = w[n]; r.key = key[n];
+    }
+    return r;
+  };
+  Meta cur = load_meta(blockIdx.x);
+  Rec pre = load_rec(cur, lane);
+
+  for (long long grp = blockIdx.x; grp < groups && !failed; grp += gridDim.x) {
+    const Meta nxt = load_meta(grp + gridDim.x);
+    const bool live = cur.live;
+    const int ci = cur.ci, cj = cur.cj, ck = cur.ck;
+    const uint32_t count = cur.count;
+    const int32_t bin = cur.bin;
+    if (live && lane < 24) sh.bcache[warp][lane] = cur.bval;
     if (lane == 0) sh.count[warp] = count;
     __syncthreads();
     uint32_t maxc = sh.count[0];
@@ -166,6 +207,7 @@ __global__ void __launch_bounds__(128, 1) tc_deposit_kernel(Geom g, TcParams tp,
     float jsum[24];
 #pragma unroll
     for (int t = 0; t < 24; ++t) jsum[t] = 0.0f;
+    if (maxc == 0) pre = load_rec(nxt, lane);
 
     for (uint32_t chunk = 0; chunk < maxc; chunk += kChunk) {
       // The buffer is free once the MMAs that read it have completed.
@@ -175,18 +217,18 @@ __global__ void __launch_bounds__(128, 1) tc_deposit_kernel(Geom g, TcParams tp,
         phase[buf] ^= 1u;
         pending[buf] = false;
       }
+      const Rec rec = pre;
+      pre = chunk + kChunk < maxc ? load_rec(cur, chunk + kChunk + lane) : load_rec(nxt, lane);
       // Particle phase: one record per lane.
-      const uint32_t k = chunk + lane;
       float bv[kCols];
       float fac[12];
 #pragma unroll
       for (int c = 0; c < kCols; ++c) bv[c] = 0.0f;
 #pragma unroll
       for (int f = 0; f < 12; ++f) fac[f] = 0.0f;
-      if (k < count) {
-        const uint32_t n = first + k;
-        const double fx = rx[n], fy = ry[n], fz = rz[n];
-        if (key[n] == bin && fx >= 0 && fx < 1 && fy >= 0 && fy < 1 && fz >= 0 && fz < 1) {
+      if (rec.present) {
+        const double fx = rec.fx, fy = rec.fy, fz = rec.fz;
+        if (rec.key == bin && fx >= 0 && fx < 1 && fy >= 0 && fy < 1 && fz >= 0 && fz < 1) {
           const float x = float(fx), y = float(fy), z = float(fz);
           float wt[8];
           cic_weights<float>(x, y, z, wt);
@@ -199,9 +241,9 @@ __global__ void __launch_bounds__(128, 1) tc_deposit_kernel(Geom g, TcParams tp,
             b[c] = val;
           }
           const Response<float> r(b[0], b[1], b[2], tp.beta_over_c);
-          const float charge = float(q[n]);
+          const float charge = float(rec.q);
           float hx, hy, hz;
-          r.apply(u[n], v[n], w[n], hx, hy, hz);
+          r.apply(rec.u, rec.v, rec.w, hx, hy, hz);
           const float qv = charge * tp.inv_volume;
           const float jc[3] = {qv * hx, qv * hy, qv * hz};
           const float scale = tp.beta_over_c * charge;
@@ -231,15 +273,12 @@ __global__ void __launch_bounds__(128, 1) tc_deposit_kernel(Geom g, TcParams tp,
       // B tile (MN-major core matrices: 8 K-rows x 16 bytes of N-values,
       // K-groups 128 B apart, 16-byte N-chunks 512 B apart).
       if constexpr (!Bf16) {
-        uint8_t* bt = sh.btile[buf][0];
+        // K-major: value (n, k) at (n%8)*16 + (n/8)*128 + (k/4)*784 + (k%4)*4.
+        uint8_t* bt = sh.btile[buf][0] + (lane >> 2) * kTf32KChunk + (lane & 3) * 4;
 #pragma unroll
-        for (int j = 0; j < kCols / 4; ++j) {
-          uint4 pack;
-          pack.x = tc::to_tf32(bv[4 * j + 0]);
-          pack.y = tc::to_tf32(bv[4 * j + 1]);
-          pack.z = tc::to_tf32(bv[4 * j + 2]);
-          pack.w = tc::to_tf32(bv[4 * j + 3]);
-          *reinterpret_cast<uint4*>(bt + (3 * warp + j) * 512 + (lane >> 3) * 128 + (lane & 7) * 16) = pack;
+        for (int c = 0; c < kCols; ++c) {
+          const int nn = kCols * warp + c;
+          *reinterpret_cast<uint32_t*>(bt + (nn & 7) * 16 + (nn >> 3) * 128) = tc::to_tf32(bv[c]);
         }
       } else {
         float hi[kCols], lo[kCols];
@@ -317,7 +356,8 @@ __global__ void __launch_bounds__(128, 1) tc_deposit_kernel(Geom g, TcParams tp,
           const uint32_t bbase = tc::smem_u32(sh.btile[buf][0]);
 #pragma unroll
           for (int s = 0; s < 4; ++s)
-            tc::mma_tf32_ts(tmem + kDcol, abase + 8 * s, tc::smem_desc(bbase + s * 128, 128, 512), idesc,
+            tc::mma_tf32_ts(tmem + kDcol, abase + 8 * s,
+                            tc::smem_desc(bbase + 2 * s * kTf32KChunk, kTf32KChunk, 128), idesc,
                             (chunk > 0 || s > 0) ? 1u : 0u);
         } else {
           const uint32_t bhi = tc::smem_u32(sh.btile[buf][0]), blo = tc::smem_u32(sh.btile[buf][1]);
@@ -408,10 +448,10 @@ __global__ void __launch_bounds__(128, 1) tc_deposit_kernel(Geom g, TcParams tp,
           const int np = c_pairs.count[t_row];
           for (int p = 0; p < np; ++p) {
             const int a = c_pairs.corner[t_row][p], s = c_pairs.stencil[t_row][p];
-            float* rec = M + wrapped(g, ci + (a & 1), cj + ((a >> 1) & 1), ck + ((a >> 2) & 1)) * 126 + s * 9;
+            const long long vertex = wrapped(g, ci + (a & 1), cj + ((a >> 1) & 1), ck + ((a >> 2) & 1));
 #pragma unroll
             for (int e = 0; e < 9; ++e)
-              if (G[e] != 0.0f) atomicAdd(rec + e, G[e]);
+              if (G[e] != 0.0f) atomicAdd(M + g.mass_index(vertex, s * 9 + e), G[e]);
           }
         }
       }
@@ -421,6 +461,7 @@ __global__ void __launch_bounds__(128, 1) tc_deposit_kernel(Geom g, TcParams tp,
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
+    cur = nxt;
   }
 
   if (failed && threadIdx.x == 0) atomicAdd(invalid, 1u << 20);

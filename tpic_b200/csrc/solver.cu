@@ -53,10 +53,11 @@ __device__ __forceinline__ void cell_curl(const Geom& g, const double* __restric
 }
 
 template <class C, class M>
-__device__ __forceinline__ void block_product(const M* __restrict__ b, C vx, C vy, C vz, C& x, C& y, C& z) {
-  x = vx * C(b[0]) + vy * C(b[1]) + vz * C(b[2]);
-  y = vx * C(b[3]) + vy * C(b[4]) + vz * C(b[5]);
-  z = vx * C(b[6]) + vy * C(b[7]) + vz * C(b[8]);
+__device__ __forceinline__ void block_product(const M* __restrict__ b, long long es, C vx, C vy, C vz, C& x, C& y,
+                                              C& z) {
+  x = vx * C(b[0]) + vy * C(b[es]) + vz * C(b[2 * es]);
+  y = vx * C(b[3 * es]) + vy * C(b[4 * es]) + vz * C(b[5 * es]);
+  z = vx * C(b[6 * es]) + vy * C(b[7 * es]) + vz * C(b[8 * es]);
 }
 
 // (M v)_g before the row volume scale: centre, then per stencil the forward
@@ -69,56 +70,147 @@ __device__ __forceinline__ void mass_product(const Geom& g, const M* __restrict_
   const long long nn = g.nodes;
   const long long at = g.node(i, j, k);
   C x, y, z;
-  block_product<C>(mass + at * 126, C(v[at]), C(v[nn + at]), C(v[2 * nn + at]), x, y, z);
+  const long long es = g.mes;
+  block_product<C>(mass + g.mass_index(at, 0), es, C(v[at]), C(v[nn + at]), C(v[2 * nn + at]), x, y, z);
 #pragma unroll
   for (int s = 1; s < 14; ++s) {
     const long long d = stencil_offset(s, 0) + (long long)g.NX * (stencil_offset(s, 1) + (long long)g.NY * stencil_offset(s, 2));
     C bx, by, bz;
     const long long f = at + d, b = at - d;
-    block_product<C>(mass + at * 126 + s * 9, C(v[f]), C(v[nn + f]), C(v[2 * nn + f]), bx, by, bz);
+    block_product<C>(mass + g.mass_index(at, s * 9), es, C(v[f]), C(v[nn + f]), C(v[2 * nn + f]), bx, by, bz);
     x += bx; y += by; z += bz;
-    block_product<C>(mass + b * 126 + s * 9, C(v[b]), C(v[nn + b]), C(v[2 * nn + b]), bx, by, bz);
+    block_product<C>(mass + g.mass_index(b, s * 9), es, C(v[b]), C(v[nn + b]), C(v[2 * nn + b]), bx, by, bz);
     x += bx; y += by; z += bz;
   }
   out[0] = x; out[1] = y; out[2] = z;
 }
 
+// Tile of unique nodes per CTA: 32 (x) x 4 (y) x 2 (z) = 256 threads.
+constexpr int kTX = 32, kTY = 4, kTZ = 2;
+
+// A(v) over the unique nodes [0,n)^3 of a tile. The input (ghosts filled) is
+// staged in shared memory with its one-node halo, each cell curl the tile
+// needs is computed once into shared memory, then every thread forms its
+// node's C2N curl, 27-block mass product and combination. Rows of the
+// duplicate endpoint planes equal their unique node's row (same inputs, same
+// operations) and are copied by duplicate_rows_kernel.
 template <class C, class M, class Out>
-__global__ void __launch_bounds__(kThreads) maxwell_apply_kernel(Geom g, C d2, C kfac, C inv_volume,
-                                                                 const M* __restrict__ mass,
-                                                                 const double* __restrict__ v,
-                                                                 Out* __restrict__ out) {
+__global__ void __launch_bounds__(kTX * kTY * kTZ) maxwell_apply_kernel(Geom g, C d2, C kfac, C inv_volume,
+                                                                        const M* __restrict__ mass,
+                                                                        const double* __restrict__ v,
+                                                                        Out* __restrict__ out) {
+  constexpr int VX = kTX + 2, VY = kTY + 2, VZ = kTZ + 2;   // nodes i0-1 .. i0+TX
+  constexpr int CX = kTX + 1, CY = kTY + 1, CZ = kTZ + 1;   // cells i0-1 .. i0+TX-1
+  __shared__ C vs[3][VZ][VY][VX];
+  __shared__ C cs[3][CZ][CY][CX];
   const C inv[3] = {C(g.inv[0]), C(g.inv[1]), C(g.inv[2])};
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < g.interior;
-       t += (long long)gridDim.x * blockDim.x) {
-    int i, j, k;
-    compact_coordinates(g, t, i, j, k);
-    // Cell curls: base (i,j,k), x (i-1), y (j-1), z (k-1), xy, xz, yz, xyz.
-    C cc[8][3];
-    cell_curl<C>(g, v, i, j, k, inv, cc[0]);
-    cell_curl<C>(g, v, i - 1, j, k, inv, cc[1]);
-    cell_curl<C>(g, v, i, j - 1, k, inv, cc[2]);
-    cell_curl<C>(g, v, i, j, k - 1, inv, cc[3]);
-    cell_curl<C>(g, v, i - 1, j - 1, k, inv, cc[4]);
-    cell_curl<C>(g, v, i - 1, j, k - 1, inv, cc[5]);
-    cell_curl<C>(g, v, i, j - 1, k - 1, inv, cc[6]);
-    cell_curl<C>(g, v, i - 1, j - 1, k - 1, inv, cc[7]);
-    // C2N curl of the cell curls (cell sources: anchor - neighbour).
-    auto dx = [&](int c) { return C(0.25) * inv[0] * (cc[0][c] - cc[1][c] + (cc[3][c] - cc[5][c]) + (cc[2][c] - cc[4][c]) + (cc[6][c] - cc[7][c])); };
-    auto dy = [&](int c) { return C(0.25) * inv[1] * (cc[0][c] - cc[2][c] + (cc[3][c] - cc[6][c]) + (cc[1][c] - cc[4][c]) + (cc[5][c] - cc[7][c])); };
-    auto dz = [&](int c) { return C(0.25) * inv[2] * (cc[0][c] - cc[3][c] + (cc[1][c] - cc[5][c]) + (cc[2][c] - cc[6][c]) + (cc[4][c] - cc[7][c])); };
-    const C curl2[3] = {dy(2) - dz(1), dz(0) - dx(2), dx(1) - dy(0)};
-    C mv[3];
-    mass_product<C>(g, mass, v, i, j, k, mv);
-    const long long at = g.node(i, j, k);
+  const int tiles_x = (g.nx + kTX - 1) / kTX, tiles_y = (g.ny + kTY - 1) / kTY;
+  const int tx = blockIdx.x % tiles_x, ty = (blockIdx.x / tiles_x) % tiles_y, tz = blockIdx.x / (tiles_x * tiles_y);
+  const int i0 = tx * kTX, j0 = ty * kTY, k0 = tz * kTZ;
+  const long long nn = g.nodes;
+  // Stage v over nodes [i0-1, i0+TX] x [j0-1, j0+TY] x [k0-1, k0+TZ]; nodes
+  // beyond n+1 (partial tiles) are never read by a live node and load 0.
+  for (int t = threadIdx.x; t < 3 * VZ * VY * VX; t += blockDim.x) {
+    const int c = t / (VZ * VY * VX), r = t % (VZ * VY * VX);
+    const int lx = r % VX, ly = (r / VX) % VY, lz = r / (VX * VY);
+    const int i = i0 - 1 + lx, j = j0 - 1 + ly, k = k0 - 1 + lz;
+    C val = C(0);
+    if (i <= g.nx + 1 && j <= g.ny + 1 && k <= g.nz + 1) val = C(v[c * nn + g.node(i, j, k)]);
+    vs[c][lz][ly][lx] = val;
+  }
+  __syncthreads();
+  // Cell curls (curl_N2C, ecsim/fields/node_cell_curl.hpp:116-126) of cells
+  // [i0-1, i0+TX-1] x ... from the staged nodes.
+  for (int t = threadIdx.x; t < CZ * CY * CX; t += blockDim.x) {
+    const int lx = t % CX, ly = (t / CX) % CY, lz = t / (CX * CY);
+    C q[3][8];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      // The mass image is narrowed to the solver storage (double) before the
-      // combination reads it back (maxwell_device.hpp:424-429,471-484).
-      const C m = C(double(mv[c] * inv_volume));
-      const C value = (C(1) * C(v[c * g.nodes + at]) + d2 * C(double(curl2[c]))) + kfac * m;
-      out[c * g.interior + t] = Out(value);
+      q[c][0] = vs[c][lz][ly][lx];         q[c][1] = vs[c][lz][ly][lx + 1];
+      q[c][2] = vs[c][lz][ly + 1][lx];     q[c][3] = vs[c][lz + 1][ly][lx];
+      q[c][4] = vs[c][lz][ly + 1][lx + 1]; q[c][5] = vs[c][lz + 1][ly][lx + 1];
+      q[c][6] = vs[c][lz + 1][ly + 1][lx]; q[c][7] = vs[c][lz + 1][ly + 1][lx + 1];
     }
+    auto dx = [&](const C* p) { return C(0.25) * inv[0] * (p[1] - p[0] + (p[5] - p[3]) + (p[4] - p[2]) + (p[7] - p[6])); };
+    auto dy = [&](const C* p) { return C(0.25) * inv[1] * (p[2] - p[0] + (p[6] - p[3]) + (p[4] - p[1]) + (p[7] - p[5])); };
+    auto dz = [&](const C* p) { return C(0.25) * inv[2] * (p[3] - p[0] + (p[5] - p[1]) + (p[6] - p[2]) + (p[7] - p[4])); };
+    // The cell curl is stored in the solver storage (double) between the two
+    // curls of the reference; a float curl survives that round trip exactly.
+    cs[0][lz][ly][lx] = C(double(dy(q[2]) - dz(q[1])));
+    cs[1][lz][ly][lx] = C(double(dz(q[0]) - dx(q[2])));
+    cs[2][lz][ly][lx] = C(double(dx(q[1]) - dy(q[0])));
+  }
+  __syncthreads();
+  const int lx = threadIdx.x % kTX, ly = (threadIdx.x / kTX) % kTY, lz = threadIdx.x / (kTX * kTY);
+  const int i = i0 + lx, j = j0 + ly, k = k0 + lz;
+  if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+  // C2N curl of the cell curls (cell sources: anchor - neighbour); the cell
+  // (i-a, j-b, k-c) of the reference's samples is cs[..][lz+1-c][ly+1-b][lx+1-a].
+  C curl2[3];
+  {
+    C p[3][8];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      p[c][0] = cs[c][lz + 1][ly + 1][lx + 1]; p[c][1] = cs[c][lz + 1][ly + 1][lx];
+      p[c][2] = cs[c][lz + 1][ly][lx + 1];     p[c][3] = cs[c][lz][ly + 1][lx + 1];
+      p[c][4] = cs[c][lz + 1][ly][lx];         p[c][5] = cs[c][lz][ly + 1][lx];
+      p[c][6] = cs[c][lz][ly][lx + 1];         p[c][7] = cs[c][lz][ly][lx];
+    }
+    auto dx = [&](const C* q) { return C(0.25) * inv[0] * (q[0] - q[1] + (q[3] - q[5]) + (q[2] - q[4]) + (q[6] - q[7])); };
+    auto dy = [&](const C* q) { return C(0.25) * inv[1] * (q[0] - q[2] + (q[3] - q[6]) + (q[1] - q[4]) + (q[5] - q[7])); };
+    auto dz = [&](const C* q) { return C(0.25) * inv[2] * (q[0] - q[3] + (q[1] - q[5]) + (q[2] - q[6]) + (q[4] - q[7])); };
+    curl2[0] = dy(p[2]) - dz(p[1]);
+    curl2[1] = dz(p[0]) - dx(p[2]);
+    curl2[2] = dx(p[1]) - dy(p[0]);
+  }
+  // Mass product: centre, then forward and backward blocks per stencil,
+  // untransposed (apply_mass_matrix_node, mass_matrix_stencil.hpp:119-149).
+  const long long at = g.node(i, j, k), es = g.mes;
+  auto vv = [&](int c, int a, int b, int d) { return vs[c][lz + 1 + d][ly + 1 + b][lx + 1 + a]; };
+  C x, y, z;
+  block_product<C>(mass + g.mass_index(at, 0), es, vv(0, 0, 0, 0), vv(1, 0, 0, 0), vv(2, 0, 0, 0), x, y, z);
+#pragma unroll
+  for (int s = 1; s < 14; ++s) {
+    const int ox = stencil_offset(s, 0), oy = stencil_offset(s, 1), oz = stencil_offset(s, 2);
+    const long long d = ox + (long long)g.NX * (oy + (long long)g.NY * oz);
+    C bx, by, bz;
+    block_product<C>(mass + g.mass_index(at, s * 9), es, vv(0, ox, oy, oz), vv(1, ox, oy, oz), vv(2, ox, oy, oz),
+                     bx, by, bz);
+    x += bx; y += by; z += bz;
+    block_product<C>(mass + g.mass_index(at - d, s * 9), es, vv(0, -ox, -oy, -oz), vv(1, -ox, -oy, -oz),
+                     vv(2, -ox, -oy, -oz), bx, by, bz);
+    x += bx; y += by; z += bz;
+  }
+  const C mv[3] = {x, y, z};
+  const long long row = i + (long long)g.inx * (j + (long long)g.iny * k);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    // The mass image is narrowed to the solver storage (double) before the
+    // combination reads it back (maxwell_device.hpp:424-429,471-484).
+    const C m = C(double(mv[c] * inv_volume));
+    const C value = (C(1) * vv(c, 0, 0, 0) + d2 * C(double(curl2[c]))) + kfac * m;
+    out[c * g.interior + row] = Out(value);
+  }
+}
+
+// Rows of the duplicate endpoint planes (index n on some axis) copy the row
+// of their periodic unique node.
+template <class Out>
+__global__ void __launch_bounds__(kThreads) duplicate_rows_kernel(Geom g, Out* __restrict__ out) {
+  // Compact rows with i == n, or j == n, or k == n: three slabs as in shell_coordinates.
+  const long long zs = (long long)g.inx * g.iny, ys = (long long)g.inx * g.nz, xs = (long long)g.ny * g.nz;
+  const long long total = zs + ys + xs;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 3 * total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int c = int(t / total);
+    long long r = t - c * total;
+    int i, j, k;
+    if (r < zs) { k = g.nz; i = int(r % g.inx); j = int(r / g.inx); }
+    else if ((r -= zs) < ys) { j = g.ny; i = int(r % g.inx); k = int(r / g.inx); }
+    else { r -= ys; i = g.nx; j = int(r % g.ny); k = int(r / g.ny); }
+    const int ui = i == g.nx ? 0 : i, uj = j == g.ny ? 0 : j, uk = k == g.nz ? 0 : k;
+    out[c * g.interior + i + (long long)g.inx * (j + (long long)g.iny * k)] =
+        out[c * g.interior + ui + (long long)g.inx * (uj + (long long)g.iny * uk)];
   }
 }
 
@@ -437,11 +529,15 @@ struct Solve {
   void check() { if (err == cudaSuccess) err = cudaGetLastError(); }
 
   template <class C, class Out> void apply(const Mass* mass, Out* out) {
-    launch_node_ghosts(w->g, w->input, 3, s);
-    const double iv = w->g.inv_volume;
-    maxwell_apply_kernel<C, Mass, Out><<<blocks(), kThreads, 0, s>>>(
-        w->g, C(w->delta * w->delta), C(w->kfac), C(iv), mass, w->input, out);
-    count_launches(1);
+    const Geom& g = w->g;
+    launch_node_ghosts(g, w->input, 3, s);
+    const double iv = g.inv_volume;
+    const unsigned tiles = unsigned(((g.nx + kTX - 1) / kTX) * ((g.ny + kTY - 1) / kTY) * ((g.nz + kTZ - 1) / kTZ));
+    maxwell_apply_kernel<C, Mass, Out><<<tiles, kTX * kTY * kTZ, 0, s>>>(
+        g, C(w->delta * w->delta), C(w->kfac), C(iv), mass, w->input, out);
+    const long long dup = (long long)g.inx * g.iny + (long long)g.inx * g.nz + (long long)g.ny * g.nz;
+    duplicate_rows_kernel<Out><<<grid_for(3 * dup, kThreads), kThreads, 0, s>>>(g, out);
+    count_launches(2);
     check();
   }
   void reduce(int filled) {

@@ -92,9 +92,11 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t start, uint32_t lbo, uint
 }
 
 // Instruction descriptor: F32 accumulator, A/B format (0 F16, 1 BF16, 2 TF32),
-// A K-major (A comes from tensor memory), B MN-major, M and N.
-__host__ __device__ constexpr uint32_t instr_desc(uint32_t ab_format, uint32_t m, uint32_t n) {
-  return (1u << 4) | (ab_format << 7) | (ab_format << 10) | (1u << 16) | ((n >> 3) << 17) | ((m >> 4) << 24);
+// A K-major (A comes from tensor memory), B MN-major (b_mn = 1) or K-major,
+// M and N. (With TF32 operands a no-swizzle MN-major B produced zero results
+// on this part; the TF32 form uses a K-major B.)
+__host__ __device__ constexpr uint32_t instr_desc(uint32_t ab_format, uint32_t m, uint32_t n, uint32_t b_mn = 1) {
+  return (1u << 4) | (ab_format << 7) | (ab_format << 10) | (b_mn << 16) | ((n >> 3) << 17) | ((m >> 4) << 24);
 }
 
 __device__ __forceinline__ uint32_t to_tf32(float x) {

@@ -40,7 +40,7 @@ def _ptr(t) -> int:
 class Simulation:
     def __init__(self, case: Case, precision: str = "double", mass_kind: str = "scalar",
                  device: int = 0, gmres_restart: int = 30, gmres_max_iterations: int = 100,
-                 keep_ids: bool = False, generate_on_device: bool = False):
+                 keep_ids: bool = False, generate_on_device: bool = False, mass_layout: str = "stencil-major"):
         self.case = case
         self.lib = _lib.load()
         self.precision = _lib.PRECISIONS[precision]
@@ -54,8 +54,10 @@ class Simulation:
         if len(counts) > _lib.MAX_SPECIES:
             raise ValueError("too many species")
         grid = _lib.Grid(g.nx, g.ny, g.nz, g.lx, g.ly, g.lz)
+        self.mass_layout = {"records": _lib.MASS_LAYOUT_RECORDS,
+                            "stencil-major": _lib.MASS_LAYOUT_STENCIL_MAJOR}[mass_layout]
         opts = _lib.Options(case.dt, case.theta, case.c, case.gmres_tol, gmres_restart,
-                            gmres_max_iterations, self.precision, max(counts))
+                            gmres_max_iterations, self.precision, max(counts), self.mass_layout)
         handle = C.c_void_p()
         _lib.check(self.lib.tpicb200_create(C.byref(grid), C.byref(opts), C.byref(handle)))
         self.ctx = handle
