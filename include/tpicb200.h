@@ -206,8 +206,12 @@ int tpicb200_sort(tpicb200_context* ctx, const tpicb200_particles* in, tpicb200_
 int tpicb200_clear_moments(tpicb200_context* ctx, void* j, void* mass, tpicb200_stream stream);
 
 /* Implicit current and mass-matrix deposition of one species, added into j
- * and mass (either may be NULL) at the periodic unique nodes; call
- * tpicb200_fold_periodic after the last species. With counts/offsets (the
+ * and mass (either may be NULL for the scalar forms) at the periodic unique
+ * nodes; call tpicb200_fold_periodic after the last species. The
+ * tensor-core forms (TF32, BF16X3; mixed precision, sorted bins) keep the
+ * cell moments of every species deposited since tpicb200_clear_moments in
+ * the context and tpicb200_fold_periodic adds them into j and mass, with no
+ * atomics and a fixed summation order. With counts/offsets (the
  * bins of p, from tpicb200_sort) the sorted cell-tile kernels run; with NULL
  * bins the per-particle kernels run (scalar forms only). Replaces
  * enqueue_sorted_current / enqueue_unsorted_current
@@ -219,8 +223,9 @@ int tpicb200_deposit(tpicb200_context* ctx, double qom, const tpicb200_particles
                      void* j, void* mass, int mass_kind, uint32_t* invalid,
                      tpicb200_stream stream);
 
-/* Periodic fold: the duplicate endpoint nodes and the one-node ghosts of j
- * and of the mass records take the values of their periodic unique node.
+/* Periodic fold: pending tensor-core cell moments are assembled into the
+ * unique nodes, then the duplicate endpoint nodes and the one-node ghosts
+ * of j and of the mass records take the values of their periodic unique node.
  * Replaces the self-periodic J.add/ghost exchange and the compact mass halo
  * (ecsim/deposition/current_assembly_device.hpp:26-53,
  * communication/mass_halo/mass_halo_device.hpp:91-160,350-364). */

@@ -458,3 +458,35 @@ def test_tc_mass_matches_oracle(torch_cuda, kind, rel, layout):
     mw_i, mg_i = interior_records(g, mw), interior_records(g, mg)
     err = np.abs(mg_i - mw_i).max() / np.abs(mw_i).max()
     assert err <= rel, err
+
+
+@pytest.mark.parametrize("kind", [2, 3])
+def test_tc_moments_accumulate_two_species(torch_cuda, kind):
+    """Two species deposited with the tensor-core forms before one fold: the
+    second species adds to the cell moments of the first (compare with the
+    oracle's sum of both)."""
+    g = GRID
+    rng = np.random.default_rng(29)
+    d1 = species_arrays(g, 1, seed=5, vth=(0.2, 0.1, 0.3), npcel=(3, 3, 3), qom=-4.0)
+    d2 = species_arrays(g, 1, seed=6, vth=(0.02, 0.01, 0.03), npcel=(2, 2, 2), qom=1.0)
+    ctx = make_ctx(g, 1, dt=0.2, max_particles=len(d1["cell"]), mass_layout=1)
+    bnode = periodic_node_field(g, smooth_random_unique(g, rng, 0.9)).astype(np.float32)
+    bn = ctx.field(bnode)
+    j, m = ctx.moments()
+    jw = np.zeros(3 * ctx.layout.node_count)
+    mw = np.zeros(126 * ctx.layout.node_count)
+    for qom, d in ((-4.0, d1), (1.0, d2)):
+        n = len(d["cell"])
+        parts, counts, offsets = ctx.sort(ctx.upload_particles(d), n)
+        ctx.deposit(qom, parts, n, bn, j, m, counts, offsets, kind=kind)
+        js, ms, bad = oracle_moments(g, 1, qom, 0.2, d, bnode)
+        assert bad == 0
+        jw += js
+        mw += ms
+    ctx.fold(j, m)
+    assert ctx.invalid_count() == 0
+    jg, mg = j.cpu().numpy().astype(np.float64), ctx.records(m)
+    assert np.abs(interior_nodes(g, jg) - interior_nodes(g, jw)).max() <= 3e-5 * np.abs(interior_nodes(g, jw)).max()
+    rel = 3e-3 if kind == 2 else 1e-4
+    mi = interior_records(g, mw)
+    assert np.abs(interior_records(g, mg) - mi).max() <= rel * np.abs(mi).max()

@@ -26,6 +26,8 @@ struct tpicb200_context {
   double* pinned = nullptr;      // host mirror of `reduced` + invalid
   int energy_blocks = 0;
   cudaEvent_t events[8]{};
+  float* moments = nullptr;      // per-cell moments of the tensor-core forms (mixed precision)
+  bool moments_pending = false;  // moments hold deposits not yet assembled
 };
 
 namespace {
@@ -142,6 +144,7 @@ int tpicb200_create(const tpicb200_grid* grid, const tpicb200_options* options, 
   alloc((void**)&ctx->invalid, 4);
   alloc((void**)&ctx->partials, size_t(ctx->energy_blocks) * (2 + 5 * TPICB200_MAX_SPECIES) * 8);
   alloc((void**)&ctx->reduced, (2 + 5 * TPICB200_MAX_SPECIES + 2) * 8);
+  if (options->precision == TPICB200_PRECISION_MIXED) alloc((void**)&ctx->moments, moment_floats(ctx->g) * 4);
   if (e == cudaSuccess) e = cudaMallocHost((void**)&ctx->pinned, (2 + 5 * TPICB200_MAX_SPECIES + 2) * 8);
   if (e == cudaSuccess) e = cudaMemset(ctx->invalid, 0, 4);
   for (auto& ev : ctx->events)
@@ -159,7 +162,7 @@ int tpicb200_destroy(tpicb200_context* ctx) {
   cudaDeviceSynchronize();
   solver_destroy(ctx->solver);
   cudaFree(ctx->cursor); cudaFree(ctx->perm); cudaFree(ctx->scan); cudaFree(ctx->invalid);
-  cudaFree(ctx->partials); cudaFree(ctx->reduced);
+  cudaFree(ctx->partials); cudaFree(ctx->reduced); cudaFree(ctx->moments);
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
   for (auto& ev : ctx->events)
     if (ev) cudaEventDestroy(ev);
@@ -212,6 +215,7 @@ int tpicb200_clear_moments(tpicb200_context* ctx, void* j, void* mass, tpicb200_
   if (int s = check_ctx(ctx)) return s;
   const size_t fb = ctx->opt.precision == TPICB200_PRECISION_DOUBLE ? 8 : 4;
   cudaError_t e = cudaSuccess;
+  ctx->moments_pending = false;
   if (j) e = cudaMemsetAsync(j, 0, 3 * size_t(ctx->g.nodes) * fb, (cudaStream_t)stream);
   if (mass && e == cudaSuccess) e = cudaMemsetAsync(mass, 0, 126 * size_t(ctx->g.nodes) * fb, (cudaStream_t)stream);
   return cuda_status(e, "moment clear failed");
@@ -236,9 +240,13 @@ int tpicb200_deposit(tpicb200_context* ctx, double qom, const tpicb200_particles
   cudaStream_t s = (cudaStream_t)stream;
   if (mass_kind == TPICB200_MASS_TF32 || mass_kind == TPICB200_MASS_BF16X3) {
     if (!counts) return fail(TPICB200_INVALID_ARGUMENT, "tensor-core mass forms need sorted bins");
-    return cuda_status(launch_deposit_tc(mass_kind, ctx->g, qom, ctx->opt.dt, ctx->opt.c, p, counts, offsets,
-                                         b_node, j, mass, inv, s),
-                       "tensor-core deposition launch failed");
+    if (!j || !mass) return fail(TPICB200_INVALID_ARGUMENT, "tensor-core forms deposit J-hat and mass together");
+    const int accumulate = ctx->moments_pending ? 1 : 0;
+    const int r = cuda_status(launch_deposit_tc(mass_kind, ctx->g, qom, ctx->opt.dt, ctx->opt.c, p, counts, offsets,
+                                                b_node, ctx->moments, accumulate, inv, s),
+                              "tensor-core deposition launch failed");
+    if (r == TPICB200_SUCCESS) ctx->moments_pending = true;
+    return r;
   }
   return cuda_status(launch_deposit(ctx->opt.precision, mass_kind, ctx->g, qom, ctx->opt.dt, ctx->opt.c, p,
                                     counts, offsets, b_node, j, mass, inv, s),
@@ -247,6 +255,14 @@ int tpicb200_deposit(tpicb200_context* ctx, double qom, const tpicb200_particles
 
 int tpicb200_fold_periodic(tpicb200_context* ctx, void* j, void* mass, tpicb200_stream stream) {
   if (int s = check_ctx(ctx)) return s;
+  if (ctx->moments_pending) {
+    // Cell moments of the tensor-core forms are added into the unique nodes first.
+    if (!j || !mass) return fail(TPICB200_INVALID_ARGUMENT, "pending tensor-core moments need J-hat and mass");
+    if (int r = cuda_status(launch_assemble_moments(ctx->g, ctx->moments, j, mass, (cudaStream_t)stream),
+                            "moment assembly failed"))
+      return r;
+    ctx->moments_pending = false;
+  }
   return cuda_status(launch_fold(ctx->opt.precision, ctx->g, j, mass, (cudaStream_t)stream), "fold launch failed");
 }
 

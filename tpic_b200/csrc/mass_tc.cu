@@ -24,8 +24,12 @@
 // tensor core consumes the previous one (tcgen05.commit -> mbarrier).
 // Operands are rounded to TF32 with round-to-nearest (cvt.rna) so the
 // rounding is unbiased; accumulation is FP32. The epilogue reads G with
-// tcgen05.ld and adds each monomial's 3x3 block to the 1, 2 or 4 canonical
-// pair records that share it (324 atomics per cell, as the reference's flush).
+// tcgen05.ld and stores it, with the cell's 8x3 current corner sums, as the
+// cell's moments (27x9 + 8x3 values, entry-major arrays over the unique
+// cells; a later species adds to them in place). No atomics: the reference's
+// flush issues up to 324 atomics per cell (mass_matrix_mma_device.hpp:141-150).
+// assemble_moments_kernel then forms every record entry of a unique node as
+// the sum of the 1, 2, 4 or 8 cell moments that share it, in a fixed order.
 // J-hat is accumulated in FP32 on the CUDA cores exactly as the scalar form.
 //
 // BF16x3 form: every operand v is split into hi = bf16(v) and lo = bf16(v - hi)
@@ -46,6 +50,8 @@ constexpr int kCells = 4;          // cells per CTA group (one per warp)
 constexpr int kChunk = 32;         // particles per chunk (one per lane)
 constexpr int kFacStride = 36;     // floats per factor row (padded against bank conflicts)
 constexpr uint32_t kTmemCols = 128;
+constexpr int kMassMoments = 27 * 9;                  // G[t][c] per cell
+constexpr int kMoments = kMassMoments + 24;           // + J corner sums [a][c]
 constexpr uint32_t kDcol = 64;
 // Per form: B columns per cell, N, bytes of one B tile, B tiles per buffer.
 // TF32 (K-major): 8 K-chunks of 4 particles, each 6 N-groups x 128 bytes,
@@ -90,14 +96,11 @@ template <bool Bf16> struct __align__(128) TcShared {
   uint8_t btile[2][Form<Bf16>::tiles][Form<Bf16>::tile_bytes];
   float fac[kCells][12][kFacStride];
   float bcache[kCells][24];
+  float stage[kMoments][kCells];
   uint64_t mbar[2];
   uint32_t tmem_base;
   uint32_t count[kCells];
 };
-
-__device__ __forceinline__ long long wrapped(const Geom& g, int i, int j, int k) {
-  return g.node(i == g.nx ? 0 : i, j == g.ny ? 0 : j, k == g.nz ? 0 : k);
-}
 
 __device__ __forceinline__ uint32_t pack_bf16(float lo_elem, float hi_elem) {
   const __nv_bfloat162 v = __floats2bfloat162_rn(lo_elem, hi_elem);  // .x (low half) = first element
@@ -113,8 +116,8 @@ __global__ void __launch_bounds__(128, 1) tc_deposit_kernel(Geom g, TcParams tp,
     const double* __restrict__ rx, const double* __restrict__ ry, const double* __restrict__ rz,
     const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w,
     const double* __restrict__ q, const int32_t* __restrict__ key, const uint32_t* __restrict__ counts,
-    const uint32_t* __restrict__ offsets, const float* __restrict__ bnode, float* __restrict__ J,
-    float* __restrict__ M, uint32_t* invalid) {
+    const uint32_t* __restrict__ offsets, const float* __restrict__ bnode, float* __restrict__ mom,
+    long long mom_stride, int accumulate, uint32_t* invalid) {
   using F = Form<Bf16>;
   constexpr int kCols = F::cols;
   constexpr int kN = F::n;
@@ -377,8 +380,9 @@ __global__ void __launch_bounds__(128, 1) tc_deposit_kernel(Geom g, TcParams tp,
     }
     if (failed) break;
 
-    // J-hat of this warp's cell: reduce-scatter of the 24 lane sums.
-    if (live) {
+    // J-hat corner sums of this warp's cell: reduce-scatter of the 24 lane
+    // sums, staged for the coalesced moment store.
+    {
       const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
       float h12[12];
 #pragma unroll
@@ -410,16 +414,17 @@ __global__ void __launch_bounds__(128, 1) tc_deposit_kernel(Geom g, TcParams tp,
         const int index0 = (b4 ? 12 : 0) + (b3 ? 6 : 0) + (b2 ? 3 : 0);
 #pragma unroll
         for (int t = 0; t < 3; ++t) {
-          const int index = index0 + t, a = index / 3, c = index % 3;
-          const float value = h3[t];
-          if (!isfinite(value)) atomicAdd(invalid, 1u);
-          else if (value != 0.0f)
-            atomicAdd(J + c * nn + wrapped(g, ci + (a & 1), cj + ((a >> 1) & 1), ck + ((a >> 2) & 1)), value);
+          float value = live ? h3[t] : 0.0f;
+          if (!isfinite(value)) {
+            atomicAdd(invalid, 1u);
+            value = 0.0f;
+          }
+          sh.stage[kMassMoments + index0 + t][warp] = value;
         }
       }
     }
 
-    // Mass: wait for the group's last MMA, read G_w and flush its pairs.
+    // Mass moments: wait for the group's last MMA and read G_w.
     if (maxc > 0) {
       const int last = buf ^ 1;
       const bool ok = tc::mbar_wait(&sh.mbar[last], phase[last]);
@@ -434,27 +439,35 @@ __global__ void __launch_bounds__(128, 1) tc_deposit_kernel(Geom g, TcParams tp,
       tc::tmem_ld8(tmem + lane_base + kDcol + kCols * warp, gbits);
       tc::tmem_ld1(tmem + lane_base + kDcol + kCols * warp + 8, g8);
       tc::tmem_wait_ld();
-      if (live && count > 0 && t_row < 27) {
+      if (t_row < 27) {
         float G[9];
 #pragma unroll
         for (int e = 0; e < 8; ++e) G[e] = __uint_as_float(gbits[e]);
         G[8] = __uint_as_float(g8);
-        bool finite_block = true;
 #pragma unroll
-        for (int e = 0; e < 9; ++e) finite_block = finite_block && isfinite(G[e]);
-        if (!finite_block) {
-          atomicAdd(invalid, 1u);
-        } else {
-          const int np = c_pairs.count[t_row];
-          for (int p = 0; p < np; ++p) {
-            const int a = c_pairs.corner[t_row][p], s = c_pairs.stencil[t_row][p];
-            const long long vertex = wrapped(g, ci + (a & 1), cj + ((a >> 1) & 1), ck + ((a >> 2) & 1));
-#pragma unroll
-            for (int e = 0; e < 9; ++e)
-              if (G[e] != 0.0f) atomicAdd(M + g.mass_index(vertex, s * 9 + e), G[e]);
+        for (int e = 0; e < 9; ++e) {
+          float value = (live && count > 0) ? G[e] : 0.0f;
+          if (!isfinite(value)) {
+            atomicAdd(invalid, 1u);
+            value = 0.0f;
           }
+          sh.stage[t_row * 9 + e][warp] = value;
         }
       }
+    } else if (t_row < 27) {
+#pragma unroll
+      for (int e = 0; e < 9; ++e) sh.stage[t_row * 9 + e][warp] = 0.0f;
+    }
+    __syncthreads();
+    // Coalesced moment store: entry q of the group's four cells is 16 bytes.
+    for (int qi = threadIdx.x; qi < kMoments; qi += blockDim.x) {
+      float4 val = make_float4(sh.stage[qi][0], sh.stage[qi][1], sh.stage[qi][2], sh.stage[qi][3]);
+      float4* dst = reinterpret_cast<float4*>(mom + qi * mom_stride + grp * kCells);
+      if (accumulate) {
+        const float4 old = *dst;
+        val.x += old.x; val.y += old.y; val.z += old.z; val.w += old.w;
+      }
+      *dst = val;
     }
     // D is overwritten by the next group's first MMA only after every warp
     // has read it.
@@ -477,11 +490,18 @@ __global__ void __launch_bounds__(128, 1) tc_deposit_kernel(Geom g, TcParams tp,
 
 }  // namespace
 
+long long moment_stride(const Geom& g) {
+  const long long cells = (long long)g.nx * g.ny * g.nz;
+  return (cells + kCells - 1) / kCells * kCells;
+}
+size_t moment_floats(const Geom& g) { return size_t(kMoments) * size_t(moment_stride(g)); }
+
 cudaError_t launch_deposit_tc(int mass_kind, const Geom& g, double qom, double dt, double c,
                               const tpicb200_particles* p, const uint32_t* counts, const uint32_t* offsets,
-                              const void* bnode, void* j, void* mass, uint32_t* invalid, cudaStream_t s) {
+                              const void* bnode, float* moments, int accumulate, uint32_t* invalid,
+                              cudaStream_t s) {
   if (mass_kind != TPICB200_MASS_TF32 && mass_kind != TPICB200_MASS_BF16X3) return cudaErrorNotSupported;
-  if (!j || !mass) return cudaErrorInvalidValue;
+  if (!moments) return cudaErrorInvalidValue;
   TcParams tp{float(qom * dt / 2 / c), float(g.inv_volume)};
   int device = 0, sms = 148;
   cudaGetDevice(&device);
@@ -497,7 +517,78 @@ cudaError_t launch_deposit_tc(int mass_kind, const Geom& g, double qom, double d
   const int pad = 47 * 1024 - int(tf32 ? sizeof(TcShared<false>) : sizeof(TcShared<true>));
   kernel<<<blocks, 128, pad, s>>>(g, tp, (const double*)p->rx, (const double*)p->ry,
       (const double*)p->rz, (const float*)p->u, (const float*)p->v, (const float*)p->w, p->q, p->cell, counts,
-      offsets, (const float*)bnode, (float*)j, (float*)mass, invalid);
+      offsets, (const float*)bnode, moments, moment_stride(g), accumulate, invalid);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+namespace {
+
+// For every stencil: the corners a whose pair (a, a + offset) lies in one
+// cell, and that pair's monomial class t.
+struct StencilPairs {
+  int count[14];
+  int corner[14][8];
+  int monomial[14][8];
+};
+constexpr StencilPairs make_stencil_pairs() {
+  StencilPairs r{};
+  for (int s = 0; s < 14; ++s)
+    for (int a = 0; a < 8; ++a) {
+      const int bx = (a & 1) + stencil_offset(s, 0), by = ((a >> 1) & 1) + stencil_offset(s, 1),
+                bz = ((a >> 2) & 1) + stencil_offset(s, 2);
+      if (bx < 0 || bx > 1 || by < 0 || by > 1 || bz < 0 || bz > 1) continue;
+      const int t = ((a & 1) + bx) + 3 * (((a >> 1) & 1) + by) + 9 * (((a >> 2) & 1) + bz);
+      r.corner[s][r.count[s]] = a;
+      r.monomial[s][r.count[s]] = t;
+      ++r.count[s];
+    }
+  return r;
+}
+__constant__ StencilPairs c_stencil_pairs = make_stencil_pairs();
+
+// Record entry k < 126 (stencil k/9, component k%9) and current component
+// k - 126 of every unique node, summed over the cells that share it in
+// increasing corner order, added to M and J.
+__global__ void __launch_bounds__(256) assemble_moments_kernel(Geom g, const float* __restrict__ mom,
+                                                               long long stride, float* __restrict__ J,
+                                                               float* __restrict__ M) {
+  const long long unique = (long long)g.nx * g.ny * g.nz;
+  const long long total = 129 * unique;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int k = int(t / unique);
+    const long long vtx = t - k * unique;
+    const int i = int(vtx % g.nx), j = int((vtx / g.nx) % g.ny), kk = int(vtx / ((long long)g.nx * g.ny));
+    auto cell_of = [&](int a) {
+      const int ci = wrap_index(i - (a & 1), g.nx), cj = wrap_index(j - ((a >> 1) & 1), g.ny),
+                ck = wrap_index(kk - ((a >> 2) & 1), g.nz);
+      return ci + (long long)g.nx * (cj + (long long)g.ny * ck);
+    };
+    const long long node = g.node(i, j, kk);
+    if (k < 126) {
+      const int s = k / 9, e = k - 9 * (k / 9);
+      float sum = 0.0f;
+      const int n = c_stencil_pairs.count[s];
+      for (int p = 0; p < n; ++p)
+        sum += mom[(c_stencil_pairs.monomial[s][p] * 9 + e) * stride + cell_of(c_stencil_pairs.corner[s][p])];
+      if (sum != 0.0f) M[g.mass_index(node, k)] += sum;
+    } else {
+      const int c = k - 126;
+      float sum = 0.0f;
+#pragma unroll
+      for (int a = 0; a < 8; ++a) sum += mom[(kMassMoments + a * 3 + c) * stride + cell_of(a)];
+      if (sum != 0.0f) J[c * g.nodes + node] += sum;
+    }
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_assemble_moments(const Geom& g, const float* moments, void* j, void* mass, cudaStream_t s) {
+  const long long total = 129LL * g.nx * g.ny * g.nz;
+  assemble_moments_kernel<<<grid_for(total, 256, 148u * 16u), 256, 0, s>>>(g, moments, moment_stride(g),
+                                                                           (float*)j, (float*)mass);
   count_launches(1);
   return cudaGetLastError();
 }
