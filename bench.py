@@ -277,13 +277,18 @@ def stage_kernel_times(sim, args, stream, repeats: int = 5) -> dict:
 
     scratch_inv = torch.zeros(1, dtype=torch.int32, device="cuda")
 
-    # Deposition (current + mass) of all species from the sorted records.
+    # Deposition (current + mass) of all species from the sorted records, as
+    # the cycle runs it: one multi-species call, then the fold (which also
+    # assembles the tensor-core forms' cell moments).
     def deposit():
-        lib.tpicb200_clear_moments(sim.ctx, st.j, st.mass, s_)
-        for s in range(ns):
-            p = st.slot[s][st.current[s]]
-            _lib.check(lib.tpicb200_deposit(sim.ctx, st.qom[s], C.byref(p), st.counts[s], st.offsets[s], st.b_node,
-                                            st.j, st.mass, st.mass_kind, scratch_inv.data_ptr(), s_))
+        _lib.check(lib.tpicb200_clear_moments(sim.ctx, st.j, st.mass, s_))
+        parts = (_lib.Particles * ns)(*[st.slot[s][st.current[s]] for s in range(ns)])
+        qom = (C.c_double * ns)(*[st.qom[s] for s in range(ns)])
+        counts = (C.c_void_p * ns)(*[st.counts[s] for s in range(ns)])
+        offsets = (C.c_void_p * ns)(*[st.offsets[s] for s in range(ns)])
+        _lib.check(lib.tpicb200_deposit_species(sim.ctx, ns, qom, parts, counts, offsets, st.b_node, st.j, st.mass,
+                                                st.mass_kind, scratch_inv.data_ptr(), s_))
+        _lib.check(lib.tpicb200_fold_periodic(sim.ctx, st.j, st.mass, s_))
     out["deposit"] = {"ms": timed(deposit),
                       "bytes": n_total * (24 + 3 * vb + 8 + 4) + nodes * (126 + 3) * fb}
 

@@ -223,6 +223,19 @@ int tpicb200_deposit(tpicb200_context* ctx, double qom, const tpicb200_particles
                      void* j, void* mass, int mass_kind, uint32_t* invalid,
                      tpicb200_stream stream);
 
+/* Deposition of ns species (arrays of ns entries: q/m, records and their
+ * bins) with the semantics of ns calls of tpicb200_deposit. The tensor-core
+ * forms read the records of both species of a pair in one pass over the
+ * cells (one record stream per cell, species in array order), so a cell's
+ * chunk padding and its moment store are paid once per pair. No single
+ * reference counterpart: the reference enqueues one species at a time
+ * (enqueue_sorted_mass_matrix, ecsim/mass_matrix/mass_matrix_deposition_device.hpp:124-182,
+ * from the species loop of simulation/actions/local_species_actions_device.hpp). */
+int tpicb200_deposit_species(tpicb200_context* ctx, int ns, const double* qom,
+                             const tpicb200_particles* species, const uint32_t* const* counts,
+                             const uint32_t* const* offsets, const void* b_node, void* j, void* mass,
+                             int mass_kind, uint32_t* invalid, tpicb200_stream stream);
+
 /* Periodic fold: pending tensor-core cell moments are assembled into the
  * unique nodes, then the duplicate endpoint nodes and the one-node ghosts
  * of j and of the mass records take the values of their periodic unique node.

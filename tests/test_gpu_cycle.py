@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from fieldutil import interior_nodes
+from fieldutil import interior_nodes, interior_records
 from tpic_b200.plasma import Case, FieldInit, GridSpec, SpeciesSpec, generate_species
 
 pytestmark = pytest.mark.gpu
@@ -93,3 +93,26 @@ def test_c1_tensor_core_energy(mass_kind, bound):
     reports = sim.run(3)
     for r in reports:
         assert abs(r.total_energy - total0) <= bound * total0
+
+
+@pytest.mark.parametrize("mass_kind,rel", [("tf32", 3e-3), ("bf16x3", 1e-4)])
+def test_c1_fused_species_deposition(mass_kind, rel):
+    """The cycle driver deposits every species of a cell in one tensor-core
+    pass (species 0 then species 1 in one record stream per cell): the
+    bootstrap deposition of both C1 species equals the oracle's sum within
+    the form's operand rounding."""
+    case = c1_case(n=16)
+    from tpic_b200.simulation import Simulation
+    sim = Simulation(case, precision="mixed", mass_kind=mass_kind, mass_layout="stencil-major")
+    sim.prepare()
+    arrays = O.case_species_arrays(case, 1, generate_species)
+    oc = O.OracleCycle(case.grid, arrays, case.dt, case.theta, case.c, case.gmres_tol, 1, b0=case.fields.b0)
+    oc.prepare()
+    g = case.grid
+    jg = interior_nodes(g, sim.field("j").cpu().numpy().astype(np.float64))
+    jw = interior_nodes(g, oc.j)
+    assert np.abs(jg - jw).max() <= rel * np.abs(jw).max()
+    mass = sim.field("mass").cpu().numpy().astype(np.float64)
+    mg = interior_records(g, np.ascontiguousarray(mass.reshape(126, -1).T).ravel())
+    mw = interior_records(g, oc.m)
+    assert np.abs(mg - mw).max() <= rel * np.abs(mw).max()

@@ -80,6 +80,9 @@ EXPORTS = {
     "tpicb200_clear_moments": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tpicb200_deposit": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(Particles), C.c_void_p, C.c_void_p,
                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "tpicb200_deposit_species": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double), C.POINTER(Particles),
+                                           C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_void_p, C.c_void_p,
+                                           C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "tpicb200_fold_periodic": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tpicb200_mass_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tpicb200_field_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,

@@ -28,6 +28,10 @@ struct tpicb200_context {
   cudaEvent_t events[8]{};
   float* moments = nullptr;      // per-cell moments of the tensor-core forms (mixed precision)
   bool moments_pending = false;  // moments hold deposits not yet assembled
+  // J and mass buffers zeroed by the last tpicb200_clear_moments that nothing
+  // else has deposited into since: the assembly may store instead of add.
+  const void* cleared_j = nullptr;
+  const void* cleared_mass = nullptr;
 };
 
 namespace {
@@ -216,6 +220,8 @@ int tpicb200_clear_moments(tpicb200_context* ctx, void* j, void* mass, tpicb200_
   const size_t fb = ctx->opt.precision == TPICB200_PRECISION_DOUBLE ? 8 : 4;
   cudaError_t e = cudaSuccess;
   ctx->moments_pending = false;
+  ctx->cleared_j = j && mass ? j : nullptr;
+  ctx->cleared_mass = j && mass ? mass : nullptr;
   if (j) e = cudaMemsetAsync(j, 0, 3 * size_t(ctx->g.nodes) * fb, (cudaStream_t)stream);
   if (mass && e == cudaSuccess) e = cudaMemsetAsync(mass, 0, 126 * size_t(ctx->g.nodes) * fb, (cudaStream_t)stream);
   return cuda_status(e, "moment clear failed");
@@ -242,12 +248,13 @@ int tpicb200_deposit(tpicb200_context* ctx, double qom, const tpicb200_particles
     if (!counts) return fail(TPICB200_INVALID_ARGUMENT, "tensor-core mass forms need sorted bins");
     if (!j || !mass) return fail(TPICB200_INVALID_ARGUMENT, "tensor-core forms deposit J-hat and mass together");
     const int accumulate = ctx->moments_pending ? 1 : 0;
-    const int r = cuda_status(launch_deposit_tc(mass_kind, ctx->g, qom, ctx->opt.dt, ctx->opt.c, p, counts, offsets,
-                                                b_node, ctx->moments, accumulate, inv, s),
+    const int r = cuda_status(launch_deposit_tc(mass_kind, ctx->g, 1, &qom, ctx->opt.dt, ctx->opt.c, &p, &counts,
+                                                &offsets, b_node, ctx->moments, accumulate, inv, s),
                               "tensor-core deposition launch failed");
     if (r == TPICB200_SUCCESS) ctx->moments_pending = true;
     return r;
   }
+  ctx->cleared_j = ctx->cleared_mass = nullptr;
   return cuda_status(launch_deposit(ctx->opt.precision, mass_kind, ctx->g, qom, ctx->opt.dt, ctx->opt.c, p,
                                     counts, offsets, b_node, j, mass, inv, s),
                      "deposition launch failed");
@@ -258,10 +265,12 @@ int tpicb200_fold_periodic(tpicb200_context* ctx, void* j, void* mass, tpicb200_
   if (ctx->moments_pending) {
     // Cell moments of the tensor-core forms are added into the unique nodes first.
     if (!j || !mass) return fail(TPICB200_INVALID_ARGUMENT, "pending tensor-core moments need J-hat and mass");
-    if (int r = cuda_status(launch_assemble_moments(ctx->g, ctx->moments, j, mass, (cudaStream_t)stream),
+    const int overwrite = j == ctx->cleared_j && mass == ctx->cleared_mass ? 1 : 0;
+    if (int r = cuda_status(launch_assemble_moments(ctx->g, ctx->moments, j, mass, overwrite, (cudaStream_t)stream),
                             "moment assembly failed"))
       return r;
     ctx->moments_pending = false;
+    ctx->cleared_j = ctx->cleared_mass = nullptr;
   }
   return cuda_status(launch_fold(ctx->opt.precision, ctx->g, j, mass, (cudaStream_t)stream), "fold launch failed");
 }
@@ -332,14 +341,55 @@ int tpicb200_energy(tpicb200_context* ctx, const void* e, const void* b_cell, co
   return TPICB200_SUCCESS;
 }
 
+int tpicb200_deposit_species(tpicb200_context* ctx, int ns, const double* qom, const tpicb200_particles* species,
+                             const uint32_t* const* counts, const uint32_t* const* offsets, const void* b_node,
+                             void* j, void* mass, int mass_kind, uint32_t* invalid, tpicb200_stream stream) {
+  if (int s = check_ctx(ctx)) return s;
+  if (ns < 0 || ns > TPICB200_MAX_SPECIES || (ns > 0 && (!qom || !species || !counts || !offsets)))
+    return fail(TPICB200_INVALID_ARGUMENT, "invalid species arrays");
+  if (mass_kind != TPICB200_MASS_TF32 && mass_kind != TPICB200_MASS_BF16X3) {
+    for (int sp = 0; sp < ns; ++sp)
+      if (int r = tpicb200_deposit(ctx, qom[sp], &species[sp], counts[sp], offsets[sp], b_node, j, mass, mass_kind,
+                                   invalid, stream))
+        return r;
+    return TPICB200_SUCCESS;
+  }
+  // Tensor-core forms: the per-species checks of tpicb200_deposit, then one
+  // fused pass per species pair.
+  if (ctx->opt.precision != TPICB200_PRECISION_MIXED)
+    return fail(TPICB200_INVALID_ARGUMENT, "tensor-core mass forms need the mixed precision mode");
+  if (!b_node) return fail(TPICB200_INVALID_ARGUMENT, "deposit needs B nodes");
+  if (!j || !mass) return fail(TPICB200_INVALID_ARGUMENT, "tensor-core forms deposit J-hat and mass together");
+  if (ns == 0) return TPICB200_SUCCESS;
+  const tpicb200_particles* parts[TPICB200_MAX_SPECIES];
+  for (int sp = 0; sp < ns; ++sp) {
+    parts[sp] = &species[sp];
+    if (int r = check_particles(ctx, parts[sp])) return r;
+    if (!counts[sp] || !offsets[sp]) return fail(TPICB200_INVALID_ARGUMENT, "tensor-core mass forms need sorted bins");
+    if (!std::isfinite(qom[sp])) return fail(TPICB200_INVALID_ARGUMENT, "deposit needs finite q/m");
+    if (!std::isfinite(qom[sp] * ctx->opt.dt / 2 / ctx->opt.c)) return fail(TPICB200_OVERFLOW, "beta/c is not finite");
+  }
+  const int r = cuda_status(launch_deposit_tc(mass_kind, ctx->g, ns, qom, ctx->opt.dt, ctx->opt.c, parts, counts,
+                                              offsets, b_node, ctx->moments, ctx->moments_pending ? 1 : 0,
+                                              invalid_or_own(ctx, invalid), (cudaStream_t)stream),
+                            "tensor-core deposition launch failed");
+  if (r == TPICB200_SUCCESS) ctx->moments_pending = true;
+  return r;
+}
+
 static int deposit_all(tpicb200_context* ctx, tpicb200_state* st, const void* b_node, cudaStream_t s) {
   if (int r = tpicb200_clear_moments(ctx, st->j, st->mass, (tpicb200_stream)s)) return r;
+  tpicb200_particles live[TPICB200_MAX_SPECIES];
+  const uint32_t* counts[TPICB200_MAX_SPECIES];
+  const uint32_t* offsets[TPICB200_MAX_SPECIES];
   for (int sp = 0; sp < st->ns; ++sp) {
-    const int cur = st->current[sp];
-    if (int r = tpicb200_deposit(ctx, st->qom[sp], &st->slot[sp][cur], st->counts[sp], st->offsets[sp], b_node,
-                                 st->j, st->mass, st->mass_kind, nullptr, (tpicb200_stream)s))
-      return r;
+    live[sp] = st->slot[sp][st->current[sp]];
+    counts[sp] = st->counts[sp];
+    offsets[sp] = st->offsets[sp];
   }
+  if (int r = tpicb200_deposit_species(ctx, st->ns, st->qom, live, counts, offsets, b_node, st->j, st->mass,
+                                       st->mass_kind, nullptr, (tpicb200_stream)s))
+    return r;
   return tpicb200_fold_periodic(ctx, st->j, st->mass, (tpicb200_stream)s);
 }
 

@@ -31,11 +31,14 @@ cudaError_t launch_fold(int precision, const Geom& g, void* j, void* mass, cudaS
 // mass_tc.cu (tcgen05 forms): per-cell moments, then their assembly into J
 // and the mass coefficients.
 size_t moment_floats(const Geom& g);
-cudaError_t launch_deposit_tc(int mass_kind, const Geom& g, double qom, double dt, double c,
-                              const tpicb200_particles* p, const uint32_t* counts,
-                              const uint32_t* offsets, const void* bnode, float* moments, int accumulate,
+// Tensor-core deposition of `ns` species (fused two per launch) into the
+// per-cell moments; `accumulate` adds to moments already present.
+cudaError_t launch_deposit_tc(int mass_kind, const Geom& g, int ns, const double* qom, double dt, double c,
+                              const tpicb200_particles* const* p, const uint32_t* const* counts,
+                              const uint32_t* const* offsets, const void* bnode, float* moments, int accumulate,
                               uint32_t* invalid, cudaStream_t s);
-cudaError_t launch_assemble_moments(const Geom& g, const float* moments, void* j, void* mass, cudaStream_t s);
+cudaError_t launch_assemble_moments(const Geom& g, const float* moments, void* j, void* mass, int overwrite,
+                                    cudaStream_t s);
 
 // fields.cu
 cudaError_t launch_node_ghosts(const Geom& g, double* f, int components, cudaStream_t s);

@@ -1,5 +1,5 @@
-// Tensor-core (tcgen05) mass-matrix assembly with the implicit current on
-// CUDA cores, one species of sorted records per launch.
+// Tensor-core (tcgen05) mass-matrix and implicit-current assembly over the
+// sorted records of up to two species per launch.
 //
 // The mass block of a corner pair is K_ab = sum_p s_p alpha_p W_pa W_pb with
 // s = (beta/c) q (ecsim/mass_matrix/mass_matrix_scalar_device.hpp:25-97). With
@@ -9,28 +9,36 @@
 // A cell's 36 canonical pair blocks are therefore 27 monomial moments
 //   G[t][c] = sum_p m_pt (s_p alpha_p[c]),  t < 27, c < 9,
 // a dense contraction over the cell's particles: D = A^T B with K = particles.
+// The implicit current of corner a, J_a = sum_p W_pa j_p with
+// j_p = q_p/V alpha_p v_p (ecsim/current/implicit_current_device.hpp), rides
+// along in three more B columns: since sum_b W_pb = 1, W_pa = sum_b W_pa W_pb
+// and J_a[c] = sum_b H[t(a, b)][c] with H[t][c] = sum_p m_pt j_p[c].
 //
 // Tensor-core mapping (one CTA of four warps works on four cells at once):
 //   A (tensor memory, M = 128 lanes x K columns): lane 32w + t holds m_pt of
 //     cell w's particles (rows 27..31 of each quadrant are zero);
-//   B (shared memory, K x N, no swizzle): columns 12w..12w+8 (TF32, N = 48,
-//     K-major core matrices of 8 N-rows x 4 K-values) or 16w..16w+8 (BF16,
+//   B (shared memory, K x N, no swizzle): columns 12w..12w+11 (TF32, N = 48,
+//     K-major core matrices of 8 N-rows x 4 K-values) or 16w..16w+11 (BF16,
 //     N = 64, MN-major core matrices of 8 K-rows x 8 N-values) hold
-//     s_p alpha_p of cell w's particle p (the rest zero);
-//   D (tensor memory, 128 x 48 FP32): D[32w + t][12w + c] = G_w[t][c]; the
-//     off-diagonal blocks are never read.
-// Each 32-particle chunk is four tcgen05.mma.kind::tf32 (K = 8) issued by one
-// thread; A and B are double-buffered so the next chunk is produced while the
-// tensor core consumes the previous one (tcgen05.commit -> mbarrier).
-// Operands are rounded to TF32 with round-to-nearest (cvt.rna) so the
-// rounding is unbiased; accumulation is FP32. The epilogue reads G with
-// tcgen05.ld and stores it, with the cell's 8x3 current corner sums, as the
-// cell's moments (27x9 + 8x3 values, entry-major arrays over the unique
-// cells; a later species adds to them in place). No atomics: the reference's
-// flush issues up to 324 atomics per cell (mass_matrix_mma_device.hpp:141-150).
+//     (s_p alpha_p, j_p) of cell w's particle p (the rest zero);
+//   D (tensor memory, 128 x 48 / 64 FP32): D[32w + t][12w + c] = G_w[t][c]
+//     (c < 9) and H_w[t][c - 9]; the off-diagonal blocks are never read.
+// Column k of a chunk holds the k-th particle of each of the four cells, so
+// the four cells share every MMA. Each 32-particle chunk is four
+// tcgen05.mma.kind::tf32 (K = 8) issued by one thread; A and B are
+// double-buffered so the next chunk is produced while the tensor core
+// consumes the previous one (tcgen05.commit -> mbarrier, bounded waits).
+// Operands are rounded to nearest (cvt.rna.tf32, bf16 RN split) so the
+// rounding is unbiased; accumulation is FP32. The epilogue reads G and H with
+// tcgen05.ld, forms the 8x3 corner currents and stores the cell's moments
+// (27x9 + 8x3 values, entry-major arrays over the unique cells; a later launch
+// adds to them in place). No atomics: the reference's flush issues up to 324
+// atomics per cell (mass_matrix_mma_device.hpp:141-150).
 // assemble_moments_kernel then forms every record entry of a unique node as
 // the sum of the 1, 2, 4 or 8 cell moments that share it, in a fixed order.
-// J-hat is accumulated in FP32 on the CUDA cores exactly as the scalar form.
+//
+// A cell's records of both species form one stream (species 0 first), so
+// the chunk padding is paid once per cell rather than once per species.
 //
 // BF16x3 form: every operand v is split into hi = bf16(v) and lo = bf16(v - hi)
 // (round-to-nearest) and D accumulates A_hi B_hi + A_hi B_lo + A_lo B_hi with
@@ -48,11 +56,13 @@ namespace {
 
 constexpr int kCells = 4;          // cells per CTA group (one per warp)
 constexpr int kChunk = 32;         // particles per chunk (one per lane)
-constexpr int kFacStride = 36;     // floats per factor row (padded against bank conflicts)
+constexpr int kFuse = 2;           // species per launch
+constexpr int kFacStride = 36;     // floats per factor row (16-byte aligned rows)
 constexpr uint32_t kTmemCols = 128;
 constexpr int kMassMoments = 27 * 9;                  // G[t][c] per cell
 constexpr int kMoments = kMassMoments + 24;           // + J corner sums [a][c]
 constexpr uint32_t kDcol = 64;
+constexpr int kCtasPerSm = 4;      // 4 x 128 tensor-memory columns = all 512
 // Per form: B columns per cell, N, bytes of one B tile, B tiles per buffer.
 // TF32 (K-major): 8 K-chunks of 4 particles, each 6 N-groups x 128 bytes,
 // padded by 16 bytes (K-chunk stride 784 B) so the 32 lanes' 4-byte stores
@@ -66,37 +76,37 @@ template <bool Bf16> struct Form {
   static constexpr int tiles = Bf16 ? 2 : 1;         // hi (+ lo)
 };
 
-// Canonical pairs sharing each monomial class: corner a and stencil s.
-struct MonomialPairs {
-  int count[27];
-  int corner[27][4];
-  int stencil[27][4];
-};
-constexpr MonomialPairs make_monomial_pairs() {
-  MonomialPairs r{};
-  for (int a = 0; a < 8; ++a)
-    for (int b = 0; b < 8; ++b) {
-      const int s = pair_stencil(a, b);
-      if (s < 0) continue;
-      const int t = ((a & 1) + (b & 1)) + 3 * (((a >> 1) & 1) + ((b >> 1) & 1)) + 9 * (((a >> 2) & 1) + ((b >> 2) & 1));
-      r.corner[t][r.count[t]] = a;
-      r.stencil[t][r.count[t]] = s;
-      ++r.count[t];
-    }
-  return r;
+// Monomial class of the corner pair (a, b).
+__host__ __device__ constexpr int monomial_class(int a, int b) {
+  return ((a & 1) + (b & 1)) + 3 * (((a >> 1) & 1) + ((b >> 1) & 1)) + 9 * (((a >> 2) & 1) + ((b >> 2) & 1));
 }
-__constant__ MonomialPairs c_pairs = make_monomial_pairs();
+
+struct TcSpecies {
+  const double* rx;
+  const double* ry;
+  const double* rz;
+  const float* u;
+  const float* v;
+  const float* w;
+  const double* q;
+  const int32_t* key;
+  const uint32_t* counts;
+  const uint32_t* offsets;
+  float beta_over_c;
+};
 
 struct TcParams {
-  float beta_over_c;
+  TcSpecies sp[kFuse];
+  int ns;
   float inv_volume;
 };
 
 template <bool Bf16> struct __align__(128) TcShared {
   uint8_t btile[2][Form<Bf16>::tiles][Form<Bf16>::tile_bytes];
-  float fac[kCells][12][kFacStride];
-  float bcache[kCells][24];
-  float stage[kMoments][kCells];
+  float fac[kCells][13][kFacStride];  // row 12 stays zero (rows 27..31 of A)
+  float bpoly[kCells][24];            // B(x, y, z) polynomial coefficients [c][k]
+  float stage[kCells][kMoments + 1];
+  float hsum[kCells][27 * 3];
   uint64_t mbar[2];
   uint32_t tmem_base;
   uint32_t count[kCells];
@@ -106,18 +116,38 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo_elem, float hi_elem) {
   const __nv_bfloat162 v = __floats2bfloat162_rn(lo_elem, hi_elem);  // .x (low half) = first element
   return *reinterpret_cast<const uint32_t*>(&v);
 }
-__device__ __forceinline__ void split_bf16(float v, float& hi, float& lo) {
-  hi = __bfloat162float(__float2bfloat16_rn(v));
-  lo = v - hi;
+// s_p alpha_p (all nine entries, row-major) and the unscaled alpha for the
+// current, as Response<float> but with the fast reciprocal: its ~1e-7
+// relative error is far below the operand rounding of the tensor-core forms.
+struct ScaledResponse {
+  float a[9];
+  float norm_square;
+  __device__ __forceinline__ ScaledResponse(float bx, float by, float bz, float beta_over_c) {
+    const float x = beta_over_c * bx, y = beta_over_c * by, z = beta_over_c * bz;
+    norm_square = x * x + y * y + z * z;
+    const float inverse = __fdividef(1.0f, 1.0f + norm_square);
+    a[0] = (1.0f + x * x) * inverse;
+    a[4] = (1.0f + y * y) * inverse;
+    a[8] = (1.0f + z * z) * inverse;
+    const float xy = x * y * inverse, xz = x * z * inverse, yz = y * z * inverse;
+    const float sx = x * inverse, sy = y * inverse, sz = z * inverse;
+    a[1] = xy + sz; a[2] = xz - sy; a[3] = xy - sz;
+    a[5] = yz + sx; a[6] = xz + sy; a[7] = yz - sx;
+  }
+};
+
+// Two values split into packed hi and lo bf16 pairs: hi = RN(v), lo = RN(v - hi).
+__device__ __forceinline__ void split_pair(float v0, float v1, uint32_t& hi, uint32_t& lo) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(v0, v1);
+  const float2 hf = __bfloat1622float2(h);
+  hi = *reinterpret_cast<const uint32_t*>(&h);
+  lo = pack_bf16(v0 - hf.x, v1 - hf.y);
 }
 
 template <bool Bf16>
-__global__ void __launch_bounds__(128, 1) tc_deposit_kernel(Geom g, TcParams tp,
-    const double* __restrict__ rx, const double* __restrict__ ry, const double* __restrict__ rz,
-    const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w,
-    const double* __restrict__ q, const int32_t* __restrict__ key, const uint32_t* __restrict__ counts,
-    const uint32_t* __restrict__ offsets, const float* __restrict__ bnode, float* __restrict__ mom,
-    long long mom_stride, int accumulate, uint32_t* invalid) {
+__global__ void __launch_bounds__(128, kCtasPerSm) tc_deposit_kernel(Geom g, TcParams tp,
+    const float* __restrict__ bnode, float* __restrict__ mom, long long mom_stride, int accumulate,
+    uint32_t* invalid) {
   using F = Form<Bf16>;
   constexpr int kCols = F::cols;
   constexpr int kN = F::n;
@@ -133,14 +163,16 @@ __global__ void __launch_bounds__(128, 1) tc_deposit_kernel(Geom g, TcParams tp,
     tc::mbar_init(&sh.mbar[1], 1);
     tc::fence_mbar_init();
   }
+  sh.fac[warp][12][lane] = 0.0f;
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
   const uint32_t tmem = sh.tmem_base;
   const uint32_t lane_base = uint32_t(32 * warp) << 16;
   constexpr uint32_t idesc = tc::instr_desc(Bf16 ? 1u : 2u, 128, kN, Bf16 ? 1u : 0u);
-  uint32_t phase[2] = {0, 0};
-  bool pending[2] = {false, false};
+  // Bit b of `phase` / `pending`: the parity to wait for on mbar[b] and
+  // whether MMAs reading buffer b are in flight.
+  uint32_t phase = 0, pending = 0;
   int buf = 0;
   bool failed = false;
 
@@ -149,13 +181,14 @@ __global__ void __launch_bounds__(128, 1) tc_deposit_kernel(Geom g, TcParams tp,
   // Monomial row of this thread in its warp's quadrant.
   const int t_row = lane;
   const int tx = t_row % 3, tyz = t_row / 3;
+  const bool two = tp.ns > 1;
 
   // Software pipeline: the metadata and B corners of the next group and the
   // records of the next chunk (possibly the next group's first) are loaded
   // while the current chunk is produced and consumed.
   struct Meta {
     int ci, cj, ck;
-    uint32_t count, first;
+    uint32_t c0, c1, f0, f1;
     int32_t bin;
     bool live;
     float bval;  // lane < 24: B corner (lane / 3) component (lane % 3)
@@ -164,17 +197,21 @@ __global__ void __launch_bounds__(128, 1) tc_deposit_kernel(Geom g, TcParams tp,
     double fx, fy, fz, q;
     float u, v, w;
     int32_t key;
-    bool present;
+    bool present, second;
   };
   auto load_meta = [&](long long grp_) {
-    Meta m{0, 0, 0, 0u, 0u, -1, false, 0.0f};
+    Meta m{0, 0, 0, 0u, 0u, 0u, 0u, -1, false, 0.0f};
     const long long cell = grp_ * kCells + warp;
     if (grp_ < groups && cell < cells) {
       m.live = true;
       m.ci = int(cell % g.nx); m.cj = int((cell / g.nx) % g.ny); m.ck = int(cell / ((long long)g.nx * g.ny));
       m.bin = g.encode(m.ci, m.cj, m.ck);
-      m.count = counts[m.bin];
-      m.first = offsets[m.bin];
+      m.c0 = tp.sp[0].counts[m.bin];
+      m.f0 = tp.sp[0].offsets[m.bin];
+      if (two) {
+        m.c1 = tp.sp[1].counts[m.bin];
+        m.f1 = tp.sp[1].offsets[m.bin];
+      }
       if (lane < 24) {
         const int a = lane / 3, c = lane % 3;
         m.bval = bnode[c * nn + g.node(m.ci + (a & 1), m.cj + ((a >> 1) & 1), m.ck + ((a >> 2) & 1))];
@@ -183,12 +220,20 @@ __global__ void __launch_bounds__(128, 1) tc_deposit_kernel(Geom g, TcParams tp,
     return m;
   };
   auto load_rec = [&](const Meta& m, uint32_t k) {
-    Rec r{0.0, 0.0, 0.0, 0.0, 0.0f, 0.0f, 0.0f, -1, false};
-    if (k < m.count) {
-      const uint32_t n = m.first + k;
+    Rec r{0.0, 0.0, 0.0, 0.0, 0.0f, 0.0f, 0.0f, -1, false, false};
+    if (k < m.c0 + m.c1) {
+      const bool s1 = k >= m.c0;
+      const uint32_t n = s1 ? m.f1 + (k - m.c0) : m.f0 + k;
       r.present = true;
-      r.fx = rx[n]; r.fy = ry[n]; r.fz = rz[n]; r.q = q[n];
-      r.u = u[n]; r.v = v[n]; r.w = w[n]; r.key = key[n];
+      r.second = s1;
+      r.fx = (s1 ? tp.sp[1].rx : tp.sp[0].rx)[n];
+      r.fy = (s1 ? tp.sp[1].ry : tp.sp[0].ry)[n];
+      r.fz = (s1 ? tp.sp[1].rz : tp.sp[0].rz)[n];
+      r.q = (s1 ? tp.sp[1].q : tp.sp[0].q)[n];
+      r.u = (s1 ? tp.sp[1].u : tp.sp[0].u)[n];
+      r.v = (s1 ? tp.sp[1].v : tp.sp[0].v)[n];
+      r.w = (s1 ? tp.sp[1].w : tp.sp[0].w)[n];
+      r.key = (s1 ? tp.sp[1].key : tp.sp[0].key)[n];
     }
     return r;
   };
@@ -198,27 +243,42 @@ __global__ void __launch_bounds__(128, 1) tc_deposit_kernel(Geom g, TcParams tp,
   for (long long grp = blockIdx.x; grp < groups && !failed; grp += gridDim.x) {
     const Meta nxt = load_meta(grp + gridDim.x);
     const bool live = cur.live;
-    const int ci = cur.ci, cj = cur.cj, ck = cur.ck;
-    const uint32_t count = cur.count;
+    const uint32_t count = cur.c0 + cur.c1;
     const int32_t bin = cur.bin;
-    if (live && lane < 24) sh.bcache[warp][lane] = cur.bval;
+    // Trilinear B as a polynomial in the cell fractions,
+    // B = c0 + c1 x + c2 y + c3 z + c4 xy + c5 xz + c6 yz + c7 xyz, from the
+    // corner values b_a (corner a = x + 2y + 4z).
+    {
+      float bc[8];
+#pragma unroll
+      for (int a = 0; a < 8; ++a) bc[a] = __shfl_sync(0xffffffffu, cur.bval, 3 * a + (lane < 3 ? lane : 0));
+      if (lane < 3) {
+        float* cp = sh.bpoly[warp] + 8 * lane;
+        const float z0 = live ? 1.0f : 0.0f;
+        cp[0] = z0 * bc[0];
+        cp[1] = z0 * (bc[1] - bc[0]);
+        cp[2] = z0 * (bc[2] - bc[0]);
+        cp[3] = z0 * (bc[4] - bc[0]);
+        cp[4] = z0 * ((bc[3] - bc[2]) - (bc[1] - bc[0]));
+        cp[5] = z0 * ((bc[5] - bc[4]) - (bc[1] - bc[0]));
+        cp[6] = z0 * ((bc[6] - bc[4]) - (bc[2] - bc[0]));
+        cp[7] = z0 * (((bc[7] - bc[6]) - (bc[5] - bc[4])) - ((bc[3] - bc[2]) - (bc[1] - bc[0])));
+      }
+    }
     if (lane == 0) sh.count[warp] = count;
     __syncthreads();
     uint32_t maxc = sh.count[0];
 #pragma unroll
     for (int c = 1; c < kCells; ++c) maxc = max(maxc, sh.count[c]);
-    float jsum[24];
-#pragma unroll
-    for (int t = 0; t < 24; ++t) jsum[t] = 0.0f;
     if (maxc == 0) pre = load_rec(nxt, lane);
 
     for (uint32_t chunk = 0; chunk < maxc; chunk += kChunk) {
       // The buffer is free once the MMAs that read it have completed.
       bool bad = false;
-      if (pending[buf]) {
-        bad = !tc::mbar_wait(&sh.mbar[buf], phase[buf]);
-        phase[buf] ^= 1u;
-        pending[buf] = false;
+      if (pending & (1u << buf)) {
+        bad = !tc::mbar_wait(&sh.mbar[buf], (phase >> buf) & 1u);
+        phase ^= 1u << buf;
+        pending &= ~(1u << buf);
       }
       const Rec rec = pre;
       pre = chunk + kChunk < maxc ? load_rec(cur, chunk + kChunk + lane) : load_rec(nxt, lane);
@@ -231,32 +291,33 @@ __global__ void __launch_bounds__(128, 1) tc_deposit_kernel(Geom g, TcParams tp,
       for (int f = 0; f < 12; ++f) fac[f] = 0.0f;
       if (rec.present) {
         const double fx = rec.fx, fy = rec.fy, fz = rec.fz;
-        if (rec.key == bin && fx >= 0 && fx < 1 && fy >= 0 && fy < 1 && fz >= 0 && fz < 1) {
+        bool ok = rec.key == bin && fx >= 0 && fx < 1 && fy >= 0 && fy < 1 && fz >= 0 && fz < 1;
+        if (ok) {
           const float x = float(fx), y = float(fy), z = float(fz);
-          float wt[8];
-          cic_weights<float>(x, y, z, wt);
           float b[3];
 #pragma unroll
           for (int c = 0; c < 3; ++c) {
-            float val = 0.0f;
-#pragma unroll
-            for (int a = 0; a < 8; ++a) val += wt[a] * sh.bcache[warp][a * 3 + c];
-            b[c] = val;
+            const float4 lo4 = *reinterpret_cast<const float4*>(&sh.bpoly[warp][8 * c]);
+            const float4 hi4 = *reinterpret_cast<const float4*>(&sh.bpoly[warp][8 * c + 4]);
+            const float t1 = fmaf(z, hi4.w, hi4.x);              // c4 + z c7
+            const float t2 = fmaf(z, hi4.y, fmaf(y, t1, lo4.y));  // c1 + y (c4 + z c7) + z c5
+            const float t3 = fmaf(z, hi4.z, lo4.z);              // c2 + z c6
+            b[c] = fmaf(z, lo4.w, fmaf(y, t3, fmaf(x, t2, lo4.x)));
           }
-          const Response<float> r(b[0], b[1], b[2], tp.beta_over_c);
+          const float bo = rec.second ? tp.sp[1].beta_over_c : tp.sp[0].beta_over_c;
+          const ScaledResponse r(b[0], b[1], b[2], bo);
           const float charge = float(rec.q);
-          float hx, hy, hz;
-          r.apply(rec.u, rec.v, rec.w, hx, hy, hz);
+          const float hx = r.a[0] * rec.u + r.a[1] * rec.v + r.a[2] * rec.w;
+          const float hy = r.a[3] * rec.u + r.a[4] * rec.v + r.a[5] * rec.w;
+          const float hz = r.a[6] * rec.u + r.a[7] * rec.v + r.a[8] * rec.w;
           const float qv = charge * tp.inv_volume;
-          const float jc[3] = {qv * hx, qv * hy, qv * hz};
-          const float scale = tp.beta_over_c * charge;
-          if (isfinite(jc[0]) && isfinite(jc[1]) && isfinite(jc[2]) && isfinite(r.norm_square) && isfinite(scale)) {
+          const float scale = bo * charge;
+          bv[9] = qv * hx; bv[10] = qv * hy; bv[11] = qv * hz;
 #pragma unroll
-            for (int a = 0; a < 8; ++a)
-#pragma unroll
-              for (int c = 0; c < 3; ++c) jsum[a * 3 + c] += __fmul_rn(jc[c], wt[a]);
-#pragma unroll
-            for (int e = 0; e < 9; ++e) bv[e] = r.a[e] * scale;
+          for (int e = 0; e < 9; ++e) bv[e] = r.a[e] * scale;
+          // One test covers every product: a non-finite input makes the sum non-finite.
+          ok = isfinite(bv[9] + bv[10] + bv[11] + r.norm_square + scale);
+          if (ok) {
             const float cx = 1.0f - x, cy = 1.0f - y, cz = 1.0f - z;
             const float X[3] = {cx * cx, x * cx, x * x};
             const float Y[3] = {cy * cy, y * cy, y * y};
@@ -267,35 +328,32 @@ __global__ void __launch_bounds__(128, 1) tc_deposit_kernel(Geom g, TcParams tp,
 #pragma unroll
               for (int ty = 0; ty < 3; ++ty) fac[3 + ty + 3 * tz] = Y[ty] * Z[tz];
           } else {
-            atomicAdd(invalid, 1u);
+#pragma unroll
+            for (int c = 0; c < 12; ++c) bv[c] = 0.0f;
           }
-        } else {
-          atomicAdd(invalid, 1u);
         }
+        if (!ok) atomicAdd(invalid, 1u);
       }
-      // B tile (MN-major core matrices: 8 K-rows x 16 bytes of N-values,
-      // K-groups 128 B apart, 16-byte N-chunks 512 B apart).
+      // B tile.
       if constexpr (!Bf16) {
         // K-major: value (n, k) at (n%8)*16 + (n/8)*128 + (k/4)*784 + (k%4)*4.
         uint8_t* bt = sh.btile[buf][0] + (lane >> 2) * kTf32KChunk + (lane & 3) * 4;
 #pragma unroll
         for (int c = 0; c < kCols; ++c) {
-          const int nn = kCols * warp + c;
-          *reinterpret_cast<uint32_t*>(bt + (nn & 7) * 16 + (nn >> 3) * 128) = tc::to_tf32(bv[c]);
+          const int n = kCols * warp + c;
+          *reinterpret_cast<uint32_t*>(bt + (n & 7) * 16 + (n >> 3) * 128) = tc::to_tf32(bv[c]);
         }
       } else {
-        float hi[kCols], lo[kCols];
-#pragma unroll
-        for (int c = 0; c < kCols; ++c) split_bf16(bv[c], hi[c], lo[c]);
+        // MN-major: 8 K-rows x 16 bytes of N-values per core matrix, K-groups
+        // 128 B apart, 16-byte N-chunks 512 B apart.
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
-          const uint4 ph = make_uint4(pack_bf16(hi[8 * j + 0], hi[8 * j + 1]), pack_bf16(hi[8 * j + 2], hi[8 * j + 3]),
-                                      pack_bf16(hi[8 * j + 4], hi[8 * j + 5]), pack_bf16(hi[8 * j + 6], hi[8 * j + 7]));
-          const uint4 pl = make_uint4(pack_bf16(lo[8 * j + 0], lo[8 * j + 1]), pack_bf16(lo[8 * j + 2], lo[8 * j + 3]),
-                                      pack_bf16(lo[8 * j + 4], lo[8 * j + 5]), pack_bf16(lo[8 * j + 6], lo[8 * j + 7]));
+          uint32_t ph[4], pl[4];
+#pragma unroll
+          for (int e = 0; e < 4; ++e) split_pair(bv[8 * j + 2 * e], bv[8 * j + 2 * e + 1], ph[e], pl[e]);
           const int off = (2 * warp + j) * 512 + (lane >> 3) * 128 + (lane & 7) * 16;
-          *reinterpret_cast<uint4*>(sh.btile[buf][0] + off) = ph;
-          *reinterpret_cast<uint4*>(sh.btile[buf][1] + off) = pl;
+          *reinterpret_cast<uint4*>(sh.btile[buf][0] + off) = make_uint4(ph[0], ph[1], ph[2], ph[3]);
+          *reinterpret_cast<uint4*>(sh.btile[buf][1] + off) = make_uint4(pl[0], pl[1], pl[2], pl[3]);
         }
       }
 #pragma unroll
@@ -305,8 +363,8 @@ __global__ void __launch_bounds__(128, 1) tc_deposit_kernel(Geom g, TcParams tp,
       // tensor-memory lane 32w + t (TF32: columns 32*buf .. +31; BF16: the
       // hi pairs in columns 32*buf .. +15 and the lo pairs in +16 .. +31).
       const bool row = t_row < 27;
-      const float* xrow = sh.fac[warp][row ? tx : 0];
-      const float* yzrow = sh.fac[warp][row ? 3 + tyz : 0];
+      const float* xrow = sh.fac[warp][row ? tx : 12];
+      const float* yzrow = sh.fac[warp][row ? 3 + tyz : 12];
       if constexpr (!Bf16) {
 #pragma unroll
         for (int q8 = 0; q8 < 4; ++q8) {
@@ -315,10 +373,10 @@ __global__ void __launch_bounds__(128, 1) tc_deposit_kernel(Geom g, TcParams tp,
           for (int h = 0; h < 2; ++h) {
             const float4 xf = *reinterpret_cast<const float4*>(xrow + 8 * q8 + 4 * h);
             const float4 yzf = *reinterpret_cast<const float4*>(yzrow + 8 * q8 + 4 * h);
-            m[4 * h + 0] = row ? tc::to_tf32(xf.x * yzf.x) : 0u;
-            m[4 * h + 1] = row ? tc::to_tf32(xf.y * yzf.y) : 0u;
-            m[4 * h + 2] = row ? tc::to_tf32(xf.z * yzf.z) : 0u;
-            m[4 * h + 3] = row ? tc::to_tf32(xf.w * yzf.w) : 0u;
+            m[4 * h + 0] = tc::to_tf32(xf.x * yzf.x);
+            m[4 * h + 1] = tc::to_tf32(xf.y * yzf.y);
+            m[4 * h + 2] = tc::to_tf32(xf.z * yzf.z);
+            m[4 * h + 3] = tc::to_tf32(xf.w * yzf.w);
           }
           tc::tmem_st8(tmem + lane_base + (buf ? 32u : 0u) + 8 * q8, m);
         }
@@ -330,16 +388,8 @@ __global__ void __launch_bounds__(128, 1) tc_deposit_kernel(Geom g, TcParams tp,
           for (int h = 0; h < 4; ++h) {
             const float4 xf = *reinterpret_cast<const float4*>(xrow + 16 * q16 + 4 * h);
             const float4 yzf = *reinterpret_cast<const float4*>(yzrow + 16 * q16 + 4 * h);
-            float v4[4] = {xf.x * yzf.x, xf.y * yzf.y, xf.z * yzf.z, xf.w * yzf.w};
-            float hi4[4], lo4[4];
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-              split_bf16(row ? v4[e] : 0.0f, hi4[e], lo4[e]);
-            }
-            mh[2 * h + 0] = pack_bf16(hi4[0], hi4[1]);
-            mh[2 * h + 1] = pack_bf16(hi4[2], hi4[3]);
-            ml[2 * h + 0] = pack_bf16(lo4[0], lo4[1]);
-            ml[2 * h + 1] = pack_bf16(lo4[2], lo4[3]);
+            split_pair(xf.x * yzf.x, xf.y * yzf.y, mh[2 * h + 0], ml[2 * h + 0]);
+            split_pair(xf.z * yzf.z, xf.w * yzf.w, mh[2 * h + 1], ml[2 * h + 1]);
           }
           tc::tmem_st8(tmem + lane_base + (buf ? 32u : 0u) + 8 * q16, mh);
           tc::tmem_st8(tmem + lane_base + (buf ? 32u : 0u) + 16 + 8 * q16, ml);
@@ -375,93 +425,60 @@ __global__ void __launch_bounds__(128, 1) tc_deposit_kernel(Geom g, TcParams tp,
         }
         tc::commit(&sh.mbar[buf]);
       }
-      pending[buf] = true;
+      pending |= 1u << buf;
       buf ^= 1;
     }
     if (failed) break;
 
-    // J-hat corner sums of this warp's cell: reduce-scatter of the 24 lane
-    // sums, staged for the coalesced moment store.
-    {
-      const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
-      float h12[12];
-#pragma unroll
-      for (int t = 0; t < 12; ++t) {
-        const float keep = b4 ? jsum[t + 12] : jsum[t];
-        const float send = b4 ? jsum[t] : jsum[t + 12];
-        h12[t] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
-      }
-      float h6[6];
-#pragma unroll
-      for (int t = 0; t < 6; ++t) {
-        const float keep = b3 ? h12[t + 6] : h12[t];
-        const float send = b3 ? h12[t] : h12[t + 6];
-        h6[t] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
-      }
-      float h3[3];
-#pragma unroll
-      for (int t = 0; t < 3; ++t) {
-        const float keep = b2 ? h6[t + 3] : h6[t];
-        const float send = b2 ? h6[t] : h6[t + 3];
-        h3[t] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
-      }
-#pragma unroll
-      for (int t = 0; t < 3; ++t) {
-        h3[t] += __shfl_xor_sync(0xffffffffu, h3[t], 2);
-        h3[t] += __shfl_xor_sync(0xffffffffu, h3[t], 1);
-      }
-      if ((lane & 3) == 0) {
-        const int index0 = (b4 ? 12 : 0) + (b3 ? 6 : 0) + (b2 ? 3 : 0);
-#pragma unroll
-        for (int t = 0; t < 3; ++t) {
-          float value = live ? h3[t] : 0.0f;
-          if (!isfinite(value)) {
-            atomicAdd(invalid, 1u);
-            value = 0.0f;
-          }
-          sh.stage[kMassMoments + index0 + t][warp] = value;
-        }
-      }
-    }
-
-    // Mass moments: wait for the group's last MMA and read G_w.
+    // Moments: wait for the group's last MMA, read G and H of this warp's
+    // cell and form the corner currents J[a][c] = sum_b H[t(a, b)][c].
+    float* stage = sh.stage[warp];
+    float* hs = sh.hsum[warp];
     if (maxc > 0) {
       const int last = buf ^ 1;
-      const bool ok = tc::mbar_wait(&sh.mbar[last], phase[last]);
-      phase[last] ^= 1u;
-      pending[last] = false;
+      const bool ok = tc::mbar_wait(&sh.mbar[last], (phase >> last) & 1u);
+      phase ^= 1u << last;
+      pending &= ~(1u << last);
       tc::fence_after_sync();
       if (__syncthreads_or(!ok)) {
         failed = true;
         break;
       }
-      uint32_t gbits[8], g8;
-      tc::tmem_ld8(tmem + lane_base + kDcol + kCols * warp, gbits);
-      tc::tmem_ld1(tmem + lane_base + kDcol + kCols * warp + 8, g8);
+      uint32_t g8[8], g4[4];
+      tc::tmem_ld8(tmem + lane_base + kDcol + kCols * warp, g8);
+      tc::tmem_ld4(tmem + lane_base + kDcol + kCols * warp + 8, g4);
       tc::tmem_wait_ld();
       if (t_row < 27) {
-        float G[9];
+        const bool use = live && count > 0;
 #pragma unroll
-        for (int e = 0; e < 8; ++e) G[e] = __uint_as_float(gbits[e]);
-        G[8] = __uint_as_float(g8);
+        for (int e = 0; e < 8; ++e) stage[t_row * 9 + e] = use ? __uint_as_float(g8[e]) : 0.0f;
+        stage[t_row * 9 + 8] = use ? __uint_as_float(g4[0]) : 0.0f;
 #pragma unroll
-        for (int e = 0; e < 9; ++e) {
-          float value = (live && count > 0) ? G[e] : 0.0f;
-          if (!isfinite(value)) {
-            atomicAdd(invalid, 1u);
-            value = 0.0f;
-          }
-          sh.stage[t_row * 9 + e][warp] = value;
-        }
+        for (int c = 0; c < 3; ++c) hs[t_row * 3 + c] = use ? __uint_as_float(g4[1 + c]) : 0.0f;
       }
-    } else if (t_row < 27) {
+      __syncwarp();
+      if (lane < 24) {
+        const int a = lane / 3, c = lane - 3 * (lane / 3);
+        float sum = 0.0f;
 #pragma unroll
-      for (int e = 0; e < 9; ++e) sh.stage[t_row * 9 + e][warp] = 0.0f;
+        for (int b = 0; b < 8; ++b) sum += hs[monomial_class(a, b) * 3 + c];
+        stage[kMassMoments + lane] = sum;
+      }
+    } else {
+      for (int i = lane; i < kMoments; i += 32) stage[i] = 0.0f;
     }
     __syncthreads();
     // Coalesced moment store: entry q of the group's four cells is 16 bytes.
+    bool bad_value = false;
     for (int qi = threadIdx.x; qi < kMoments; qi += blockDim.x) {
-      float4 val = make_float4(sh.stage[qi][0], sh.stage[qi][1], sh.stage[qi][2], sh.stage[qi][3]);
+      float4 val = make_float4(sh.stage[0][qi], sh.stage[1][qi], sh.stage[2][qi], sh.stage[3][qi]);
+      if (!isfinite(val.x + val.y + val.z + val.w)) {
+        bad_value = true;
+        val.x = isfinite(val.x) ? val.x : 0.0f;
+        val.y = isfinite(val.y) ? val.y : 0.0f;
+        val.z = isfinite(val.z) ? val.z : 0.0f;
+        val.w = isfinite(val.w) ? val.w : 0.0f;
+      }
       float4* dst = reinterpret_cast<float4*>(mom + qi * mom_stride + grp * kCells);
       if (accumulate) {
         const float4 old = *dst;
@@ -469,6 +486,7 @@ __global__ void __launch_bounds__(128, 1) tc_deposit_kernel(Geom g, TcParams tp,
       }
       *dst = val;
     }
+    if (bad_value) atomicAdd(invalid, 1u);
     // D is overwritten by the next group's first MMA only after every warp
     // has read it.
     tc::fence_before_sync();
@@ -481,7 +499,7 @@ __global__ void __launch_bounds__(128, 1) tc_deposit_kernel(Geom g, TcParams tp,
   // Retire in-flight MMAs (bounded) before freeing tensor memory.
 #pragma unroll
   for (int b = 0; b < 2; ++b)
-    if (pending[b]) tc::mbar_wait(&sh.mbar[b], phase[b]);
+    if (pending & (1u << b)) tc::mbar_wait(&sh.mbar[b], (phase >> b) & 1u);
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
@@ -496,30 +514,43 @@ long long moment_stride(const Geom& g) {
 }
 size_t moment_floats(const Geom& g) { return size_t(kMoments) * size_t(moment_stride(g)); }
 
-cudaError_t launch_deposit_tc(int mass_kind, const Geom& g, double qom, double dt, double c,
-                              const tpicb200_particles* p, const uint32_t* counts, const uint32_t* offsets,
-                              const void* bnode, float* moments, int accumulate, uint32_t* invalid,
-                              cudaStream_t s) {
+cudaError_t launch_deposit_tc(int mass_kind, const Geom& g, int ns, const double* qom, double dt, double c,
+                              const tpicb200_particles* const* p, const uint32_t* const* counts,
+                              const uint32_t* const* offsets, const void* bnode, float* moments, int accumulate,
+                              uint32_t* invalid, cudaStream_t s) {
   if (mass_kind != TPICB200_MASS_TF32 && mass_kind != TPICB200_MASS_BF16X3) return cudaErrorNotSupported;
-  if (!moments) return cudaErrorInvalidValue;
-  TcParams tp{float(qom * dt / 2 / c), float(g.inv_volume)};
+  if (!moments || ns < 1) return cudaErrorInvalidValue;
   int device = 0, sms = 148;
   cudaGetDevice(&device);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   const long long cells = (long long)g.nx * g.ny * g.nz;
   const long long groups = (cells + kCells - 1) / kCells;
-  const unsigned blocks = unsigned(std::min<long long>(groups, 4LL * sms));
+  const unsigned blocks = unsigned(std::min<long long>(groups, (long long)kCtasPerSm * sms));
   // Dynamic shared-memory padding brings each CTA to ~47 KB, so at most four
   // CTAs (4 x 128 tensor-memory columns = all 512) are resident per SM and
-  // no tcgen05.alloc ever waits for another CTA's columns.
+  // no tcgen05.alloc ever waits for another CTA's columns; the maximum
+  // shared-memory carveout lets all four be resident.
   const bool tf32 = mass_kind == TPICB200_MASS_TF32;
   auto kernel = tf32 ? tc_deposit_kernel<false> : tc_deposit_kernel<true>;
   const int pad = 47 * 1024 - int(tf32 ? sizeof(TcShared<false>) : sizeof(TcShared<true>));
-  kernel<<<blocks, 128, pad, s>>>(g, tp, (const double*)p->rx, (const double*)p->ry,
-      (const double*)p->rz, (const float*)p->u, (const float*)p->v, (const float*)p->w, p->q, p->cell, counts,
-      offsets, (const float*)bnode, moments, moment_stride(g), accumulate, invalid);
-  count_launches(1);
-  return cudaGetLastError();
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  if (e != cudaSuccess) return e;
+  for (int first = 0; first < ns; first += kFuse) {
+    TcParams tp{};
+    tp.ns = std::min(kFuse, ns - first);
+    tp.inv_volume = float(g.inv_volume);
+    for (int i = 0; i < tp.ns; ++i) {
+      const tpicb200_particles* sp = p[first + i];
+      tp.sp[i] = TcSpecies{(const double*)sp->rx, (const double*)sp->ry, (const double*)sp->rz,
+                           (const float*)sp->u, (const float*)sp->v, (const float*)sp->w, sp->q, sp->cell,
+                           counts[first + i], offsets[first + i], float(qom[first + i] * dt / 2 / c)};
+    }
+    kernel<<<blocks, 128, pad, s>>>(g, tp, (const float*)bnode, moments, moment_stride(g),
+                                    (accumulate || first > 0) ? 1 : 0, invalid);
+    count_launches(1);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 namespace {
@@ -531,7 +562,7 @@ struct StencilPairs {
   int corner[14][8];
   int monomial[14][8];
 };
-constexpr StencilPairs make_stencil_pairs() {
+__host__ __device__ constexpr StencilPairs make_stencil_pairs() {
   StencilPairs r{};
   for (int s = 0; s < 14; ++s)
     for (int a = 0; a < 8; ++a) {
@@ -545,50 +576,66 @@ constexpr StencilPairs make_stencil_pairs() {
     }
   return r;
 }
-__constant__ StencilPairs c_stencil_pairs = make_stencil_pairs();
 
-// Record entry k < 126 (stencil k/9, component k%9) and current component
-// k - 126 of every unique node, summed over the cells that share it in
-// increasing corner order, added to M and J.
-__global__ void __launch_bounds__(256) assemble_moments_kernel(Geom g, const float* __restrict__ mom,
+// One thread per unique node: every record entry (stencil s, component e) is
+// the sum, in increasing corner order, of the moments G[t][e] of the cells
+// holding the pairs (a, a + offset_s); current component c is the sum of the
+// eight corner sums J[a][c] of the cells around the node. The tables are
+// compile-time constants, so the loops unroll into straight loads whose
+// addresses are consecutive across the warp (consecutive nodes, consecutive
+// cells). `overwrite` stores the sums (J and M were cleared and nothing else
+// was deposited); otherwise they are added.
+__global__ void __launch_bounds__(128) assemble_moments_kernel(Geom g, const float* __restrict__ mom,
                                                                long long stride, float* __restrict__ J,
-                                                               float* __restrict__ M) {
-  const long long unique = (long long)g.nx * g.ny * g.nz;
-  const long long total = 129 * unique;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-       t += (long long)gridDim.x * blockDim.x) {
-    const int k = int(t / unique);
-    const long long vtx = t - k * unique;
-    const int i = int(vtx % g.nx), j = int((vtx / g.nx) % g.ny), kk = int(vtx / ((long long)g.nx * g.ny));
-    auto cell_of = [&](int a) {
-      const int ci = wrap_index(i - (a & 1), g.nx), cj = wrap_index(j - ((a >> 1) & 1), g.ny),
-                ck = wrap_index(kk - ((a >> 2) & 1), g.nz);
-      return ci + (long long)g.nx * (cj + (long long)g.ny * ck);
-    };
-    const long long node = g.node(i, j, kk);
-    if (k < 126) {
-      const int s = k / 9, e = k - 9 * (k / 9);
-      float sum = 0.0f;
-      const int n = c_stencil_pairs.count[s];
-      for (int p = 0; p < n; ++p)
-        sum += mom[(c_stencil_pairs.monomial[s][p] * 9 + e) * stride + cell_of(c_stencil_pairs.corner[s][p])];
-      if (sum != 0.0f) M[g.mass_index(node, k)] += sum;
-    } else {
-      const int c = k - 126;
+                                                               float* __restrict__ M, int overwrite) {
+  constexpr StencilPairs pairs = make_stencil_pairs();
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const long long unique = (long long)nx * ny * nz;
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < unique;
+       v += (long long)gridDim.x * blockDim.x) {
+    const int i = int(v % nx);
+    const long long r = v / nx;
+    const int j = int(r % ny), k = int(r / ny);
+    // Cells of corner a: the node is corner a of cell (i - a_x, j - a_y, k - a_z).
+    const int i0 = i, i1 = i > 0 ? i - 1 : nx - 1;
+    const int j0 = j, j1 = j > 0 ? j - 1 : ny - 1;
+    const int k0 = k, k1 = k > 0 ? k - 1 : nz - 1;
+    long long cell[8];
+#pragma unroll
+    for (int a = 0; a < 8; ++a)
+      cell[a] = ((a & 1) ? i1 : i0) + (long long)nx * (((a & 2) ? j1 : j0) + (long long)ny * ((a & 4) ? k1 : k0));
+    const long long node = g.node(i, j, k);
+#pragma unroll
+    for (int st = 0; st < 14; ++st) {
+#pragma unroll
+      for (int e = 0; e < 9; ++e) {
+        float sum = 0.0f;
+#pragma unroll
+        for (int p = 0; p < 8; ++p)
+          if (p < pairs.count[st])
+            sum += __ldg(mom + (pairs.monomial[st][p] * 9 + e) * stride + cell[pairs.corner[st][p]]);
+        float* dst = M + g.mass_index(node, st * 9 + e);
+        *dst = overwrite ? sum : *dst + sum;
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
       float sum = 0.0f;
 #pragma unroll
-      for (int a = 0; a < 8; ++a) sum += mom[(kMassMoments + a * 3 + c) * stride + cell_of(a)];
-      if (sum != 0.0f) J[c * g.nodes + node] += sum;
+      for (int a = 0; a < 8; ++a) sum += __ldg(mom + (kMassMoments + a * 3 + c) * stride + cell[a]);
+      float* dst = J + c * g.nodes + node;
+      *dst = overwrite ? sum : *dst + sum;
     }
   }
 }
 
 }  // namespace
 
-cudaError_t launch_assemble_moments(const Geom& g, const float* moments, void* j, void* mass, cudaStream_t s) {
-  const long long total = 129LL * g.nx * g.ny * g.nz;
-  assemble_moments_kernel<<<grid_for(total, 256, 148u * 16u), 256, 0, s>>>(g, moments, moment_stride(g),
-                                                                           (float*)j, (float*)mass);
+cudaError_t launch_assemble_moments(const Geom& g, const float* moments, void* j, void* mass, int overwrite,
+                                    cudaStream_t s) {
+  const long long unique = (long long)g.nx * g.ny * g.nz;
+  assemble_moments_kernel<<<grid_for(unique, 128, 148u * 16u), 128, 0, s>>>(g, moments, moment_stride(g), (float*)j,
+                                                                            (float*)mass, overwrite);
   count_launches(1);
   return cudaGetLastError();
 }
