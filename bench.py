@@ -292,12 +292,14 @@ def stage_kernel_times(sim, args, stream, repeats: int = 5) -> dict:
     out["deposit"] = {"ms": timed(deposit),
                       "bytes": n_total * (24 + 3 * vb + 8 + 4) + nodes * (126 + 3) * fb}
 
-    # Sort of all species (ping-pong into the idle slot and back, one each way).
+    # Sort of all species as the cycle runs it (the binned sort of records
+    # grouped by the live bins; ping-pong into the idle slot and back).
     def sort_once():
         for s in range(ns):
             cur = st.current[s]
-            _lib.check(lib.tpicb200_sort(sim.ctx, C.byref(st.slot[s][cur]), C.byref(st.slot[s][1 - cur]),
-                                         st.counts[s], st.offsets[s], scratch_inv.data_ptr(), s_))
+            _lib.check(lib.tpicb200_sort_binned(sim.ctx, C.byref(st.slot[s][cur]), st.counts[s], st.offsets[s],
+                                                C.byref(st.slot[s][1 - cur]), st.counts[s], st.offsets[s],
+                                                scratch_inv.data_ptr(), s_))
             st.current[s] = 1 - cur
     out["sort"] = {"ms": timed(sort_once), "bytes": n_total * (4 + 2 * (24 + 3 * vb + 8 + 4))}
     # Make sure the live slot is the sorted one with valid bins (an even number of sorts ran).

@@ -201,6 +201,23 @@ int tpicb200_sort(tpicb200_context* ctx, const tpicb200_particles* in, tpicb200_
                   uint32_t* counts, uint32_t* offsets, uint32_t* invalid,
                   tpicb200_stream stream);
 
+/* Stable sort of records that are grouped by the bins (in_counts,
+ * in_offsets) of an earlier tpicb200_sort and whose keys changed since (the
+ * mover updates keys in place): the same output, counts and offsets as
+ * tpicb200_sort of the same input. When every record moved to one of the 27
+ * cells around its bin (periodic) and the old bins tile the records in key
+ * order, the records go straight to their output positions through per-cell
+ * transfer counts; any other input takes the general path, which the device
+ * selects without a host round trip. in_counts/in_offsets may alias
+ * counts/offsets (they are read before the new bins are written). No single
+ * reference counterpart: it replaces FullParticleSort::enqueue
+ * (simulation/actions/local_species_actions_device.hpp:202-216 ->
+ * lpfx/algorithm/particle/device/cuda_hip/sort.hpp:64-260) on the cycle's
+ * post-mover sort. */
+int tpicb200_sort_binned(tpicb200_context* ctx, const tpicb200_particles* in, const uint32_t* in_counts,
+                         const uint32_t* in_offsets, tpicb200_particles* out, uint32_t* counts,
+                         uint32_t* offsets, uint32_t* invalid, tpicb200_stream stream);
+
 /* Zero J (node field) and the mass records. Replaces enqueue_clear_mass_matrix
  * (ecsim/mass_matrix/mass_matrix_deposition_device.hpp:107-121) and the moment clear. */
 int tpicb200_clear_moments(tpicb200_context* ctx, void* j, void* mass, tpicb200_stream stream);

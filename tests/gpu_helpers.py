@@ -100,6 +100,20 @@ class StageContext:
                                           offsets.data_ptr(), self.invalid.data_ptr(), self.stream))
         return dst, counts, offsets
 
+    def sort_binned(self, src: dict, n: int, in_counts, in_offsets, with_id=None, alias=False):
+        """tpicb200_sort_binned; with `alias` the new bins overwrite in_counts/in_offsets."""
+        dst = self.empty_particles(n, ("id" in src) if with_id is None else with_id)
+        if alias:
+            counts, offsets = in_counts, in_offsets
+        else:
+            counts = torch.zeros(self.layout.bin_count, dtype=torch.int32, device="cuda")
+            offsets = torch.zeros(self.layout.bin_count + 1, dtype=torch.int32, device="cuda")
+        pin, pout = self.struct(src, n), self.struct(dst, n)
+        _lib.check(self.lib.tpicb200_sort_binned(self.ctx, C.byref(pin), in_counts.data_ptr(), in_offsets.data_ptr(),
+                                                 C.byref(pout), counts.data_ptr(), offsets.data_ptr(),
+                                                 self.invalid.data_ptr(), self.stream))
+        return dst, counts, offsets
+
     def records(self, m) -> np.ndarray:
         """Mass coefficients of a device buffer in TPIC's record order (float64)."""
         a = m.cpu().numpy().astype(np.float64)

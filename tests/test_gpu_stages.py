@@ -34,13 +34,6 @@ def species_arrays(g, precision, seed=3, vth=(0.6, 0.5, 0.4), npcel=(2, 2, 2), q
     return d
 
 
-@pytest.fixture(scope="module")
-def torch_cuda():
-    import torch
-    assert torch.cuda.is_available()
-    return torch
-
-
 def make_ctx(g, precision, **kw):
     from gpu_helpers import StageContext
     return StageContext(g, precision=precision, **kw)

@@ -20,6 +20,7 @@ struct tpicb200_context {
   uint32_t* cursor = nullptr;
   uint32_t* perm = nullptr;
   uint32_t* scan = nullptr;
+  uint32_t* binned = nullptr;    // binned-sort state, old bins and transfer counts
   uint32_t* invalid = nullptr;   // context's own invalid counter
   double* partials = nullptr;    // energy reduction partials
   double* reduced = nullptr;     // energy reduction results
@@ -145,6 +146,7 @@ int tpicb200_create(const tpicb200_grid* grid, const tpicb200_options* options, 
   alloc((void**)&ctx->cursor, size_t(ctx->g.bins) * 4);
   alloc((void**)&ctx->perm, size_t(options->max_particles) * 4);
   alloc((void**)&ctx->scan, sort_scan_words(ctx->g.bins) * 4);
+  alloc((void**)&ctx->binned, binned_scratch_words(ctx->g) * 4);
   alloc((void**)&ctx->invalid, 4);
   alloc((void**)&ctx->partials, size_t(ctx->energy_blocks) * (2 + 5 * TPICB200_MAX_SPECIES) * 8);
   alloc((void**)&ctx->reduced, (2 + 5 * TPICB200_MAX_SPECIES + 2) * 8);
@@ -165,7 +167,7 @@ int tpicb200_destroy(tpicb200_context* ctx) {
   if (!ctx) return TPICB200_SUCCESS;
   cudaDeviceSynchronize();
   solver_destroy(ctx->solver);
-  cudaFree(ctx->cursor); cudaFree(ctx->perm); cudaFree(ctx->scan); cudaFree(ctx->invalid);
+  cudaFree(ctx->cursor); cudaFree(ctx->perm); cudaFree(ctx->scan); cudaFree(ctx->binned); cudaFree(ctx->invalid);
   cudaFree(ctx->partials); cudaFree(ctx->reduced); cudaFree(ctx->moments);
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
   for (auto& ev : ctx->events)
@@ -213,6 +215,26 @@ int tpicb200_sort(tpicb200_context* ctx, const tpicb200_particles* in, tpicb200_
   return cuda_status(launch_sort(ctx->opt.precision, ctx->g, in, out, counts, offsets, ctx->cursor, ctx->perm,
                                  ctx->scan, invalid_or_own(ctx, invalid), (cudaStream_t)stream),
                      "sort launch failed");
+}
+
+int tpicb200_sort_binned(tpicb200_context* ctx, const tpicb200_particles* in, const uint32_t* in_counts,
+                         const uint32_t* in_offsets, tpicb200_particles* out, uint32_t* counts,
+                         uint32_t* offsets, uint32_t* invalid, tpicb200_stream stream) {
+  if (int s = check_ctx(ctx)) return s;
+  if (!in_counts || !in_offsets) return fail(TPICB200_INVALID_ARGUMENT, "binned sort needs the input's bins");
+  if (!binned_sort_applies(ctx->g, in ? in->count : 0, ctx->opt.max_particles))
+    return tpicb200_sort(ctx, in, out, counts, offsets, invalid, stream);
+  if (int s = check_particles(ctx, in)) return s;
+  if (!out || !counts || !offsets) return fail(TPICB200_INVALID_ARGUMENT, "sort needs output records and bins");
+  if (in->count && (!out->rx || !out->ry || !out->rz || !out->u || !out->v || !out->w || !out->q ||
+                    !out->cell || (in->id && !out->id)))
+    return fail(TPICB200_INVALID_ARGUMENT, "null output attribute");
+  if (in->count && (in->rx == out->rx || in->cell == out->cell))
+    return fail(TPICB200_INVALID_ARGUMENT, "sort input and output alias");
+  return cuda_status(launch_sort_binned(ctx->opt.precision, ctx->g, in, in_counts, in_offsets, out, counts, offsets,
+                                        ctx->cursor, ctx->perm, ctx->scan, ctx->binned, invalid_or_own(ctx, invalid),
+                                        (cudaStream_t)stream),
+                     "binned sort launch failed");
 }
 
 int tpicb200_clear_moments(tpicb200_context* ctx, void* j, void* mass, tpicb200_stream stream) {
@@ -393,12 +415,17 @@ static int deposit_all(tpicb200_context* ctx, tpicb200_state* st, const void* b_
   return tpicb200_fold_periodic(ctx, st->j, st->mass, (tpicb200_stream)s);
 }
 
-static int sort_all(tpicb200_context* ctx, tpicb200_state* st, cudaStream_t s) {
+// `binned`: the live slots are grouped by the state's bins (the cycle's
+// post-mover sort); otherwise (startup) the general sort runs.
+static int sort_all(tpicb200_context* ctx, tpicb200_state* st, bool binned, cudaStream_t s) {
   for (int sp = 0; sp < st->ns; ++sp) {
     const int cur = st->current[sp];
     tpicb200_particles* in = &st->slot[sp][cur];
     tpicb200_particles* out = &st->slot[sp][1 - cur];
-    if (int r = tpicb200_sort(ctx, in, out, st->counts[sp], st->offsets[sp], nullptr, (tpicb200_stream)s)) return r;
+    const int r = binned ? tpicb200_sort_binned(ctx, in, st->counts[sp], st->offsets[sp], out, st->counts[sp],
+                                                st->offsets[sp], nullptr, (tpicb200_stream)s)
+                         : tpicb200_sort(ctx, in, out, st->counts[sp], st->offsets[sp], nullptr, (tpicb200_stream)s);
+    if (r) return r;
     st->current[sp] = 1 - cur;
   }
   return TPICB200_SUCCESS;
@@ -425,7 +452,7 @@ int tpicb200_prepare(tpicb200_context* ctx, tpicb200_state* st, tpicb200_stream 
   if (int r = check_state(ctx, st)) return r;
   cudaStream_t s = (cudaStream_t)stream;
   if (int r = tpicb200_magnetic_to_nodes(ctx, st->b_cell, st->b_node, stream)) return r;
-  if (int r = sort_all(ctx, st, s)) return r;
+  if (int r = sort_all(ctx, st, false, s)) return r;
   return deposit_all(ctx, st, st->b_node, s);
 }
 
@@ -460,7 +487,7 @@ int tpicb200_cycle(tpicb200_context* ctx, tpicb200_state* st, int ncycles, tpicb
     if (int r = tpicb200_field_advance(ctx, st->e, st->b_cell, st->e_theta, st->b_cell_next, st->b_node_next, stream))
       return r;
     cudaEventRecord(ev[3], s);
-    if (int r = sort_all(ctx, st, s)) return r;
+    if (int r = sort_all(ctx, st, true, s)) return r;
     cudaEventRecord(ev[4], s);
     // Deposition of the moved records with the next B.
     if (int r = deposit_all(ctx, st, st->b_node_next, s)) return r;

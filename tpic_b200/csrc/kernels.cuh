@@ -20,6 +20,16 @@ cudaError_t launch_sort(int precision, const Geom& g, const tpicb200_particles* 
                         tpicb200_particles* out, uint32_t* counts, uint32_t* offsets,
                         uint32_t* cursor, uint32_t* perm, uint32_t* scan_scratch,
                         uint32_t* invalid, cudaStream_t s);
+// Sort of records grouped by the bins (in_counts, in_offsets) of an earlier
+// sort, keys updated since: neighbour moves go through the transfer-count
+// path, anything else through the general sort (same stable order).
+size_t binned_scratch_words(const Geom& g);
+bool binned_sort_applies(const Geom& g, uint32_t count, size_t max_particles);
+cudaError_t launch_sort_binned(int precision, const Geom& g, const tpicb200_particles* in,
+                               const uint32_t* in_counts, const uint32_t* in_offsets, tpicb200_particles* out,
+                               uint32_t* counts, uint32_t* offsets, uint32_t* cursor, uint32_t* perm,
+                               uint32_t* scan_scratch, uint32_t* binned_scratch, uint32_t* invalid,
+                               cudaStream_t s);
 
 // deposit.cu
 cudaError_t launch_deposit(int precision, int mass_kind, const Geom& g, double qom, double dt,

@@ -52,9 +52,28 @@ __device__ __forceinline__ void aggregated_add(uint32_t* base, int32_t key, bool
   }
 }
 
+// `gate`: the kernels of the general path run only when it is null or holds a
+// nonzero word (the binned sort's fallback flag).
+__device__ __forceinline__ bool closed(const uint32_t* gate) { return gate && *gate == 0; }
+
+__global__ void __launch_bounds__(256) fill_kernel(uint32_t* out, long long n, uint32_t value,
+                                                   const uint32_t* gate) {
+  if (closed(gate)) return;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = value;
+}
+
+__global__ void __launch_bounds__(256) copy_kernel(uint32_t* out, const uint32_t* __restrict__ in, long long n,
+                                                   const uint32_t* gate) {
+  if (closed(gate)) return;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = in[i];
+}
+
 __global__ void __launch_bounds__(256) histogram_kernel(Geom g, const int32_t* __restrict__ keys,
                                                         uint32_t count, uint32_t* counts,
-                                                        uint32_t* flag) {
+                                                        uint32_t* flag, const uint32_t* gate) {
+  if (closed(gate)) return;
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < count; base += stride) {
     const uint32_t i = base + (threadIdx.x & 31);
@@ -69,9 +88,9 @@ __global__ void __launch_bounds__(256) histogram_kernel(Geom g, const int32_t* _
 
 __global__ void __launch_bounds__(kScanThreads) scan_reduce_kernel(const uint32_t* __restrict__ counts,
                                                                    long long bins, uint32_t* block_sums,
-                                                                   const uint32_t* flag) {
+                                                                   const uint32_t* flag, const uint32_t* gate) {
   __shared__ uint32_t scratch[kScanThreads / 32];
-  if (*flag) return;
+  if (closed(gate) || *flag) return;
   const long long base = (long long)blockIdx.x * kScanTile;
   uint32_t sum = 0;
 #pragma unroll
@@ -85,9 +104,9 @@ __global__ void __launch_bounds__(kScanThreads) scan_reduce_kernel(const uint32_
 
 // Exclusive scan of the block sums by one block of 1024 threads.
 __global__ void __launch_bounds__(1024) scan_block_sums_kernel(uint32_t* block_sums, int nblocks,
-                                                               const uint32_t* flag) {
+                                                               const uint32_t* flag, const uint32_t* gate) {
   __shared__ uint32_t warp_totals[32];
-  if (*flag) return;
+  if (closed(gate) || *flag) return;
   const int per = (nblocks + 1023) / 1024;
   const int first = threadIdx.x * per;
   uint32_t local = 0;
@@ -126,9 +145,10 @@ __global__ void __launch_bounds__(1024) scan_block_sums_kernel(uint32_t* block_s
 __global__ void __launch_bounds__(kScanThreads) scan_down_kernel(const uint32_t* __restrict__ counts,
                                                                  long long bins,
                                                                  const uint32_t* __restrict__ block_sums,
-                                                                 uint32_t* offsets, const uint32_t* flag) {
+                                                                 uint32_t* offsets, const uint32_t* flag,
+                                                                 const uint32_t* gate) {
   __shared__ uint32_t warp_totals[kScanThreads / 32];
-  if (*flag) return;
+  if (closed(gate) || *flag) return;
   const long long base = (long long)blockIdx.x * kScanTile + (long long)threadIdx.x * kScanItems;
   uint32_t items[kScanItems];
   uint32_t local = 0;
@@ -160,8 +180,8 @@ __global__ void __launch_bounds__(kScanThreads) scan_down_kernel(const uint32_t*
 
 __global__ void __launch_bounds__(256) place_kernel(const int32_t* __restrict__ keys, uint32_t count,
                                                     uint32_t* cursor, uint32_t* perm,
-                                                    const uint32_t* flag) {
-  if (*flag) return;
+                                                    const uint32_t* flag, const uint32_t* gate) {
+  if (closed(gate) || *flag) return;
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < count; base += stride) {
     const uint32_t i = base + (threadIdx.x & 31);
@@ -194,9 +214,9 @@ __global__ void __launch_bounds__(256) fixup_small_kernel(const uint32_t* __rest
                                                           const uint32_t* __restrict__ offsets,
                                                           long long bins, uint32_t* perm,
                                                           uint32_t* large_count, uint32_t* large_bins,
-                                                          const uint32_t* flag) {
+                                                          const uint32_t* flag, const uint32_t* gate) {
   __shared__ uint32_t buffer[8][kWarpBinCapacity];
-  if (*flag) return;
+  if (closed(gate) || *flag) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint32_t* s = buffer[warp];
   const long long warps = (long long)gridDim.x * 8;
@@ -233,9 +253,9 @@ __global__ void __launch_bounds__(1024) fixup_large_kernel(const uint32_t* __res
                                                            uint32_t* perm, uint32_t* scratch,
                                                            const uint32_t* large_count,
                                                            const uint32_t* large_bins,
-                                                           const uint32_t* flag) {
+                                                           const uint32_t* flag, const uint32_t* gate) {
   __shared__ uint32_t s[kBlockBinCapacity];
-  if (*flag) return;
+  if (closed(gate) || *flag) return;
   const uint32_t nlarge = *large_count;
   for (uint32_t item = blockIdx.x; item < nlarge; item += gridDim.x) {
     const uint32_t bin = large_bins[item];
@@ -298,8 +318,8 @@ __global__ void __launch_bounds__(256) gather_kernel(const uint32_t* __restrict_
     const double* __restrict__ iq, const int32_t* __restrict__ ikey, const uint64_t* __restrict__ iid,
     double* __restrict__ orx, double* __restrict__ ory, double* __restrict__ orz,
     Vel* __restrict__ ou, Vel* __restrict__ ov, Vel* __restrict__ ow, double* __restrict__ oq,
-    int32_t* __restrict__ okey, uint64_t* __restrict__ oid, const uint32_t* flag) {
-  if (*flag) return;
+    int32_t* __restrict__ okey, uint64_t* __restrict__ oid, const uint32_t* flag, const uint32_t* gate) {
+  if (closed(gate) || *flag) return;
   for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < count; p += gridDim.x * blockDim.x) {
     const uint32_t s = perm[p];
     orx[p] = irx[s]; ory[p] = iry[s]; orz[p] = irz[s];
@@ -310,7 +330,8 @@ __global__ void __launch_bounds__(256) gather_kernel(const uint32_t* __restrict_
   }
 }
 
-__global__ void report_kernel(const uint32_t* flag, uint32_t* invalid) {
+__global__ void report_kernel(const uint32_t* flag, uint32_t* invalid, const uint32_t* gate) {
+  if (closed(gate)) return;
   if (*flag && invalid) atomicAdd(invalid, 1u);
 }
 
@@ -321,10 +342,12 @@ size_t sort_scan_words(long long bins) {
   return size_t(nblocks) + 2 + size_t(bins);
 }
 
-cudaError_t launch_sort(int precision, const Geom& g, const tpicb200_particles* in,
-                        tpicb200_particles* out, uint32_t* counts, uint32_t* offsets,
-                        uint32_t* cursor, uint32_t* perm, uint32_t* scan_scratch,
-                        uint32_t* invalid, cudaStream_t s) {
+namespace {
+
+// The general sort; with a gate, every step runs only when *gate != 0.
+cudaError_t enqueue_general(int precision, const Geom& g, const tpicb200_particles* in, tpicb200_particles* out,
+                            uint32_t* counts, uint32_t* offsets, uint32_t* cursor, uint32_t* perm,
+                            uint32_t* scan_scratch, uint32_t* invalid, const uint32_t* gate, cudaStream_t s) {
   const long long bins = g.bins;
   const int nblocks = int((bins + kScanTile - 1) / kScanTile);
   ScanScratch sc{scan_scratch, scan_scratch + nblocks, scan_scratch + nblocks + 1,
@@ -332,37 +355,451 @@ cudaError_t launch_sort(int precision, const Geom& g, const tpicb200_particles* 
   const uint32_t n = in->count;
   cudaError_t e;
   if ((e = cudaMemsetAsync(sc.flag, 0, 2 * sizeof(uint32_t), s)) != cudaSuccess) return e;
-  if ((e = cudaMemsetAsync(counts, 0, size_t(bins) * sizeof(uint32_t), s)) != cudaSuccess) return e;
-  if (n) histogram_kernel<<<grid_for(n, 256, 148u * 8u), 256, 0, s>>>(g, in->cell, n, counts, sc.flag);
-  scan_reduce_kernel<<<nblocks, kScanThreads, 0, s>>>(counts, bins, sc.block_sums, sc.flag);
-  scan_block_sums_kernel<<<1, 1024, 0, s>>>(sc.block_sums, nblocks, sc.flag);
-  scan_down_kernel<<<nblocks, kScanThreads, 0, s>>>(counts, bins, sc.block_sums, offsets, sc.flag);
-  if ((e = cudaMemcpyAsync(cursor, offsets, size_t(bins) * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
-                           s)) != cudaSuccess)
-    return e;
+  fill_kernel<<<grid_for(bins, 256, 148u * 8u), 256, 0, s>>>(counts, bins, 0u, gate);
+  if (n) histogram_kernel<<<grid_for(n, 256, 148u * 8u), 256, 0, s>>>(g, in->cell, n, counts, sc.flag, gate);
+  scan_reduce_kernel<<<nblocks, kScanThreads, 0, s>>>(counts, bins, sc.block_sums, sc.flag, gate);
+  scan_block_sums_kernel<<<1, 1024, 0, s>>>(sc.block_sums, nblocks, sc.flag, gate);
+  scan_down_kernel<<<nblocks, kScanThreads, 0, s>>>(counts, bins, sc.block_sums, offsets, sc.flag, gate);
+  copy_kernel<<<grid_for(bins, 256, 148u * 8u), 256, 0, s>>>(cursor, offsets, bins, gate);
+  int launches = 7;
   if (n) {
-    place_kernel<<<grid_for(n, 256, 148u * 8u), 256, 0, s>>>(in->cell, n, cursor, perm, sc.flag);
+    place_kernel<<<grid_for(n, 256, 148u * 8u), 256, 0, s>>>(in->cell, n, cursor, perm, sc.flag, gate);
     fixup_small_kernel<<<grid_for(bins, 256, 148u * 16u), 256, 0, s>>>(
-        counts, offsets, bins, perm, sc.large_count, sc.large_bins, sc.flag);
+        counts, offsets, bins, perm, sc.large_count, sc.large_bins, sc.flag, gate);
     fixup_large_kernel<<<148, 1024, 0, s>>>(counts, offsets, perm, (uint32_t*)out->cell,
-                                            sc.large_count, sc.large_bins, sc.flag);
+                                            sc.large_count, sc.large_bins, sc.flag, gate);
     const unsigned gb = grid_for(n, 256, 148u * 8u);
     if (precision == TPICB200_PRECISION_DOUBLE)
       gather_kernel<double><<<gb, 256, 0, s>>>(perm, n, (const double*)in->rx, (const double*)in->ry,
           (const double*)in->rz, (const double*)in->u, (const double*)in->v, (const double*)in->w,
           in->q, in->cell, in->id, (double*)out->rx, (double*)out->ry, (double*)out->rz,
           (double*)out->u, (double*)out->v, (double*)out->w, out->q, out->cell,
-          in->id ? out->id : nullptr, sc.flag);
+          in->id ? out->id : nullptr, sc.flag, gate);
     else
       gather_kernel<float><<<gb, 256, 0, s>>>(perm, n, (const double*)in->rx, (const double*)in->ry,
           (const double*)in->rz, (const float*)in->u, (const float*)in->v, (const float*)in->w,
           in->q, in->cell, in->id, (double*)out->rx, (double*)out->ry, (double*)out->rz,
           (float*)out->u, (float*)out->v, (float*)out->w, out->q, out->cell,
-          in->id ? out->id : nullptr, sc.flag);
+          in->id ? out->id : nullptr, sc.flag, gate);
+    launches += 4;
   }
-  report_kernel<<<1, 1, 0, s>>>(sc.flag, invalid);
-  count_launches(n ? 9 : 4);
+  report_kernel<<<1, 1, 0, s>>>(sc.flag, invalid, gate);
+  count_launches(launches + 1);
+  return cudaGetLastError();
+}
+
+// ---- Binned sort: the input is grouped by the bins of an earlier sort ----
+//
+// After the mover a species' records are still grouped by the cells of the
+// previous sort, in increasing key order, and almost every record moved to
+// one of the 27 cells around its old one. The stable order of a destination
+// bin is then: its source cells in increasing key order and, within one
+// source, the records in input order. So
+//   1. classify (warp per old interior cell): the direction d < 27 of every
+//      record (periodic wrap; nx, ny, nz >= 3 keep the 27 destinations
+//      distinct) and the transfer counts T[d][c]; any record that did not
+//      move to a neighbour, any invalid key, or old bins that are not a
+//      key-ordered partition of the records raise the fallback flag;
+//   2. counts (thread per bin): counts'[b] = sum_d T[d][b - d];
+//   3. scan of the counts;
+//   4. bases (thread per interior bin): walking the 27 sources of b in key
+//      order, T[d][c] becomes the first output position of c's records that
+//      moved by d;
+//   5. scatter (warp per old interior cell): a record goes to its base plus
+//      its rank among the earlier records of its cell with the same d.
+// With the fallback flag raised, the general sort (enqueued between steps 1
+// and 2, gated on the flag) runs instead and steps 2-5 return at once; the
+// output is the same stable order either way.
+
+constexpr int kBinnedThreads = 256;
+constexpr int kBinnedWarps = kBinnedThreads / 32;
+
+struct BinnedState {
+  uint32_t fallback;
+  uint32_t pad;
+  unsigned long long total;  // records in the old bins
+};
+
+__device__ __forceinline__ int periodic_step(int d, int n) {
+  if (d == n - 1) return -1;
+  if (d == 1 - n) return 1;
+  return d;
+}
+
+// Direction code of a record of old interior cell (i, j, k) whose key is now
+// `key`, or -1 when the key is invalid or not one of the 27 neighbours.
+__device__ __forceinline__ int move_direction(const Geom& g, int i, int j, int k, int32_t key) {
+  if (key < 0 || key >= g.bins) return -1;
+  int a, b, c;
+  g.decode(key, a, b, c);
+  if (!g.interior_cell(a, b, c)) return -1;
+  const int dx = periodic_step(a - i, g.nx), dy = periodic_step(b - j, g.ny), dz = periodic_step(c - k, g.nz);
+  if (dx < -1 || dx > 1 || dy < -1 || dy > 1 || dz < -1 || dz > 1) return -1;
+  return (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1);
+}
+
+// A warp takes 32 consecutive old interior cells at a time. Their records
+// form one contiguous range (the bins between them are empty), streamed 32
+// at a time; each lane finds its record's cell by a binary search over the
+// 32 cell starts in shared memory.
+struct CellRun {
+  uint32_t start[32];  // first record of each cell (ascending)
+  uint32_t begin, end; // record range of the run
+};
+
+// Loads the run of cells u0 .. u0 + 31 (lane l: cell u0 + l) into `run`;
+// returns the lane's cell key (or -1 past the last cell).
+__device__ __forceinline__ int32_t load_run(const Geom& g, long long u0, long long cells,
+                                            const uint32_t* __restrict__ old_counts,
+                                            const uint32_t* __restrict__ old_offsets, CellRun& run, int& ci,
+                                            int& cj, int& ck) {
+  const int lane = threadIdx.x & 31;
+  const long long u = u0 + lane;
+  const bool valid = u < cells;
+  int32_t key = -1;
+  uint32_t off = 0xffffffffu, stop = 0;
+  ci = cj = ck = 0;
+  if (valid) {
+    ci = int(u % g.nx);
+    const long long r = u / g.nx;
+    cj = int(r % g.ny);
+    ck = int(r / g.ny);
+    key = g.encode(ci, cj, ck);
+    off = old_offsets[key];
+    stop = off + old_counts[key];
+  }
+  run.start[lane] = off;
+  const unsigned live = __ballot_sync(0xffffffffu, valid);
+  const int last = 31 - __clz(live);
+  const uint32_t begin = __shfl_sync(0xffffffffu, off, 0);
+  const uint32_t end = __shfl_sync(0xffffffffu, stop, last);
+  if (lane == 0) {
+    run.begin = begin;
+    run.end = end;
+  }
+  __syncwarp();
+  return key;
+}
+
+// Cell (lane index within the run) of record p: the last cell whose start is
+// at most p (empty cells share their successor's start).
+__device__ __forceinline__ int run_cell(const CellRun& run, uint32_t p) {
+  int c = 0;
+#pragma unroll
+  for (int step = 16; step > 0; step >>= 1)
+    if (run.start[c + step] <= p) c += step;
+  return c;
+}
+
+__global__ void __launch_bounds__(kBinnedThreads) classify_kernel(Geom g, const int32_t* __restrict__ keys,
+    uint32_t n, const uint32_t* __restrict__ old_counts, const uint32_t* __restrict__ old_offsets,
+    uint32_t* __restrict__ transfer, uint8_t* __restrict__ code, BinnedState* state) {
+  __shared__ CellRun runs[kBinnedWarps];
+  __shared__ int32_t coords[kBinnedWarps][3][32];  // (i, j, k) of each cell of the run
+  __shared__ uint32_t hist[kBinnedWarps][27][33];
+  __shared__ unsigned long long partial[kBinnedWarps];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const long long cells = (long long)g.nx * g.ny * g.nz;
+  bool bad = false;
+  unsigned long long total = 0;
+  // The old bins must tile the records in key order: disjoint ranges in
+  // increasing key order, records only in interior cells.
+  for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < g.bins;
+       b += (long long)gridDim.x * blockDim.x) {
+    const uint32_t off = old_offsets[b], cnt = old_counts[b];
+    if ((unsigned long long)off + cnt > old_offsets[b + 1]) bad = true;
+    if (cnt) {
+      int i, j, k;
+      g.decode(int32_t(b), i, j, k);
+      if (!g.interior_cell(i, j, k)) bad = true;
+    }
+    total += cnt;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0 && old_offsets[g.bins] > n) bad = true;
+  CellRun& run = runs[warp];
+  for (long long u0 = ((long long)blockIdx.x * kBinnedWarps + warp) * 32; u0 < cells;
+       u0 += (long long)gridDim.x * kBinnedWarps * 32) {
+    int ci, cj, ck;
+    load_run(g, u0, cells, old_counts, old_offsets, run, ci, cj, ck);
+    coords[warp][0][lane] = ci;
+    coords[warp][1][lane] = cj;
+    coords[warp][2][lane] = ck;
+#pragma unroll
+    for (int d = 0; d < 27; ++d) hist[warp][d][lane] = 0;
+    __syncwarp();
+    const uint32_t begin = run.begin, end = run.end;
+    if (begin > end || end > n) {  // bins that do not describe the records: no walk over them
+      bad = true;
+      continue;
+    }
+    // Four chunks per step: the key loads of all four are in flight together.
+    for (uint32_t p0 = begin; p0 < end; p0 += 128) {
+      int32_t key[4];
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        const uint32_t p = p0 + 32 * m + lane;
+        key[m] = p < end ? keys[p] : 0;
+      }
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        if (p0 + 32 * m >= end) break;
+        const uint32_t p = p0 + 32 * m + lane;
+        const bool live = p < end;
+        int c = 0, d = -1;
+        if (live) {
+          c = run_cell(run, p);
+          d = move_direction(g, coords[warp][0][c], coords[warp][1][c], coords[warp][2][c], key[m]);
+          if (d < 0) bad = true;
+          code[p] = uint8_t(d < 0 ? 0xff : d);
+        }
+        const int slot = d < 0 ? -1 : c * 27 + d;
+        const unsigned peers = __match_any_sync(0xffffffffu, slot);
+        if (slot >= 0 && lane == __ffs(peers) - 1) hist[warp][d][c] += __popc(peers);
+        __syncwarp();
+      }
+    }
+    if (u0 + lane < cells)
+#pragma unroll
+      for (int d = 0; d < 27; ++d) transfer[(long long)d * cells + u0 + lane] = hist[warp][d][lane];
+    __syncwarp();
+  }
+  total = warp_sum(total);
+  if (lane == 0) partial[warp] = total;
+  const bool any_bad = __syncthreads_or(bad);
+  if (threadIdx.x == 0) {
+    unsigned long long block_total = 0;
+    for (int w = 0; w < kBinnedWarps; ++w) block_total += partial[w];
+    atomicAdd(&state->total, block_total);
+    if (any_bad) atomicExch(&state->fallback, 1u);
+  }
+}
+
+__global__ void decide_kernel(uint32_t n, BinnedState* state) {
+  if (state->total != (unsigned long long)n) state->fallback = 1;
+}
+
+__global__ void __launch_bounds__(256) binned_counts_kernel(Geom g, const uint32_t* __restrict__ transfer,
+                                                            uint32_t* counts, const BinnedState* state) {
+  if (state->fallback) return;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const long long cells = (long long)nx * ny * nz;
+  for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < g.bins;
+       b += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    g.decode(int32_t(b), i, j, k);
+    uint32_t sum = 0;
+    if (g.interior_cell(i, j, k)) {
+#pragma unroll
+      for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+        for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+          for (int dx = -1; dx <= 1; ++dx) {
+            const int si = wrap_index(i - dx, nx), sj = wrap_index(j - dy, ny), sk = wrap_index(k - dz, nz);
+            const int d = (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1);
+            sum += transfer[d * cells + si + (long long)nx * (sj + (long long)ny * sk)];
+          }
+    }
+    counts[b] = sum;
+  }
+}
+
+// Directions along one axis in increasing source coordinate: the sources of
+// destination x are x - d (periodic).
+__device__ __forceinline__ void source_order(int x, int n, int (&d)[3]) {
+  if (x == 0) { d[0] = 0; d[1] = -1; d[2] = 1; }
+  else if (x == n - 1) { d[0] = -1; d[1] = 1; d[2] = 0; }
+  else { d[0] = 1; d[1] = 0; d[2] = -1; }
+}
+
+__global__ void __launch_bounds__(256) binned_bases_kernel(Geom g, const uint32_t* __restrict__ offsets,
+                                                           uint32_t* transfer, const BinnedState* state) {
+  if (state->fallback) return;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const long long cells = (long long)nx * ny * nz;
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < cells;
+       v += (long long)gridDim.x * blockDim.x) {
+    const int i = int(v % nx);
+    const long long r = v / nx;
+    const int j = int(r % ny), k = int(r / ny);
+    int ox[3], oy[3], oz[3];
+    source_order(i, nx, ox);
+    source_order(j, ny, oy);
+    source_order(k, nz, oz);
+    // Sources (periodic neighbours x - d) in increasing key order.
+    long long index[27];
+    uint32_t count[27];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int b = 0; b < 3; ++b)
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          const int dx = ox[a], dy = oy[b], dz = oz[c];
+          int si = i - dx, sj = j - dy, sk = k - dz;
+          si = si < 0 ? si + nx : (si >= nx ? si - nx : si);
+          sj = sj < 0 ? sj + ny : (sj >= ny ? sj - ny : sj);
+          sk = sk < 0 ? sk + nz : (sk >= nz ? sk - nz : sk);
+          const int e = a + 3 * b + 9 * c;
+          index[e] = ((dx + 1) + 3 * (dy + 1) + 9 * (dz + 1)) * cells + si + (long long)nx * (sj + (long long)ny * sk);
+          count[e] = transfer[index[e]];
+        }
+    uint32_t base = offsets[g.encode(i, j, k)];
+#pragma unroll
+    for (int e = 0; e < 27; ++e) {
+      transfer[index[e]] = base;
+      base += count[e];
+    }
+  }
+}
+
+template <class Vel>
+__global__ void __launch_bounds__(kBinnedThreads) binned_scatter_kernel(Geom g, uint32_t n,
+    const uint32_t* __restrict__ old_counts, const uint32_t* __restrict__ old_offsets,
+    const uint32_t* __restrict__ transfer, const uint8_t* __restrict__ code,
+    const double* __restrict__ irx, const double* __restrict__ iry, const double* __restrict__ irz,
+    const Vel* __restrict__ iu, const Vel* __restrict__ iv, const Vel* __restrict__ iw,
+    const double* __restrict__ iq, const int32_t* __restrict__ ikey, const uint64_t* __restrict__ iid,
+    double* __restrict__ orx, double* __restrict__ ory, double* __restrict__ orz,
+    Vel* __restrict__ ou, Vel* __restrict__ ov, Vel* __restrict__ ow, double* __restrict__ oq,
+    int32_t* __restrict__ okey, uint64_t* __restrict__ oid, const BinnedState* state) {
+  __shared__ CellRun runs[kBinnedWarps];
+  __shared__ uint32_t cursor[kBinnedWarps][27][33];
+  if (state->fallback) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const long long cells = (long long)g.nx * g.ny * g.nz;
+  const unsigned below = (1u << lane) - 1u;
+  CellRun& run = runs[warp];
+  for (long long u0 = ((long long)blockIdx.x * kBinnedWarps + warp) * 32; u0 < cells;
+       u0 += (long long)gridDim.x * kBinnedWarps * 32) {
+    int ci, cj, ck;
+    load_run(g, u0, cells, old_counts, old_offsets, run, ci, cj, ck);
+    if (u0 + lane < cells)
+#pragma unroll
+      for (int d = 0; d < 27; ++d) cursor[warp][d][lane] = transfer[(long long)d * cells + u0 + lane];
+    __syncwarp();
+    const uint32_t begin = run.begin, end = run.end;
+    // Software pipeline: the records of the next chunk are loaded while the
+    // current one is placed.
+    struct Rec {
+      double rx, ry, rz, q;
+      Vel u, v, w;
+      int32_t key;
+      uint64_t id;
+      int d;
+    };
+    auto load = [&](uint32_t p) {
+      Rec r{0, 0, 0, 0, Vel(0), Vel(0), Vel(0), 0, 0, 0};
+      if (p < end) {
+        r.rx = irx[p]; r.ry = iry[p]; r.rz = irz[p];
+        r.u = iu[p]; r.v = iv[p]; r.w = iw[p];
+        r.q = iq[p];
+        r.key = ikey[p];
+        if (oid) r.id = iid[p];
+        r.d = code[p];
+      }
+      return r;
+    };
+    Rec cur = load(begin + lane);
+    for (uint32_t p0 = begin; p0 < end; p0 += 32) {
+      const uint32_t p = p0 + lane;
+      const Rec nxt = load(p + 32);
+      const bool live = p < end;
+      const int c = live ? run_cell(run, p) : 0;
+      const int d = cur.d;
+      const int slot = live ? c * 27 + d : -1;
+      const unsigned peers = __match_any_sync(0xffffffffu, slot);
+      if (live) {
+        const uint32_t o = cursor[warp][d][c] + __popc(peers & below);
+        orx[o] = cur.rx; ory[o] = cur.ry; orz[o] = cur.rz;
+        ou[o] = cur.u; ov[o] = cur.v; ow[o] = cur.w;
+        oq[o] = cur.q;
+        okey[o] = cur.key;
+        if (oid) oid[o] = cur.id;
+      }
+      __syncwarp();
+      if (live && lane == __ffs(peers) - 1) cursor[warp][d][c] += __popc(peers);
+      __syncwarp();
+      cur = nxt;
+    }
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_sort(int precision, const Geom& g, const tpicb200_particles* in,
+                        tpicb200_particles* out, uint32_t* counts, uint32_t* offsets,
+                        uint32_t* cursor, uint32_t* perm, uint32_t* scan_scratch,
+                        uint32_t* invalid, cudaStream_t s) {
+  out->count = in->count;
+  return enqueue_general(precision, g, in, out, counts, offsets, cursor, perm, scan_scratch, invalid, nullptr, s);
+}
+
+size_t binned_scratch_words(const Geom& g) {
+  const long long cells = (long long)g.nx * g.ny * g.nz;
+  return size_t(2 * g.bins + 1) + size_t(27 * cells) + 4;
+}
+
+bool binned_sort_applies(const Geom& g, uint32_t count, size_t max_particles) {
+  return g.nx >= 3 && g.ny >= 3 && g.nz >= 3 && count <= max_particles;
+}
+
+cudaError_t launch_sort_binned(int precision, const Geom& g, const tpicb200_particles* in,
+                               const uint32_t* in_counts, const uint32_t* in_offsets, tpicb200_particles* out,
+                               uint32_t* counts, uint32_t* offsets, uint32_t* cursor, uint32_t* perm,
+                               uint32_t* scan_scratch, uint32_t* binned_scratch, uint32_t* invalid,
+                               cudaStream_t s) {
+  const long long bins = g.bins;
+  const long long cells = (long long)g.nx * g.ny * g.nz;
+  const uint32_t n = in->count;
   out->count = n;
+  // Scratch: state (4 words, 8-byte aligned), old counts, old offsets, transfer.
+  BinnedState* state = reinterpret_cast<BinnedState*>(binned_scratch);
+  uint32_t* old_counts = binned_scratch + 4;
+  uint32_t* old_offsets = old_counts + bins;
+  uint32_t* transfer = old_offsets + bins + 1;
+  uint8_t* code = reinterpret_cast<uint8_t*>(perm);
+  cudaError_t e;
+  // The old bins are copied first: the new ones may overwrite them in place.
+  if ((e = cudaMemsetAsync(state, 0, sizeof(BinnedState), s)) != cudaSuccess) return e;
+  if ((e = cudaMemcpyAsync(old_counts, in_counts, size_t(bins) * 4, cudaMemcpyDeviceToDevice, s)) != cudaSuccess)
+    return e;
+  if ((e = cudaMemcpyAsync(old_offsets, in_offsets, size_t(bins + 1) * 4, cudaMemcpyDeviceToDevice, s)) !=
+      cudaSuccess)
+    return e;
+  // One warp per run of 32 cells.
+  const unsigned warps_grid = grid_for((cells + 31) / 32 * 32, kBinnedThreads, 148u * 8u);
+  classify_kernel<<<warps_grid, kBinnedThreads, 0, s>>>(g, in->cell, n, old_counts, old_offsets, transfer, code,
+                                                        state);
+  decide_kernel<<<1, 1, 0, s>>>(n, state);
+  count_launches(2);
+  // General sort, gated on the fallback flag.
+  if ((e = enqueue_general(precision, g, in, out, counts, offsets, cursor, perm, scan_scratch, invalid,
+                           &state->fallback, s)) != cudaSuccess)
+    return e;
+  // Binned steps 2-5, each returning at once on fallback.
+  binned_counts_kernel<<<grid_for(bins, 256, 148u * 16u), 256, 0, s>>>(g, transfer, counts, state);
+  const int nblocks = int((bins + kScanTile - 1) / kScanTile);
+  // The scan kernels take the fallback flag as their stop flag: they run only
+  // when it is clear.
+  ScanScratch sc{scan_scratch, scan_scratch + nblocks, scan_scratch + nblocks + 1, scan_scratch + nblocks + 2};
+  scan_reduce_kernel<<<nblocks, kScanThreads, 0, s>>>(counts, bins, sc.block_sums, &state->fallback, nullptr);
+  scan_block_sums_kernel<<<1, 1024, 0, s>>>(sc.block_sums, nblocks, &state->fallback, nullptr);
+  scan_down_kernel<<<nblocks, kScanThreads, 0, s>>>(counts, bins, sc.block_sums, offsets, &state->fallback, nullptr);
+  binned_bases_kernel<<<grid_for(cells, 256, 148u * 16u), 256, 0, s>>>(g, offsets, transfer, state);
+  if (precision == TPICB200_PRECISION_DOUBLE)
+    binned_scatter_kernel<double><<<warps_grid, kBinnedThreads, 0, s>>>(g, n, old_counts, old_offsets, transfer,
+        code, (const double*)in->rx, (const double*)in->ry, (const double*)in->rz, (const double*)in->u,
+        (const double*)in->v, (const double*)in->w, in->q, in->cell, in->id, (double*)out->rx, (double*)out->ry,
+        (double*)out->rz, (double*)out->u, (double*)out->v, (double*)out->w, out->q, out->cell,
+        in->id ? out->id : nullptr, state);
+  else
+    binned_scatter_kernel<float><<<warps_grid, kBinnedThreads, 0, s>>>(g, n, old_counts, old_offsets, transfer,
+        code, (const double*)in->rx, (const double*)in->ry, (const double*)in->rz, (const float*)in->u,
+        (const float*)in->v, (const float*)in->w, in->q, in->cell, in->id, (double*)out->rx, (double*)out->ry,
+        (double*)out->rz, (float*)out->u, (float*)out->v, (float*)out->w, out->q, out->cell,
+        in->id ? out->id : nullptr, state);
+  count_launches(6);
   return cudaGetLastError();
 }
 
