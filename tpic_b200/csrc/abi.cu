@@ -26,7 +26,7 @@ struct tpicb200_context {
   double* reduced = nullptr;     // energy reduction results
   double* pinned = nullptr;      // host mirror of `reduced` + invalid
   int energy_blocks = 0;
-  cudaEvent_t events[8]{};
+  cudaEvent_t events[6 + 2 * TPICB200_MAX_SPECIES]{};
   float* moments = nullptr;      // per-cell moments of the tensor-core forms (mixed precision)
   bool moments_pending = false;  // moments hold deposits not yet assembled
   // J and mass buffers zeroed by the last tpicb200_clear_moments that nothing
@@ -198,7 +198,7 @@ int tpicb200_mover(tpicb200_context* ctx, double qom, tpicb200_particles* p, con
   const double beta = qom * ctx->opt.dt / 2;
   if (!std::isfinite(beta)) return fail(TPICB200_OVERFLOW, "q/m*dt/2 is not finite");
   return cuda_status(launch_mover(ctx->opt.precision, ctx->g, qom, ctx->opt.dt, ctx->opt.c, p, e_theta,
-                                  b_node, invalid_or_own(ctx, invalid), (cudaStream_t)stream),
+                                  b_node, invalid_or_own(ctx, invalid), nullptr, (cudaStream_t)stream),
                      "mover launch failed");
 }
 
@@ -222,7 +222,7 @@ int tpicb200_sort_binned(tpicb200_context* ctx, const tpicb200_particles* in, co
                          uint32_t* offsets, uint32_t* invalid, tpicb200_stream stream) {
   if (int s = check_ctx(ctx)) return s;
   if (!in_counts || !in_offsets) return fail(TPICB200_INVALID_ARGUMENT, "binned sort needs the input's bins");
-  if (!binned_sort_applies(ctx->g, in ? in->count : 0, ctx->opt.max_particles))
+  if (!binned_sort_applies(ctx->g))
     return tpicb200_sort(ctx, in, out, counts, offsets, invalid, stream);
   if (int s = check_particles(ctx, in)) return s;
   if (!out || !counts || !offsets) return fail(TPICB200_INVALID_ARGUMENT, "sort needs output records and bins");
@@ -415,17 +415,13 @@ static int deposit_all(tpicb200_context* ctx, tpicb200_state* st, const void* b_
   return tpicb200_fold_periodic(ctx, st->j, st->mass, (tpicb200_stream)s);
 }
 
-// `binned`: the live slots are grouped by the state's bins (the cycle's
-// post-mover sort); otherwise (startup) the general sort runs.
-static int sort_all(tpicb200_context* ctx, tpicb200_state* st, bool binned, cudaStream_t s) {
+// Startup sort of every species' live slot into its idle slot.
+static int sort_all(tpicb200_context* ctx, tpicb200_state* st, cudaStream_t s) {
   for (int sp = 0; sp < st->ns; ++sp) {
     const int cur = st->current[sp];
     tpicb200_particles* in = &st->slot[sp][cur];
     tpicb200_particles* out = &st->slot[sp][1 - cur];
-    const int r = binned ? tpicb200_sort_binned(ctx, in, st->counts[sp], st->offsets[sp], out, st->counts[sp],
-                                                st->offsets[sp], nullptr, (tpicb200_stream)s)
-                         : tpicb200_sort(ctx, in, out, st->counts[sp], st->offsets[sp], nullptr, (tpicb200_stream)s);
-    if (r) return r;
+    if (int r = tpicb200_sort(ctx, in, out, st->counts[sp], st->offsets[sp], nullptr, (tpicb200_stream)s)) return r;
     st->current[sp] = 1 - cur;
   }
   return TPICB200_SUCCESS;
@@ -447,12 +443,56 @@ static int check_state(tpicb200_context* ctx, tpicb200_state* st) {
   return TPICB200_SUCCESS;
 }
 
+// The mover of species sp on its live slot, then the sort into the idle
+// slot; `moved` and `sorted` are recorded after each. On grids whose extents
+// are all at least 3 the mover emits direction codes and transfer counts and
+// the binned sort places the records by them; otherwise the general sort runs.
+static int move_and_sort(tpicb200_context* ctx, tpicb200_state* st, int sp, cudaEvent_t moved, cudaEvent_t sorted,
+                         cudaStream_t s) {
+  const int cur = st->current[sp];
+  tpicb200_particles* in = &st->slot[sp][cur];
+  tpicb200_particles* out = &st->slot[sp][1 - cur];
+  const double qom = st->qom[sp];
+  if (int r = check_particles(ctx, in)) return r;
+  if (!std::isfinite(qom) || !std::isfinite(qom * ctx->opt.dt / 2)) return fail(TPICB200_OVERFLOW, "q/m*dt/2 is not finite");
+  if (in->count && (!out->rx || !out->ry || !out->rz || !out->u || !out->v || !out->w || !out->q || !out->cell ||
+                    (in->id && !out->id)))
+    return fail(TPICB200_INVALID_ARGUMENT, "null attribute in the idle slot");
+  if (in->count && (in->rx == out->rx || in->cell == out->cell))
+    return fail(TPICB200_INVALID_ARGUMENT, "live and idle slots alias");
+  const int p = ctx->opt.precision;
+  if (!binned_sort_applies(ctx->g)) {
+    cudaError_t e = launch_mover(p, ctx->g, qom, ctx->opt.dt, ctx->opt.c, in, st->e_theta, st->b_node, ctx->invalid,
+                                 nullptr, s);
+    if (e == cudaSuccess) e = cudaEventRecord(moved, s);
+    if (e == cudaSuccess)
+      e = launch_sort(p, ctx->g, in, out, st->counts[sp], st->offsets[sp], ctx->cursor, ctx->perm, ctx->scan,
+                      ctx->invalid, s);
+    if (e == cudaSuccess) e = cudaEventRecord(sorted, s);
+    if (e != cudaSuccess) return cuda_status(e, "mover or sort launch failed");
+    st->current[sp] = 1 - cur;
+    return TPICB200_SUCCESS;
+  }
+  const BinnedScratch b = binned_scratch(ctx->g, ctx->binned, ctx->perm);
+  cudaError_t e = binned_begin(ctx->g, b, st->counts[sp], st->offsets[sp], true, s);
+  if (e == cudaSuccess)
+    e = launch_mover(p, ctx->g, qom, ctx->opt.dt, ctx->opt.c, in, st->e_theta, st->b_node, ctx->invalid, &b, s);
+  if (e == cudaSuccess) e = cudaEventRecord(moved, s);
+  if (e == cudaSuccess)
+    e = binned_finish(p, ctx->g, b, false, in, out, st->counts[sp], st->offsets[sp], ctx->cursor, ctx->perm,
+                      ctx->scan, ctx->invalid, s);
+  if (e == cudaSuccess) e = cudaEventRecord(sorted, s);
+  if (e != cudaSuccess) return cuda_status(e, "mover or binned sort launch failed");
+  st->current[sp] = 1 - cur;
+  return TPICB200_SUCCESS;
+}
+
 int tpicb200_prepare(tpicb200_context* ctx, tpicb200_state* st, tpicb200_stream stream) {
   if (int s = check_ctx(ctx)) return s;
   if (int r = check_state(ctx, st)) return r;
   cudaStream_t s = (cudaStream_t)stream;
   if (int r = tpicb200_magnetic_to_nodes(ctx, st->b_cell, st->b_node, stream)) return r;
-  if (int r = sort_all(ctx, st, false, s)) return r;
+  if (int r = sort_all(ctx, st, s)) return r;
   return deposit_all(ctx, st, st->b_node, s);
 }
 
@@ -471,6 +511,7 @@ int tpicb200_cycle(tpicb200_context* ctx, tpicb200_state* st, int ncycles, tpicb
   if (ncycles < 0) return fail(TPICB200_INVALID_ARGUMENT, "negative cycle count");
   cudaStream_t s = (cudaStream_t)stream;
   cudaEvent_t* ev = ctx->events;
+  cudaEvent_t* sev = ctx->events + 6;  // per species: after its mover, after its sort
   for (int cycle = 0; cycle < ncycles; ++cycle) {
     tpicb200_cycle_report report{};
     cudaEventRecord(ev[0], s);
@@ -478,20 +519,17 @@ int tpicb200_cycle(tpicb200_context* ctx, tpicb200_state* st, int ncycles, tpicb
     if (int r = tpicb200_field_solve(ctx, st->e, st->b_cell, st->j, st->mass, st->e_theta, &report.gmres, stream))
       return r;
     cudaEventRecord(ev[1], s);
-    // Movers gather the old B nodes and E_theta.
+    // Per species: the mover (gathering the old B nodes and E_theta), then the
+    // sort of the moved records into the idle slot.
     for (int sp = 0; sp < st->ns; ++sp)
-      if (int r = tpicb200_mover(ctx, st->qom[sp], &st->slot[sp][st->current[sp]], st->e_theta, st->b_node, nullptr,
-                                 stream))
-        return r;
+      if (int r = move_and_sort(ctx, st, sp, sev[2 * sp], sev[2 * sp + 1], s)) return r;
     cudaEventRecord(ev[2], s);
     if (int r = tpicb200_field_advance(ctx, st->e, st->b_cell, st->e_theta, st->b_cell_next, st->b_node_next, stream))
       return r;
     cudaEventRecord(ev[3], s);
-    if (int r = sort_all(ctx, st, true, s)) return r;
-    cudaEventRecord(ev[4], s);
     // Deposition of the moved records with the next B.
     if (int r = deposit_all(ctx, st, st->b_node_next, s)) return r;
-    cudaEventRecord(ev[5], s);
+    cudaEventRecord(ev[4], s);
     std::swap(st->b_cell, st->b_cell_next);
     std::swap(st->b_node, st->b_node_next);
     if (reports) {
@@ -507,11 +545,22 @@ int tpicb200_cycle(tpicb200_context* ctx, tpicb200_state* st, int ncycles, tpicb
         report.total_energy += out[2 + 5 * sp];
       }
     }
-    cudaEventRecord(ev[6], s);
+    cudaEventRecord(ev[5], s);
     uint32_t bad = 0;
     if (int r = read_invalid(ctx, s, &bad)) return r;
     if (bad) return fail(TPICB200_INVALID_DATA, "the cycle raised the invalid-data flag");
-    for (int k = 0; k < 6; ++k) cudaEventElapsedTime(&report.stage_ms[k], ev[k], ev[k + 1]);
+    // Stage times: solve, move, advance, sort, deposit, fold + diagnostics.
+    float t = 0.0f;
+    cudaEventElapsedTime(&report.stage_ms[0], ev[0], ev[1]);
+    for (int sp = 0; sp < st->ns; ++sp) {
+      cudaEventElapsedTime(&t, sp == 0 ? ev[1] : sev[2 * sp - 1], sev[2 * sp]);
+      report.stage_ms[1] += t;
+      cudaEventElapsedTime(&t, sev[2 * sp], sev[2 * sp + 1]);
+      report.stage_ms[3] += t;
+    }
+    cudaEventElapsedTime(&report.stage_ms[2], ev[2], ev[3]);
+    cudaEventElapsedTime(&report.stage_ms[4], ev[3], ev[4]);
+    cudaEventElapsedTime(&report.stage_ms[5], ev[4], ev[5]);
     if (reports) reports[cycle] = report;
   }
   return TPICB200_SUCCESS;

@@ -132,6 +132,23 @@ __device__ __forceinline__ int wrap_index(int i, int n) {
   return r < 0 ? r + n : r;
 }
 
+// Step d = to - from along a periodic axis of n >= 3 cells, folded to
+// -1 / +1 across the periodic face (other values are returned unchanged).
+__host__ __device__ __forceinline__ int periodic_step(int d, int n) {
+  if (d == n - 1) return -1;
+  if (d == 1 - n) return 1;
+  return d;
+}
+
+// Direction code (dx+1) + 3(dy+1) + 9(dz+1) < 27 of a move from cell
+// (i, j, k) to cell (a, b, c) of a periodic grid with every extent >= 3, or
+// -1 when the destination is not one of the 27 cells around the source.
+__device__ __forceinline__ int move_code(const Geom& g, int i, int j, int k, int a, int b, int c) {
+  const int dx = periodic_step(a - i, g.nx), dy = periodic_step(b - j, g.ny), dz = periodic_step(c - k, g.nz);
+  if (dx < -1 || dx > 1 || dy < -1 || dy > 1 || dz < -1 || dz > 1) return -1;
+  return (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1);
+}
+
 // The non-unique vertices of a node field: every vertex of the (n+3)^3 box
 // outside the unique periodic nodes [0, n)^3, enumerated as three z slabs
 // (k = -1, n, n+1), then three y slabs and three x slabs of the remainder.

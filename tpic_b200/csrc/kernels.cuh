@@ -9,9 +9,12 @@ namespace tpicb200 {
 void count_launches(unsigned n);
 
 // mover.cu
+struct BinnedScratch;
+// With `binned`, the mover also writes direction codes and transfer counts
+// for binned_finish (after binned_begin with zeroed transfer counts).
 cudaError_t launch_mover(int precision, const Geom& g, double qom, double dt, double c,
                          tpicb200_particles* p, const double* theta, const void* bnode,
-                         uint32_t* invalid, cudaStream_t s);
+                         uint32_t* invalid, const BinnedScratch* binned, cudaStream_t s);
 
 // sort.cu: scratch needs `bins` cursor words, `capacity` permutation words and
 // the scan workspace returned by sort_scan_words().
@@ -23,12 +26,35 @@ cudaError_t launch_sort(int precision, const Geom& g, const tpicb200_particles* 
 // Sort of records grouped by the bins (in_counts, in_offsets) of an earlier
 // sort, keys updated since: neighbour moves go through the transfer-count
 // path, anything else through the general sort (same stable order).
+struct BinnedState {
+  uint32_t fallback;         // nonzero: the general sort produces the output
+  uint32_t pad;
+  unsigned long long total;  // records in the old bins
+};
+struct BinnedScratch {
+  BinnedState* state;
+  uint32_t* old_counts;   // copy of the input's bins
+  uint32_t* old_offsets;
+  uint32_t* transfer;     // [27][interior cells]: counts, then output bases
+  uint8_t* code;          // direction code per record (0xff: not a neighbour move)
+};
 size_t binned_scratch_words(const Geom& g);
-bool binned_sort_applies(const Geom& g, uint32_t count, size_t max_particles);
+bool binned_sort_applies(const Geom& g);
+BinnedScratch binned_scratch(const Geom& g, uint32_t* words, uint32_t* perm);
+// Copies the input's bins and clears the state (and the transfer counts when
+// the mover will add into them).
+cudaError_t binned_begin(const Geom& g, const BinnedScratch& b, const uint32_t* in_counts,
+                         const uint32_t* in_offsets, bool zero_transfer, cudaStream_t s);
+// Validation, (classification when `classify`), counts, scan, bases, scatter
+// and the gated general sort.
+cudaError_t binned_finish(int precision, const Geom& g, const BinnedScratch& b, bool classify,
+                          const tpicb200_particles* in, tpicb200_particles* out, uint32_t* counts,
+                          uint32_t* offsets, uint32_t* cursor, uint32_t* perm, uint32_t* scan_scratch,
+                          uint32_t* invalid, cudaStream_t s);
 cudaError_t launch_sort_binned(int precision, const Geom& g, const tpicb200_particles* in,
                                const uint32_t* in_counts, const uint32_t* in_offsets, tpicb200_particles* out,
                                uint32_t* counts, uint32_t* offsets, uint32_t* cursor, uint32_t* perm,
-                               uint32_t* scan_scratch, uint32_t* binned_scratch, uint32_t* invalid,
+                               uint32_t* scan_scratch, uint32_t* binned_words, uint32_t* invalid,
                                cudaStream_t s);
 
 // deposit.cu

@@ -136,12 +136,13 @@ struct ScaledResponse {
   }
 };
 
-// Two values split into packed hi and lo bf16 pairs: hi = RN(v), lo = RN(v - hi).
-__device__ __forceinline__ void split_pair(float v0, float v1, uint32_t& hi, uint32_t& lo) {
-  const __nv_bfloat162 h = __floats2bfloat162_rn(v0, v1);
-  const float2 hf = __bfloat1622float2(h);
+// Two values split into packed hi and lo bf16 pairs: hi = RN(v), lo = RN(v - hi)
+// (v - hi is exact; the packed FMA v + (-1) hi evaluates both lanes at once).
+__device__ __forceinline__ void split_pair(float2 v, uint32_t& hi, uint32_t& lo) {
+  const __nv_bfloat162 h = __float22bfloat162_rn(v);
+  const float2 r = __ffma2_rn(__bfloat1622float2(h), make_float2(-1.0f, -1.0f), v);
   hi = *reinterpret_cast<const uint32_t*>(&h);
-  lo = pack_bf16(v0 - hf.x, v1 - hf.y);
+  lo = pack_bf16(r.x, r.y);
 }
 
 template <bool Bf16>
@@ -350,7 +351,7 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_deposit_kernel(Geom g, TcP
         for (int j = 0; j < 2; ++j) {
           uint32_t ph[4], pl[4];
 #pragma unroll
-          for (int e = 0; e < 4; ++e) split_pair(bv[8 * j + 2 * e], bv[8 * j + 2 * e + 1], ph[e], pl[e]);
+          for (int e = 0; e < 4; ++e) split_pair(make_float2(bv[8 * j + 2 * e], bv[8 * j + 2 * e + 1]), ph[e], pl[e]);
           const int off = (2 * warp + j) * 512 + (lane >> 3) * 128 + (lane & 7) * 16;
           *reinterpret_cast<uint4*>(sh.btile[buf][0] + off) = make_uint4(ph[0], ph[1], ph[2], ph[3]);
           *reinterpret_cast<uint4*>(sh.btile[buf][1] + off) = make_uint4(pl[0], pl[1], pl[2], pl[3]);
@@ -373,10 +374,12 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_deposit_kernel(Geom g, TcP
           for (int h = 0; h < 2; ++h) {
             const float4 xf = *reinterpret_cast<const float4*>(xrow + 8 * q8 + 4 * h);
             const float4 yzf = *reinterpret_cast<const float4*>(yzrow + 8 * q8 + 4 * h);
-            m[4 * h + 0] = tc::to_tf32(xf.x * yzf.x);
-            m[4 * h + 1] = tc::to_tf32(xf.y * yzf.y);
-            m[4 * h + 2] = tc::to_tf32(xf.z * yzf.z);
-            m[4 * h + 3] = tc::to_tf32(xf.w * yzf.w);
+            const float2 lo2 = __fmul2_rn(make_float2(xf.x, xf.y), make_float2(yzf.x, yzf.y));
+            const float2 hi2 = __fmul2_rn(make_float2(xf.z, xf.w), make_float2(yzf.z, yzf.w));
+            m[4 * h + 0] = tc::to_tf32(lo2.x);
+            m[4 * h + 1] = tc::to_tf32(lo2.y);
+            m[4 * h + 2] = tc::to_tf32(hi2.x);
+            m[4 * h + 3] = tc::to_tf32(hi2.y);
           }
           tc::tmem_st8(tmem + lane_base + (buf ? 32u : 0u) + 8 * q8, m);
         }
@@ -388,8 +391,8 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_deposit_kernel(Geom g, TcP
           for (int h = 0; h < 4; ++h) {
             const float4 xf = *reinterpret_cast<const float4*>(xrow + 16 * q16 + 4 * h);
             const float4 yzf = *reinterpret_cast<const float4*>(yzrow + 16 * q16 + 4 * h);
-            split_pair(xf.x * yzf.x, xf.y * yzf.y, mh[2 * h + 0], ml[2 * h + 0]);
-            split_pair(xf.z * yzf.z, xf.w * yzf.w, mh[2 * h + 1], ml[2 * h + 1]);
+            split_pair(__fmul2_rn(make_float2(xf.x, xf.y), make_float2(yzf.x, yzf.y)), mh[2 * h + 0], ml[2 * h + 0]);
+            split_pair(__fmul2_rn(make_float2(xf.z, xf.w), make_float2(yzf.z, yzf.w)), mh[2 * h + 1], ml[2 * h + 1]);
           }
           tc::tmem_st8(tmem + lane_base + (buf ? 32u : 0u) + 8 * q16, mh);
           tc::tmem_st8(tmem + lane_base + (buf ? 32u : 0u) + 16 + 8 * q16, ml);

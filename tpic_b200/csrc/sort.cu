@@ -395,68 +395,43 @@ cudaError_t enqueue_general(int precision, const Geom& g, const tpicb200_particl
 // one of the 27 cells around its old one. The stable order of a destination
 // bin is then: its source cells in increasing key order and, within one
 // source, the records in input order. So
-//   1. classify (warp per old interior cell): the direction d < 27 of every
-//      record (periodic wrap; nx, ny, nz >= 3 keep the 27 destinations
-//      distinct) and the transfer counts T[d][c]; any record that did not
-//      move to a neighbour, any invalid key, or old bins that are not a
-//      key-ordered partition of the records raise the fallback flag;
-//   2. counts (thread per bin): counts'[b] = sum_d T[d][b - d];
-//   3. scan of the counts;
-//   4. bases (thread per interior bin): walking the 27 sources of b in key
+//   1. direction codes d < 27 of every record and transfer counts T[d][c]
+//      per old interior cell c: from the mover itself (it knows both cells)
+//      or from classify_kernel (old cell from the bins, new from the key);
+//      periodic wrap, nx, ny, nz >= 3 keep the 27 destinations distinct;
+//   2. validation: the old bins must tile the records in key order;
+//   3. counts (thread per bin): counts'[b] = sum_d T[d][b - d];
+//   4. scan of the counts;
+//   5. bases (thread per interior bin): walking the 27 sources of b in key
 //      order, T[d][c] becomes the first output position of c's records that
 //      moved by d;
-//   5. scatter (warp per old interior cell): a record goes to its base plus
-//      its rank among the earlier records of its cell with the same d.
-// With the fallback flag raised, the general sort (enqueued between steps 1
-// and 2, gated on the flag) runs instead and steps 2-5 return at once; the
-// output is the same stable order either way.
+//   6. scatter (a warp per run of 32 old cells): a record goes to its base
+//      plus its rank among the earlier records of its cell with the same d,
+//      after checking that old cell + d is the cell of its key.
+// Any record that did not move to a neighbour, any invalid key, bins that do
+// not tile the records or a failed scatter check raise the fallback flag,
+// and the general sort, enqueued last and gated on the flag, rewrites the
+// whole output. The output is the same stable order either way.
 
 constexpr int kBinnedThreads = 256;
 constexpr int kBinnedWarps = kBinnedThreads / 32;
 
-struct BinnedState {
-  uint32_t fallback;
-  uint32_t pad;
-  unsigned long long total;  // records in the old bins
-};
-
-__device__ __forceinline__ int periodic_step(int d, int n) {
-  if (d == n - 1) return -1;
-  if (d == 1 - n) return 1;
-  return d;
-}
-
-// Direction code of a record of old interior cell (i, j, k) whose key is now
-// `key`, or -1 when the key is invalid or not one of the 27 neighbours.
-__device__ __forceinline__ int move_direction(const Geom& g, int i, int j, int k, int32_t key) {
-  if (key < 0 || key >= g.bins) return -1;
-  int a, b, c;
-  g.decode(key, a, b, c);
-  if (!g.interior_cell(a, b, c)) return -1;
-  const int dx = periodic_step(a - i, g.nx), dy = periodic_step(b - j, g.ny), dz = periodic_step(c - k, g.nz);
-  if (dx < -1 || dx > 1 || dy < -1 || dy > 1 || dz < -1 || dz > 1) return -1;
-  return (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1);
-}
-
 // A warp takes 32 consecutive old interior cells at a time. Their records
-// form one contiguous range (the bins between them are empty), streamed 32
-// at a time; each lane finds its record's cell by a binary search over the
-// 32 cell starts in shared memory.
+// form one contiguous range (the bins between them are empty); each lane
+// finds its record's cell by a binary search over the 32 cell starts.
 struct CellRun {
   uint32_t start[32];  // first record of each cell (ascending)
   uint32_t begin, end; // record range of the run
 };
 
-// Loads the run of cells u0 .. u0 + 31 (lane l: cell u0 + l) into `run`;
-// returns the lane's cell key (or -1 past the last cell).
-__device__ __forceinline__ int32_t load_run(const Geom& g, long long u0, long long cells,
-                                            const uint32_t* __restrict__ old_counts,
-                                            const uint32_t* __restrict__ old_offsets, CellRun& run, int& ci,
-                                            int& cj, int& ck) {
+// Loads the run of cells u0 .. u0 + 31 (lane l: cell u0 + l) into `run`.
+__device__ __forceinline__ void load_run(const Geom& g, long long u0, long long cells,
+                                         const uint32_t* __restrict__ old_counts,
+                                         const uint32_t* __restrict__ old_offsets, CellRun& run, int& ci, int& cj,
+                                         int& ck) {
   const int lane = threadIdx.x & 31;
   const long long u = u0 + lane;
   const bool valid = u < cells;
-  int32_t key = -1;
   uint32_t off = 0xffffffffu, stop = 0;
   ci = cj = ck = 0;
   if (valid) {
@@ -464,7 +439,7 @@ __device__ __forceinline__ int32_t load_run(const Geom& g, long long u0, long lo
     const long long r = u / g.nx;
     cj = int(r % g.ny);
     ck = int(r / g.ny);
-    key = g.encode(ci, cj, ck);
+    const int32_t key = g.encode(ci, cj, ck);
     off = old_offsets[key];
     stop = off + old_counts[key];
   }
@@ -478,7 +453,6 @@ __device__ __forceinline__ int32_t load_run(const Geom& g, long long u0, long lo
     run.end = end;
   }
   __syncwarp();
-  return key;
 }
 
 // Cell (lane index within the run) of record p: the last cell whose start is
@@ -491,19 +465,25 @@ __device__ __forceinline__ int run_cell(const CellRun& run, uint32_t p) {
   return c;
 }
 
-__global__ void __launch_bounds__(kBinnedThreads) classify_kernel(Geom g, const int32_t* __restrict__ keys,
-    uint32_t n, const uint32_t* __restrict__ old_counts, const uint32_t* __restrict__ old_offsets,
-    uint32_t* __restrict__ transfer, uint8_t* __restrict__ code, BinnedState* state) {
-  __shared__ CellRun runs[kBinnedWarps];
-  __shared__ int32_t coords[kBinnedWarps][3][32];  // (i, j, k) of each cell of the run
-  __shared__ uint32_t hist[kBinnedWarps][27][33];
-  __shared__ unsigned long long partial[kBinnedWarps];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const long long cells = (long long)g.nx * g.ny * g.nz;
+// Direction code of a record of old interior cell (i, j, k) whose key is now
+// `key`, or -1 when the key is invalid or not one of the 27 neighbours.
+__device__ __forceinline__ int key_move_code(const Geom& g, int i, int j, int k, int32_t key) {
+  if (key < 0 || key >= g.bins) return -1;
+  int a, b, c;
+  g.decode(key, a, b, c);
+  if (!g.interior_cell(a, b, c)) return -1;
+  return move_code(g, i, j, k, a, b, c);
+}
+
+// The old bins must tile the records in key order: disjoint ranges in
+// increasing key order, records only in interior cells, n records in all.
+__global__ void __launch_bounds__(256) validate_bins_kernel(Geom g, uint32_t n,
+                                                            const uint32_t* __restrict__ old_counts,
+                                                            const uint32_t* __restrict__ old_offsets,
+                                                            BinnedState* state) {
+  __shared__ unsigned long long partial[8];
   bool bad = false;
   unsigned long long total = 0;
-  // The old bins must tile the records in key order: disjoint ranges in
-  // increasing key order, records only in interior cells.
   for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < g.bins;
        b += (long long)gridDim.x * blockDim.x) {
     const uint32_t off = old_offsets[b], cnt = old_counts[b];
@@ -516,6 +496,30 @@ __global__ void __launch_bounds__(kBinnedThreads) classify_kernel(Geom g, const 
     total += cnt;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0 && old_offsets[g.bins] > n) bad = true;
+  total = warp_sum(total);
+  if ((threadIdx.x & 31) == 0) partial[threadIdx.x >> 5] = total;
+  const bool any_bad = __syncthreads_or(bad);
+  if (threadIdx.x == 0) {
+    unsigned long long block_total = 0;
+    for (int w = 0; w < 8; ++w) block_total += partial[w];
+    atomicAdd(&state->total, block_total);
+    if (any_bad) atomicExch(&state->fallback, 1u);
+  }
+}
+
+__global__ void decide_kernel(uint32_t n, BinnedState* state) {
+  if (state->total != (unsigned long long)n) state->fallback = 1;
+}
+
+__global__ void __launch_bounds__(kBinnedThreads) classify_kernel(Geom g, const int32_t* __restrict__ keys,
+    uint32_t n, const uint32_t* __restrict__ old_counts, const uint32_t* __restrict__ old_offsets,
+    uint32_t* __restrict__ transfer, uint8_t* __restrict__ code, BinnedState* state) {
+  __shared__ CellRun runs[kBinnedWarps];
+  __shared__ int32_t coords[kBinnedWarps][3][32];  // (i, j, k) of each cell of the run
+  __shared__ uint32_t hist[kBinnedWarps][27][33];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const long long cells = (long long)g.nx * g.ny * g.nz;
+  bool bad = false;
   CellRun& run = runs[warp];
   for (long long u0 = ((long long)blockIdx.x * kBinnedWarps + warp) * 32; u0 < cells;
        u0 += (long long)gridDim.x * kBinnedWarps * 32) {
@@ -548,7 +552,7 @@ __global__ void __launch_bounds__(kBinnedThreads) classify_kernel(Geom g, const 
         int c = 0, d = -1;
         if (live) {
           c = run_cell(run, p);
-          d = move_direction(g, coords[warp][0][c], coords[warp][1][c], coords[warp][2][c], key[m]);
+          d = key_move_code(g, coords[warp][0][c], coords[warp][1][c], coords[warp][2][c], key[m]);
           if (d < 0) bad = true;
           code[p] = uint8_t(d < 0 ? 0xff : d);
         }
@@ -563,19 +567,7 @@ __global__ void __launch_bounds__(kBinnedThreads) classify_kernel(Geom g, const 
       for (int d = 0; d < 27; ++d) transfer[(long long)d * cells + u0 + lane] = hist[warp][d][lane];
     __syncwarp();
   }
-  total = warp_sum(total);
-  if (lane == 0) partial[warp] = total;
-  const bool any_bad = __syncthreads_or(bad);
-  if (threadIdx.x == 0) {
-    unsigned long long block_total = 0;
-    for (int w = 0; w < kBinnedWarps; ++w) block_total += partial[w];
-    atomicAdd(&state->total, block_total);
-    if (any_bad) atomicExch(&state->fallback, 1u);
-  }
-}
-
-__global__ void decide_kernel(uint32_t n, BinnedState* state) {
-  if (state->total != (unsigned long long)n) state->fallback = 1;
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicExch(&state->fallback, 1u);
 }
 
 __global__ void __launch_bounds__(256) binned_counts_kernel(Geom g, const uint32_t* __restrict__ transfer,
@@ -662,18 +654,24 @@ __global__ void __launch_bounds__(kBinnedThreads) binned_scatter_kernel(Geom g, 
     const double* __restrict__ iq, const int32_t* __restrict__ ikey, const uint64_t* __restrict__ iid,
     double* __restrict__ orx, double* __restrict__ ory, double* __restrict__ orz,
     Vel* __restrict__ ou, Vel* __restrict__ ov, Vel* __restrict__ ow, double* __restrict__ oq,
-    int32_t* __restrict__ okey, uint64_t* __restrict__ oid, const BinnedState* state) {
+    int32_t* __restrict__ okey, uint64_t* __restrict__ oid, BinnedState* state) {
   __shared__ CellRun runs[kBinnedWarps];
+  __shared__ int32_t coords[kBinnedWarps][3][32];
   __shared__ uint32_t cursor[kBinnedWarps][27][33];
   if (state->fallback) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const long long cells = (long long)g.nx * g.ny * g.nz;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const long long cells = (long long)nx * ny * nz;
   const unsigned below = (1u << lane) - 1u;
+  bool bad = false;
   CellRun& run = runs[warp];
   for (long long u0 = ((long long)blockIdx.x * kBinnedWarps + warp) * 32; u0 < cells;
        u0 += (long long)gridDim.x * kBinnedWarps * 32) {
     int ci, cj, ck;
     load_run(g, u0, cells, old_counts, old_offsets, run, ci, cj, ck);
+    coords[warp][0][lane] = ci;
+    coords[warp][1][lane] = cj;
+    coords[warp][2][lane] = ck;
     if (u0 + lane < cells)
 #pragma unroll
       for (int d = 0; d < 27; ++d) cursor[warp][d][lane] = transfer[(long long)d * cells + u0 + lane];
@@ -704,18 +702,34 @@ __global__ void __launch_bounds__(kBinnedThreads) binned_scatter_kernel(Geom g, 
     for (uint32_t p0 = begin; p0 < end; p0 += 32) {
       const uint32_t p = p0 + lane;
       const Rec nxt = load(p + 32);
-      const bool live = p < end;
+      bool live = p < end;
       const int c = live ? run_cell(run, p) : 0;
       const int d = cur.d;
+      if (live) {
+        // The record must land in the cell of its key: old cell + d.
+        int a = coords[warp][0][c] + (d % 3) - 1, b = coords[warp][1][c] + (d / 3) % 3 - 1,
+            e = coords[warp][2][c] + d / 9 - 1;
+        a = a < 0 ? a + nx : (a >= nx ? a - nx : a);
+        b = b < 0 ? b + ny : (b >= ny ? b - ny : b);
+        e = e < 0 ? e + nz : (e >= nz ? e - nz : e);
+        if (d >= 27 || g.encode(a, b, e) != cur.key) {
+          bad = true;
+          live = false;
+        }
+      }
       const int slot = live ? c * 27 + d : -1;
       const unsigned peers = __match_any_sync(0xffffffffu, slot);
       if (live) {
         const uint32_t o = cursor[warp][d][c] + __popc(peers & below);
-        orx[o] = cur.rx; ory[o] = cur.ry; orz[o] = cur.rz;
-        ou[o] = cur.u; ov[o] = cur.v; ow[o] = cur.w;
-        oq[o] = cur.q;
-        okey[o] = cur.key;
-        if (oid) oid[o] = cur.id;
+        if (o < n) {
+          orx[o] = cur.rx; ory[o] = cur.ry; orz[o] = cur.rz;
+          ou[o] = cur.u; ov[o] = cur.v; ow[o] = cur.w;
+          oq[o] = cur.q;
+          okey[o] = cur.key;
+          if (oid) oid[o] = cur.id;
+        } else {
+          bad = true;
+        }
       }
       __syncwarp();
       if (live && lane == __ffs(peers) - 1) cursor[warp][d][c] += __popc(peers);
@@ -723,6 +737,7 @@ __global__ void __launch_bounds__(kBinnedThreads) binned_scatter_kernel(Geom g, 
       cur = nxt;
     }
   }
+  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicExch(&state->fallback, 1u);
 }
 
 }  // namespace
@@ -737,70 +752,92 @@ cudaError_t launch_sort(int precision, const Geom& g, const tpicb200_particles* 
 
 size_t binned_scratch_words(const Geom& g) {
   const long long cells = (long long)g.nx * g.ny * g.nz;
-  return size_t(2 * g.bins + 1) + size_t(27 * cells) + 4;
+  return 4 + size_t(2 * g.bins + 1) + size_t(27 * cells);
 }
 
-bool binned_sort_applies(const Geom& g, uint32_t count, size_t max_particles) {
-  return g.nx >= 3 && g.ny >= 3 && g.nz >= 3 && count <= max_particles;
+bool binned_sort_applies(const Geom& g) { return g.nx >= 3 && g.ny >= 3 && g.nz >= 3; }
+
+BinnedScratch binned_scratch(const Geom& g, uint32_t* words, uint32_t* perm) {
+  BinnedScratch b;
+  b.state = reinterpret_cast<BinnedState*>(words);  // 4 words, 8-byte aligned
+  b.old_counts = words + 4;
+  b.old_offsets = b.old_counts + g.bins;
+  b.transfer = b.old_offsets + g.bins + 1;
+  b.code = reinterpret_cast<uint8_t*>(perm);
+  return b;
+}
+
+cudaError_t binned_begin(const Geom& g, const BinnedScratch& b, const uint32_t* in_counts,
+                         const uint32_t* in_offsets, bool zero_transfer, cudaStream_t s) {
+  // The old bins are copied first: the new ones may overwrite them in place.
+  cudaError_t e;
+  if ((e = cudaMemsetAsync(b.state, 0, sizeof(BinnedState), s)) != cudaSuccess) return e;
+  if ((e = cudaMemcpyAsync(b.old_counts, in_counts, size_t(g.bins) * 4, cudaMemcpyDeviceToDevice, s)) !=
+      cudaSuccess)
+    return e;
+  if ((e = cudaMemcpyAsync(b.old_offsets, in_offsets, size_t(g.bins + 1) * 4, cudaMemcpyDeviceToDevice, s)) !=
+      cudaSuccess)
+    return e;
+  if (zero_transfer)
+    e = cudaMemsetAsync(b.transfer, 0, size_t(27) * size_t((long long)g.nx * g.ny * g.nz) * 4, s);
+  return e;
+}
+
+cudaError_t binned_finish(int precision, const Geom& g, const BinnedScratch& b, bool classify,
+                          const tpicb200_particles* in, tpicb200_particles* out, uint32_t* counts,
+                          uint32_t* offsets, uint32_t* cursor, uint32_t* perm, uint32_t* scan_scratch,
+                          uint32_t* invalid, cudaStream_t s) {
+  const long long bins = g.bins;
+  const long long cells = (long long)g.nx * g.ny * g.nz;
+  const uint32_t n = in->count;
+  out->count = n;
+  // One warp per run of 32 cells.
+  const unsigned runs_grid = grid_for((cells + 31) / 32 * 32, kBinnedThreads, 148u * 8u);
+  validate_bins_kernel<<<grid_for(bins, 256, 148u * 8u), 256, 0, s>>>(g, n, b.old_counts, b.old_offsets, b.state);
+  decide_kernel<<<1, 1, 0, s>>>(n, b.state);
+  int launches = 2;
+  if (classify) {
+    classify_kernel<<<runs_grid, kBinnedThreads, 0, s>>>(g, in->cell, n, b.old_counts, b.old_offsets, b.transfer,
+                                                        b.code, b.state);
+    ++launches;
+  }
+  binned_counts_kernel<<<grid_for(bins, 256, 148u * 16u), 256, 0, s>>>(g, b.transfer, counts, b.state);
+  const int nblocks = int((bins + kScanTile - 1) / kScanTile);
+  // The scan kernels take the fallback flag as their stop flag: they run only
+  // when it is clear.
+  ScanScratch sc{scan_scratch, scan_scratch + nblocks, scan_scratch + nblocks + 1, scan_scratch + nblocks + 2};
+  scan_reduce_kernel<<<nblocks, kScanThreads, 0, s>>>(counts, bins, sc.block_sums, &b.state->fallback, nullptr);
+  scan_block_sums_kernel<<<1, 1024, 0, s>>>(sc.block_sums, nblocks, &b.state->fallback, nullptr);
+  scan_down_kernel<<<nblocks, kScanThreads, 0, s>>>(counts, bins, sc.block_sums, offsets, &b.state->fallback,
+                                                    nullptr);
+  binned_bases_kernel<<<grid_for(cells, 256, 148u * 16u), 256, 0, s>>>(g, offsets, b.transfer, b.state);
+  if (precision == TPICB200_PRECISION_DOUBLE)
+    binned_scatter_kernel<double><<<runs_grid, kBinnedThreads, 0, s>>>(g, n, b.old_counts, b.old_offsets,
+        b.transfer, b.code, (const double*)in->rx, (const double*)in->ry, (const double*)in->rz,
+        (const double*)in->u, (const double*)in->v, (const double*)in->w, in->q, in->cell, in->id,
+        (double*)out->rx, (double*)out->ry, (double*)out->rz, (double*)out->u, (double*)out->v, (double*)out->w,
+        out->q, out->cell, in->id ? out->id : nullptr, b.state);
+  else
+    binned_scatter_kernel<float><<<runs_grid, kBinnedThreads, 0, s>>>(g, n, b.old_counts, b.old_offsets,
+        b.transfer, b.code, (const double*)in->rx, (const double*)in->ry, (const double*)in->rz,
+        (const float*)in->u, (const float*)in->v, (const float*)in->w, in->q, in->cell, in->id,
+        (double*)out->rx, (double*)out->ry, (double*)out->rz, (float*)out->u, (float*)out->v, (float*)out->w,
+        out->q, out->cell, in->id ? out->id : nullptr, b.state);
+  count_launches(launches + 6);
+  if (cudaError_t e = cudaGetLastError(); e != cudaSuccess) return e;
+  // General sort, gated on the fallback flag: it rewrites every output.
+  return enqueue_general(precision, g, in, out, counts, offsets, cursor, perm, scan_scratch, invalid,
+                         &b.state->fallback, s);
 }
 
 cudaError_t launch_sort_binned(int precision, const Geom& g, const tpicb200_particles* in,
                                const uint32_t* in_counts, const uint32_t* in_offsets, tpicb200_particles* out,
                                uint32_t* counts, uint32_t* offsets, uint32_t* cursor, uint32_t* perm,
-                               uint32_t* scan_scratch, uint32_t* binned_scratch, uint32_t* invalid,
+                               uint32_t* scan_scratch, uint32_t* binned_words, uint32_t* invalid,
                                cudaStream_t s) {
-  const long long bins = g.bins;
-  const long long cells = (long long)g.nx * g.ny * g.nz;
-  const uint32_t n = in->count;
-  out->count = n;
-  // Scratch: state (4 words, 8-byte aligned), old counts, old offsets, transfer.
-  BinnedState* state = reinterpret_cast<BinnedState*>(binned_scratch);
-  uint32_t* old_counts = binned_scratch + 4;
-  uint32_t* old_offsets = old_counts + bins;
-  uint32_t* transfer = old_offsets + bins + 1;
-  uint8_t* code = reinterpret_cast<uint8_t*>(perm);
-  cudaError_t e;
-  // The old bins are copied first: the new ones may overwrite them in place.
-  if ((e = cudaMemsetAsync(state, 0, sizeof(BinnedState), s)) != cudaSuccess) return e;
-  if ((e = cudaMemcpyAsync(old_counts, in_counts, size_t(bins) * 4, cudaMemcpyDeviceToDevice, s)) != cudaSuccess)
-    return e;
-  if ((e = cudaMemcpyAsync(old_offsets, in_offsets, size_t(bins + 1) * 4, cudaMemcpyDeviceToDevice, s)) !=
-      cudaSuccess)
-    return e;
-  // One warp per run of 32 cells.
-  const unsigned warps_grid = grid_for((cells + 31) / 32 * 32, kBinnedThreads, 148u * 8u);
-  classify_kernel<<<warps_grid, kBinnedThreads, 0, s>>>(g, in->cell, n, old_counts, old_offsets, transfer, code,
-                                                        state);
-  decide_kernel<<<1, 1, 0, s>>>(n, state);
-  count_launches(2);
-  // General sort, gated on the fallback flag.
-  if ((e = enqueue_general(precision, g, in, out, counts, offsets, cursor, perm, scan_scratch, invalid,
-                           &state->fallback, s)) != cudaSuccess)
-    return e;
-  // Binned steps 2-5, each returning at once on fallback.
-  binned_counts_kernel<<<grid_for(bins, 256, 148u * 16u), 256, 0, s>>>(g, transfer, counts, state);
-  const int nblocks = int((bins + kScanTile - 1) / kScanTile);
-  // The scan kernels take the fallback flag as their stop flag: they run only
-  // when it is clear.
-  ScanScratch sc{scan_scratch, scan_scratch + nblocks, scan_scratch + nblocks + 1, scan_scratch + nblocks + 2};
-  scan_reduce_kernel<<<nblocks, kScanThreads, 0, s>>>(counts, bins, sc.block_sums, &state->fallback, nullptr);
-  scan_block_sums_kernel<<<1, 1024, 0, s>>>(sc.block_sums, nblocks, &state->fallback, nullptr);
-  scan_down_kernel<<<nblocks, kScanThreads, 0, s>>>(counts, bins, sc.block_sums, offsets, &state->fallback, nullptr);
-  binned_bases_kernel<<<grid_for(cells, 256, 148u * 16u), 256, 0, s>>>(g, offsets, transfer, state);
-  if (precision == TPICB200_PRECISION_DOUBLE)
-    binned_scatter_kernel<double><<<warps_grid, kBinnedThreads, 0, s>>>(g, n, old_counts, old_offsets, transfer,
-        code, (const double*)in->rx, (const double*)in->ry, (const double*)in->rz, (const double*)in->u,
-        (const double*)in->v, (const double*)in->w, in->q, in->cell, in->id, (double*)out->rx, (double*)out->ry,
-        (double*)out->rz, (double*)out->u, (double*)out->v, (double*)out->w, out->q, out->cell,
-        in->id ? out->id : nullptr, state);
-  else
-    binned_scatter_kernel<float><<<warps_grid, kBinnedThreads, 0, s>>>(g, n, old_counts, old_offsets, transfer,
-        code, (const double*)in->rx, (const double*)in->ry, (const double*)in->rz, (const float*)in->u,
-        (const float*)in->v, (const float*)in->w, in->q, in->cell, in->id, (double*)out->rx, (double*)out->ry,
-        (double*)out->rz, (float*)out->u, (float*)out->v, (float*)out->w, out->q, out->cell,
-        in->id ? out->id : nullptr, state);
-  count_launches(6);
-  return cudaGetLastError();
+  const BinnedScratch b = binned_scratch(g, binned_words, perm);
+  if (cudaError_t e = binned_begin(g, b, in_counts, in_offsets, false, s); e != cudaSuccess) return e;
+  return binned_finish(precision, g, b, true, in, out, counts, offsets, cursor, perm, scan_scratch, invalid, s);
 }
 
 }  // namespace tpicb200
