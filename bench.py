@@ -130,7 +130,7 @@ def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    cores = os.cpu_count() or 1
+    cores = args.cpu_workers or os.cpu_count() or 1
     scale = args.cpu_scale
     ctx = mp.get_context("spawn")
     t0 = time.perf_counter()
@@ -151,6 +151,21 @@ def run_reference(args) -> None:
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "wall_s": wall}
     print(json.dumps(line), flush=True)
+
+
+def max_over_ranks(seconds: float, dist, device) -> float:
+    """The slowest rank's time (every rank takes part; a no-op on one rank)."""
+    if dist is None:
+        return seconds
+    import torch
+    t = torch.tensor([seconds], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(world: int, particles: int, steps: int, seconds: float) -> float:
+    """Whole-job particles*cycles/s of `world` replicas timed as the slowest."""
+    return world * particles * steps / seconds
 
 
 def run_gpu(args) -> None:
@@ -197,12 +212,8 @@ def run_gpu(args) -> None:
         stop.record(stream)
         barrier()
     launches = lib.tpicb200_launch_count() - launches0
-    seconds = start.elapsed_time(stop) / 1e3
-    if dist is not None:
-        t = torch.tensor([seconds], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        seconds = float(t.item())
-    value = world * nparticles * args.steps / seconds
+    seconds = max_over_ranks(start.elapsed_time(stop) / 1e3, dist, "cuda")
+    value = replica_rate(world, nparticles, args.steps, seconds)
     drift = max(abs(r.total_energy - total0) / abs(total0) for r in reports)
     stage_names = ["solve", "move", "advance", "sort", "deposit", "fold_diagnostics"]
     stages = {name: float(np.mean([r.stage_ms[k] for r in reports])) for k, name in enumerate(stage_names)}
@@ -361,13 +372,9 @@ def end_to_end(sim, args, stream, barrier, nparticles, world, dist) -> dict:
     reports = sim.run(steps)  # energy scalars read back to the host every cycle
     stop.record(stream)
     barrier()
-    seconds = start.elapsed_time(stop) / 1e3
-    if dist is not None:
-        t = torch.tensor([seconds], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        seconds = float(t.item())
+    seconds = max_over_ranks(start.elapsed_time(stop) / 1e3, dist, "cuda")
     d2h = (2 + 5 * sim.state.ns) * 8 + 4
-    return {"value": world * nparticles * steps / seconds, "unit": UNIT,
+    return {"value": replica_rate(world, nparticles, steps, seconds), "unit": UNIT,
             "h2d_bytes_per_step": int(h2d / steps), "d2h_bytes_per_step": d2h,
             "seconds": seconds, "cycles": len(reports)}
 
@@ -383,6 +390,7 @@ def main():
     ap.add_argument("--scale", type=int, default=128, help="cells per axis of the workload")
     ap.add_argument("--cpu-scale", type=int, default=24, help="cells per axis of the CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-workers", type=int, default=0, help="host processes of the reference arm (0: all cores)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("at least 3 warm-up steps")

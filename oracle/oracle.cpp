@@ -445,6 +445,9 @@ long oracle_node_count(const oracle_grid* g) { return Layout(to_grid(g)).nodes; 
 long oracle_cell_count(const oracle_grid* g) { return Layout(to_grid(g)).cells; }
 long oracle_bin_count(const oracle_grid* g) { return Layout(to_grid(g)).bins; }
 int oracle_pair_stencil(int a, int b) { return pair_stencil(a, b); }
+void oracle_stencil_offset(int s, int* out) {
+  out[0] = kStencil[s][0]; out[1] = kStencil[s][1]; out[2] = kStencil[s][2];
+}
 
 void oracle_cic_weights_f64(double x, double y, double z, double* w) { cic<double>(x, y, z, w); }
 void oracle_cic_weights_f32(float x, float y, float z, float* w) { cic<float>(x, y, z, w); }

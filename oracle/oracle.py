@@ -69,6 +69,7 @@ def load():
                                              vp, vp]
         lib.oracle_field_energy.argtypes = [C.POINTER(OGrid), vp, vp, vp]
         lib.oracle_species_scalars.argtypes = [C.c_int, C.c_double, vp, vp, vp, vp, C.c_long, vp]
+        lib.oracle_stencil_offset.argtypes = [C.c_int, vp]
         lib.oracle_pair_stencil.restype = C.c_int
         lib.oracle_pair_stencil.argtypes = [C.c_int, C.c_int]
         lib.oracle_cic_weights_f64.argtypes = [C.c_double, C.c_double, C.c_double, vp]

@@ -10,7 +10,8 @@ import numpy as np
 import pytest
 
 from tpic_b200.plasma import GridSpec
-from test_gpu_stages import make_ctx, oracle_sort
+from reference_fixtures import oracle_sort
+from test_gpu_stages import make_ctx
 
 pytestmark = pytest.mark.gpu
 
