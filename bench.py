@@ -13,6 +13,12 @@ current + mass deposition, fold, commit, energy diagnostics) through the C
 ABI's tpicb200_cycle. Inputs stay resident in HBM (13 GB of particle
 records per slot, far larger than the 126 MB L2).
 
+The headline form (--mass-matrix, default the BF16x3 tensor-core assembly)
+and the comparison form (--compare, default the plain FP32 CUDA-core
+assembly) are each timed on the same workload; each runs --drift-cycles
+cycles (default 100) from the same initial state for its relative energy
+drift. The line reports both and their ratio ("plain_fp32_form").
+
   python bench.py [--gpus N --steps K --warmup W] [--mass-matrix scalar|scalar-f64|tf32|bf16x3]
   python bench.py --impl reference ...   (the CPU implementation of the path)
 
@@ -69,15 +75,18 @@ class ClockSampler:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, index: int):
+    def __init__(self, index: int, enabled: bool = True):
         self.index = index
+        self.enabled = enabled
         self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         self.proc = None
 
     def __enter__(self):
+        if not self.enabled:
+            return self
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.file,
+                                          "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.file,
                                          stderr=subprocess.DEVNULL)
         except FileNotFoundError:
             self.proc = None
@@ -184,40 +193,52 @@ def run_gpu(args) -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
 
     case = workload(args.scale, 4)
-    t_gen = time.perf_counter()
-    sim = Simulation(case, precision=args.precision, mass_kind=args.mass_matrix, device=local,
-                     generate_on_device=True)
-    gen_s = time.perf_counter() - t_gen
     nparticles = sum(case.grid.cells * sp.ppc for sp in case.species)
     stream = torch.cuda.current_stream()
-    lib = sim.lib
-
-    sim.prepare()
-    w0 = sim.energy()
-    total0 = w0[0] + w0[1] + sum(w0[2 + 5 * s] for s in range(len(case.species)))
-    warm = sim.run(args.warmup)
 
     def barrier():
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize()
 
-    # ---- device-resident timing -------------------------------------------------
-    launches0 = lib.tpicb200_launch_count()
-    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    barrier()
-    with ClockSampler(local) as clocks:
-        start.record(stream)
-        reports = sim.run(args.steps)
-        stop.record(stream)
+    def timed_form(mass_kind, sample_clocks):
+        """Warm-up, the timed cycles, then more cycles up to --drift-cycles for
+        the energy drift (the simulation stays open for the caller)."""
+        t_gen = time.perf_counter()
+        sim = Simulation(case, precision=args.precision, mass_kind=mass_kind, device=local, generate_on_device=True)
+        gen_s = time.perf_counter() - t_gen
+        sim.prepare()
+        w0 = sim.energy()
+        total0 = w0[0] + w0[1] + sum(w0[2 + 5 * s] for s in range(len(case.species)))
+        history = sim.run(args.warmup)
+        launches0 = sim.lib.tpicb200_launch_count()
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         barrier()
-    launches = lib.tpicb200_launch_count() - launches0
-    seconds = max_over_ranks(start.elapsed_time(stop) / 1e3, dist, "cuda")
-    value = replica_rate(world, nparticles, args.steps, seconds)
-    drift = max(abs(r.total_energy - total0) / abs(total0) for r in reports)
-    stage_names = ["solve", "move", "advance", "sort", "deposit", "fold_diagnostics"]
-    stages = {name: float(np.mean([r.stage_ms[k] for r in reports])) for k, name in enumerate(stage_names)}
-    gmres_it = float(np.mean([r.gmres_iterations for r in reports]))
+        with ClockSampler(local, enabled=sample_clocks) as clocks:
+            start.record(stream)
+            reports = sim.run(args.steps)
+            stop.record(stream)
+            barrier()
+        launches = sim.lib.tpicb200_launch_count() - launches0
+        seconds = max_over_ranks(start.elapsed_time(stop) / 1e3, dist, "cuda")
+        history += reports
+        if len(history) < args.drift_cycles:
+            history += sim.run(args.drift_cycles - len(history))
+        drift = max(abs(r.total_energy - total0) / abs(total0) for r in history)
+        stage_names = ["solve", "move", "advance", "sort", "deposit", "fold_diagnostics"]
+        result = {"value": replica_rate(world, nparticles, args.steps, seconds),
+                  "ms_per_step": 1e3 * seconds / args.steps,
+                  "energy_drift": {"cycles": len(history), "max_relative": drift},
+                  "stages_ms": {name: float(np.mean([r.stage_ms[k] for r in reports]))
+                                for k, name in enumerate(stage_names)},
+                  "gmres_iterations": float(np.mean([r.gmres_iterations for r in reports])),
+                  "launches": int(launches), "generation_s": gen_s}
+        return sim, result, clocks
+
+    sim, headline, clocks = timed_form(args.mass_matrix, True)
+    value = headline["value"]
+    seconds = headline["ms_per_step"] * args.steps / 1e3
+    lib = sim.lib
 
     # ---- dominant-kernel roofline: per-stage kernels timed alone -----------------
     kernels = stage_kernel_times(sim, args, stream)
@@ -225,7 +246,7 @@ def run_gpu(args) -> None:
     dominant = max(kernels, key=lambda k: kernels[k]["ms"])
     dk = kernels[dominant]
     achieved = dk["bytes"] / (dk["ms"] / 1e3) / 1e9
-    traffic = load_traffic(dominant)
+    traffic = load_traffic(dominant, nparticles)
     roofline = {"kernel": dominant, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "peak_source": peak_kind,
                 "traffic": traffic, "algorithmic_bytes": dk["bytes"],
@@ -234,11 +255,21 @@ def run_gpu(args) -> None:
 
     # ---- end to end through the public API with host buffers -----------------------
     e2e = end_to_end(sim, args, stream, barrier, nparticles, world, dist)
-
     sim.close()
+    del sim
+
+    # ---- the plain FP32 CUDA-core form on the same workload -------------------------
+    comparison = None
+    if args.compare != "none":
+        other, plain, _ = timed_form(args.compare, False)
+        other.close()
+        del other
+        comparison = {"mass_matrix": args.compare, **plain,
+                      "speedup": value / plain["value"]}
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": 1e3 * seconds / args.steps, "higher_is_better": True,
+                "warmup": args.warmup, "ms_per_step": headline["ms_per_step"], "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32" if args.precision == "mixed" else "f64", "data": "synthetic",
                 "config": {"workload": f"3-D uniform thermal plasma, {args.scale}^3 cells, box 20^3 d_i, "
@@ -246,9 +277,10 @@ def run_gpu(args) -> None:
                            "precision": args.precision, "mass_matrix": args.mass_matrix, "dt": case.dt,
                            "theta": case.theta, "gmres_tol": case.gmres_tol, "l2": "inputs larger than L2",
                            "parallelism": f"replicas x{world}"},
-                "energy_drift": drift, "gmres_iterations": gmres_it, "stages_ms": stages,
-                "clocks": clocks.summary(), "e2e": e2e, "gpu_launches": int(launches),
-                "roofline": roofline, "generation_s": gen_s}
+                "energy_drift": headline["energy_drift"], "gmres_iterations": headline["gmres_iterations"],
+                "stages_ms": headline["stages_ms"], "plain_fp32_form": comparison,
+                "clocks": clocks.summary(), "e2e": e2e, "gpu_launches": headline["launches"],
+                "roofline": roofline, "generation_s": headline["generation_s"]}
         if not args.no_cpu_baseline:
             cb = cpu_oracle_rate(args.cpu_scale, 4, 2, 0)
             line["cpu_baseline"] = {"value": cb["particles"] * cb["cycles"] / cb["seconds"], "unit": UNIT,
@@ -337,11 +369,14 @@ def stage_kernel_times(sim, args, stream, repeats: int = 5) -> dict:
     return out
 
 
-def load_traffic(kernel: str):
-    """DRAM bytes per launch from the committed ncu capture summary, if any."""
+def load_traffic(stage: str, particles: int):
+    """DRAM bytes of one launch of a stage at this workload, from the committed
+    ncu capture summary (bytes per particle at the workload's loading of 128
+    particles per cell, captured on a smaller grid of the same loading), if any."""
     path = ROOT / "profiles" / "traffic.json"
     try:
-        return json.loads(path.read_text()).get(kernel)
+        entry = json.loads(path.read_text())[stage]
+        return entry["dram_bytes_per_particle"] * particles
     except Exception:
         return None
 
@@ -385,7 +420,10 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["tpic_b200", "reference"], default="tpic_b200")
-    ap.add_argument("--mass-matrix", default="scalar", choices=["scalar", "scalar-f64", "tf32", "bf16x3"])
+    ap.add_argument("--mass-matrix", default="bf16x3", choices=["scalar", "scalar-f64", "tf32", "bf16x3"])
+    ap.add_argument("--compare", default="scalar", choices=["scalar", "scalar-f64", "tf32", "bf16x3", "none"],
+                    help="second form timed on the same workload (default: the plain FP32 CUDA-core form)")
+    ap.add_argument("--drift-cycles", type=int, default=100, help="cycles of the energy-drift run of each form")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "double"])
     ap.add_argument("--scale", type=int, default=128, help="cells per axis of the workload")
     ap.add_argument("--cpu-scale", type=int, default=24, help="cells per axis of the CPU sample")

@@ -4,7 +4,7 @@
  * TPIC exposes its hot path as stream-ordered C++ template "enqueue"
  * functions that take LPFx owners, an executor (CUDA stream) and an
  * `unsigned* invalid` device flag, return an lpfx::ErrorCode, allocate
- * nothing and never synchronise (SURVEY boundary; e.g.
+ * nothing and never synchronise (e.g.
  * include/tpic/ecsim/deposition/current_deposition_device.hpp:285-313).
  * The reference promises no binary ABI (docs/developer/architecture.md:459-460),
  * so this header is the plain-C form of those entry points: caller-owned
@@ -195,8 +195,8 @@ int tpicb200_mover(tpicb200_context* ctx, double qom, tpicb200_particles* p,
  * Replaces FullParticleSort::enqueue (ecsim/particles/particle_sort_device.hpp:132-145)
  * whose device sort is unstable within a bin; this one is bit-exact against
  * the stable host sort (lpfx/algorithm/particle/host/sort.hpp:205-290).
- * in and out must not alias; an out-of-range key increments *invalid and the
- * call returns TPICB200_INVALID_DATA after synchronising. */
+ * in and out must not alias; an out-of-range key stops the sort on the
+ * device (no record is written) and increments *invalid. */
 int tpicb200_sort(tpicb200_context* ctx, const tpicb200_particles* in, tpicb200_particles* out,
                   uint32_t* counts, uint32_t* offsets, uint32_t* invalid,
                   tpicb200_stream stream);
@@ -300,9 +300,12 @@ int tpicb200_energy(tpicb200_context* ctx, const void* e, const void* b_cell,
  * (docs/developer/architecture.md:161-171). */
 int tpicb200_prepare(tpicb200_context* ctx, tpicb200_state* state, tpicb200_stream stream);
 
-/* ncycles ECSIM cycles: solve, move (old B), field advance, sort, deposit
- * (next B), fold, commit; reports (may be NULL) receive one entry per cycle
- * with the energies of the committed state. Host-blocking. */
+/* ncycles ECSIM cycles: solve; per species the mover (old B) and the sort
+ * of the moved records (the mover emits the direction codes the binned sort
+ * places records by, see tpicb200_sort_binned); field advance; deposition
+ * of every species (next B); fold; commit. reports (may be NULL) receive one
+ * entry per cycle with the energies of the committed state. Host-blocking;
+ * returns TPICB200_INVALID_DATA when a cycle raised the invalid flag. */
 int tpicb200_cycle(tpicb200_context* ctx, tpicb200_state* state, int ncycles,
                    tpicb200_cycle_report* reports, tpicb200_stream stream);
 
