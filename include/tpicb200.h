@@ -218,6 +218,30 @@ int tpicb200_sort_binned(tpicb200_context* ctx, const tpicb200_particles* in, co
                          const uint32_t* in_offsets, tpicb200_particles* out, uint32_t* counts,
                          uint32_t* offsets, uint32_t* invalid, tpicb200_stream stream);
 
+/* Capacity of tpicb200_sort_static: records per call and halo-2 bins
+ * ((nx+4)(ny+4)(nz+4)) of the grid. */
+#define TPICB200_SORT_STATIC_MAX_RECORDS 1048576
+#define TPICB200_SORT_STATIC_MAX_BINS 1048576
+
+/* The stable counting sort of tpicb200_sort (same output, counts, offsets
+ * and invalid-key behaviour) without a context and without allocating
+ * anything: its scratch (permutation, cursors, scan sums; 12.6 MB) is one
+ * fixed device array of the library. No counterpart in the reference: it
+ * serves callers that cannot allocate device memory for a sort (no context,
+ * memory held by another allocator's pool, or a loop that must not pay an
+ * allocation's implicit device synchronisation). Limits: at most
+ * TPICB200_SORT_STATIC_MAX_RECORDS records on grids of at most
+ * TPICB200_SORT_STATIC_MAX_BINS bins; larger inputs return
+ * TPICB200_CAPACITY_EXCEEDED and enqueue nothing. The first call on each
+ * device (with that device current) resolves the array's address; make that
+ * call before any stream capture. Every call shares the one array: calls
+ * that overlap in time (on other streams or host threads) race on it and
+ * must be ordered on one stream. precision: TPICB200_PRECISION_* (the
+ * velocity type of the records). */
+int tpicb200_sort_static(const tpicb200_grid* grid, int precision, const tpicb200_particles* in,
+                         tpicb200_particles* out, uint32_t* counts, uint32_t* offsets, uint32_t* invalid,
+                         tpicb200_stream stream);
+
 /* Zero J (node field) and the mass records. Replaces enqueue_clear_mass_matrix
  * (ecsim/mass_matrix/mass_matrix_deposition_device.hpp:107-121) and the moment clear. */
 int tpicb200_clear_moments(tpicb200_context* ctx, void* j, void* mass, tpicb200_stream stream);

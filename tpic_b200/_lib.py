@@ -79,6 +79,8 @@ EXPORTS = {
                                 C.c_void_p, C.c_void_p, C.c_void_p]),
     "tpicb200_sort_binned": (C.c_int, [C.c_void_p, C.POINTER(Particles), C.c_void_p, C.c_void_p,
                                        C.POINTER(Particles), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tpicb200_sort_static": (C.c_int, [C.POINTER(Grid), C.c_int, C.POINTER(Particles), C.POINTER(Particles),
+                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tpicb200_clear_moments": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tpicb200_deposit": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(Particles), C.c_void_p, C.c_void_p,
                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),

@@ -237,6 +237,33 @@ int tpicb200_sort_binned(tpicb200_context* ctx, const tpicb200_particles* in, co
                      "binned sort launch failed");
 }
 
+int tpicb200_sort_static(const tpicb200_grid* grid, int precision, const tpicb200_particles* in,
+                         tpicb200_particles* out, uint32_t* counts, uint32_t* offsets, uint32_t* invalid,
+                         tpicb200_stream stream) {
+  if (!grid || !in || !out || !counts || !offsets)
+    return fail(TPICB200_INVALID_ARGUMENT, "static sort needs a grid, records and bins");
+  if (grid->nx < 1 || grid->ny < 1 || grid->nz < 1 || !(grid->lx > 0) || !(grid->ly > 0) || !(grid->lz > 0))
+    return fail(TPICB200_INVALID_ARGUMENT, "invalid grid");
+  if (precision != TPICB200_PRECISION_DOUBLE && precision != TPICB200_PRECISION_MIXED)
+    return fail(TPICB200_INVALID_ARGUMENT, "unknown precision");
+  const Geom g = make_geom(*grid);
+  if (in->count > TPICB200_SORT_STATIC_MAX_RECORDS)
+    return fail(TPICB200_CAPACITY_EXCEEDED, "static sort: more than TPICB200_SORT_STATIC_MAX_RECORDS (1048576) records");
+  if (g.bins > TPICB200_SORT_STATIC_MAX_BINS)
+    return fail(TPICB200_CAPACITY_EXCEEDED, "static sort: grid has more than TPICB200_SORT_STATIC_MAX_BINS (1048576) bins");
+  if (in->count && (!in->rx || !in->ry || !in->rz || !in->u || !in->v || !in->w || !in->q || !in->cell))
+    return fail(TPICB200_INVALID_ARGUMENT, "null particle attribute");
+  if (in->count && (!out->rx || !out->ry || !out->rz || !out->u || !out->v || !out->w || !out->q ||
+                    !out->cell || (in->id && !out->id)))
+    return fail(TPICB200_INVALID_ARGUMENT, "null output attribute");
+  if (in->count && (in->rx == out->rx || in->cell == out->cell))
+    return fail(TPICB200_INVALID_ARGUMENT, "sort input and output alias");
+  uint32_t* scratch = nullptr;
+  if (int r = cuda_status(sort_static_setup(&scratch), "static sort set-up (device symbol address) failed")) return r;
+  return cuda_status(launch_sort_static(precision, g, in, out, counts, offsets, invalid, scratch, (cudaStream_t)stream),
+                     "static sort launch failed");
+}
+
 int tpicb200_clear_moments(tpicb200_context* ctx, void* j, void* mass, tpicb200_stream stream) {
   if (int s = check_ctx(ctx)) return s;
   const size_t fb = ctx->opt.precision == TPICB200_PRECISION_DOUBLE ? 8 : 4;

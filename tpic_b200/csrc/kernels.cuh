@@ -57,6 +57,14 @@ cudaError_t launch_sort_binned(int precision, const Geom& g, const tpicb200_part
                                uint32_t* scan_scratch, uint32_t* binned_words, uint32_t* invalid,
                                cudaStream_t s);
 
+// Context-free sort on the file-scope scratch array (no allocation): the
+// first call on a device resolves the array's address (sort_static_setup).
+long long sort_static_scratch_bytes();
+cudaError_t sort_static_setup(uint32_t** scratch);
+cudaError_t launch_sort_static(int precision, const Geom& g, const tpicb200_particles* in, tpicb200_particles* out,
+                               uint32_t* counts, uint32_t* offsets, uint32_t* invalid, uint32_t* scratch,
+                               cudaStream_t s);
+
 // deposit.cu
 cudaError_t launch_deposit(int precision, int mass_kind, const Geom& g, double qom, double dt,
                            double c, const tpicb200_particles* p, const uint32_t* counts,

@@ -18,6 +18,8 @@
 // test the sort's own flag) and is reported through *invalid.
 #include "kernels.cuh"
 
+#include <mutex>
+
 namespace tpicb200 {
 namespace {
 
@@ -838,6 +840,67 @@ cudaError_t launch_sort_binned(int precision, const Geom& g, const tpicb200_part
   const BinnedScratch b = binned_scratch(g, binned_words, perm);
   if (cudaError_t e = binned_begin(g, b, in_counts, in_offsets, false, s); e != cudaSuccess) return e;
   return binned_finish(precision, g, b, true, in, out, counts, offsets, cursor, perm, scan_scratch, invalid, s);
+}
+
+// ---- Sort without a context and without allocation ----
+//
+// Some callers cannot allocate device memory for a sort: a caller that owns
+// no context (the sort needs one only for its scratch), a caller whose device
+// memory is held by another allocator's pool, or a loop that must not pay
+// cudaMalloc's implicit device synchronisation. For them the general sort runs
+// on a fixed file-scope scratch array instead of context buffers, for inputs
+// up to TPICB200_SORT_STATIC_MAX_RECORDS records over up to
+// TPICB200_SORT_STATIC_MAX_BINS bins; larger inputs are rejected. Every call
+// shares the one array, so calls that overlap in time (other streams, other
+// host threads) race on it; they must be ordered on one stream.
+
+namespace {
+
+constexpr long long kStaticRecords = TPICB200_SORT_STATIC_MAX_RECORDS;
+constexpr long long kStaticBins = TPICB200_SORT_STATIC_MAX_BINS;
+constexpr long long kStaticScanWords = (kStaticBins + kScanTile - 1) / kScanTile + 2 + kStaticBins;
+// Permutation, cursors, then the scan block sums, flags and large-bin list.
+constexpr long long kStaticWords = kStaticRecords + kStaticBins + kStaticScanWords;
+
+static __device__ __align__(256) uint32_t g_static_scratch[kStaticWords];
+
+constexpr int kStaticMaxDevices = 64;
+std::mutex g_static_mutex;
+uint32_t* g_static_address[kStaticMaxDevices] = {};
+
+}  // namespace
+
+long long sort_static_scratch_bytes() { return kStaticWords * 4; }
+
+cudaError_t sort_static_setup(uint32_t** scratch) {
+  int device = 0;
+  cudaError_t e = cudaGetDevice(&device);
+  if (e != cudaSuccess) return e;
+  if (device < 0 || device >= kStaticMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_static_mutex);
+  if (!g_static_address[device]) {
+    // Once per device, with that device current: the array's device address.
+    uint32_t* ptr = nullptr;
+    e = cudaGetSymbolAddress((void**)&ptr, g_static_scratch);
+    if (e != cudaSuccess) return e;
+    g_static_address[device] = ptr;
+  }
+  *scratch = g_static_address[device];
+  return cudaSuccess;
+}
+
+cudaError_t launch_sort_static(int precision, const Geom& g, const tpicb200_particles* in, tpicb200_particles* out,
+                               uint32_t* counts, uint32_t* offsets, uint32_t* invalid, uint32_t* scratch,
+                               cudaStream_t s) {
+  if ((long long)in->count > kStaticRecords || g.bins > kStaticBins) return cudaErrorInvalidValue;
+  uint32_t* perm = scratch;
+  uint32_t* cursor = perm + kStaticRecords;
+  uint32_t* scan = cursor + kStaticBins;
+  // The general sort clears what must start at zero on every call: its
+  // flags and large-bin count (memset), the counts (fill); the cursors are
+  // copied from the offsets and the permutation is fully written.
+  out->count = in->count;
+  return enqueue_general(precision, g, in, out, counts, offsets, cursor, perm, scan, invalid, nullptr, s);
 }
 
 }  // namespace tpicb200
