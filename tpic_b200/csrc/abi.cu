@@ -502,6 +502,7 @@ static int move_and_sort(tpicb200_context* ctx, tpicb200_state* st, int sp, cuda
   }
   const BinnedScratch b = binned_scratch(ctx->g, ctx->binned, ctx->perm);
   cudaError_t e = binned_begin(ctx->g, b, st->counts[sp], st->offsets[sp], true, s);
+  if (e == cudaSuccess) e = binned_validate(ctx->g, b, in->count, s);
   if (e == cudaSuccess)
     e = launch_mover(p, ctx->g, qom, ctx->opt.dt, ctx->opt.c, in, st->e_theta, st->b_node, ctx->invalid, &b, s);
   if (e == cudaSuccess) e = cudaEventRecord(moved, s);

@@ -28,7 +28,7 @@ cudaError_t launch_sort(int precision, const Geom& g, const tpicb200_particles* 
 // path, anything else through the general sort (same stable order).
 struct BinnedState {
   uint32_t fallback;         // nonzero: the general sort produces the output
-  uint32_t pad;
+  uint32_t bins_bad;         // nonzero: the old bins do not tile the records
   unsigned long long total;  // records in the old bins
 };
 struct BinnedScratch {
@@ -45,8 +45,11 @@ BinnedScratch binned_scratch(const Geom& g, uint32_t* words, uint32_t* perm);
 // the mover will add into them).
 cudaError_t binned_begin(const Geom& g, const BinnedScratch& b, const uint32_t* in_counts,
                          const uint32_t* in_offsets, bool zero_transfer, cudaStream_t s);
-// Validation, (classification when `classify`), counts, scan, bases, scatter
-// and the gated general sort.
+// Checks that the old bins tile the n records in key order (else raises
+// bins_bad and fallback).
+cudaError_t binned_validate(const Geom& g, const BinnedScratch& b, uint32_t n, cudaStream_t s);
+// (Classification when `classify`), counts, scan, bases, scatter and the
+// gated general sort; binned_validate must have run.
 cudaError_t binned_finish(int precision, const Geom& g, const BinnedScratch& b, bool classify,
                           const tpicb200_particles* in, tpicb200_particles* out, uint32_t* counts,
                           uint32_t* offsets, uint32_t* cursor, uint32_t* perm, uint32_t* scan_scratch,

@@ -1,6 +1,4 @@
-// Implicit theta-scheme particle mover, one thread per record. Ahead of the
-// binned sort it also emits each record's direction code and the per-cell
-// transfer counts (the sort then skips its own classification pass).
+// Implicit theta-scheme particle mover.
 //
 // Restates push_and_classify_particle (ecsim/particles/particle_mover_device.hpp:37-122)
 // with the whole-domain periodic wrap of classify_particle_point
@@ -9,10 +7,22 @@
 // reference's expressions evaluate under strict IEEE rules, so new fractions,
 // velocities and cell keys are bit-identical to the CPU oracle.
 //
-// HBM-bound: per record it reads key (4 B), charge (8 B), three double
+// Two kernels share one push:
+//  - mover_kernel, one thread per record, gathers the 48 field values of a
+//    record from global memory (they hit L1/L2 because records are sorted);
+//  - run_mover_kernel, for records grouped by the bins of the previous sort
+//    (the cycle's path): a warp takes a run of up to 32 consecutive cells of
+//    one x-row, stages the B and E_theta nodes of the run (33 x 2 x 2 nodes,
+//    converted once to the compute type) in shared memory and streams the
+//    run's records, gathering from shared memory. A record whose key is not
+//    its bin's cell gathers from global memory instead. Both forms evaluate
+//    the same products in the same order, so the results are identical.
+// Ahead of the binned sort both also emit each record's direction code and
+// the per-cell transfer counts (the sort then needs no classification pass).
+//
+// HBM-bound: per record the push reads key (4 B), charge (8 B), three double
 // fractions (24 B) and three velocities, and writes the fractions, the
-// velocities and the key; the 48 field gathers hit L1/L2 because records are
-// sorted by cell.
+// velocities and the key.
 #include "kernels.cuh"
 
 #include <climits>
@@ -26,161 +36,316 @@ struct MoverParams {
   double dt, inv[3];
 };
 
-template <class C, class F>
-__device__ __forceinline__ C gather8(const F* __restrict__ f, long long base, const int* off,
-                                     const C w[8]) {
-  C value = 0;
-#pragma unroll
-  for (int a = 0; a < 8; ++a) value += w[a] * C(__ldg(f + base + off[a]));
-  return value;
-}
-
 // Direction codes and transfer counts of a mover that feeds the binned sort.
 struct MoveCodes {
   uint8_t* code;        // per record: direction code, 0xff when not a neighbour move
   uint32_t* transfer;   // [27][interior cells], added into
   uint32_t* fallback;   // raised when any record did not move to a neighbour
+  const uint32_t* bins_bad;  // the old bins do not tile the records
   long long cells;
 };
 
-// Resident CTAs per SM the mover is compiled for (register budget).
+template <class P>
+struct Records {
+  typename P::Pos* __restrict__ rx;
+  typename P::Pos* __restrict__ ry;
+  typename P::Pos* __restrict__ rz;
+  typename P::Vel* __restrict__ u;
+  typename P::Vel* __restrict__ v;
+  typename P::Vel* __restrict__ w;
+  const double* __restrict__ q;
+  int32_t* __restrict__ key;
+};
+
+// Corner values from global memory: node box of cell (ci, cj, ck).
+template <class P>
+struct GlobalFields {
+  const double* __restrict__ theta;
+  const typename P::Fld* __restrict__ bnode;
+  long long nn, base;
+  int off[8];
+  // which 0: B, 1: E_theta; component c; corner a.
+  __device__ __forceinline__ typename P::VC operator()(int which, int c, int a) const {
+    using C = typename P::VC;
+    return which ? C(__ldg(theta + c * nn + base + off[a])) : C(__ldg(bnode + c * nn + base + off[a]));
+  }
+};
+
+// Corner values staged in shared memory for a run: [which][c][z][y][x].
+constexpr int kRunCells = 32;
+constexpr int kRunNodes = kRunCells + 1;
+template <class C>
+struct SharedFields {
+  const C* s;  // 2 x 3 x 2 x 2 x kRunNodes values
+  int x;       // cell offset in the run
+  __device__ __forceinline__ C operator()(int which, int c, int a) const {
+    return s[(((which * 3 + c) * 2 + ((a >> 2) & 1)) * 2 + ((a >> 1) & 1)) * kRunNodes + x + (a & 1)];
+  }
+};
+
+template <class C, class F>
+__device__ __forceinline__ C gather8(const F& field, int which, int c, const C w[8]) {
+  C value = 0;
+#pragma unroll
+  for (int a = 0; a < 8; ++a) value += w[a] * field(which, c, a);
+  return value;
+}
+
+// The push of record n, whose valid interior cell (ci, cj, ck) was decoded
+// from its key. Returns the direction code of the move (-1: invalid, or a
+// move beyond the 27 neighbouring cells when Coded).
+template <class P, bool Coded, class F>
+__device__ __forceinline__ int push(const Geom& g, const MoverParams<P>& mp, const Records<P>& r, uint32_t n,
+                                    int ci, int cj, int ck, typename P::Pos fx, typename P::Pos fy,
+                                    typename P::Pos fz, const F& field, uint32_t* invalid) {
+  using C = typename P::VC;
+  using Pos = typename P::Pos;
+  using Vel = typename P::Vel;
+  C wt[8];
+  cic_weights<C>(C(fx), C(fy), C(fz), wt);
+  const C bx = gather8<C>(field, 0, 0, wt);
+  const C by = gather8<C>(field, 0, 1, wt);
+  const C bz = gather8<C>(field, 0, 2, wt);
+  const C ex = gather8<C>(field, 1, 0, wt);
+  const C ey = gather8<C>(field, 1, 1, wt);
+  const C ez = gather8<C>(field, 1, 2, wt);
+  const Response<C> rs(bx, by, bz, mp.beta_over_c);
+  const C uu = C(r.u[n]), vv = C(r.v[n]), ww = C(r.w[n]);
+  C hx, hy, hz, ax, ay, az;
+  rs.apply(uu, vv, ww, hx, hy, hz);
+  rs.apply(ex, ey, ez, ax, ay, az);
+  const C px = hx + mp.beta * ax, py = hy + mp.beta * ay, pz = hz + mp.beta * az;
+  const Vel vel[3] = {Vel(C(2) * px - uu), Vel(C(2) * py - vv), Vel(C(2) * pz - ww)};
+  long long cell[3] = {ci, cj, ck};
+  Pos frac[3] = {fx, fy, fz};
+  const int ext[3] = {g.nx, g.ny, g.nz};
+  bool ok = true;
+#pragma unroll
+  for (int axis = 0; axis < 3; ++axis) {
+    if (!isfinite(vel[axis])) { ok = false; break; }
+    const Pos displacement = Pos(mp.dt * double(vel[axis]) * mp.inv[axis]);
+    const Pos moved = frac[axis] + displacement;
+    const double shift = floor(double(moved));
+    if (!(shift >= double(INT_MIN) && shift <= double(INT_MAX))) { ok = false; break; }
+    cell[axis] += (long long)shift;
+    frac[axis] = moved - Pos(shift);
+    if (frac[axis] == Pos(1)) {  // a tiny negative crossing rounded up to the endpoint
+      ++cell[axis];
+      frac[axis] = Pos(0);
+    }
+  }
+  if (!ok) {
+    atomicAdd(invalid, 1u);
+    return -1;
+  }
+#pragma unroll
+  for (int axis = 0; axis < 3; ++axis) {
+    const long long e = ext[axis];
+    if (cell[axis] < 0 || cell[axis] >= e) {
+      const long long m = cell[axis] % e;
+      cell[axis] = m < 0 ? m + e : m;
+    }
+  }
+  r.key[n] = g.encode(int(cell[0]), int(cell[1]), int(cell[2]));
+  r.rx[n] = frac[0]; r.ry[n] = frac[1]; r.rz[n] = frac[2];
+  r.u[n] = vel[0]; r.v[n] = vel[1]; r.w[n] = vel[2];
+  return Coded ? move_code(g, ci, cj, ck, int(cell[0]), int(cell[1]), int(cell[2])) : 0;
+}
+
+// Record checks before the push: a valid interior key, a finite charge and
+// fractions in [0, 1). Writes the decoded cell.
+template <class P>
+__device__ __forceinline__ bool record_ok(const Geom& g, int32_t k0, double charge, typename P::Pos fx,
+                                          typename P::Pos fy, typename P::Pos fz, int& ci, int& cj, int& ck) {
+  using Pos = typename P::Pos;
+  if (!(k0 >= 0 && (long long)k0 < g.bins)) return false;
+  g.decode(k0, ci, cj, ck);
+  return g.interior_cell(ci, cj, ck) && isfinite(charge) && fx >= Pos(0) && fx < Pos(1) && fy >= Pos(0) &&
+         fy < Pos(1) && fz >= Pos(0) && fz < Pos(1);
+}
+
+template <class P>
+__device__ __forceinline__ GlobalFields<P> global_fields(const Geom& g, const double* theta,
+                                                         const typename P::Fld* bnode, int ci, int cj, int ck) {
+  // Corner offsets of the node box (an x-y plane of nodes is far below 2^31).
+  const int plane = g.NX * g.NY;
+  return GlobalFields<P>{theta, bnode, g.nodes, g.node(ci, cj, ck),
+                         {0, 1, g.NX, g.NX + 1, plane, plane + 1, plane + g.NX, plane + g.NX + 1}};
+}
+
+// Codes and transfer counts of one warp-wide step (every lane of the warp
+// calls it): one atomic per run of consecutive lanes with the same
+// (old cell, direction); records are sorted by old cell, so a warp holds few.
+__device__ __forceinline__ void record_codes(const MoveCodes& mc, bool live, uint32_t n, int d, long long old_cell) {
+  const int lane = threadIdx.x & 31;
+  if (live) mc.code[n] = uint8_t(d < 0 ? 0xff : d);
+  const long long slot = d < 0 ? -1 : old_cell * 27 + d;
+  const long long left = __shfl_up_sync(0xffffffffu, slot, 1);
+  const unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || slot != left);
+  if (d >= 0 && ((heads >> lane) & 1u)) {
+    const unsigned later = heads & ~((2u << lane) - 1u);
+    const int next = later ? __ffs(later) - 1 : 32;
+    atomicAdd(mc.transfer + d * mc.cells + old_cell, unsigned(next - lane));
+  }
+  if (__any_sync(0xffffffffu, live && d < 0) && lane == 0) atomicExch(mc.fallback, 1u);
+}
+
+// Resident CTAs per SM the movers are compiled for (register budget).
 #ifndef TPICB200_MOVER_MIN_BLOCKS
 #define TPICB200_MOVER_MIN_BLOCKS 4
 #endif
 
+// One thread per record. With a gate, the kernel runs only when *gate != 0.
 template <class P, bool Coded>
 __global__ void __launch_bounds__(256, TPICB200_MOVER_MIN_BLOCKS) mover_kernel(Geom g, MoverParams<P> mp,
-    typename P::Pos* __restrict__ rx, typename P::Pos* __restrict__ ry,
-    typename P::Pos* __restrict__ rz, typename P::Vel* __restrict__ u,
-    typename P::Vel* __restrict__ v, typename P::Vel* __restrict__ w,
-    const double* __restrict__ q, int32_t* __restrict__ key, uint32_t count,
-    const double* __restrict__ theta, const typename P::Fld* __restrict__ bnode,
-    uint32_t* __restrict__ invalid, MoveCodes mc) {
-  using C = typename P::VC;
+    Records<P> r, uint32_t count, const double* __restrict__ theta, const typename P::Fld* __restrict__ bnode,
+    uint32_t* __restrict__ invalid, MoveCodes mc, const uint32_t* gate) {
   using Pos = typename P::Pos;
-  using Vel = typename P::Vel;
-  const long long nn = g.nodes;
-  // Corner offsets of the node box (an x-y plane of nodes is far below 2^31).
-  const int plane = g.NX * g.NY;
-  const int off[8] = {0, 1, g.NX, g.NX + 1, plane, plane + 1, plane + g.NX, plane + g.NX + 1};
-  // Moves record n; returns its direction code (-1: invalid record, or a
-  // move beyond the 27 neighbouring cells) and its old interior cell.
-  auto move = [&](uint32_t n, long long& old_cell) -> int {
-    const int32_t k0 = key[n];
-    const double charge = q[n];
-    const Pos fx = rx[n], fy = ry[n], fz = rz[n];
-    int ci, cj, ck;
-    bool ok = k0 >= 0 && (long long)k0 < g.bins;
-    if (ok) {
-      g.decode(k0, ci, cj, ck);
-      ok = g.interior_cell(ci, cj, ck) && isfinite(charge) && fx >= Pos(0) && fx < Pos(1) &&
-           fy >= Pos(0) && fy < Pos(1) && fz >= Pos(0) && fz < Pos(1);
-    }
-    if (!ok) {
-      atomicAdd(invalid, 1u);
-      return -1;
-    }
-    C wt[8];
-    cic_weights<C>(C(fx), C(fy), C(fz), wt);
-    const long long base = g.node(ci, cj, ck);
-    const C bx = gather8<C>(bnode, base, off, wt);
-    const C by = gather8<C>(bnode + nn, base, off, wt);
-    const C bz = gather8<C>(bnode + 2 * nn, base, off, wt);
-    const C ex = gather8<C>(theta, base, off, wt);
-    const C ey = gather8<C>(theta + nn, base, off, wt);
-    const C ez = gather8<C>(theta + 2 * nn, base, off, wt);
-    const Response<C> r(bx, by, bz, mp.beta_over_c);
-    const C uu = C(u[n]), vv = C(v[n]), ww = C(w[n]);
-    C hx, hy, hz, ax, ay, az;
-    r.apply(uu, vv, ww, hx, hy, hz);
-    r.apply(ex, ey, ez, ax, ay, az);
-    const C px = hx + mp.beta * ax, py = hy + mp.beta * ay, pz = hz + mp.beta * az;
-    const Vel vel[3] = {Vel(C(2) * px - uu), Vel(C(2) * py - vv), Vel(C(2) * pz - ww)};
-    long long cell[3] = {ci, cj, ck};
-    Pos frac[3] = {fx, fy, fz};
-    const int ext[3] = {g.nx, g.ny, g.nz};
-#pragma unroll
-    for (int axis = 0; axis < 3; ++axis) {
-      if (!isfinite(vel[axis])) { ok = false; break; }
-      const Pos displacement = Pos(mp.dt * double(vel[axis]) * mp.inv[axis]);
-      const Pos moved = frac[axis] + displacement;
-      const double shift = floor(double(moved));
-      if (!(shift >= double(INT_MIN) && shift <= double(INT_MAX))) { ok = false; break; }
-      cell[axis] += (long long)shift;
-      frac[axis] = moved - Pos(shift);
-      if (frac[axis] == Pos(1)) {  // a tiny negative crossing rounded up to the endpoint
-        ++cell[axis];
-        frac[axis] = Pos(0);
-      }
-    }
-    if (!ok) {
-      atomicAdd(invalid, 1u);
-      return -1;
-    }
-#pragma unroll
-    for (int axis = 0; axis < 3; ++axis) {
-      const long long e = ext[axis];
-      if (cell[axis] < 0 || cell[axis] >= e) {
-        const long long m = cell[axis] % e;
-        cell[axis] = m < 0 ? m + e : m;
-      }
-    }
-    key[n] = g.encode(int(cell[0]), int(cell[1]), int(cell[2]));
-    rx[n] = frac[0]; ry[n] = frac[1]; rz[n] = frac[2];
-    u[n] = vel[0]; v[n] = vel[1]; w[n] = vel[2];
-    old_cell = ci + (long long)g.nx * (cj + (long long)g.ny * ck);
-    return Coded ? move_code(g, ci, cj, ck, int(cell[0]), int(cell[1]), int(cell[2])) : 0;
-  };
+  if (gate && *gate == 0) return;
   const int lane = threadIdx.x & 31;
   const uint32_t stride = gridDim.x * blockDim.x;
   // Warp-uniform loop: lane l of a warp takes record base + l.
   for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < count; base += stride) {
     const uint32_t n = base + lane;
     long long old_cell = 0;
-    const int d = n < count ? move(n, old_cell) : -1;
-    if constexpr (Coded) {
-      if (n < count) mc.code[n] = uint8_t(d < 0 ? 0xff : d);
-      // Transfer counts: one atomic per run of consecutive lanes with the same
-      // (old cell, direction); records are sorted by old cell, so a warp holds
-      // few runs.
-      const long long slot = d < 0 ? -1 : old_cell * 27 + d;
-      const long long left = __shfl_up_sync(0xffffffffu, slot, 1);
-      const unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || slot != left);
-      if (d >= 0 && ((heads >> lane) & 1u)) {
-        const unsigned later = heads & ~((2u << lane) - 1u);
-        const int next = later ? __ffs(later) - 1 : 32;
-        atomicAdd(mc.transfer + d * mc.cells + old_cell, unsigned(next - lane));
+    int d = -1;
+    if (n < count) {
+      const int32_t k0 = r.key[n];
+      const double charge = r.q[n];
+      const Pos fx = r.rx[n], fy = r.ry[n], fz = r.rz[n];
+      int ci, cj, ck;
+      if (record_ok<P>(g, k0, charge, fx, fy, fz, ci, cj, ck)) {
+        d = push<P, Coded>(g, mp, r, n, ci, cj, ck, fx, fy, fz, global_fields<P>(g, theta, bnode, ci, cj, ck),
+                           invalid);
+        old_cell = ci + (long long)g.nx * (cj + (long long)g.ny * ck);
+      } else {
+        atomicAdd(invalid, 1u);
       }
-      if (__any_sync(0xffffffffu, n < count && d < 0) && lane == 0) atomicExch(mc.fallback, 1u);
     }
+    if constexpr (Coded) record_codes(mc, n < count, n, d, old_cell);
+  }
+}
+
+// Runs of up to 32 cells of one x-row; records grouped by the bins
+// (old_counts, old_offsets), which validate_bins has checked (the kernel
+// returns at once when they do not tile the records).
+constexpr int kRunWarps = 4;
+
+template <class P>
+__global__ void __launch_bounds__(kRunWarps * 32, 2 * TPICB200_MOVER_MIN_BLOCKS) run_mover_kernel(Geom g,
+    MoverParams<P> mp, Records<P> r, uint32_t count, const double* __restrict__ theta,
+    const typename P::Fld* __restrict__ bnode, const uint32_t* __restrict__ old_counts,
+    const uint32_t* __restrict__ old_offsets, uint32_t* __restrict__ invalid, MoveCodes mc) {
+  using C = typename P::VC;
+  using Pos = typename P::Pos;
+  constexpr int kStaged = 2 * 3 * 2 * 2 * kRunNodes;
+  __shared__ C fields[kRunWarps][kStaged];
+  __shared__ uint32_t starts[kRunWarps][kRunCells];
+  if (*mc.bins_bad) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int segments = (g.nx + kRunCells - 1) / kRunCells;
+  const long long runs = (long long)segments * g.ny * g.nz;
+  C* sf = fields[warp];
+  uint32_t* st = starts[warp];
+  for (long long run = (long long)blockIdx.x * kRunWarps + warp; run < runs; run += (long long)gridDim.x * kRunWarps) {
+    const int seg = int(run % segments);
+    const long long row = run / segments;
+    const int j = int(row % g.ny), k = int(row / g.ny);
+    const int i0 = seg * kRunCells;
+    const int len = min(kRunCells, g.nx - i0);
+    // Cells of the run and their record ranges.
+    uint32_t off = 0xffffffffu, stop = 0;
+    if (lane < len) {
+      const int32_t key = g.encode(i0 + lane, j, k);
+      off = old_offsets[key];
+      stop = off + old_counts[key];
+    }
+    st[lane] = off;
+    const uint32_t begin = __shfl_sync(0xffffffffu, off, 0);
+    const uint32_t end = min(__shfl_sync(0xffffffffu, stop, len - 1), count);
+    // Stage the run's nodes: x in [i0, i0 + len], y in {j, j+1}, z in {k, k+1}.
+    const int nodes_x = len + 1;
+    for (int t = lane; t < 24 * nodes_x; t += 32) {
+      const int x = t % nodes_x, rest = t / nodes_x;  // rest = ((which*3 + c)*2 + z)*2 + y
+      const int y = rest & 1, z = (rest >> 1) & 1, c = (rest >> 2) % 3, which = (rest >> 2) / 3;
+      const long long at = c * g.nodes + g.node(i0 + x, j + y, k + z);
+      sf[rest * kRunNodes + x] = which ? C(__ldg(theta + at)) : C(__ldg(bnode + at));
+    }
+    __syncwarp();
+    for (uint32_t p0 = begin; p0 < end; p0 += 32) {
+      const uint32_t n = p0 + lane;
+      const bool live = n < end;
+      long long old_cell = 0;
+      int d = -1;
+      if (live) {
+        const int32_t k0 = r.key[n];
+        const double charge = r.q[n];
+        const Pos fx = r.rx[n], fy = r.ry[n], fz = r.rz[n];
+        int c = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1)
+          if (st[c + step] <= n) c += step;
+        int ci, cj, ck;
+        if (record_ok<P>(g, k0, charge, fx, fy, fz, ci, cj, ck)) {
+          if (ci == i0 + c && cj == j && ck == k)
+            d = push<P, true>(g, mp, r, n, ci, cj, ck, fx, fy, fz, SharedFields<C>{sf, c}, invalid);
+          else
+            d = push<P, true>(g, mp, r, n, ci, cj, ck, fx, fy, fz, global_fields<P>(g, theta, bnode, ci, cj, ck),
+                              invalid);
+          old_cell = ci + (long long)g.nx * (cj + (long long)g.ny * ck);
+        } else {
+          atomicAdd(invalid, 1u);
+        }
+      }
+      record_codes(mc, live, n, d, old_cell);
+    }
+    __syncwarp();
   }
 }
 
 template <class P>
-cudaError_t launch(const Geom& g, double qom, double dt, double c, tpicb200_particles* p,
-                   const double* theta, const void* bnode, uint32_t* invalid, const BinnedScratch* binned,
-                   cudaStream_t s) {
+MoverParams<P> mover_params(const Geom& g, double qom, double dt, double c) {
   MoverParams<P> mp;
   const double beta = qom * dt / 2;  // prepare_particle_mover_parameters: double, converted once
   mp.beta = typename P::VC(beta);
   mp.beta_over_c = typename P::VC(beta / c);
   mp.dt = dt;
   for (int a = 0; a < 3; ++a) mp.inv[a] = 1.0 / (a == 0 ? g.dx : a == 1 ? g.dy : g.dz);
+  return mp;
+}
+
+template <class P>
+Records<P> records(tpicb200_particles* p) {
+  return Records<P>{(typename P::Pos*)p->rx, (typename P::Pos*)p->ry, (typename P::Pos*)p->rz,
+                    (typename P::Vel*)p->u, (typename P::Vel*)p->v, (typename P::Vel*)p->w, p->q, p->cell};
+}
+
+template <class P>
+cudaError_t launch(const Geom& g, double qom, double dt, double c, tpicb200_particles* p,
+                   const double* theta, const void* bnode, uint32_t* invalid, const BinnedScratch* binned,
+                   cudaStream_t s) {
+  const MoverParams<P> mp = mover_params<P>(g, qom, dt, c);
   if (p->count == 0) return cudaSuccess;
   const unsigned blocks = grid_for(p->count, 256, 148u * 8u);
-  MoveCodes mc{nullptr, nullptr, nullptr, (long long)g.nx * g.ny * g.nz};
-  auto kernel = mover_kernel<P, false>;
-  if (binned) {
-    mc.code = binned->code;
-    mc.transfer = binned->transfer;
-    mc.fallback = &binned->state->fallback;
-    kernel = mover_kernel<P, true>;
+  const Records<P> r = records<P>(p);
+  const auto* bn = (const typename P::Fld*)bnode;
+  if (!binned) {
+    mover_kernel<P, false><<<blocks, 256, 0, s>>>(g, mp, r, p->count, theta, bn, invalid,
+                                                  MoveCodes{nullptr, nullptr, nullptr, nullptr, 0}, nullptr);
+    count_launches(1);
+    return cudaGetLastError();
   }
-  kernel<<<blocks, 256, 0, s>>>(g, mp, (typename P::Pos*)p->rx, (typename P::Pos*)p->ry,
-      (typename P::Pos*)p->rz, (typename P::Vel*)p->u, (typename P::Vel*)p->v,
-      (typename P::Vel*)p->w, p->q, p->cell, p->count, theta,
-      (const typename P::Fld*)bnode, invalid, mc);
-  count_launches(1);
+  // Bins checked by validate_bins: the run mover; otherwise the per-record
+  // mover moves every record. Exactly one of the two works (the choice
+  // depends only on the bins, not on flags the movers themselves raise).
+  MoveCodes mc{binned->code, binned->transfer, &binned->state->fallback, &binned->state->bins_bad,
+               (long long)g.nx * g.ny * g.nz};
+  const long long runs = (long long)((g.nx + kRunCells - 1) / kRunCells) * g.ny * g.nz;
+  run_mover_kernel<P><<<grid_for(runs * 32, kRunWarps * 32, 148u * 8u), kRunWarps * 32, 0, s>>>(
+      g, mp, r, p->count, theta, bn, binned->old_counts, binned->old_offsets, invalid, mc);
+  mover_kernel<P, false><<<blocks, 256, 0, s>>>(g, mp, r, p->count, theta, bn, invalid, mc,
+                                                &binned->state->bins_bad);
+  count_launches(2);
   return cudaGetLastError();
 }
 

@@ -505,12 +505,18 @@ __global__ void __launch_bounds__(256) validate_bins_kernel(Geom g, uint32_t n,
     unsigned long long block_total = 0;
     for (int w = 0; w < 8; ++w) block_total += partial[w];
     atomicAdd(&state->total, block_total);
-    if (any_bad) atomicExch(&state->fallback, 1u);
+    if (any_bad) {
+      atomicExch(&state->bins_bad, 1u);
+      atomicExch(&state->fallback, 1u);
+    }
   }
 }
 
 __global__ void decide_kernel(uint32_t n, BinnedState* state) {
-  if (state->total != (unsigned long long)n) state->fallback = 1;
+  if (state->total != (unsigned long long)n) {
+    state->bins_bad = 1;
+    state->fallback = 1;
+  }
 }
 
 __global__ void __launch_bounds__(kBinnedThreads) classify_kernel(Geom g, const int32_t* __restrict__ keys,
@@ -785,6 +791,13 @@ cudaError_t binned_begin(const Geom& g, const BinnedScratch& b, const uint32_t* 
   return e;
 }
 
+cudaError_t binned_validate(const Geom& g, const BinnedScratch& b, uint32_t n, cudaStream_t s) {
+  validate_bins_kernel<<<grid_for(g.bins, 256, 148u * 8u), 256, 0, s>>>(g, n, b.old_counts, b.old_offsets, b.state);
+  decide_kernel<<<1, 1, 0, s>>>(n, b.state);
+  count_launches(2);
+  return cudaGetLastError();
+}
+
 cudaError_t binned_finish(int precision, const Geom& g, const BinnedScratch& b, bool classify,
                           const tpicb200_particles* in, tpicb200_particles* out, uint32_t* counts,
                           uint32_t* offsets, uint32_t* cursor, uint32_t* perm, uint32_t* scan_scratch,
@@ -795,9 +808,7 @@ cudaError_t binned_finish(int precision, const Geom& g, const BinnedScratch& b, 
   out->count = n;
   // One warp per run of 32 cells.
   const unsigned runs_grid = grid_for((cells + 31) / 32 * 32, kBinnedThreads, 148u * 8u);
-  validate_bins_kernel<<<grid_for(bins, 256, 148u * 8u), 256, 0, s>>>(g, n, b.old_counts, b.old_offsets, b.state);
-  decide_kernel<<<1, 1, 0, s>>>(n, b.state);
-  int launches = 2;
+  int launches = 0;
   if (classify) {
     classify_kernel<<<runs_grid, kBinnedThreads, 0, s>>>(g, in->cell, n, b.old_counts, b.old_offsets, b.transfer,
                                                         b.code, b.state);
@@ -839,6 +850,7 @@ cudaError_t launch_sort_binned(int precision, const Geom& g, const tpicb200_part
                                cudaStream_t s) {
   const BinnedScratch b = binned_scratch(g, binned_words, perm);
   if (cudaError_t e = binned_begin(g, b, in_counts, in_offsets, false, s); e != cudaSuccess) return e;
+  if (cudaError_t e = binned_validate(g, b, in->count, s); e != cudaSuccess) return e;
   return binned_finish(precision, g, b, true, in, out, counts, offsets, cursor, perm, scan_scratch, invalid, s);
 }
 
