@@ -19,14 +19,16 @@ struct tpicb200_context {
   SolverWorkspace* solver = nullptr;
   uint32_t* cursor = nullptr;
   uint32_t* perm = nullptr;
+  uint32_t* perm2 = nullptr;     // ranks of the second species of a pair (the cycle)
   uint32_t* scan = nullptr;
   uint32_t* binned = nullptr;    // binned-sort state, old bins and transfer counts
+  uint16_t* codes = nullptr;     // binned-sort run code per record
   uint32_t* invalid = nullptr;   // context's own invalid counter
   double* partials = nullptr;    // energy reduction partials
   double* reduced = nullptr;     // energy reduction results
   double* pinned = nullptr;      // host mirror of `reduced` + invalid
   int energy_blocks = 0;
-  cudaEvent_t events[6 + 2 * TPICB200_MAX_SPECIES]{};
+  cudaEvent_t events[6 + 3 * TPICB200_MAX_SPECIES]{};
   float* moments = nullptr;      // per-cell moments of the tensor-core forms (mixed precision)
   bool moments_pending = false;  // moments hold deposits not yet assembled
   // J and mass buffers zeroed by the last tpicb200_clear_moments that nothing
@@ -145,8 +147,10 @@ int tpicb200_create(const tpicb200_grid* grid, const tpicb200_options* options, 
   };
   alloc((void**)&ctx->cursor, size_t(ctx->g.bins) * 4);
   alloc((void**)&ctx->perm, size_t(options->max_particles) * 4);
+  alloc((void**)&ctx->perm2, size_t(options->max_particles) * 4);
   alloc((void**)&ctx->scan, sort_scan_words(ctx->g.bins) * 4);
   alloc((void**)&ctx->binned, binned_scratch_words(ctx->g) * 4);
+  alloc((void**)&ctx->codes, size_t(options->max_particles) * 2);
   alloc((void**)&ctx->invalid, 4);
   alloc((void**)&ctx->partials, size_t(ctx->energy_blocks) * (2 + 5 * TPICB200_MAX_SPECIES) * 8);
   alloc((void**)&ctx->reduced, (2 + 5 * TPICB200_MAX_SPECIES + 2) * 8);
@@ -167,7 +171,8 @@ int tpicb200_destroy(tpicb200_context* ctx) {
   if (!ctx) return TPICB200_SUCCESS;
   cudaDeviceSynchronize();
   solver_destroy(ctx->solver);
-  cudaFree(ctx->cursor); cudaFree(ctx->perm); cudaFree(ctx->scan); cudaFree(ctx->binned); cudaFree(ctx->invalid);
+  cudaFree(ctx->cursor); cudaFree(ctx->perm); cudaFree(ctx->perm2); cudaFree(ctx->scan); cudaFree(ctx->binned); cudaFree(ctx->codes);
+  cudaFree(ctx->invalid);
   cudaFree(ctx->partials); cudaFree(ctx->reduced); cudaFree(ctx->moments);
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
   for (auto& ev : ctx->events)
@@ -232,7 +237,8 @@ int tpicb200_sort_binned(tpicb200_context* ctx, const tpicb200_particles* in, co
   if (in->count && (in->rx == out->rx || in->cell == out->cell))
     return fail(TPICB200_INVALID_ARGUMENT, "sort input and output alias");
   return cuda_status(launch_sort_binned(ctx->opt.precision, ctx->g, in, in_counts, in_offsets, out, counts, offsets,
-                                        ctx->cursor, ctx->perm, ctx->scan, ctx->binned, invalid_or_own(ctx, invalid),
+                                        ctx->cursor, ctx->perm, ctx->scan, ctx->binned, ctx->codes,
+                                        invalid_or_own(ctx, invalid),
                                         (cudaStream_t)stream),
                      "binned sort launch failed");
 }
@@ -298,14 +304,14 @@ int tpicb200_deposit(tpicb200_context* ctx, double qom, const tpicb200_particles
     if (!j || !mass) return fail(TPICB200_INVALID_ARGUMENT, "tensor-core forms deposit J-hat and mass together");
     const int accumulate = ctx->moments_pending ? 1 : 0;
     const int r = cuda_status(launch_deposit_tc(mass_kind, ctx->g, 1, &qom, ctx->opt.dt, ctx->opt.c, &p, &counts,
-                                                &offsets, b_node, ctx->moments, accumulate, inv, s),
+                                                &offsets, b_node, ctx->moments, accumulate, inv, nullptr, s),
                               "tensor-core deposition launch failed");
     if (r == TPICB200_SUCCESS) ctx->moments_pending = true;
     return r;
   }
   ctx->cleared_j = ctx->cleared_mass = nullptr;
   return cuda_status(launch_deposit(ctx->opt.precision, mass_kind, ctx->g, qom, ctx->opt.dt, ctx->opt.c, p,
-                                    counts, offsets, b_node, j, mass, inv, s),
+                                    counts, offsets, b_node, j, mass, inv, nullptr, s),
                      "deposition launch failed");
 }
 
@@ -420,7 +426,7 @@ int tpicb200_deposit_species(tpicb200_context* ctx, int ns, const double* qom, c
   }
   const int r = cuda_status(launch_deposit_tc(mass_kind, ctx->g, ns, qom, ctx->opt.dt, ctx->opt.c, parts, counts,
                                               offsets, b_node, ctx->moments, ctx->moments_pending ? 1 : 0,
-                                              invalid_or_own(ctx, invalid), (cudaStream_t)stream),
+                                              invalid_or_own(ctx, invalid), nullptr, (cudaStream_t)stream),
                             "tensor-core deposition launch failed");
   if (r == TPICB200_SUCCESS) ctx->moments_pending = true;
   return r;
@@ -470,12 +476,16 @@ static int check_state(tpicb200_context* ctx, tpicb200_state* st) {
   return TPICB200_SUCCESS;
 }
 
-// The mover of species sp on its live slot, then the sort into the idle
-// slot; `moved` and `sorted` are recorded after each. On grids whose extents
-// are all at least 3 the mover emits direction codes and transfer counts and
-// the binned sort places the records by them; otherwise the general sort runs.
-static int move_and_sort(tpicb200_context* ctx, tpicb200_state* st, int sp, cudaEvent_t moved, cudaEvent_t sorted,
-                         cudaStream_t s) {
+// The mover of species sp on its live slot, then the sort of the moved
+// records into the idle slot; `moved` and `sorted` are recorded after each.
+// On grids whose extents are all at least 3 the mover emits direction codes
+// and transfer counts and the binned sort ranks the records by them: perm
+// receives the ranks (sorted position -> record of the live slot) and the
+// sorted records are left for the deposition to write (*deferred = true);
+// otherwise the general sort writes them (*deferred = false). The caller
+// flips the live slot once the idle slot holds the sorted records.
+static int move_and_sort(tpicb200_context* ctx, tpicb200_state* st, int sp, uint32_t* perm, cudaEvent_t moved,
+                         cudaEvent_t sorted, bool* deferred, cudaStream_t s) {
   const int cur = st->current[sp];
   tpicb200_particles* in = &st->slot[sp][cur];
   tpicb200_particles* out = &st->slot[sp][1 - cur];
@@ -493,25 +503,70 @@ static int move_and_sort(tpicb200_context* ctx, tpicb200_state* st, int sp, cuda
                                  nullptr, s);
     if (e == cudaSuccess) e = cudaEventRecord(moved, s);
     if (e == cudaSuccess)
-      e = launch_sort(p, ctx->g, in, out, st->counts[sp], st->offsets[sp], ctx->cursor, ctx->perm, ctx->scan,
+      e = launch_sort(p, ctx->g, in, out, st->counts[sp], st->offsets[sp], ctx->cursor, perm, ctx->scan,
                       ctx->invalid, s);
     if (e == cudaSuccess) e = cudaEventRecord(sorted, s);
     if (e != cudaSuccess) return cuda_status(e, "mover or sort launch failed");
-    st->current[sp] = 1 - cur;
+    *deferred = false;
     return TPICB200_SUCCESS;
   }
-  const BinnedScratch b = binned_scratch(ctx->g, ctx->binned, ctx->perm);
+  const BinnedScratch b = binned_scratch(ctx->g, ctx->binned, ctx->codes);
   cudaError_t e = binned_begin(ctx->g, b, st->counts[sp], st->offsets[sp], true, s);
   if (e == cudaSuccess) e = binned_validate(ctx->g, b, in->count, s);
   if (e == cudaSuccess)
     e = launch_mover(p, ctx->g, qom, ctx->opt.dt, ctx->opt.c, in, st->e_theta, st->b_node, ctx->invalid, &b, s);
   if (e == cudaSuccess) e = cudaEventRecord(moved, s);
   if (e == cudaSuccess)
-    e = binned_finish(p, ctx->g, b, false, in, out, st->counts[sp], st->offsets[sp], ctx->cursor, ctx->perm,
+    e = binned_finish(p, ctx->g, b, false, false, in, out, st->counts[sp], st->offsets[sp], ctx->cursor, perm,
                       ctx->scan, ctx->invalid, s);
   if (e == cudaSuccess) e = cudaEventRecord(sorted, s);
   if (e != cudaSuccess) return cuda_status(e, "mover or binned sort launch failed");
-  st->current[sp] = 1 - cur;
+  *deferred = true;
+  return TPICB200_SUCCESS;
+}
+
+// Deposition of species [first, first + count) (at most two) from their
+// live slots after move_and_sort: deferred sorts are completed here (the
+// records are read through the ranks and written sorted into the idle slot),
+// then every species of the pair flips to its idle slot.
+static int deposit_pair(tpicb200_context* ctx, tpicb200_state* st, int first, int count, uint32_t* const* perms,
+                        const bool* deferred, bool accumulate, cudaStream_t s) {
+  const tpicb200_particles* parts[2];
+  const uint32_t* counts[2];
+  const uint32_t* offsets[2];
+  SortedCopy copy[2];
+  const SortedCopy* copies[2];
+  double qom[2];
+  for (int i = 0; i < count; ++i) {
+    const int sp = first + i;
+    const int cur = st->current[sp];
+    // A deferred sort: read the moved records (live slot) through the ranks.
+    // Otherwise the idle slot already holds the sorted records: read it in place.
+    parts[i] = deferred[i] ? &st->slot[sp][cur] : &st->slot[sp][1 - cur];
+    copy[i] = SortedCopy{deferred[i] ? perms[i] : nullptr, st->slot[sp][1 - cur]};
+    copies[i] = &copy[i];
+    counts[i] = st->counts[sp];
+    offsets[i] = st->offsets[sp];
+    qom[i] = st->qom[sp];
+  }
+  const int kind = st->mass_kind;
+  const int p = ctx->opt.precision;
+  cudaError_t e = cudaSuccess;
+  if (kind == TPICB200_MASS_TF32 || kind == TPICB200_MASS_BF16X3) {
+    if (p != TPICB200_PRECISION_MIXED)
+      return fail(TPICB200_INVALID_ARGUMENT, "tensor-core mass forms need the mixed precision mode");
+    e = launch_deposit_tc(kind, ctx->g, count, qom, ctx->opt.dt, ctx->opt.c, parts, counts, offsets, st->b_node_next,
+                          ctx->moments, accumulate ? 1 : 0, ctx->invalid, copies, s);
+    if (e == cudaSuccess) ctx->moments_pending = true;
+  } else {
+    ctx->cleared_j = ctx->cleared_mass = nullptr;
+    for (int i = 0; i < count && e == cudaSuccess; ++i)
+      e = launch_deposit(p, kind, ctx->g, qom[i], ctx->opt.dt, ctx->opt.c, parts[i], counts[i], offsets[i],
+                         st->b_node_next, st->j, st->mass, ctx->invalid, copies[i], s);
+  }
+  for (int i = 0; i < count && e == cudaSuccess; ++i) e = launch_copy_ids(parts[i], copies[i], s);
+  if (e != cudaSuccess) return cuda_status(e, "deposition launch failed");
+  for (int i = 0; i < count; ++i) st->current[first + i] = 1 - st->current[first + i];
   return TPICB200_SUCCESS;
 }
 
@@ -537,9 +592,12 @@ int tpicb200_cycle(tpicb200_context* ctx, tpicb200_state* st, int ncycles, tpicb
   if (int s = check_ctx(ctx)) return s;
   if (int r = check_state(ctx, st)) return r;
   if (ncycles < 0) return fail(TPICB200_INVALID_ARGUMENT, "negative cycle count");
+  const int kind = st->mass_kind;
+  if (kind < TPICB200_MASS_SCALAR || kind > TPICB200_MASS_BF16X3) return fail(TPICB200_INVALID_ARGUMENT, "unknown mass kind");
   cudaStream_t s = (cudaStream_t)stream;
   cudaEvent_t* ev = ctx->events;
-  cudaEvent_t* sev = ctx->events + 6;  // per species: after its mover, after its sort
+  cudaEvent_t* sev = ctx->events + 6;  // per species: after its mover, after its sort, after its pair's deposition
+  uint32_t* perms[2] = {ctx->perm, ctx->perm2};
   for (int cycle = 0; cycle < ncycles; ++cycle) {
     tpicb200_cycle_report report{};
     cudaEventRecord(ev[0], s);
@@ -547,17 +605,26 @@ int tpicb200_cycle(tpicb200_context* ctx, tpicb200_state* st, int ncycles, tpicb
     if (int r = tpicb200_field_solve(ctx, st->e, st->b_cell, st->j, st->mass, st->e_theta, &report.gmres, stream))
       return r;
     cudaEventRecord(ev[1], s);
-    // Per species: the mover (gathering the old B nodes and E_theta), then the
-    // sort of the moved records into the idle slot.
-    for (int sp = 0; sp < st->ns; ++sp)
-      if (int r = move_and_sort(ctx, st, sp, sev[2 * sp], sev[2 * sp + 1], s)) return r;
-    cudaEventRecord(ev[2], s);
+    // Field advance: E^{n+1} and the next B from E_theta (the movers read
+    // E_theta and the old B nodes, which the advance does not touch).
     if (int r = tpicb200_field_advance(ctx, st->e, st->b_cell, st->e_theta, st->b_cell_next, st->b_node_next, stream))
       return r;
+    cudaEventRecord(ev[2], s);
+    // Per pair of species: the mover and the sort of each, then one
+    // deposition of both with the next B that also writes the sorted records.
+    if (int r = tpicb200_clear_moments(ctx, st->j, st->mass, stream)) return r;
+    for (int first = 0; first < st->ns; first += 2) {
+      const int count = st->ns - first < 2 ? st->ns - first : 2;
+      bool deferred[2] = {false, false};
+      for (int i = 0; i < count; ++i)
+        if (int r = move_and_sort(ctx, st, first + i, perms[i], sev[3 * (first + i)], sev[3 * (first + i) + 1],
+                                  &deferred[i], s))
+          return r;
+      if (int r = deposit_pair(ctx, st, first, count, perms, deferred, first > 0, s)) return r;
+      cudaEventRecord(sev[3 * first + 2], s);
+    }
+    if (int r = tpicb200_fold_periodic(ctx, st->j, st->mass, stream)) return r;
     cudaEventRecord(ev[3], s);
-    // Deposition of the moved records with the next B.
-    if (int r = deposit_all(ctx, st, st->b_node_next, s)) return r;
-    cudaEventRecord(ev[4], s);
     std::swap(st->b_cell, st->b_cell_next);
     std::swap(st->b_node, st->b_node_next);
     if (reports) {
@@ -573,22 +640,29 @@ int tpicb200_cycle(tpicb200_context* ctx, tpicb200_state* st, int ncycles, tpicb
         report.total_energy += out[2 + 5 * sp];
       }
     }
-    cudaEventRecord(ev[5], s);
+    cudaEventRecord(ev[4], s);
     uint32_t bad = 0;
     if (int r = read_invalid(ctx, s, &bad)) return r;
     if (bad) return fail(TPICB200_INVALID_DATA, "the cycle raised the invalid-data flag");
     // Stage times: solve, move, advance, sort, deposit, fold + diagnostics.
     float t = 0.0f;
     cudaEventElapsedTime(&report.stage_ms[0], ev[0], ev[1]);
-    for (int sp = 0; sp < st->ns; ++sp) {
-      cudaEventElapsedTime(&t, sp == 0 ? ev[1] : sev[2 * sp - 1], sev[2 * sp]);
-      report.stage_ms[1] += t;
-      cudaEventElapsedTime(&t, sev[2 * sp], sev[2 * sp + 1]);
-      report.stage_ms[3] += t;
+    cudaEventElapsedTime(&report.stage_ms[2], ev[1], ev[2]);
+    for (int first = 0; first < st->ns; first += 2) {
+      const int count = st->ns - first < 2 ? st->ns - first : 2;
+      for (int i = 0; i < count; ++i) {
+        const int sp = first + i;
+        cudaEventElapsedTime(&t, sp == 0 ? ev[2] : (i == 0 ? sev[3 * (sp - 2) + 2] : sev[3 * (sp - 1) + 1]),
+                             sev[3 * sp]);
+        report.stage_ms[1] += t;
+        cudaEventElapsedTime(&t, sev[3 * sp], sev[3 * sp + 1]);
+        report.stage_ms[3] += t;
+      }
+      cudaEventElapsedTime(&t, sev[3 * (first + count - 1) + 1], sev[3 * first + 2]);
+      report.stage_ms[4] += t;
     }
-    cudaEventElapsedTime(&report.stage_ms[2], ev[2], ev[3]);
-    cudaEventElapsedTime(&report.stage_ms[4], ev[3], ev[4]);
-    cudaEventElapsedTime(&report.stage_ms[5], ev[4], ev[5]);
+    const int last_pair = (st->ns - 1) / 2 * 2;
+    cudaEventElapsedTime(&report.stage_ms[5], sev[3 * last_pair + 2], ev[4]);
     if (reports) reports[cycle] = report;
   }
   return TPICB200_SUCCESS;

@@ -149,6 +149,25 @@ __device__ __forceinline__ int move_code(const Geom& g, int i, int j, int k, int
   return (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1);
 }
 
+// Runs of the binned sort and the run mover: up to 32 consecutive interior
+// cells of one x-row (segment, j, k). A record's run code packs its move
+// direction d < 27 (bits 0-4) and its cell's offset in the run (bits 5-9);
+// kNoMove marks a record that did not move to a neighbour.
+constexpr int kRunCells = 32;
+constexpr uint16_t kNoMove = 0xffff;
+__host__ __device__ __forceinline__ long long run_count(const Geom& g) {
+  return (long long)((g.nx + kRunCells - 1) / kRunCells) * g.ny * g.nz;
+}
+__host__ __device__ __forceinline__ void run_cells(const Geom& g, long long run, int& i0, int& len, int& j, int& k) {
+  const int segments = (g.nx + kRunCells - 1) / kRunCells;
+  const int seg = int(run % segments);
+  const long long row = run / segments;
+  j = int(row % g.ny);
+  k = int(row / g.ny);
+  i0 = seg * kRunCells;
+  len = g.nx - i0 < kRunCells ? g.nx - i0 : kRunCells;
+}
+
 // The non-unique vertices of a node field: every vertex of the (n+3)^3 box
 // outside the unique periodic nodes [0, n)^3, enumerated as three z slabs
 // (k = -1, n, n+1), then three y slabs and three x slabs of the remainder.

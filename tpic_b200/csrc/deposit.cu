@@ -143,7 +143,10 @@ __global__ void __launch_bounds__(128) sorted_deposit_kernel(Geom g, DepositPara
     const typename P::Vel* __restrict__ w, const double* __restrict__ q,
     const int32_t* __restrict__ key, const uint32_t* __restrict__ counts,
     const uint32_t* __restrict__ offsets, const typename P::Fld* __restrict__ bnode,
-    typename P::Fld* __restrict__ J, typename P::Mass* __restrict__ M, uint32_t* invalid) {
+    typename P::Fld* __restrict__ J, typename P::Mass* __restrict__ M, uint32_t* invalid,
+    const uint32_t* __restrict__ perm, double* __restrict__ orx, double* __restrict__ ory,
+    double* __restrict__ orz, typename P::Vel* __restrict__ ou, typename P::Vel* __restrict__ ov,
+    typename P::Vel* __restrict__ ow, double* __restrict__ oq, int32_t* __restrict__ okey) {
   using C = typename P::VC;
   using Cur = typename P::Fld;
   using Mass = typename P::Mass;
@@ -185,8 +188,16 @@ __global__ void __launch_bounds__(128) sorted_deposit_kernel(Geom g, DepositPara
       for (int e = 0; e < 9; ++e) as[e] = MC(0);
       const uint32_t offset = chunk + lane;
       if (offset < count) {
-        const uint32_t n = first + offset;
+        // With perm, the record at sorted position `pos` is read through it
+        // and copied to that position of the sorted slot.
+        const uint32_t pos = first + offset;
+        const uint32_t n = perm ? perm[pos] : pos;
         const double fx = rx[n], fy = ry[n], fz = rz[n];
+        if (perm) {
+          orx[pos] = fx; ory[pos] = fy; orz[pos] = fz;
+          ou[pos] = u[n]; ov[pos] = v[n]; ow[pos] = w[n];
+          oq[pos] = q[n]; okey[pos] = key[n];
+        }
         bool ok = key[n] == bin && fx >= 0 && fx < 1 && fy >= 0 && fy < 1 && fz >= 0 && fz < 1;
         if (ok) {
           const double charge = q[n];
@@ -364,19 +375,22 @@ __global__ void __launch_bounds__(256) fold_mass_kernel(Geom g, T* __restrict__ 
 }
 
 template <class P, class MC>
-cudaError_t launch_typed(bool mass_only_scalar, const Geom& g, DepositParams dp, const tpicb200_particles* p,
-                         const uint32_t* counts, const uint32_t* offsets, const void* bnode, void* j,
-                         void* mass, uint32_t* invalid, cudaStream_t s) {
-  (void)mass_only_scalar;
+cudaError_t launch_typed(const Geom& g, DepositParams dp, const tpicb200_particles* p, const uint32_t* counts,
+                         const uint32_t* offsets, const void* bnode, void* j, void* mass, uint32_t* invalid,
+                         const SortedCopy* copy, cudaStream_t s) {
   using Vel = typename P::Vel;
   using Fld = typename P::Fld;
   using Mass = typename P::Mass;
   if (counts && offsets) {
     const long long cells = (long long)g.nx * g.ny * g.nz;
     const unsigned blocks = grid_for((cells + 3) / 4, 1, 148u * 64u);
+    const bool c = copy && copy->perm;
     sorted_deposit_kernel<P, MC><<<blocks, 128, 0, s>>>(g, dp, (const double*)p->rx, (const double*)p->ry,
         (const double*)p->rz, (const Vel*)p->u, (const Vel*)p->v, (const Vel*)p->w, p->q, p->cell,
-        counts, offsets, (const Fld*)bnode, (Fld*)j, (Mass*)mass, invalid);
+        counts, offsets, (const Fld*)bnode, (Fld*)j, (Mass*)mass, invalid, c ? copy->perm : nullptr,
+        c ? (double*)copy->out.rx : nullptr, c ? (double*)copy->out.ry : nullptr,
+        c ? (double*)copy->out.rz : nullptr, c ? (Vel*)copy->out.u : nullptr, c ? (Vel*)copy->out.v : nullptr,
+        c ? (Vel*)copy->out.w : nullptr, c ? copy->out.q : nullptr, c ? copy->out.cell : nullptr);
     count_launches(1);
   } else if (p->count) {
     unsorted_deposit_kernel<P, MC><<<grid_for(p->count, 128, 148u * 16u), 128, 0, s>>>(g, dp,
@@ -393,13 +407,29 @@ cudaError_t launch_typed(bool mass_only_scalar, const Geom& g, DepositParams dp,
 cudaError_t launch_deposit(int precision, int mass_kind, const Geom& g, double qom, double dt,
                            double c, const tpicb200_particles* p, const uint32_t* counts,
                            const uint32_t* offsets, const void* bnode, void* j, void* mass,
-                           uint32_t* invalid, cudaStream_t s) {
+                           uint32_t* invalid, const SortedCopy* copy, cudaStream_t s) {
   DepositParams dp{qom * dt / 2 / c, g.inv_volume};
   if (precision == TPICB200_PRECISION_DOUBLE)
-    return launch_typed<PDouble, double>(true, g, dp, p, counts, offsets, bnode, j, mass, invalid, s);
+    return launch_typed<PDouble, double>(g, dp, p, counts, offsets, bnode, j, mass, invalid, copy, s);
   if (mass_kind == TPICB200_MASS_SCALAR_F64)
-    return launch_typed<PMixed, double>(true, g, dp, p, counts, offsets, bnode, j, mass, invalid, s);
-  return launch_typed<PMixed, float>(true, g, dp, p, counts, offsets, bnode, j, mass, invalid, s);
+    return launch_typed<PMixed, double>(g, dp, p, counts, offsets, bnode, j, mass, invalid, copy, s);
+  return launch_typed<PMixed, float>(g, dp, p, counts, offsets, bnode, j, mass, invalid, copy, s);
+}
+
+namespace {
+__global__ void __launch_bounds__(256) copy_ids_kernel(const uint32_t* __restrict__ perm,
+                                                       const uint64_t* __restrict__ in, uint64_t* __restrict__ out,
+                                                       uint32_t count) {
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < count; p += gridDim.x * blockDim.x)
+    out[p] = in[perm[p]];
+}
+}  // namespace
+
+cudaError_t launch_copy_ids(const tpicb200_particles* in, const SortedCopy* copy, cudaStream_t s) {
+  if (!copy || !copy->perm || !in->id || !copy->out.id || in->count == 0) return cudaSuccess;
+  copy_ids_kernel<<<grid_for(in->count, 256, 148u * 8u), 256, 0, s>>>(copy->perm, in->id, copy->out.id, in->count);
+  count_launches(1);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_fold(int precision, const Geom& g, void* j, void* mass, cudaStream_t s) {

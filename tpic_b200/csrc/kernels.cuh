@@ -36,11 +36,11 @@ struct BinnedScratch {
   uint32_t* old_counts;   // copy of the input's bins
   uint32_t* old_offsets;
   uint32_t* transfer;     // [27][interior cells]: counts, then output bases
-  uint8_t* code;          // direction code per record (0xff: not a neighbour move)
+  uint16_t* code;         // run code per record (direction, cell in run; kNoMove)
 };
 size_t binned_scratch_words(const Geom& g);
 bool binned_sort_applies(const Geom& g);
-BinnedScratch binned_scratch(const Geom& g, uint32_t* words, uint32_t* perm);
+BinnedScratch binned_scratch(const Geom& g, uint32_t* words, uint16_t* codes);
 // Copies the input's bins and clears the state (and the transfer counts when
 // the mover will add into them).
 cudaError_t binned_begin(const Geom& g, const BinnedScratch& b, const uint32_t* in_counts,
@@ -48,17 +48,19 @@ cudaError_t binned_begin(const Geom& g, const BinnedScratch& b, const uint32_t* 
 // Checks that the old bins tile the n records in key order (else raises
 // bins_bad and fallback).
 cudaError_t binned_validate(const Geom& g, const BinnedScratch& b, uint32_t n, cudaStream_t s);
-// (Classification when `classify`), counts, scan, bases, scatter and the
-// gated general sort; binned_validate must have run.
-cudaError_t binned_finish(int precision, const Geom& g, const BinnedScratch& b, bool classify,
+// (Classification when `classify`), counts, scan, bases, the ranks (perm:
+// sorted position -> input record), the gather of the sorted records when
+// `materialize`, and the gated general sort (which always writes `out` and
+// the same perm); binned_validate must have run.
+cudaError_t binned_finish(int precision, const Geom& g, const BinnedScratch& b, bool classify, bool materialize,
                           const tpicb200_particles* in, tpicb200_particles* out, uint32_t* counts,
                           uint32_t* offsets, uint32_t* cursor, uint32_t* perm, uint32_t* scan_scratch,
                           uint32_t* invalid, cudaStream_t s);
 cudaError_t launch_sort_binned(int precision, const Geom& g, const tpicb200_particles* in,
                                const uint32_t* in_counts, const uint32_t* in_offsets, tpicb200_particles* out,
                                uint32_t* counts, uint32_t* offsets, uint32_t* cursor, uint32_t* perm,
-                               uint32_t* scan_scratch, uint32_t* binned_words, uint32_t* invalid,
-                               cudaStream_t s);
+                               uint32_t* scan_scratch, uint32_t* binned_words, uint16_t* codes,
+                               uint32_t* invalid, cudaStream_t s);
 
 // Context-free sort on the file-scope scratch array (no allocation): the
 // first call on a device resolves the array's address (sort_static_setup).
@@ -68,11 +70,23 @@ cudaError_t launch_sort_static(int precision, const Geom& g, const tpicb200_part
                                uint32_t* counts, uint32_t* offsets, uint32_t* invalid, uint32_t* scratch,
                                cudaStream_t s);
 
+// The sort's gather fused into the deposition: records are read through
+// perm (sorted position -> record of the read slot) and written at their
+// sorted positions into `out` as they are read. perm == nullptr: the
+// records are read in place, in sorted order, and nothing is written.
+struct SortedCopy {
+  const uint32_t* perm;
+  tpicb200_particles out;
+};
+// Writes out.id[p] = in.id[perm[p]] for the records a fused deposition
+// copied (the deposition kernels copy every other attribute).
+cudaError_t launch_copy_ids(const tpicb200_particles* in, const SortedCopy* copy, cudaStream_t s);
+
 // deposit.cu
 cudaError_t launch_deposit(int precision, int mass_kind, const Geom& g, double qom, double dt,
                            double c, const tpicb200_particles* p, const uint32_t* counts,
                            const uint32_t* offsets, const void* bnode, void* j, void* mass,
-                           uint32_t* invalid, cudaStream_t s);
+                           uint32_t* invalid, const SortedCopy* copy, cudaStream_t s);
 cudaError_t launch_fold(int precision, const Geom& g, void* j, void* mass, cudaStream_t s);
 
 // mass_tc.cu (tcgen05 forms): per-cell moments, then their assembly into J
@@ -83,7 +97,7 @@ size_t moment_floats(const Geom& g);
 cudaError_t launch_deposit_tc(int mass_kind, const Geom& g, int ns, const double* qom, double dt, double c,
                               const tpicb200_particles* const* p, const uint32_t* const* counts,
                               const uint32_t* const* offsets, const void* bnode, float* moments, int accumulate,
-                              uint32_t* invalid, cudaStream_t s);
+                              uint32_t* invalid, const SortedCopy* const* copies, cudaStream_t s);
 cudaError_t launch_assemble_moments(const Geom& g, const float* moments, void* j, void* mass, int overwrite,
                                     cudaStream_t s);
 

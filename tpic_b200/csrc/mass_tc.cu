@@ -93,6 +93,16 @@ struct TcSpecies {
   const uint32_t* counts;
   const uint32_t* offsets;
   float beta_over_c;
+  // Sorted copy (perm null: records read in place).
+  const uint32_t* perm;
+  double* orx;
+  double* ory;
+  double* orz;
+  float* ou;
+  float* ov;
+  float* ow;
+  double* oq;
+  int32_t* okey;
 };
 
 struct TcParams {
@@ -198,6 +208,7 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_deposit_kernel(Geom g, TcP
     double fx, fy, fz, q;
     float u, v, w;
     int32_t key;
+    uint32_t pos;  // sorted position
     bool present, second;
   };
   auto load_meta = [&](long long grp_) {
@@ -221,10 +232,12 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_deposit_kernel(Geom g, TcP
     return m;
   };
   auto load_rec = [&](const Meta& m, uint32_t k) {
-    Rec r{0.0, 0.0, 0.0, 0.0, 0.0f, 0.0f, 0.0f, -1, false, false};
+    Rec r{0.0, 0.0, 0.0, 0.0, 0.0f, 0.0f, 0.0f, -1, 0u, false, false};
     if (k < m.c0 + m.c1) {
       const bool s1 = k >= m.c0;
-      const uint32_t n = s1 ? m.f1 + (k - m.c0) : m.f0 + k;
+      r.pos = s1 ? m.f1 + (k - m.c0) : m.f0 + k;
+      const uint32_t* perm = s1 ? tp.sp[1].perm : tp.sp[0].perm;
+      const uint32_t n = perm ? perm[r.pos] : r.pos;
       r.present = true;
       r.second = s1;
       r.fx = (s1 ? tp.sp[1].rx : tp.sp[0].rx)[n];
@@ -291,6 +304,14 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_deposit_kernel(Geom g, TcP
 #pragma unroll
       for (int f = 0; f < 12; ++f) fac[f] = 0.0f;
       if (rec.present) {
+        // The sorted copy of the record, when the sort left it to this pass.
+        const TcSpecies& sp = rec.second ? tp.sp[1] : tp.sp[0];
+        if (sp.perm) {
+          const uint32_t o = rec.pos;
+          sp.orx[o] = rec.fx; sp.ory[o] = rec.fy; sp.orz[o] = rec.fz;
+          sp.ou[o] = rec.u; sp.ov[o] = rec.v; sp.ow[o] = rec.w;
+          sp.oq[o] = rec.q; sp.okey[o] = rec.key;
+        }
         const double fx = rec.fx, fy = rec.fy, fz = rec.fz;
         bool ok = rec.key == bin && fx >= 0 && fx < 1 && fy >= 0 && fy < 1 && fz >= 0 && fz < 1;
         if (ok) {
@@ -520,7 +541,7 @@ size_t moment_floats(const Geom& g) { return size_t(kMoments) * size_t(moment_st
 cudaError_t launch_deposit_tc(int mass_kind, const Geom& g, int ns, const double* qom, double dt, double c,
                               const tpicb200_particles* const* p, const uint32_t* const* counts,
                               const uint32_t* const* offsets, const void* bnode, float* moments, int accumulate,
-                              uint32_t* invalid, cudaStream_t s) {
+                              uint32_t* invalid, const SortedCopy* const* copies, cudaStream_t s) {
   if (mass_kind != TPICB200_MASS_TF32 && mass_kind != TPICB200_MASS_BF16X3) return cudaErrorNotSupported;
   if (!moments || ns < 1) return cudaErrorInvalidValue;
   int device = 0, sms = 148;
@@ -544,9 +565,16 @@ cudaError_t launch_deposit_tc(int mass_kind, const Geom& g, int ns, const double
     tp.inv_volume = float(g.inv_volume);
     for (int i = 0; i < tp.ns; ++i) {
       const tpicb200_particles* sp = p[first + i];
+      const SortedCopy* cp = copies ? copies[first + i] : nullptr;
+      const bool copy = cp && cp->perm;
       tp.sp[i] = TcSpecies{(const double*)sp->rx, (const double*)sp->ry, (const double*)sp->rz,
                            (const float*)sp->u, (const float*)sp->v, (const float*)sp->w, sp->q, sp->cell,
-                           counts[first + i], offsets[first + i], float(qom[first + i] * dt / 2 / c)};
+                           counts[first + i], offsets[first + i], float(qom[first + i] * dt / 2 / c),
+                           copy ? cp->perm : nullptr, copy ? (double*)cp->out.rx : nullptr,
+                           copy ? (double*)cp->out.ry : nullptr, copy ? (double*)cp->out.rz : nullptr,
+                           copy ? (float*)cp->out.u : nullptr, copy ? (float*)cp->out.v : nullptr,
+                           copy ? (float*)cp->out.w : nullptr, copy ? cp->out.q : nullptr,
+                           copy ? cp->out.cell : nullptr};
     }
     kernel<<<blocks, 128, pad, s>>>(g, tp, (const float*)bnode, moments, moment_stride(g),
                                     (accumulate || first > 0) ? 1 : 0, invalid);

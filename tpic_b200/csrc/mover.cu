@@ -38,7 +38,7 @@ struct MoverParams {
 
 // Direction codes and transfer counts of a mover that feeds the binned sort.
 struct MoveCodes {
-  uint8_t* code;        // per record: direction code, 0xff when not a neighbour move
+  uint16_t* code;       // per record: run code (direction, cell in run), kNoMove when not a neighbour move
   uint32_t* transfer;   // [27][interior cells], added into
   uint32_t* fallback;   // raised when any record did not move to a neighbour
   const uint32_t* bins_bad;  // the old bins do not tile the records
@@ -72,7 +72,6 @@ struct GlobalFields {
 };
 
 // Corner values staged in shared memory for a run: [which][c][z][y][x].
-constexpr int kRunCells = 32;
 constexpr int kRunNodes = kRunCells + 1;
 template <class C>
 struct SharedFields {
@@ -173,12 +172,13 @@ __device__ __forceinline__ GlobalFields<P> global_fields(const Geom& g, const do
                          {0, 1, g.NX, g.NX + 1, plane, plane + 1, plane + g.NX, plane + g.NX + 1}};
 }
 
-// Codes and transfer counts of one warp-wide step (every lane of the warp
+// Run codes and transfer counts of one warp-wide step (every lane of the warp
 // calls it): one atomic per run of consecutive lanes with the same
 // (old cell, direction); records are sorted by old cell, so a warp holds few.
-__device__ __forceinline__ void record_codes(const MoveCodes& mc, bool live, uint32_t n, int d, long long old_cell) {
+__device__ __forceinline__ void record_codes(const MoveCodes& mc, bool live, uint32_t n, int d, int run_cell,
+                                             long long old_cell) {
   const int lane = threadIdx.x & 31;
-  if (live) mc.code[n] = uint8_t(d < 0 ? 0xff : d);
+  if (live) mc.code[n] = d < 0 ? kNoMove : uint16_t(d | (run_cell << 5));
   const long long slot = d < 0 ? -1 : old_cell * 27 + d;
   const long long left = __shfl_up_sync(0xffffffffu, slot, 1);
   const unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || slot != left);
@@ -196,37 +196,25 @@ __device__ __forceinline__ void record_codes(const MoveCodes& mc, bool live, uin
 #endif
 
 // One thread per record. With a gate, the kernel runs only when *gate != 0.
-template <class P, bool Coded>
+template <class P>
 __global__ void __launch_bounds__(256, TPICB200_MOVER_MIN_BLOCKS) mover_kernel(Geom g, MoverParams<P> mp,
     Records<P> r, uint32_t count, const double* __restrict__ theta, const typename P::Fld* __restrict__ bnode,
-    uint32_t* __restrict__ invalid, MoveCodes mc, const uint32_t* gate) {
+    uint32_t* __restrict__ invalid, const uint32_t* gate) {
   using Pos = typename P::Pos;
   if (gate && *gate == 0) return;
-  const int lane = threadIdx.x & 31;
-  const uint32_t stride = gridDim.x * blockDim.x;
-  // Warp-uniform loop: lane l of a warp takes record base + l.
-  for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < count; base += stride) {
-    const uint32_t n = base + lane;
-    long long old_cell = 0;
-    int d = -1;
-    if (n < count) {
-      const int32_t k0 = r.key[n];
-      const double charge = r.q[n];
-      const Pos fx = r.rx[n], fy = r.ry[n], fz = r.rz[n];
-      int ci, cj, ck;
-      if (record_ok<P>(g, k0, charge, fx, fy, fz, ci, cj, ck)) {
-        d = push<P, Coded>(g, mp, r, n, ci, cj, ck, fx, fy, fz, global_fields<P>(g, theta, bnode, ci, cj, ck),
-                           invalid);
-        old_cell = ci + (long long)g.nx * (cj + (long long)g.ny * ck);
-      } else {
-        atomicAdd(invalid, 1u);
-      }
-    }
-    if constexpr (Coded) record_codes(mc, n < count, n, d, old_cell);
+  for (uint32_t n = blockIdx.x * blockDim.x + threadIdx.x; n < count; n += gridDim.x * blockDim.x) {
+    const int32_t k0 = r.key[n];
+    const double charge = r.q[n];
+    const Pos fx = r.rx[n], fy = r.ry[n], fz = r.rz[n];
+    int ci, cj, ck;
+    if (record_ok<P>(g, k0, charge, fx, fy, fz, ci, cj, ck))
+      push<P, false>(g, mp, r, n, ci, cj, ck, fx, fy, fz, global_fields<P>(g, theta, bnode, ci, cj, ck), invalid);
+    else
+      atomicAdd(invalid, 1u);
   }
 }
 
-// Runs of up to 32 cells of one x-row; records grouped by the bins
+// Runs of up to kRunCells cells of one x-row; records grouped by the bins
 // (old_counts, old_offsets), which validate_bins has checked (the kernel
 // returns at once when they do not tile the records).
 constexpr int kRunWarps = 4;
@@ -243,16 +231,12 @@ __global__ void __launch_bounds__(kRunWarps * 32, 2 * TPICB200_MOVER_MIN_BLOCKS)
   __shared__ uint32_t starts[kRunWarps][kRunCells];
   if (*mc.bins_bad) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int segments = (g.nx + kRunCells - 1) / kRunCells;
-  const long long runs = (long long)segments * g.ny * g.nz;
+  const long long runs = run_count(g);
   C* sf = fields[warp];
   uint32_t* st = starts[warp];
   for (long long run = (long long)blockIdx.x * kRunWarps + warp; run < runs; run += (long long)gridDim.x * kRunWarps) {
-    const int seg = int(run % segments);
-    const long long row = run / segments;
-    const int j = int(row % g.ny), k = int(row / g.ny);
-    const int i0 = seg * kRunCells;
-    const int len = min(kRunCells, g.nx - i0);
+    int i0, len, j, k;
+    run_cells(g, run, i0, len, j, k);
     // Cells of the run and their record ranges.
     uint32_t off = 0xffffffffu, stop = 0;
     if (lane < len) {
@@ -276,12 +260,11 @@ __global__ void __launch_bounds__(kRunWarps * 32, 2 * TPICB200_MOVER_MIN_BLOCKS)
       const uint32_t n = p0 + lane;
       const bool live = n < end;
       long long old_cell = 0;
-      int d = -1;
+      int d = -1, c = 0;
       if (live) {
         const int32_t k0 = r.key[n];
         const double charge = r.q[n];
         const Pos fx = r.rx[n], fy = r.ry[n], fz = r.rz[n];
-        int c = 0;
 #pragma unroll
         for (int step = 16; step > 0; step >>= 1)
           if (st[c + step] <= n) c += step;
@@ -297,7 +280,7 @@ __global__ void __launch_bounds__(kRunWarps * 32, 2 * TPICB200_MOVER_MIN_BLOCKS)
           atomicAdd(invalid, 1u);
         }
       }
-      record_codes(mc, live, n, d, old_cell);
+      record_codes(mc, live, n, d, c, old_cell);
     }
     __syncwarp();
   }
@@ -330,8 +313,7 @@ cudaError_t launch(const Geom& g, double qom, double dt, double c, tpicb200_part
   const Records<P> r = records<P>(p);
   const auto* bn = (const typename P::Fld*)bnode;
   if (!binned) {
-    mover_kernel<P, false><<<blocks, 256, 0, s>>>(g, mp, r, p->count, theta, bn, invalid,
-                                                  MoveCodes{nullptr, nullptr, nullptr, nullptr, 0}, nullptr);
+    mover_kernel<P><<<blocks, 256, 0, s>>>(g, mp, r, p->count, theta, bn, invalid, nullptr);
     count_launches(1);
     return cudaGetLastError();
   }
@@ -340,11 +322,10 @@ cudaError_t launch(const Geom& g, double qom, double dt, double c, tpicb200_part
   // depends only on the bins, not on flags the movers themselves raise).
   MoveCodes mc{binned->code, binned->transfer, &binned->state->fallback, &binned->state->bins_bad,
                (long long)g.nx * g.ny * g.nz};
-  const long long runs = (long long)((g.nx + kRunCells - 1) / kRunCells) * g.ny * g.nz;
+  const long long runs = run_count(g);
   run_mover_kernel<P><<<grid_for(runs * 32, kRunWarps * 32, 148u * 8u), kRunWarps * 32, 0, s>>>(
       g, mp, r, p->count, theta, bn, binned->old_counts, binned->old_offsets, invalid, mc);
-  mover_kernel<P, false><<<blocks, 256, 0, s>>>(g, mp, r, p->count, theta, bn, invalid, mc,
-                                                &binned->state->bins_bad);
+  mover_kernel<P><<<blocks, 256, 0, s>>>(g, mp, r, p->count, theta, bn, invalid, &binned->state->bins_bad);
   count_launches(2);
   return cudaGetLastError();
 }

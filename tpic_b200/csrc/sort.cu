@@ -407,63 +407,47 @@ cudaError_t enqueue_general(int precision, const Geom& g, const tpicb200_particl
 //   5. bases (thread per interior bin): walking the 27 sources of b in key
 //      order, T[d][c] becomes the first output position of c's records that
 //      moved by d;
-//   6. scatter (a warp per run of 32 old cells): a record goes to its base
-//      plus its rank among the earlier records of its cell with the same d,
-//      after checking that old cell + d is the cell of its key.
+//   6. rank (a warp per run of up to 32 old cells of an x-row): a record's
+//      position is its base plus its rank among the earlier records of its
+//      cell with the same d, after checking that old cell + d is the cell of
+//      its key; one gather then writes the sorted records.
 // Any record that did not move to a neighbour, any invalid key, bins that do
 // not tile the records or a failed scatter check raise the fallback flag,
 // and the general sort, enqueued last and gated on the flag, rewrites the
-// whole output. The output is the same stable order either way.
+// whole output (the binned gather is skipped). The output is the same stable
+// order either way.
 
 constexpr int kBinnedThreads = 256;
 constexpr int kBinnedWarps = kBinnedThreads / 32;
 
-// A warp takes 32 consecutive old interior cells at a time. Their records
-// form one contiguous range (the bins between them are empty); each lane
-// finds its record's cell by a binary search over the 32 cell starts.
-struct CellRun {
-  uint32_t start[32];  // first record of each cell (ascending)
-  uint32_t begin, end; // record range of the run
-};
-
-// Loads the run of cells u0 .. u0 + 31 (lane l: cell u0 + l) into `run`.
-__device__ __forceinline__ void load_run(const Geom& g, long long u0, long long cells,
-                                         const uint32_t* __restrict__ old_counts,
-                                         const uint32_t* __restrict__ old_offsets, CellRun& run, int& ci, int& cj,
-                                         int& ck) {
+// A warp takes a run (up to 32 consecutive old interior cells of one x-row,
+// run_cells) at a time. The run's records form one contiguous range; lane l
+// holds cell l's record range. Writes the cells' first records to `start`
+// (empty cells share their successor's start; unused entries are ~0) and
+// returns the run's record range.
+__device__ __forceinline__ void load_run_bins(const Geom& g, int i0, int len, int j, int k,
+                                              const uint32_t* __restrict__ old_counts,
+                                              const uint32_t* __restrict__ old_offsets, uint32_t* start,
+                                              uint32_t& begin, uint32_t& end) {
   const int lane = threadIdx.x & 31;
-  const long long u = u0 + lane;
-  const bool valid = u < cells;
   uint32_t off = 0xffffffffu, stop = 0;
-  ci = cj = ck = 0;
-  if (valid) {
-    ci = int(u % g.nx);
-    const long long r = u / g.nx;
-    cj = int(r % g.ny);
-    ck = int(r / g.ny);
-    const int32_t key = g.encode(ci, cj, ck);
+  if (lane < len) {
+    const int32_t key = g.encode(i0 + lane, j, k);
     off = old_offsets[key];
     stop = off + old_counts[key];
   }
-  run.start[lane] = off;
-  const unsigned live = __ballot_sync(0xffffffffu, valid);
-  const int last = 31 - __clz(live);
-  const uint32_t begin = __shfl_sync(0xffffffffu, off, 0);
-  const uint32_t end = __shfl_sync(0xffffffffu, stop, last);
-  if (lane == 0) {
-    run.begin = begin;
-    run.end = end;
-  }
+  start[lane] = off;
+  begin = __shfl_sync(0xffffffffu, off, 0);
+  end = __shfl_sync(0xffffffffu, stop, len - 1);
   __syncwarp();
 }
 
-// Cell (lane index within the run) of record p: the last cell whose start is
-// at most p (empty cells share their successor's start).
-__device__ __forceinline__ int run_cell(const CellRun& run, uint32_t p) {
+// Cell (offset in the run) of record p: the last cell whose start is at most p.
+__device__ __forceinline__ int run_cell(const uint32_t* start, uint32_t p) {
   int c = 0;
 #pragma unroll
   for (int step = 16; step > 0; step >>= 1)
-    if (run.start[c + step] <= p) c += step;
+    if (start[c + step] <= p) c += step;
   return c;
 }
 
@@ -521,25 +505,23 @@ __global__ void decide_kernel(uint32_t n, BinnedState* state) {
 
 __global__ void __launch_bounds__(kBinnedThreads) classify_kernel(Geom g, const int32_t* __restrict__ keys,
     uint32_t n, const uint32_t* __restrict__ old_counts, const uint32_t* __restrict__ old_offsets,
-    uint32_t* __restrict__ transfer, uint8_t* __restrict__ code, BinnedState* state) {
-  __shared__ CellRun runs[kBinnedWarps];
-  __shared__ int32_t coords[kBinnedWarps][3][32];  // (i, j, k) of each cell of the run
+    uint32_t* __restrict__ transfer, uint16_t* __restrict__ code, BinnedState* state) {
+  __shared__ uint32_t starts[kBinnedWarps][kRunCells];
   __shared__ uint32_t hist[kBinnedWarps][27][33];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const long long cells = (long long)g.nx * g.ny * g.nz;
+  const long long runs = run_count(g);
   bool bad = false;
-  CellRun& run = runs[warp];
-  for (long long u0 = ((long long)blockIdx.x * kBinnedWarps + warp) * 32; u0 < cells;
-       u0 += (long long)gridDim.x * kBinnedWarps * 32) {
-    int ci, cj, ck;
-    load_run(g, u0, cells, old_counts, old_offsets, run, ci, cj, ck);
-    coords[warp][0][lane] = ci;
-    coords[warp][1][lane] = cj;
-    coords[warp][2][lane] = ck;
+  uint32_t* start = starts[warp];
+  for (long long run = (long long)blockIdx.x * kBinnedWarps + warp; run < runs;
+       run += (long long)gridDim.x * kBinnedWarps) {
+    int i0, len, j, k;
+    run_cells(g, run, i0, len, j, k);
+    uint32_t begin, end;
+    load_run_bins(g, i0, len, j, k, old_counts, old_offsets, start, begin, end);
 #pragma unroll
     for (int d = 0; d < 27; ++d) hist[warp][d][lane] = 0;
     __syncwarp();
-    const uint32_t begin = run.begin, end = run.end;
     if (begin > end || end > n) {  // bins that do not describe the records: no walk over them
       bad = true;
       continue;
@@ -559,10 +541,10 @@ __global__ void __launch_bounds__(kBinnedThreads) classify_kernel(Geom g, const 
         const bool live = p < end;
         int c = 0, d = -1;
         if (live) {
-          c = run_cell(run, p);
-          d = key_move_code(g, coords[warp][0][c], coords[warp][1][c], coords[warp][2][c], key[m]);
+          c = run_cell(start, p);
+          d = key_move_code(g, i0 + c, j, k, key[m]);
           if (d < 0) bad = true;
-          code[p] = uint8_t(d < 0 ? 0xff : d);
+          code[p] = d < 0 ? kNoMove : uint16_t(d | (c << 5));
         }
         const int slot = d < 0 ? -1 : c * 27 + d;
         const unsigned peers = __match_any_sync(0xffffffffu, slot);
@@ -570,9 +552,11 @@ __global__ void __launch_bounds__(kBinnedThreads) classify_kernel(Geom g, const 
         __syncwarp();
       }
     }
-    if (u0 + lane < cells)
+    if (lane < len) {
+      const long long u = i0 + lane + (long long)g.nx * (j + (long long)g.ny * k);
 #pragma unroll
-      for (int d = 0; d < 27; ++d) transfer[(long long)d * cells + u0 + lane] = hist[warp][d][lane];
+      for (int d = 0; d < 27; ++d) transfer[(long long)d * cells + u] = hist[warp][d][lane];
+    }
     __syncwarp();
   }
   if (__syncthreads_or(bad) && threadIdx.x == 0) atomicExch(&state->fallback, 1u);
@@ -653,96 +637,89 @@ __global__ void __launch_bounds__(256) binned_bases_kernel(Geom g, const uint32_
   }
 }
 
-template <class Vel>
-__global__ void __launch_bounds__(kBinnedThreads) binned_scatter_kernel(Geom g, uint32_t n,
+// Rank of each live lane among the live lanes of its slot and the slot's
+// lane mask: one ballot per distinct slot value in the warp (a chunk of
+// sorted records holds few).
+__device__ __forceinline__ unsigned slot_group(int slot, bool live) {
+  unsigned rem = __ballot_sync(0xffffffffu, live), group = 0;
+  while (rem) {
+    const int leader = __ffs(rem) - 1;
+    const int s = __shfl_sync(0xffffffffu, slot, leader);
+    const unsigned m = __ballot_sync(0xffffffffu, live && slot == s);
+    if (live && slot == s) group = m;
+    rem &= ~m;
+  }
+  return group;
+}
+
+// Output position of every record: perm[position] = record. The record goes
+// to its base plus its rank among the earlier records of its cell with the
+// same direction, after the check that its old cell + d is the cell of its
+// key; the sorted records are then written by gather_kernel, whose stores
+// are coalesced (records that changed cell would otherwise each write
+// partial sectors of nine arrays).
+__global__ void __launch_bounds__(kBinnedThreads) binned_rank_kernel(Geom g, uint32_t n,
     const uint32_t* __restrict__ old_counts, const uint32_t* __restrict__ old_offsets,
-    const uint32_t* __restrict__ transfer, const uint8_t* __restrict__ code,
-    const double* __restrict__ irx, const double* __restrict__ iry, const double* __restrict__ irz,
-    const Vel* __restrict__ iu, const Vel* __restrict__ iv, const Vel* __restrict__ iw,
-    const double* __restrict__ iq, const int32_t* __restrict__ ikey, const uint64_t* __restrict__ iid,
-    double* __restrict__ orx, double* __restrict__ ory, double* __restrict__ orz,
-    Vel* __restrict__ ou, Vel* __restrict__ ov, Vel* __restrict__ ow, double* __restrict__ oq,
-    int32_t* __restrict__ okey, uint64_t* __restrict__ oid, BinnedState* state) {
-  __shared__ CellRun runs[kBinnedWarps];
-  __shared__ int32_t coords[kBinnedWarps][3][32];
+    const uint32_t* __restrict__ transfer, const uint16_t* __restrict__ code, const int32_t* __restrict__ keys,
+    uint32_t* __restrict__ perm, BinnedState* state) {
+  __shared__ uint32_t starts[kBinnedWarps][kRunCells];
   __shared__ uint32_t cursor[kBinnedWarps][27][33];
   if (state->fallback) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const long long cells = (long long)nx * ny * nz;
+  const long long runs = run_count(g);
   const unsigned below = (1u << lane) - 1u;
   bool bad = false;
-  CellRun& run = runs[warp];
-  for (long long u0 = ((long long)blockIdx.x * kBinnedWarps + warp) * 32; u0 < cells;
-       u0 += (long long)gridDim.x * kBinnedWarps * 32) {
-    int ci, cj, ck;
-    load_run(g, u0, cells, old_counts, old_offsets, run, ci, cj, ck);
-    coords[warp][0][lane] = ci;
-    coords[warp][1][lane] = cj;
-    coords[warp][2][lane] = ck;
-    if (u0 + lane < cells)
+  for (long long run = (long long)blockIdx.x * kBinnedWarps + warp; run < runs;
+       run += (long long)gridDim.x * kBinnedWarps) {
+    int i0, len, j, k;
+    run_cells(g, run, i0, len, j, k);
+    uint32_t begin, end;
+    load_run_bins(g, i0, len, j, k, old_counts, old_offsets, starts[warp], begin, end);
+    if (lane < len) {
+      const long long u = i0 + lane + (long long)nx * (j + (long long)ny * k);
 #pragma unroll
-      for (int d = 0; d < 27; ++d) cursor[warp][d][lane] = transfer[(long long)d * cells + u0 + lane];
+      for (int d = 0; d < 27; ++d) cursor[warp][d][lane] = transfer[(long long)d * cells + u];
+    }
     __syncwarp();
-    const uint32_t begin = run.begin, end = run.end;
-    // Software pipeline: the records of the next chunk are loaded while the
-    // current one is placed.
-    struct Rec {
-      double rx, ry, rz, q;
-      Vel u, v, w;
-      int32_t key;
-      uint64_t id;
-      int d;
-    };
-    auto load = [&](uint32_t p) {
-      Rec r{0, 0, 0, 0, Vel(0), Vel(0), Vel(0), 0, 0, 0};
-      if (p < end) {
-        r.rx = irx[p]; r.ry = iry[p]; r.rz = irz[p];
-        r.u = iu[p]; r.v = iv[p]; r.w = iw[p];
-        r.q = iq[p];
-        r.key = ikey[p];
-        if (oid) r.id = iid[p];
-        r.d = code[p];
+    // Four chunks per step: their loads are in flight together.
+    for (uint32_t p0 = begin; p0 < end; p0 += 128) {
+      uint16_t cd[4];
+      int32_t key[4];
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        const uint32_t p = p0 + 32 * m + lane;
+        cd[m] = p < end ? code[p] : kNoMove;
+        key[m] = p < end ? keys[p] : 0;
       }
-      return r;
-    };
-    Rec cur = load(begin + lane);
-    for (uint32_t p0 = begin; p0 < end; p0 += 32) {
-      const uint32_t p = p0 + lane;
-      const Rec nxt = load(p + 32);
-      bool live = p < end;
-      const int c = live ? run_cell(run, p) : 0;
-      const int d = cur.d;
-      if (live) {
-        // The record must land in the cell of its key: old cell + d.
-        int a = coords[warp][0][c] + (d % 3) - 1, b = coords[warp][1][c] + (d / 3) % 3 - 1,
-            e = coords[warp][2][c] + d / 9 - 1;
-        a = a < 0 ? a + nx : (a >= nx ? a - nx : a);
-        b = b < 0 ? b + ny : (b >= ny ? b - ny : b);
-        e = e < 0 ? e + nz : (e >= nz ? e - nz : e);
-        if (d >= 27 || g.encode(a, b, e) != cur.key) {
-          bad = true;
-          live = false;
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        if (p0 + 32 * m >= end) break;
+        const uint32_t p = p0 + 32 * m + lane;
+        bool live = p < end;
+        const int d = cd[m] & 31, c = (cd[m] >> 5) & 31;
+        if (live) {
+          // The record must land in the cell of its key: its old cell + d.
+          int a = i0 + c + (d % 3) - 1, b = j + (d / 3) % 3 - 1, e = k + d / 9 - 1;
+          a = a < 0 ? a + nx : (a >= nx ? a - nx : a);
+          b = b < 0 ? b + ny : (b >= ny ? b - ny : b);
+          e = e < 0 ? e + nz : (e >= nz ? e - nz : e);
+          if (cd[m] == kNoMove || d >= 27 || c >= len || g.encode(a, b, e) != key[m]) {
+            bad = true;
+            live = false;
+          }
         }
-      }
-      const int slot = live ? c * 27 + d : -1;
-      const unsigned peers = __match_any_sync(0xffffffffu, slot);
-      if (live) {
-        const uint32_t o = cursor[warp][d][c] + __popc(peers & below);
-        if (o < n) {
-          orx[o] = cur.rx; ory[o] = cur.ry; orz[o] = cur.rz;
-          ou[o] = cur.u; ov[o] = cur.v; ow[o] = cur.w;
-          oq[o] = cur.q;
-          okey[o] = cur.key;
-          if (oid) oid[o] = cur.id;
-        } else {
-          bad = true;
+        const unsigned group = slot_group(c * 27 + d, live);
+        if (live) {
+          const uint32_t o = cursor[warp][d][c] + __popc(group & below);
+          if (o < n) perm[o] = p;
+          else bad = true;
         }
+        __syncwarp();
+        if (live && lane == __ffs(group) - 1) cursor[warp][d][c] += __popc(group);
+        __syncwarp();
       }
-      __syncwarp();
-      if (live && lane == __ffs(peers) - 1) cursor[warp][d][c] += __popc(peers);
-      __syncwarp();
-      cur = nxt;
     }
   }
   if (__any_sync(0xffffffffu, bad) && lane == 0) atomicExch(&state->fallback, 1u);
@@ -765,13 +742,13 @@ size_t binned_scratch_words(const Geom& g) {
 
 bool binned_sort_applies(const Geom& g) { return g.nx >= 3 && g.ny >= 3 && g.nz >= 3; }
 
-BinnedScratch binned_scratch(const Geom& g, uint32_t* words, uint32_t* perm) {
+BinnedScratch binned_scratch(const Geom& g, uint32_t* words, uint16_t* codes) {
   BinnedScratch b;
   b.state = reinterpret_cast<BinnedState*>(words);  // 4 words, 8-byte aligned
   b.old_counts = words + 4;
   b.old_offsets = b.old_counts + g.bins;
   b.transfer = b.old_offsets + g.bins + 1;
-  b.code = reinterpret_cast<uint8_t*>(perm);
+  b.code = codes;
   return b;
 }
 
@@ -798,7 +775,7 @@ cudaError_t binned_validate(const Geom& g, const BinnedScratch& b, uint32_t n, c
   return cudaGetLastError();
 }
 
-cudaError_t binned_finish(int precision, const Geom& g, const BinnedScratch& b, bool classify,
+cudaError_t binned_finish(int precision, const Geom& g, const BinnedScratch& b, bool classify, bool materialize,
                           const tpicb200_particles* in, tpicb200_particles* out, uint32_t* counts,
                           uint32_t* offsets, uint32_t* cursor, uint32_t* perm, uint32_t* scan_scratch,
                           uint32_t* invalid, cudaStream_t s) {
@@ -806,8 +783,8 @@ cudaError_t binned_finish(int precision, const Geom& g, const BinnedScratch& b, 
   const long long cells = (long long)g.nx * g.ny * g.nz;
   const uint32_t n = in->count;
   out->count = n;
-  // One warp per run of 32 cells.
-  const unsigned runs_grid = grid_for((cells + 31) / 32 * 32, kBinnedThreads, 148u * 8u);
+  // One warp per run (up to 32 cells of an x-row).
+  const unsigned runs_grid = grid_for(run_count(g) * 32, kBinnedThreads, 148u * 8u);
   int launches = 0;
   if (classify) {
     classify_kernel<<<runs_grid, kBinnedThreads, 0, s>>>(g, in->cell, n, b.old_counts, b.old_offsets, b.transfer,
@@ -824,18 +801,26 @@ cudaError_t binned_finish(int precision, const Geom& g, const BinnedScratch& b, 
   scan_down_kernel<<<nblocks, kScanThreads, 0, s>>>(counts, bins, sc.block_sums, offsets, &b.state->fallback,
                                                     nullptr);
   binned_bases_kernel<<<grid_for(cells, 256, 148u * 16u), 256, 0, s>>>(g, offsets, b.transfer, b.state);
-  if (precision == TPICB200_PRECISION_DOUBLE)
-    binned_scatter_kernel<double><<<runs_grid, kBinnedThreads, 0, s>>>(g, n, b.old_counts, b.old_offsets,
-        b.transfer, b.code, (const double*)in->rx, (const double*)in->ry, (const double*)in->rz,
-        (const double*)in->u, (const double*)in->v, (const double*)in->w, in->q, in->cell, in->id,
-        (double*)out->rx, (double*)out->ry, (double*)out->rz, (double*)out->u, (double*)out->v, (double*)out->w,
-        out->q, out->cell, in->id ? out->id : nullptr, b.state);
-  else
-    binned_scatter_kernel<float><<<runs_grid, kBinnedThreads, 0, s>>>(g, n, b.old_counts, b.old_offsets,
-        b.transfer, b.code, (const double*)in->rx, (const double*)in->ry, (const double*)in->rz,
-        (const float*)in->u, (const float*)in->v, (const float*)in->w, in->q, in->cell, in->id,
-        (double*)out->rx, (double*)out->ry, (double*)out->rz, (float*)out->u, (float*)out->v, (float*)out->w,
-        out->q, out->cell, in->id ? out->id : nullptr, b.state);
+  binned_rank_kernel<<<runs_grid, kBinnedThreads, 0, s>>>(g, n, b.old_counts, b.old_offsets, b.transfer, b.code,
+                                                           in->cell, perm, b.state);
+  // The gather writes the records unless a check raised the fallback flag
+  // (without `materialize` the caller reads the records through perm).
+  if (n && materialize) {
+    const unsigned gb = grid_for(n, 256, 148u * 8u);
+    if (precision == TPICB200_PRECISION_DOUBLE)
+      gather_kernel<double><<<gb, 256, 0, s>>>(perm, n, (const double*)in->rx, (const double*)in->ry,
+          (const double*)in->rz, (const double*)in->u, (const double*)in->v, (const double*)in->w,
+          in->q, in->cell, in->id, (double*)out->rx, (double*)out->ry, (double*)out->rz,
+          (double*)out->u, (double*)out->v, (double*)out->w, out->q, out->cell,
+          in->id ? out->id : nullptr, &b.state->fallback, nullptr);
+    else
+      gather_kernel<float><<<gb, 256, 0, s>>>(perm, n, (const double*)in->rx, (const double*)in->ry,
+          (const double*)in->rz, (const float*)in->u, (const float*)in->v, (const float*)in->w,
+          in->q, in->cell, in->id, (double*)out->rx, (double*)out->ry, (double*)out->rz,
+          (float*)out->u, (float*)out->v, (float*)out->w, out->q, out->cell,
+          in->id ? out->id : nullptr, &b.state->fallback, nullptr);
+    ++launches;
+  }
   count_launches(launches + 6);
   if (cudaError_t e = cudaGetLastError(); e != cudaSuccess) return e;
   // General sort, gated on the fallback flag: it rewrites every output.
@@ -846,12 +831,13 @@ cudaError_t binned_finish(int precision, const Geom& g, const BinnedScratch& b, 
 cudaError_t launch_sort_binned(int precision, const Geom& g, const tpicb200_particles* in,
                                const uint32_t* in_counts, const uint32_t* in_offsets, tpicb200_particles* out,
                                uint32_t* counts, uint32_t* offsets, uint32_t* cursor, uint32_t* perm,
-                               uint32_t* scan_scratch, uint32_t* binned_words, uint32_t* invalid,
-                               cudaStream_t s) {
-  const BinnedScratch b = binned_scratch(g, binned_words, perm);
+                               uint32_t* scan_scratch, uint32_t* binned_words, uint16_t* codes,
+                               uint32_t* invalid, cudaStream_t s) {
+  const BinnedScratch b = binned_scratch(g, binned_words, codes);
   if (cudaError_t e = binned_begin(g, b, in_counts, in_offsets, false, s); e != cudaSuccess) return e;
   if (cudaError_t e = binned_validate(g, b, in->count, s); e != cudaSuccess) return e;
-  return binned_finish(precision, g, b, true, in, out, counts, offsets, cursor, perm, scan_scratch, invalid, s);
+  return binned_finish(precision, g, b, true, true, in, out, counts, offsets, cursor, perm, scan_scratch, invalid,
+                       s);
 }
 
 // ---- Sort without a context and without allocation ----
