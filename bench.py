@@ -300,6 +300,7 @@ def stage_kernel_times(sim, args, stream, repeats: int = 5) -> dict:
     lib, st = sim.lib, sim.state
     s_ = C.c_void_p(stream.cuda_stream)
     g = sim.case.grid
+    sim.materialize()  # the stage calls below take sorted live slots
     ns = st.ns
     vb = 4 if args.precision == "mixed" else 8
     fb = vb
@@ -387,6 +388,7 @@ def end_to_end(sim, args, stream, barrier, nparticles, world, dist) -> dict:
     fields) from pinned host memory, prepares, runs the cycles and reads the
     per-cycle energy reports back to the host."""
     import torch
+    sim.materialize()
     live = []
     for s in range(sim.state.ns):
         slot = sim.slots[s][sim.state.current[s]]

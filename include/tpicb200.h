@@ -154,6 +154,16 @@ typedef struct {
   void* mass;       /* mass records */
   double* e_theta;  /* solver node field */
   int mass_kind;    /* TPICB200_MASS_* */
+  /* Optional rank buffers (uint32, the slots' capacity; NULL: not used).
+   * With ranks[s] set, tpicb200_cycle leaves species s ranked (ranked[s]
+   * nonzero): the live slot holds the moved records in the order of the
+   * previous sort and ranks[s][p] is the live record at sorted position p of
+   * the bins counts/offsets; the next cycle's mover reads through the ranks
+   * and writes the moved records in that order into the idle slot, the sort
+   * only ranks, the deposition reads through the ranks. tpicb200_materialize
+   * writes the sorted records into the live slot (ranked[s] = 0). */
+  uint32_t* ranks[TPICB200_MAX_SPECIES];
+  int ranked[TPICB200_MAX_SPECIES];
 } tpicb200_state;
 
 typedef struct {
@@ -323,6 +333,11 @@ int tpicb200_energy(tpicb200_context* ctx, const void* e, const void* b_cell,
 /* Startup: B nodes from cells, the first sort and the bootstrap deposition
  * (docs/developer/architecture.md:161-171). */
 int tpicb200_prepare(tpicb200_context* ctx, tpicb200_state* state, tpicb200_stream stream);
+
+/* Sorted records of every ranked species: the live records are gathered
+ * through their ranks into the idle slot, which becomes live (ranked[s] = 0).
+ * A no-op for species that are not ranked. */
+int tpicb200_materialize(tpicb200_context* ctx, tpicb200_state* state, tpicb200_stream stream);
 
 /* ncycles ECSIM cycles: solve; per species the mover (old B) and the sort
  * of the moved records (the mover emits the direction codes the binned sort

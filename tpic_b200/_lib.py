@@ -57,7 +57,8 @@ class State(C.Structure):
                 ("counts", C.c_void_p * MAX_SPECIES), ("offsets", C.c_void_p * MAX_SPECIES),
                 ("e", C.c_void_p), ("b_cell", C.c_void_p), ("b_node", C.c_void_p),
                 ("b_cell_next", C.c_void_p), ("b_node_next", C.c_void_p), ("j", C.c_void_p),
-                ("mass", C.c_void_p), ("e_theta", C.c_void_p), ("mass_kind", C.c_int)]
+                ("mass", C.c_void_p), ("e_theta", C.c_void_p), ("mass_kind", C.c_int),
+                ("ranks", C.c_void_p * MAX_SPECIES), ("ranked", C.c_int * MAX_SPECIES)]
 
 
 class CycleReport(C.Structure):
@@ -97,6 +98,7 @@ EXPORTS = {
     "tpicb200_energy": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(Particles),
                                   C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_double), C.c_void_p]),
     "tpicb200_prepare": (C.c_int, [C.c_void_p, C.POINTER(State), C.c_void_p]),
+    "tpicb200_materialize": (C.c_int, [C.c_void_p, C.POINTER(State), C.c_void_p]),
     "tpicb200_cycle": (C.c_int, [C.c_void_p, C.POINTER(State), C.c_int, C.POINTER(CycleReport), C.c_void_p]),
 }
 

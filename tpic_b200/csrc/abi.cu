@@ -202,8 +202,8 @@ int tpicb200_mover(tpicb200_context* ctx, double qom, tpicb200_particles* p, con
     return fail(TPICB200_INVALID_ARGUMENT, "mover needs E_theta, B nodes and a finite q/m");
   const double beta = qom * ctx->opt.dt / 2;
   if (!std::isfinite(beta)) return fail(TPICB200_OVERFLOW, "q/m*dt/2 is not finite");
-  return cuda_status(launch_mover(ctx->opt.precision, ctx->g, qom, ctx->opt.dt, ctx->opt.c, p, e_theta,
-                                  b_node, invalid_or_own(ctx, invalid), nullptr, (cudaStream_t)stream),
+  return cuda_status(launch_mover(ctx->opt.precision, ctx->g, qom, ctx->opt.dt, ctx->opt.c, p, nullptr, nullptr,
+                                  e_theta, b_node, invalid_or_own(ctx, invalid), nullptr, (cudaStream_t)stream),
                      "mover launch failed");
 }
 
@@ -476,16 +476,30 @@ static int check_state(tpicb200_context* ctx, tpicb200_state* st) {
   return TPICB200_SUCCESS;
 }
 
-// The mover of species sp on its live slot, then the sort of the moved
-// records into the idle slot; `moved` and `sorted` are recorded after each.
-// On grids whose extents are all at least 3 the mover emits direction codes
-// and transfer counts and the binned sort ranks the records by them: perm
-// receives the ranks (sorted position -> record of the live slot) and the
-// sorted records are left for the deposition to write (*deferred = true);
-// otherwise the general sort writes them (*deferred = false). The caller
-// flips the live slot once the idle slot holds the sorted records.
+// How the deposition reads a species after move_and_sort, and whether the
+// live slot flips after it.
+struct DepositPlan {
+  const tpicb200_particles* read;  // records the deposition reads
+  SortedCopy copy;                 // through which ranks, and where to write them sorted
+  bool flip;                       // the idle slot becomes live after the deposition
+};
+
+// The mover of species sp, then the sort of the moved records;
+// `moved` and `sorted` are recorded after each. On grids whose extents are
+// all at least 3 the mover emits direction codes and transfer counts and the
+// binned sort ranks the records by them:
+//  - a species with a rank buffer (state.ranks) is moved out of place: the
+//    mover reads the live records through the previous ranks (when ranked)
+//    and writes the moved records in the previous sorted order into the idle
+//    slot, which becomes live; the new ranks go to the rank buffer and the
+//    species stays ranked (the deposition reads through the ranks);
+//  - otherwise the mover moves in place, the ranks go to `perm`, and the
+//    deposition reads through them and writes the sorted records into the
+//    idle slot.
+// On smaller grids the mover moves in place and the general sort writes the
+// sorted records.
 static int move_and_sort(tpicb200_context* ctx, tpicb200_state* st, int sp, uint32_t* perm, cudaEvent_t moved,
-                         cudaEvent_t sorted, bool* deferred, cudaStream_t s) {
+                         cudaEvent_t sorted, DepositPlan* plan, cudaStream_t s) {
   const int cur = st->current[sp];
   tpicb200_particles* in = &st->slot[sp][cur];
   tpicb200_particles* out = &st->slot[sp][1 - cur];
@@ -497,54 +511,69 @@ static int move_and_sort(tpicb200_context* ctx, tpicb200_state* st, int sp, uint
     return fail(TPICB200_INVALID_ARGUMENT, "null attribute in the idle slot");
   if (in->count && (in->rx == out->rx || in->cell == out->cell))
     return fail(TPICB200_INVALID_ARGUMENT, "live and idle slots alias");
+  out->count = in->count;
   const int p = ctx->opt.precision;
+  const tpicb200_particles none{};
   if (!binned_sort_applies(ctx->g)) {
-    cudaError_t e = launch_mover(p, ctx->g, qom, ctx->opt.dt, ctx->opt.c, in, st->e_theta, st->b_node, ctx->invalid,
-                                 nullptr, s);
+    if (st->ranked[sp]) return fail(TPICB200_INVALID_STATE, "ranked species on a grid without the binned sort");
+    cudaError_t e = launch_mover(p, ctx->g, qom, ctx->opt.dt, ctx->opt.c, in, nullptr, nullptr, st->e_theta,
+                                 st->b_node, ctx->invalid, nullptr, s);
     if (e == cudaSuccess) e = cudaEventRecord(moved, s);
     if (e == cudaSuccess)
       e = launch_sort(p, ctx->g, in, out, st->counts[sp], st->offsets[sp], ctx->cursor, perm, ctx->scan,
                       ctx->invalid, s);
     if (e == cudaSuccess) e = cudaEventRecord(sorted, s);
     if (e != cudaSuccess) return cuda_status(e, "mover or sort launch failed");
-    *deferred = false;
+    *plan = DepositPlan{out, SortedCopy{nullptr, none}, true};
     return TPICB200_SUCCESS;
   }
   const BinnedScratch b = binned_scratch(ctx->g, ctx->binned, ctx->codes);
   cudaError_t e = binned_begin(ctx->g, b, st->counts[sp], st->offsets[sp], true, s);
   if (e == cudaSuccess) e = binned_validate(ctx->g, b, in->count, s);
+  const bool ranks = st->ranks[sp] != nullptr;
+  if (ranks) {
+    // Out of place: the moved records, in the previous sorted order, go live.
+    if (e == cudaSuccess)
+      e = launch_mover(p, ctx->g, qom, ctx->opt.dt, ctx->opt.c, in, out, st->ranked[sp] ? st->ranks[sp] : nullptr,
+                       st->e_theta, st->b_node, ctx->invalid, &b, s);
+    if (e == cudaSuccess) e = cudaEventRecord(moved, s);
+    if (e == cudaSuccess)
+      e = binned_finish(p, ctx->g, b, false, false, out, in, st->counts[sp], st->offsets[sp], ctx->cursor,
+                        st->ranks[sp], ctx->scan, ctx->invalid, s);
+    if (e == cudaSuccess) e = cudaEventRecord(sorted, s);
+    if (e != cudaSuccess) return cuda_status(e, "mover or binned sort launch failed");
+    st->current[sp] = 1 - cur;
+    st->ranked[sp] = 1;
+    *plan = DepositPlan{out, SortedCopy{st->ranks[sp], none}, false};
+    return TPICB200_SUCCESS;
+  }
+  if (st->ranked[sp]) return fail(TPICB200_INVALID_STATE, "ranked species without a rank buffer");
   if (e == cudaSuccess)
-    e = launch_mover(p, ctx->g, qom, ctx->opt.dt, ctx->opt.c, in, st->e_theta, st->b_node, ctx->invalid, &b, s);
+    e = launch_mover(p, ctx->g, qom, ctx->opt.dt, ctx->opt.c, in, nullptr, nullptr, st->e_theta, st->b_node,
+                     ctx->invalid, &b, s);
   if (e == cudaSuccess) e = cudaEventRecord(moved, s);
   if (e == cudaSuccess)
     e = binned_finish(p, ctx->g, b, false, false, in, out, st->counts[sp], st->offsets[sp], ctx->cursor, perm,
                       ctx->scan, ctx->invalid, s);
   if (e == cudaSuccess) e = cudaEventRecord(sorted, s);
   if (e != cudaSuccess) return cuda_status(e, "mover or binned sort launch failed");
-  *deferred = true;
+  *plan = DepositPlan{in, SortedCopy{perm, *out}, true};
   return TPICB200_SUCCESS;
 }
 
-// Deposition of species [first, first + count) (at most two) from their
-// live slots after move_and_sort: deferred sorts are completed here (the
-// records are read through the ranks and written sorted into the idle slot),
-// then every species of the pair flips to its idle slot.
-static int deposit_pair(tpicb200_context* ctx, tpicb200_state* st, int first, int count, uint32_t* const* perms,
-                        const bool* deferred, bool accumulate, cudaStream_t s) {
+// Deposition of species [first, first + count) (at most two) after
+// move_and_sort, as their plans say; then the planned slot flips.
+static int deposit_pair(tpicb200_context* ctx, tpicb200_state* st, int first, int count, const DepositPlan* plan,
+                        bool accumulate, cudaStream_t s) {
   const tpicb200_particles* parts[2];
   const uint32_t* counts[2];
   const uint32_t* offsets[2];
-  SortedCopy copy[2];
   const SortedCopy* copies[2];
   double qom[2];
   for (int i = 0; i < count; ++i) {
     const int sp = first + i;
-    const int cur = st->current[sp];
-    // A deferred sort: read the moved records (live slot) through the ranks.
-    // Otherwise the idle slot already holds the sorted records: read it in place.
-    parts[i] = deferred[i] ? &st->slot[sp][cur] : &st->slot[sp][1 - cur];
-    copy[i] = SortedCopy{deferred[i] ? perms[i] : nullptr, st->slot[sp][1 - cur]};
-    copies[i] = &copy[i];
+    parts[i] = plan[i].read;
+    copies[i] = &plan[i].copy;
     counts[i] = st->counts[sp];
     offsets[i] = st->offsets[sp];
     qom[i] = st->qom[sp];
@@ -566,7 +595,27 @@ static int deposit_pair(tpicb200_context* ctx, tpicb200_state* st, int first, in
   }
   for (int i = 0; i < count && e == cudaSuccess; ++i) e = launch_copy_ids(parts[i], copies[i], s);
   if (e != cudaSuccess) return cuda_status(e, "deposition launch failed");
-  for (int i = 0; i < count; ++i) st->current[first + i] = 1 - st->current[first + i];
+  for (int i = 0; i < count; ++i)
+    if (plan[i].flip) st->current[first + i] = 1 - st->current[first + i];
+  return TPICB200_SUCCESS;
+}
+
+int tpicb200_materialize(tpicb200_context* ctx, tpicb200_state* st, tpicb200_stream stream) {
+  if (int s = check_ctx(ctx)) return s;
+  if (int r = check_state(ctx, st)) return r;
+  for (int sp = 0; sp < st->ns; ++sp) {
+    if (!st->ranked[sp]) continue;
+    if (!st->ranks[sp]) return fail(TPICB200_INVALID_STATE, "ranked species without a rank buffer");
+    const int cur = st->current[sp];
+    tpicb200_particles* in = &st->slot[sp][cur];
+    tpicb200_particles* out = &st->slot[sp][1 - cur];
+    if (int r = check_particles(ctx, in)) return r;
+    if (int r = cuda_status(launch_sorted_gather(ctx->opt.precision, st->ranks[sp], in, out, (cudaStream_t)stream),
+                            "materialize gather failed"))
+      return r;
+    st->current[sp] = 1 - cur;
+    st->ranked[sp] = 0;
+  }
   return TPICB200_SUCCESS;
 }
 
@@ -576,6 +625,7 @@ int tpicb200_prepare(tpicb200_context* ctx, tpicb200_state* st, tpicb200_stream 
   cudaStream_t s = (cudaStream_t)stream;
   if (int r = tpicb200_magnetic_to_nodes(ctx, st->b_cell, st->b_node, stream)) return r;
   if (int r = sort_all(ctx, st, s)) return r;
+  for (int sp = 0; sp < st->ns; ++sp) st->ranked[sp] = 0;
   return deposit_all(ctx, st, st->b_node, s);
 }
 
@@ -615,12 +665,12 @@ int tpicb200_cycle(tpicb200_context* ctx, tpicb200_state* st, int ncycles, tpicb
     if (int r = tpicb200_clear_moments(ctx, st->j, st->mass, stream)) return r;
     for (int first = 0; first < st->ns; first += 2) {
       const int count = st->ns - first < 2 ? st->ns - first : 2;
-      bool deferred[2] = {false, false};
+      DepositPlan plan[2];
       for (int i = 0; i < count; ++i)
         if (int r = move_and_sort(ctx, st, first + i, perms[i], sev[3 * (first + i)], sev[3 * (first + i) + 1],
-                                  &deferred[i], s))
+                                  &plan[i], s))
           return r;
-      if (int r = deposit_pair(ctx, st, first, count, perms, deferred, first > 0, s)) return r;
+      if (int r = deposit_pair(ctx, st, first, count, plan, first > 0, s)) return r;
       cudaEventRecord(sev[3 * first + 2], s);
     }
     if (int r = tpicb200_fold_periodic(ctx, st->j, st->mass, stream)) return r;

@@ -193,7 +193,7 @@ __global__ void __launch_bounds__(128) sorted_deposit_kernel(Geom g, DepositPara
         const uint32_t pos = first + offset;
         const uint32_t n = perm ? perm[pos] : pos;
         const double fx = rx[n], fy = ry[n], fz = rz[n];
-        if (perm) {
+        if (orx) {
           orx[pos] = fx; ory[pos] = fy; orz[pos] = fz;
           ou[pos] = u[n]; ov[pos] = v[n]; ow[pos] = w[n];
           oq[pos] = q[n]; okey[pos] = key[n];
@@ -384,10 +384,10 @@ cudaError_t launch_typed(const Geom& g, DepositParams dp, const tpicb200_particl
   if (counts && offsets) {
     const long long cells = (long long)g.nx * g.ny * g.nz;
     const unsigned blocks = grid_for((cells + 3) / 4, 1, 148u * 64u);
-    const bool c = copy && copy->perm;
+    const bool c = copy && copy->perm && copy->out.rx;
     sorted_deposit_kernel<P, MC><<<blocks, 128, 0, s>>>(g, dp, (const double*)p->rx, (const double*)p->ry,
         (const double*)p->rz, (const Vel*)p->u, (const Vel*)p->v, (const Vel*)p->w, p->q, p->cell,
-        counts, offsets, (const Fld*)bnode, (Fld*)j, (Mass*)mass, invalid, c ? copy->perm : nullptr,
+        counts, offsets, (const Fld*)bnode, (Fld*)j, (Mass*)mass, invalid, copy ? copy->perm : nullptr,
         c ? (double*)copy->out.rx : nullptr, c ? (double*)copy->out.ry : nullptr,
         c ? (double*)copy->out.rz : nullptr, c ? (Vel*)copy->out.u : nullptr, c ? (Vel*)copy->out.v : nullptr,
         c ? (Vel*)copy->out.w : nullptr, c ? copy->out.q : nullptr, c ? copy->out.cell : nullptr);
@@ -426,7 +426,7 @@ __global__ void __launch_bounds__(256) copy_ids_kernel(const uint32_t* __restric
 }  // namespace
 
 cudaError_t launch_copy_ids(const tpicb200_particles* in, const SortedCopy* copy, cudaStream_t s) {
-  if (!copy || !copy->perm || !in->id || !copy->out.id || in->count == 0) return cudaSuccess;
+  if (!copy || !copy->perm || !copy->out.rx || !in->id || !copy->out.id || in->count == 0) return cudaSuccess;
   copy_ids_kernel<<<grid_for(in->count, 256, 148u * 8u), 256, 0, s>>>(copy->perm, in->id, copy->out.id, in->count);
   count_launches(1);
   return cudaGetLastError();

@@ -12,9 +12,12 @@ void count_launches(unsigned n);
 struct BinnedScratch;
 // With `binned`, the mover also writes direction codes and transfer counts
 // for binned_finish (after binned_begin with zeroed transfer counts).
+// out (null: in place) receives the moved records, read through ranks when
+// given (position p of out <- record ranks[p] of p).
 cudaError_t launch_mover(int precision, const Geom& g, double qom, double dt, double c,
-                         tpicb200_particles* p, const double* theta, const void* bnode,
-                         uint32_t* invalid, const BinnedScratch* binned, cudaStream_t s);
+                         tpicb200_particles* p, tpicb200_particles* out, const uint32_t* ranks,
+                         const double* theta, const void* bnode, uint32_t* invalid, const BinnedScratch* binned,
+                         cudaStream_t s);
 
 // sort.cu: scratch needs `bins` cursor words, `capacity` permutation words and
 // the scan workspace returned by sort_scan_words().
@@ -70,10 +73,10 @@ cudaError_t launch_sort_static(int precision, const Geom& g, const tpicb200_part
                                uint32_t* counts, uint32_t* offsets, uint32_t* invalid, uint32_t* scratch,
                                cudaStream_t s);
 
-// The sort's gather fused into the deposition: records are read through
-// perm (sorted position -> record of the read slot) and written at their
-// sorted positions into `out` as they are read. perm == nullptr: the
-// records are read in place, in sorted order, and nothing is written.
+// Records read through perm (sorted position -> record of the read slot;
+// null: read in place, in sorted order). With out.rx set, each record is
+// also written at its sorted position into `out` (the sort's gather fused
+// into the deposition).
 struct SortedCopy {
   const uint32_t* perm;
   tpicb200_particles out;
@@ -81,6 +84,10 @@ struct SortedCopy {
 // Writes out.id[p] = in.id[perm[p]] for the records a fused deposition
 // copied (the deposition kernels copy every other attribute).
 cudaError_t launch_copy_ids(const tpicb200_particles* in, const SortedCopy* copy, cudaStream_t s);
+
+// Sorted records: out[p] = in[perm[p]] for every attribute (ids included).
+cudaError_t launch_sorted_gather(int precision, const uint32_t* perm, const tpicb200_particles* in,
+                                 tpicb200_particles* out, cudaStream_t s);
 
 // deposit.cu
 cudaError_t launch_deposit(int precision, int mass_kind, const Geom& g, double qom, double dt,

@@ -306,7 +306,7 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_deposit_kernel(Geom g, TcP
       if (rec.present) {
         // The sorted copy of the record, when the sort left it to this pass.
         const TcSpecies& sp = rec.second ? tp.sp[1] : tp.sp[0];
-        if (sp.perm) {
+        if (sp.orx) {
           const uint32_t o = rec.pos;
           sp.orx[o] = rec.fx; sp.ory[o] = rec.fy; sp.orz[o] = rec.fz;
           sp.ou[o] = rec.u; sp.ov[o] = rec.v; sp.ow[o] = rec.w;
@@ -566,11 +566,11 @@ cudaError_t launch_deposit_tc(int mass_kind, const Geom& g, int ns, const double
     for (int i = 0; i < tp.ns; ++i) {
       const tpicb200_particles* sp = p[first + i];
       const SortedCopy* cp = copies ? copies[first + i] : nullptr;
-      const bool copy = cp && cp->perm;
+      const bool copy = cp && cp->perm && cp->out.rx;
       tp.sp[i] = TcSpecies{(const double*)sp->rx, (const double*)sp->ry, (const double*)sp->rz,
                            (const float*)sp->u, (const float*)sp->v, (const float*)sp->w, sp->q, sp->cell,
                            counts[first + i], offsets[first + i], float(qom[first + i] * dt / 2 / c),
-                           copy ? cp->perm : nullptr, copy ? (double*)cp->out.rx : nullptr,
+                           cp ? cp->perm : nullptr, copy ? (double*)cp->out.rx : nullptr,
                            copy ? (double*)cp->out.ry : nullptr, copy ? (double*)cp->out.rz : nullptr,
                            copy ? (float*)cp->out.u : nullptr, copy ? (float*)cp->out.v : nullptr,
                            copy ? (float*)cp->out.w : nullptr, copy ? cp->out.q : nullptr,

@@ -7,7 +7,10 @@
 // reference's expressions evaluate under strict IEEE rules, so new fractions,
 // velocities and cell keys are bit-identical to the CPU oracle.
 //
-// Two kernels share one push:
+// Two kernels share one push. Each moves record n of the read slot into
+// position p of the written slot: in place (n = p), or, for a ranked
+// species, n = ranks[p] of the previous sort into the other slot, which then
+// holds the moved records in the previous sorted order.
 //  - mover_kernel, one thread per record, gathers the 48 field values of a
 //    record from global memory (they hit L1/L2 because records are sorted);
 //  - run_mover_kernel, for records grouped by the bins of the previous sort
@@ -53,9 +56,30 @@ struct Records {
   typename P::Vel* __restrict__ u;
   typename P::Vel* __restrict__ v;
   typename P::Vel* __restrict__ w;
-  const double* __restrict__ q;
+  double* __restrict__ q;
   int32_t* __restrict__ key;
+  uint64_t* __restrict__ id;
 };
+
+// Where the movers read and write: record n of `in` (n = ranks[p] when
+// ranks are given, else p) is moved into position p of `out`; with out ==
+// in and no ranks the move is in place.
+template <class P>
+struct MoveIo {
+  Records<P> in, out;
+  const uint32_t* __restrict__ ranks;
+  bool copy;  // out is another slot: every attribute is written
+};
+
+// A record that is not moved (invalid) is copied unchanged by a copying mover.
+template <class P>
+__device__ __forceinline__ void copy_record(const MoveIo<P>& io, uint32_t n, uint32_t p) {
+  if (!io.copy) return;
+  io.out.rx[p] = io.in.rx[n]; io.out.ry[p] = io.in.ry[n]; io.out.rz[p] = io.in.rz[n];
+  io.out.u[p] = io.in.u[n]; io.out.v[p] = io.in.v[n]; io.out.w[p] = io.in.w[n];
+  io.out.q[p] = io.in.q[n]; io.out.key[p] = io.in.key[n];
+  if (io.out.id) io.out.id[p] = io.in.id[n];
+}
 
 // Corner values from global memory: node box of cell (ci, cj, ck).
 template <class P>
@@ -94,9 +118,10 @@ __device__ __forceinline__ C gather8(const F& field, int which, int c, const C w
 // from its key. Returns the direction code of the move (-1: invalid, or a
 // move beyond the 27 neighbouring cells when Coded).
 template <class P, bool Coded, class F>
-__device__ __forceinline__ int push(const Geom& g, const MoverParams<P>& mp, const Records<P>& r, uint32_t n,
-                                    int ci, int cj, int ck, typename P::Pos fx, typename P::Pos fy,
-                                    typename P::Pos fz, const F& field, uint32_t* invalid) {
+__device__ __forceinline__ int push(const Geom& g, const MoverParams<P>& mp, const MoveIo<P>& io, uint32_t n,
+                                    uint32_t p, int ci, int cj, int ck, typename P::Pos fx, typename P::Pos fy,
+                                    typename P::Pos fz, double charge, const F& field, uint32_t* invalid) {
+  const Records<P>& r = io.in;
   using C = typename P::VC;
   using Pos = typename P::Pos;
   using Vel = typename P::Vel;
@@ -135,6 +160,7 @@ __device__ __forceinline__ int push(const Geom& g, const MoverParams<P>& mp, con
   }
   if (!ok) {
     atomicAdd(invalid, 1u);
+    copy_record(io, n, p);
     return -1;
   }
 #pragma unroll
@@ -145,9 +171,14 @@ __device__ __forceinline__ int push(const Geom& g, const MoverParams<P>& mp, con
       cell[axis] = m < 0 ? m + e : m;
     }
   }
-  r.key[n] = g.encode(int(cell[0]), int(cell[1]), int(cell[2]));
-  r.rx[n] = frac[0]; r.ry[n] = frac[1]; r.rz[n] = frac[2];
-  r.u[n] = vel[0]; r.v[n] = vel[1]; r.w[n] = vel[2];
+  const Records<P>& o = io.out;
+  o.key[p] = g.encode(int(cell[0]), int(cell[1]), int(cell[2]));
+  o.rx[p] = frac[0]; o.ry[p] = frac[1]; o.rz[p] = frac[2];
+  o.u[p] = vel[0]; o.v[p] = vel[1]; o.w[p] = vel[2];
+  if (io.copy) {
+    o.q[p] = charge;
+    if (o.id) o.id[p] = r.id[n];
+  }
   return Coded ? move_code(g, ci, cj, ck, int(cell[0]), int(cell[1]), int(cell[2])) : 0;
 }
 
@@ -198,19 +229,24 @@ __device__ __forceinline__ void record_codes(const MoveCodes& mc, bool live, uin
 // One thread per record. With a gate, the kernel runs only when *gate != 0.
 template <class P>
 __global__ void __launch_bounds__(256, TPICB200_MOVER_MIN_BLOCKS) mover_kernel(Geom g, MoverParams<P> mp,
-    Records<P> r, uint32_t count, const double* __restrict__ theta, const typename P::Fld* __restrict__ bnode,
+    MoveIo<P> io, uint32_t count, const double* __restrict__ theta, const typename P::Fld* __restrict__ bnode,
     uint32_t* __restrict__ invalid, const uint32_t* gate) {
   using Pos = typename P::Pos;
   if (gate && *gate == 0) return;
-  for (uint32_t n = blockIdx.x * blockDim.x + threadIdx.x; n < count; n += gridDim.x * blockDim.x) {
+  const Records<P>& r = io.in;
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < count; p += gridDim.x * blockDim.x) {
+    const uint32_t n = io.ranks ? io.ranks[p] : p;
     const int32_t k0 = r.key[n];
     const double charge = r.q[n];
     const Pos fx = r.rx[n], fy = r.ry[n], fz = r.rz[n];
     int ci, cj, ck;
-    if (record_ok<P>(g, k0, charge, fx, fy, fz, ci, cj, ck))
-      push<P, false>(g, mp, r, n, ci, cj, ck, fx, fy, fz, global_fields<P>(g, theta, bnode, ci, cj, ck), invalid);
-    else
+    if (record_ok<P>(g, k0, charge, fx, fy, fz, ci, cj, ck)) {
+      push<P, false>(g, mp, io, n, p, ci, cj, ck, fx, fy, fz, charge, global_fields<P>(g, theta, bnode, ci, cj, ck),
+                     invalid);
+    } else {
       atomicAdd(invalid, 1u);
+      copy_record(io, n, p);
+    }
   }
 }
 
@@ -221,7 +257,7 @@ constexpr int kRunWarps = 4;
 
 template <class P>
 __global__ void __launch_bounds__(kRunWarps * 32, 2 * TPICB200_MOVER_MIN_BLOCKS) run_mover_kernel(Geom g,
-    MoverParams<P> mp, Records<P> r, uint32_t count, const double* __restrict__ theta,
+    MoverParams<P> mp, MoveIo<P> io, uint32_t count, const double* __restrict__ theta,
     const typename P::Fld* __restrict__ bnode, const uint32_t* __restrict__ old_counts,
     const uint32_t* __restrict__ old_offsets, uint32_t* __restrict__ invalid, MoveCodes mc) {
   using C = typename P::VC;
@@ -256,31 +292,34 @@ __global__ void __launch_bounds__(kRunWarps * 32, 2 * TPICB200_MOVER_MIN_BLOCKS)
       sf[rest * kRunNodes + x] = which ? C(__ldg(theta + at)) : C(__ldg(bnode + at));
     }
     __syncwarp();
+    const Records<P>& r = io.in;
     for (uint32_t p0 = begin; p0 < end; p0 += 32) {
-      const uint32_t n = p0 + lane;
-      const bool live = n < end;
+      const uint32_t p = p0 + lane;  // position in the sorted order of the bins
+      const bool live = p < end;
       long long old_cell = 0;
       int d = -1, c = 0;
       if (live) {
+        const uint32_t n = io.ranks ? io.ranks[p] : p;
         const int32_t k0 = r.key[n];
         const double charge = r.q[n];
         const Pos fx = r.rx[n], fy = r.ry[n], fz = r.rz[n];
 #pragma unroll
         for (int step = 16; step > 0; step >>= 1)
-          if (st[c + step] <= n) c += step;
+          if (st[c + step] <= p) c += step;
         int ci, cj, ck;
         if (record_ok<P>(g, k0, charge, fx, fy, fz, ci, cj, ck)) {
           if (ci == i0 + c && cj == j && ck == k)
-            d = push<P, true>(g, mp, r, n, ci, cj, ck, fx, fy, fz, SharedFields<C>{sf, c}, invalid);
+            d = push<P, true>(g, mp, io, n, p, ci, cj, ck, fx, fy, fz, charge, SharedFields<C>{sf, c}, invalid);
           else
-            d = push<P, true>(g, mp, r, n, ci, cj, ck, fx, fy, fz, global_fields<P>(g, theta, bnode, ci, cj, ck),
-                              invalid);
+            d = push<P, true>(g, mp, io, n, p, ci, cj, ck, fx, fy, fz, charge,
+                              global_fields<P>(g, theta, bnode, ci, cj, ck), invalid);
           old_cell = ci + (long long)g.nx * (cj + (long long)g.ny * ck);
         } else {
           atomicAdd(invalid, 1u);
+          copy_record(io, n, p);
         }
       }
-      record_codes(mc, live, n, d, c, old_cell);
+      record_codes(mc, live, p, d, c, old_cell);
     }
     __syncwarp();
   }
@@ -298,22 +337,22 @@ MoverParams<P> mover_params(const Geom& g, double qom, double dt, double c) {
 }
 
 template <class P>
-Records<P> records(tpicb200_particles* p) {
+Records<P> records(const tpicb200_particles* p) {
   return Records<P>{(typename P::Pos*)p->rx, (typename P::Pos*)p->ry, (typename P::Pos*)p->rz,
-                    (typename P::Vel*)p->u, (typename P::Vel*)p->v, (typename P::Vel*)p->w, p->q, p->cell};
+                    (typename P::Vel*)p->u, (typename P::Vel*)p->v, (typename P::Vel*)p->w, p->q, p->cell, p->id};
 }
 
 template <class P>
-cudaError_t launch(const Geom& g, double qom, double dt, double c, tpicb200_particles* p,
-                   const double* theta, const void* bnode, uint32_t* invalid, const BinnedScratch* binned,
-                   cudaStream_t s) {
+cudaError_t launch(const Geom& g, double qom, double dt, double c, tpicb200_particles* p, tpicb200_particles* out,
+                   const uint32_t* ranks, const double* theta, const void* bnode, uint32_t* invalid,
+                   const BinnedScratch* binned, cudaStream_t s) {
   const MoverParams<P> mp = mover_params<P>(g, qom, dt, c);
   if (p->count == 0) return cudaSuccess;
   const unsigned blocks = grid_for(p->count, 256, 148u * 8u);
-  const Records<P> r = records<P>(p);
+  const MoveIo<P> io{records<P>(p), records<P>(out ? out : p), ranks, out != nullptr && out != p};
   const auto* bn = (const typename P::Fld*)bnode;
   if (!binned) {
-    mover_kernel<P><<<blocks, 256, 0, s>>>(g, mp, r, p->count, theta, bn, invalid, nullptr);
+    mover_kernel<P><<<blocks, 256, 0, s>>>(g, mp, io, p->count, theta, bn, invalid, nullptr);
     count_launches(1);
     return cudaGetLastError();
   }
@@ -324,8 +363,8 @@ cudaError_t launch(const Geom& g, double qom, double dt, double c, tpicb200_part
                (long long)g.nx * g.ny * g.nz};
   const long long runs = run_count(g);
   run_mover_kernel<P><<<grid_for(runs * 32, kRunWarps * 32, 148u * 8u), kRunWarps * 32, 0, s>>>(
-      g, mp, r, p->count, theta, bn, binned->old_counts, binned->old_offsets, invalid, mc);
-  mover_kernel<P><<<blocks, 256, 0, s>>>(g, mp, r, p->count, theta, bn, invalid, &binned->state->bins_bad);
+      g, mp, io, p->count, theta, bn, binned->old_counts, binned->old_offsets, invalid, mc);
+  mover_kernel<P><<<blocks, 256, 0, s>>>(g, mp, io, p->count, theta, bn, invalid, &binned->state->bins_bad);
   count_launches(2);
   return cudaGetLastError();
 }
@@ -333,11 +372,12 @@ cudaError_t launch(const Geom& g, double qom, double dt, double c, tpicb200_part
 }  // namespace
 
 cudaError_t launch_mover(int precision, const Geom& g, double qom, double dt, double c,
-                         tpicb200_particles* p, const double* theta, const void* bnode,
-                         uint32_t* invalid, const BinnedScratch* binned, cudaStream_t s) {
+                         tpicb200_particles* p, tpicb200_particles* out, const uint32_t* ranks,
+                         const double* theta, const void* bnode, uint32_t* invalid, const BinnedScratch* binned,
+                         cudaStream_t s) {
   if (precision == TPICB200_PRECISION_DOUBLE)
-    return launch<PDouble>(g, qom, dt, c, p, theta, bnode, invalid, binned, s);
-  return launch<PMixed>(g, qom, dt, c, p, theta, bnode, invalid, binned, s);
+    return launch<PDouble>(g, qom, dt, c, p, out, ranks, theta, bnode, invalid, binned, s);
+  return launch<PMixed>(g, qom, dt, c, p, out, ranks, theta, bnode, invalid, binned, s);
 }
 
 }  // namespace tpicb200

@@ -321,7 +321,7 @@ __global__ void __launch_bounds__(256) gather_kernel(const uint32_t* __restrict_
     double* __restrict__ orx, double* __restrict__ ory, double* __restrict__ orz,
     Vel* __restrict__ ou, Vel* __restrict__ ov, Vel* __restrict__ ow, double* __restrict__ oq,
     int32_t* __restrict__ okey, uint64_t* __restrict__ oid, const uint32_t* flag, const uint32_t* gate) {
-  if (closed(gate) || *flag) return;
+  if (closed(gate) || (flag && *flag)) return;
   for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < count; p += gridDim.x * blockDim.x) {
     const uint32_t s = perm[p];
     orx[p] = irx[s]; ory[p] = iry[s]; orz[p] = irz[s];
@@ -733,6 +733,27 @@ cudaError_t launch_sort(int precision, const Geom& g, const tpicb200_particles* 
                         uint32_t* invalid, cudaStream_t s) {
   out->count = in->count;
   return enqueue_general(precision, g, in, out, counts, offsets, cursor, perm, scan_scratch, invalid, nullptr, s);
+}
+
+cudaError_t launch_sorted_gather(int precision, const uint32_t* perm, const tpicb200_particles* in,
+                                 tpicb200_particles* out, cudaStream_t s) {
+  const uint32_t n = in->count;
+  out->count = n;
+  if (!n) return cudaSuccess;
+  const unsigned gb = grid_for(n, 256, 148u * 8u);
+  const uint32_t* zero = nullptr;  // no stop flag
+  if (precision == TPICB200_PRECISION_DOUBLE)
+    gather_kernel<double><<<gb, 256, 0, s>>>(perm, n, (const double*)in->rx, (const double*)in->ry,
+        (const double*)in->rz, (const double*)in->u, (const double*)in->v, (const double*)in->w, in->q, in->cell,
+        in->id, (double*)out->rx, (double*)out->ry, (double*)out->rz, (double*)out->u, (double*)out->v,
+        (double*)out->w, out->q, out->cell, in->id ? out->id : nullptr, zero, nullptr);
+  else
+    gather_kernel<float><<<gb, 256, 0, s>>>(perm, n, (const double*)in->rx, (const double*)in->ry,
+        (const double*)in->rz, (const float*)in->u, (const float*)in->v, (const float*)in->w, in->q, in->cell,
+        in->id, (double*)out->rx, (double*)out->ry, (double*)out->rz, (float*)out->u, (float*)out->v,
+        (float*)out->w, out->q, out->cell, in->id ? out->id : nullptr, zero, nullptr);
+  count_launches(1);
+  return cudaGetLastError();
 }
 
 size_t binned_scratch_words(const Geom& g) {

@@ -80,6 +80,7 @@ class Simulation:
         self.stream = torch.cuda.current_stream(dev)
         self.slots = []
         self.bins = []
+        self.ranks = []
         st = _lib.State()
         st.ns = len(case.species)
         for s, sp in enumerate(case.species):
@@ -107,6 +108,12 @@ class Simulation:
             cnt = torch.zeros(bins, dtype=torch.int32, device=dev)
             off = torch.zeros(bins + 1, dtype=torch.int32, device=dev)
             self.bins.append((cnt, off))
+            # Rank buffer: the cycle keeps the species ranked (the live slot
+            # plus its ranks is the sorted view; materialize() writes it out).
+            rk = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
+            self.ranks.append(rk)
+            st.ranks[s] = rk.data_ptr()
+            st.ranked[s] = 0
             st.qom[s] = sp.qom
             for k in range(2):
                 st.slot[s][k] = self._particles(slot[k], n)
@@ -133,7 +140,13 @@ class Simulation:
     def _stream(self) -> C.c_void_p:
         return C.c_void_p(self.stream.cuda_stream)
 
+    def materialize(self) -> None:
+        """Writes the sorted records of every ranked species into its live slot."""
+        _lib.check(self.lib.tpicb200_materialize(self.ctx, C.byref(self.state), self._stream()))
+
     def live(self, s: int) -> dict:
+        """Live records of species s, sorted by cell (materialized first)."""
+        self.materialize()
         return self.slots[s][self.state.current[s]]
 
     def prepare(self) -> None:
