@@ -63,6 +63,7 @@ constexpr int kMassMoments = 27 * 9;                  // G[t][c] per cell
 constexpr int kMoments = kMassMoments + 24;           // + J corner sums [a][c]
 constexpr uint32_t kDcol = 64;
 constexpr int kCtasPerSm = 4;      // 4 x 128 tensor-memory columns = all 512
+constexpr int kPermBuf = 256;      // ranks of a cell staged ahead (per warp and group)
 // Per form: B columns per cell, N, bytes of one B tile, B tiles per buffer.
 // TF32 (K-major): 8 K-chunks of 4 particles, each 6 N-groups x 128 bytes,
 // padded by 16 bytes (K-chunk stride 784 B) so the 32 lanes' 4-byte stores
@@ -117,6 +118,7 @@ template <bool Bf16> struct __align__(128) TcShared {
   float bpoly[kCells][24];            // B(x, y, z) polynomial coefficients [c][k]
   float stage[kCells][kMoments + 1];
   float hsum[kCells][27 * 3];
+  uint32_t sperm[2][kCells][kPermBuf];  // ranks of the cell of the current / next group
   uint64_t mbar[2];
   uint32_t tmem_base;
   uint32_t count[kCells];
@@ -231,13 +233,27 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_deposit_kernel(Geom g, TcP
     }
     return m;
   };
-  auto load_rec = [&](const Meta& m, uint32_t k) {
+  // Records read through ranks: each warp copies its next cell's ranks to
+  // shared memory a group ahead (cp.async), so that a record load waits for
+  // a shared-memory read rather than a second global load.
+  const bool gathered = tp.sp[0].perm || (two && tp.sp[1].perm);
+  auto prefetch_ranks = [&](const Meta& m, int b) {
+    if (!m.live) return;
+    const uint32_t total = min(m.c0 + m.c1, uint32_t(kPermBuf));
+    for (uint32_t k = lane; k < total; k += 32) {
+      const bool s1 = k >= m.c0;
+      const uint32_t* perm = s1 ? tp.sp[1].perm : tp.sp[0].perm;
+      if (perm) tc::cp_async4(&sh.sperm[b][warp][k], perm + (s1 ? m.f1 + (k - m.c0) : m.f0 + k));
+    }
+    tc::cp_async_commit();
+  };
+  auto load_rec = [&](const Meta& m, uint32_t k, int b) {
     Rec r{0.0, 0.0, 0.0, 0.0, 0.0f, 0.0f, 0.0f, -1, 0u, false, false};
     if (k < m.c0 + m.c1) {
       const bool s1 = k >= m.c0;
       r.pos = s1 ? m.f1 + (k - m.c0) : m.f0 + k;
       const uint32_t* perm = s1 ? tp.sp[1].perm : tp.sp[0].perm;
-      const uint32_t n = perm ? perm[r.pos] : r.pos;
+      const uint32_t n = perm ? (k < uint32_t(kPermBuf) ? sh.sperm[b][warp][k] : perm[r.pos]) : r.pos;
       r.present = true;
       r.second = s1;
       r.fx = (s1 ? tp.sp[1].rx : tp.sp[0].rx)[n];
@@ -252,7 +268,13 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_deposit_kernel(Geom g, TcP
     return r;
   };
   Meta cur = load_meta(blockIdx.x);
-  Rec pre = load_rec(cur, lane);
+  int rb = 0;  // rank buffer of the current group
+  if (gathered) {
+    prefetch_ranks(cur, rb);
+    tc::cp_async_wait_all();
+    __syncwarp();
+  }
+  Rec pre = load_rec(cur, lane, rb);
 
   for (long long grp = blockIdx.x; grp < groups && !failed; grp += gridDim.x) {
     const Meta nxt = load_meta(grp + gridDim.x);
@@ -284,7 +306,16 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_deposit_kernel(Geom g, TcP
     uint32_t maxc = sh.count[0];
 #pragma unroll
     for (int c = 1; c < kCells; ++c) maxc = max(maxc, sh.count[c]);
-    if (maxc == 0) pre = load_rec(nxt, lane);
+    // The next group's ranks travel while this group is processed.
+    if (gathered) prefetch_ranks(nxt, rb ^ 1);
+    auto load_next_group = [&]() {
+      if (gathered) {
+        tc::cp_async_wait_all();
+        __syncwarp();
+      }
+      return load_rec(nxt, lane, rb ^ 1);
+    };
+    if (maxc == 0) pre = load_next_group();
 
     for (uint32_t chunk = 0; chunk < maxc; chunk += kChunk) {
       // The buffer is free once the MMAs that read it have completed.
@@ -295,7 +326,7 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_deposit_kernel(Geom g, TcP
         pending &= ~(1u << buf);
       }
       const Rec rec = pre;
-      pre = chunk + kChunk < maxc ? load_rec(cur, chunk + kChunk + lane) : load_rec(nxt, lane);
+      pre = chunk + kChunk < maxc ? load_rec(cur, chunk + kChunk + lane, rb) : load_next_group();
       // Particle phase: one record per lane.
       float bv[kCols];
       float fac[12];
@@ -517,6 +548,7 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_deposit_kernel(Geom g, TcP
     __syncthreads();
     tc::fence_after_sync();
     cur = nxt;
+    rb ^= 1;
   }
 
   if (failed && threadIdx.x == 0) atomicAdd(invalid, 1u << 20);

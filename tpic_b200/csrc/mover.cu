@@ -293,13 +293,19 @@ __global__ void __launch_bounds__(kRunWarps * 32, 2 * TPICB200_MOVER_MIN_BLOCKS)
     }
     __syncwarp();
     const Records<P>& r = io.in;
+    // The ranks of the next chunk are loaded one chunk ahead, so the record
+    // loads do not wait for a rank load.
+    uint32_t n_next = 0;
+    if (io.ranks && begin + lane < end) n_next = io.ranks[begin + lane];
     for (uint32_t p0 = begin; p0 < end; p0 += 32) {
       const uint32_t p = p0 + lane;  // position in the sorted order of the bins
       const bool live = p < end;
+      const uint32_t n_rank = n_next;
+      if (io.ranks && p + 32 < end) n_next = io.ranks[p + 32];
       long long old_cell = 0;
       int d = -1, c = 0;
       if (live) {
-        const uint32_t n = io.ranks ? io.ranks[p] : p;
+        const uint32_t n = io.ranks ? n_rank : p;
         const int32_t k0 = r.key[n];
         const double charge = r.q[n];
         const Pos fx = r.rx[n], fy = r.ry[n], fz = r.rz[n];

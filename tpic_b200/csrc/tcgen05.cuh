@@ -87,6 +87,13 @@ __device__ __forceinline__ void mma_f16_ts(uint32_t d, uint32_t a, uint64_t bdes
                :: "r"(d), "r"(a), "l"(bdesc), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u) : "memory");
 }
 
+// Asynchronous 4-byte copy global -> shared (completion: cp_async_wait_all).
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" :: "r"(smem_u32(smem)), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // Shared-memory matrix descriptor, no swizzle (canonical core matrices of
 // 8 rows x 16 bytes): start address, leading-dimension byte offset (LBO),
 // stride-dimension byte offset (SBO), version 1 for sm_100.
