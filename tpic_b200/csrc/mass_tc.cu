@@ -119,7 +119,8 @@ template <bool Bf16> struct __align__(128) TcShared {
   float stage[kCells][kMoments + 1];
   float hsum[kCells][27 * 3];
   uint32_t sperm[2][kCells][kPermBuf];  // ranks of the cell of the current / next group
-  uint64_t mbar[2];
+  uint64_t mbar[2];  // MMAs that read buffer b have completed
+  uint64_t full[2];  // the four warps have written buffer b
   uint32_t tmem_base;
   uint32_t count[kCells];
 };
@@ -174,6 +175,8 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_deposit_kernel(Geom g, TcP
   if (threadIdx.x == 0) {
     tc::mbar_init(&sh.mbar[0], 1);
     tc::mbar_init(&sh.mbar[1], 1);
+    tc::mbar_init(&sh.full[0], kCells);
+    tc::mbar_init(&sh.full[1], kCells);
     tc::fence_mbar_init();
   }
   sh.fac[warp][12][lane] = 0.0f;
@@ -186,8 +189,12 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_deposit_kernel(Geom g, TcP
   // Bit b of `phase` / `pending`: the parity to wait for on mbar[b] and
   // whether MMAs reading buffer b are in flight.
   uint32_t phase = 0, pending = 0;
+  uint32_t full_phase = 0;  // bit b: the parity of full[b] the MMA thread waits for
   int buf = 0;
   bool failed = false;
+  // A bounded wait that timed out: the warps finish the group, which then
+  // ends the kernel with the error bit (every warp reaches the same barriers).
+  bool bad = false;
 
   const long long cells = (long long)g.nx * g.ny * g.nz;
   const long long groups = (cells + kCells - 1) / kCells;
@@ -319,9 +326,8 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_deposit_kernel(Geom g, TcP
 
     for (uint32_t chunk = 0; chunk < maxc; chunk += kChunk) {
       // The buffer is free once the MMAs that read it have completed.
-      bool bad = false;
       if (pending & (1u << buf)) {
-        bad = !tc::mbar_wait(&sh.mbar[buf], (phase >> buf) & 1u);
+        if (!tc::mbar_wait(&sh.mbar[buf], (phase >> buf) & 1u)) bad = true;
         phase ^= 1u << buf;
         pending &= ~(1u << buf);
       }
@@ -453,11 +459,13 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_deposit_kernel(Geom g, TcP
       tc::tmem_wait_st();
       tc::fence_proxy_async_smem();
       tc::fence_before_sync();
-      if (__syncthreads_or(bad)) {
-        failed = true;
-        break;
-      }
+      // This warp's share of the chunk is written: one arrival per warp; the
+      // MMA thread waits for all four, the other warps go on.
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(&sh.full[buf]);
       if (threadIdx.x == 0) {
+        if (!tc::mbar_wait(&sh.full[buf], (full_phase >> buf) & 1u)) bad = true;
+        full_phase ^= 1u << buf;
         tc::fence_after_sync();
         const uint32_t abase = tmem + (buf ? 32u : 0u);
         if constexpr (!Bf16) {
@@ -483,7 +491,6 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_deposit_kernel(Geom g, TcP
       pending |= 1u << buf;
       buf ^= 1;
     }
-    if (failed) break;
 
     // Moments: wait for the group's last MMA, read G and H of this warp's
     // cell and form the corner currents J[a][c] = sum_b H[t(a, b)][c].
@@ -495,7 +502,7 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_deposit_kernel(Geom g, TcP
       phase ^= 1u << last;
       pending &= ~(1u << last);
       tc::fence_after_sync();
-      if (__syncthreads_or(!ok)) {
+      if (__syncthreads_or(!ok || bad)) {
         failed = true;
         break;
       }

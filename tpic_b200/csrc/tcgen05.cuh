@@ -68,6 +68,12 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32
   return false;
 }
 
+// One arrival on the mbarrier (release: this thread's earlier writes are
+// visible to the thread that observes the phase completion).
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(smem_u32(bar)) : "memory");
+}
+
 // The mbarrier arrives once every tcgen05 operation issued so far by this
 // thread has completed.
 __device__ __forceinline__ void commit(uint64_t* bar) {
