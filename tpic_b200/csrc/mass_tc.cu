@@ -647,47 +647,38 @@ __host__ __device__ constexpr StencilPairs make_stencil_pairs() {
   return r;
 }
 
-// One thread per unique node: every record entry (stencil s, component e) is
-// the sum, in increasing corner order, of the moments G[t][e] of the cells
-// holding the pairs (a, a + offset_s); current component c is the sum of the
-// eight corner sums J[a][c] of the cells around the node. The tables are
-// compile-time constants, so the loops unroll into straight loads whose
-// addresses are consecutive across the warp (consecutive nodes, consecutive
-// cells). `overwrite` stores the sums (J and M were cleared and nothing else
+// One thread per (unique node, stencil): the stencil's nine record entries
+// of the node, each the sum, in increasing corner order, of the moments
+// G[t][e] of the cells holding the pairs (a, a + offset_s); "stencil" 14 is
+// the current, whose component c is the sum of the eight corner sums
+// J[a][c] of the cells around the node. The stencil is the grid's y index
+// and each case is unrolled from the compile-time tables, so a thread holds
+// at most nine sums and the loads of a warp are consecutive across its
+// nodes. `overwrite` stores the sums (J and M were cleared and nothing else
 // was deposited); otherwise they are added.
-__global__ void __launch_bounds__(128) assemble_moments_kernel(Geom g, const float* __restrict__ mom,
-                                                               long long stride, float* __restrict__ J,
-                                                               float* __restrict__ M, int overwrite) {
+template <int S>
+__device__ __forceinline__ void assemble_stencil(const Geom& g, const long long (&cell)[8], long long node,
+                                                 const float* __restrict__ mom, long long stride,
+                                                 float* __restrict__ J, float* __restrict__ M, int overwrite) {
   constexpr StencilPairs pairs = make_stencil_pairs();
-  const int nx = g.nx, ny = g.ny, nz = g.nz;
-  const long long unique = (long long)nx * ny * nz;
-  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < unique;
-       v += (long long)gridDim.x * blockDim.x) {
-    const int i = int(v % nx);
-    const long long r = v / nx;
-    const int j = int(r % ny), k = int(r / ny);
-    // Cells of corner a: the node is corner a of cell (i - a_x, j - a_y, k - a_z).
-    const int i0 = i, i1 = i > 0 ? i - 1 : nx - 1;
-    const int j0 = j, j1 = j > 0 ? j - 1 : ny - 1;
-    const int k0 = k, k1 = k > 0 ? k - 1 : nz - 1;
-    long long cell[8];
+  if constexpr (S < 14) {
+    float sum[9];
 #pragma unroll
-    for (int a = 0; a < 8; ++a)
-      cell[a] = ((a & 1) ? i1 : i0) + (long long)nx * (((a & 2) ? j1 : j0) + (long long)ny * ((a & 4) ? k1 : k0));
-    const long long node = g.node(i, j, k);
+    for (int e = 0; e < 9; ++e) sum[e] = 0.0f;
 #pragma unroll
-    for (int st = 0; st < 14; ++st) {
+    for (int p = 0; p < 8; ++p) {
+      if (p < pairs.count[S]) {
 #pragma unroll
-      for (int e = 0; e < 9; ++e) {
-        float sum = 0.0f;
-#pragma unroll
-        for (int p = 0; p < 8; ++p)
-          if (p < pairs.count[st])
-            sum += __ldg(mom + (pairs.monomial[st][p] * 9 + e) * stride + cell[pairs.corner[st][p]]);
-        float* dst = M + g.mass_index(node, st * 9 + e);
-        *dst = overwrite ? sum : *dst + sum;
+        for (int e = 0; e < 9; ++e)
+          sum[e] += __ldg(mom + (pairs.monomial[S][p] * 9 + e) * stride + cell[pairs.corner[S][p]]);
       }
     }
+#pragma unroll
+    for (int e = 0; e < 9; ++e) {
+      float* dst = M + g.mass_index(node, S * 9 + e);
+      *dst = overwrite ? sum[e] : *dst + sum[e];
+    }
+  } else {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       float sum = 0.0f;
@@ -699,13 +690,49 @@ __global__ void __launch_bounds__(128) assemble_moments_kernel(Geom g, const flo
   }
 }
 
+__global__ void __launch_bounds__(128) assemble_moments_kernel(Geom g, const float* __restrict__ mom,
+                                                               long long stride, float* __restrict__ J,
+                                                               float* __restrict__ M, int overwrite) {
+  const int nx = g.nx, ny = g.ny;
+  const long long unique = (long long)nx * ny * g.nz;
+  const long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (v >= unique) return;
+  const int i = int(v % nx);
+  const long long r = v / nx;
+  const int j = int(r % ny), k = int(r / ny);
+  // Cells of corner a: the node is corner a of cell (i - a_x, j - a_y, k - a_z).
+  const int i1 = i > 0 ? i - 1 : nx - 1, j1 = j > 0 ? j - 1 : ny - 1, k1 = k > 0 ? k - 1 : g.nz - 1;
+  long long cell[8];
+#pragma unroll
+  for (int a = 0; a < 8; ++a)
+    cell[a] = ((a & 1) ? i1 : i) + (long long)nx * (((a & 2) ? j1 : j) + (long long)ny * ((a & 4) ? k1 : k));
+  const long long node = g.node(i, j, k);
+  switch (blockIdx.y) {
+    case 0: assemble_stencil<0>(g, cell, node, mom, stride, J, M, overwrite); break;
+    case 1: assemble_stencil<1>(g, cell, node, mom, stride, J, M, overwrite); break;
+    case 2: assemble_stencil<2>(g, cell, node, mom, stride, J, M, overwrite); break;
+    case 3: assemble_stencil<3>(g, cell, node, mom, stride, J, M, overwrite); break;
+    case 4: assemble_stencil<4>(g, cell, node, mom, stride, J, M, overwrite); break;
+    case 5: assemble_stencil<5>(g, cell, node, mom, stride, J, M, overwrite); break;
+    case 6: assemble_stencil<6>(g, cell, node, mom, stride, J, M, overwrite); break;
+    case 7: assemble_stencil<7>(g, cell, node, mom, stride, J, M, overwrite); break;
+    case 8: assemble_stencil<8>(g, cell, node, mom, stride, J, M, overwrite); break;
+    case 9: assemble_stencil<9>(g, cell, node, mom, stride, J, M, overwrite); break;
+    case 10: assemble_stencil<10>(g, cell, node, mom, stride, J, M, overwrite); break;
+    case 11: assemble_stencil<11>(g, cell, node, mom, stride, J, M, overwrite); break;
+    case 12: assemble_stencil<12>(g, cell, node, mom, stride, J, M, overwrite); break;
+    case 13: assemble_stencil<13>(g, cell, node, mom, stride, J, M, overwrite); break;
+    default: assemble_stencil<14>(g, cell, node, mom, stride, J, M, overwrite); break;
+  }
+}
+
 }  // namespace
 
 cudaError_t launch_assemble_moments(const Geom& g, const float* moments, void* j, void* mass, int overwrite,
                                     cudaStream_t s) {
   const long long unique = (long long)g.nx * g.ny * g.nz;
-  assemble_moments_kernel<<<grid_for(unique, 128, 148u * 16u), 128, 0, s>>>(g, moments, moment_stride(g), (float*)j,
-                                                                            (float*)mass, overwrite);
+  const dim3 grid(unsigned((unique + 127) / 128), 15);
+  assemble_moments_kernel<<<grid, 128, 0, s>>>(g, moments, moment_stride(g), (float*)j, (float*)mass, overwrite);
   count_launches(1);
   return cudaGetLastError();
 }
