@@ -569,6 +569,543 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_deposit_kernel(Geom g, TcP
   if (warp == 0) tc::tmem_dealloc(tmem, kTmemCols);
 }
 
+
+// ---------------------------------------------------------------------------
+// Stream form of the BF16x3 deposition.
+//
+// Each warp owns a sequence of batches of four consecutive cells (batches
+// gw, gw + W, gw + 2W, ... for global warp gw of W) and walks a batch's
+// records as one stream, 32 per chunk (one per lane), without padding between
+// cells: a chunk may hold the tail of one cell and the head of the next
+// nonempty cell. The warp's quadrant of D therefore holds two accumulator
+// blocks that alternate between consecutive nonempty cells (the cell's
+// parity), and a cell is flushed - read from tensor memory, then zeroed - as
+// soon as the MMAs of its last chunk have completed and before the next chunk
+// is issued. Every batch starts a new chunk, so a cell's summation order
+// depends only on its batch's counts: the moments are reproducible.
+//
+// The four warps of a CTA share every MMA (M = 128 = four quadrants of 32
+// monomial rows; rows 27..31 of a quadrant stay zero):
+//   A (shared memory, MN-major, 128 x 32, BF16 hi and lo): row 32w + t,
+//     column k holds m_t of warp w's lane-k record;
+//   B (shared memory, MN-major, 32 x 96, BF16 hi and lo): columns 24w..24w+23
+//     belong to warp w: parity 0 uses columns 0..7 and 8..11 of them, parity 1
+//     columns 16..23 and 12..15; a lane writes its 12 values (s alpha, j) in
+//     its parity's block and zeros in the other;
+//   D (tensor memory, 128 x 96 FP32): D[32w + t][24w + 16p + c] = G[t][c]
+//     (c < 8) and D[32w + t][24w + 8 + 4p + c] = (G[t][8], H[t][0..2]).
+// Both operands are single-buffered: a warp writes chunk j's A and B after the
+// MMAs of chunk j - 1 have completed, which it waits for anyway to flush the
+// cells that ended in chunk j - 1. The warps build the A rows of their own
+// records directly (27 products per lane), with no transposition.
+//
+// Records are fetched in a three-stage software pipeline per warp: the walk
+// of chunk j + 2 issues the rank loads, chunk j + 1's record loads are in
+// flight, chunk j is computed. A warp that has run out of batches keeps
+// arriving with no data while any warp of its CTA still has chunks (each
+// warp publishes, per chunk, whether it has another), and the CTA's warps
+// leave the loop together.
+constexpr int kBatch = 4;                  // cells per batch
+constexpr int kStreamN = 96;               // B columns: 4 quadrants x 2 parities x 12
+constexpr uint32_t kStreamTmemCols = 128;  // D uses 96 of them
+constexpr int kMetaSlots = 3;              // batches of chunks j .. j + 2
+
+struct StreamMeta {
+  uint32_t n[kBatch];   // records of the cell (both species)
+  uint32_t c0[kBatch];  // species-0 records
+  uint32_t f0[kBatch];  // first sorted position, species 0
+  uint32_t f1[kBatch];  // first sorted position, species 1
+  int32_t bin[kBatch];
+  float bpoly[kBatch][24];
+};
+
+struct __align__(16) StreamShared {
+  uint8_t a[2][128 * 32 * 2];        // A hi, lo: 16 M-chunks x 512 B (4 K-groups x 128 B)
+  uint8_t b[2][kStreamN / 8 * 512];  // B hi, lo: 12 N-chunks x 512 B
+  float stage[kCells][kBatch][kMoments + 1];
+  float scratch[kCells][96];  // a batch's B corners / the H rows of a flushed cell
+  StreamMeta meta[kCells][kMetaSlots];
+  uint32_t more[2];  // byte w of word j & 1: warp w has a chunk after chunk j
+  uint64_t mma_bar;  // the MMAs of a chunk have completed
+  uint64_t full_bar; // the four warps have written a chunk's operands
+  uint32_t tmem_base;
+};
+
+// Per-lane record of a chunk: rank (record index in the read slot), sorted
+// position, flags (1 present, 2 second species, slot << 2, parity << 4).
+struct StreamLane {
+  uint32_t idx, pos, flags;
+};
+// Warp-uniform chunk description: batch and bits (ended cells 0-3,
+// nonempty cells 4-7, parities 8-11, last chunk of the batch 12, valid 13,
+// metadata slot 14-15).
+struct StreamInfo {
+  int bid;
+  uint32_t bits;
+};
+struct StreamRec {
+  double fx, fy, fz, q;
+  float u, v, w;
+  int32_t key;
+  uint32_t pos, flags;
+};
+struct MetaRegs {
+  uint32_t c0, c1, f0, f1;
+  int32_t bin;
+  float corner[3];
+};
+
+__global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcParams tp,
+    const float* __restrict__ bnode, float* __restrict__ mom, long long mom_stride, int accumulate,
+    uint32_t* invalid, int batches) {
+  extern __shared__ __align__(16) uint8_t stream_smem[];
+  StreamShared& sh = *reinterpret_cast<StreamShared*>(stream_smem);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int W = int(gridDim.x) * kCells;
+  const long long nn = g.nodes;
+  const long long cells = (long long)g.nx * g.ny * g.nz;
+  const bool two = tp.ns > 1;
+  if (warp == 0) {
+    tc::tmem_alloc(&sh.tmem_base, kStreamTmemCols);
+    tc::tmem_relinquish();
+  }
+  if (threadIdx.x == 0) {
+    tc::mbar_init(&sh.mma_bar, 1);
+    tc::mbar_init(&sh.full_bar, kCells);
+    tc::fence_mbar_init();
+    sh.more[0] = sh.more[1] = 0u;
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = sh.tmem_base;
+  // This warp's 24 accumulator columns, in its own 32 lanes.
+  const uint32_t dq = tmem + (uint32_t(32 * warp) << 16) + 24u * warp;
+  {
+    const uint32_t z[8] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
+    tc::tmem_st8(dq, z);
+    tc::tmem_st8(dq + 8, z);
+    tc::tmem_st8(dq + 16, z);
+    tc::tmem_wait_st();
+  }
+  constexpr uint32_t idesc = tc::instr_desc(1u, 128, kStreamN, 1u, 1u);
+
+  // Batch metadata: lanes 0..3 load the counts and offsets of cell slot
+  // `lane`; lane l loads B corner values (l >> 2) + 8i of slot l & 3.
+  auto fetch_meta = [&](int bid) {
+    MetaRegs r{0u, 0u, 0u, 0u, -1, {0.0f, 0.0f, 0.0f}};
+    const long long cell = (long long)bid * kBatch + (lane & 3);
+    if (bid < batches && cell < cells) {
+      const uint32_t c = uint32_t(cell), nx = uint32_t(g.nx), ny = uint32_t(g.ny);
+      const uint32_t row = c / nx;
+      const int ci = int(c - row * nx), cj = int(row % ny), ck = int(row / ny);
+      r.bin = g.encode(ci, cj, ck);
+      if (lane < kBatch) {
+        r.c0 = tp.sp[0].counts[r.bin];
+        r.f0 = tp.sp[0].offsets[r.bin];
+        if (two) {
+          r.c1 = tp.sp[1].counts[r.bin];
+          r.f1 = tp.sp[1].offsets[r.bin];
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        const int idx = (lane >> 2) + 8 * i, a = idx / 3, comp = idx - 3 * a;
+        r.corner[i] = bnode[comp * nn + g.node(ci + (a & 1), cj + ((a >> 1) & 1), ck + ((a >> 2) & 1))];
+      }
+    }
+    return r;
+  };
+  // Writes a batch's metadata into slot `slot`: counts, offsets, bins and
+  // the trilinear B of each cell as a polynomial in the cell fractions,
+  // B = c0 + c1 x + c2 y + c3 z + c4 xy + c5 xz + c6 yz + c7 xyz. Returns the
+  // nonempty cells (bits 0-3) and their parities (bits 4-7).
+  auto store_meta = [&](const MetaRegs& r, int slot) -> uint32_t {
+    StreamMeta& m = sh.meta[warp][slot];
+    float* tmp = sh.scratch[warp];
+    if (lane < kBatch) {
+      m.n[lane] = r.c0 + r.c1;
+      m.c0[lane] = r.c0;
+      m.f0[lane] = r.f0;
+      m.f1[lane] = r.f1;
+      m.bin[lane] = r.bin;
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) tmp[(lane & 3) * 24 + (lane >> 2) + 8 * i] = r.corner[i];
+    const uint32_t nonempty = __ballot_sync(0xffffffffu, lane < kBatch && r.c0 + r.c1 > 0u) & 0xFu;
+    __syncwarp();
+    if (lane < 3 * kBatch) {
+      const int s = lane / 3, c = lane - 3 * s;
+      float bc[8];
+#pragma unroll
+      for (int a = 0; a < 8; ++a) bc[a] = tmp[s * 24 + 3 * a + c];
+      float* cp = m.bpoly[s] + 8 * c;
+      cp[0] = bc[0];
+      cp[1] = bc[1] - bc[0];
+      cp[2] = bc[2] - bc[0];
+      cp[3] = bc[4] - bc[0];
+      cp[4] = (bc[3] - bc[2]) - (bc[1] - bc[0]);
+      cp[5] = (bc[5] - bc[4]) - (bc[1] - bc[0]);
+      cp[6] = (bc[6] - bc[4]) - (bc[2] - bc[0]);
+      cp[7] = ((bc[7] - bc[6]) - (bc[5] - bc[4])) - ((bc[3] - bc[2]) - (bc[1] - bc[0]));
+    }
+    __syncwarp();
+    uint32_t parity = 0;
+#pragma unroll
+    for (int s = 0; s < kBatch; ++s) parity |= (uint32_t(__popc(nonempty & ((1u << s) - 1u))) & 1u) << s;
+    return nonempty | (parity << 4);
+  };
+
+  // The walk (warp-uniform cursor over this warp's batches).
+  int cbid = blockIdx.x * kCells + warp;  // current batch
+  int cseq = 0;                           // batches entered so far - 1
+  int ca = 0;                             // cell slot of the next record
+  uint32_t co = 0;                        // records of that cell already taken
+  uint32_t cbits = 0;                     // nonempty | parity << 4 of the batch
+  bool cend = cbid >= batches, cnext = false;
+  MetaRegs pf = fetch_meta(cbid);
+  if (!cend) {
+    cbits = store_meta(pf, 0);
+    pf = fetch_meta(cbid + W);
+  }
+  auto walk = [&](StreamLane& L, StreamInfo& I) {
+    L = StreamLane{0u, 0u, 0u};
+    I = StreamInfo{0, 0u};
+    if (cnext) {  // the previous chunk finished the batch
+      cnext = false;
+      cbid += W;
+      ++cseq;
+      if (cbid >= batches) {
+        cend = true;
+      } else {
+        cbits = store_meta(pf, cseq % kMetaSlots);
+        pf = fetch_meta(cbid + W);
+        ca = 0;
+        co = 0;
+      }
+    }
+    if (cend) return;
+    const StreamMeta& m = sh.meta[warp][cseq % kMetaSlots];
+    const uint32_t nonempty = cbits & 0xFu;
+    uint32_t ended = 0;
+    int a = ca;
+    while (a < kBatch && !((nonempty >> a) & 1u)) ended |= 1u << a++;
+    int slot = -1;
+    uint32_t k = 0;
+    int next_a = kBatch;
+    uint32_t next_o = 0;
+    if (a < kBatch) {
+      const uint32_t rem = m.n[a] - co;
+      if (uint32_t(lane) < rem) {
+        slot = a;
+        k = co + lane;
+      }
+      if (rem > 32u) {
+        next_a = a;
+        next_o = co + 32u;
+      } else {
+        ended |= 1u << a;
+        int b = a + 1;
+        while (b < kBatch && !((nonempty >> b) & 1u)) ended |= 1u << b++;
+        if (b < kBatch) {
+          const uint32_t nb = m.n[b];
+          if (uint32_t(lane) >= rem && uint32_t(lane) - rem < nb) {
+            slot = b;
+            k = lane - rem;
+          }
+          if (rem + nb <= 32u) {
+            ended |= 1u << b;
+            int c = b + 1;
+            while (c < kBatch && !((nonempty >> c) & 1u)) ended |= 1u << c++;
+            next_a = c;
+          } else {
+            next_a = b;
+            next_o = 32u - rem;
+          }
+        }
+      }
+    } else {
+      ended = 0xFu;
+    }
+    const bool last = next_a >= kBatch;
+    I.bid = cbid;
+    I.bits = ended | ((cbits & 0xFFu) << 4) | (last ? 1u << 12 : 0u) | (1u << 13) |
+             (uint32_t(cseq % kMetaSlots) << 14);
+    if (slot >= 0) {
+      const uint32_t c0 = m.c0[slot];
+      const bool s1 = k >= c0;
+      L.pos = s1 ? m.f1[slot] + (k - c0) : m.f0[slot] + k;
+      const uint32_t* perm = s1 ? tp.sp[1].perm : tp.sp[0].perm;
+      L.idx = perm ? __ldg(perm + L.pos) : L.pos;
+      L.flags = 1u | (s1 ? 2u : 0u) | (uint32_t(slot) << 2) | (((cbits >> (4 + slot)) & 1u) << 4);
+    }
+    if (last) {
+      cnext = true;
+    } else {
+      ca = next_a;
+      co = next_o;
+    }
+  };
+  auto load_rec = [&](const StreamLane& L) {
+    StreamRec r{0.0, 0.0, 0.0, 0.0, 0.0f, 0.0f, 0.0f, -1, L.pos, L.flags};
+    if (L.flags & 1u) {
+      const TcSpecies& sp = (L.flags & 2u) ? tp.sp[1] : tp.sp[0];
+      const uint32_t n = L.idx;
+      r.fx = sp.rx[n];
+      r.fy = sp.ry[n];
+      r.fz = sp.rz[n];
+      r.q = sp.q[n];
+      r.u = sp.u[n];
+      r.v = sp.v[n];
+      r.w = sp.w[n];
+      r.key = sp.key[n];
+    }
+    return r;
+  };
+  // Moments of the cells that ended in a chunk whose MMAs have completed;
+  // a batch's moments are stored when its last cell is done.
+  auto flush = [&](const StreamInfo& I) {
+    const uint32_t ended = I.bits & 0xFu;
+    if (!((I.bits >> 13) & 1u) || ended == 0u) return;
+    const uint32_t nonempty = (I.bits >> 4) & 0xFu, parity = (I.bits >> 8) & 0xFu;
+    float* hs = sh.scratch[warp];
+#pragma unroll 1
+    for (int s = 0; s < kBatch; ++s) {
+      if (!((ended >> s) & 1u)) continue;
+      float* st = sh.stage[warp][s];
+      if ((nonempty >> s) & 1u) {
+        const uint32_t p = (parity >> s) & 1u;
+        uint32_t g8[8], g4[4];
+        tc::tmem_ld8(dq + 16u * p, g8);
+        tc::tmem_ld4(dq + 8u + 4u * p, g4);
+        tc::tmem_wait_ld();
+        const uint32_t z8[8] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
+        const uint32_t z4[4] = {0u, 0u, 0u, 0u};
+        tc::tmem_st8(dq + 16u * p, z8);
+        tc::tmem_st4(dq + 8u + 4u * p, z4);
+        if (lane < 27) {
+#pragma unroll
+          for (int e = 0; e < 8; ++e) st[lane * 9 + e] = __uint_as_float(g8[e]);
+          st[lane * 9 + 8] = __uint_as_float(g4[0]);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) hs[lane * 3 + c] = __uint_as_float(g4[1 + c]);
+        }
+        __syncwarp();
+        if (lane < 24) {
+          const int a = lane / 3, c = lane - 3 * (lane / 3);
+          float sum = 0.0f;
+#pragma unroll
+          for (int b = 0; b < 8; ++b) sum += hs[monomial_class(a, b) * 3 + c];
+          st[kMassMoments + lane] = sum;
+        }
+        __syncwarp();
+      } else {
+        for (int q = lane; q < kMoments; q += 32) st[q] = 0.0f;
+      }
+    }
+    if ((I.bits >> 12) & 1u) {
+      __syncwarp();
+      bool bad_value = false;
+      float* base = mom + (long long)I.bid * kBatch;
+      for (int q = lane; q < kMoments; q += 32) {
+        float4 val = make_float4(sh.stage[warp][0][q], sh.stage[warp][1][q], sh.stage[warp][2][q],
+                                 sh.stage[warp][3][q]);
+        if (!isfinite(val.x + val.y + val.z + val.w)) {
+          bad_value = true;
+          val.x = isfinite(val.x) ? val.x : 0.0f;
+          val.y = isfinite(val.y) ? val.y : 0.0f;
+          val.z = isfinite(val.z) ? val.z : 0.0f;
+          val.w = isfinite(val.w) ? val.w : 0.0f;
+        }
+        float4* dst = reinterpret_cast<float4*>(base + q * mom_stride);
+        if (accumulate) {
+          const float4 old = *dst;
+          val.x += old.x; val.y += old.y; val.z += old.z; val.w += old.w;
+        }
+        *dst = val;
+      }
+      if (bad_value) atomicAdd(invalid, 1u);
+      __syncwarp();
+    }
+  };
+
+  StreamLane l2;
+  StreamInfo i2;
+  walk(l2, i2);  // chunk 0
+  StreamRec r1 = load_rec(l2);
+  StreamInfo i1 = i2;
+  walk(l2, i2);  // chunk 1
+  StreamInfo ip{0, 0u};  // the previous chunk, whose cells are flushed next
+  bool bad = false;
+  uint32_t issued = 0;   // chunks whose MMAs thread 0 committed
+  const int kofs = (lane >> 3) * 128 + (lane & 7) * 16;  // lane's K row in a 512-byte core group
+  for (uint32_t j = 0;; ++j) {
+    const StreamRec r0 = r1;
+    const StreamInfo i0 = i1;
+    r1 = load_rec(l2);
+    i1 = i2;
+    walk(l2, i2);
+    const bool have = (i0.bits >> 13) & 1u;
+
+    // Particle phase: (s alpha, j) and the per-axis factors of one record.
+    float bv[12], X[3], YZ[9];
+#pragma unroll
+    for (int c = 0; c < 12; ++c) bv[c] = 0.0f;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) X[c] = 0.0f;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) YZ[c] = 0.0f;
+    uint32_t par = 0;
+    if (have && (r0.flags & 1u)) {
+      const int slot = (r0.flags >> 2) & 3;
+      par = (r0.flags >> 4) & 1u;
+      const bool second = r0.flags & 2u;
+      const TcSpecies& sp = second ? tp.sp[1] : tp.sp[0];
+      if (sp.orx) {
+        const uint32_t o = r0.pos;
+        sp.orx[o] = r0.fx; sp.ory[o] = r0.fy; sp.orz[o] = r0.fz;
+        sp.ou[o] = r0.u; sp.ov[o] = r0.v; sp.ow[o] = r0.w;
+        sp.oq[o] = r0.q; sp.okey[o] = r0.key;
+      }
+      const StreamMeta& m = sh.meta[warp][(i0.bits >> 14) & 3u];
+      const double fx = r0.fx, fy = r0.fy, fz = r0.fz;
+      bool ok = r0.key == m.bin[slot] && fx >= 0 && fx < 1 && fy >= 0 && fy < 1 && fz >= 0 && fz < 1;
+      if (ok) {
+        const float x = float(fx), y = float(fy), z = float(fz);
+        float b[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const float4 lo4 = *reinterpret_cast<const float4*>(&m.bpoly[slot][8 * c]);
+          const float4 hi4 = *reinterpret_cast<const float4*>(&m.bpoly[slot][8 * c + 4]);
+          const float t1 = fmaf(z, hi4.w, hi4.x);              // c4 + z c7
+          const float t2 = fmaf(z, hi4.y, fmaf(y, t1, lo4.y));  // c1 + y (c4 + z c7) + z c5
+          const float t3 = fmaf(z, hi4.z, lo4.z);              // c2 + z c6
+          b[c] = fmaf(z, lo4.w, fmaf(y, t3, fmaf(x, t2, lo4.x)));
+        }
+        const float bo = sp.beta_over_c;
+        const ScaledResponse r(b[0], b[1], b[2], bo);
+        const float charge = float(r0.q);
+        const float hx = r.a[0] * r0.u + r.a[1] * r0.v + r.a[2] * r0.w;
+        const float hy = r.a[3] * r0.u + r.a[4] * r0.v + r.a[5] * r0.w;
+        const float hz = r.a[6] * r0.u + r.a[7] * r0.v + r.a[8] * r0.w;
+        const float qv = charge * tp.inv_volume;
+        const float scale = bo * charge;
+        bv[9] = qv * hx; bv[10] = qv * hy; bv[11] = qv * hz;
+#pragma unroll
+        for (int e = 0; e < 9; ++e) bv[e] = r.a[e] * scale;
+        ok = isfinite(bv[9] + bv[10] + bv[11] + r.norm_square + scale);
+        if (ok) {
+          const float cx = 1.0f - x, cy = 1.0f - y, cz = 1.0f - z;
+          X[0] = cx * cx; X[1] = x * cx; X[2] = x * x;
+          const float Y[3] = {cy * cy, y * cy, y * y};
+          const float Z[3] = {cz * cz, z * cz, z * z};
+#pragma unroll
+          for (int tz = 0; tz < 3; ++tz)
+#pragma unroll
+            for (int ty = 0; ty < 3; ++ty) YZ[ty + 3 * tz] = Y[ty] * Z[tz];
+        } else {
+#pragma unroll
+          for (int c = 0; c < 12; ++c) bv[c] = 0.0f;
+        }
+      }
+      if (!ok) atomicAdd(invalid, 1u);
+    }
+
+    // The MMAs of chunk j - 1 have completed: flush the cells that ended in
+    // it; a warp without chunks learns whether any warp of the CTA has one.
+    if (j > 0) {
+      const bool done = tc::mbar_wait(&sh.mma_bar, (j - 1) & 1u);
+      if (__any_sync(0xffffffffu, !done)) {
+        bad = true;
+        break;
+      }
+      tc::fence_after_sync();
+      flush(ip);
+      if (!have) {
+        const bool seen = tc::mbar_wait(&sh.full_bar, (j - 1) & 1u);
+        if (__any_sync(0xffffffffu, !seen)) {
+          bad = true;
+          break;
+        }
+        if (*reinterpret_cast<volatile uint32_t*>(&sh.more[(j - 1) & 1u]) == 0u) break;
+      }
+    }
+    if (have) {
+      // B: 12 values in the parity's block, zeros in the other.
+      uint32_t bh[6], bl[6];
+#pragma unroll
+      for (int e = 0; e < 6; ++e) split_pair(make_float2(bv[2 * e], bv[2 * e + 1]), bh[e], bl[e]);
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const uint32_t* w = h ? bl : bh;
+        uint8_t* base = sh.b[h] + kofs;
+        *reinterpret_cast<uint4*>(base + (3 * warp + 2 * par) * 512) = make_uint4(w[0], w[1], w[2], w[3]);
+        *reinterpret_cast<uint4*>(base + (3 * warp + 2 - 2 * par) * 512) = make_uint4(0u, 0u, 0u, 0u);
+        *reinterpret_cast<uint4*>(base + (3 * warp + 1) * 512) =
+            par ? make_uint4(0u, 0u, w[4], w[5]) : make_uint4(w[4], w[5], 0u, 0u);
+      }
+      // A: the 27 monomials m_t = X[t % 3] YZ[t / 3] of this lane's record.
+      uint32_t ah[16], al[16];
+#pragma unroll
+      for (int i = 0; i < 14; ++i) {
+        const int t0 = 2 * i, t1 = 2 * i + 1;
+        const float2 f = make_float2(X[t0 % 3], t1 < 27 ? X[t1 % 3] : 0.0f);
+        const float2 y = make_float2(YZ[t0 / 3], t1 < 27 ? YZ[t1 / 3] : 0.0f);
+        split_pair(__fmul2_rn(f, y), ah[i], al[i]);
+      }
+      ah[14] = ah[15] = al[14] = al[15] = 0u;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const int off = (4 * warp + c) * 512 + kofs;
+        *reinterpret_cast<uint4*>(sh.a[0] + off) = make_uint4(ah[4 * c], ah[4 * c + 1], ah[4 * c + 2], ah[4 * c + 3]);
+        *reinterpret_cast<uint4*>(sh.a[1] + off) = make_uint4(al[4 * c], al[4 * c + 1], al[4 * c + 2], al[4 * c + 3]);
+      }
+    }
+    if (lane == 0)
+      reinterpret_cast<volatile uint8_t*>(&sh.more[j & 1u])[warp] = uint8_t((i1.bits >> 13) & 1u);
+    tc::tmem_wait_st();
+    tc::fence_proxy_async_smem();
+    tc::fence_before_sync();
+    __syncwarp();
+    if (lane == 0) tc::mbar_arrive(&sh.full_bar);
+    if (warp == 0) {
+      bool ok = true;
+      if (lane == 0) {
+        ok = tc::mbar_wait(&sh.full_bar, j & 1u);
+        if (ok) {
+          tc::fence_after_sync();
+          const uint32_t ah = tc::smem_u32(sh.a[0]), al = tc::smem_u32(sh.a[1]);
+          const uint32_t bh = tc::smem_u32(sh.b[0]), bl = tc::smem_u32(sh.b[1]);
+#pragma unroll
+          for (int s = 0; s < 2; ++s) {
+            const uint64_t dah = tc::smem_desc(ah + s * 256, 128, 512), dal = tc::smem_desc(al + s * 256, 128, 512);
+            const uint64_t dbh = tc::smem_desc(bh + s * 256, 128, 512), dbl = tc::smem_desc(bl + s * 256, 128, 512);
+            tc::mma_f16_ss(tmem, dah, dbh, idesc, 1u);
+            tc::mma_f16_ss(tmem, dah, dbl, idesc, 1u);
+            tc::mma_f16_ss(tmem, dal, dbh, idesc, 1u);
+          }
+          tc::commit(&sh.mma_bar);
+          ++issued;
+        }
+      }
+      if (!__shfl_sync(0xffffffffu, ok ? 1 : 0, 0)) {
+        bad = true;
+        break;
+      }
+    }
+    ip = i0;
+  }
+
+  if (bad && lane == 0) atomicAdd(invalid, 1u << 20);
+  // After a failed wait MMAs may still be in flight: retire them (bounded)
+  // before the tensor memory is freed.
+  if (threadIdx.x == 0 && issued > 0) tc::mbar_wait(&sh.mma_bar, (issued - 1) & 1u);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  if (warp == 0) tc::tmem_dealloc(tmem, kStreamTmemCols);
+}
+
 }  // namespace
 
 long long moment_stride(const Geom& g) {
@@ -587,16 +1124,29 @@ cudaError_t launch_deposit_tc(int mass_kind, const Geom& g, int ns, const double
   cudaGetDevice(&device);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   const long long cells = (long long)g.nx * g.ny * g.nz;
+  if (cells > (1LL << 31) - 64) return cudaErrorInvalidValue;
   const long long groups = (cells + kCells - 1) / kCells;
-  const unsigned blocks = unsigned(std::min<long long>(groups, (long long)kCtasPerSm * sms));
-  // Dynamic shared-memory padding brings each CTA to ~47 KB, so at most four
-  // CTAs (4 x 128 tensor-memory columns = all 512) are resident per SM and
-  // no tcgen05.alloc ever waits for another CTA's columns; the maximum
-  // shared-memory carveout lets all four be resident.
   const bool tf32 = mass_kind == TPICB200_MASS_TF32;
-  auto kernel = tf32 ? tc_deposit_kernel<false> : tc_deposit_kernel<true>;
-  const int pad = 47 * 1024 - int(tf32 ? sizeof(TcShared<false>) : sizeof(TcShared<true>));
-  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  cudaError_t e = cudaSuccess;
+  // TF32: one CTA group of four cells at a time. Dynamic shared-memory
+  // padding brings each CTA to ~47 KB, so at most four CTAs (4 x 128
+  // tensor-memory columns = all 512) are resident per SM and no
+  // tcgen05.alloc ever waits for another CTA's columns; the maximum
+  // shared-memory carveout lets all four be resident.
+  // BF16x3: the stream kernel, ~53 KB of dynamic shared memory per CTA (four
+  // resident per SM, 128 tensor-memory columns each).
+  auto kernel = tc_deposit_kernel<false>;
+  const int pad = 47 * 1024 - int(sizeof(TcShared<false>));
+  unsigned blocks = unsigned(std::min<long long>(groups, (long long)kCtasPerSm * sms));
+  const int stream_bytes = int(sizeof(StreamShared));
+  if (tf32) {
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  } else {
+    blocks = unsigned(std::min<long long>((groups + kCells - 1) / kCells, (long long)kCtasPerSm * sms));
+    e = cudaFuncSetAttribute(tc_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, stream_bytes);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(tc_stream_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  }
   if (e != cudaSuccess) return e;
   for (int first = 0; first < ns; first += kFuse) {
     TcParams tp{};
@@ -615,8 +1165,12 @@ cudaError_t launch_deposit_tc(int mass_kind, const Geom& g, int ns, const double
                            copy ? (float*)cp->out.w : nullptr, copy ? cp->out.q : nullptr,
                            copy ? cp->out.cell : nullptr};
     }
-    kernel<<<blocks, 128, pad, s>>>(g, tp, (const float*)bnode, moments, moment_stride(g),
-                                    (accumulate || first > 0) ? 1 : 0, invalid);
+    const int acc = (accumulate || first > 0) ? 1 : 0;
+    if (tf32)
+      kernel<<<blocks, 128, pad, s>>>(g, tp, (const float*)bnode, moments, moment_stride(g), acc, invalid);
+    else
+      tc_stream_kernel<<<blocks, 128, stream_bytes, s>>>(g, tp, (const float*)bnode, moments, moment_stride(g), acc,
+                                                         invalid, int(groups));
     count_launches(1);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }

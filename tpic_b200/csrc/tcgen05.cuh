@@ -31,6 +31,10 @@ __device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t (&v)[8])
                :: "r"(taddr), "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]),
                   "r"(v[7]) : "memory");
 }
+__device__ __forceinline__ void tmem_st4(uint32_t taddr, const uint32_t (&v)[4]) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};"
+               :: "r"(taddr), "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]) : "memory");
+}
 __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&v)[8]) {
   asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
@@ -93,6 +97,13 @@ __device__ __forceinline__ void mma_f16_ts(uint32_t d, uint32_t a, uint64_t bdes
                :: "r"(d), "r"(a), "l"(bdesc), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u) : "memory");
 }
 
+// D[tmem] (+)= A[smem] x B[smem] with kind::f16 (K = 16).
+__device__ __forceinline__ void mma_f16_ss(uint32_t d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc) {
+  asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+               "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+               :: "r"(d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc) : "memory");
+}
+
 // Asynchronous 4-byte copy global -> shared (completion: cp_async_wait_all).
 __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" :: "r"(smem_u32(smem)), "l"(gmem) : "memory");
@@ -109,11 +120,14 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t start, uint32_t lbo, uint
 }
 
 // Instruction descriptor: F32 accumulator, A/B format (0 F16, 1 BF16, 2 TF32),
-// A K-major (A comes from tensor memory), B MN-major (b_mn = 1) or K-major,
-// M and N. (With TF32 operands a no-swizzle MN-major B produced zero results
-// on this part; the TF32 form uses a K-major B.)
-__host__ __device__ constexpr uint32_t instr_desc(uint32_t ab_format, uint32_t m, uint32_t n, uint32_t b_mn = 1) {
-  return (1u << 4) | (ab_format << 7) | (ab_format << 10) | (b_mn << 16) | ((n >> 3) << 17) | ((m >> 4) << 24);
+// B MN-major (b_mn = 1) or K-major, A K-major (always so from tensor memory)
+// or MN-major (a_mn = 1, shared memory), M and N. (With TF32 operands a
+// no-swizzle MN-major B produced zero results on this part; the TF32 form
+// uses a K-major B.)
+__host__ __device__ constexpr uint32_t instr_desc(uint32_t ab_format, uint32_t m, uint32_t n, uint32_t b_mn = 1,
+                                                  uint32_t a_mn = 0) {
+  return (1u << 4) | (ab_format << 7) | (ab_format << 10) | (a_mn << 15) | (b_mn << 16) | ((n >> 3) << 17) |
+         ((m >> 4) << 24);
 }
 
 __device__ __forceinline__ uint32_t to_tf32(float x) {
