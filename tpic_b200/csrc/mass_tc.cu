@@ -575,14 +575,16 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_deposit_kernel(Geom g, TcP
 //
 // Each warp owns a sequence of batches of four consecutive cells (batches
 // gw, gw + W, gw + 2W, ... for global warp gw of W) and walks a batch's
-// records as one stream, 32 per chunk (one per lane), without padding between
-// cells: a chunk may hold the tail of one cell and the head of the next
-// nonempty cell. The warp's quadrant of D therefore holds two accumulator
-// blocks that alternate between consecutive nonempty cells (the cell's
-// parity), and a cell is flushed - read from tensor memory, then zeroed - as
-// soon as the MMAs of its last chunk have completed and before the next chunk
-// is issued. Every batch starts a new chunk, so a cell's summation order
-// depends only on its batch's counts: the moments are reproducible.
+// records as one stream - cell by cell, species 0 before species 1 in a
+// cell - 32 per chunk (one per lane), without padding between cells: a chunk
+// may hold the tail of one cell and the head of the next nonempty cell. The
+// warp's quadrant of D therefore holds two accumulator blocks that alternate
+// between consecutive nonempty cells (the cell's parity), and a cell is
+// flushed - read from tensor memory, then zeroed - once the MMAs of its last
+// chunk have completed and before the warp's next chunk is issued. A chunk
+// ends early where it would reach a third nonempty cell. Every batch starts a
+// new chunk, so a cell's summation order depends only on its batch's counts:
+// the moments are reproducible.
 //
 // The four warps of a CTA share every MMA (M = 128 = four quadrants of 32
 // monomial rows; rows 27..31 of a quadrant stay zero):
@@ -597,24 +599,24 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_deposit_kernel(Geom g, TcP
 // Both operands are single-buffered: a warp writes chunk j's A and B after the
 // MMAs of chunk j - 1 have completed, which it waits for anyway to flush the
 // cells that ended in chunk j - 1. The warps build the A rows of their own
-// records directly (27 products per lane), with no transposition.
+// records directly (27 products per lane), with no transposition. The last
+// warp to finish writing a chunk's operands (an acquire-release counter per
+// chunk parity) issues its MMAs, so no warp waits for the others.
 //
 // Records are fetched in a three-stage software pipeline per warp: the walk
 // of chunk j + 2 issues the rank loads, chunk j + 1's record loads are in
 // flight, chunk j is computed. A warp that has run out of batches keeps
 // arriving with no data while any warp of its CTA still has chunks (each
-// warp publishes, per chunk, whether it has another), and the CTA's warps
-// leave the loop together.
+// warp publishes, per chunk, whether it has another; the issuer publishes
+// the CTA's answer), and the CTA's warps leave the loop together.
 constexpr int kBatch = 4;                  // cells per batch
 constexpr int kStreamN = 96;               // B columns: 4 quadrants x 2 parities x 12
 constexpr uint32_t kStreamTmemCols = 128;  // D uses 96 of them
 constexpr int kMetaSlots = 3;              // batches of chunks j .. j + 2
 
 struct StreamMeta {
-  uint32_t n[kBatch];   // records of the cell (both species)
-  uint32_t c0[kBatch];  // species-0 records
-  uint32_t f0[kBatch];  // first sorted position, species 0
-  uint32_t f1[kBatch];  // first sorted position, species 1
+  uint32_t split[kBatch];   // stream position of the cell's first species-1 record
+  uint32_t off[kBatch][2];  // sorted position - stream position, species 0 / 1
   int32_t bin[kBatch];
   float bpoly[kBatch][24];
 };
@@ -625,9 +627,10 @@ struct __align__(16) StreamShared {
   float stage[kCells][kBatch][kMoments + 1];
   float scratch[kCells][96];  // a batch's B corners / the H rows of a flushed cell
   StreamMeta meta[kCells][kMetaSlots];
-  uint32_t more[2];  // byte w of word j & 1: warp w has a chunk after chunk j
-  uint64_t mma_bar;  // the MMAs of a chunk have completed
-  uint64_t full_bar; // the four warps have written a chunk's operands
+  uint32_t more[2];     // byte w of word j & 1: warp w has a chunk after chunk j
+  uint32_t arrived[2];  // arrivals of the chunks of each parity (monotonic)
+  uint32_t decision;    // (chunk << 1) | (some warp has a chunk after it)
+  uint64_t mma_bar;     // the MMAs of a chunk have completed
   uint32_t tmem_base;
 };
 
@@ -637,8 +640,7 @@ struct StreamLane {
   uint32_t idx, pos, flags;
 };
 // Warp-uniform chunk description: batch and bits (ended cells 0-3,
-// nonempty cells 4-7, parities 8-11, last chunk of the batch 12, valid 13,
-// metadata slot 14-15).
+// nonempty cells 4-7, parities 8-11, valid 13, metadata slot 14-15).
 struct StreamInfo {
   int bid;
   uint32_t bits;
@@ -671,9 +673,10 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
   }
   if (threadIdx.x == 0) {
     tc::mbar_init(&sh.mma_bar, 1);
-    tc::mbar_init(&sh.full_bar, kCells);
     tc::fence_mbar_init();
     sh.more[0] = sh.more[1] = 0u;
+    sh.arrived[0] = sh.arrived[1] = 0u;
+    sh.decision = 0xFFFFFFFEu;
   }
   tc::fence_before_sync();
   __syncthreads();
@@ -716,23 +719,44 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
     }
     return r;
   };
-  // Writes a batch's metadata into slot `slot`: counts, offsets, bins and
-  // the trilinear B of each cell as a polynomial in the cell fractions,
-  // B = c0 + c1 x + c2 y + c3 z + c4 xy + c5 xz + c6 yz + c7 xyz. Returns the
-  // nonempty cells (bits 0-3) and their parities (bits 4-7).
-  auto store_meta = [&](const MetaRegs& r, int slot) -> uint32_t {
-    StreamMeta& m = sh.meta[warp][slot];
+  // The walk: a warp-uniform cursor over this warp's batches. Per batch,
+  // the cumulative record starts of its cells (start of slot s = b[s],
+  // b[0] = 0, b[4] = total), the nonempty cells and their parities.
+  int cbid = blockIdx.x * kCells + warp;  // current batch
+  int cslot = 0;                          // its metadata slot
+  uint32_t cb1 = 0, cb2 = 0, cb3 = 0, ctot = 0;
+  uint32_t cbits = 0;  // nonempty | parity << 4 of the batch
+  uint32_t cbase = 0;  // stream position of the next chunk
+  uint32_t cdone = 0;  // cells of the batch already ended
+  bool cend = cbid >= batches, cnext = false;
+  // Writes a batch's metadata into its slot and sets the cursor's batch
+  // state: counts and offsets, bins and the trilinear B of each cell as a
+  // polynomial in the cell fractions,
+  // B = c0 + c1 x + c2 y + c3 z + c4 xy + c5 xz + c6 yz + c7 xyz.
+  auto enter_batch = [&](const MetaRegs& r) {
+    StreamMeta& m = sh.meta[warp][cslot];
     float* tmp = sh.scratch[warp];
+    const uint32_t n = r.c0 + r.c1;
+    uint32_t incl = n;  // inclusive scan over lanes 0..3
+#pragma unroll
+    for (int o = 1; o < kBatch; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+      if ((lane & 3) >= o) incl += t;
+    }
+    const uint32_t start = incl - n;
     if (lane < kBatch) {
-      m.n[lane] = r.c0 + r.c1;
-      m.c0[lane] = r.c0;
-      m.f0[lane] = r.f0;
-      m.f1[lane] = r.f1;
+      m.split[lane] = start + r.c0;
+      m.off[lane][0] = r.f0 - start;
+      m.off[lane][1] = r.f1 - (start + r.c0);
       m.bin[lane] = r.bin;
     }
 #pragma unroll
     for (int i = 0; i < 3; ++i) tmp[(lane & 3) * 24 + (lane >> 2) + 8 * i] = r.corner[i];
-    const uint32_t nonempty = __ballot_sync(0xffffffffu, lane < kBatch && r.c0 + r.c1 > 0u) & 0xFu;
+    cb1 = __shfl_sync(0xffffffffu, incl, 0);
+    cb2 = __shfl_sync(0xffffffffu, incl, 1);
+    cb3 = __shfl_sync(0xffffffffu, incl, 2);
+    ctot = __shfl_sync(0xffffffffu, incl, 3);
+    const uint32_t nonempty = __ballot_sync(0xffffffffu, lane < kBatch && n > 0u) & 0xFu;
     __syncwarp();
     if (lane < 3 * kBatch) {
       const int s = lane / 3, c = lane - 3 * s;
@@ -753,19 +777,13 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
     uint32_t parity = 0;
 #pragma unroll
     for (int s = 0; s < kBatch; ++s) parity |= (uint32_t(__popc(nonempty & ((1u << s) - 1u))) & 1u) << s;
-    return nonempty | (parity << 4);
+    cbits = nonempty | (parity << 4);
+    cbase = 0;
+    cdone = 0;
   };
-
-  // The walk (warp-uniform cursor over this warp's batches).
-  int cbid = blockIdx.x * kCells + warp;  // current batch
-  int cseq = 0;                           // batches entered so far - 1
-  int ca = 0;                             // cell slot of the next record
-  uint32_t co = 0;                        // records of that cell already taken
-  uint32_t cbits = 0;                     // nonempty | parity << 4 of the batch
-  bool cend = cbid >= batches, cnext = false;
   MetaRegs pf = fetch_meta(cbid);
   if (!cend) {
-    cbits = store_meta(pf, 0);
+    enter_batch(pf);
     pf = fetch_meta(cbid + W);
   }
   auto walk = [&](StreamLane& L, StreamInfo& I) {
@@ -774,77 +792,47 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
     if (cnext) {  // the previous chunk finished the batch
       cnext = false;
       cbid += W;
-      ++cseq;
+      cslot = cslot == kMetaSlots - 1 ? 0 : cslot + 1;
       if (cbid >= batches) {
         cend = true;
       } else {
-        cbits = store_meta(pf, cseq % kMetaSlots);
+        enter_batch(pf);
         pf = fetch_meta(cbid + W);
-        ca = 0;
-        co = 0;
       }
     }
     if (cend) return;
-    const StreamMeta& m = sh.meta[warp][cseq % kMetaSlots];
-    const uint32_t nonempty = cbits & 0xFu;
-    uint32_t ended = 0;
-    int a = ca;
-    while (a < kBatch && !((nonempty >> a) & 1u)) ended |= 1u << a++;
-    int slot = -1;
-    uint32_t k = 0;
-    int next_a = kBatch;
-    uint32_t next_o = 0;
-    if (a < kBatch) {
-      const uint32_t rem = m.n[a] - co;
-      if (uint32_t(lane) < rem) {
-        slot = a;
-        k = co + lane;
-      }
-      if (rem > 32u) {
-        next_a = a;
-        next_o = co + 32u;
-      } else {
-        ended |= 1u << a;
-        int b = a + 1;
-        while (b < kBatch && !((nonempty >> b) & 1u)) ended |= 1u << b++;
-        if (b < kBatch) {
-          const uint32_t nb = m.n[b];
-          if (uint32_t(lane) >= rem && uint32_t(lane) - rem < nb) {
-            slot = b;
-            k = lane - rem;
-          }
-          if (rem + nb <= 32u) {
-            ended |= 1u << b;
-            int c = b + 1;
-            while (c < kBatch && !((nonempty >> c) & 1u)) ended |= 1u << c++;
-            next_a = c;
-          } else {
-            next_a = b;
-            next_o = 32u - rem;
-          }
-        }
-      }
-    } else {
-      ended = 0xFu;
-    }
-    const bool last = next_a >= kBatch;
+    // The chunk [cbase, end): at most 32 records, and no record of a third
+    // nonempty cell: end <= the second cell boundary above cbase.
+    uint32_t first = ctot, second = ctot;
+    first = cb3 > cbase ? cb3 : first;
+    first = cb2 > cbase ? cb2 : first;
+    first = cb1 > cbase ? cb1 : first;
+    second = cb3 > first ? cb3 : second;
+    second = cb2 > first ? cb2 : second;
+    second = cb1 > first ? cb1 : second;
+    const uint32_t end = min(cbase + 32u, second);
+    // Cells ending in this chunk (empty cells at or below `end` included).
+    uint32_t ended = (cb1 <= end ? 1u : 0u) | (cb2 <= end ? 2u : 0u) | (cb3 <= end ? 4u : 0u) |
+                     (ctot <= end ? 8u : 0u);
+    ended &= ~cdone;
+    cdone |= ended;
+    const bool last = end >= ctot;
     I.bid = cbid;
-    I.bits = ended | ((cbits & 0xFFu) << 4) | (last ? 1u << 12 : 0u) | (1u << 13) |
-             (uint32_t(cseq % kMetaSlots) << 14);
-    if (slot >= 0) {
-      const uint32_t c0 = m.c0[slot];
-      const bool s1 = k >= c0;
-      L.pos = s1 ? m.f1[slot] + (k - c0) : m.f0[slot] + k;
+    I.bits = ended | ((cbits & 0xFFu) << 4) | (1u << 13) | (uint32_t(cslot) << 14);
+    const uint32_t p = cbase + lane;
+    if (p < end) {
+      const int slot = (p >= cb1 ? 1 : 0) + (p >= cb2 ? 1 : 0) + (p >= cb3 ? 1 : 0);
+      const StreamMeta& m = sh.meta[warp][cslot];
+      const uint32_t s1 = p >= m.split[slot] ? 1u : 0u;
+      L.pos = p + m.off[slot][s1];
       const uint32_t* perm = s1 ? tp.sp[1].perm : tp.sp[0].perm;
       L.idx = perm ? __ldg(perm + L.pos) : L.pos;
-      L.flags = 1u | (s1 ? 2u : 0u) | (uint32_t(slot) << 2) | (((cbits >> (4 + slot)) & 1u) << 4);
+      L.flags = 1u | (s1 << 1) | (uint32_t(slot) << 2) | (((cbits >> (4 + slot)) & 1u) << 4);
     }
-    if (last) {
+    if (last)
       cnext = true;
-    } else {
-      ca = next_a;
-      co = next_o;
-    }
+    else
+      cbase = end;
   };
   auto load_rec = [&](const StreamLane& L) {
     StreamRec r{0.0, 0.0, 0.0, 0.0, 0.0f, 0.0f, 0.0f, -1, L.pos, L.flags};
@@ -863,7 +851,7 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
     return r;
   };
   // Moments of the cells that ended in a chunk whose MMAs have completed;
-  // a batch's moments are stored when its last cell is done.
+  // a batch's moments are stored when its last cell (slot 3) is done.
   auto flush = [&](const StreamInfo& I) {
     const uint32_t ended = I.bits & 0xFu;
     if (!((I.bits >> 13) & 1u) || ended == 0u) return;
@@ -903,7 +891,7 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
         for (int q = lane; q < kMoments; q += 32) st[q] = 0.0f;
       }
     }
-    if ((I.bits >> 12) & 1u) {
+    if ((ended >> 3) & 1u) {
       __syncwarp();
       bool bad_value = false;
       float* base = mom + (long long)I.bid * kBatch;
@@ -937,7 +925,7 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
   walk(l2, i2);  // chunk 1
   StreamInfo ip{0, 0u};  // the previous chunk, whose cells are flushed next
   bool bad = false;
-  uint32_t issued = 0;   // chunks whose MMAs thread 0 committed
+  uint32_t last_arrived = 0xFFFFFFFFu;  // the last chunk this warp arrived for
   const int kofs = (lane >> 3) * 128 + (lane & 7) * 16;  // lane's K row in a 512-byte core group
   for (uint32_t j = 0;; ++j) {
     const StreamRec r0 = r1;
@@ -1022,12 +1010,18 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
       tc::fence_after_sync();
       flush(ip);
       if (!have) {
-        const bool seen = tc::mbar_wait(&sh.full_bar, (j - 1) & 1u);
+        // The issuer of chunk j - 1 published whether any warp has chunk j.
+        uint32_t d = 0;
+        bool seen = false;
+        for (uint32_t i = 0; i < (1u << 22) && !seen; ++i) {
+          d = tc::ld_acquire(&sh.decision);
+          seen = (d >> 1) == ((j - 1) & 0x7FFFFFFFu);
+        }
         if (__any_sync(0xffffffffu, !seen)) {
           bad = true;
           break;
         }
-        if (*reinterpret_cast<volatile uint32_t*>(&sh.more[(j - 1) & 1u]) == 0u) break;
+        if (!(d & 1u)) break;
       }
     }
     if (have) {
@@ -1067,39 +1061,36 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
     tc::fence_proxy_async_smem();
     tc::fence_before_sync();
     __syncwarp();
-    if (lane == 0) tc::mbar_arrive(&sh.full_bar);
-    if (warp == 0) {
-      bool ok = true;
-      if (lane == 0) {
-        ok = tc::mbar_wait(&sh.full_bar, j & 1u);
-        if (ok) {
-          tc::fence_after_sync();
-          const uint32_t ah = tc::smem_u32(sh.a[0]), al = tc::smem_u32(sh.a[1]);
-          const uint32_t bh = tc::smem_u32(sh.b[0]), bl = tc::smem_u32(sh.b[1]);
+    // Arrival: the warp whose add completes the chunk's four arrivals issues
+    // its MMAs (the counter of parity j & 1 has seen 4 (j >> 1) arrivals of
+    // the earlier chunks of that parity).
+    if (lane == 0) {
+      const uint32_t old = tc::atom_add_acq_rel(&sh.arrived[j & 1u], 1u);
+      if (old == 4u * (j >> 1) + 3u) {
+        const uint32_t any = *reinterpret_cast<volatile uint32_t*>(&sh.more[j & 1u]) != 0u ? 1u : 0u;
+        tc::st_release(&sh.decision, ((j & 0x7FFFFFFFu) << 1) | any);
+        tc::fence_after_sync();
+        const uint32_t ah = tc::smem_u32(sh.a[0]), al = tc::smem_u32(sh.a[1]);
+        const uint32_t bh = tc::smem_u32(sh.b[0]), bl = tc::smem_u32(sh.b[1]);
 #pragma unroll
-          for (int s = 0; s < 2; ++s) {
-            const uint64_t dah = tc::smem_desc(ah + s * 256, 128, 512), dal = tc::smem_desc(al + s * 256, 128, 512);
-            const uint64_t dbh = tc::smem_desc(bh + s * 256, 128, 512), dbl = tc::smem_desc(bl + s * 256, 128, 512);
-            tc::mma_f16_ss(tmem, dah, dbh, idesc, 1u);
-            tc::mma_f16_ss(tmem, dah, dbl, idesc, 1u);
-            tc::mma_f16_ss(tmem, dal, dbh, idesc, 1u);
-          }
-          tc::commit(&sh.mma_bar);
-          ++issued;
+        for (int s = 0; s < 2; ++s) {
+          const uint64_t dah = tc::smem_desc(ah + s * 256, 128, 512), dal = tc::smem_desc(al + s * 256, 128, 512);
+          const uint64_t dbh = tc::smem_desc(bh + s * 256, 128, 512), dbl = tc::smem_desc(bl + s * 256, 128, 512);
+          tc::mma_f16_ss(tmem, dah, dbh, idesc, 1u);
+          tc::mma_f16_ss(tmem, dah, dbl, idesc, 1u);
+          tc::mma_f16_ss(tmem, dal, dbh, idesc, 1u);
         }
-      }
-      if (!__shfl_sync(0xffffffffu, ok ? 1 : 0, 0)) {
-        bad = true;
-        break;
+        tc::commit(&sh.mma_bar);
       }
     }
+    last_arrived = j;
     ip = i0;
   }
 
   if (bad && lane == 0) atomicAdd(invalid, 1u << 20);
-  // After a failed wait MMAs may still be in flight: retire them (bounded)
-  // before the tensor memory is freed.
-  if (threadIdx.x == 0 && issued > 0) tc::mbar_wait(&sh.mma_bar, (issued - 1) & 1u);
+  // After a failed wait the MMAs of the last chunk may still be in flight:
+  // wait for them (bounded) before the tensor memory is freed.
+  if (bad && lane == 0 && last_arrived != 0xFFFFFFFFu) tc::mbar_wait(&sh.mma_bar, last_arrived & 1u);
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
