@@ -31,8 +31,9 @@
 // Operands are rounded to nearest (cvt.rna.tf32, bf16 RN split) so the
 // rounding is unbiased; accumulation is FP32. The epilogue reads G and H with
 // tcgen05.ld, forms the 8x3 corner currents and stores the cell's moments
-// (27x9 + 8x3 values, entry-major arrays over the unique cells; a later launch
-// adds to them in place). No atomics: the reference's flush issues up to 324
+// (27x9 + 8x3 values; each group of four consecutive cells has one
+// contiguous record of 16-byte words, word q = entry q of the four cells; a
+// later launch adds to them in place). No atomics: the reference's flush issues up to 324
 // atomics per cell (mass_matrix_mma_device.hpp:141-150).
 // assemble_moments_kernel then forms every record entry of a unique node as
 // the sum of the 1, 2, 4 or 8 cell moments that share it, in a fixed order.
@@ -61,6 +62,11 @@ constexpr int kFacStride = 36;     // floats per factor row (16-byte aligned row
 constexpr uint32_t kTmemCols = 128;
 constexpr int kMassMoments = 27 * 9;                  // G[t][c] per cell
 constexpr int kMoments = kMassMoments + 24;           // + J corner sums [a][c]
+// Moment layout: each group of four consecutive cells has one contiguous
+// record of kMoments 16-byte words, word q holding entry q of the four cells.
+__host__ __device__ constexpr long long moment_index(long long cell, int q) {
+  return ((cell >> 2) * kMoments + q) * 4 + (cell & 3);
+}
 constexpr uint32_t kDcol = 64;
 constexpr int kCtasPerSm = 4;      // 4 x 128 tensor-memory columns = all 512
 constexpr int kPermBuf = 256;      // ranks of a cell staged ahead (per warp and group)
@@ -160,7 +166,7 @@ __device__ __forceinline__ void split_pair(float2 v, uint32_t& hi, uint32_t& lo)
 
 template <bool Bf16>
 __global__ void __launch_bounds__(128, kCtasPerSm) tc_deposit_kernel(Geom g, TcParams tp,
-    const float* __restrict__ bnode, float* __restrict__ mom, long long mom_stride, int accumulate,
+    const float* __restrict__ bnode, float* __restrict__ mom, int accumulate,
     uint32_t* invalid) {
   using F = Form<Bf16>;
   constexpr int kCols = F::cols;
@@ -530,7 +536,8 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_deposit_kernel(Geom g, TcP
       for (int i = lane; i < kMoments; i += 32) stage[i] = 0.0f;
     }
     __syncthreads();
-    // Coalesced moment store: entry q of the group's four cells is 16 bytes.
+    // Moment store: entry q of the group's four cells is one 16-byte word of
+    // the group's contiguous record (coalesced across q).
     bool bad_value = false;
     for (int qi = threadIdx.x; qi < kMoments; qi += blockDim.x) {
       float4 val = make_float4(sh.stage[0][qi], sh.stage[1][qi], sh.stage[2][qi], sh.stage[3][qi]);
@@ -541,7 +548,7 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_deposit_kernel(Geom g, TcP
         val.z = isfinite(val.z) ? val.z : 0.0f;
         val.w = isfinite(val.w) ? val.w : 0.0f;
       }
-      float4* dst = reinterpret_cast<float4*>(mom + qi * mom_stride + grp * kCells);
+      float4* dst = reinterpret_cast<float4*>(mom + (grp * kMoments + qi) * kCells);
       if (accumulate) {
         const float4 old = *dst;
         val.x += old.x; val.y += old.y; val.z += old.z; val.w += old.w;
@@ -658,7 +665,7 @@ struct MetaRegs {
 };
 
 __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcParams tp,
-    const float* __restrict__ bnode, float* __restrict__ mom, long long mom_stride, int accumulate,
+    const float* __restrict__ bnode, float* __restrict__ mom, int accumulate,
     uint32_t* invalid, int batches) {
   extern __shared__ __align__(16) uint8_t stream_smem[];
   StreamShared& sh = *reinterpret_cast<StreamShared*>(stream_smem);
@@ -894,7 +901,7 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
     if ((ended >> 3) & 1u) {
       __syncwarp();
       bool bad_value = false;
-      float* base = mom + (long long)I.bid * kBatch;
+      float* base = mom + (long long)I.bid * kMoments * kBatch;
       for (int q = lane; q < kMoments; q += 32) {
         float4 val = make_float4(sh.stage[warp][0][q], sh.stage[warp][1][q], sh.stage[warp][2][q],
                                  sh.stage[warp][3][q]);
@@ -905,7 +912,7 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
           val.z = isfinite(val.z) ? val.z : 0.0f;
           val.w = isfinite(val.w) ? val.w : 0.0f;
         }
-        float4* dst = reinterpret_cast<float4*>(base + q * mom_stride);
+        float4* dst = reinterpret_cast<float4*>(base + q * kBatch);
         if (accumulate) {
           const float4 old = *dst;
           val.x += old.x; val.y += old.y; val.z += old.z; val.w += old.w;
@@ -1158,9 +1165,9 @@ cudaError_t launch_deposit_tc(int mass_kind, const Geom& g, int ns, const double
     }
     const int acc = (accumulate || first > 0) ? 1 : 0;
     if (tf32)
-      kernel<<<blocks, 128, pad, s>>>(g, tp, (const float*)bnode, moments, moment_stride(g), acc, invalid);
+      kernel<<<blocks, 128, pad, s>>>(g, tp, (const float*)bnode, moments, acc, invalid);
     else
-      tc_stream_kernel<<<blocks, 128, stream_bytes, s>>>(g, tp, (const float*)bnode, moments, moment_stride(g), acc,
+      tc_stream_kernel<<<blocks, 128, stream_bytes, s>>>(g, tp, (const float*)bnode, moments, acc,
                                                          invalid, int(groups));
     count_launches(1);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -1203,7 +1210,7 @@ __host__ __device__ constexpr StencilPairs make_stencil_pairs() {
 // was deposited); otherwise they are added.
 template <int S>
 __device__ __forceinline__ void assemble_stencil(const Geom& g, const long long (&cell)[8], long long node,
-                                                 const float* __restrict__ mom, long long stride,
+                                                 const float* __restrict__ mom,
                                                  float* __restrict__ J, float* __restrict__ M, int overwrite) {
   constexpr StencilPairs pairs = make_stencil_pairs();
   if constexpr (S < 14) {
@@ -1215,7 +1222,7 @@ __device__ __forceinline__ void assemble_stencil(const Geom& g, const long long 
       if (p < pairs.count[S]) {
 #pragma unroll
         for (int e = 0; e < 9; ++e)
-          sum[e] += __ldg(mom + (pairs.monomial[S][p] * 9 + e) * stride + cell[pairs.corner[S][p]]);
+          sum[e] += __ldg(mom + moment_index(cell[pairs.corner[S][p]], pairs.monomial[S][p] * 9 + e));
       }
     }
 #pragma unroll
@@ -1228,7 +1235,7 @@ __device__ __forceinline__ void assemble_stencil(const Geom& g, const long long 
     for (int c = 0; c < 3; ++c) {
       float sum = 0.0f;
 #pragma unroll
-      for (int a = 0; a < 8; ++a) sum += __ldg(mom + (kMassMoments + a * 3 + c) * stride + cell[a]);
+      for (int a = 0; a < 8; ++a) sum += __ldg(mom + moment_index(cell[a], kMassMoments + a * 3 + c));
       float* dst = J + c * g.nodes + node;
       *dst = overwrite ? sum : *dst + sum;
     }
@@ -1236,8 +1243,8 @@ __device__ __forceinline__ void assemble_stencil(const Geom& g, const long long 
 }
 
 __global__ void __launch_bounds__(128) assemble_moments_kernel(Geom g, const float* __restrict__ mom,
-                                                               long long stride, float* __restrict__ J,
-                                                               float* __restrict__ M, int overwrite) {
+                                                               float* __restrict__ J, float* __restrict__ M,
+                                                               int overwrite) {
   const int nx = g.nx, ny = g.ny;
   const long long unique = (long long)nx * ny * g.nz;
   const long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -1253,21 +1260,21 @@ __global__ void __launch_bounds__(128) assemble_moments_kernel(Geom g, const flo
     cell[a] = ((a & 1) ? i1 : i) + (long long)nx * (((a & 2) ? j1 : j) + (long long)ny * ((a & 4) ? k1 : k));
   const long long node = g.node(i, j, k);
   switch (blockIdx.y) {
-    case 0: assemble_stencil<0>(g, cell, node, mom, stride, J, M, overwrite); break;
-    case 1: assemble_stencil<1>(g, cell, node, mom, stride, J, M, overwrite); break;
-    case 2: assemble_stencil<2>(g, cell, node, mom, stride, J, M, overwrite); break;
-    case 3: assemble_stencil<3>(g, cell, node, mom, stride, J, M, overwrite); break;
-    case 4: assemble_stencil<4>(g, cell, node, mom, stride, J, M, overwrite); break;
-    case 5: assemble_stencil<5>(g, cell, node, mom, stride, J, M, overwrite); break;
-    case 6: assemble_stencil<6>(g, cell, node, mom, stride, J, M, overwrite); break;
-    case 7: assemble_stencil<7>(g, cell, node, mom, stride, J, M, overwrite); break;
-    case 8: assemble_stencil<8>(g, cell, node, mom, stride, J, M, overwrite); break;
-    case 9: assemble_stencil<9>(g, cell, node, mom, stride, J, M, overwrite); break;
-    case 10: assemble_stencil<10>(g, cell, node, mom, stride, J, M, overwrite); break;
-    case 11: assemble_stencil<11>(g, cell, node, mom, stride, J, M, overwrite); break;
-    case 12: assemble_stencil<12>(g, cell, node, mom, stride, J, M, overwrite); break;
-    case 13: assemble_stencil<13>(g, cell, node, mom, stride, J, M, overwrite); break;
-    default: assemble_stencil<14>(g, cell, node, mom, stride, J, M, overwrite); break;
+    case 0: assemble_stencil<0>(g, cell, node, mom, J, M, overwrite); break;
+    case 1: assemble_stencil<1>(g, cell, node, mom, J, M, overwrite); break;
+    case 2: assemble_stencil<2>(g, cell, node, mom, J, M, overwrite); break;
+    case 3: assemble_stencil<3>(g, cell, node, mom, J, M, overwrite); break;
+    case 4: assemble_stencil<4>(g, cell, node, mom, J, M, overwrite); break;
+    case 5: assemble_stencil<5>(g, cell, node, mom, J, M, overwrite); break;
+    case 6: assemble_stencil<6>(g, cell, node, mom, J, M, overwrite); break;
+    case 7: assemble_stencil<7>(g, cell, node, mom, J, M, overwrite); break;
+    case 8: assemble_stencil<8>(g, cell, node, mom, J, M, overwrite); break;
+    case 9: assemble_stencil<9>(g, cell, node, mom, J, M, overwrite); break;
+    case 10: assemble_stencil<10>(g, cell, node, mom, J, M, overwrite); break;
+    case 11: assemble_stencil<11>(g, cell, node, mom, J, M, overwrite); break;
+    case 12: assemble_stencil<12>(g, cell, node, mom, J, M, overwrite); break;
+    case 13: assemble_stencil<13>(g, cell, node, mom, J, M, overwrite); break;
+    default: assemble_stencil<14>(g, cell, node, mom, J, M, overwrite); break;
   }
 }
 
@@ -1277,7 +1284,7 @@ cudaError_t launch_assemble_moments(const Geom& g, const float* moments, void* j
                                     cudaStream_t s) {
   const long long unique = (long long)g.nx * g.ny * g.nz;
   const dim3 grid(unsigned((unique + 127) / 128), 15);
-  assemble_moments_kernel<<<grid, 128, 0, s>>>(g, moments, moment_stride(g), (float*)j, (float*)mass, overwrite);
+  assemble_moments_kernel<<<grid, 128, 0, s>>>(g, moments, (float*)j, (float*)mass, overwrite);
   count_launches(1);
   return cudaGetLastError();
 }
