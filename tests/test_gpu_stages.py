@@ -266,13 +266,15 @@ def test_field_advance_matches_oracle(torch_cuda, precision):
 
 # --------------------------------------------------------------------------
 # Tensor-core (tcgen05) mass assembly.
+@pytest.mark.parametrize("nx", [5, 8])
 @pytest.mark.parametrize("kind", [2, 3])
-def test_tc_exact_inputs(torch_cuda, kind):
+def test_tc_exact_inputs(torch_cuda, kind, nx):
     """Inputs exactly representable in TF32 (fractions in {0, 1/4, 1/2, 3/4},
     B = 0 so alpha = I, power-of-two charges): every product is exact, so the
     tensor-core mass matrix must equal the FP64 oracle to FP32 accumulation
-    rounding. Checks the operand layouts, descriptors and the pair epilogue."""
-    g = GridSpec(5, 4, 3, 5.0, 4.0, 3.0)
+    rounding. Checks the operand layouts, descriptors and the pair epilogue;
+    nx = 8 takes the four-node assembly, nx = 5 the per-node one."""
+    g = GridSpec(nx, 4, 3, float(nx), 4.0, 3.0)
     rng = np.random.default_rng(17)
     rows = []
     for cell in range(g.cells):
@@ -297,9 +299,10 @@ def test_tc_exact_inputs(torch_cuda, kind):
     assert np.abs(got - want).max() <= 1e-6 * np.abs(want).max()
 
 
-@pytest.mark.parametrize("kind,rel,layout", [(2, 3e-3, 0), (3, 1e-4, 0), (2, 3e-3, 1), (3, 1e-4, 1)])
-def test_tc_mass_matches_oracle(torch_cuda, kind, rel, layout):
-    g = GRID
+@pytest.mark.parametrize("kind,rel,layout,nx", [(2, 3e-3, 0, 6), (3, 1e-4, 0, 6), (2, 3e-3, 1, 6), (3, 1e-4, 1, 6),
+                                                 (3, 1e-4, 1, 8), (2, 3e-3, 0, 8)])
+def test_tc_mass_matches_oracle(torch_cuda, kind, rel, layout, nx):
+    g = GRID if nx == GRID.nx else GridSpec(nx, GRID.ny, GRID.nz, GRID.lx * nx / GRID.nx, GRID.ly, GRID.lz)
     rng = np.random.default_rng(23)
     d = species_arrays(g, 1, vth=(0.2, 0.1, 0.3), npcel=(4, 4, 4))
     n = len(d["cell"])

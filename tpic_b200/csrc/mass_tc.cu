@@ -1203,8 +1203,8 @@ __host__ __device__ constexpr StencilPairs make_stencil_pairs() {
 // of the node, each the sum, in increasing corner order, of the moments
 // G[t][e] of the cells holding the pairs (a, a + offset_s); "stencil" 14 is
 // the current, whose component c is the sum of the eight corner sums
-// J[a][c] of the cells around the node. The stencil is the grid's y index
-// and each case is unrolled from the compile-time tables, so a thread holds
+// J[a][c] of the cells around the node. The stencil is the block index
+// modulo 15 and each case is unrolled from the compile-time tables, so a thread holds
 // at most nine sums and the loads of a warp are consecutive across its
 // nodes. `overwrite` stores the sums (J and M were cleared and nothing else
 // was deposited); otherwise they are added.
@@ -1247,7 +1247,9 @@ __global__ void __launch_bounds__(128) assemble_moments_kernel(Geom g, const flo
                                                                int overwrite) {
   const int nx = g.nx, ny = g.ny;
   const long long unique = (long long)nx * ny * g.nz;
-  const long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  // The stencil is the fast block index (see assemble_quads_kernel).
+  const int stencil = int(blockIdx.x % 15);
+  const long long v = (blockIdx.x / 15) * (long long)blockDim.x + threadIdx.x;
   if (v >= unique) return;
   const int i = int(v % nx);
   const long long r = v / nx;
@@ -1259,7 +1261,7 @@ __global__ void __launch_bounds__(128) assemble_moments_kernel(Geom g, const flo
   for (int a = 0; a < 8; ++a)
     cell[a] = ((a & 1) ? i1 : i) + (long long)nx * (((a & 2) ? j1 : j) + (long long)ny * ((a & 4) ? k1 : k));
   const long long node = g.node(i, j, k);
-  switch (blockIdx.y) {
+  switch (stencil) {
     case 0: assemble_stencil<0>(g, cell, node, mom, J, M, overwrite); break;
     case 1: assemble_stencil<1>(g, cell, node, mom, J, M, overwrite); break;
     case 2: assemble_stencil<2>(g, cell, node, mom, J, M, overwrite); break;
@@ -1278,13 +1280,106 @@ __global__ void __launch_bounds__(128) assemble_moments_kernel(Geom g, const flo
   }
 }
 
+// Rows of a multiple of four cells: one thread per (four consecutive nodes
+// 4m .. 4m + 3 of an x-row, stencil), so that every 16-byte word of a
+// four-cell record serves four nodes at once. Corner a_x = 0 reads the
+// nodes' own group of cells (4m .. 4m + 3); corner a_x = 1 reads cells
+// 4m - 1 .. 4m + 2: the last cell of the previous group (periodic in x), then
+// the first three of the own group. Sums in increasing corner order, as the
+// per-node kernel.
+template <int S>
+__device__ __forceinline__ void assemble_quad(const Geom& g, int m, int j, int k, const float* __restrict__ mom,
+                                              float* __restrict__ J, float* __restrict__ M, int overwrite) {
+  constexpr StencilPairs pairs = make_stencil_pairs();
+  constexpr int kSums = S < 14 ? 9 : 3;
+  const int ny = g.ny, nz = g.nz, qx = g.nx >> 2;
+  const int j1 = j > 0 ? j - 1 : ny - 1, k1 = k > 0 ? k - 1 : nz - 1;
+  const int mp = m > 0 ? m - 1 : qx - 1;
+  const float4* mom4 = reinterpret_cast<const float4*>(mom);
+  float sum[kSums][4];
+#pragma unroll
+  for (int e = 0; e < kSums; ++e)
+#pragma unroll
+    for (int n = 0; n < 4; ++n) sum[e][n] = 0.0f;
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    const long long row = (long long)((a & 2) ? j1 : j) + (long long)ny * ((a & 4) ? k1 : k);
+    const long long own = row * qx + m, prev = row * qx + mp;
+    auto add = [&](int q, int e) {
+      const float4 v = __ldg(mom4 + own * kMoments + q);
+      if (a & 1) {
+        const float p3 = __ldg(mom + (prev * kMoments + q) * 4 + 3);
+        sum[e][0] += p3; sum[e][1] += v.x; sum[e][2] += v.y; sum[e][3] += v.z;
+      } else {
+        sum[e][0] += v.x; sum[e][1] += v.y; sum[e][2] += v.z; sum[e][3] += v.w;
+      }
+    };
+    if constexpr (S < 14) {
+#pragma unroll
+      for (int p = 0; p < 8; ++p)
+        if (p < pairs.count[S] && pairs.corner[S][p] == a)
+#pragma unroll
+          for (int e = 0; e < 9; ++e) add(pairs.monomial[S][p] * 9 + e, e);
+    } else {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) add(kMassMoments + a * 3 + c, c);
+    }
+  }
+#pragma unroll
+  for (int n = 0; n < 4; ++n) {
+    const long long node = g.node(4 * m + n, j, k);
+#pragma unroll
+    for (int e = 0; e < kSums; ++e) {
+      float* dst = S < 14 ? M + g.mass_index(node, S * 9 + e) : J + e * g.nodes + node;
+      *dst = overwrite ? sum[e][n] : *dst + sum[e][n];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(128) assemble_quads_kernel(Geom g, const float* __restrict__ mom,
+                                                             float* __restrict__ J, float* __restrict__ M,
+                                                             int overwrite) {
+  const int qx = g.nx >> 2, ny = g.ny;
+  const long long quads = (long long)qx * ny * g.nz;
+  // The stencil is the fast block index, so that the 15 blocks of the same
+  // nodes run together and share the cell moments in L2.
+  const int stencil = int(blockIdx.x % 15);
+  const long long v = (blockIdx.x / 15) * (long long)blockDim.x + threadIdx.x;
+  if (v >= quads) return;
+  const int m = int(v % qx);
+  const long long r = v / qx;
+  const int j = int(r % ny), k = int(r / ny);
+  switch (stencil) {
+    case 0: assemble_quad<0>(g, m, j, k, mom, J, M, overwrite); break;
+    case 1: assemble_quad<1>(g, m, j, k, mom, J, M, overwrite); break;
+    case 2: assemble_quad<2>(g, m, j, k, mom, J, M, overwrite); break;
+    case 3: assemble_quad<3>(g, m, j, k, mom, J, M, overwrite); break;
+    case 4: assemble_quad<4>(g, m, j, k, mom, J, M, overwrite); break;
+    case 5: assemble_quad<5>(g, m, j, k, mom, J, M, overwrite); break;
+    case 6: assemble_quad<6>(g, m, j, k, mom, J, M, overwrite); break;
+    case 7: assemble_quad<7>(g, m, j, k, mom, J, M, overwrite); break;
+    case 8: assemble_quad<8>(g, m, j, k, mom, J, M, overwrite); break;
+    case 9: assemble_quad<9>(g, m, j, k, mom, J, M, overwrite); break;
+    case 10: assemble_quad<10>(g, m, j, k, mom, J, M, overwrite); break;
+    case 11: assemble_quad<11>(g, m, j, k, mom, J, M, overwrite); break;
+    case 12: assemble_quad<12>(g, m, j, k, mom, J, M, overwrite); break;
+    case 13: assemble_quad<13>(g, m, j, k, mom, J, M, overwrite); break;
+    default: assemble_quad<14>(g, m, j, k, mom, J, M, overwrite); break;
+  }
+}
+
 }  // namespace
 
 cudaError_t launch_assemble_moments(const Geom& g, const float* moments, void* j, void* mass, int overwrite,
                                     cudaStream_t s) {
   const long long unique = (long long)g.nx * g.ny * g.nz;
-  const dim3 grid(unsigned((unique + 127) / 128), 15);
-  assemble_moments_kernel<<<grid, 128, 0, s>>>(g, moments, (float*)j, (float*)mass, overwrite);
+  const long long items = g.nx % 4 == 0 ? unique / 4 : unique;
+  const long long blocks = (items + 127) / 128 * 15;
+  if (blocks > 0x7FFFFFFFLL) return cudaErrorInvalidValue;
+  if (g.nx % 4 == 0)
+    assemble_quads_kernel<<<unsigned(blocks), 128, 0, s>>>(g, moments, (float*)j, (float*)mass, overwrite);
+  else
+    assemble_moments_kernel<<<unsigned(blocks), 128, 0, s>>>(g, moments, (float*)j, (float*)mass, overwrite);
   count_launches(1);
   return cudaGetLastError();
 }
