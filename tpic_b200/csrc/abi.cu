@@ -25,6 +25,8 @@ struct tpicb200_context {
   uint16_t* codes = nullptr;     // binned-sort run code per record
   uint32_t* invalid = nullptr;   // context's own invalid counter
   double* partials = nullptr;    // energy reduction partials
+  double* mover_partials = nullptr;  // species scalars of the cycle's movers (5 rows per species)
+  int mover_written[TPICB200_MAX_SPECIES]{};
   double* reduced = nullptr;     // energy reduction results
   double* pinned = nullptr;      // host mirror of `reduced` + invalid
   int energy_blocks = 0;
@@ -153,6 +155,7 @@ int tpicb200_create(const tpicb200_grid* grid, const tpicb200_options* options, 
   alloc((void**)&ctx->codes, size_t(options->max_particles) * 2);
   alloc((void**)&ctx->invalid, 4);
   alloc((void**)&ctx->partials, size_t(ctx->energy_blocks) * (2 + 5 * TPICB200_MAX_SPECIES) * 8);
+  alloc((void**)&ctx->mover_partials, size_t(kMoverPartials) * 5 * TPICB200_MAX_SPECIES * 8);
   alloc((void**)&ctx->reduced, (2 + 5 * TPICB200_MAX_SPECIES + 2) * 8);
   if (options->precision == TPICB200_PRECISION_MIXED) alloc((void**)&ctx->moments, moment_floats(ctx->g) * 4);
   if (e == cudaSuccess) e = cudaMallocHost((void**)&ctx->pinned, (2 + 5 * TPICB200_MAX_SPECIES + 2) * 8);
@@ -173,7 +176,7 @@ int tpicb200_destroy(tpicb200_context* ctx) {
   solver_destroy(ctx->solver);
   cudaFree(ctx->cursor); cudaFree(ctx->perm); cudaFree(ctx->perm2); cudaFree(ctx->scan); cudaFree(ctx->binned); cudaFree(ctx->codes);
   cudaFree(ctx->invalid);
-  cudaFree(ctx->partials); cudaFree(ctx->reduced); cudaFree(ctx->moments);
+  cudaFree(ctx->partials); cudaFree(ctx->mover_partials); cudaFree(ctx->reduced); cudaFree(ctx->moments);
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
   for (auto& ev : ctx->events)
     if (ev) cudaEventDestroy(ev);
@@ -203,7 +206,8 @@ int tpicb200_mover(tpicb200_context* ctx, double qom, tpicb200_particles* p, con
   const double beta = qom * ctx->opt.dt / 2;
   if (!std::isfinite(beta)) return fail(TPICB200_OVERFLOW, "q/m*dt/2 is not finite");
   return cuda_status(launch_mover(ctx->opt.precision, ctx->g, qom, ctx->opt.dt, ctx->opt.c, p, nullptr, nullptr,
-                                  e_theta, b_node, invalid_or_own(ctx, invalid), nullptr, (cudaStream_t)stream),
+                                  e_theta, b_node, invalid_or_own(ctx, invalid), nullptr, nullptr,
+                                  (cudaStream_t)stream),
                      "mover launch failed");
 }
 
@@ -499,7 +503,7 @@ struct DepositPlan {
 // On smaller grids the mover moves in place and the general sort writes the
 // sorted records.
 static int move_and_sort(tpicb200_context* ctx, tpicb200_state* st, int sp, uint32_t* perm, cudaEvent_t moved,
-                         cudaEvent_t sorted, DepositPlan* plan, cudaStream_t s) {
+                         cudaEvent_t sorted, DepositPlan* plan, const SpeciesScalars* scalars, cudaStream_t s) {
   const int cur = st->current[sp];
   tpicb200_particles* in = &st->slot[sp][cur];
   tpicb200_particles* out = &st->slot[sp][1 - cur];
@@ -517,7 +521,7 @@ static int move_and_sort(tpicb200_context* ctx, tpicb200_state* st, int sp, uint
   if (!binned_sort_applies(ctx->g)) {
     if (st->ranked[sp]) return fail(TPICB200_INVALID_STATE, "ranked species on a grid without the binned sort");
     cudaError_t e = launch_mover(p, ctx->g, qom, ctx->opt.dt, ctx->opt.c, in, nullptr, nullptr, st->e_theta,
-                                 st->b_node, ctx->invalid, nullptr, s);
+                                 st->b_node, ctx->invalid, nullptr, scalars, s);
     if (e == cudaSuccess) e = cudaEventRecord(moved, s);
     if (e == cudaSuccess)
       e = launch_sort(p, ctx->g, in, out, st->counts[sp], st->offsets[sp], ctx->cursor, perm, ctx->scan,
@@ -535,7 +539,7 @@ static int move_and_sort(tpicb200_context* ctx, tpicb200_state* st, int sp, uint
     // Out of place: the moved records, in the previous sorted order, go live.
     if (e == cudaSuccess)
       e = launch_mover(p, ctx->g, qom, ctx->opt.dt, ctx->opt.c, in, out, st->ranked[sp] ? st->ranks[sp] : nullptr,
-                       st->e_theta, st->b_node, ctx->invalid, &b, s);
+                       st->e_theta, st->b_node, ctx->invalid, &b, scalars, s);
     if (e == cudaSuccess) e = cudaEventRecord(moved, s);
     if (e == cudaSuccess)
       e = binned_finish(p, ctx->g, b, false, false, out, in, st->counts[sp], st->offsets[sp], ctx->cursor,
@@ -550,7 +554,7 @@ static int move_and_sort(tpicb200_context* ctx, tpicb200_state* st, int sp, uint
   if (st->ranked[sp]) return fail(TPICB200_INVALID_STATE, "ranked species without a rank buffer");
   if (e == cudaSuccess)
     e = launch_mover(p, ctx->g, qom, ctx->opt.dt, ctx->opt.c, in, nullptr, nullptr, st->e_theta, st->b_node,
-                     ctx->invalid, &b, s);
+                     ctx->invalid, &b, scalars, s);
   if (e == cudaSuccess) e = cudaEventRecord(moved, s);
   if (e == cudaSuccess)
     e = binned_finish(p, ctx->g, b, false, false, in, out, st->counts[sp], st->offsets[sp], ctx->cursor, perm,
@@ -637,6 +641,27 @@ static int read_invalid(tpicb200_context* ctx, cudaStream_t s, uint32_t* value) 
   return TPICB200_SUCCESS;
 }
 
+// The cycle's energy report: the field energies of the committed fields and
+// the species scalars the movers accumulated (the values tpicb200_energy
+// computes from the live slots, summed in the movers' block order).
+static int cycle_energy(tpicb200_context* ctx, const tpicb200_state* st, double* out, cudaStream_t s) {
+  const int blocks = ctx->energy_blocks;
+  cudaError_t err = launch_field_energy(ctx->opt.precision, ctx->g, st->e, st->b_cell, ctx->partials, blocks, s);
+  if (err == cudaSuccess) err = launch_reduce_rows(ctx->partials, ctx->reduced, 2, blocks, blocks, 2, s);
+  for (int sp = 0; sp < st->ns && err == cudaSuccess; ++sp)
+    err = launch_reduce_rows(ctx->mover_partials + size_t(kMoverPartials) * 5 * sp, ctx->reduced + 2 + 5 * sp, 5,
+                             kMoverPartials, ctx->mover_written[sp], ctx->mover_written[sp] > 0 ? 5 : 0, s);
+  const int rows = 2 + 5 * st->ns;
+  if (err == cudaSuccess) err = cudaMemcpyAsync(ctx->pinned, ctx->reduced, rows * 8, cudaMemcpyDeviceToHost, s);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+  if (err != cudaSuccess) return cuda_status(err, "energy reduction failed");
+  const double norm = ctx->g.volume / (8 * 3.14159265358979323846);
+  out[0] = norm * ctx->pinned[0];
+  out[1] = norm * ctx->pinned[1];
+  for (int r = 2; r < rows; ++r) out[r] = ctx->pinned[r];
+  return TPICB200_SUCCESS;
+}
+
 int tpicb200_cycle(tpicb200_context* ctx, tpicb200_state* st, int ncycles, tpicb200_cycle_report* reports,
                    tpicb200_stream stream) {
   if (int s = check_ctx(ctx)) return s;
@@ -666,10 +691,14 @@ int tpicb200_cycle(tpicb200_context* ctx, tpicb200_state* st, int ncycles, tpicb
     for (int first = 0; first < st->ns; first += 2) {
       const int count = st->ns - first < 2 ? st->ns - first : 2;
       DepositPlan plan[2];
-      for (int i = 0; i < count; ++i)
-        if (int r = move_and_sort(ctx, st, first + i, perms[i], sev[3 * (first + i)], sev[3 * (first + i) + 1],
-                                  &plan[i], s))
+      for (int i = 0; i < count; ++i) {
+        const int sp = first + i;
+        const SpeciesScalars scalars{ctx->mover_partials + size_t(kMoverPartials) * 5 * sp, kMoverPartials,
+                                     &ctx->mover_written[sp]};
+        if (int r = move_and_sort(ctx, st, sp, perms[i], sev[3 * sp], sev[3 * sp + 1], &plan[i],
+                                  reports ? &scalars : nullptr, s))
           return r;
+      }
       if (int r = deposit_pair(ctx, st, first, count, plan, first > 0, s)) return r;
       cudaEventRecord(sev[3 * first + 2], s);
     }
@@ -678,10 +707,8 @@ int tpicb200_cycle(tpicb200_context* ctx, tpicb200_state* st, int ncycles, tpicb
     std::swap(st->b_cell, st->b_cell_next);
     std::swap(st->b_node, st->b_node_next);
     if (reports) {
-      tpicb200_particles live[TPICB200_MAX_SPECIES];
-      for (int sp = 0; sp < st->ns; ++sp) live[sp] = st->slot[sp][st->current[sp]];
       double out[2 + 5 * TPICB200_MAX_SPECIES];
-      if (int r = tpicb200_energy(ctx, st->e, st->b_cell, live, st->qom, st->ns, out, stream)) return r;
+      if (int r = cycle_energy(ctx, st, out, s)) return r;
       report.field_energy[0] = out[0];
       report.field_energy[1] = out[1];
       report.total_energy = out[0] + out[1];

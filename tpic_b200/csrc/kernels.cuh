@@ -10,14 +10,25 @@ void count_launches(unsigned n);
 
 // mover.cu
 struct BinnedScratch;
+// Species scalars accumulated by the movers (kinetic energy, charge,
+// momentum of the moved records): row r of the partial sums at
+// partials + r * stride, `written` partials per row (set by launch_mover;
+// at most kMoverPartials).
+constexpr int kMoverPartials = 2 * 148 * 8;
+struct SpeciesScalars {
+  double* partials;
+  long long stride;
+  int* written;
+};
 // With `binned`, the mover also writes direction codes and transfer counts
 // for binned_finish (after binned_begin with zeroed transfer counts).
 // out (null: in place) receives the moved records, read through ranks when
-// given (position p of out <- record ranks[p] of p).
+// given (position p of out <- record ranks[p] of p). With `scalars`, the
+// species scalars of the moved records.
 cudaError_t launch_mover(int precision, const Geom& g, double qom, double dt, double c,
                          tpicb200_particles* p, tpicb200_particles* out, const uint32_t* ranks,
                          const double* theta, const void* bnode, uint32_t* invalid, const BinnedScratch* binned,
-                         cudaStream_t s);
+                         const SpeciesScalars* scalars, cudaStream_t s);
 
 // sort.cu: scratch needs `bins` cursor words, `capacity` permutation words and
 // the scan workspace returned by sort_scan_words().

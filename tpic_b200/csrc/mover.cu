@@ -37,7 +37,50 @@ template <class P>
 struct MoverParams {
   typename P::VC beta, beta_over_c;
   double dt, inv[3];
+  double inverse_qom;
 };
+
+// Species scalars of the moved records (the sums of species_kernel:
+// kinetic energy, charge, momentum), accumulated by the movers: each block
+// writes its five partial sums at partials[r * stride + offset + block].
+struct MoverScalars {
+  double* partials;  // null: not accumulated
+  long long stride;
+  int offset;
+};
+
+// Per-thread sums of the five scalars: in registers (RegisterSums) or, where
+// registers are short, in the thread's column of a shared-memory array
+// (SharedSums: entry r at sums[r * 32]).
+struct RegisterSums {
+  double (&acc)[5];
+  __device__ __forceinline__ void add(int r, double v) const { acc[r] += v; }
+};
+struct SharedSums {
+  double* sums;
+  __device__ __forceinline__ void add(int r, double v) const { sums[r * 32] += v; }
+};
+template <class Sums>
+__device__ __forceinline__ void add_scalars(const Sums& acc, double charge, double inverse_qom, double vx, double vy,
+                                            double vz) {
+  const double mass = charge * inverse_qom;
+  acc.add(0, 0.5 * mass * (vx * vx + vy * vy + vz * vz));
+  acc.add(1, charge);
+  acc.add(2, mass * vx);
+  acc.add(3, mass * vy);
+  acc.add(4, mass * vz);
+}
+
+// Block sums of the five scalars into the block's partials (every thread of
+// the block calls it; scratch holds Threads / 32 doubles).
+template <int Threads>
+__device__ __forceinline__ void store_scalars(const MoverScalars& sc, const double (&acc)[5], double* scratch) {
+#pragma unroll
+  for (int r = 0; r < 5; ++r) {
+    const double total = block_sum<Threads>(acc[r], scratch);
+    if (threadIdx.x == 0) sc.partials[r * sc.stride + sc.offset + blockIdx.x] = total;
+  }
+}
 
 // Direction codes and transfer counts of a mover that feeds the binned sort.
 struct MoveCodes {
@@ -117,10 +160,11 @@ __device__ __forceinline__ C gather8(const F& field, int which, int c, const C w
 // The push of record n, whose valid interior cell (ci, cj, ck) was decoded
 // from its key. Returns the direction code of the move (-1: invalid, or a
 // move beyond the 27 neighbouring cells when Coded).
-template <class P, bool Coded, class F>
+template <class P, bool Coded, class F, class Sums>
 __device__ __forceinline__ int push(const Geom& g, const MoverParams<P>& mp, const MoveIo<P>& io, uint32_t n,
                                     uint32_t p, int ci, int cj, int ck, typename P::Pos fx, typename P::Pos fy,
-                                    typename P::Pos fz, double charge, const F& field, uint32_t* invalid) {
+                                    typename P::Pos fz, double charge, const F& field, uint32_t* invalid,
+                                    const Sums* acc) {
   const Records<P>& r = io.in;
   using C = typename P::VC;
   using Pos = typename P::Pos;
@@ -171,6 +215,7 @@ __device__ __forceinline__ int push(const Geom& g, const MoverParams<P>& mp, con
       cell[axis] = m < 0 ? m + e : m;
     }
   }
+  if (acc) add_scalars(*acc, charge, mp.inverse_qom, double(vel[0]), double(vel[1]), double(vel[2]));
   const Records<P>& o = io.out;
   o.key[p] = g.encode(int(cell[0]), int(cell[1]), int(cell[2]));
   o.rx[p] = frac[0]; o.ry[p] = frac[1]; o.rz[p] = frac[2];
@@ -230,9 +275,14 @@ __device__ __forceinline__ void record_codes(const MoveCodes& mc, bool live, uin
 template <class P>
 __global__ void __launch_bounds__(256, TPICB200_MOVER_MIN_BLOCKS) mover_kernel(Geom g, MoverParams<P> mp,
     MoveIo<P> io, uint32_t count, const double* __restrict__ theta, const typename P::Fld* __restrict__ bnode,
-    uint32_t* __restrict__ invalid, const uint32_t* gate) {
+    uint32_t* __restrict__ invalid, const uint32_t* gate, MoverScalars sc) {
   using Pos = typename P::Pos;
-  if (gate && *gate == 0) return;
+  __shared__ double scratch[8];
+  double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  if (gate && *gate == 0) {
+    if (sc.partials && threadIdx.x < 5) sc.partials[threadIdx.x * sc.stride + sc.offset + blockIdx.x] = 0.0;
+    return;
+  }
   const Records<P>& r = io.in;
   for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < count; p += gridDim.x * blockDim.x) {
     const uint32_t n = io.ranks ? io.ranks[p] : p;
@@ -241,13 +291,15 @@ __global__ void __launch_bounds__(256, TPICB200_MOVER_MIN_BLOCKS) mover_kernel(G
     const Pos fx = r.rx[n], fy = r.ry[n], fz = r.rz[n];
     int ci, cj, ck;
     if (record_ok<P>(g, k0, charge, fx, fy, fz, ci, cj, ck)) {
+      const RegisterSums sums{acc};
       push<P, false>(g, mp, io, n, p, ci, cj, ck, fx, fy, fz, charge, global_fields<P>(g, theta, bnode, ci, cj, ck),
-                     invalid);
+                     invalid, sc.partials ? &sums : nullptr);
     } else {
       atomicAdd(invalid, 1u);
       copy_record(io, n, p);
     }
   }
+  if (sc.partials) store_scalars<256>(sc, acc, scratch);
 }
 
 // Runs of up to kRunCells cells of one x-row; records grouped by the bins
@@ -259,15 +311,24 @@ template <class P>
 __global__ void __launch_bounds__(kRunWarps * 32, 2 * TPICB200_MOVER_MIN_BLOCKS) run_mover_kernel(Geom g,
     MoverParams<P> mp, MoveIo<P> io, uint32_t count, const double* __restrict__ theta,
     const typename P::Fld* __restrict__ bnode, const uint32_t* __restrict__ old_counts,
-    const uint32_t* __restrict__ old_offsets, uint32_t* __restrict__ invalid, MoveCodes mc) {
+    const uint32_t* __restrict__ old_offsets, uint32_t* __restrict__ invalid, MoveCodes mc, MoverScalars sc) {
   using C = typename P::VC;
   using Pos = typename P::Pos;
   constexpr int kStaged = 2 * 3 * 2 * 2 * kRunNodes;
   __shared__ C fields[kRunWarps][kStaged];
   __shared__ uint32_t starts[kRunWarps][kRunCells];
-  if (*mc.bins_bad) return;
+  __shared__ double scratch[kRunWarps];
+  __shared__ double lane_sums[kRunWarps][5][32];
+  if (*mc.bins_bad) {
+    if (sc.partials && threadIdx.x < 5) sc.partials[threadIdx.x * sc.stride + sc.offset + blockIdx.x] = 0.0;
+    return;
+  }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const long long runs = run_count(g);
+  const SharedSums sums{&lane_sums[warp][0][lane]};
+#pragma unroll
+  for (int r = 0; r < 5; ++r) lane_sums[warp][r][lane] = 0.0;
+  const SharedSums* acc = sc.partials ? &sums : nullptr;
   C* sf = fields[warp];
   uint32_t* st = starts[warp];
   for (long long run = (long long)blockIdx.x * kRunWarps + warp; run < runs; run += (long long)gridDim.x * kRunWarps) {
@@ -315,10 +376,11 @@ __global__ void __launch_bounds__(kRunWarps * 32, 2 * TPICB200_MOVER_MIN_BLOCKS)
         int ci, cj, ck;
         if (record_ok<P>(g, k0, charge, fx, fy, fz, ci, cj, ck)) {
           if (ci == i0 + c && cj == j && ck == k)
-            d = push<P, true>(g, mp, io, n, p, ci, cj, ck, fx, fy, fz, charge, SharedFields<C>{sf, c}, invalid);
+            d = push<P, true>(g, mp, io, n, p, ci, cj, ck, fx, fy, fz, charge, SharedFields<C>{sf, c}, invalid,
+                              acc);
           else
             d = push<P, true>(g, mp, io, n, p, ci, cj, ck, fx, fy, fz, charge,
-                              global_fields<P>(g, theta, bnode, ci, cj, ck), invalid);
+                              global_fields<P>(g, theta, bnode, ci, cj, ck), invalid, acc);
           old_cell = ci + (long long)g.nx * (cj + (long long)g.ny * ck);
         } else {
           atomicAdd(invalid, 1u);
@@ -328,6 +390,12 @@ __global__ void __launch_bounds__(kRunWarps * 32, 2 * TPICB200_MOVER_MIN_BLOCKS)
       record_codes(mc, live, p, d, c, old_cell);
     }
     __syncwarp();
+  }
+  if (sc.partials) {
+    double own[5];
+#pragma unroll
+    for (int r = 0; r < 5; ++r) own[r] = lane_sums[warp][r][lane];
+    store_scalars<kRunWarps * 32>(sc, own, scratch);
   }
 }
 
@@ -339,6 +407,7 @@ MoverParams<P> mover_params(const Geom& g, double qom, double dt, double c) {
   mp.beta_over_c = typename P::VC(beta / c);
   mp.dt = dt;
   for (int a = 0; a < 3; ++a) mp.inv[a] = 1.0 / (a == 0 ? g.dx : a == 1 ? g.dy : g.dz);
+  mp.inverse_qom = 1.0 / qom;
   return mp;
 }
 
@@ -351,15 +420,18 @@ Records<P> records(const tpicb200_particles* p) {
 template <class P>
 cudaError_t launch(const Geom& g, double qom, double dt, double c, tpicb200_particles* p, tpicb200_particles* out,
                    const uint32_t* ranks, const double* theta, const void* bnode, uint32_t* invalid,
-                   const BinnedScratch* binned, cudaStream_t s) {
+                   const BinnedScratch* binned, const SpeciesScalars* scalars, cudaStream_t s) {
   const MoverParams<P> mp = mover_params<P>(g, qom, dt, c);
+  if (scalars) *scalars->written = 0;
   if (p->count == 0) return cudaSuccess;
   const unsigned blocks = grid_for(p->count, 256, 148u * 8u);
   const MoveIo<P> io{records<P>(p), records<P>(out ? out : p), ranks, out != nullptr && out != p};
   const auto* bn = (const typename P::Fld*)bnode;
+  MoverScalars sc{scalars ? scalars->partials : nullptr, scalars ? scalars->stride : 0, 0};
   if (!binned) {
-    mover_kernel<P><<<blocks, 256, 0, s>>>(g, mp, io, p->count, theta, bn, invalid, nullptr);
+    mover_kernel<P><<<blocks, 256, 0, s>>>(g, mp, io, p->count, theta, bn, invalid, nullptr, sc);
     count_launches(1);
+    if (scalars) *scalars->written = int(blocks);
     return cudaGetLastError();
   }
   // Bins checked by validate_bins: the run mover; otherwise the per-record
@@ -368,10 +440,13 @@ cudaError_t launch(const Geom& g, double qom, double dt, double c, tpicb200_part
   MoveCodes mc{binned->code, binned->transfer, &binned->state->fallback, &binned->state->bins_bad,
                (long long)g.nx * g.ny * g.nz};
   const long long runs = run_count(g);
-  run_mover_kernel<P><<<grid_for(runs * 32, kRunWarps * 32, 148u * 8u), kRunWarps * 32, 0, s>>>(
-      g, mp, io, p->count, theta, bn, binned->old_counts, binned->old_offsets, invalid, mc);
-  mover_kernel<P><<<blocks, 256, 0, s>>>(g, mp, io, p->count, theta, bn, invalid, &binned->state->bins_bad);
+  const unsigned run_blocks = grid_for(runs * 32, kRunWarps * 32, 148u * 8u);
+  run_mover_kernel<P><<<run_blocks, kRunWarps * 32, 0, s>>>(g, mp, io, p->count, theta, bn, binned->old_counts,
+                                                            binned->old_offsets, invalid, mc, sc);
+  sc.offset = int(run_blocks);
+  mover_kernel<P><<<blocks, 256, 0, s>>>(g, mp, io, p->count, theta, bn, invalid, &binned->state->bins_bad, sc);
   count_launches(2);
+  if (scalars) *scalars->written = int(run_blocks + blocks);
   return cudaGetLastError();
 }
 
@@ -380,10 +455,10 @@ cudaError_t launch(const Geom& g, double qom, double dt, double c, tpicb200_part
 cudaError_t launch_mover(int precision, const Geom& g, double qom, double dt, double c,
                          tpicb200_particles* p, tpicb200_particles* out, const uint32_t* ranks,
                          const double* theta, const void* bnode, uint32_t* invalid, const BinnedScratch* binned,
-                         cudaStream_t s) {
+                         const SpeciesScalars* scalars, cudaStream_t s) {
   if (precision == TPICB200_PRECISION_DOUBLE)
-    return launch<PDouble>(g, qom, dt, c, p, out, ranks, theta, bnode, invalid, binned, s);
-  return launch<PMixed>(g, qom, dt, c, p, out, ranks, theta, bnode, invalid, binned, s);
+    return launch<PDouble>(g, qom, dt, c, p, out, ranks, theta, bnode, invalid, binned, scalars, s);
+  return launch<PMixed>(g, qom, dt, c, p, out, ranks, theta, bnode, invalid, binned, scalars, s);
 }
 
 }  // namespace tpicb200
