@@ -228,15 +228,20 @@ __device__ __forceinline__ int push(const Geom& g, const MoverParams<P>& mp, con
 }
 
 // Record checks before the push: a valid interior key, a finite charge and
-// fractions in [0, 1). Writes the decoded cell.
+// fractions in [0, 1). record_ok writes the decoded cell; fields_ok checks
+// a record whose key is already known to be a given interior cell's.
+template <class P>
+__device__ __forceinline__ bool fields_ok(double charge, typename P::Pos fx, typename P::Pos fy, typename P::Pos fz) {
+  using Pos = typename P::Pos;
+  return isfinite(charge) && fx >= Pos(0) && fx < Pos(1) && fy >= Pos(0) && fy < Pos(1) && fz >= Pos(0) &&
+         fz < Pos(1);
+}
 template <class P>
 __device__ __forceinline__ bool record_ok(const Geom& g, int32_t k0, double charge, typename P::Pos fx,
                                           typename P::Pos fy, typename P::Pos fz, int& ci, int& cj, int& ck) {
-  using Pos = typename P::Pos;
   if (!(k0 >= 0 && (long long)k0 < g.bins)) return false;
   g.decode(k0, ci, cj, ck);
-  return g.interior_cell(ci, cj, ck) && isfinite(charge) && fx >= Pos(0) && fx < Pos(1) && fy >= Pos(0) &&
-         fy < Pos(1) && fz >= Pos(0) && fz < Pos(1);
+  return g.interior_cell(ci, cj, ck) && fields_ok<P>(charge, fx, fy, fz);
 }
 
 template <class P>
@@ -373,9 +378,11 @@ __global__ void __launch_bounds__(kRunWarps * 32, 2 * TPICB200_MOVER_MIN_BLOCKS)
 #pragma unroll
         for (int step = 16; step > 0; step >>= 1)
           if (st[c + step] <= p) c += step;
-        int ci, cj, ck;
-        if (record_ok<P>(g, k0, charge, fx, fy, fz, ci, cj, ck)) {
-          if (ci == i0 + c && cj == j && ck == k)
+        int ci = i0 + c, cj = j, ck = k;
+        // A record in its bin's cell needs no key decode.
+        const bool home = k0 == g.encode(ci, cj, ck);
+        if (home ? fields_ok<P>(charge, fx, fy, fz) : record_ok<P>(g, k0, charge, fx, fy, fz, ci, cj, ck)) {
+          if (home)
             d = push<P, true>(g, mp, io, n, p, ci, cj, ck, fx, fy, fz, charge, SharedFields<C>{sf, c}, invalid,
                               acc);
           else
