@@ -322,19 +322,53 @@ def stage_kernel_times(sim, args, stream, repeats: int = 5) -> dict:
     scratch_inv = torch.zeros(1, dtype=torch.int32, device="cuda")
 
     # Deposition (current + mass) of all species from the sorted records, as
-    # the cycle runs it: one multi-species call, then the fold (which also
-    # assembles the tensor-core forms' cell moments).
+    # the cycle runs it: one multi-species call. The tensor-core forms write
+    # per-cell moments (267 floats per cell, groups of four cells), which the
+    # fold assembles; the scalar forms deposit J and the mass records.
+    cells = g.nx * g.ny * g.nz
+    tc_form = st.mass_kind in (_lib.MASS_KINDS["tf32"], _lib.MASS_KINDS["bf16x3"])
+    moment_bytes = 267 * 4 * ((cells + 3) // 4 * 4)
+    parts = (_lib.Particles * ns)(*[st.slot[s][st.current[s]] for s in range(ns)])
+    qom = (C.c_double * ns)(*[st.qom[s] for s in range(ns)])
+    counts = (C.c_void_p * ns)(*[st.counts[s] for s in range(ns)])
+    offsets = (C.c_void_p * ns)(*[st.offsets[s] for s in range(ns)])
+
     def deposit():
-        _lib.check(lib.tpicb200_clear_moments(sim.ctx, st.j, st.mass, s_))
-        parts = (_lib.Particles * ns)(*[st.slot[s][st.current[s]] for s in range(ns)])
-        qom = (C.c_double * ns)(*[st.qom[s] for s in range(ns)])
-        counts = (C.c_void_p * ns)(*[st.counts[s] for s in range(ns)])
-        offsets = (C.c_void_p * ns)(*[st.offsets[s] for s in range(ns)])
         _lib.check(lib.tpicb200_deposit_species(sim.ctx, ns, qom, parts, counts, offsets, st.b_node, st.j, st.mass,
                                                 st.mass_kind, scratch_inv.data_ptr(), s_))
+
+    def clear_and_deposit():
+        _lib.check(lib.tpicb200_clear_moments(sim.ctx, st.j, st.mass, s_))
+        deposit()
+
+    def fold():
         _lib.check(lib.tpicb200_fold_periodic(sim.ctx, st.j, st.mass, s_))
-    out["deposit"] = {"ms": timed(deposit),
-                      "bytes": n_total * (24 + 3 * vb + 8 + 4) + nodes * (126 + 3) * fb}
+
+    def timed_after(setup, fn):
+        """Device time of fn alone, after an untimed setup before each run."""
+        setup()
+        fn()
+        torch.cuda.synchronize()
+        total = 0.0
+        for _ in range(repeats):
+            setup()
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            fn()
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            total += ev0.elapsed_time(ev1)
+        return total / repeats
+
+    clear = lambda: _lib.check(lib.tpicb200_clear_moments(sim.ctx, st.j, st.mass, s_))
+    out["deposit"] = {"ms": timed_after(clear, deposit),
+                      "bytes": n_total * (24 + 3 * vb + 8 + 4) + (moment_bytes if tc_form else
+                                                                  nodes * (126 + 3) * fb)}
+    # The fold: for the tensor-core forms the moment assembly (moments read,
+    # J and the mass records written) and the periodic fold.
+    clear_and_deposit()
+    out["assembly"] = {"ms": timed(fold),
+                       "bytes": (moment_bytes if tc_form else 0) + nodes * (126 + 3) * fb}
 
     # Sort of all species as the cycle runs it (the binned sort of records
     # grouped by the live bins; ping-pong into the idle slot and back).

@@ -687,7 +687,15 @@ int tpicb200_cycle(tpicb200_context* ctx, tpicb200_state* st, int ncycles, tpicb
     cudaEventRecord(ev[2], s);
     // Per pair of species: the mover and the sort of each, then one
     // deposition of both with the next B that also writes the sorted records.
-    if (int r = tpicb200_clear_moments(ctx, st->j, st->mass, stream)) return r;
+    // The tensor-core forms need no cleared J and mass: the assembly stores
+    // every entry of the unique nodes and the fold copies every other vertex.
+    if ((kind == TPICB200_MASS_TF32 || kind == TPICB200_MASS_BF16X3) && st->ns > 0) {
+      ctx->moments_pending = false;
+      ctx->cleared_j = st->j;
+      ctx->cleared_mass = st->mass;
+    } else if (int r = tpicb200_clear_moments(ctx, st->j, st->mass, stream)) {
+      return r;
+    }
     for (int first = 0; first < st->ns; first += 2) {
       const int count = st->ns - first < 2 ? st->ns - first : 2;
       DepositPlan plan[2];
