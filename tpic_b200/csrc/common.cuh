@@ -201,6 +201,11 @@ __device__ __forceinline__ void shell_coordinates(const Geom& g, long long t, in
   k = int(r / g.ny);
 }
 
+// Requests the 128-byte line holding p into L2 (no register, no wait).
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+  asm volatile("prefetch.global.L2 [%0];" :: "l"(p));
+}
+
 template <class T> __device__ __forceinline__ T warp_sum(T v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);

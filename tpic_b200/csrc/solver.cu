@@ -173,6 +173,19 @@ __global__ void __launch_bounds__(kTX * kTY * kTZ) maxwell_apply_kernel(Geom g, 
   for (int s = 1; s < 14; ++s) {
     const int ox = stencil_offset(s, 0), oy = stencil_offset(s, 1), oz = stencil_offset(s, 2);
     const long long d = ox + (long long)g.NX * (oy + (long long)g.NY * oz);
+    // The next stencil's forward and backward rows are requested into L2
+    // while this one is applied: the loads of a block then wait for L2, not
+    // for HBM (the kernel is bound by memory latency; prefetches hold no
+    // registers).
+    if (s + 1 < 14) {
+      const int sn = s + 1;
+      const long long dn = stencil_offset(sn, 0) + (long long)g.NX * (stencil_offset(sn, 1) + (long long)g.NY * stencil_offset(sn, 2));
+#pragma unroll
+      for (int e = 0; e < 9; ++e) {
+        prefetch_l2(mass + g.mass_index(at, sn * 9 + e));
+        prefetch_l2(mass + g.mass_index(at - dn, sn * 9 + e));
+      }
+    }
     C bx, by, bz;
     block_product<C>(mass + g.mass_index(at, s * 9), es, vv(0, ox, oy, oz), vv(1, ox, oy, oz), vv(2, ox, oy, oz),
                      bx, by, bz);
