@@ -634,6 +634,7 @@ struct __align__(16) StreamShared {
   float stage[kCells][kBatch][kMoments + 1];
   float scratch[kCells][96];  // a batch's B corners / the H rows of a flushed cell
   StreamMeta meta[kCells][kMetaSlots];
+  uint32_t rank[kCells][4][32];  // per warp, chunk j & 3: each lane's record index (cp.async)
   uint32_t more[2];     // byte w of word j & 1: warp w has a chunk after chunk j
   uint32_t arrived[2];  // arrivals of the chunks of each parity (monotonic)
   uint32_t decision;    // (chunk << 1) | (some warp has a chunk after it)
@@ -793,7 +794,7 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
     enter_batch(pf);
     pf = fetch_meta(cbid + W);
   }
-  auto walk = [&](StreamLane& L, StreamInfo& I) {
+  auto walk = [&](StreamLane& L, StreamInfo& I, uint32_t chunk) {
     L = StreamLane{0u, 0u, 0u};
     I = StreamInfo{0, 0u};
     if (cnext) {  // the previous chunk finished the batch
@@ -833,13 +834,28 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
       const uint32_t s1 = p >= m.split[slot] ? 1u : 0u;
       L.pos = p + m.off[slot][s1];
       const uint32_t* perm = s1 ? tp.sp[1].perm : tp.sp[0].perm;
-      L.idx = perm ? __ldg(perm + L.pos) : L.pos;
+      uint32_t* dst = &sh.rank[warp][chunk & 3u][lane];
+      if (perm)
+        tc::cp_async4(dst, perm + L.pos);
+      else
+        *dst = L.pos;
       L.flags = 1u | (s1 << 1) | (uint32_t(slot) << 2) | (((cbits >> (4 + slot)) & 1u) << 4);
     }
     if (last)
       cnext = true;
     else
       cbase = end;
+  };
+  // The record index of a walked chunk (its rank copy has completed) and an
+  // L2 prefetch of the record, one chunk before its loads are issued.
+  auto prefetch_rec = [&](StreamLane& L, uint32_t chunk) {
+    L.idx = sh.rank[warp][chunk & 3u][lane];
+    if (L.flags & 1u) {
+      const TcSpecies& sp = (L.flags & 2u) ? tp.sp[1] : tp.sp[0];
+      const uint32_t n = L.idx;
+      prefetch_l2(sp.rx + n); prefetch_l2(sp.ry + n); prefetch_l2(sp.rz + n); prefetch_l2(sp.q + n);
+      prefetch_l2(sp.u + n); prefetch_l2(sp.v + n); prefetch_l2(sp.w + n); prefetch_l2(sp.key + n);
+    }
   };
   auto load_rec = [&](const StreamLane& L) {
     StreamRec r{0.0, 0.0, 0.0, 0.0, 0.0f, 0.0f, 0.0f, -1, L.pos, L.flags};
@@ -924,12 +940,23 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
     }
   };
 
-  StreamLane l2;
-  StreamInfo i2;
-  walk(l2, i2);  // chunk 0
-  StreamRec r1 = load_rec(l2);
-  StreamInfo i1 = i2;
-  walk(l2, i2);  // chunk 1
+  // Per-warp pipeline: chunk j + 3 walked (ranks copying), j + 2
+  // prefetched into L2, j + 1 loaded into registers, j computed.
+  StreamLane la, lb, lc;
+  StreamInfo ia, ib, ic;
+  // One cp.async group per walked chunk (empty when no rank is copied).
+  walk(la, ia, 0u);
+  tc::cp_async_commit();
+  walk(lb, ib, 1u);
+  tc::cp_async_commit();
+  walk(lc, ic, 2u);
+  tc::cp_async_commit();
+  tc::cp_async_wait_group<2>();
+  prefetch_rec(la, 0u);
+  tc::cp_async_wait_group<1>();
+  prefetch_rec(lb, 1u);
+  StreamRec r1 = load_rec(la);
+  StreamInfo i1 = ia;
   StreamInfo ip{0, 0u};  // the previous chunk, whose cells are flushed next
   bool bad = false;
   uint32_t last_arrived = 0xFFFFFFFFu;  // the last chunk this warp arrived for
@@ -937,9 +964,18 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
   for (uint32_t j = 0;; ++j) {
     const StreamRec r0 = r1;
     const StreamInfo i0 = i1;
-    r1 = load_rec(l2);
-    i1 = i2;
-    walk(l2, i2);
+    r1 = load_rec(lb);
+    i1 = ib;
+    StreamLane ld;
+    StreamInfo id;
+    walk(ld, id, j + 3u);
+    tc::cp_async_commit();
+    tc::cp_async_wait_group<1>();
+    prefetch_rec(lc, j + 2u);
+    lb = lc;
+    ib = ic;
+    lc = ld;
+    ic = id;
     const bool have = (i0.bits >> 13) & 1u;
 
     // Particle phase: (s alpha, j) and the per-axis factors of one record.
@@ -1094,6 +1130,7 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
     ip = i0;
   }
 
+  tc::cp_async_wait_all();
   if (bad && lane == 0) atomicAdd(invalid, 1u << 20);
   // After a failed wait the MMAs of the last chunk may still be in flight:
   // wait for them (bounded) before the tensor memory is freed.

@@ -127,6 +127,10 @@ __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+// Waits until at most N of this thread's committed cp.async groups are pending.
+template <int N> __device__ __forceinline__ void cp_async_wait_group() {
+  asm volatile("cp.async.wait_group %0;" :: "n"(N) : "memory");
+}
 
 // Shared-memory matrix descriptor, no swizzle (canonical core matrices of
 // 8 rows x 16 bytes): start address, leading-dimension byte offset (LBO),
