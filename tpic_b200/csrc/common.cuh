@@ -206,6 +206,32 @@ __device__ __forceinline__ void prefetch_l2(const void* p) {
   asm volatile("prefetch.global.L2 [%0];" :: "l"(p));
 }
 
+// shell_coordinates in 32-bit arithmetic (t < shell_count < 2^31).
+__device__ __forceinline__ void shell_coordinates32(const Geom& g, uint32_t t, int& i, int& j, int& k) {
+  const uint32_t NX = uint32_t(g.NX), zs = NX * uint32_t(g.NY), ys = NX * uint32_t(g.nz),
+                 xs = uint32_t(g.ny) * uint32_t(g.nz);
+  if (t < 3 * zs) {
+    const uint32_t p = t / zs, r = t - p * zs;
+    k = p == 0 ? -1 : g.nz + int(p) - 1;
+    i = int(r % NX) - 1;
+    j = int(r / NX) - 1;
+    return;
+  }
+  t -= 3 * zs;
+  if (t < 3 * ys) {
+    const uint32_t p = t / ys, r = t - p * ys;
+    j = p == 0 ? -1 : g.ny + int(p) - 1;
+    i = int(r % NX) - 1;
+    k = int(r / NX);
+    return;
+  }
+  t -= 3 * ys;
+  const uint32_t p = t / xs, r = t - p * xs;
+  i = p == 0 ? -1 : g.nx + int(p) - 1;
+  j = int(r % uint32_t(g.ny));
+  k = int(r / uint32_t(g.ny));
+}
+
 template <class T> __device__ __forceinline__ T warp_sum(T v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);

@@ -356,6 +356,21 @@ __global__ void __launch_bounds__(256) fold_field_kernel(Geom g, T* __restrict__
   }
 }
 
+// Stencil-major layout: one thread per shell vertex copies its 126 entries
+// (each entry a coalesced row across the warp's vertices); the vertex is
+// decoded once (32-bit arithmetic: a shell holds far fewer than 2^31 vertices).
+template <class T>
+__global__ void __launch_bounds__(256) fold_mass_rows_kernel(Geom g, T* __restrict__ m) {
+  const uint32_t shell = uint32_t(shell_count(g));
+  for (uint32_t sv = blockIdx.x * blockDim.x + threadIdx.x; sv < shell; sv += gridDim.x * blockDim.x) {
+    int i, j, k;
+    shell_coordinates32(g, sv, i, j, k);
+    const long long to = g.node(i, j, k), from = g.node(wrap_index(i, g.nx), wrap_index(j, g.ny), wrap_index(k, g.nz));
+#pragma unroll 6
+    for (int e = 0; e < 126; ++e) m[g.mass_index(to, e)] = m[g.mass_index(from, e)];
+  }
+}
+
 template <class T>
 __global__ void __launch_bounds__(256) fold_mass_kernel(Geom g, T* __restrict__ m) {
   const long long total = shell_count(g) * 126;
@@ -440,9 +455,15 @@ cudaError_t launch_fold(int precision, const Geom& g, void* j, void* mass, cudaS
     count_launches(1);
   }
   if (mass) {
-    const unsigned blocks = grid_for(126 * shell_count(g), 256, 148u * 8u);
-    if (precision == TPICB200_PRECISION_DOUBLE) fold_mass_kernel<double><<<blocks, 256, 0, s>>>(g, (double*)mass);
-    else fold_mass_kernel<float><<<blocks, 256, 0, s>>>(g, (float*)mass);
+    if (g.mes != 1) {
+      const unsigned blocks = grid_for(shell_count(g), 256, 148u * 8u);
+      if (precision == TPICB200_PRECISION_DOUBLE) fold_mass_rows_kernel<double><<<blocks, 256, 0, s>>>(g, (double*)mass);
+      else fold_mass_rows_kernel<float><<<blocks, 256, 0, s>>>(g, (float*)mass);
+    } else {
+      const unsigned blocks = grid_for(126 * shell_count(g), 256, 148u * 8u);
+      if (precision == TPICB200_PRECISION_DOUBLE) fold_mass_kernel<double><<<blocks, 256, 0, s>>>(g, (double*)mass);
+      else fold_mass_kernel<float><<<blocks, 256, 0, s>>>(g, (float*)mass);
+    }
     count_launches(1);
   }
   return cudaGetLastError();

@@ -25,10 +25,13 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kDotTile = 4;
 
+// Interior coordinates of compact index t (32-bit arithmetic: solver_create
+// requires 3 (n+1)^3 < 2^31).
 __device__ __forceinline__ void compact_coordinates(const Geom& g, long long t, int& i, int& j, int& k) {
-  i = int(t % g.inx);
-  j = int((t / g.inx) % g.iny);
-  k = int(t / ((long long)g.inx * g.iny));
+  const uint32_t u = uint32_t(t), inx = uint32_t(g.inx), row = u / inx;
+  i = int(u - row * inx);
+  j = int(row % uint32_t(g.iny));
+  k = int(row / uint32_t(g.iny));
 }
 
 // curl_N2C at cell (i,j,k) of the double node field `v` in arithmetic C.
@@ -211,12 +214,11 @@ __global__ void __launch_bounds__(kTX * kTY * kTZ) maxwell_apply_kernel(Geom g, 
 template <class Out>
 __global__ void __launch_bounds__(kThreads) duplicate_rows_kernel(Geom g, Out* __restrict__ out) {
   // Compact rows with i == n, or j == n, or k == n: three slabs as in shell_coordinates.
-  const long long zs = (long long)g.inx * g.iny, ys = (long long)g.inx * g.nz, xs = (long long)g.ny * g.nz;
-  const long long total = zs + ys + xs;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 3 * total;
-       t += (long long)gridDim.x * blockDim.x) {
+  const uint32_t zs = uint32_t(g.inx) * g.iny, ys = uint32_t(g.inx) * g.nz, xs = uint32_t(g.ny) * g.nz;
+  const uint32_t total = zs + ys + xs;
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < 3 * total; t += gridDim.x * blockDim.x) {
     const int c = int(t / total);
-    long long r = t - c * total;
+    uint32_t r = t - c * total;
     int i, j, k;
     if (r < zs) { k = g.nz; i = int(r % g.inx); j = int(r / g.inx); }
     else if ((r -= zs) < ys) { j = g.ny; i = int(r % g.inx); k = int(r / g.inx); }
@@ -401,15 +403,17 @@ __global__ void __launch_bounds__(kThreads) normalize_kernel(Geom g, const Src* 
   if (blockIdx.x == 0 && threadIdx.x == 0) run_tail(tail, norm2[0]);
   const double n2 = norm2[0];
   const double scale = n2 > 0.0 ? 1.0 / sqrt(n2) : 0.0;
-  const long long count = 3 * g.interior;
-  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < count;
-       n += (long long)gridDim.x * blockDim.x) {
-    const S value = S(double(source[n]) * scale);
-    target[n] = value;
-    const long long c = n / g.interior, t = n - c * g.interior;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < g.interior;
+       t += (long long)gridDim.x * blockDim.x) {
     int i, j, k;
     compact_coordinates(g, t, i, j, k);
-    input[c * g.nodes + g.node(i, j, k)] = double(value);
+    const long long at = g.node(i, j, k);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const S value = S(double(source[c * g.interior + t]) * scale);
+      target[c * g.interior + t] = value;
+      input[c * g.nodes + at] = double(value);
+    }
   }
 }
 
@@ -474,6 +478,10 @@ struct SolverWorkspace {
 
 SolverWorkspace* solver_create(int precision, const Geom& g, int restart, double dt, double theta,
                                double c, cudaError_t* err) {
+  if (3 * g.interior >= (1LL << 31)) {  // the compact-index kernels use 32-bit arithmetic
+    *err = cudaErrorInvalidValue;
+    return nullptr;
+  }
   auto* w = new SolverWorkspace();
   w->precision = precision;
   w->g = g;
