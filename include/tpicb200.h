@@ -348,6 +348,88 @@ int tpicb200_materialize(tpicb200_context* ctx, tpicb200_state* state, tpicb200_
 int tpicb200_cycle(tpicb200_context* ctx, tpicb200_state* state, int ncycles,
                    tpicb200_cycle_report* reports, tpicb200_stream stream);
 
+/* ------------------------------------------------------------------------
+ * Input decks and analytic initial cases (host code, no device needed).
+ *
+ * TPIC reads a run from an input deck of `key = value` lines ('#' starts a
+ * comment, a list is whitespace-separated, the last assignment of a key
+ * wins; src/config/simulation_parameters.cpp:55-200) and prepares the case
+ * the deck's `Case` names (include/tpic/initialization/cases/initial_case.hpp:27-60).
+ * These entry points read the keys of the periodic, unsmoothed, one-rank
+ * path and the cases built here: Uniform, Weibel, TwoStream and the Harris
+ * sheet family (GEMHarris, GEM, GEMnoPert, DoubleGEM, DoubleGEMnoPert,
+ * plasmoidChain). Other case names, wall boundaries, smoothing and Ampere
+ * currents are rejected with TPICB200_INVALID_ARGUMENT.
+ * ------------------------------------------------------------------------ */
+#define TPICB200_CASE_NAME_MAX 32
+typedef struct {
+  double rho;          /* rhoINIT */
+  double qom;          /* qom */
+  double vth[3];       /* uth, vth, wth */
+  double drift[3];     /* u0, v0, w0 */
+  int npcel[3];        /* npcelx, npcely, npcelz */
+  int center_velocity; /* CenterInitialVelocity */
+} tpicb200_deck_species;
+
+typedef struct {
+  char case_name[TPICB200_CASE_NAME_MAX]; /* Case */
+  tpicb200_grid grid;                     /* Lx, Ly, Lz, nxc, nyc, nzc */
+  double dt, theta, c, gmres_tol;         /* dt, th, c, GMREStol */
+  int ncycles;                            /* ncycles */
+  int ns;                                 /* ns */
+  tpicb200_deck_species species[TPICB200_MAX_SPECIES];
+  double b0[3];                           /* B0x, B0y, B0z (uniform background) */
+  /* Harris sheet family (harris_sheet.hpp) */
+  double delta, harris_b0x;               /* delta, HarrisB0x */
+  double pert_gem, pert_hump;             /* pertGEM, pertHump */
+  double deltax_hump, deltay_hump;        /* deltaxHump, deltayHump */
+  double kx_hump, ky_hump;                /* kxHump, kyHump (negative: box modes) */
+  /* Weibel (weibel.hpp) */
+  int weibel_mode_x;                      /* WeibelSeedModeX */
+  double weibel_amplitude;                /* WeibelSeedAmplitude */
+  double weibel_growth_rate;              /* WeibelSeedGrowthRate */
+  /* TwoStream (two_stream.hpp) */
+  int two_stream_mode_x;                  /* TwoStreamSeedModeX */
+  double two_stream_amplitude;            /* TwoStreamSeedDensityAmplitude */
+  double two_stream_phase;                /* TwoStreamSeedPhase */
+  int quiet_start;                        /* QuietStart: subcell centres */
+  int ignored_keys;                       /* deck keys this front end does not read */
+} tpicb200_deck;
+
+/* Fills *out from the deck text with TPIC's defaults for absent keys
+ * (th = 1, c = 1, GMREStol = 1e-3, delta = 0.5, deltaxHump = 8,
+ * deltayHump = 4, kxHump = kyHump = -1). Replaces SimulationParameters'
+ * parse_simulation_parameters (src/config/simulation_parameters.cpp:208-396)
+ * for these keys; a malformed line, a missing required key (dt, ncycles,
+ * ns, Case, per-species lists), too short a list, an unknown case name or
+ * an out-of-scope option returns TPICB200_INVALID_ARGUMENT with the line
+ * and key in tpicb200_last_error(). */
+int tpicb200_deck_parse(const char* text, tpicb200_deck* out);
+
+/* The case's analytic initial fields at n physical points (x, y, z),
+ * double precision: e[3n] and b[3n] (component-major: e[c*n + p]); b
+ * includes the uniform background B0 once. Replaces initial_electric and
+ * initial_magnetic (src/initialization/initial_case.cpp:146-162) with the
+ * case coefficients of prepare_initial_case; returns
+ * TPICB200_INVALID_ARGUMENT when the case is not admitted and
+ * TPICB200_OVERFLOW for a nonfinite coordinate or sample. */
+int tpicb200_case_fields(const tpicb200_deck* deck, long long n, const double* x, const double* y,
+                         const double* z, double* e, double* b);
+
+/* The loading profile of species s at n particles: physical position
+ * (x, y, z) and cell row j (the y cell index of the particle's cell). Writes
+ * the density sample (rhoINIT/(4 pi), shaped by the case), the density
+ * multiplier and the drift (drift[3n], component-major); the macro-charge
+ * is then q = (sign(qom) (dx dy) dz / ppc * density) * multiplier and the
+ * velocity drift + thermal * normal. Replaces the case Profile::evaluate of
+ * initial_particle_load_kernel (initialization/particles/particle_loading_device.hpp:120-143,
+ * cases/case_interface.hpp:60-77): TwoStream's electron density seed, the
+ * Harris sheet density of drifting species (the mean of the cell's two
+ * y-node values of sech^2) and the double sheet's drift sign. */
+int tpicb200_case_profile(const tpicb200_deck* deck, int s, long long n, const double* x, const double* y,
+                          const double* z, const int* cell_j, double* density, double* multiplier,
+                          double* drift);
+
 #ifdef __cplusplus
 }
 #endif

@@ -120,7 +120,8 @@ class OracleCycle:
     mover)."""
 
     def __init__(self, grid, species, dt, theta=0.5, c=1.0, gmres_tol=1e-8, precision=0,
-                 restart=30, max_iterations=100, e0=(0.0, 0.0, 0.0), b0=(0.0, 0.0, 0.0)):
+                 restart=30, max_iterations=100, e0=(0.0, 0.0, 0.0), b0=(0.0, 0.0, 0.0), e_node=None,
+                 b_cell=None):
         self.lib = load()
         self.og = OGrid(grid.nx, grid.ny, grid.nz, grid.lx / grid.nx, grid.ly / grid.ny, grid.lz / grid.nz)
         self.grid = grid
@@ -139,6 +140,11 @@ class OracleCycle:
         for k in range(3):
             self.e[k * n:(k + 1) * n] = e0[k]
             self.b[k * cl:(k + 1) * cl] = b0[k]
+        # Sampled initial fields (node and cell layouts, halos included).
+        if e_node is not None:
+            self.e[:] = np.asarray(e_node, dtype=np.float64).reshape(-1)
+        if b_cell is not None:
+            self.b[:] = np.asarray(b_cell, dtype=np.float64).reshape(-1)
         # Fields are stored in the precision's storage type between stages.
         self.e = self.e.astype(self.fdt).astype(np.float64)
         self.b = self.b.astype(self.fdt).astype(np.float64)

@@ -67,6 +67,26 @@ class CycleReport(C.Structure):
                 ("stage_ms", C.c_float * 6)]
 
 
+CASE_NAME_MAX = 32
+
+
+class DeckSpecies(C.Structure):
+    _fields_ = [("rho", C.c_double), ("qom", C.c_double), ("vth", C.c_double * 3), ("drift", C.c_double * 3),
+                ("npcel", C.c_int * 3), ("center_velocity", C.c_int)]
+
+
+class Deck(C.Structure):
+    _fields_ = [("case_name", C.c_char * CASE_NAME_MAX), ("grid", Grid),
+                ("dt", C.c_double), ("theta", C.c_double), ("c", C.c_double), ("gmres_tol", C.c_double),
+                ("ncycles", C.c_int), ("ns", C.c_int), ("species", DeckSpecies * MAX_SPECIES),
+                ("b0", C.c_double * 3), ("delta", C.c_double), ("harris_b0x", C.c_double),
+                ("pert_gem", C.c_double), ("pert_hump", C.c_double), ("deltax_hump", C.c_double),
+                ("deltay_hump", C.c_double), ("kx_hump", C.c_double), ("ky_hump", C.c_double),
+                ("weibel_mode_x", C.c_int), ("weibel_amplitude", C.c_double), ("weibel_growth_rate", C.c_double),
+                ("two_stream_mode_x", C.c_int), ("two_stream_amplitude", C.c_double),
+                ("two_stream_phase", C.c_double), ("quiet_start", C.c_int), ("ignored_keys", C.c_int)]
+
+
 EXPORTS = {
     "tpicb200_version": (C.c_char_p, []),
     "tpicb200_last_error": (C.c_char_p, []),
@@ -99,6 +119,11 @@ EXPORTS = {
                                   C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_double), C.c_void_p]),
     "tpicb200_prepare": (C.c_int, [C.c_void_p, C.POINTER(State), C.c_void_p]),
     "tpicb200_materialize": (C.c_int, [C.c_void_p, C.POINTER(State), C.c_void_p]),
+    "tpicb200_deck_parse": (C.c_int, [C.c_char_p, C.POINTER(Deck)]),
+    "tpicb200_case_fields": (C.c_int, [C.POINTER(Deck), C.c_longlong, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.c_void_p, C.c_void_p]),
+    "tpicb200_case_profile": (C.c_int, [C.POINTER(Deck), C.c_int, C.c_longlong, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tpicb200_cycle": (C.c_int, [C.c_void_p, C.POINTER(State), C.c_int, C.POINTER(CycleReport), C.c_void_p]),
 }
 

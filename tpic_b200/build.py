@@ -23,7 +23,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
           "-Xptxas", "-warn-spills"]
 PER_FILE = {"mover.cu": ["-fmad=false"]}
-SOURCES = ["abi.cu", "mover.cu", "sort.cu", "deposit.cu", "fields.cu", "solver.cu", "mass_tc.cu"]
+SOURCES = ["abi.cu", "mover.cu", "sort.cu", "deposit.cu", "fields.cu", "solver.cu", "mass_tc.cu", "cases.cu"]
 
 
 def nvcc() -> str:

@@ -3,10 +3,14 @@
 
 #include "common.cuh"
 
+#include <string>
+
 namespace tpicb200 {
 
 // Host-side count of the kernels this library launched (tpicb200_launch_count).
 void count_launches(unsigned n);
+// Records the message tpicb200_last_error() returns on this thread; returns status.
+int report_error(int status, const std::string& message);
 
 // mover.cu
 struct BinnedScratch;

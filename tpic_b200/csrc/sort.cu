@@ -579,7 +579,11 @@ __global__ void __launch_bounds__(256) binned_counts_kernel(Geom g, const uint32
         for (int dy = -1; dy <= 1; ++dy)
 #pragma unroll
           for (int dx = -1; dx <= 1; ++dx) {
-            const int si = wrap_index(i - dx, nx), sj = wrap_index(j - dy, ny), sk = wrap_index(k - dz, nz);
+            // Neighbour offsets are -1..1: a conditional wrap (no modulo).
+            int si = i - dx, sj = j - dy, sk = k - dz;
+            si = si < 0 ? si + nx : (si >= nx ? si - nx : si);
+            sj = sj < 0 ? sj + ny : (sj >= ny ? sj - ny : sj);
+            sk = sk < 0 ? sk + nz : (sk >= nz ? sk - nz : sk);
             const int d = (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1);
             sum += transfer[d * cells + si + (long long)nx * (sj + (long long)ny * sk)];
           }

@@ -52,11 +52,21 @@ def _uniform(r, xp=np):
 
 @dataclass
 class SpeciesSpec:
+    """One species' loading: q/m, rhoINIT, particles per cell per axis,
+    thermal speeds and drift. quiet: particles at their subcell centres
+    (TPIC's QuietStart). center: the charge-weighted mean of the sampled
+    velocities is removed around the loaded drift (CenterInitialVelocity).
+    profile: a case's loading profile, profile(x, y, z, cell_j) ->
+    (density, multiplier, drift[3, n]) at the particles' physical positions
+    (None: uniform, density rho/(4 pi))."""
     qom: float
     rho: float = 1.0
     npcel: tuple = (2, 2, 2)
     vth: tuple = (0.0, 0.0, 0.0)
     drift: tuple = (0.0, 0.0, 0.0)
+    quiet: bool = False
+    center: bool = False
+    profile: object = None
 
     @property
     def ppc(self) -> int:
@@ -119,8 +129,10 @@ def generate_species(grid: GridSpec, sp: SpeciesSpec, species_index: int, seed: 
     out = {}
     cells = [ci, cj, ck]
     fr = []
+    if (sp.profile is not None or sp.center) and xp is not np:
+        raise ValueError("case loading profiles and velocity centring load on the host (numpy)")
     for axis, (s, r, npc) in enumerate(zip((sub_x, sub_y, sub_z), a[:3], (npx, npy, npz))):
-        off = _uniform(r, xp)
+        off = xp.full_like(_uniform(r, xp), 0.5) if sp.quiet else _uniform(r, xp)
         sf = s.astype(np.float64) if xp is np else s.to(xp.float64)
         f = (sf + off) * (1.0 / npc)
         carry = f >= 1.0
@@ -135,18 +147,35 @@ def generate_species(grid: GridSpec, sp: SpeciesSpec, species_index: int, seed: 
     r34 = xp.sqrt(-2.0 * xp.log(u3))
     normals = (r12 * xp.cos(2.0 * math.pi * u2), r12 * xp.sin(2.0 * math.pi * u2),
                r34 * xp.cos(2.0 * math.pi * u4))
-    vel = []
-    for axis in range(3):
-        value = sp.drift[axis] + sp.vth[axis] * normals[axis]
-        vel.append(value.astype(velocity_dtype) if xp is np else value.to(velocity_dtype))
     dx, dy, dz = grid.spacing
     volume = (dx * dy) * dz
-    q = (1.0 if sp.qom > 0 else -1.0) * volume / ppc * (sp.rho / (4 * math.pi))
+    q_factor = (1.0 if sp.qom > 0 else -1.0) * volume / ppc
+    drift = [np.full(count, sp.drift[axis]) for axis in range(3)] if xp is np else sp.drift
+    if sp.profile is not None:
+        # The case profile at the stored position and cell (after the
+        # endpoint carry), as TPIC's loader evaluates it
+        # (particle_loading_device.hpp:120-143): q = (q_factor*density)*multiplier.
+        x = (cells[0] + fr[0]) * dx
+        y = (cells[1] + fr[1]) * dy
+        z = (cells[2] + fr[2]) * dz
+        density, multiplier, drift3 = sp.profile(x, y, z, cells[1].astype(np.int32))
+        q = (q_factor * density) * multiplier
+        drift = [drift3[axis] for axis in range(3)]
+    else:
+        q = q_factor * (sp.rho / (4 * math.pi))
+    vel = []
+    for axis in range(3):
+        value = drift[axis] + sp.vth[axis] * normals[axis]
+        vel.append(value.astype(velocity_dtype) if xp is np else value.to(velocity_dtype))
+    if sp.center:
+        if first != 0 or count != total:
+            raise ValueError("velocity centring needs the whole species")
+        vel = center_velocities(vel, drift, np.broadcast_to(q, (count,)), velocity_dtype)
     key = grid.encode(cells[0], cells[1], cells[2])
     if xp is np:
         out.update(rx=fr[0], ry=fr[1], rz=fr[2], u=vel[0], v=vel[1], w=vel[2],
-                   q=np.full(count, q, dtype=np.float64), cell=key.astype(np.int32),
-                   id=n.astype(np.uint64))
+                   q=np.broadcast_to(np.asarray(q, dtype=np.float64), (count,)).copy(),
+                   cell=key.astype(np.int32), id=n.astype(np.uint64))
     else:
         out.update(rx=fr[0], ry=fr[1], rz=fr[2], u=vel[0], v=vel[1], w=vel[2],
                    q=xp.full((count,), q, dtype=xp.float64, device=device), cell=key.to(xp.int32),
@@ -154,10 +183,26 @@ def generate_species(grid: GridSpec, sp: SpeciesSpec, species_index: int, seed: 
     return out
 
 
+def center_velocities(vel, drift, q, velocity_dtype):
+    """TPIC's velocity centring (initialization/particles/particle_centering_device.hpp:36-100):
+    the loaded drift is removed (stored in the velocity type), the
+    charge-weighted mean of what remains is subtracted and the drift put back
+    (each stored velocity formed in double and narrowed once)."""
+    rest = [(vel[a].astype(np.float64) - 0.0 + -1.0 * drift[a]).astype(velocity_dtype) for a in range(3)]
+    qsum = float(np.sum(q))
+    mean = [float(np.sum(q * rest[a].astype(np.float64))) / qsum if qsum != 0.0 else 0.0 for a in range(3)]
+    return [((rest[a].astype(np.float64) - mean[a]) + 1.0 * drift[a]).astype(velocity_dtype) for a in range(3)]
+
+
 @dataclass
 class FieldInit:
+    """Initial fields: uniform E and B, or full node (E) and cell (B) arrays
+    in the layouts of include/tpicb200.h, halos included (e_node: 3 x
+    (nx+3)(ny+3)(nz+3), b_cell: 3 x (nx+2)(ny+2)(nz+2), component-major)."""
     e0: tuple = (0.0, 0.0, 0.0)
     b0: tuple = (0.0, 0.0, 0.0)
+    e_node: object = None
+    b_cell: object = None
 
 
 @dataclass

@@ -77,6 +77,10 @@ class Simulation:
         for k in range(3):
             self.e[k * nodes:(k + 1) * nodes] = case.fields.e0[k]
             self.b_cell[k * cells:(k + 1) * cells] = case.fields.b0[k]
+        if case.fields.e_node is not None:
+            self.e.copy_(torch.as_tensor(np.asarray(case.fields.e_node, dtype=np.float64).reshape(-1)))
+        if case.fields.b_cell is not None:
+            self.b_cell.copy_(torch.as_tensor(np.asarray(case.fields.b_cell, dtype=np.float64).reshape(-1)))
         self.stream = torch.cuda.current_stream(dev)
         self.slots = []
         self.bins = []
@@ -94,7 +98,7 @@ class Simulation:
                 if keep_ids:
                     slot[-1]["id"] = torch.empty(n, dtype=torch.int64, device=dev)
             vdt_np = np.float64 if self.precision == _lib.PRECISION_DOUBLE else np.float32
-            if generate_on_device:
+            if generate_on_device and sp.profile is None and not sp.center:
                 data = generate_species(g, sp, s, seed=case.seed, velocity_dtype=self.vdt, xp=torch,
                                         device=dev)
             else:
