@@ -430,6 +430,42 @@ int tpicb200_case_profile(const tpicb200_deck* deck, int s, long long n, const d
                           const double* z, const int* cell_j, double* density, double* multiplier,
                           double* drift);
 
+/* ------------------------------------------------------------------------
+ * Device particle loading.
+ * ------------------------------------------------------------------------ */
+
+/* Loads records [first, first + p->count) of species s of the deck into p,
+ * in load order, on the stream: TPIC's dense load (initial_particle_load_kernel,
+ * initialization/particles/particle_loading_device.hpp:75-160) with this
+ * library's random stream in place of cuRAND XORWOW. Record n of species s:
+ *   two Philox-4x32-10 blocks (Salmon et al., SC'11) with counter
+ *   (n mod 2^32, n / 2^32, s, 0 | 1) and key (seed mod 2^32, seed / 2^32);
+ *   uniforms (r + 1/2) 2^-32: block 0 words 0-2 are the subcell offsets
+ *   (1/2 with QuietStart), word 3 with block 1 words 0-2 give three normals
+ *   by Box-Muller, (sqrt(-2 ln u1) cos(2 pi u2), sqrt(-2 ln u1) sin(2 pi u2),
+ *   sqrt(-2 ln u3) cos(2 pi u4));
+ *   cell = n / ppc and subcell = n mod ppc (x fastest), fraction
+ *   (subcell + offset) / npcel per axis, a fraction of exactly one carrying
+ *   into the next (periodic) cell;
+ *   the case profile at the stored position and cell gives the density,
+ *   multiplier and drift (tpicb200_case_profile); velocity drift + thermal *
+ *   normal stored in the context's velocity type, charge (q_factor *
+ *   density) * multiplier, id n.
+ * The deck's grid must be the context's. A nonfinite velocity or charge
+ * counts in *invalid (NULL: the context's counter). */
+int tpicb200_load_species(tpicb200_context* ctx, const tpicb200_deck* deck, int s, uint64_t seed,
+                          uint64_t first, tpicb200_particles* p, uint32_t* invalid, tpicb200_stream stream);
+
+/* CenterInitialVelocity of species s, p holding the whole species as loaded
+ * (before any sort or move): the loaded drift is removed from every
+ * velocity, the charge-weighted mean of the rest (FP64 sums in a fixed
+ * order) is subtracted and the drift put back, each stored velocity formed
+ * in double and narrowed once (initialization/particles/particle_centering_device.hpp:36-100).
+ * A zero charge sum leaves the rest unshifted; a nonfinite sum, mean or
+ * velocity counts in *invalid. Stream-ordered. */
+int tpicb200_center_velocities(tpicb200_context* ctx, const tpicb200_deck* deck, int s, tpicb200_particles* p,
+                               uint32_t* invalid, tpicb200_stream stream);
+
 #ifdef __cplusplus
 }
 #endif

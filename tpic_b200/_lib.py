@@ -125,6 +125,10 @@ EXPORTS = {
     "tpicb200_case_profile": (C.c_int, [C.POINTER(Deck), C.c_int, C.c_longlong, C.c_void_p, C.c_void_p, C.c_void_p,
                                         C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tpicb200_cycle": (C.c_int, [C.c_void_p, C.POINTER(State), C.c_int, C.POINTER(CycleReport), C.c_void_p]),
+    "tpicb200_load_species": (C.c_int, [C.c_void_p, C.POINTER(Deck), C.c_int, C.c_uint64, C.c_uint64,
+                                        C.POINTER(Particles), C.c_void_p, C.c_void_p]),
+    "tpicb200_center_velocities": (C.c_int, [C.c_void_p, C.POINTER(Deck), C.c_int, C.POINTER(Particles), C.c_void_p,
+                                             C.c_void_p]),
 }
 
 _lib = None

@@ -1,9 +1,9 @@
 """Builds the sm_100a shared library tpic_b200/libtpicb200.so with nvcc.
 
 Every kernel file is compiled for `-gencode arch=compute_100a,code=sm_100a`
-with line info; the mover is compiled with `-fmad=false` so that its
-arithmetic rounds every multiply and add on its own, like the reference's
-expressions under strict IEEE evaluation. The library is built in-tree so
+with line info; the mover and the particle loader are compiled with
+`-fmad=false` so that their arithmetic rounds every multiply and add on its
+own, like the reference's expressions under strict IEEE evaluation. The library is built in-tree so
 that it travels with the repository snapshot.
 """
 from __future__ import annotations
@@ -22,8 +22,9 @@ LIBRARY = HERE / "libtpicb200.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
           "-Xptxas", "-warn-spills"]
-PER_FILE = {"mover.cu": ["-fmad=false"]}
-SOURCES = ["abi.cu", "mover.cu", "sort.cu", "deposit.cu", "fields.cu", "solver.cu", "mass_tc.cu", "cases.cu"]
+PER_FILE = {"mover.cu": ["-fmad=false"], "load.cu": ["-fmad=false"]}
+SOURCES = ["abi.cu", "mover.cu", "sort.cu", "deposit.cu", "fields.cu", "solver.cu", "mass_tc.cu", "cases.cu",
+           "load.cu"]
 
 
 def nvcc() -> str:

@@ -28,6 +28,7 @@ struct tpicb200_context {
   double* mover_partials = nullptr;  // species scalars of the cycle's movers (5 rows per species)
   int mover_written[TPICB200_MAX_SPECIES]{};
   double* reduced = nullptr;     // energy reduction results
+  double* center = nullptr;      // velocity-centring partials (4 rows of energy_blocks) and 4 sums
   double* pinned = nullptr;      // host mirror of `reduced` + invalid
   int energy_blocks = 0;
   cudaEvent_t events[6 + 3 * TPICB200_MAX_SPECIES]{};
@@ -158,6 +159,7 @@ int tpicb200_create(const tpicb200_grid* grid, const tpicb200_options* options, 
   alloc((void**)&ctx->partials, size_t(ctx->energy_blocks) * (2 + 5 * TPICB200_MAX_SPECIES) * 8);
   alloc((void**)&ctx->mover_partials, size_t(kMoverPartials) * 5 * TPICB200_MAX_SPECIES * 8);
   alloc((void**)&ctx->reduced, (2 + 5 * TPICB200_MAX_SPECIES + 2) * 8);
+  alloc((void**)&ctx->center, (size_t(4) * ctx->energy_blocks + 4) * 8);
   if (options->precision == TPICB200_PRECISION_MIXED) alloc((void**)&ctx->moments, moment_floats(ctx->g) * 4);
   if (e == cudaSuccess) e = cudaMallocHost((void**)&ctx->pinned, (2 + 5 * TPICB200_MAX_SPECIES + 2) * 8);
   if (e == cudaSuccess) e = cudaMemset(ctx->invalid, 0, 4);
@@ -178,6 +180,7 @@ int tpicb200_destroy(tpicb200_context* ctx) {
   cudaFree(ctx->cursor); cudaFree(ctx->perm); cudaFree(ctx->perm2); cudaFree(ctx->scan); cudaFree(ctx->binned); cudaFree(ctx->codes);
   cudaFree(ctx->invalid);
   cudaFree(ctx->partials); cudaFree(ctx->mover_partials); cudaFree(ctx->reduced); cudaFree(ctx->moments);
+  cudaFree(ctx->center);
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
   for (auto& ev : ctx->events)
     if (ev) cudaEventDestroy(ev);
@@ -376,6 +379,64 @@ int tpicb200_magnetic_to_nodes(tpicb200_context* ctx, void* b_cell, void* b_node
   cudaError_t err = launch_cell_ghosts(ctx->opt.precision, ctx->g, b_cell, (cudaStream_t)stream);
   if (err == cudaSuccess) err = launch_cell_to_node(ctx->opt.precision, ctx->g, b_cell, b_node, (cudaStream_t)stream);
   return cuda_status(err, "cell-to-node failed");
+}
+
+namespace {
+int check_deck_grid(const tpicb200_context* ctx, const tpicb200_deck* deck, int s) {
+  if (!deck || s < 0 || s >= deck->ns || s >= TPICB200_MAX_SPECIES)
+    return fail(TPICB200_INVALID_ARGUMENT, "invalid deck or species index");
+  const Geom dg = make_geom(deck->grid);
+  if (dg.nx != ctx->g.nx || dg.ny != ctx->g.ny || dg.nz != ctx->g.nz || dg.dx != ctx->g.dx || dg.dy != ctx->g.dy ||
+      dg.dz != ctx->g.dz)
+    return fail(TPICB200_INVALID_ARGUMENT, "the deck's grid is not the context's");
+  return TPICB200_SUCCESS;
+}
+}  // namespace
+
+int tpicb200_load_species(tpicb200_context* ctx, const tpicb200_deck* deck, int s, uint64_t seed, uint64_t first,
+                          tpicb200_particles* p, uint32_t* invalid, tpicb200_stream stream) {
+  if (int st = check_ctx(ctx)) return st;
+  if (int st = check_deck_grid(ctx, deck, s)) return st;
+  if (int st = check_particles(ctx, p)) return st;
+  const tpicb200_deck_species& sp = deck->species[s];
+  if (sp.npcel[0] < 1 || sp.npcel[1] < 1 || sp.npcel[2] < 1)
+    return fail(TPICB200_INVALID_ARGUMENT, "npcel must be positive");
+  const unsigned long long ppc = (unsigned long long)sp.npcel[0] * sp.npcel[1] * sp.npcel[2];
+  const unsigned long long total = ppc * (unsigned long long)ctx->g.nx * ctx->g.ny * ctx->g.nz;
+  if (ppc > 0xffffffffULL || first > total || p->count > total - first)
+    return fail(TPICB200_INVALID_ARGUMENT, "records beyond the species' cells x particles per cell");
+  CaseProfile prof{};
+  if (int st = case_profile_of(deck, s, &prof)) return st;
+  LoadPlan plan{};
+  plan.first = first;
+  plan.ppc = uint32_t(ppc);
+  for (int a = 0; a < 3; ++a) {
+    plan.npc[a] = sp.npcel[a];
+    plan.inverse_npc[a] = 1.0 / sp.npcel[a];
+    plan.vth[a] = sp.vth[a];
+  }
+  plan.q_factor = (sp.qom > 0 ? 1.0 : -1.0) * ctx->g.volume / double(ppc);
+  plan.key0 = uint32_t(seed);
+  plan.key1 = uint32_t(seed >> 32);
+  plan.species = uint32_t(s);
+  plan.quiet = deck->quiet_start ? 1 : 0;
+  return cuda_status(launch_load_species(ctx->opt.precision, ctx->g, plan, prof, p, invalid_or_own(ctx, invalid),
+                                         (cudaStream_t)stream),
+                     "particle loading launch failed");
+}
+
+int tpicb200_center_velocities(tpicb200_context* ctx, const tpicb200_deck* deck, int s, tpicb200_particles* p,
+                               uint32_t* invalid, tpicb200_stream stream) {
+  if (int st = check_ctx(ctx)) return st;
+  if (int st = check_deck_grid(ctx, deck, s)) return st;
+  if (int st = check_particles(ctx, p)) return st;
+  CaseProfile prof{};
+  if (int st = case_profile_of(deck, s, &prof)) return st;
+  const int blocks = ctx->energy_blocks;
+  return cuda_status(launch_center_velocities(ctx->opt.precision, ctx->g, prof, p, ctx->center, blocks,
+                                              ctx->center + 4 * blocks, invalid_or_own(ctx, invalid),
+                                              (cudaStream_t)stream),
+                     "velocity centring launch failed");
 }
 
 int tpicb200_energy(tpicb200_context* ctx, const void* e, const void* b_cell, const tpicb200_particles* species,

@@ -21,6 +21,7 @@
 //              two y nodes (cases/harris_sheet.hpp:68-106).
 // Every expression keeps the reference's operation order, so the fields are
 // bit-identical to TPIC's on the same host math library.
+#include "cases.cuh"
 #include "kernels.cuh"
 
 #include <cmath>
@@ -349,14 +350,38 @@ void case_electric(const tpicb200_deck& d, const Prepared& p, double x, double e
   }
 }
 
-double sech_squared(double v) {
-  const double ch = std::cosh(v);
-  return 1.0 / (ch * ch);
-}
-
 int deck_failure(const DeckError& e) { return report_error(TPICB200_INVALID_ARGUMENT, e.message); }
 
+CaseProfile profile_of(const tpicb200_deck& d, const Prepared& p, int s) {
+  const tpicb200_deck_species& sp = d.species[s];
+  CaseProfile c{};
+  c.density = sp.rho / kFourPi;
+  for (int a = 0; a < 3; ++a) c.drift[a] = sp.drift[a];
+  c.density_seed = p.density_seed[s] ? 1 : 0;
+  c.wavenumber = p.wavenumber;
+  c.amplitude = d.two_stream_amplitude;
+  c.phase = d.two_stream_phase;
+  c.harris_density = is_harris(p.name) && p.harris_density[s] ? 1 : 0;
+  c.is_double = p.is_double ? 1 : 0;
+  c.ly = d.grid.ly;
+  c.delta = d.delta;
+  c.dy = d.grid.ly / d.grid.ny;
+  return c;
+}
+
 }  // namespace
+
+int case_profile_of(const tpicb200_deck* deck, int s, CaseProfile* out) {
+  if (!deck || !out || s < 0 || s >= deck->ns || s >= TPICB200_MAX_SPECIES)
+    return report_error(TPICB200_INVALID_ARGUMENT, "invalid deck or species index");
+  try {
+    *out = profile_of(*deck, prepare(*deck), s);
+    return TPICB200_SUCCESS;
+  } catch (const DeckError& err) {
+    return deck_failure(err);
+  }
+}
+
 }  // namespace tpicb200
 
 using namespace tpicb200;
@@ -500,28 +525,11 @@ extern "C" int tpicb200_case_profile(const tpicb200_deck* deck, int s, long long
     return report_error(TPICB200_INVALID_ARGUMENT, "invalid case-profile arguments");
   try {
     const Prepared p = prepare(*deck);
-    const tpicb200_deck_species& sp = deck->species[s];
-    const double base = sp.rho / kFourPi;
-    const double ly = deck->grid.ly, delta = deck->delta, dy = deck->grid.ly / deck->grid.ny;
-    auto harris_shape = [&](double yy) {
-      if (p.is_double) return sech_squared((yy - 0.25 * ly) / delta) + sech_squared((yy - 0.75 * ly) / delta);
-      return sech_squared((yy - 0.5 * ly) / delta);
-    };
+    const CaseProfile c = profile_of(*deck, p, s);
     for (long long i = 0; i < n; ++i) {
-      double dens = base, mult = 1.0;
-      double v[3] = {sp.drift[0], sp.drift[1], sp.drift[2]};
-      if (p.density_seed[s]) mult = 1.0 + deck->two_stream_amplitude * std::cos(p.wavenumber * x[i] + deck->two_stream_phase);
-      if (is_harris(p.name)) {
-        if (p.harris_density[s]) {
-          const double lower_y = 0.0 + cell_j[i] * dy;
-          const double nodes = harris_shape(lower_y) + harris_shape(lower_y + dy);
-          dens = dens * 0.5 * nodes;
-        }
-        if (p.is_double) v[2] = v[2] * -std::tanh((y[i] - 0.5 * ly) / delta);
-      }
-      density[i] = dens;
-      multiplier[i] = mult;
-      for (int c = 0; c < 3; ++c) drift[c * n + i] = v[c];
+      double v[3];
+      c.evaluate(x[i], y[i], cell_j[i], density[i], multiplier[i], v);
+      for (int a = 0; a < 3; ++a) drift[a * n + i] = v[a];
     }
     return TPICB200_SUCCESS;
   } catch (const DeckError& err) {

@@ -1,6 +1,7 @@
 // Host-side launch entry points of the kernel files (internal to the library).
 #pragma once
 
+#include "cases.cuh"
 #include "common.cuh"
 
 #include <string>
@@ -152,5 +153,27 @@ int solver_solve(SolverWorkspace* w, const void* e, const void* bcell, const voi
                  int max_iterations, double tol, cudaStream_t s, cudaError_t* err);
 cudaError_t solver_mass_apply(SolverWorkspace* w, const void* mass, const double* in, double* out,
                               cudaStream_t s);
+
+// cases.cu: the loading profile of species s of an admitted deck.
+int case_profile_of(const tpicb200_deck* deck, int s, CaseProfile* out);
+
+// load.cu
+struct LoadPlan {
+  uint64_t first;          // load index of the first record
+  uint32_t ppc;            // particles per cell
+  int npc[3];              // npcel per axis
+  double inverse_npc[3];   // 1.0 / npcel
+  double q_factor;         // sign(qom) * volume / ppc
+  double vth[3];
+  uint32_t key0, key1;     // Philox key (seed)
+  uint32_t species;        // Philox counter word 2
+  int quiet;               // subcell centres
+};
+cudaError_t launch_load_species(int precision, const Geom& g, const LoadPlan& plan, const CaseProfile& prof,
+                                tpicb200_particles* p, uint32_t* invalid, cudaStream_t s);
+// partials: 4 rows of `blocks` doubles; sums: 4 doubles.
+cudaError_t launch_center_velocities(int precision, const Geom& g, const CaseProfile& prof, tpicb200_particles* p,
+                                     double* partials, int blocks, double* sums, uint32_t* invalid,
+                                     cudaStream_t s);
 
 }  // namespace tpicb200

@@ -111,4 +111,35 @@ def to_case(deck: _lib.Deck, seed: int = 0, ncycles: int | None = None) -> Case:
     """The run the deck describes, ready for Simulation (and the oracle)."""
     return Case(grid=grid_of(deck), species=species_of(deck), dt=deck.dt, theta=deck.theta, c=deck.c,
                 gmres_tol=deck.gmres_tol, ncycles=deck.ncycles if ncycles is None else ncycles,
-                fields=initial_fields(deck), seed=seed)
+                fields=initial_fields(deck), seed=seed, deck=deck)
+
+
+def deck_of(case: Case) -> _lib.Deck:
+    """The deck a case was made from, or, for a case of uniform species
+    built in code, the Uniform deck that loads the same records."""
+    if case.deck is not None:
+        return case.deck
+    if any(sp.profile is not None for sp in case.species):
+        raise ValueError("a species with a loading profile needs the deck it came from")
+    quiet = {bool(sp.quiet) for sp in case.species}
+    if len(quiet) > 1:
+        raise ValueError("QuietStart applies to every species of a deck")
+    if len(case.species) > _lib.MAX_SPECIES:
+        raise ValueError("too many species")
+    d = _lib.Deck()
+    d.case_name = b"Uniform"
+    g = case.grid
+    d.grid = _lib.Grid(g.nx, g.ny, g.nz, g.lx, g.ly, g.lz)
+    d.dt, d.theta, d.c, d.gmres_tol, d.ncycles = case.dt, case.theta, case.c, case.gmres_tol, case.ncycles
+    d.ns = len(case.species)
+    d.b0[:] = tuple(case.fields.b0)
+    d.delta, d.deltax_hump, d.deltay_hump, d.kx_hump, d.ky_hump = 0.5, 8.0, 4.0, -1.0, -1.0
+    d.quiet_start = int(quiet.pop()) if quiet else 0
+    for s, sp in enumerate(case.species):
+        ds = d.species[s]
+        ds.rho, ds.qom = sp.rho, sp.qom
+        ds.vth[:] = tuple(sp.vth)
+        ds.drift[:] = tuple(sp.drift)
+        ds.npcel[:] = tuple(sp.npcel)
+        ds.center_velocity = int(bool(sp.center))
+    return d

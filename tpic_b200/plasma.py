@@ -4,8 +4,9 @@ TPIC loads particles with cuRAND's XORWOW stream
 (initialization/particles/particle_loading_device.hpp:32-53); that generator
 is not reproduced. This module defines its own counter-based stream,
 Philox-4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy
-as 1, 2, 3", SC'11), so that the same host arrays feed the CUDA path, the CPU
-oracle and every test, bit for bit.
+as 1, 2, 3", SC'11). `generate_species` is its host (numpy) form, which
+feeds the CPU oracle and the tests; the library's loader
+(tpicb200_load_species) is the device form of the same stream.
 
 Per particle with global load index `n` of species `s`:
   block A = philox((n_lo, n_hi, s, 0), seed) -> subcell offsets x, y, z and u1
@@ -16,7 +17,8 @@ The load order follows TPIC's dense path (particle_loading_device.hpp:85-120):
 cell = n // ppc (x fastest), subcell = n % ppc (x fastest), fraction =
 (subcell + offset) / npcel on each axis, a stored fraction of exactly one
 carries into the next cell; velocity = drift + thermal * normal; macro-charge
-q = sign(qom) * V/ppc * rho/(4 pi) (src/initialization/prepared_initialization.cpp:36-70).
+q = sign(qom) * V/ppc * rho/(4 pi) (src/initialization/prepared_initialization.cpp:36-70),
+shaped by a case profile where the species has one.
 """
 from __future__ import annotations
 
@@ -46,8 +48,8 @@ def philox4x32(c0, c1, c2, c3, k0: int, k1: int, xp=np):
     return c0, c1, c2, c3
 
 
-def _uniform(r, xp=np):
-    return (r.astype(xp.float64) if xp is np else r.to(dtype=xp.float64)) * 2.0**-32 + 2.0**-33
+def _uniform(r):
+    return r.astype(np.float64) * 2.0**-32 + 2.0**-33
 
 
 @dataclass
@@ -95,32 +97,24 @@ class GridSpec:
 
 
 def generate_species(grid: GridSpec, sp: SpeciesSpec, species_index: int, seed: int = 0,
-                     velocity_dtype=np.float64, first: int = 0, count: int | None = None,
-                     xp=np, device=None) -> dict:
-    """Records [first, first+count) of one uniform species, in load order.
-
-    xp = numpy (host arrays) or torch (device arrays on `device`); both give
-    the same integer stream, and the same values up to the last bit of the
-    transcendental functions of Box-Muller.
+                     velocity_dtype=np.float64, first: int = 0, count: int | None = None) -> dict:
+    """Records [first, first+count) of one species, in load order, on the
+    host (numpy). The library's loader (tpicb200_load_species) produces the
+    same records on the device: positions, keys and ids bit for bit,
+    velocities and charges to the last bits of log/cos/sin/cosh.
     """
     ppc = sp.ppc
     total = grid.cells * ppc
     if count is None:
         count = total - first
     k0, k1 = seed & MASK, (seed >> 32) & MASK
-    if xp is np:
-        n = np.arange(first, first + count, dtype=np.int64)
-        zeros = np.zeros_like(n)
-        ones = np.ones_like(n)
-        sidx = np.full_like(n, species_index)
-    else:
-        n = xp.arange(first, first + count, dtype=xp.int64, device=device)
-        zeros = xp.zeros_like(n)
-        ones = xp.ones_like(n)
-        sidx = xp.full_like(n, species_index)
+    n = np.arange(first, first + count, dtype=np.int64)
+    zeros = np.zeros_like(n)
+    ones = np.ones_like(n)
+    sidx = np.full_like(n, species_index)
     lo, hi = n & MASK, (n >> 32) & MASK
-    a = philox4x32(lo, hi, sidx, zeros, k0, k1, xp)
-    b = philox4x32(lo, hi, sidx, ones, k0, k1, xp)
+    a = philox4x32(lo, hi, sidx, zeros, k0, k1)
+    b = philox4x32(lo, hi, sidx, ones, k0, k1)
     cell = n // ppc
     sub = n % ppc
     npx, npy, npz = sp.npcel
@@ -129,28 +123,25 @@ def generate_species(grid: GridSpec, sp: SpeciesSpec, species_index: int, seed: 
     out = {}
     cells = [ci, cj, ck]
     fr = []
-    if (sp.profile is not None or sp.center) and xp is not np:
-        raise ValueError("case loading profiles and velocity centring load on the host (numpy)")
     for axis, (s, r, npc) in enumerate(zip((sub_x, sub_y, sub_z), a[:3], (npx, npy, npz))):
-        off = xp.full_like(_uniform(r, xp), 0.5) if sp.quiet else _uniform(r, xp)
-        sf = s.astype(np.float64) if xp is np else s.to(xp.float64)
-        f = (sf + off) * (1.0 / npc)
+        off = np.full_like(_uniform(r), 0.5) if sp.quiet else _uniform(r)
+        f = (s.astype(np.float64) + off) * (1.0 / npc)
         carry = f >= 1.0
-        f = xp.where(carry, xp.zeros_like(f), f)
-        cells[axis] = cells[axis] + (carry.astype(np.int64) if xp is np else carry.to(xp.int64))
+        f = np.where(carry, np.zeros_like(f), f)
+        cells[axis] = cells[axis] + carry.astype(np.int64)
         fr.append(f)
     extents = (grid.nx, grid.ny, grid.nz)
     for axis in range(3):
         cells[axis] = cells[axis] % extents[axis]
-    u1, u2, u3, u4 = _uniform(a[3], xp), _uniform(b[0], xp), _uniform(b[1], xp), _uniform(b[2], xp)
-    r12 = xp.sqrt(-2.0 * xp.log(u1))
-    r34 = xp.sqrt(-2.0 * xp.log(u3))
-    normals = (r12 * xp.cos(2.0 * math.pi * u2), r12 * xp.sin(2.0 * math.pi * u2),
-               r34 * xp.cos(2.0 * math.pi * u4))
+    u1, u2, u3, u4 = _uniform(a[3]), _uniform(b[0]), _uniform(b[1]), _uniform(b[2])
+    r12 = np.sqrt(-2.0 * np.log(u1))
+    r34 = np.sqrt(-2.0 * np.log(u3))
+    normals = (r12 * np.cos(2.0 * math.pi * u2), r12 * np.sin(2.0 * math.pi * u2),
+               r34 * np.cos(2.0 * math.pi * u4))
     dx, dy, dz = grid.spacing
     volume = (dx * dy) * dz
     q_factor = (1.0 if sp.qom > 0 else -1.0) * volume / ppc
-    drift = [np.full(count, sp.drift[axis]) for axis in range(3)] if xp is np else sp.drift
+    drift = [np.full(count, sp.drift[axis]) for axis in range(3)]
     if sp.profile is not None:
         # The case profile at the stored position and cell (after the
         # endpoint carry), as TPIC's loader evaluates it
@@ -163,23 +154,15 @@ def generate_species(grid: GridSpec, sp: SpeciesSpec, species_index: int, seed: 
         drift = [drift3[axis] for axis in range(3)]
     else:
         q = q_factor * (sp.rho / (4 * math.pi))
-    vel = []
-    for axis in range(3):
-        value = drift[axis] + sp.vth[axis] * normals[axis]
-        vel.append(value.astype(velocity_dtype) if xp is np else value.to(velocity_dtype))
+    vel = [(drift[axis] + sp.vth[axis] * normals[axis]).astype(velocity_dtype) for axis in range(3)]
     if sp.center:
         if first != 0 or count != total:
             raise ValueError("velocity centring needs the whole species")
         vel = center_velocities(vel, drift, np.broadcast_to(q, (count,)), velocity_dtype)
     key = grid.encode(cells[0], cells[1], cells[2])
-    if xp is np:
-        out.update(rx=fr[0], ry=fr[1], rz=fr[2], u=vel[0], v=vel[1], w=vel[2],
-                   q=np.broadcast_to(np.asarray(q, dtype=np.float64), (count,)).copy(),
-                   cell=key.astype(np.int32), id=n.astype(np.uint64))
-    else:
-        out.update(rx=fr[0], ry=fr[1], rz=fr[2], u=vel[0], v=vel[1], w=vel[2],
-                   q=xp.full((count,), q, dtype=xp.float64, device=device), cell=key.to(xp.int32),
-                   id=n.clone())
+    out.update(rx=fr[0], ry=fr[1], rz=fr[2], u=vel[0], v=vel[1], w=vel[2],
+               q=np.broadcast_to(np.asarray(q, dtype=np.float64), (count,)).copy(),
+               cell=key.astype(np.int32), id=n.astype(np.uint64))
     return out
 
 
@@ -217,3 +200,4 @@ class Case:
     ncycles: int = 1
     fields: FieldInit = field(default_factory=FieldInit)
     seed: int = 0
+    deck: object = None   # the tpicb200_deck it came from (tpic_b200.deck), if any

@@ -20,6 +20,7 @@ import numpy as np
 import torch
 
 from . import _lib
+from .deck import deck_of
 from .plasma import Case, generate_species
 
 
@@ -97,17 +98,14 @@ class Simulation:
                               ("cell", torch.int32))})
                 if keep_ids:
                     slot[-1]["id"] = torch.empty(n, dtype=torch.int64, device=dev)
-            vdt_np = np.float64 if self.precision == _lib.PRECISION_DOUBLE else np.float32
-            if generate_on_device and sp.profile is None and not sp.center:
-                data = generate_species(g, sp, s, seed=case.seed, velocity_dtype=self.vdt, xp=torch,
-                                        device=dev)
+            if generate_on_device:
+                self._load_on_device(deck_of(case), s, sp, slot[0], n)
             else:
+                vdt_np = np.float64 if self.precision == _lib.PRECISION_DOUBLE else np.float32
                 data = generate_species(g, sp, s, seed=case.seed, velocity_dtype=vdt_np)
-            for k, t in slot[0].items():
-                src = data[k]
-                if isinstance(src, np.ndarray):
-                    src = torch.from_numpy(src.view(np.int64) if k == "id" else src)
-                t.copy_(src.view(torch.int64) if k == "id" and src.dtype != torch.int64 else src)
+                for k, t in slot[0].items():
+                    src = data[k]
+                    t.copy_(torch.from_numpy(src.view(np.int64) if k == "id" else src))
             self.slots.append(slot)
             cnt = torch.zeros(bins, dtype=torch.int32, device=dev)
             off = torch.zeros(bins + 1, dtype=torch.int32, device=dev)
@@ -131,6 +129,19 @@ class Simulation:
         self.state = st
         self.reports: list[Report] = []
         self.prepared = False
+
+    def _load_on_device(self, deck, s: int, sp, slot: dict, n: int) -> None:
+        """Species s loaded (and centred) by the library's device loader."""
+        p = self._particles(slot, n)
+        invalid = torch.zeros(1, dtype=torch.int32, device=self.device)
+        stream = self._stream()
+        _lib.check(self.lib.tpicb200_load_species(self.ctx, C.byref(deck), s, self.case.seed, 0, C.byref(p),
+                                                  invalid.data_ptr(), stream))
+        if sp.center:
+            _lib.check(self.lib.tpicb200_center_velocities(self.ctx, C.byref(deck), s, C.byref(p),
+                                                           invalid.data_ptr(), stream))
+        if int(invalid.item()) != 0:
+            raise _lib.TpicError(_lib.OVERFLOW, f"species {s}: nonfinite velocity or charge at loading")
 
     @staticmethod
     def _particles(slot: dict, n: int) -> _lib.Particles:
