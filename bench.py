@@ -20,6 +20,7 @@ cycles (default 100) from the same initial state for its relative energy
 drift. The line reports both and their ratio ("plain_fp32_form").
 
   python bench.py [--gpus N --steps K --warmup W] [--mass-matrix scalar|scalar-f64|tf32|bf16x3]
+  python bench.py --deck tpic_b200/decks/harris2d_256x128.inp ...   (a deck's workload)
   python bench.py --impl reference ...   (the CPU implementation of the path)
 
 N > 1 runs N independent replicas (the path is timed on one GPU; the
@@ -192,8 +193,21 @@ def run_gpu(args) -> None:
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
 
-    case = workload(args.scale, 4)
+    if args.deck:
+        from tpic_b200 import deck as D
+        parsed = D.load(args.deck)
+        case = D.to_case(parsed)
+    else:
+        case = workload(args.scale, 4)
     nparticles = sum(case.grid.cells * sp.ppc for sp in case.species)
+    g = case.grid
+    if args.deck:
+        ppcs = "/".join(str(sp.ppc) for sp in case.species)
+        workload_name = (f"deck {Path(args.deck).name}: {D.case_name(parsed)}, {g.nx}x{g.ny}x{g.nz} cells, "
+                         f"box {g.lx:g}x{g.ly:g}x{g.lz:g}, {len(case.species)} species x {ppcs} ppc")
+    else:
+        workload_name = (f"3-D uniform thermal plasma, {args.scale}^3 cells, box 20^3 d_i, "
+                         f"2 species x 64 ppc, mass ratio 64")
     stream = torch.cuda.current_stream()
 
     def barrier():
@@ -205,7 +219,8 @@ def run_gpu(args) -> None:
         """Warm-up, the timed cycles, then more cycles up to --drift-cycles for
         the energy drift (the simulation stays open for the caller)."""
         t_gen = time.perf_counter()
-        sim = Simulation(case, precision=args.precision, mass_kind=mass_kind, device=local, generate_on_device=True)
+        sim = Simulation(case, precision=args.precision, mass_kind=mass_kind, device=local, generate_on_device=True,
+                         gmres_max_iterations=args.gmres_max_iterations)
         gen_s = time.perf_counter() - t_gen
         sim.prepare()
         w0 = sim.energy()
@@ -246,7 +261,7 @@ def run_gpu(args) -> None:
     dominant = max(kernels, key=lambda k: kernels[k]["ms"])
     dk = kernels[dominant]
     achieved = dk["bytes"] / (dk["ms"] / 1e3) / 1e9
-    traffic = load_traffic(dominant, nparticles)
+    traffic = None if args.deck else load_traffic(dominant, nparticles)
     roofline = {"kernel": dominant, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "peak_source": peak_kind,
                 "traffic": traffic, "algorithmic_bytes": dk["bytes"],
@@ -267,21 +282,24 @@ def run_gpu(args) -> None:
         comparison = {"mass_matrix": args.compare, **plain,
                       "speedup": value / plain["value"]}
 
+    record_bytes = 24 + 3 * (4 if args.precision == "mixed" else 8) + 8 + 4
+    l2_note = ("inputs larger than L2" if nparticles * record_bytes > 126e6 else
+               "inputs smaller than L2 (not flushed: a cycle's records fit in L2)")
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": headline["ms_per_step"], "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32" if args.precision == "mixed" else "f64", "data": "synthetic",
-                "config": {"workload": f"3-D uniform thermal plasma, {args.scale}^3 cells, box 20^3 d_i, "
-                                       f"2 species x 64 ppc, mass ratio 64", "particles": nparticles,
+                "config": {"workload": workload_name, "particles": nparticles,
                            "precision": args.precision, "mass_matrix": args.mass_matrix, "dt": case.dt,
-                           "theta": case.theta, "gmres_tol": case.gmres_tol, "l2": "inputs larger than L2",
+                           "theta": case.theta, "gmres_tol": case.gmres_tol,
+                           "gmres_max_iterations": args.gmres_max_iterations, "l2": l2_note,
                            "parallelism": f"replicas x{world}"},
                 "energy_drift": headline["energy_drift"], "gmres_iterations": headline["gmres_iterations"],
                 "stages_ms": headline["stages_ms"], "plain_fp32_form": comparison,
                 "clocks": clocks.summary(), "e2e": e2e, "gpu_launches": headline["launches"],
                 "roofline": roofline, "generation_s": headline["generation_s"]}
-        if not args.no_cpu_baseline:
+        if not args.no_cpu_baseline and not args.deck:
             cb = cpu_oracle_rate(args.cpu_scale, 4, 2, 0)
             line["cpu_baseline"] = {"value": cb["particles"] * cb["cycles"] / cb["seconds"], "unit": UNIT,
                                     "cores": 1, "kind": "port",
@@ -461,6 +479,10 @@ def main():
     ap.add_argument("--drift-cycles", type=int, default=100, help="cycles of the energy-drift run of each form")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "double"])
     ap.add_argument("--scale", type=int, default=128, help="cells per axis of the workload")
+    ap.add_argument("--gmres-max-iterations", type=int, default=100,
+                    help="GMRES step limit per solve (TPIC fixes 100, config/physics.hpp:20)")
+    ap.add_argument("--deck", default=None,
+                    help="a TPIC input deck (e.g. tpic_b200/decks/*.inp) as the workload instead of the default")
     ap.add_argument("--cpu-scale", type=int, default=24, help="cells per axis of the CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-workers", type=int, default=0, help="host processes of the reference arm (0: all cores)")

@@ -96,6 +96,8 @@ Geom make_geom(const tpicb200_grid& grid) {
   g.inv_volume = 1.0 / g.volume;
   g.mvs = 126;
   g.mes = 1;
+  g.run_len = kRunCells;
+  while (g.run_len > 1 && (long long)((g.nx + g.run_len - 1) / g.run_len) * g.ny * g.nz < kRunTarget) g.run_len >>= 1;
   return g;
 }
 }  // namespace tpicb200

@@ -28,6 +28,10 @@ struct Geom {
   // Mass storage: entry k = 9*stencil + component of vertex v lives at
   // v*mvs + k*mes: (126, 1) for TPIC's records, (1, nodes) stencil-major.
   long long mvs, mes;
+  // Cells per run of the run mover and the binned sort (a power of two,
+  // 1..kRunCells): a warp walks one run's records, so small grids use
+  // shorter runs to keep enough warps in flight.
+  int run_len;
 
   __host__ __device__ __forceinline__ long long mass_index(long long vertex, int k) const {
     return vertex * mvs + (long long)k * mes;
@@ -132,8 +136,9 @@ __device__ __forceinline__ int wrap_index(int i, int n) {
   return r < 0 ? r + n : r;
 }
 
-// Step d = to - from along a periodic axis of n >= 3 cells, folded to
-// -1 / +1 across the periodic face (other values are returned unchanged).
+// Step d = to - from along a periodic axis of n cells, folded to -1 / +1
+// across the periodic face (other values are returned unchanged). With n = 2
+// the move 0 -> 1 is -1 and 1 -> 0 is +1; with n = 1 every step is 0.
 __host__ __device__ __forceinline__ int periodic_step(int d, int n) {
   if (d == n - 1) return -1;
   if (d == 1 - n) return 1;
@@ -141,7 +146,7 @@ __host__ __device__ __forceinline__ int periodic_step(int d, int n) {
 }
 
 // Direction code (dx+1) + 3(dy+1) + 9(dz+1) < 27 of a move from cell
-// (i, j, k) to cell (a, b, c) of a periodic grid with every extent >= 3, or
+// (i, j, k) to cell (a, b, c) of a periodic grid, or
 // -1 when the destination is not one of the 27 cells around the source.
 __device__ __forceinline__ int move_code(const Geom& g, int i, int j, int k, int a, int b, int c) {
   const int dx = periodic_step(a - i, g.nx), dy = periodic_step(b - j, g.ny), dz = periodic_step(c - k, g.nz);
@@ -149,23 +154,25 @@ __device__ __forceinline__ int move_code(const Geom& g, int i, int j, int k, int
   return (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1);
 }
 
-// Runs of the binned sort and the run mover: up to 32 consecutive interior
-// cells of one x-row (segment, j, k). A record's run code packs its move
+// Runs of the binned sort and the run mover: up to g.run_len (at most
+// kRunCells = 32) consecutive interior cells of one x-row (segment, j, k). A record's run code packs its move
 // direction d < 27 (bits 0-4) and its cell's offset in the run (bits 5-9);
 // kNoMove marks a record that did not move to a neighbour.
 constexpr int kRunCells = 32;
 constexpr uint16_t kNoMove = 0xffff;
+// Runs wanted before the run length shrinks below kRunCells.
+constexpr long long kRunTarget = 16384;
 __host__ __device__ __forceinline__ long long run_count(const Geom& g) {
-  return (long long)((g.nx + kRunCells - 1) / kRunCells) * g.ny * g.nz;
+  return (long long)((g.nx + g.run_len - 1) / g.run_len) * g.ny * g.nz;
 }
 __host__ __device__ __forceinline__ void run_cells(const Geom& g, long long run, int& i0, int& len, int& j, int& k) {
-  const int segments = (g.nx + kRunCells - 1) / kRunCells;
+  const int segments = (g.nx + g.run_len - 1) / g.run_len;
   const int seg = int(run % segments);
   const long long row = run / segments;
   j = int(row % g.ny);
   k = int(row / g.ny);
-  i0 = seg * kRunCells;
-  len = g.nx - i0 < kRunCells ? g.nx - i0 : kRunCells;
+  i0 = seg * g.run_len;
+  len = g.nx - i0 < g.run_len ? g.nx - i0 : g.run_len;
 }
 
 // The non-unique vertices of a node field: every vertex of the (n+3)^3 box

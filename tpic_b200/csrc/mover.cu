@@ -307,7 +307,7 @@ __global__ void __launch_bounds__(256, TPICB200_MOVER_MIN_BLOCKS) mover_kernel(G
   if (sc.partials) store_scalars<256>(sc, acc, scratch);
 }
 
-// Runs of up to kRunCells cells of one x-row; records grouped by the bins
+// Runs of up to g.run_len cells of one x-row; records grouped by the bins
 // (old_counts, old_offsets), which validate_bins has checked (the kernel
 // returns at once when they do not tile the records).
 constexpr int kRunWarps = 4;

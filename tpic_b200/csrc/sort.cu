@@ -400,7 +400,9 @@ cudaError_t enqueue_general(int precision, const Geom& g, const tpicb200_particl
 //   1. direction codes d < 27 of every record and transfer counts T[d][c]
 //      per old interior cell c: from the mover itself (it knows both cells)
 //      or from classify_kernel (old cell from the bins, new from the key);
-//      periodic wrap, nx, ny, nz >= 3 keep the 27 destinations distinct;
+//      periodic_step gives each (source, destination) pair one code on
+//      any extent (on an axis of two cells 0 -> 1 is -1 and 1 -> 0 is +1; on
+//      an axis of one cell every step is 0);
 //   2. validation: the old bins must tile the records in key order;
 //   3. counts (thread per bin): counts'[b] = sum_d T[d][b - d];
 //   4. scan of the counts;
@@ -420,8 +422,8 @@ cudaError_t enqueue_general(int precision, const Geom& g, const tpicb200_particl
 constexpr int kBinnedThreads = 256;
 constexpr int kBinnedWarps = kBinnedThreads / 32;
 
-// A warp takes a run (up to 32 consecutive old interior cells of one x-row,
-// run_cells) at a time. The run's records form one contiguous range; lane l
+// A warp takes a run (up to g.run_len <= 32 consecutive old interior cells
+// of one x-row, run_cells) at a time. The run's records form one contiguous range; lane l
 // holds cell l's record range. Writes the cells' first records to `start`
 // (empty cells share their successor's start; unused entries are ~0) and
 // returns the run's record range.
@@ -765,7 +767,11 @@ size_t binned_scratch_words(const Geom& g) {
   return 4 + size_t(2 * g.bins + 1) + size_t(27 * cells);
 }
 
-bool binned_sort_applies(const Geom& g) { return g.nx >= 3 && g.ny >= 3 && g.nz >= 3; }
+// Every periodic grid: on an axis of one or two cells each (source, destination)
+// pair still has exactly one direction code (periodic_step), so the sources
+// of a destination stay in increasing key order with no two nonempty
+// directions sharing a source.
+bool binned_sort_applies(const Geom& g) { return g.nx >= 1 && g.ny >= 1 && g.nz >= 1; }
 
 BinnedScratch binned_scratch(const Geom& g, uint32_t* words, uint16_t* codes) {
   BinnedScratch b;
