@@ -247,6 +247,7 @@ def run_gpu(args) -> None:
                   "stages_ms": {name: float(np.mean([r.stage_ms[k] for r in reports]))
                                 for k, name in enumerate(stage_names)},
                   "gmres_iterations": float(np.mean([r.gmres_iterations for r in reports])),
+                  "gmres_host_waits": float(np.mean([r.gmres_host_waits for r in reports])),
                   "launches": int(launches), "generation_s": gen_s}
         return sim, result, clocks
 
@@ -296,6 +297,7 @@ def run_gpu(args) -> None:
                            "gmres_max_iterations": args.gmres_max_iterations, "l2": l2_note,
                            "parallelism": f"replicas x{world}"},
                 "energy_drift": headline["energy_drift"], "gmres_iterations": headline["gmres_iterations"],
+                "gmres_host_waits": headline["gmres_host_waits"],
                 "stages_ms": headline["stages_ms"], "plain_fp32_form": comparison,
                 "clocks": clocks.summary(), "e2e": e2e, "gpu_launches": headline["launches"],
                 "roofline": roofline, "generation_s": headline["generation_s"]}

@@ -132,6 +132,7 @@ typedef struct {
 typedef struct {
   int converged, iterations;
   double initial_residual, residual, rhs_norm, relative_residual;
+  int host_waits;  /* times the solve waited for the device (once per restart cycle, plus one) */
 } tpicb200_gmres_result;
 
 /* Whole-cycle state: every pointer is a caller-owned device buffer.

@@ -48,7 +48,8 @@ class Layout(C.Structure):
 
 class GmresResult(C.Structure):
     _fields_ = [("converged", C.c_int), ("iterations", C.c_int), ("initial_residual", C.c_double),
-                ("residual", C.c_double), ("rhs_norm", C.c_double), ("relative_residual", C.c_double)]
+                ("residual", C.c_double), ("rhs_norm", C.c_double), ("relative_residual", C.c_double),
+                ("host_waits", C.c_int)]
 
 
 class State(C.Structure):

@@ -77,6 +77,8 @@ uint32_t* invalid_or_own(tpicb200_context* ctx, uint32_t* invalid) {
 namespace tpicb200 {
 static std::atomic<unsigned long long> g_launches{0};
 void count_launches(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+unsigned long long launches_so_far() { return g_launches.load(std::memory_order_relaxed); }
+void uncount_launches(unsigned long long n) { g_launches.fetch_sub(n, std::memory_order_relaxed); }
 int report_error(int status, const std::string& message) { return fail(status, message); }
 
 Geom make_geom(const tpicb200_grid& grid) {

@@ -10,6 +10,10 @@ namespace tpicb200 {
 
 // Host-side count of the kernels this library launched (tpicb200_launch_count).
 void count_launches(unsigned n);
+// The counter's value, and a correction for launches that were captured into
+// a graph rather than run (the graph's runs are counted when they happen).
+unsigned long long launches_so_far();
+void uncount_launches(unsigned long long n);
 // Records the message tpicb200_last_error() returns on this thread; returns status.
 int report_error(int status, const std::string& message);
 

@@ -1,9 +1,15 @@
 // Matrix-free field solve: the implicit Maxwell operator
 //   A(v) = v + delta^2 curl_C2N(curl_N2C v) + k (M v)/V
 // fused into one kernel per interior node, and restarted GMRES with FP64
-// reductions, device-side Givens rotations and two scalars read back per
-// Arnoldi step, restating Gmres::host_blocking_solve
-// (ecsim/gmres/gmres_device.hpp:353-454) and its kernels (:137-292).
+// reductions and device-side Givens rotations, restating
+// Gmres::host_blocking_solve (ecsim/gmres/gmres_device.hpp:353-454) and its
+// kernels (:137-292). TPIC reads two scalars back after every Arnoldi step
+// to decide whether to stop; here the decision is taken on the device (an
+// ArnoldiControl record the step kernels read and a one-thread kernel
+// updates), and the steps of a restart cycle run as one CUDA graph whose
+// WHILE node repeats the step until that kernel clears its condition, so the
+// host waits once per restart cycle. The stopping rule, and so the
+// iteration count, is TPIC's.
 //
 // The reference applies A in four launches with three intermediate fields
 // (N2C curl, C2N curl, M v, combination; ecsim/maxwell/maxwell_device.hpp:433-484).
@@ -16,6 +22,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstring>
 #include <limits>
 #include <vector>
 
@@ -24,6 +32,17 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kDotTile = 4;
+
+// Device-side state of one restart cycle's Arnoldi steps.
+struct ArnoldiControl {
+  int col;        // the step the step kernels take (0-based)
+  int completed;  // steps completed in this cycle
+  int columns;    // step limit of this cycle
+  int stop;       // 0 running; 1 stopped (tolerance, breakdown or limit); 2 nonfinite estimate
+  int breakdown;  // the last step's subdiagonal was zero
+  int pad;
+  double tolerance;
+};
 
 // Interior coordinates of compact index t (32-bit arithmetic: solver_create
 // requires 3 (n+1)^3 < 2^31).
@@ -285,8 +304,9 @@ __global__ void __launch_bounds__(kThreads) pack_storage_kernel(Geom g, const T*
 template <class S>
 __global__ void __launch_bounds__(kThreads) dot_batch_kernel(const S* __restrict__ basis, const S* __restrict__ image,
                                                              double* __restrict__ partials, long long count,
-                                                             int columns) {
+                                                             const ArnoldiControl* __restrict__ ctl) {
   __shared__ double scratch[kDotTile][kThreads / 32];
+  const int columns = ctl->col + 1;
   for (int first = blockIdx.y * kDotTile; first < columns; first += gridDim.y * kDotTile) {
     double sum[kDotTile] = {0, 0, 0, 0};
     for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < count;
@@ -335,10 +355,12 @@ __global__ void __launch_bounds__(kThreads) residual_kernel(const double* __rest
 // (gmres_orthogonalize_squared_norm_kernel, gmres_device.hpp:243-263).
 template <class S>
 __global__ void __launch_bounds__(kThreads) orthogonalize_kernel(const S* __restrict__ basis, const double* __restrict__ dots,
-                                                                 S* __restrict__ image, double* __restrict__ column,
-                                                                 double* __restrict__ partials, long long count,
-                                                                 int columns) {
+                                                                 S* __restrict__ image, double* __restrict__ hessenberg,
+                                                                 int leading, double* __restrict__ partials,
+                                                                 long long count, const ArnoldiControl* __restrict__ ctl) {
   __shared__ double scratch[kThreads / 32];
+  const int columns = ctl->col + 1;
+  double* column = hessenberg + (long long)ctl->col * leading;
   double norm2 = 0;
   for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < count;
        n += (long long)gridDim.x * blockDim.x) {
@@ -355,12 +377,13 @@ __global__ void __launch_bounds__(kThreads) orthogonalize_kernel(const S* __rest
 }
 
 struct ArnoldiTail {
-  double* column;
+  double* column;  // the Hessenberg matrix (column `step` at step * leading)
   double* cosine;
   double* sine;
   double* rhs;
   double* status;
-  int step;  // -1: restart tail (rhs[0] = norm)
+  int step;        // -1: restart tail (rhs[0] = norm)
+  int leading;
 };
 
 // Restart tail and Arnoldi least-squares update
@@ -372,7 +395,7 @@ __device__ void run_tail(const ArnoldiTail& t, double norm2) {
   }
   const int step = t.step;
   const double sub = sqrt(norm2);
-  double* column = t.column;
+  double* column = t.column + (long long)step * t.leading;
   column[step + 1] = sub;
   for (int row = 0; row < step; ++row) {
     const double upper = column[row], lower = column[row + 1];
@@ -396,10 +419,17 @@ __device__ void run_tail(const ArnoldiTail& t, double norm2) {
 
 // target = source / sqrt(norm2[0]) (zero for a zero norm), also stored into
 // the operator input field (gmres_normalize_kernel, gmres_device.hpp:224-237).
+// With `ctl`, the step's column: target is basis column ctl->col + 1 of
+// `target` (columns `stride` apart) and the tail runs step ctl->col.
 template <class Src, class S>
 __global__ void __launch_bounds__(kThreads) normalize_kernel(Geom g, const Src* __restrict__ source,
                                                              const double* __restrict__ norm2, S* __restrict__ target,
-                                                             double* __restrict__ input, ArnoldiTail tail) {
+                                                             long long stride, double* __restrict__ input,
+                                                             ArnoldiTail tail, const ArnoldiControl* __restrict__ ctl) {
+  if (ctl) {
+    tail.step = ctl->col;
+    target += (long long)(tail.step + 1) * stride;
+  }
   if (blockIdx.x == 0 && threadIdx.x == 0) run_tail(tail, norm2[0]);
   const double n2 = norm2[0];
   const double scale = n2 > 0.0 ? 1.0 / sqrt(n2) : 0.0;
@@ -419,7 +449,8 @@ __global__ void __launch_bounds__(kThreads) normalize_kernel(Geom g, const Src* 
 
 // gmres_back_substitute_kernel, gmres_device.hpp:267-277 (one thread).
 __global__ void back_substitute_kernel(const double* hessenberg, const double* rhs, double* coefficients,
-                                       int leading, int columns) {
+                                       int leading, const ArnoldiControl* ctl) {
+  const int columns = ctl->completed;
   for (int row = columns - 1; row >= 0; --row) {
     double sum = 0;
     for (int column = row + 1; column < columns; ++column)
@@ -434,13 +465,63 @@ template <class S>
 __global__ void __launch_bounds__(kThreads) update_solution_kernel(const S* __restrict__ basis,
                                                                    const double* __restrict__ coefficients,
                                                                    double* __restrict__ x, long long count,
-                                                                   int columns) {
+                                                                   const ArnoldiControl* __restrict__ ctl) {
+  const int columns = ctl->completed;
   for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < count;
        n += (long long)gridDim.x * blockDim.x) {
     double value = x[n];
     for (int c = 0; c < columns; ++c) value += coefficients[c] * double(basis[(long long)c * count + n]);
     x[n] = value;
   }
+}
+
+// Sums of the dot partials of the step's columns (rows [0, ctl->col]).
+__global__ void __launch_bounds__(256) reduce_columns_kernel(const double* __restrict__ partials, double* out,
+                                                             int row_stride, const ArnoldiControl* __restrict__ ctl) {
+  __shared__ double scratch[8];
+  const int row = blockIdx.x;
+  if (row > ctl->col) return;
+  double sum = 0;
+  for (int i = threadIdx.x; i < row_stride; i += blockDim.x) sum += partials[(long long)row * row_stride + i];
+  sum = block_sum<256>(sum, scratch);
+  if (threadIdx.x == 0) out[row] = sum;
+}
+
+// role 0: zero the counter and clear the condition; role 1 (the IF body):
+// count a run.
+__global__ void condition_probe_kernel(cudaGraphConditionalHandle handle, unsigned* counter, int role) {
+  if (role == 0) {
+    *counter = 0;
+    cudaGraphSetConditional(handle, 0u);
+  } else {
+    *counter += 1;
+  }
+}
+
+__global__ void arnoldi_begin_kernel(ArnoldiControl* ctl, int columns, double tolerance) {
+  ctl->col = 0;
+  ctl->completed = 0;
+  ctl->columns = columns;
+  ctl->stop = 0;
+  ctl->breakdown = 0;
+  ctl->tolerance = tolerance;
+}
+
+// After step ctl->col: TPIC's stopping rule on the least-squares residual
+// estimate status[0] and the breakdown flag status[1]
+// (gmres_device.hpp:420-436); in the graph, the WHILE condition stays set
+// while the cycle runs and is cleared at the latest after ctl->columns steps.
+__global__ void arnoldi_end_kernel(ArnoldiControl* ctl, const double* status, cudaGraphConditionalHandle handle,
+                                   int conditional) {
+  const int col = ctl->col;
+  const double estimate = status[0], breakdown = status[1];
+  const bool finite = isfinite(estimate) && isfinite(breakdown);
+  ctl->completed = col + 1;
+  ctl->breakdown = breakdown != 0.0;
+  const bool stop = !finite || estimate <= ctl->tolerance || breakdown != 0.0 || col + 1 >= ctl->columns;
+  ctl->stop = !finite ? 2 : (stop ? 1 : 0);
+  ctl->col = col + 1;
+  if (conditional) cudaGraphSetConditional(handle, stop ? 0u : 1u);
 }
 
 }  // namespace
@@ -464,8 +545,17 @@ struct SolverWorkspace {
   double* partials = nullptr;
   double* state = nullptr;
   double* pinned = nullptr;
+  ArnoldiControl* ctl = nullptr;
   int batch;
   size_t scalar_bytes;
+  // The Arnoldi-step loop as a graph (built for one mass pointer).
+  cudaStream_t capture = nullptr;
+  cudaGraph_t loop_graph = nullptr;
+  cudaGraphExec_t loop_exec = nullptr;
+  const void* loop_mass = nullptr;
+  unsigned loop_launches = 0;   // kernels of one step
+  bool loop_unavailable = false;
+  bool conditional_checked = false;
 
   double* hessenberg() { return state; }
   double* cosine() { return state + (size_t)restart * (restart + 1); }
@@ -513,7 +603,9 @@ SolverWorkspace* solver_create(int precision, const Geom& g, int restart, double
   alloc((void**)&w->values, w->batch * sizeof(double));
   alloc((void**)&w->partials, (size_t)w->batch * w->rblocks * sizeof(double));
   alloc((void**)&w->state, ((size_t)restart * (restart + 1) + 4 * restart + 3) * sizeof(double));
-  if (e == cudaSuccess) e = cudaMallocHost((void**)&w->pinned, 2 * sizeof(double));
+  alloc((void**)&w->ctl, sizeof(ArnoldiControl));
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&w->pinned, 2 * sizeof(double) + sizeof(ArnoldiControl));
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&w->capture, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaMemset(w->input, 0, 3 * g.nodes * sizeof(double));
   if (e == cudaSuccess) e = cudaMemset(w->rhs, 0, 3 * g.nodes * sizeof(double));
   *err = e;
@@ -528,7 +620,10 @@ void solver_destroy(SolverWorkspace* w) {
   if (!w) return;
   cudaFree(w->basis); cudaFree(w->image); cudaFree(w->x); cudaFree(w->b); cudaFree(w->r);
   cudaFree(w->ximage); cudaFree(w->input); cudaFree(w->rhs); cudaFree(w->values);
-  cudaFree(w->partials); cudaFree(w->state);
+  cudaFree(w->partials); cudaFree(w->state); cudaFree(w->ctl);
+  if (w->loop_exec) cudaGraphExecDestroy(w->loop_exec);
+  if (w->loop_graph) cudaGraphDestroy(w->loop_graph);
+  if (w->capture) cudaStreamDestroy(w->capture);
   if (w->pinned) cudaFreeHost(w->pinned);
   delete w;
 }
@@ -545,37 +640,193 @@ struct Solve {
   SolverWorkspace* w;
   cudaStream_t s;
   cudaError_t err = cudaSuccess;
+  int waits = 0;
 
   unsigned blocks() const { return grid_for(w->g.interior, kThreads); }
   void check() { if (err == cudaSuccess) err = cudaGetLastError(); }
 
-  template <class C, class Out> void apply(const Mass* mass, Out* out) {
+  template <class C, class Out> void apply(const Mass* mass, Out* out, cudaStream_t st) {
     const Geom& g = w->g;
-    launch_node_ghosts(g, w->input, 3, s);
+    launch_node_ghosts(g, w->input, 3, st);
     const double iv = g.inv_volume;
     const unsigned tiles = unsigned(((g.nx + kTX - 1) / kTX) * ((g.ny + kTY - 1) / kTY) * ((g.nz + kTZ - 1) / kTZ));
-    maxwell_apply_kernel<C, Mass, Out><<<tiles, kTX * kTY * kTZ, 0, s>>>(
+    maxwell_apply_kernel<C, Mass, Out><<<tiles, kTX * kTY * kTZ, 0, st>>>(
         g, C(w->delta * w->delta), C(w->kfac), C(iv), mass, w->input, out);
     const long long dup = (long long)g.inx * g.iny + (long long)g.inx * g.nz + (long long)g.ny * g.nz;
-    duplicate_rows_kernel<Out><<<grid_for(3 * dup, kThreads), kThreads, 0, s>>>(g, out);
+    duplicate_rows_kernel<Out><<<grid_for(3 * dup, kThreads), kThreads, 0, st>>>(g, out);
     count_launches(2);
     check();
   }
   void reduce(int filled) {
     launch_reduce_rows(w->partials, w->values, w->batch, w->rblocks, w->rblocks, filled, s);
   }
-  bool read_controls(const double* src, double out[2]) {
+  // Waits for the stream and copies two doubles at `src` (and, with
+  // `control`, the Arnoldi control record) to the host.
+  bool read_back(const double* src, double out[2], ArnoldiControl* control = nullptr) {
     if (err != cudaSuccess) return false;
-    err = cudaMemcpyAsync(w->pinned, src, 2 * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (src) err = cudaMemcpyAsync(w->pinned, src, 2 * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (control && err == cudaSuccess)
+      err = cudaMemcpyAsync(w->pinned + 2, w->ctl, sizeof(ArnoldiControl), cudaMemcpyDeviceToHost, s);
     if (err == cudaSuccess) err = cudaStreamSynchronize(s);
-    out[0] = w->pinned[0];
-    out[1] = w->pinned[1];
+    ++waits;
+    if (src) {
+      out[0] = w->pinned[0];
+      out[1] = w->pinned[1];
+    }
+    if (control) std::memcpy(control, w->pinned + 2, sizeof(ArnoldiControl));
     return err == cudaSuccess;
   }
   void apply_solution(const Mass* mass) {
     unpack_kernel<double><<<blocks(), kThreads, 0, s>>>(w->g, w->x, w->input);
     count_launches(1);
-    apply<double, double>(mass, w->ximage);
+    apply<double, double>(mass, w->ximage, s);
+  }
+
+  // One Arnoldi step (the step index and the stopping decision live in
+  // w->ctl): A v_col, classical Gram-Schmidt against columns 0..col, the
+  // normalized v_{col+1} with the Givens update of the least-squares
+  // problem, and the stopping rule.
+  void step(const Mass* mass, cudaStream_t st, cudaGraphConditionalHandle handle, int conditional) {
+    const Geom& g = w->g;
+    const long long N = w->count;
+    const int m = w->restart;
+    S* image = (S*)w->image;
+    S* basis = w->template basis_col<S>(0);
+    apply<S, S>(mass, image, st);
+    const dim3 grid(w->rblocks, (m + kDotTile - 1) / kDotTile);
+    dot_batch_kernel<S><<<grid, kThreads, 0, st>>>(basis, image, w->partials, N, w->ctl);
+    reduce_columns_kernel<<<m, 256, 0, st>>>(w->partials, w->values, int(w->rblocks), w->ctl);
+    orthogonalize_kernel<S><<<w->rblocks, kThreads, 0, st>>>(basis, w->values, image, w->hessenberg(), m + 1,
+                                                             w->partials, N, w->ctl);
+    launch_reduce_rows(w->partials, w->values, w->batch, w->rblocks, w->rblocks, 1, st);
+    normalize_kernel<S, S><<<w->rblocks, kThreads, 0, st>>>(
+        g, image, w->values, basis, N, w->input,
+        ArnoldiTail{w->hessenberg(), w->cosine(), w->sine(), w->ls_rhs(), w->status(), 0, m + 1}, w->ctl);
+    arnoldi_end_kernel<<<1, 1, 0, st>>>(w->ctl, w->status(), handle, conditional);
+    count_launches(5);
+    check();
+  }
+
+  // The restart cycle's steps as one graph: a WHILE node whose body is one
+  // step(); arnoldi_end_kernel clears the condition when the cycle stops,
+  // at the latest after ctl->columns <= restart steps. Before the first such
+  // graph, conditional_self_test() checks on this device that a kernel's
+  // cudaGraphSetConditional takes effect. Built once per mass pointer; false
+  // when conditional graphs are not available, and the host loop steps.
+  bool loop_ready(const Mass* mass) {
+    if (w->loop_unavailable || err != cudaSuccess) return false;
+    if (w->loop_exec && w->loop_mass == (const void*)mass) return true;
+    if (w->loop_exec) cudaGraphExecDestroy(w->loop_exec);
+    if (w->loop_graph) cudaGraphDestroy(w->loop_graph);
+    w->loop_exec = nullptr;
+    w->loop_graph = nullptr;
+    const char* stage = "self-test";
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    bool ok = conditional_self_test();
+    if (ok) {
+      stage = "graph";
+      ok = cudaGraphCreate(&graph, 0) == cudaSuccess;
+    }
+    cudaGraphConditionalHandle handle{};
+    if (ok) {
+      stage = "handle";
+      ok = cudaGraphConditionalHandleCreate(&handle, graph, 1u, cudaGraphCondAssignDefault) == cudaSuccess;
+    }
+    cudaGraphNodeParams params{};
+    params.type = cudaGraphNodeTypeConditional;
+    params.conditional.handle = handle;
+    params.conditional.type = cudaGraphCondTypeWhile;
+    params.conditional.size = 1;
+    cudaGraphNode_t node;
+    if (ok) {
+      stage = "conditional node";
+      ok = cudaGraphAddNode(&node, graph, nullptr, 0, &params) == cudaSuccess;
+    }
+    if (ok) {
+      stage = "capture";
+      const unsigned long long before = launches_so_far();
+      cudaGraph_t body = params.conditional.phGraph_out[0];
+      ok = cudaStreamBeginCaptureToGraph(w->capture, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) ==
+           cudaSuccess;
+      if (ok) {
+        const cudaError_t saved = err;
+        step(mass, w->capture, handle, 1);
+        cudaGraph_t captured = nullptr;
+        ok = cudaStreamEndCapture(w->capture, &captured) == cudaSuccess && err == cudaSuccess;
+        err = saved;
+      }
+      const unsigned long long captured_launches = launches_so_far() - before;
+      uncount_launches(captured_launches);
+      w->loop_launches = unsigned(captured_launches);
+    }
+    if (ok) {
+      stage = "instantiate";
+      ok = cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+    }
+    if (!ok) {
+      const cudaError_t why = cudaGetLastError();
+      if (exec) cudaGraphExecDestroy(exec);
+      if (graph) cudaGraphDestroy(graph);
+      std::fprintf(stderr,
+                   "tpicb200: the GMRES step graph is unavailable (%s: %s); the host steps the Arnoldi loop\n", stage,
+                   cudaGetErrorString(why));
+      w->loop_unavailable = true;
+      return false;
+    }
+    w->loop_graph = graph;
+    w->loop_exec = exec;
+    w->loop_mass = mass;
+    return true;
+  }
+
+  // A graph of one kernel that clears a conditional handle (default 1)
+  // followed by an IF node on it whose body counts its runs: true when the
+  // body did not run, i.e. the device-side condition took effect.
+  bool conditional_self_test() {
+    if (w->conditional_checked) return true;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaGraphConditionalHandle handle{};
+    bool ok = cudaGraphCreate(&graph, 0) == cudaSuccess &&
+              cudaGraphConditionalHandleCreate(&handle, graph, 1u, cudaGraphCondAssignDefault) == cudaSuccess;
+    unsigned* counter = reinterpret_cast<unsigned*>(w->ctl);  // free between solves
+    cudaGraphNode_t clear_node = nullptr, if_node = nullptr;
+    if (ok) {
+      ok = cudaStreamBeginCaptureToGraph(w->capture, graph, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) ==
+           cudaSuccess;
+      if (ok) {
+        condition_probe_kernel<<<1, 1, 0, w->capture>>>(handle, counter, 0);
+        cudaGraph_t captured = nullptr;
+        ok = cudaStreamEndCapture(w->capture, &captured) == cudaSuccess;
+      }
+    }
+    size_t count = 1;
+    ok = ok && cudaGraphGetNodes(graph, &clear_node, &count) == cudaSuccess && count == 1;
+    cudaGraphNodeParams params{};
+    params.type = cudaGraphNodeTypeConditional;
+    params.conditional.handle = handle;
+    params.conditional.type = cudaGraphCondTypeIf;
+    params.conditional.size = 1;
+    ok = ok && cudaGraphAddNode(&if_node, graph, &clear_node, 1, &params) == cudaSuccess;
+    if (ok) {
+      ok = cudaStreamBeginCaptureToGraph(w->capture, params.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                         cudaStreamCaptureModeRelaxed) == cudaSuccess;
+      if (ok) {
+        condition_probe_kernel<<<1, 1, 0, w->capture>>>(handle, counter, 1);
+        cudaGraph_t captured = nullptr;
+        ok = cudaStreamEndCapture(w->capture, &captured) == cudaSuccess;
+      }
+    }
+    ok = ok && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+    ok = ok && cudaGraphLaunch(exec, s) == cudaSuccess;
+    unsigned ran = 1;
+    ok = ok && cudaMemcpyAsync(&ran, counter, sizeof(unsigned), cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+         cudaStreamSynchronize(s) == cudaSuccess;
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    w->conditional_checked = ok && ran == 0;
+    return w->conditional_checked;
   }
 
   int run(const void* e, const void* bcell, const void* j, const void* mass_v, double* etheta,
@@ -585,6 +836,7 @@ struct Solve {
     const long long N = w->count;
     const int m = w->restart;
     tpicb200_gmres_result res{};
+    const bool graph = loop_ready(mass);
     // Initial guess E^n (the copy of E into theta, maxwell_device.hpp:134-147) and the RHS.
     pack_storage_kernel<Fld><<<blocks(), kThreads, 0, s>>>(g, (const Fld*)e, w->x);
     launch_rhs(P::id, g, w->delta, w->kfac, e, bcell, j, w->rhs, s);
@@ -596,7 +848,7 @@ struct Solve {
     count_launches(1);
     reduce(2);
     double controls[2];
-    if (!read_controls(w->values, controls)) return TPICB200_BACKEND_FAILURE;
+    if (!read_back(w->values, controls)) return TPICB200_BACKEND_FAILURE;
     if (!std::isfinite(controls[0]) || !std::isfinite(controls[1])) return TPICB200_OVERFLOW;
     res.residual = res.initial_residual = std::sqrt(controls[0]);
     res.rhs_norm = std::sqrt(controls[1]);
@@ -611,53 +863,43 @@ struct Solve {
       cudaMemsetAsync(w->state, 0, ((size_t)m * (m + 1) + 4 * m + 3) * sizeof(double), s);
       // values[0] holds |r|^2 of the residual just formed.
       normalize_kernel<double, S><<<w->rblocks, kThreads, 0, s>>>(
-          g, w->r, w->values, w->template basis_col<S>(0), w->input,
-          ArnoldiTail{nullptr, nullptr, nullptr, w->ls_rhs(), nullptr, -1});
-      count_launches(1);
-      check();
+          g, w->r, w->values, w->template basis_col<S>(0), N, w->input,
+          ArnoldiTail{nullptr, nullptr, nullptr, w->ls_rhs(), nullptr, -1, 0}, nullptr);
       const int columns = std::min(m, max_iterations - res.iterations);
       const double cycle_tolerance =
           refined ? std::max(atol, res.residual * 16.0 * double(std::numeric_limits<S>::epsilon())) : atol;
-      int completed = 0;
-      bool breakdown = false;
-      for (int col = 0; col < columns; ++col) {
-        S* image = (S*)w->image;
-        apply<S, S>(mass, image);
-        const dim3 grid(w->rblocks, (col + 1 + kDotTile - 1) / kDotTile);
-        dot_batch_kernel<S><<<grid, kThreads, 0, s>>>(w->template basis_col<S>(0), image, w->partials, N, col + 1);
-        reduce(col + 1);
-        double* h_column = w->hessenberg() + (size_t)col * (m + 1);
-        orthogonalize_kernel<S><<<w->rblocks, kThreads, 0, s>>>(w->template basis_col<S>(0), w->values, image,
-                                                               h_column, w->partials, N, col + 1);
-        reduce(1);
-        normalize_kernel<S, S><<<w->rblocks, kThreads, 0, s>>>(
-            g, image, w->values, w->template basis_col<S>(col + 1), w->input,
-            ArnoldiTail{h_column, w->cosine(), w->sine(), w->ls_rhs(), w->status(), col});
-        count_launches(3);
-        check();
-        double st[2];
-        if (!read_controls(w->status(), st)) return TPICB200_BACKEND_FAILURE;
-        if (!std::isfinite(st[0]) || !std::isfinite(st[1])) return TPICB200_OVERFLOW;
-        completed = col + 1;
-        breakdown = st[1] != 0.0;
-        if (st[0] <= cycle_tolerance || breakdown) break;
-      }
-      back_substitute_kernel<<<1, 1, 0, s>>>(w->hessenberg(), w->ls_rhs(), w->coefficients(), m + 1, completed);
-      update_solution_kernel<S><<<grid_for(N, kThreads), kThreads, 0, s>>>(w->template basis_col<S>(0),
-                                                                          w->coefficients(), w->x, N, completed);
+      arnoldi_begin_kernel<<<1, 1, 0, s>>>(w->ctl, columns, cycle_tolerance);
       count_launches(2);
       check();
-      res.iterations += completed;
+      ArnoldiControl control{};
+      if (graph) {
+        if (err == cudaSuccess) err = cudaGraphLaunch(w->loop_exec, s);
+      } else {
+        for (int col = 0; col < columns; ++col) {
+          step(mass, s, cudaGraphConditionalHandle{}, 0);
+          if (!read_back(nullptr, nullptr, &control)) return TPICB200_BACKEND_FAILURE;
+          if (control.stop) break;
+        }
+      }
+      back_substitute_kernel<<<1, 1, 0, s>>>(w->hessenberg(), w->ls_rhs(), w->coefficients(), m + 1, w->ctl);
+      update_solution_kernel<S><<<grid_for(N, kThreads), kThreads, 0, s>>>(w->template basis_col<S>(0),
+                                                                          w->coefficients(), w->x, N, w->ctl);
+      count_launches(2);
+      check();
       apply_solution(mass);
       residual_kernel<false><<<w->rblocks, kThreads, 0, s>>>(w->b, w->ximage, w->r, w->partials, N);
       count_launches(1);
       reduce(1);
-      if (!read_controls(w->values, controls)) return TPICB200_BACKEND_FAILURE;
+      if (!read_back(w->values, controls, &control)) return TPICB200_BACKEND_FAILURE;
+      if (graph) count_launches(w->loop_launches * unsigned(control.completed));
+      if (control.stop == 2) return TPICB200_OVERFLOW;
       if (!std::isfinite(controls[0]) || controls[0] < 0) return TPICB200_OVERFLOW;
+      res.iterations += control.completed;
       res.residual = std::sqrt(controls[0]);
       converged();
-      if (breakdown && !res.converged) break;
+      if (control.breakdown && !res.converged) break;
     }
+    res.host_waits = waits;
     if (result) *result = res;
     if (!res.converged) return TPICB200_NOT_CONVERGED;
     unpack_kernel<double><<<blocks(), kThreads, 0, s>>>(g, w->x, etheta);

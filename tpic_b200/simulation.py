@@ -32,6 +32,7 @@ class Report:
     kinetic: tuple
     total_energy: float
     stage_ms: tuple
+    gmres_host_waits: int = 0
 
 
 def _ptr(t) -> int:
@@ -177,7 +178,8 @@ class Simulation:
         ns = self.state.ns
         for r in reports[:ncycles]:
             out.append(Report(r.gmres.iterations, r.gmres.relative_residual, tuple(r.field_energy),
-                              tuple(r.species[s][0] for s in range(ns)), r.total_energy, tuple(r.stage_ms)))
+                              tuple(r.species[s][0] for s in range(ns)), r.total_energy, tuple(r.stage_ms),
+                              r.gmres.host_waits))
         self.reports.extend(out)
         return out
 
