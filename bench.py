@@ -346,8 +346,8 @@ def stage_kernel_times(sim, args, stream, repeats: int = 5) -> dict:
     # per-cell moments (267 floats per cell, groups of four cells), which the
     # fold assembles; the scalar forms deposit J and the mass records.
     cells = g.nx * g.ny * g.nz
-    tc_form = st.mass_kind in (_lib.MASS_KINDS["tf32"], _lib.MASS_KINDS["bf16x3"])
-    moment_bytes = 267 * 4 * ((cells + 3) // 4 * 4)
+    tc_form = st.mass_kind in (_lib.MASS_KINDS["tf32"], _lib.MASS_KINDS["bf16x3"], _lib.MASS_KINDS["moments-f64"])
+    moment_bytes = 267 * (8 if st.mass_kind == _lib.MASS_KINDS["moments-f64"] else 4) * ((cells + 3) // 4 * 4)
     parts = (_lib.Particles * ns)(*[st.slot[s][st.current[s]] for s in range(ns)])
     qom = (C.c_double * ns)(*[st.qom[s] for s in range(ns)])
     counts = (C.c_void_p * ns)(*[st.counts[s] for s in range(ns)])
@@ -475,8 +475,9 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["tpic_b200", "reference"], default="tpic_b200")
-    ap.add_argument("--mass-matrix", default="bf16x3", choices=["scalar", "scalar-f64", "tf32", "bf16x3"])
-    ap.add_argument("--compare", default="scalar", choices=["scalar", "scalar-f64", "tf32", "bf16x3", "none"],
+    ap.add_argument("--mass-matrix", default="bf16x3", choices=["scalar", "scalar-f64", "tf32", "bf16x3", "moments-f64"])
+    ap.add_argument("--compare", default="scalar",
+                    choices=["scalar", "scalar-f64", "tf32", "bf16x3", "moments-f64", "none"],
                     help="second form timed on the same workload (default: the plain FP32 CUDA-core form)")
     ap.add_argument("--drift-cycles", type=int, default=100, help="cycles of the energy-drift run of each form")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "double"])

@@ -92,7 +92,10 @@ enum {
   TPICB200_MASS_SCALAR = 0,     /* CUDA cores, the precision mode's compute type */
   TPICB200_MASS_SCALAR_F64 = 1, /* CUDA cores, FP64 cell sums, narrowed once at the flush */
   TPICB200_MASS_TF32 = 2,       /* tcgen05 tensor cores, TF32 operands, FP32 accumulation */
-  TPICB200_MASS_BF16X3 = 3      /* tcgen05, BF16 hi/lo split products, FP32 accumulation */
+  TPICB200_MASS_BF16X3 = 3,     /* tcgen05, BF16 hi/lo split products, FP32 accumulation */
+  TPICB200_MASS_MOMENTS_F64 = 4 /* CUDA cores, FP64 per-cell moments (27 pair-weight classes x
+                                   (9 response + 3 current) entries), then a per-node assembly;
+                                   DOUBLE precision only */
 };
 
 typedef struct {

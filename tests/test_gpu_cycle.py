@@ -36,10 +36,11 @@ def run_both(case, precision, cycles, mass_kind="scalar", mass_layout="records")
     return sim, reports, oc, energies
 
 
-@pytest.mark.parametrize("mass_layout", ["records", "stencil-major"])
-def test_c1_cycle_matches_oracle_fp64(mass_layout):
+@pytest.mark.parametrize("mass_layout,mass_kind", [("records", "scalar"), ("stencil-major", "scalar"),
+                                                   ("records", "moments-f64"), ("stencil-major", "moments-f64")])
+def test_c1_cycle_matches_oracle_fp64(mass_layout, mass_kind):
     case = c1_case(n=16)
-    sim, reports, oc, energies = run_both(case, 0, 3, mass_layout=mass_layout)
+    sim, reports, oc, energies = run_both(case, 0, 3, mass_kind=mass_kind, mass_layout=mass_layout)
     for r, e, og in zip(reports, energies, oc.gmres):
         assert r.gmres_iterations == og.iterations
         # The Arnoldi steps of a restart cycle run as one graph: one wait for

@@ -265,13 +265,15 @@ def stage_timings(precision, mass_kind, level_deposit, level_move, n=64, ppc_axi
     return out
 
 
-@pytest.mark.parametrize("form", ["fp64", "mixed-bf16x3"])
+@pytest.mark.parametrize("form", ["fp64", "fp64-moments", "mixed-bf16x3"])
 def test_stage_times_against_the_reference_kernels(form):
     """Both sides timed on the same records (64^3 cells, 2 species x 64 per
     cell, sorted): the figures are reported; the check is that every kernel
     ran without raising the invalid flag."""
     if form == "fp64":
         t = stage_timings("double", "scalar", 0, 0)
+    elif form == "fp64-moments":
+        t = stage_timings("double", "moments-f64", 0, None)
     else:
         t = stage_timings("mixed", "bf16x3", 1, 1)
     t["form"] = form

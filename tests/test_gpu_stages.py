@@ -173,16 +173,18 @@ def test_deposit_matches_oracle(torch_cuda, precision, kind, sorted_bins, layout
     assert_moments(g, j.cpu().numpy().astype(np.float64), ctx.records(m), jw, mw, rel)
 
 
-@pytest.mark.parametrize("precision,kind", [(0, 0), (1, 0), (1, 1)])
+@pytest.mark.parametrize("precision,kind", [(0, 0), (1, 0), (1, 1), (0, 4)])
 def test_reference_mass_fixture(torch_cuda, precision, kind):
     g, d, bnode = reference_mass_fixture(precision)
     n = len(d["cell"])
     ctx = make_ctx(g, precision, dt=0.14, max_particles=n)
     parts = ctx.upload_particles(d)
     parts, counts, offsets = ctx.sort(parts, n)  # the fixture is already in key order
-    _, m = ctx.moments()
-    ctx.deposit(-1.0, parts, n, ctx.field(bnode), None, m, counts, offsets, kind=kind)
-    ctx.fold(None, m)
+    j, m = ctx.moments()
+    if kind != 4:  # the moment form deposits J-hat and the mass together
+        j = None
+    ctx.deposit(-1.0, parts, n, ctx.field(bnode), j, m, counts, offsets, kind=kind)
+    ctx.fold(j, m)
     want = host_matrix_core_mass(g, d, bnode, -0.07)
     got = m.cpu().numpy().astype(np.float64)
     wi, gi = interior_records(g, want), interior_records(g, got)
@@ -323,6 +325,35 @@ def test_tc_mass_matches_oracle(torch_cuda, kind, rel, layout, nx):
     mw_i, mg_i = interior_records(g, mw), interior_records(g, mg)
     err = np.abs(mg_i - mw_i).max() / np.abs(mw_i).max()
     assert err <= rel, err
+
+
+@pytest.mark.parametrize("layout,nx", [(0, 6), (1, 6), (1, 8), (0, 8)])
+def test_fp64_moments_match_oracle(torch_cuda, layout, nx):
+    """The FP64 moment form (double precision): J-hat and the mass records
+    equal the oracle's scalar deposition to the rounding of the regrouped
+    sums, for both mass layouts and both assembly paths (nx a multiple of
+    four or not), two species adding into one set of moments."""
+    g = GRID if nx == GRID.nx else GridSpec(nx, GRID.ny, GRID.nz, GRID.lx * nx / GRID.nx, GRID.ly, GRID.lz)
+    rng = np.random.default_rng(31)
+    d1 = species_arrays(g, 0, seed=5, vth=(0.2, 0.1, 0.3), npcel=(4, 4, 4), qom=-4.0)
+    d2 = species_arrays(g, 0, seed=6, vth=(0.02, 0.01, 0.03), npcel=(3, 3, 3), qom=1.0)
+    ctx = make_ctx(g, 0, dt=0.2, max_particles=len(d1["cell"]), mass_layout=layout)
+    bnode = periodic_node_field(g, smooth_random_unique(g, rng, 0.9))
+    bn = ctx.field(bnode)
+    j, m = ctx.moments()
+    jw = np.zeros(3 * ctx.layout.node_count)
+    mw = np.zeros(126 * ctx.layout.node_count)
+    for qom, d in ((-4.0, d1), (1.0, d2)):
+        n = len(d["cell"])
+        parts, counts, offsets = ctx.sort(ctx.upload_particles(d), n)
+        ctx.deposit(qom, parts, n, bn, j, m, counts, offsets, kind=4)
+        js, ms, bad = oracle_moments(g, 0, qom, 0.2, d, bnode)
+        assert bad == 0
+        jw += js
+        mw += ms
+    ctx.fold(j, m)
+    assert ctx.invalid_count() == 0
+    assert_moments(g, j.cpu().numpy(), ctx.records(m), jw, mw, 1e-13)
 
 
 @pytest.mark.parametrize("kind", [2, 3])

@@ -14,12 +14,13 @@ LIBRARY = Path(__file__).resolve().parent / "libtpicb200.so"
 SUCCESS, INVALID_ARGUMENT, INVALID_STATE, OVERFLOW, BACKEND_FAILURE = 0, 1, 2, 3, 4
 NOT_CONVERGED, CAPACITY_EXCEEDED, INVALID_DATA = 5, 6, 7
 PRECISION_DOUBLE, PRECISION_MIXED = 0, 1
-MASS_SCALAR, MASS_SCALAR_F64, MASS_TF32, MASS_BF16X3 = 0, 1, 2, 3
+MASS_SCALAR, MASS_SCALAR_F64, MASS_TF32, MASS_BF16X3, MASS_MOMENTS_F64 = 0, 1, 2, 3, 4
 MASS_LAYOUT_RECORDS, MASS_LAYOUT_STENCIL_MAJOR = 0, 1
 MAX_SPECIES = 8
 
 MASS_KINDS = {"scalar": MASS_SCALAR, "scalar-f64": MASS_SCALAR_F64, "fp64": MASS_SCALAR_F64,
-              "tf32": MASS_TF32, "bf16x3": MASS_BF16X3, "matrix-core": MASS_TF32}
+              "tf32": MASS_TF32, "bf16x3": MASS_BF16X3, "matrix-core": MASS_TF32,
+              "moments-f64": MASS_MOMENTS_F64}
 PRECISIONS = {"double": PRECISION_DOUBLE, "mixed": PRECISION_MIXED}
 
 

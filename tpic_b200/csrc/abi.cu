@@ -32,7 +32,7 @@ struct tpicb200_context {
   double* pinned = nullptr;      // host mirror of `reduced` + invalid
   int energy_blocks = 0;
   cudaEvent_t events[6 + 3 * TPICB200_MAX_SPECIES]{};
-  float* moments = nullptr;      // per-cell moments of the tensor-core forms (mixed precision)
+  void* moments = nullptr;       // per-cell moments of the moment forms (float: tensor core; double: FP64)
   bool moments_pending = false;  // moments hold deposits not yet assembled
   // J and mass buffers zeroed by the last tpicb200_clear_moments that nothing
   // else has deposited into since: the assembly may store instead of add.
@@ -70,6 +70,35 @@ int check_particles(const tpicb200_context* ctx, const tpicb200_particles* p) {
 
 uint32_t* invalid_or_own(tpicb200_context* ctx, uint32_t* invalid) {
   return invalid ? invalid : ctx->invalid;
+}
+
+// Forms that deposit per-cell moments, assembled into J and the mass records
+// by the fold: the tensor-core forms (mixed precision) and the FP64 moments.
+bool moment_form(int kind) {
+  return kind == TPICB200_MASS_TF32 || kind == TPICB200_MASS_BF16X3 || kind == TPICB200_MASS_MOMENTS_F64;
+}
+
+// The mass form is admitted by the precision mode.
+int check_mass_kind(const tpicb200_context* ctx, int kind) {
+  if (kind < TPICB200_MASS_SCALAR || kind > TPICB200_MASS_MOMENTS_F64)
+    return fail(TPICB200_INVALID_ARGUMENT, "unknown mass kind");
+  const bool dbl = ctx->opt.precision == TPICB200_PRECISION_DOUBLE;
+  if (dbl && (kind == TPICB200_MASS_TF32 || kind == TPICB200_MASS_BF16X3))
+    return fail(TPICB200_INVALID_ARGUMENT, "tensor-core mass forms need the mixed precision mode");
+  if (!dbl && kind == TPICB200_MASS_MOMENTS_F64)
+    return fail(TPICB200_INVALID_ARGUMENT, "the FP64 moment form needs the double precision mode");
+  return TPICB200_SUCCESS;
+}
+
+cudaError_t launch_moments(tpicb200_context* ctx, int kind, int ns, const double* qom,
+                           const tpicb200_particles* const* parts, const uint32_t* const* counts,
+                           const uint32_t* const* offsets, const void* b_node, int accumulate, uint32_t* invalid,
+                           const SortedCopy* const* copies, cudaStream_t s) {
+  if (kind == TPICB200_MASS_MOMENTS_F64)
+    return launch_deposit_moments_f64(ctx->g, ns, qom, ctx->opt.dt, ctx->opt.c, parts, counts, offsets, b_node,
+                                      (double*)ctx->moments, accumulate, invalid, copies, s);
+  return launch_deposit_tc(kind, ctx->g, ns, qom, ctx->opt.dt, ctx->opt.c, parts, counts, offsets, b_node,
+                           (float*)ctx->moments, accumulate, invalid, copies, s);
 }
 
 }  // namespace
@@ -164,7 +193,7 @@ int tpicb200_create(const tpicb200_grid* grid, const tpicb200_options* options, 
   alloc((void**)&ctx->mover_partials, size_t(kMoverPartials) * 5 * TPICB200_MAX_SPECIES * 8);
   alloc((void**)&ctx->reduced, (2 + 5 * TPICB200_MAX_SPECIES + 2) * 8);
   alloc((void**)&ctx->center, (size_t(4) * ctx->energy_blocks + 4) * 8);
-  if (options->precision == TPICB200_PRECISION_MIXED) alloc((void**)&ctx->moments, moment_floats(ctx->g) * 4);
+  alloc((void**)&ctx->moments, moment_floats(ctx->g) * (options->precision == TPICB200_PRECISION_MIXED ? 4 : 8));
   if (e == cudaSuccess) e = cudaMallocHost((void**)&ctx->pinned, (2 + 5 * TPICB200_MAX_SPECIES + 2) * 8);
   if (e == cudaSuccess) e = cudaMemset(ctx->invalid, 0, 4);
   for (auto& ev : ctx->events)
@@ -302,22 +331,18 @@ int tpicb200_deposit(tpicb200_context* ctx, double qom, const tpicb200_particles
   if (!b_node || !std::isfinite(qom)) return fail(TPICB200_INVALID_ARGUMENT, "deposit needs B nodes and finite q/m");
   if ((counts == nullptr) != (offsets == nullptr))
     return fail(TPICB200_INVALID_ARGUMENT, "counts and offsets go together");
-  const bool dbl = ctx->opt.precision == TPICB200_PRECISION_DOUBLE;
-  if (mass_kind < TPICB200_MASS_SCALAR || mass_kind > TPICB200_MASS_BF16X3)
-    return fail(TPICB200_INVALID_ARGUMENT, "unknown mass kind");
-  if (dbl && mass_kind != TPICB200_MASS_SCALAR && mass_kind != TPICB200_MASS_SCALAR_F64)
-    return fail(TPICB200_INVALID_ARGUMENT, "tensor-core mass forms need the mixed precision mode");
+  if (int r = check_mass_kind(ctx, mass_kind)) return r;
   const double boc = qom * ctx->opt.dt / 2 / ctx->opt.c;
   if (!std::isfinite(boc)) return fail(TPICB200_OVERFLOW, "beta/c is not finite");
   uint32_t* inv = invalid_or_own(ctx, invalid);
   cudaStream_t s = (cudaStream_t)stream;
-  if (mass_kind == TPICB200_MASS_TF32 || mass_kind == TPICB200_MASS_BF16X3) {
-    if (!counts) return fail(TPICB200_INVALID_ARGUMENT, "tensor-core mass forms need sorted bins");
-    if (!j || !mass) return fail(TPICB200_INVALID_ARGUMENT, "tensor-core forms deposit J-hat and mass together");
+  if (moment_form(mass_kind)) {
+    if (!counts) return fail(TPICB200_INVALID_ARGUMENT, "moment mass forms need sorted bins");
+    if (!j || !mass) return fail(TPICB200_INVALID_ARGUMENT, "moment mass forms deposit J-hat and mass together");
     const int accumulate = ctx->moments_pending ? 1 : 0;
-    const int r = cuda_status(launch_deposit_tc(mass_kind, ctx->g, 1, &qom, ctx->opt.dt, ctx->opt.c, &p, &counts,
-                                                &offsets, b_node, ctx->moments, accumulate, inv, nullptr, s),
-                              "tensor-core deposition launch failed");
+    const int r = cuda_status(launch_moments(ctx, mass_kind, 1, &qom, &p, &counts, &offsets, b_node, accumulate, inv,
+                                             nullptr, s),
+                              "moment deposition launch failed");
     if (r == TPICB200_SUCCESS) ctx->moments_pending = true;
     return r;
   }
@@ -330,10 +355,11 @@ int tpicb200_deposit(tpicb200_context* ctx, double qom, const tpicb200_particles
 int tpicb200_fold_periodic(tpicb200_context* ctx, void* j, void* mass, tpicb200_stream stream) {
   if (int s = check_ctx(ctx)) return s;
   if (ctx->moments_pending) {
-    // Cell moments of the tensor-core forms are added into the unique nodes first.
-    if (!j || !mass) return fail(TPICB200_INVALID_ARGUMENT, "pending tensor-core moments need J-hat and mass");
+    // Cell moments of the moment forms are added into the unique nodes first.
+    if (!j || !mass) return fail(TPICB200_INVALID_ARGUMENT, "pending cell moments need J-hat and mass");
     const int overwrite = j == ctx->cleared_j && mass == ctx->cleared_mass ? 1 : 0;
-    if (int r = cuda_status(launch_assemble_moments(ctx->g, ctx->moments, j, mass, overwrite, (cudaStream_t)stream),
+    if (int r = cuda_status(launch_assemble_moments(ctx->opt.precision, ctx->g, ctx->moments, j, mass, overwrite,
+                                                    (cudaStream_t)stream),
                             "moment assembly failed"))
       return r;
     ctx->moments_pending = false;
@@ -472,32 +498,31 @@ int tpicb200_deposit_species(tpicb200_context* ctx, int ns, const double* qom, c
   if (int s = check_ctx(ctx)) return s;
   if (ns < 0 || ns > TPICB200_MAX_SPECIES || (ns > 0 && (!qom || !species || !counts || !offsets)))
     return fail(TPICB200_INVALID_ARGUMENT, "invalid species arrays");
-  if (mass_kind != TPICB200_MASS_TF32 && mass_kind != TPICB200_MASS_BF16X3) {
+  if (!moment_form(mass_kind)) {
     for (int sp = 0; sp < ns; ++sp)
       if (int r = tpicb200_deposit(ctx, qom[sp], &species[sp], counts[sp], offsets[sp], b_node, j, mass, mass_kind,
                                    invalid, stream))
         return r;
     return TPICB200_SUCCESS;
   }
-  // Tensor-core forms: the per-species checks of tpicb200_deposit, then one
+  // Moment forms: the per-species checks of tpicb200_deposit, then one
   // fused pass per species pair.
-  if (ctx->opt.precision != TPICB200_PRECISION_MIXED)
-    return fail(TPICB200_INVALID_ARGUMENT, "tensor-core mass forms need the mixed precision mode");
+  if (int r = check_mass_kind(ctx, mass_kind)) return r;
   if (!b_node) return fail(TPICB200_INVALID_ARGUMENT, "deposit needs B nodes");
-  if (!j || !mass) return fail(TPICB200_INVALID_ARGUMENT, "tensor-core forms deposit J-hat and mass together");
+  if (!j || !mass) return fail(TPICB200_INVALID_ARGUMENT, "moment mass forms deposit J-hat and mass together");
   if (ns == 0) return TPICB200_SUCCESS;
   const tpicb200_particles* parts[TPICB200_MAX_SPECIES];
   for (int sp = 0; sp < ns; ++sp) {
     parts[sp] = &species[sp];
     if (int r = check_particles(ctx, parts[sp])) return r;
-    if (!counts[sp] || !offsets[sp]) return fail(TPICB200_INVALID_ARGUMENT, "tensor-core mass forms need sorted bins");
+    if (!counts[sp] || !offsets[sp]) return fail(TPICB200_INVALID_ARGUMENT, "moment mass forms need sorted bins");
     if (!std::isfinite(qom[sp])) return fail(TPICB200_INVALID_ARGUMENT, "deposit needs finite q/m");
     if (!std::isfinite(qom[sp] * ctx->opt.dt / 2 / ctx->opt.c)) return fail(TPICB200_OVERFLOW, "beta/c is not finite");
   }
-  const int r = cuda_status(launch_deposit_tc(mass_kind, ctx->g, ns, qom, ctx->opt.dt, ctx->opt.c, parts, counts,
-                                              offsets, b_node, ctx->moments, ctx->moments_pending ? 1 : 0,
-                                              invalid_or_own(ctx, invalid), nullptr, (cudaStream_t)stream),
-                            "tensor-core deposition launch failed");
+  const int r = cuda_status(launch_moments(ctx, mass_kind, ns, qom, parts, counts, offsets, b_node,
+                                           ctx->moments_pending ? 1 : 0, invalid_or_own(ctx, invalid), nullptr,
+                                           (cudaStream_t)stream),
+                            "moment deposition launch failed");
   if (r == TPICB200_SUCCESS) ctx->moments_pending = true;
   return r;
 }
@@ -651,11 +676,10 @@ static int deposit_pair(tpicb200_context* ctx, tpicb200_state* st, int first, in
   const int kind = st->mass_kind;
   const int p = ctx->opt.precision;
   cudaError_t e = cudaSuccess;
-  if (kind == TPICB200_MASS_TF32 || kind == TPICB200_MASS_BF16X3) {
-    if (p != TPICB200_PRECISION_MIXED)
-      return fail(TPICB200_INVALID_ARGUMENT, "tensor-core mass forms need the mixed precision mode");
-    e = launch_deposit_tc(kind, ctx->g, count, qom, ctx->opt.dt, ctx->opt.c, parts, counts, offsets, st->b_node_next,
-                          ctx->moments, accumulate ? 1 : 0, ctx->invalid, copies, s);
+  if (moment_form(kind)) {
+    if (int r = check_mass_kind(ctx, kind)) return r;
+    e = launch_moments(ctx, kind, count, qom, parts, counts, offsets, st->b_node_next, accumulate ? 1 : 0,
+                       ctx->invalid, copies, s);
     if (e == cudaSuccess) ctx->moments_pending = true;
   } else {
     ctx->cleared_j = ctx->cleared_mass = nullptr;
@@ -734,7 +758,7 @@ int tpicb200_cycle(tpicb200_context* ctx, tpicb200_state* st, int ncycles, tpicb
   if (int r = check_state(ctx, st)) return r;
   if (ncycles < 0) return fail(TPICB200_INVALID_ARGUMENT, "negative cycle count");
   const int kind = st->mass_kind;
-  if (kind < TPICB200_MASS_SCALAR || kind > TPICB200_MASS_BF16X3) return fail(TPICB200_INVALID_ARGUMENT, "unknown mass kind");
+  if (int r = check_mass_kind(ctx, kind)) return r;
   cudaStream_t s = (cudaStream_t)stream;
   cudaEvent_t* ev = ctx->events;
   cudaEvent_t* sev = ctx->events + 6;  // per species: after its mover, after its sort, after its pair's deposition
@@ -753,9 +777,9 @@ int tpicb200_cycle(tpicb200_context* ctx, tpicb200_state* st, int ncycles, tpicb
     cudaEventRecord(ev[2], s);
     // Per pair of species: the mover and the sort of each, then one
     // deposition of both with the next B that also writes the sorted records.
-    // The tensor-core forms need no cleared J and mass: the assembly stores
+    // The moment forms need no cleared J and mass: the assembly stores
     // every entry of the unique nodes and the fold copies every other vertex.
-    if ((kind == TPICB200_MASS_TF32 || kind == TPICB200_MASS_BF16X3) && st->ns > 0) {
+    if (moment_form(kind) && st->ns > 0) {
       ctx->moments_pending = false;
       ctx->cleared_j = st->j;
       ctx->cleared_mass = st->mass;

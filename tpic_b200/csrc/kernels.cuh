@@ -125,8 +125,15 @@ cudaError_t launch_deposit_tc(int mass_kind, const Geom& g, int ns, const double
                               const tpicb200_particles* const* p, const uint32_t* const* counts,
                               const uint32_t* const* offsets, const void* bnode, float* moments, int accumulate,
                               uint32_t* invalid, const SortedCopy* const* copies, cudaStream_t s);
-cudaError_t launch_assemble_moments(const Geom& g, const float* moments, void* j, void* mass, int overwrite,
-                                    cudaStream_t s);
+// FP64 CUDA-core form of the same moments (double precision; double moments).
+cudaError_t launch_deposit_moments_f64(const Geom& g, int ns, const double* qom, double dt, double c,
+                                       const tpicb200_particles* const* p, const uint32_t* const* counts,
+                                       const uint32_t* const* offsets, const void* bnode, double* moments,
+                                       int accumulate, uint32_t* invalid, const SortedCopy* const* copies,
+                                       cudaStream_t s);
+// Moments (float or double, as the precision mode) into J and the mass records.
+cudaError_t launch_assemble_moments(int precision, const Geom& g, const void* moments, void* j, void* mass,
+                                    int overwrite, cudaStream_t s);
 
 // fields.cu
 cudaError_t launch_node_ghosts(const Geom& g, double* f, int components, cudaStream_t s);

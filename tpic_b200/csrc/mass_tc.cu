@@ -1245,15 +1245,15 @@ __host__ __device__ constexpr StencilPairs make_stencil_pairs() {
 // at most nine sums and the loads of a warp are consecutive across its
 // nodes. `overwrite` stores the sums (J and M were cleared and nothing else
 // was deposited); otherwise they are added.
-template <int S>
+template <class T, int S>
 __device__ __forceinline__ void assemble_stencil(const Geom& g, const long long (&cell)[8], long long node,
-                                                 const float* __restrict__ mom,
-                                                 float* __restrict__ J, float* __restrict__ M, int overwrite) {
+                                                 const T* __restrict__ mom,
+                                                 T* __restrict__ J, T* __restrict__ M, int overwrite) {
   constexpr StencilPairs pairs = make_stencil_pairs();
   if constexpr (S < 14) {
-    float sum[9];
+    T sum[9];
 #pragma unroll
-    for (int e = 0; e < 9; ++e) sum[e] = 0.0f;
+    for (int e = 0; e < 9; ++e) sum[e] = T(0);
 #pragma unroll
     for (int p = 0; p < 8; ++p) {
       if (p < pairs.count[S]) {
@@ -1264,23 +1264,24 @@ __device__ __forceinline__ void assemble_stencil(const Geom& g, const long long 
     }
 #pragma unroll
     for (int e = 0; e < 9; ++e) {
-      float* dst = M + g.mass_index(node, S * 9 + e);
+      T* dst = M + g.mass_index(node, S * 9 + e);
       *dst = overwrite ? sum[e] : *dst + sum[e];
     }
   } else {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      float sum = 0.0f;
+      T sum = T(0);
 #pragma unroll
       for (int a = 0; a < 8; ++a) sum += __ldg(mom + moment_index(cell[a], kMassMoments + a * 3 + c));
-      float* dst = J + c * g.nodes + node;
+      T* dst = J + c * g.nodes + node;
       *dst = overwrite ? sum : *dst + sum;
     }
   }
 }
 
-__global__ void __launch_bounds__(128) assemble_moments_kernel(Geom g, const float* __restrict__ mom,
-                                                               float* __restrict__ J, float* __restrict__ M,
+template <class T>
+__global__ void __launch_bounds__(128) assemble_moments_kernel(Geom g, const T* __restrict__ mom,
+                                                               T* __restrict__ J, T* __restrict__ M,
                                                                int overwrite) {
   const int nx = g.nx, ny = g.ny;
   const long long unique = (long long)nx * ny * g.nz;
@@ -1299,21 +1300,21 @@ __global__ void __launch_bounds__(128) assemble_moments_kernel(Geom g, const flo
     cell[a] = ((a & 1) ? i1 : i) + (long long)nx * (((a & 2) ? j1 : j) + (long long)ny * ((a & 4) ? k1 : k));
   const long long node = g.node(i, j, k);
   switch (stencil) {
-    case 0: assemble_stencil<0>(g, cell, node, mom, J, M, overwrite); break;
-    case 1: assemble_stencil<1>(g, cell, node, mom, J, M, overwrite); break;
-    case 2: assemble_stencil<2>(g, cell, node, mom, J, M, overwrite); break;
-    case 3: assemble_stencil<3>(g, cell, node, mom, J, M, overwrite); break;
-    case 4: assemble_stencil<4>(g, cell, node, mom, J, M, overwrite); break;
-    case 5: assemble_stencil<5>(g, cell, node, mom, J, M, overwrite); break;
-    case 6: assemble_stencil<6>(g, cell, node, mom, J, M, overwrite); break;
-    case 7: assemble_stencil<7>(g, cell, node, mom, J, M, overwrite); break;
-    case 8: assemble_stencil<8>(g, cell, node, mom, J, M, overwrite); break;
-    case 9: assemble_stencil<9>(g, cell, node, mom, J, M, overwrite); break;
-    case 10: assemble_stencil<10>(g, cell, node, mom, J, M, overwrite); break;
-    case 11: assemble_stencil<11>(g, cell, node, mom, J, M, overwrite); break;
-    case 12: assemble_stencil<12>(g, cell, node, mom, J, M, overwrite); break;
-    case 13: assemble_stencil<13>(g, cell, node, mom, J, M, overwrite); break;
-    default: assemble_stencil<14>(g, cell, node, mom, J, M, overwrite); break;
+    case 0: assemble_stencil<T, 0>(g, cell, node, mom, J, M, overwrite); break;
+    case 1: assemble_stencil<T, 1>(g, cell, node, mom, J, M, overwrite); break;
+    case 2: assemble_stencil<T, 2>(g, cell, node, mom, J, M, overwrite); break;
+    case 3: assemble_stencil<T, 3>(g, cell, node, mom, J, M, overwrite); break;
+    case 4: assemble_stencil<T, 4>(g, cell, node, mom, J, M, overwrite); break;
+    case 5: assemble_stencil<T, 5>(g, cell, node, mom, J, M, overwrite); break;
+    case 6: assemble_stencil<T, 6>(g, cell, node, mom, J, M, overwrite); break;
+    case 7: assemble_stencil<T, 7>(g, cell, node, mom, J, M, overwrite); break;
+    case 8: assemble_stencil<T, 8>(g, cell, node, mom, J, M, overwrite); break;
+    case 9: assemble_stencil<T, 9>(g, cell, node, mom, J, M, overwrite); break;
+    case 10: assemble_stencil<T, 10>(g, cell, node, mom, J, M, overwrite); break;
+    case 11: assemble_stencil<T, 11>(g, cell, node, mom, J, M, overwrite); break;
+    case 12: assemble_stencil<T, 12>(g, cell, node, mom, J, M, overwrite); break;
+    case 13: assemble_stencil<T, 13>(g, cell, node, mom, J, M, overwrite); break;
+    default: assemble_stencil<T, 14>(g, cell, node, mom, J, M, overwrite); break;
   }
 }
 
@@ -1324,31 +1325,42 @@ __global__ void __launch_bounds__(128) assemble_moments_kernel(Geom g, const flo
 // 4m - 1 .. 4m + 2: the last cell of the previous group (periodic in x), then
 // the first three of the own group. Sums in increasing corner order, as the
 // per-node kernel.
-template <int S>
-__device__ __forceinline__ void assemble_quad(const Geom& g, int m, int j, int k, const float* __restrict__ mom,
-                                              float* __restrict__ J, float* __restrict__ M, int overwrite) {
+// The 16-byte (float) or two 16-byte (double) words of one moment entry of a
+// group of four cells.
+__device__ __forceinline__ void load_quad(const float* p, float (&v)[4]) {
+  const float4 x = __ldg(reinterpret_cast<const float4*>(p));
+  v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+}
+__device__ __forceinline__ void load_quad(const double* p, double (&v)[4]) {
+  const double2 x = __ldg(reinterpret_cast<const double2*>(p)), y = __ldg(reinterpret_cast<const double2*>(p) + 1);
+  v[0] = x.x; v[1] = x.y; v[2] = y.x; v[3] = y.y;
+}
+
+template <class T, int S>
+__device__ __forceinline__ void assemble_quad(const Geom& g, int m, int j, int k, const T* __restrict__ mom,
+                                              T* __restrict__ J, T* __restrict__ M, int overwrite) {
   constexpr StencilPairs pairs = make_stencil_pairs();
   constexpr int kSums = S < 14 ? 9 : 3;
   const int ny = g.ny, nz = g.nz, qx = g.nx >> 2;
   const int j1 = j > 0 ? j - 1 : ny - 1, k1 = k > 0 ? k - 1 : nz - 1;
   const int mp = m > 0 ? m - 1 : qx - 1;
-  const float4* mom4 = reinterpret_cast<const float4*>(mom);
-  float sum[kSums][4];
+  T sum[kSums][4];
 #pragma unroll
   for (int e = 0; e < kSums; ++e)
 #pragma unroll
-    for (int n = 0; n < 4; ++n) sum[e][n] = 0.0f;
+    for (int n = 0; n < 4; ++n) sum[e][n] = T(0);
 #pragma unroll
   for (int a = 0; a < 8; ++a) {
     const long long row = (long long)((a & 2) ? j1 : j) + (long long)ny * ((a & 4) ? k1 : k);
     const long long own = row * qx + m, prev = row * qx + mp;
     auto add = [&](int q, int e) {
-      const float4 v = __ldg(mom4 + own * kMoments + q);
+      T v[4];
+      load_quad(mom + (own * kMoments + q) * 4, v);
       if (a & 1) {
-        const float p3 = __ldg(mom + (prev * kMoments + q) * 4 + 3);
-        sum[e][0] += p3; sum[e][1] += v.x; sum[e][2] += v.y; sum[e][3] += v.z;
+        const T p3 = __ldg(mom + (prev * kMoments + q) * 4 + 3);
+        sum[e][0] += p3; sum[e][1] += v[0]; sum[e][2] += v[1]; sum[e][3] += v[2];
       } else {
-        sum[e][0] += v.x; sum[e][1] += v.y; sum[e][2] += v.z; sum[e][3] += v.w;
+        sum[e][0] += v[0]; sum[e][1] += v[1]; sum[e][2] += v[2]; sum[e][3] += v[3];
       }
     };
     if constexpr (S < 14) {
@@ -1367,14 +1379,15 @@ __device__ __forceinline__ void assemble_quad(const Geom& g, int m, int j, int k
     const long long node = g.node(4 * m + n, j, k);
 #pragma unroll
     for (int e = 0; e < kSums; ++e) {
-      float* dst = S < 14 ? M + g.mass_index(node, S * 9 + e) : J + e * g.nodes + node;
+      T* dst = S < 14 ? M + g.mass_index(node, S * 9 + e) : J + e * g.nodes + node;
       *dst = overwrite ? sum[e][n] : *dst + sum[e][n];
     }
   }
 }
 
-__global__ void __launch_bounds__(128) assemble_quads_kernel(Geom g, const float* __restrict__ mom,
-                                                             float* __restrict__ J, float* __restrict__ M,
+template <class T>
+__global__ void __launch_bounds__(128) assemble_quads_kernel(Geom g, const T* __restrict__ mom,
+                                                             T* __restrict__ J, T* __restrict__ M,
                                                              int overwrite) {
   const int qx = g.nx >> 2, ny = g.ny;
   const long long quads = (long long)qx * ny * g.nz;
@@ -1387,38 +1400,248 @@ __global__ void __launch_bounds__(128) assemble_quads_kernel(Geom g, const float
   const long long r = v / qx;
   const int j = int(r % ny), k = int(r / ny);
   switch (stencil) {
-    case 0: assemble_quad<0>(g, m, j, k, mom, J, M, overwrite); break;
-    case 1: assemble_quad<1>(g, m, j, k, mom, J, M, overwrite); break;
-    case 2: assemble_quad<2>(g, m, j, k, mom, J, M, overwrite); break;
-    case 3: assemble_quad<3>(g, m, j, k, mom, J, M, overwrite); break;
-    case 4: assemble_quad<4>(g, m, j, k, mom, J, M, overwrite); break;
-    case 5: assemble_quad<5>(g, m, j, k, mom, J, M, overwrite); break;
-    case 6: assemble_quad<6>(g, m, j, k, mom, J, M, overwrite); break;
-    case 7: assemble_quad<7>(g, m, j, k, mom, J, M, overwrite); break;
-    case 8: assemble_quad<8>(g, m, j, k, mom, J, M, overwrite); break;
-    case 9: assemble_quad<9>(g, m, j, k, mom, J, M, overwrite); break;
-    case 10: assemble_quad<10>(g, m, j, k, mom, J, M, overwrite); break;
-    case 11: assemble_quad<11>(g, m, j, k, mom, J, M, overwrite); break;
-    case 12: assemble_quad<12>(g, m, j, k, mom, J, M, overwrite); break;
-    case 13: assemble_quad<13>(g, m, j, k, mom, J, M, overwrite); break;
-    default: assemble_quad<14>(g, m, j, k, mom, J, M, overwrite); break;
+    case 0: assemble_quad<T, 0>(g, m, j, k, mom, J, M, overwrite); break;
+    case 1: assemble_quad<T, 1>(g, m, j, k, mom, J, M, overwrite); break;
+    case 2: assemble_quad<T, 2>(g, m, j, k, mom, J, M, overwrite); break;
+    case 3: assemble_quad<T, 3>(g, m, j, k, mom, J, M, overwrite); break;
+    case 4: assemble_quad<T, 4>(g, m, j, k, mom, J, M, overwrite); break;
+    case 5: assemble_quad<T, 5>(g, m, j, k, mom, J, M, overwrite); break;
+    case 6: assemble_quad<T, 6>(g, m, j, k, mom, J, M, overwrite); break;
+    case 7: assemble_quad<T, 7>(g, m, j, k, mom, J, M, overwrite); break;
+    case 8: assemble_quad<T, 8>(g, m, j, k, mom, J, M, overwrite); break;
+    case 9: assemble_quad<T, 9>(g, m, j, k, mom, J, M, overwrite); break;
+    case 10: assemble_quad<T, 10>(g, m, j, k, mom, J, M, overwrite); break;
+    case 11: assemble_quad<T, 11>(g, m, j, k, mom, J, M, overwrite); break;
+    case 12: assemble_quad<T, 12>(g, m, j, k, mom, J, M, overwrite); break;
+    case 13: assemble_quad<T, 13>(g, m, j, k, mom, J, M, overwrite); break;
+    default: assemble_quad<T, 14>(g, m, j, k, mom, J, M, overwrite); break;
   }
+}
+
+
+// ---------------------------------------------------------------------------
+// FP64 CUDA-core form of the moment deposition (double precision).
+//
+// The same per-cell moments as the tensor-core forms, G[t][e] = sum_p m_pt
+// (s_p alpha_p[e]) and H[t][c] = sum_p m_pt j_p[c], accumulated in FP64 on
+// the CUDA cores: a warp per cell; per chunk of 32 records each lane forms
+// one record's B gather, response, s alpha, j and per-axis pair weights
+// ((1-x)^2, x(1-x), x^2) into shared memory, then lane t < 27 adds every
+// record's m_pt s alpha (9 values) and m_pt j (3) into its registers. The
+// flush stores G and the corner currents J_a[c] = sum_b H[t(a,b)][c] into the
+// double moment records, which the assembly adds into J and the mass records
+// as for the tensor-core forms. Per record this is 27 x 12 fused
+// multiply-adds, where the reference's scalar and matrix-core kernels form
+// the 64 corner-pair products of 9 entries (mass_matrix_scalar_device.hpp:25-97,
+// mass_matrix_mma_device.hpp:58-150).
+struct F64Species {
+  const double* rx;
+  const double* ry;
+  const double* rz;
+  const double* u;
+  const double* v;
+  const double* w;
+  const double* q;
+  const int32_t* key;
+  const uint32_t* counts;
+  const uint32_t* offsets;
+  double beta_over_c;
+  const uint32_t* perm;  // sorted position -> record (null: records in sorted order)
+  double* orx;           // sorted copy (null: none)
+  double* ory;
+  double* orz;
+  double* ou;
+  double* ov;
+  double* ow;
+  double* oq;
+  int32_t* okey;
+};
+
+struct F64Params {
+  F64Species sp[kFuse];
+  int ns;
+  double inv_volume;
+};
+
+constexpr int kF64Warps = 4;
+struct F64Warp {
+  double bc[24];        // B at the cell's corners, [c][a]
+  double pw[32][9];     // per record: x, y and z pair-weight classes
+  double src[32][12];   // per record: s alpha[9], j[3]
+  double hs[27][3];     // H of the cell at the flush
+};
+
+__global__ void __launch_bounds__(kF64Warps * 32) moments_f64_kernel(Geom g, F64Params fp,
+                                                                     const double* __restrict__ bnode,
+                                                                     double* __restrict__ mom, int accumulate,
+                                                                     uint32_t* invalid) {
+  __shared__ F64Warp shared[kF64Warps];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  F64Warp& S = shared[warp];
+  const int nx = g.nx, ny = g.ny;
+  const long long cells = (long long)nx * ny * g.nz, nn = g.nodes;
+  const int tx = lane % 3, ty = (lane / 3) % 3, tz = lane / 9;
+  uint32_t bad = 0;
+  for (long long cell = (long long)blockIdx.x * kF64Warps + warp; cell < cells;
+       cell += (long long)gridDim.x * kF64Warps) {
+    const int ci = int(cell % nx), cj = int((cell / nx) % ny), ck = int(cell / ((long long)nx * ny));
+    const int32_t key = g.encode(ci, cj, ck);
+    if (lane < 24) {
+      const int c = lane >> 3, a = lane & 7;
+      S.bc[lane] = bnode[c * nn + g.node(ci + (a & 1), cj + ((a >> 1) & 1), ck + ((a >> 2) & 1))];
+    }
+    __syncwarp();
+    double G[9], H[3];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) G[e] = 0.0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) H[c] = 0.0;
+    for (int si = 0; si < fp.ns; ++si) {
+      const F64Species& sp = fp.sp[si];
+      const uint32_t begin = sp.offsets[key], n = sp.counts[key];
+      for (uint32_t c0 = 0; c0 < n; c0 += 32) {
+        const uint32_t m = n - c0 < 32u ? n - c0 : 32u;
+        if (lane < int(m)) {
+          const uint32_t pos = begin + c0 + lane;
+          const uint32_t r = sp.perm ? sp.perm[pos] : pos;
+          const double fx = sp.rx[r], fy = sp.ry[r], fz = sp.rz[r];
+          const double u = sp.u[r], v = sp.v[r], w = sp.w[r], q = sp.q[r];
+          const int32_t k0 = sp.key[r];
+          if (sp.orx) {
+            sp.orx[pos] = fx; sp.ory[pos] = fy; sp.orz[pos] = fz;
+            sp.ou[pos] = u; sp.ov[pos] = v; sp.ow[pos] = w; sp.oq[pos] = q; sp.okey[pos] = k0;
+          }
+          double* pw = S.pw[lane];
+          double* src = S.src[lane];
+          bool ok = k0 == key && fx >= 0 && fx < 1 && fy >= 0 && fy < 1 && fz >= 0 && fz < 1;
+          if (ok) {
+            double wt[8];
+            cic_weights<double>(fx, fy, fz, wt);
+            double b[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              double val = 0;
+#pragma unroll
+              for (int a = 0; a < 8; ++a) val += wt[a] * S.bc[c * 8 + a];
+              b[c] = val;
+            }
+            const Response<double> resp(b[0], b[1], b[2], sp.beta_over_c);
+            const double scale = sp.beta_over_c * q;
+            double hx, hy, hz;
+            resp.apply(u, v, w, hx, hy, hz);
+            const double qv = q * fp.inv_volume;
+#pragma unroll
+            for (int e = 0; e < 9; ++e) src[e] = resp.a[e] * scale;
+            src[9] = qv * hx; src[10] = qv * hy; src[11] = qv * hz;
+            for (int e = 0; e < 12; ++e) ok = ok && isfinite(src[e]);
+            const double cx = 1.0 - fx, cy = 1.0 - fy, cz = 1.0 - fz;
+            pw[0] = cx * cx; pw[1] = cx * fx; pw[2] = fx * fx;
+            pw[3] = cy * cy; pw[4] = cy * fy; pw[5] = fy * fy;
+            pw[6] = cz * cz; pw[7] = cz * fz; pw[8] = fz * fz;
+          }
+          if (!ok) {
+            ++bad;
+#pragma unroll
+            for (int e = 0; e < 12; ++e) src[e] = 0.0;
+#pragma unroll
+            for (int e = 0; e < 9; ++e) pw[e] = 0.0;
+          }
+        }
+        __syncwarp();
+        if (lane < 27) {
+          for (uint32_t k = 0; k < m; ++k) {
+            const double mt = (S.pw[k][tx] * S.pw[k][3 + ty]) * S.pw[k][6 + tz];
+            const double* src = S.src[k];
+#pragma unroll
+            for (int e = 0; e < 9; ++e) G[e] += mt * src[e];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) H[c] += mt * src[9 + c];
+          }
+        }
+        __syncwarp();
+      }
+    }
+    if (lane < 27) {
+#pragma unroll
+      for (int e = 0; e < 9; ++e) {
+        double* dst = mom + moment_index(cell, lane * 9 + e);
+        *dst = accumulate ? *dst + G[e] : G[e];
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) S.hs[lane][c] = H[c];
+    }
+    __syncwarp();
+    if (lane < 24) {
+      const int a = lane / 3, c = lane % 3;
+      double sum = 0.0;
+#pragma unroll
+      for (int b = 0; b < 8; ++b) sum += S.hs[monomial_class(a, b)][c];
+      double* dst = mom + moment_index(cell, kMassMoments + a * 3 + c);
+      *dst = accumulate ? *dst + sum : sum;
+    }
+    __syncwarp();
+  }
+  bad = warp_sum(bad);
+  if (bad && lane == 0) atomicAdd(invalid, bad);
 }
 
 }  // namespace
 
-cudaError_t launch_assemble_moments(const Geom& g, const float* moments, void* j, void* mass, int overwrite,
-                                    cudaStream_t s) {
+cudaError_t launch_assemble_moments(int precision, const Geom& g, const void* moments, void* j, void* mass,
+                                    int overwrite, cudaStream_t s) {
   const long long unique = (long long)g.nx * g.ny * g.nz;
   const long long items = g.nx % 4 == 0 ? unique / 4 : unique;
   const long long blocks = (items + 127) / 128 * 15;
   if (blocks > 0x7FFFFFFFLL) return cudaErrorInvalidValue;
-  if (g.nx % 4 == 0)
-    assemble_quads_kernel<<<unsigned(blocks), 128, 0, s>>>(g, moments, (float*)j, (float*)mass, overwrite);
-  else
-    assemble_moments_kernel<<<unsigned(blocks), 128, 0, s>>>(g, moments, (float*)j, (float*)mass, overwrite);
+  if (precision == TPICB200_PRECISION_DOUBLE) {
+    if (g.nx % 4 == 0)
+      assemble_quads_kernel<double><<<unsigned(blocks), 128, 0, s>>>(g, (const double*)moments, (double*)j,
+                                                                    (double*)mass, overwrite);
+    else
+      assemble_moments_kernel<double><<<unsigned(blocks), 128, 0, s>>>(g, (const double*)moments, (double*)j,
+                                                                      (double*)mass, overwrite);
+  } else if (g.nx % 4 == 0) {
+    assemble_quads_kernel<float><<<unsigned(blocks), 128, 0, s>>>(g, (const float*)moments, (float*)j,
+                                                                 (float*)mass, overwrite);
+  } else {
+    assemble_moments_kernel<float><<<unsigned(blocks), 128, 0, s>>>(g, (const float*)moments, (float*)j,
+                                                                   (float*)mass, overwrite);
+  }
   count_launches(1);
   return cudaGetLastError();
+}
+
+cudaError_t launch_deposit_moments_f64(const Geom& g, int ns, const double* qom, double dt, double c,
+                                       const tpicb200_particles* const* p, const uint32_t* const* counts,
+                                       const uint32_t* const* offsets, const void* bnode, double* moments,
+                                       int accumulate, uint32_t* invalid, const SortedCopy* const* copies,
+                                       cudaStream_t s) {
+  if (!moments || ns < 1) return cudaErrorInvalidValue;
+  const long long cells = (long long)g.nx * g.ny * g.nz;
+  const unsigned blocks = unsigned(std::min<long long>((cells + kF64Warps - 1) / kF64Warps, 148LL * 16));
+  for (int first = 0; first < ns; first += kFuse) {
+    F64Params fp{};
+    fp.ns = std::min(kFuse, ns - first);
+    fp.inv_volume = g.inv_volume;
+    for (int i = 0; i < fp.ns; ++i) {
+      const tpicb200_particles* sp = p[first + i];
+      const SortedCopy* cp = copies ? copies[first + i] : nullptr;
+      const bool copy = cp && cp->perm && cp->out.rx;
+      fp.sp[i] = F64Species{(const double*)sp->rx, (const double*)sp->ry, (const double*)sp->rz,
+                            (const double*)sp->u, (const double*)sp->v, (const double*)sp->w, sp->q, sp->cell,
+                            counts[first + i], offsets[first + i], qom[first + i] * dt / 2 / c,
+                            cp ? cp->perm : nullptr, copy ? (double*)cp->out.rx : nullptr,
+                            copy ? (double*)cp->out.ry : nullptr, copy ? (double*)cp->out.rz : nullptr,
+                            copy ? (double*)cp->out.u : nullptr, copy ? (double*)cp->out.v : nullptr,
+                            copy ? (double*)cp->out.w : nullptr, copy ? cp->out.q : nullptr,
+                            copy ? cp->out.cell : nullptr};
+    }
+    moments_f64_kernel<<<blocks, kF64Warps * 32, 0, s>>>(g, fp, (const double*)bnode, moments,
+                                                        (accumulate || first > 0) ? 1 : 0, invalid);
+    count_launches(1);
+    if (cudaError_t e = cudaGetLastError()) return e;
+  }
+  return cudaSuccess;
 }
 
 }  // namespace tpicb200
