@@ -1425,14 +1425,16 @@ __global__ void __launch_bounds__(128) assemble_quads_kernel(Geom g, const T* __
 // The same per-cell moments as the tensor-core forms, G[t][e] = sum_p m_pt
 // (s_p alpha_p[e]) and H[t][c] = sum_p m_pt j_p[c], accumulated in FP64 on
 // the CUDA cores: a warp per cell; per chunk of 32 records each lane forms
-// one record's B gather, response, s alpha, j and per-axis pair weights
-// ((1-x)^2, x(1-x), x^2) into shared memory, then lane t < 27 adds every
-// record's m_pt s alpha (9 values) and m_pt j (3) into its registers. The
-// flush stores G and the corner currents J_a[c] = sum_b H[t(a,b)][c] into the
-// double moment records, which the assembly adds into J and the mass records
-// as for the tensor-core forms. Per record this is 27 x 12 fused
-// multiply-adds, where the reference's scalar and matrix-core kernels form
-// the 64 corner-pair products of 9 entries (mass_matrix_scalar_device.hpp:25-97,
+// one record's B gather, response, s alpha and j (12 values) and its 27
+// pair-weight products m_t = (X_tx Y_ty) Z_tz into shared memory; then lane
+// 3b + q (b < 9, q < 3) adds, for every record of the chunk, the products of
+// m_t for t = 3b .. 3b+2 and entries 4q .. 4q+3 of the 12 into a 3 x 4 block
+// of registers (7 shared loads per 12 fused multiply-adds). The flush stores
+// G and the corner currents J_a[c] = sum_b H[t(a,b)][c] into the double
+// moment records, which the assembly adds into J and the mass records as for
+// the tensor-core forms. Per record this is 27 x 12 fused multiply-adds,
+// where the reference's scalar and matrix-core kernels form the 64
+// corner-pair products of 9 entries (mass_matrix_scalar_device.hpp:25-97,
 // mass_matrix_mma_device.hpp:58-150).
 struct F64Species {
   const double* rx;
@@ -1464,11 +1466,15 @@ struct F64Params {
 };
 
 constexpr int kF64Warps = 4;
+// Row pitches with an odd number of 8-byte words past a multiple of 32 banks
+// keep the lanes' row stores spread over the banks.
+constexpr int kF64MPitch = 29;
+constexpr int kF64SPitch = 13;
 struct F64Warp {
-  double bc[24];        // B at the cell's corners, [c][a]
-  double pw[32][9];     // per record: x, y and z pair-weight classes
-  double src[32][12];   // per record: s alpha[9], j[3]
-  double hs[27][3];     // H of the cell at the flush
+  double bc[24];                 // B at the cell's corners, [c][a]
+  double m[32][kF64MPitch];      // per record: the 27 pair-weight products
+  double src[32][kF64SPitch];    // per record: s alpha[9], j[3]
+  double hs[27][3];              // H of the cell at the flush
 };
 
 __global__ void __launch_bounds__(kF64Warps * 32) moments_f64_kernel(Geom g, F64Params fp,
@@ -1480,7 +1486,7 @@ __global__ void __launch_bounds__(kF64Warps * 32) moments_f64_kernel(Geom g, F64
   F64Warp& S = shared[warp];
   const int nx = g.nx, ny = g.ny;
   const long long cells = (long long)nx * ny * g.nz, nn = g.nodes;
-  const int tx = lane % 3, ty = (lane / 3) % 3, tz = lane / 9;
+  const int t0 = 3 * (lane / 3), e0 = 4 * (lane % 3);  // this lane's block (lane < 27)
   uint32_t bad = 0;
   for (long long cell = (long long)blockIdx.x * kF64Warps + warp; cell < cells;
        cell += (long long)gridDim.x * kF64Warps) {
@@ -1491,11 +1497,11 @@ __global__ void __launch_bounds__(kF64Warps * 32) moments_f64_kernel(Geom g, F64
       S.bc[lane] = bnode[c * nn + g.node(ci + (a & 1), cj + ((a >> 1) & 1), ck + ((a >> 2) & 1))];
     }
     __syncwarp();
-    double G[9], H[3];
+    double acc[3][4];
 #pragma unroll
-    for (int e = 0; e < 9; ++e) G[e] = 0.0;
+    for (int i = 0; i < 3; ++i)
 #pragma unroll
-    for (int c = 0; c < 3; ++c) H[c] = 0.0;
+      for (int e = 0; e < 4; ++e) acc[i][e] = 0.0;
     for (int si = 0; si < fp.ns; ++si) {
       const F64Species& sp = fp.sp[si];
       const uint32_t begin = sp.offsets[key], n = sp.counts[key];
@@ -1511,7 +1517,7 @@ __global__ void __launch_bounds__(kF64Warps * 32) moments_f64_kernel(Geom g, F64
             sp.orx[pos] = fx; sp.ory[pos] = fy; sp.orz[pos] = fz;
             sp.ou[pos] = u; sp.ov[pos] = v; sp.ow[pos] = w; sp.oq[pos] = q; sp.okey[pos] = k0;
           }
-          double* pw = S.pw[lane];
+          double* mt = S.m[lane];
           double* src = S.src[lane];
           bool ok = k0 == key && fx >= 0 && fx < 1 && fy >= 0 && fy < 1 && fz >= 0 && fz < 1;
           if (ok) {
@@ -1535,27 +1541,37 @@ __global__ void __launch_bounds__(kF64Warps * 32) moments_f64_kernel(Geom g, F64
             src[9] = qv * hx; src[10] = qv * hy; src[11] = qv * hz;
             for (int e = 0; e < 12; ++e) ok = ok && isfinite(src[e]);
             const double cx = 1.0 - fx, cy = 1.0 - fy, cz = 1.0 - fz;
-            pw[0] = cx * cx; pw[1] = cx * fx; pw[2] = fx * fx;
-            pw[3] = cy * cy; pw[4] = cy * fy; pw[5] = fy * fy;
-            pw[6] = cz * cz; pw[7] = cz * fz; pw[8] = fz * fz;
+            const double px[3] = {cx * cx, cx * fx, fx * fx};
+            const double py[3] = {cy * cy, cy * fy, fy * fy};
+            const double pz[3] = {cz * cz, cz * fz, fz * fz};
+#pragma unroll
+            for (int ty = 0; ty < 3; ++ty)
+#pragma unroll
+              for (int tx = 0; tx < 3; ++tx) {
+                const double pxy = px[tx] * py[ty];
+#pragma unroll
+                for (int tz = 0; tz < 3; ++tz) mt[tx + 3 * ty + 9 * tz] = pxy * pz[tz];
+              }
           }
           if (!ok) {
             ++bad;
 #pragma unroll
             for (int e = 0; e < 12; ++e) src[e] = 0.0;
 #pragma unroll
-            for (int e = 0; e < 9; ++e) pw[e] = 0.0;
+            for (int t = 0; t < 27; ++t) mt[t] = 0.0;
           }
         }
         __syncwarp();
         if (lane < 27) {
           for (uint32_t k = 0; k < m; ++k) {
-            const double mt = (S.pw[k][tx] * S.pw[k][3 + ty]) * S.pw[k][6 + tz];
-            const double* src = S.src[k];
+            const double* mk = S.m[k] + t0;
+            const double* sk = S.src[k] + e0;
+            const double mv[3] = {mk[0], mk[1], mk[2]};
+            const double sv[4] = {sk[0], sk[1], sk[2], sk[3]};
 #pragma unroll
-            for (int e = 0; e < 9; ++e) G[e] += mt * src[e];
+            for (int i = 0; i < 3; ++i)
 #pragma unroll
-            for (int c = 0; c < 3; ++c) H[c] += mt * src[9 + c];
+              for (int e = 0; e < 4; ++e) acc[i][e] += mv[i] * sv[e];
           }
         }
         __syncwarp();
@@ -1563,12 +1579,17 @@ __global__ void __launch_bounds__(kF64Warps * 32) moments_f64_kernel(Geom g, F64
     }
     if (lane < 27) {
 #pragma unroll
-      for (int e = 0; e < 9; ++e) {
-        double* dst = mom + moment_index(cell, lane * 9 + e);
-        *dst = accumulate ? *dst + G[e] : G[e];
-      }
+      for (int i = 0; i < 3; ++i)
 #pragma unroll
-      for (int c = 0; c < 3; ++c) S.hs[lane][c] = H[c];
+        for (int e = 0; e < 4; ++e) {
+          const int t = t0 + i, entry = e0 + e;
+          if (entry < 9) {
+            double* dst = mom + moment_index(cell, t * 9 + entry);
+            *dst = accumulate ? *dst + acc[i][e] : acc[i][e];
+          } else {
+            S.hs[t][entry - 9] = acc[i][e];
+          }
+        }
     }
     __syncwarp();
     if (lane < 24) {
