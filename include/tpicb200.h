@@ -44,9 +44,10 @@
  *                               residuals and solution (refined cycles).
  *
  * Threading: a context is used by one host thread at a time; calls are
- * stream-ordered and not re-entrant. No entry point allocates memory except
- * tpicb200_create. The product fails loudly (TPICB200_BACKEND_FAILURE)
- * without a usable sm_100 device; there is no CPU fallback.
+ * stream-ordered and not re-entrant. No entry point allocates device memory
+ * except tpicb200_create (the checkpoint calls stage through host memory).
+ * The product fails loudly (TPICB200_BACKEND_FAILURE) without a usable
+ * sm_100 device; there is no CPU fallback.
  */
 #ifndef TPICB200_H
 #define TPICB200_H
@@ -469,6 +470,55 @@ int tpicb200_load_species(tpicb200_context* ctx, const tpicb200_deck* deck, int 
  * velocity counts in *invalid. Stream-ordered. */
 int tpicb200_center_velocities(tpicb200_context* ctx, const tpicb200_deck* deck, int s, tpicb200_particles* p,
                                uint32_t* invalid, tpicb200_stream stream);
+
+/* ------------------------------------------------------------------------
+ * Checkpoints and restart (docs/user/output.md "Checkpoints and restart",
+ * src/io/checkpoint.cpp): a checkpoint holds E at the nodes, B at the cells
+ * and every particle record in their stored types, with the cycle number;
+ * everything else is rebuilt at restart by tpicb200_prepare. One piece file
+ * per checkpoint directory `<directory>/checkpoint_tNNNNNN_n000001/
+ * checkpoint_tNNNNNN_r000000.tpcb` (this library's binary format: a header
+ * and the arrays, with an FNV-1a 64-bit checksum of the payload). A piece is
+ * written under a hidden name, flushed and renamed, so a checkpoint is
+ * complete when its piece is listed; writing one removes the older complete
+ * checkpoints of the directory.
+ * ------------------------------------------------------------------------ */
+typedef struct {
+  int version;                    /* format version (1) */
+  int precision;                  /* TPICB200_PRECISION_* of the stored types */
+  int cycle;                      /* cycles completed at the checkpoint */
+  int ns;
+  tpicb200_grid grid;
+  double dt, c;
+  double qom[TPICB200_MAX_SPECIES];
+  uint32_t count[TPICB200_MAX_SPECIES];  /* records per species */
+  int has_id[TPICB200_MAX_SPECIES];      /* ids stored */
+} tpicb200_checkpoint_info;
+
+/* Writes the state (after tpicb200_prepare or a cycle; ranked species are
+ * materialized first) as the checkpoint of `cycle` under `directory`
+ * (created if absent). Host-blocking. TPICB200_BACKEND_FAILURE for a file
+ * system error, with the path in tpicb200_last_error(). */
+int tpicb200_checkpoint_write(tpicb200_context* ctx, tpicb200_state* state, const char* directory, int cycle,
+                              tpicb200_stream stream);
+
+/* The newest complete checkpoint piece under `directory` into path[size]:
+ * TPICB200_SUCCESS, or TPICB200_INVALID_ARGUMENT when there is none (or the
+ * path does not fit). Replaces find_restart_checkpoint (src/io/checkpoint.cpp:362). */
+int tpicb200_checkpoint_find(const char* directory, char* path, size_t size);
+
+/* The header of a checkpoint piece (host only): the sizes a caller needs to
+ * allocate the state it restores into. TPICB200_INVALID_DATA for a file that
+ * is not a complete piece of this format. */
+int tpicb200_checkpoint_info_read(const char* path, tpicb200_checkpoint_info* info);
+
+/* Restores E, B (cells) and the particle records of a piece into the state's
+ * live slots (counts set from the piece), after checking that the run is
+ * the checkpoint's: grid, dt, c, species count, q/m and storage precision
+ * (prepare_restart, src/io/checkpoint.cpp:388-470). The checksum is verified
+ * before anything is written. Then call tpicb200_prepare. Host-blocking. */
+int tpicb200_checkpoint_read(tpicb200_context* ctx, tpicb200_state* state, const char* path,
+                             tpicb200_checkpoint_info* info, tpicb200_stream stream);
 
 #ifdef __cplusplus
 }

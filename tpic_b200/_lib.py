@@ -89,6 +89,12 @@ class Deck(C.Structure):
                 ("two_stream_phase", C.c_double), ("quiet_start", C.c_int), ("ignored_keys", C.c_int)]
 
 
+class CheckpointInfo(C.Structure):
+    _fields_ = [("version", C.c_int), ("precision", C.c_int), ("cycle", C.c_int), ("ns", C.c_int), ("grid", Grid),
+                ("dt", C.c_double), ("c", C.c_double), ("qom", C.c_double * MAX_SPECIES),
+                ("count", C.c_uint32 * MAX_SPECIES), ("has_id", C.c_int * MAX_SPECIES)]
+
+
 EXPORTS = {
     "tpicb200_version": (C.c_char_p, []),
     "tpicb200_last_error": (C.c_char_p, []),
@@ -131,6 +137,11 @@ EXPORTS = {
                                         C.POINTER(Particles), C.c_void_p, C.c_void_p]),
     "tpicb200_center_velocities": (C.c_int, [C.c_void_p, C.POINTER(Deck), C.c_int, C.POINTER(Particles), C.c_void_p,
                                              C.c_void_p]),
+    "tpicb200_checkpoint_write": (C.c_int, [C.c_void_p, C.POINTER(State), C.c_char_p, C.c_int, C.c_void_p]),
+    "tpicb200_checkpoint_find": (C.c_int, [C.c_char_p, C.c_char_p, C.c_size_t]),
+    "tpicb200_checkpoint_info_read": (C.c_int, [C.c_char_p, C.POINTER(CheckpointInfo)]),
+    "tpicb200_checkpoint_read": (C.c_int, [C.c_void_p, C.POINTER(State), C.c_char_p, C.POINTER(CheckpointInfo),
+                                           C.c_void_p]),
 }
 
 _lib = None

@@ -15,6 +15,7 @@ using namespace tpicb200;
 struct tpicb200_context {
   int device = 0;
   Geom g{};
+  tpicb200_grid grid{};
   tpicb200_options opt{};
   SolverWorkspace* solver = nullptr;
   uint32_t* cursor = nullptr;
@@ -168,6 +169,7 @@ int tpicb200_create(const tpicb200_grid* grid, const tpicb200_options* options, 
   auto* ctx = new tpicb200_context();
   ctx->device = device;
   ctx->g = make_geom(*grid);
+  ctx->grid = *grid;
   if (options->mass_layout == TPICB200_MASS_LAYOUT_STENCIL_MAJOR) {
     ctx->g.mvs = 1;
     ctx->g.mes = ctx->g.nodes;
@@ -693,6 +695,20 @@ static int deposit_pair(tpicb200_context* ctx, tpicb200_state* st, int first, in
     if (plan[i].flip) st->current[first + i] = 1 - st->current[first + i];
   return TPICB200_SUCCESS;
 }
+
+}  // extern "C"
+
+namespace tpicb200 {
+const Geom& context_geom(const tpicb200_context* ctx) { return ctx->g; }
+const tpicb200_options& context_options(const tpicb200_context* ctx) { return ctx->opt; }
+const tpicb200_grid& context_grid(const tpicb200_context* ctx) { return ctx->grid; }
+int context_check_state(tpicb200_context* ctx, tpicb200_state* st) {
+  if (int s = check_ctx(ctx)) return s;
+  return check_state(ctx, st);
+}
+}  // namespace tpicb200
+
+extern "C" {
 
 int tpicb200_materialize(tpicb200_context* ctx, tpicb200_state* st, tpicb200_stream stream) {
   if (int s = check_ctx(ctx)) return s;

@@ -17,6 +17,13 @@ void uncount_launches(unsigned long long n);
 // Records the message tpicb200_last_error() returns on this thread; returns status.
 int report_error(int status, const std::string& message);
 
+// abi.cu: the context's geometry, options and state checks, for the
+// host-side entry points of other files.
+const Geom& context_geom(const tpicb200_context* ctx);
+const tpicb200_options& context_options(const tpicb200_context* ctx);
+const tpicb200_grid& context_grid(const tpicb200_context* ctx);
+int context_check_state(tpicb200_context* ctx, tpicb200_state* st);
+
 // mover.cu
 struct BinnedScratch;
 // Species scalars accumulated by the movers (kinetic energy, charge,

@@ -42,7 +42,8 @@ def _ptr(t) -> int:
 class Simulation:
     def __init__(self, case: Case, precision: str = "double", mass_kind: str = "scalar",
                  device: int = 0, gmres_restart: int = 30, gmres_max_iterations: int = 100,
-                 keep_ids: bool = False, generate_on_device: bool = False, mass_layout: str = "stencil-major"):
+                 keep_ids: bool = False, generate_on_device: bool = False, mass_layout: str = "stencil-major",
+                 generate: bool = True):
         self.case = case
         self.lib = _lib.load()
         self.precision = _lib.PRECISIONS[precision]
@@ -99,7 +100,9 @@ class Simulation:
                               ("cell", torch.int32))})
                 if keep_ids:
                     slot[-1]["id"] = torch.empty(n, dtype=torch.int64, device=dev)
-            if generate_on_device:
+            if not generate:
+                pass  # the records come from a checkpoint (Simulation.restart)
+            elif generate_on_device:
                 self._load_on_device(deck_of(case), s, sp, slot[0], n)
             else:
                 vdt_np = np.float64 if self.precision == _lib.PRECISION_DOUBLE else np.float32
@@ -130,6 +133,7 @@ class Simulation:
         self.state = st
         self.reports: list[Report] = []
         self.prepared = False
+        self.cycle = 0  # cycles completed (restored from a checkpoint by restart)
 
     def _load_on_device(self, deck, s: int, sp, slot: dict, n: int) -> None:
         """Species s loaded (and centred) by the library's device loader."""
@@ -174,6 +178,7 @@ class Simulation:
             self.prepare()
         reports = (_lib.CycleReport * max(ncycles, 1))()
         _lib.check(self.lib.tpicb200_cycle(self.ctx, C.byref(self.state), ncycles, reports, self._stream()))
+        self.cycle += ncycles
         out = []
         ns = self.state.ns
         for r in reports[:ncycles]:
@@ -182,6 +187,35 @@ class Simulation:
                               r.gmres.host_waits))
         self.reports.extend(out)
         return out
+
+    def checkpoint(self, directory) -> str:
+        """Writes the checkpoint of the current cycle under `directory`
+        (E, B and every record; older checkpoints there are removed) and
+        returns the piece's path."""
+        if not self.prepared:
+            self.prepare()
+        _lib.check(self.lib.tpicb200_checkpoint_write(self.ctx, C.byref(self.state), str(directory).encode(),
+                                                      self.cycle, self._stream()))
+        return find_checkpoint(directory)
+
+    @classmethod
+    def restart(cls, case: Case, directory, **kwargs) -> "Simulation":
+        """The run continued from the newest complete checkpoint under
+        `directory`: the case's grid, dt, c, species and storage precision
+        must be the checkpoint's; E, B and the records come from it and
+        everything else is rebuilt (tpicb200_prepare)."""
+        path = find_checkpoint(directory)
+        info = checkpoint_info(path)
+        sim = cls(case, generate=False, **kwargs)
+        for s in range(info.ns):
+            if info.count[s] != sim.state.slot[s][0].count:
+                raise ValueError(f"species {s}: the checkpoint holds {info.count[s]} records, the case "
+                                 f"{sim.state.slot[s][0].count}")
+        _lib.check(sim.lib.tpicb200_checkpoint_read(sim.ctx, C.byref(sim.state), path.encode(), C.byref(info),
+                                                    sim._stream()))
+        sim.cycle = info.cycle
+        sim.prepare()
+        return sim
 
     def energy(self) -> np.ndarray:
         ns = self.state.ns
@@ -214,3 +248,16 @@ class Simulation:
             self.close()
         except Exception:
             pass
+
+
+def find_checkpoint(directory) -> str:
+    """The newest complete checkpoint piece under `directory`."""
+    buf = C.create_string_buffer(4096)
+    _lib.check(_lib.load().tpicb200_checkpoint_find(str(directory).encode(), buf, len(buf)))
+    return buf.value.decode()
+
+
+def checkpoint_info(path) -> _lib.CheckpointInfo:
+    info = _lib.CheckpointInfo()
+    _lib.check(_lib.load().tpicb200_checkpoint_info_read(str(path).encode(), C.byref(info)))
+    return info
