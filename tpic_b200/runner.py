@@ -1,0 +1,167 @@
+"""Deck runner: `python -m tpic_b200 --run deck.inp --mass-matrix ...`.
+
+Runs a TPIC input deck through the library the way TPIC's driver runs a
+one-rank periodic case (src/main.cpp `--run`, `--mass-matrix`, `--restart`):
+the deck's case and species, `ncycles` cycles, the energy diagnostics rows of
+TPIC's `diagnostics.csv` (docs/user/output.md, "diagnostics.csv": cycle, time,
+state, electric, magnetic, kinetic and total energy, the change of the total
+energy from the run's first state, charge and momentum, then per species
+kinetic energy, charge and momentum) every `DiagnosticsOutputCycle` cycles and
+at the final state, and checkpoints every `RestartOutputCycle` cycles under
+`RestartDirName`. `--restart` continues from the newest complete checkpoint,
+and the diagnostics file continues after a `# restart at cycle N` line.
+"""
+from __future__ import annotations
+
+import argparse
+import math
+import sys
+from pathlib import Path
+
+from . import deck as D
+
+FORMS = ("scalar", "scalar-f64", "tf32", "bf16x3", "moments-f64", "matrix-core")
+
+HEADER = (
+    "# electric_energy = V/(8 pi) sum over unique nodes |E|^2; magnetic_energy = V/(8 pi) sum over cells |B|^2;\n"
+    "# kinetic_energy = sum 1/2 (q/qom) |v|^2; momentum = sum (q/qom) v; charge = sum q.\n"
+    "# state=pre_solve identifies the state before the cycle's solve/push; state=final identifies the completed "
+    "run state.\n"
+    "# time is physical simulation time at the recorded state; total_energy_change = total_energy - the total "
+    "energy of the run's first state, kept across restarts (absolute units).\n")
+
+
+def columns(ns: int) -> str:
+    cols = ["cycle", "time", "state", "electric_energy", "magnetic_energy", "kinetic_energy", "total_energy",
+            "total_energy_change", "charge", "momentum_x", "momentum_y", "momentum_z"]
+    for s in range(ns):
+        cols += [f"kinetic_energy_{s}", f"charge_{s}", f"momentum_x_{s}", f"momentum_y_{s}", f"momentum_z_{s}"]
+    return ",".join(cols)
+
+
+def row(cycle: int, dt: float, final: bool, field: tuple, species: tuple, initial_total: float) -> str:
+    """One diagnostics.csv row from the field energies (E, B) and the species
+    scalars (kinetic, charge, momentum x, y, z per species)."""
+    kinetic = sum(sp[0] for sp in species)
+    total = field[0] + field[1] + kinetic
+    sums = [sum(sp[k] for sp in species) for k in range(1, 5)]
+    values = [field[0], field[1], kinetic, total, total - initial_total, *sums]
+    for sp in species:
+        values += list(sp)
+    return ",".join([str(cycle), repr(cycle * dt), "final" if final else "pre_solve"] + [repr(float(v)) for v in values])
+
+
+def first_total(csv_path: Path) -> float | None:
+    """The total energy of the first row of an existing diagnostics file."""
+    if not csv_path.exists():
+        return None
+    for line in csv_path.read_text().splitlines():
+        if line and line[0].isdigit():
+            fields = line.split(",")
+            return float(fields[6])
+    return None
+
+
+def resolve_form(form: str, precision: str) -> str:
+    """TPIC's `--mass-matrix matrix-core` is its tensor-core form: here BF16x3
+    in mixed precision and the FP64 moment form in double precision."""
+    if form == "matrix-core":
+        return "moments-f64" if precision == "double" else "bf16x3"
+    return form
+
+
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser(prog="python -m tpic_b200", description="Run a TPIC input deck on one B200.")
+    ap.add_argument("--run", required=True, metavar="DECK", help="TPIC input deck (.inp)")
+    ap.add_argument("--mass-matrix", default="matrix-core", choices=FORMS)
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "double"])
+    ap.add_argument("--restart", action="store_true", help="continue from the newest complete checkpoint")
+    ap.add_argument("--output", default=".", help="directory of diagnostics.csv and RestartDirName")
+    ap.add_argument("--cycles", type=int, default=None, help="last cycle of the run (default: the deck's ncycles)")
+    ap.add_argument("--diagnostics-cycle", type=int, default=1, help="DiagnosticsOutputCycle (<= 0: final row only)")
+    ap.add_argument("--restart-cycle", type=int, default=0, help="RestartOutputCycle (<= 0: no checkpoints)")
+    ap.add_argument("--restart-dir", default="data", help="RestartDirName, under --output")
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--gmres-max-iterations", type=int, default=100)
+    ap.add_argument("--device", type=int, default=0)
+    return ap.parse_args(argv)
+
+
+def run(args) -> int:
+    from .simulation import Simulation
+    deck = D.load(args.run)
+    case = D.to_case(deck, seed=args.seed)
+    last = deck.ncycles if args.cycles is None else args.cycles
+    form = resolve_form(args.mass_matrix, args.precision)
+    out = Path(args.output)
+    out.mkdir(parents=True, exist_ok=True)
+    ckpt_dir = out / args.restart_dir
+    csv_path = out / "diagnostics.csv"
+    kw = dict(precision=args.precision, mass_kind=form, device=args.device,
+              gmres_max_iterations=args.gmres_max_iterations)
+    ns = len(case.species)
+    if args.restart:
+        sim = Simulation.restart(case, ckpt_dir, **kw)
+        initial = first_total(csv_path)
+        # The restarted run replaces the rows from its checkpoint cycle on.
+        kept = []
+        if csv_path.exists():
+            for line in csv_path.read_text().splitlines():
+                if line and line[0].isdigit() and int(line.split(",")[0]) >= sim.cycle:
+                    continue
+                kept.append(line)
+        else:
+            kept = (HEADER + columns(ns)).splitlines()
+        kept.append(f"# restart at cycle {sim.cycle}")
+        csv_path.write_text("\n".join(kept) + "\n")
+    else:
+        sim = Simulation(case, generate_on_device=True, **kw)
+        sim.prepare()
+        initial = None
+        with open(csv_path, "w") as f:
+            f.write(HEADER + columns(ns) + "\n")
+    if last < sim.cycle:
+        raise SystemExit(f"the run's last cycle {last} lies before the checkpoint cycle {sim.cycle}")
+    w = sim.energy()
+    field = (w[0], w[1])
+    species = tuple(tuple(w[2 + 5 * s:7 + 5 * s]) for s in range(ns))
+    if initial is None:
+        initial = field[0] + field[1] + sum(sp[0] for sp in species)
+    cadence = args.diagnostics_cycle if args.diagnostics_cycle > 0 else 0
+    ckpt = args.restart_cycle if args.restart_cycle > 0 else 0
+
+    def record(final: bool) -> None:
+        line = row(sim.cycle, case.dt, final, field, species, initial)
+        with open(csv_path, "a") as f:
+            f.write(line + "\n")
+        total = field[0] + field[1] + sum(sp[0] for sp in species)
+        print(f"cycle {sim.cycle:6d}  total energy {total:.10e}  change {total - initial:+.3e}", flush=True)
+
+    if (cadence and sim.cycle % cadence == 0) or sim.cycle == last:
+        record(sim.cycle == last)
+    while sim.cycle < last:
+        stops = [last]
+        if cadence:
+            stops.append((sim.cycle // cadence + 1) * cadence)
+        if ckpt:
+            stops.append((sim.cycle // ckpt + 1) * ckpt)
+        n = min(stops) - sim.cycle
+        reports = sim.run(n)
+        r = reports[-1]
+        field, species = tuple(r.field_energy), r.species_scalars
+        if ckpt and (sim.cycle % ckpt == 0 or sim.cycle == last):
+            sim.checkpoint(ckpt_dir)
+        if sim.cycle == last or (cadence and sim.cycle % cadence == 0):
+            record(sim.cycle == last)
+        if not all(math.isfinite(x) for x in field):
+            raise SystemExit("nonfinite field energy")
+    sim.close()
+    return 0
+
+
+def main(argv=None) -> int:
+    return run(parse_args(argv))
+
+
+if __name__ == "__main__":
+    sys.exit(main())

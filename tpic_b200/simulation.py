@@ -33,6 +33,7 @@ class Report:
     total_energy: float
     stage_ms: tuple
     gmres_host_waits: int = 0
+    species_scalars: tuple = ()  # per species: kinetic energy, charge, momentum x, y, z
 
 
 def _ptr(t) -> int:
@@ -184,7 +185,7 @@ class Simulation:
         for r in reports[:ncycles]:
             out.append(Report(r.gmres.iterations, r.gmres.relative_residual, tuple(r.field_energy),
                               tuple(r.species[s][0] for s in range(ns)), r.total_energy, tuple(r.stage_ms),
-                              r.gmres.host_waits))
+                              r.gmres.host_waits, tuple(tuple(r.species[s][:5]) for s in range(ns))))
         self.reports.extend(out)
         return out
 
