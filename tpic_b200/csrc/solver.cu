@@ -107,8 +107,11 @@ __device__ __forceinline__ void mass_product(const Geom& g, const M* __restrict_
   out[0] = x; out[1] = y; out[2] = z;
 }
 
-// Tile of unique nodes per CTA: 32 (x) x 4 (y) x 2 (z) = 256 threads.
+// Tile of unique nodes per CTA, 256 threads: 32 (x) x 4 (y) x 2 (z), or
+// 32 x 8 x 1 on grids of one cell along z, where a second z layer would hold
+// no node (when that leaves enough CTAs to fill the GPU).
 constexpr int kTX = 32, kTY = 4, kTZ = 2;
+constexpr int kThinTY = 8;
 
 // A(v) over the unique nodes [0,n)^3 of a tile. The input (ghosts filled) is
 // staged in shared memory with its one-node halo, each cell curl the tile
@@ -116,19 +119,19 @@ constexpr int kTX = 32, kTY = 4, kTZ = 2;
 // node's C2N curl, 27-block mass product and combination. Rows of the
 // duplicate endpoint planes equal their unique node's row (same inputs, same
 // operations) and are copied by duplicate_rows_kernel.
-template <class C, class M, class Out>
-__global__ void __launch_bounds__(kTX * kTY * kTZ) maxwell_apply_kernel(Geom g, C d2, C kfac, C inv_volume,
+template <class C, class M, class Out, int TX, int TY, int TZ>
+__global__ void __launch_bounds__(TX * TY * TZ) maxwell_apply_kernel(Geom g, C d2, C kfac, C inv_volume,
                                                                         const M* __restrict__ mass,
                                                                         const double* __restrict__ v,
                                                                         Out* __restrict__ out) {
-  constexpr int VX = kTX + 2, VY = kTY + 2, VZ = kTZ + 2;   // nodes i0-1 .. i0+TX
-  constexpr int CX = kTX + 1, CY = kTY + 1, CZ = kTZ + 1;   // cells i0-1 .. i0+TX-1
+  constexpr int VX = TX + 2, VY = TY + 2, VZ = TZ + 2;   // nodes i0-1 .. i0+TX
+  constexpr int CX = TX + 1, CY = TY + 1, CZ = TZ + 1;   // cells i0-1 .. i0+TX-1
   __shared__ C vs[3][VZ][VY][VX];
   __shared__ C cs[3][CZ][CY][CX];
   const C inv[3] = {C(g.inv[0]), C(g.inv[1]), C(g.inv[2])};
-  const int tiles_x = (g.nx + kTX - 1) / kTX, tiles_y = (g.ny + kTY - 1) / kTY;
+  const int tiles_x = (g.nx + TX - 1) / TX, tiles_y = (g.ny + TY - 1) / TY;
   const int tx = blockIdx.x % tiles_x, ty = (blockIdx.x / tiles_x) % tiles_y, tz = blockIdx.x / (tiles_x * tiles_y);
-  const int i0 = tx * kTX, j0 = ty * kTY, k0 = tz * kTZ;
+  const int i0 = tx * TX, j0 = ty * TY, k0 = tz * TZ;
   const long long nn = g.nodes;
   // Stage v over nodes [i0-1, i0+TX] x [j0-1, j0+TY] x [k0-1, k0+TZ]; nodes
   // beyond n+1 (partial tiles) are never read by a live node and load 0.
@@ -163,7 +166,7 @@ __global__ void __launch_bounds__(kTX * kTY * kTZ) maxwell_apply_kernel(Geom g, 
     cs[2][lz][ly][lx] = C(double(dx(q[1]) - dy(q[0])));
   }
   __syncthreads();
-  const int lx = threadIdx.x % kTX, ly = (threadIdx.x / kTX) % kTY, lz = threadIdx.x / (kTX * kTY);
+  const int lx = threadIdx.x % TX, ly = (threadIdx.x / TX) % TY, lz = threadIdx.x / (TX * TY);
   const int i = i0 + lx, j = j0 + ly, k = k0 + lz;
   if (i >= g.nx || j >= g.ny || k >= g.nz) return;
   // C2N curl of the cell curls (cell sources: anchor - neighbour); the cell
@@ -649,9 +652,18 @@ struct Solve {
     const Geom& g = w->g;
     launch_node_ghosts(g, w->input, 3, st);
     const double iv = g.inv_volume;
-    const unsigned tiles = unsigned(((g.nx + kTX - 1) / kTX) * ((g.ny + kTY - 1) / kTY) * ((g.nz + kTZ - 1) / kTZ));
-    maxwell_apply_kernel<C, Mass, Out><<<tiles, kTX * kTY * kTZ, 0, st>>>(
-        g, C(w->delta * w->delta), C(w->kfac), C(iv), mass, w->input, out);
+    // The thin tile where it still gives two CTAs per SM (148 SMs).
+    const long long thin_tiles = (long long)((g.nx + kTX - 1) / kTX) * ((g.ny + kThinTY - 1) / kThinTY);
+    if (g.nz == 1 && thin_tiles >= 2 * 148) {
+      const unsigned tiles = unsigned(thin_tiles);
+      maxwell_apply_kernel<C, Mass, Out, kTX, kThinTY, 1><<<tiles, kTX * kThinTY, 0, st>>>(
+          g, C(w->delta * w->delta), C(w->kfac), C(iv), mass, w->input, out);
+    } else {
+      const unsigned tiles =
+          unsigned(((g.nx + kTX - 1) / kTX) * ((g.ny + kTY - 1) / kTY) * ((g.nz + kTZ - 1) / kTZ));
+      maxwell_apply_kernel<C, Mass, Out, kTX, kTY, kTZ><<<tiles, kTX * kTY * kTZ, 0, st>>>(
+          g, C(w->delta * w->delta), C(w->kfac), C(iv), mass, w->input, out);
+    }
     const long long dup = (long long)g.inx * g.iny + (long long)g.inx * g.nz + (long long)g.ny * g.nz;
     duplicate_rows_kernel<Out><<<grid_for(3 * dup, kThreads), kThreads, 0, st>>>(g, out);
     count_launches(2);
