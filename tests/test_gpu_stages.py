@@ -15,6 +15,7 @@ import numpy as np
 import pytest
 
 import oracle as O
+from tpic_b200 import _lib
 from fieldutil import (bits, interior_nodes, interior_records, periodic_cell_field, periodic_node_field,
                        smooth_random_unique)
 from reference_fixtures import (host_matrix_core_mass, mover_edge_records, ogrid, oracle_moments, oracle_mover,
@@ -244,6 +245,63 @@ def test_field_solve_matches_oracle(torch_cuda, layout):
     assert res.iterations == ores.iterations
     got, want = interior_nodes(g, et.cpu().numpy()), interior_nodes(g, oc.theta_field)
     assert np.abs(got - want).max() <= 3e-10 * np.abs(want).max() + 3e-12
+
+
+def test_gmres_iteration_limit_commits_nothing(torch_cuda):
+    """gmres_device.cpp:220-222: a solve stopped by the iteration limit reports
+    it and leaves the solution field untouched."""
+    g = GRID
+    oc = prepared_oracle(g, 0)
+    rng = np.random.default_rng(4)
+    e = periodic_node_field(g, smooth_random_unique(g, rng, 0.01))
+    bcell = periodic_cell_field(g, smooth_random_unique(g, rng, 0.05))
+    import torch
+    ctx = make_ctx(g, 0, dt=0.2, tol=1e-14, max_iterations=1)
+    et = torch.full((3 * ctx.layout.node_count,), 7.0, dtype=torch.float64, device="cuda")
+    res = _lib.GmresResult()
+    status = ctx.lib.tpicb200_field_solve(ctx.ctx, ctx.field(e).data_ptr(), ctx.field(bcell).data_ptr(),
+                                          ctx.field(oc.j).data_ptr(), ctx.mass_from_records(oc.m).data_ptr(),
+                                          et.data_ptr(), C.byref(res), ctx.stream)
+    assert status == _lib.NOT_CONVERGED
+    assert not res.converged and res.iterations == 1
+    assert bool((et == 7.0).all())
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_gmres_short_restarts_converge(torch_cuda, precision):
+    """gmres_device.cpp:223-235: restart length 2, several restart cycles to
+    1e-10 (the mixed mode through its refined cycles), the solution equal to
+    the oracle's GMRES(2) solution; one host wait per restart cycle plus one."""
+    g = GRID
+    oc = prepared_oracle(g, precision)
+    rng = np.random.default_rng(6)
+    oc.e = periodic_node_field(g, smooth_random_unique(g, rng, 0.01))
+    bcell = periodic_cell_field(g, smooth_random_unique(g, rng, 0.05))
+    oc.b = bcell
+    oc.restart = 2
+    ctx = make_ctx(g, precision, dt=0.2, tol=1e-10, restart=2)
+    mass = ctx.mass_from_records(oc.m.astype(ctx.np_fdt).astype(np.float64))
+    et, res = ctx.field_solve(ctx.field(oc.e), ctx.field(bcell), ctx.field(oc.j), mass)
+    assert res.converged and res.iterations > 2 and res.relative_residual <= 1e-10
+    assert res.host_waits == 1 + (res.iterations + 1) // 2 or precision == 1
+    if precision == 0:
+        ores = oc.solve()
+        assert res.iterations == ores.iterations
+        got, want = interior_nodes(g, et.cpu().numpy()), interior_nodes(g, oc.theta_field)
+        assert np.abs(got - want).max() <= 3e-10 * np.abs(want).max() + 3e-12
+
+
+def test_gmres_zero_rhs(torch_cuda):
+    """gmres_device.cpp:243-248: a zero right-hand side (no field, current or
+    mass) converges at once with a zero solution."""
+    g = GRID
+    ctx = make_ctx(g, 0, dt=0.2, tol=1e-10)
+    nodes, cells = ctx.layout.node_count, ctx.layout.cell_count
+    zero_nodes = np.zeros(3 * nodes)
+    et, res = ctx.field_solve(ctx.field(zero_nodes), ctx.field(np.zeros(3 * cells)), ctx.field(zero_nodes),
+                              ctx.mass_from_records(np.zeros(126 * nodes)))
+    assert res.converged and res.iterations == 0 and res.rhs_norm == 0.0 and res.host_waits == 1
+    assert float(et.abs().max()) == 0.0
 
 
 @pytest.mark.parametrize("precision", [0, 1])
