@@ -213,6 +213,30 @@ __device__ __forceinline__ void prefetch_l2(const void* p) {
   asm volatile("prefetch.global.L2 [%0];" :: "l"(p));
 }
 
+// Programmatic dependent launch: a kernel launched with programmatic stream
+// serialization may be scheduled while its predecessor drains; it waits here
+// for the predecessor's completion and memory before touching its results.
+// Without that launch attribute the wait returns at once.
+__device__ __forceinline__ void wait_for_predecessor() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+// Launches `kernel` so that it may overlap the tail of the previous kernel
+// on the stream (it must call wait_for_predecessor() first).
+template <class... Params, class... Args>
+inline cudaError_t launch_programmatic(void (*kernel)(Params...), dim3 grid, dim3 block, size_t smem,
+                                       cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t config{};
+  config.gridDim = grid;
+  config.blockDim = block;
+  config.dynamicSmemBytes = smem;
+  config.stream = s;
+  cudaLaunchAttribute attribute[1];
+  attribute[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attribute[0].val.programmaticStreamSerializationAllowed = 1;
+  config.attrs = attribute;
+  config.numAttrs = 1;
+  return cudaLaunchKernelEx(&config, kernel, args...);
+}
+
 // shell_coordinates in 32-bit arithmetic (t < shell_count < 2^31).
 __device__ __forceinline__ void shell_coordinates32(const Geom& g, uint32_t t, int& i, int& j, int& k) {
   const uint32_t NX = uint32_t(g.NX), zs = NX * uint32_t(g.NY), ys = NX * uint32_t(g.nz),

@@ -66,6 +66,7 @@ __device__ __forceinline__ void interior_node_coordinates(const Geom& g, long lo
 
 template <class T>
 __global__ void __launch_bounds__(256) node_fill_kernel(Geom g, T* __restrict__ f, int components) {
+  wait_for_predecessor();
   const long long shell = shell_count(g), total = shell * components;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
@@ -244,6 +245,7 @@ __global__ void __launch_bounds__(256) species_kernel(const Vel* __restrict__ u,
 // device/block_reduction_device.hpp:23-44).
 __global__ void __launch_bounds__(256) reduce_rows_kernel(const double* __restrict__ partials, double* out,
                                                           int row_stride, int count, int filled) {
+  wait_for_predecessor();
   __shared__ double scratch[8];
   const int row = blockIdx.x;
   if (row >= filled) {
@@ -266,9 +268,11 @@ __global__ void __launch_bounds__(256) copy_node_kernel(long long total, const T
 
 }  // namespace
 
-cudaError_t launch_node_ghosts(const Geom& g, double* f, int components, cudaStream_t s) {
-  node_fill_kernel<double><<<grid_for(shell_count(g) * components, 256), 256, 0, s>>>(g, f, components);
+cudaError_t launch_node_ghosts(const Geom& g, double* f, int components, cudaStream_t s, bool programmatic) {
+  const unsigned blocks = grid_for(shell_count(g) * components, 256);
   count_launches(1);
+  if (programmatic) return launch_programmatic(node_fill_kernel<double>, blocks, 256, 0, s, g, f, components);
+  node_fill_kernel<double><<<blocks, 256, 0, s>>>(g, f, components);
   return cudaGetLastError();
 }
 
@@ -352,9 +356,12 @@ cudaError_t launch_species_scalars(int precision, const tpicb200_particles* p, d
 }
 
 cudaError_t launch_reduce_rows(const double* partials, double* out, int rows, int row_stride, int count,
-                               int filled, cudaStream_t s) {
-  reduce_rows_kernel<<<rows, 256, 0, s>>>(partials, out, row_stride, count, filled);
+                               int filled, cudaStream_t s, bool programmatic) {
   count_launches(1);
+  if (programmatic)
+    return launch_programmatic(reduce_rows_kernel, unsigned(rows), 256, 0, s, partials, out, row_stride, count,
+                               filled);
+  reduce_rows_kernel<<<rows, 256, 0, s>>>(partials, out, row_stride, count, filled);
   return cudaGetLastError();
 }
 

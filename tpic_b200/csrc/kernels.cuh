@@ -143,7 +143,8 @@ cudaError_t launch_assemble_moments(int precision, const Geom& g, const void* mo
                                     int overwrite, cudaStream_t s);
 
 // fields.cu
-cudaError_t launch_node_ghosts(const Geom& g, double* f, int components, cudaStream_t s);
+cudaError_t launch_node_ghosts(const Geom& g, double* f, int components, cudaStream_t s,
+                               bool programmatic = false);
 cudaError_t launch_cell_ghosts(int precision, const Geom& g, void* f, cudaStream_t s);
 cudaError_t launch_cell_to_node(int precision, const Geom& g, const void* cellf, void* node,
                                 cudaStream_t s);
@@ -156,8 +157,10 @@ cudaError_t launch_field_energy(int precision, const Geom& g, const void* e, con
                                 double* partials, int blocks, cudaStream_t s);
 cudaError_t launch_species_scalars(int precision, const tpicb200_particles* p, double qom,
                                    double* partials, int blocks, cudaStream_t s);
+// `programmatic`: launched with programmatic stream serialization (the
+// kernels wait for their predecessor before reading).
 cudaError_t launch_reduce_rows(const double* partials, double* out, int rows, int row_stride,
-                               int count, int filled, cudaStream_t s);
+                               int count, int filled, cudaStream_t s, bool programmatic = false);
 cudaError_t launch_copy_node_field(const Geom& g, const void* in, int in_double, double* out,
                                    cudaStream_t s);
 

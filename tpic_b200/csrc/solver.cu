@@ -124,6 +124,7 @@ __global__ void __launch_bounds__(TX * TY * TZ) maxwell_apply_kernel(Geom g, C d
                                                                         const M* __restrict__ mass,
                                                                         const double* __restrict__ v,
                                                                         Out* __restrict__ out) {
+  wait_for_predecessor();
   constexpr int VX = TX + 2, VY = TY + 2, VZ = TZ + 2;   // nodes i0-1 .. i0+TX
   constexpr int CX = TX + 1, CY = TY + 1, CZ = TZ + 1;   // cells i0-1 .. i0+TX-1
   __shared__ C vs[3][VZ][VY][VX];
@@ -235,6 +236,7 @@ __global__ void __launch_bounds__(TX * TY * TZ) maxwell_apply_kernel(Geom g, C d
 // of their periodic unique node.
 template <class Out>
 __global__ void __launch_bounds__(kThreads) duplicate_rows_kernel(Geom g, Out* __restrict__ out) {
+  wait_for_predecessor();
   // Compact rows with i == n, or j == n, or k == n: three slabs as in shell_coordinates.
   const uint32_t zs = uint32_t(g.inx) * g.iny, ys = uint32_t(g.inx) * g.nz, xs = uint32_t(g.ny) * g.nz;
   const uint32_t total = zs + ys + xs;
@@ -308,6 +310,7 @@ template <class S>
 __global__ void __launch_bounds__(kThreads) dot_batch_kernel(const S* __restrict__ basis, const S* __restrict__ image,
                                                              double* __restrict__ partials, long long count,
                                                              const ArnoldiControl* __restrict__ ctl) {
+  wait_for_predecessor();
   __shared__ double scratch[kDotTile][kThreads / 32];
   const int columns = ctl->col + 1;
   for (int first = blockIdx.y * kDotTile; first < columns; first += gridDim.y * kDotTile) {
@@ -361,6 +364,7 @@ __global__ void __launch_bounds__(kThreads) orthogonalize_kernel(const S* __rest
                                                                  S* __restrict__ image, double* __restrict__ hessenberg,
                                                                  int leading, double* __restrict__ partials,
                                                                  long long count, const ArnoldiControl* __restrict__ ctl) {
+  wait_for_predecessor();
   __shared__ double scratch[kThreads / 32];
   const int columns = ctl->col + 1;
   double* column = hessenberg + (long long)ctl->col * leading;
@@ -429,6 +433,7 @@ __global__ void __launch_bounds__(kThreads) normalize_kernel(Geom g, const Src* 
                                                              const double* __restrict__ norm2, S* __restrict__ target,
                                                              long long stride, double* __restrict__ input,
                                                              ArnoldiTail tail, const ArnoldiControl* __restrict__ ctl) {
+  wait_for_predecessor();
   if (ctl) {
     tail.step = ctl->col;
     target += (long long)(tail.step + 1) * stride;
@@ -481,6 +486,7 @@ __global__ void __launch_bounds__(kThreads) update_solution_kernel(const S* __re
 // Sums of the dot partials of the step's columns (rows [0, ctl->col]).
 __global__ void __launch_bounds__(256) reduce_columns_kernel(const double* __restrict__ partials, double* out,
                                                              int row_stride, const ArnoldiControl* __restrict__ ctl) {
+  wait_for_predecessor();
   __shared__ double scratch[8];
   const int row = blockIdx.x;
   if (row > ctl->col) return;
@@ -516,6 +522,7 @@ __global__ void arnoldi_begin_kernel(ArnoldiControl* ctl, int columns, double to
 // while the cycle runs and is cleared at the latest after ctl->columns steps.
 __global__ void arnoldi_end_kernel(ArnoldiControl* ctl, const double* status, cudaGraphConditionalHandle handle,
                                    int conditional) {
+  wait_for_predecessor();
   const int col = ctl->col;
   const double estimate = status[0], breakdown = status[1];
   const bool finite = isfinite(estimate) && isfinite(breakdown);
@@ -648,24 +655,27 @@ struct Solve {
   unsigned blocks() const { return grid_for(w->g.interior, kThreads); }
   void check() { if (err == cudaSuccess) err = cudaGetLastError(); }
 
+  // The step's kernels are launched with programmatic stream serialization:
+  // each may be scheduled while its predecessor drains and waits for it
+  // (wait_for_predecessor) before reading its results.
   template <class C, class Out> void apply(const Mass* mass, Out* out, cudaStream_t st) {
     const Geom& g = w->g;
-    launch_node_ghosts(g, w->input, 3, st);
+    launch_node_ghosts(g, w->input, 3, st, true);
     const double iv = g.inv_volume;
     // The thin tile where it still gives two CTAs per SM (148 SMs).
     const long long thin_tiles = (long long)((g.nx + kTX - 1) / kTX) * ((g.ny + kThinTY - 1) / kThinTY);
     if (g.nz == 1 && thin_tiles >= 2 * 148) {
       const unsigned tiles = unsigned(thin_tiles);
-      maxwell_apply_kernel<C, Mass, Out, kTX, kThinTY, 1><<<tiles, kTX * kThinTY, 0, st>>>(
-          g, C(w->delta * w->delta), C(w->kfac), C(iv), mass, w->input, out);
+      launch_programmatic(maxwell_apply_kernel<C, Mass, Out, kTX, kThinTY, 1>, tiles, kTX * kThinTY, 0, st, g,
+                          C(w->delta * w->delta), C(w->kfac), C(iv), mass, (const double*)w->input, out);
     } else {
       const unsigned tiles =
           unsigned(((g.nx + kTX - 1) / kTX) * ((g.ny + kTY - 1) / kTY) * ((g.nz + kTZ - 1) / kTZ));
-      maxwell_apply_kernel<C, Mass, Out, kTX, kTY, kTZ><<<tiles, kTX * kTY * kTZ, 0, st>>>(
-          g, C(w->delta * w->delta), C(w->kfac), C(iv), mass, w->input, out);
+      launch_programmatic(maxwell_apply_kernel<C, Mass, Out, kTX, kTY, kTZ>, tiles, kTX * kTY * kTZ, 0, st, g,
+                          C(w->delta * w->delta), C(w->kfac), C(iv), mass, (const double*)w->input, out);
     }
     const long long dup = (long long)g.inx * g.iny + (long long)g.inx * g.nz + (long long)g.ny * g.nz;
-    duplicate_rows_kernel<Out><<<grid_for(3 * dup, kThreads), kThreads, 0, st>>>(g, out);
+    launch_programmatic(duplicate_rows_kernel<Out>, grid_for(3 * dup, kThreads), kThreads, 0, st, g, out);
     count_launches(2);
     check();
   }
@@ -706,15 +716,19 @@ struct Solve {
     S* basis = w->template basis_col<S>(0);
     apply<S, S>(mass, image, st);
     const dim3 grid(w->rblocks, (m + kDotTile - 1) / kDotTile);
-    dot_batch_kernel<S><<<grid, kThreads, 0, st>>>(basis, image, w->partials, N, w->ctl);
-    reduce_columns_kernel<<<m, 256, 0, st>>>(w->partials, w->values, int(w->rblocks), w->ctl);
-    orthogonalize_kernel<S><<<w->rblocks, kThreads, 0, st>>>(basis, w->values, image, w->hessenberg(), m + 1,
-                                                             w->partials, N, w->ctl);
-    launch_reduce_rows(w->partials, w->values, w->batch, w->rblocks, w->rblocks, 1, st);
-    normalize_kernel<S, S><<<w->rblocks, kThreads, 0, st>>>(
-        g, image, w->values, basis, N, w->input,
-        ArnoldiTail{w->hessenberg(), w->cosine(), w->sine(), w->ls_rhs(), w->status(), 0, m + 1}, w->ctl);
-    arnoldi_end_kernel<<<1, 1, 0, st>>>(w->ctl, w->status(), handle, conditional);
+    launch_programmatic(dot_batch_kernel<S>, grid, kThreads, 0, st, (const S*)basis, (const S*)image, w->partials, N,
+                        (const ArnoldiControl*)w->ctl);
+    launch_programmatic(reduce_columns_kernel, unsigned(m), 256, 0, st, (const double*)w->partials, w->values,
+                        int(w->rblocks), (const ArnoldiControl*)w->ctl);
+    launch_programmatic(orthogonalize_kernel<S>, w->rblocks, kThreads, 0, st, (const S*)basis,
+                        (const double*)w->values, image, w->hessenberg(), m + 1, w->partials, N,
+                        (const ArnoldiControl*)w->ctl);
+    launch_reduce_rows(w->partials, w->values, w->batch, w->rblocks, w->rblocks, 1, st, true);
+    launch_programmatic(normalize_kernel<S, S>, w->rblocks, kThreads, 0, st, g, (const S*)image,
+                        (const double*)w->values, basis, N, w->input,
+                        ArnoldiTail{w->hessenberg(), w->cosine(), w->sine(), w->ls_rhs(), w->status(), 0, m + 1},
+                        (const ArnoldiControl*)w->ctl);
+    launch_programmatic(arnoldi_end_kernel, 1u, 1u, 0, st, w->ctl, (const double*)w->status(), handle, conditional);
     count_launches(5);
     check();
   }
