@@ -118,9 +118,10 @@ constexpr int kThinTY = 8;
 // needs is computed once into shared memory, then every thread forms its
 // node's C2N curl, 27-block mass product and combination. Rows of the
 // duplicate endpoint planes equal their unique node's row (same inputs, same
-// operations) and are copied by duplicate_rows_kernel.
+// operations) and are copied by duplicate_rows_kernel. Registers are bounded
+// for four CTAs per SM in float (64) and three in double (85).
 template <class C, class M, class Out, int TX, int TY, int TZ>
-__global__ void __launch_bounds__(TX * TY * TZ) maxwell_apply_kernel(Geom g, C d2, C kfac, C inv_volume,
+__global__ void __launch_bounds__(TX * TY * TZ, sizeof(C) == 4 ? 4 : 3) maxwell_apply_kernel(Geom g, C d2, C kfac, C inv_volume,
                                                                         const M* __restrict__ mass,
                                                                         const double* __restrict__ v,
                                                                         Out* __restrict__ out) {
@@ -134,6 +135,23 @@ __global__ void __launch_bounds__(TX * TY * TZ) maxwell_apply_kernel(Geom g, C d
   const int tx = blockIdx.x % tiles_x, ty = (blockIdx.x / tiles_x) % tiles_y, tz = blockIdx.x / (tiles_x * tiles_y);
   const int i0 = tx * TX, j0 = ty * TY, k0 = tz * TZ;
   const long long nn = g.nodes;
+  // The centre block and the first stencil's forward and backward rows of
+  // this thread's node are requested into L2 before the staging below, so
+  // the mass stream is in flight while v and the curls are staged.
+  {
+    const int pi = i0 + int(threadIdx.x % TX), pj = j0 + int((threadIdx.x / TX) % TY),
+              pk = k0 + int(threadIdx.x / (TX * TY));
+    if (pi < g.nx && pj < g.ny && pk < g.nz) {
+      const long long pat = g.node(pi, pj, pk);
+      const long long d1 = stencil_offset(1, 0) + (long long)g.NX * (stencil_offset(1, 1) + (long long)g.NY * stencil_offset(1, 2));
+#pragma unroll
+      for (int e = 0; e < 9; ++e) {
+        prefetch_l2(mass + g.mass_index(pat, e));
+        prefetch_l2(mass + g.mass_index(pat, 9 + e));
+        prefetch_l2(mass + g.mass_index(pat - d1, 9 + e));
+      }
+    }
+  }
   // Stage v over nodes [i0-1, i0+TX] x [j0-1, j0+TY] x [k0-1, k0+TZ]; nodes
   // beyond n+1 (partial tiles) are never read by a live node and load 0.
   for (int t = threadIdx.x; t < 3 * VZ * VY * VX; t += blockDim.x) {
