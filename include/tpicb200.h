@@ -112,7 +112,14 @@ typedef struct {
   int precision;            /* TPICB200_PRECISION_* */
   uint32_t max_particles;   /* capacity of the sort scratch (largest species) */
   int mass_layout;          /* TPICB200_MASS_LAYOUT_* (0: TPIC records) */
+  /* Energy-conserving smoothing (TPIC ECSimSmoothing = energy_conserving,
+   * config/physics.cpp:65-70): on when smooth_iterations > 0 and
+   * smooth_alpha < 1. Zero-initialized options leave it off. */
+  int smooth_iterations;    /* SmoothNiter: passes of S, >= 0 */
+  double smooth_alpha;      /* Smooth: Face7 centre weight in [0, 1] */
+  int smooth_operator;      /* TPICB200_SMOOTH_FACE7 or TPICB200_SMOOTH_BINOMIAL27 */
 } tpicb200_options;
+enum { TPICB200_SMOOTH_FACE7 = 0, TPICB200_SMOOTH_BINOMIAL27 = 1 };
 
 typedef struct {
   void* rx; void* ry; void* rz; /* double */
@@ -256,6 +263,17 @@ int tpicb200_sort_binned(tpicb200_context* ctx, const tpicb200_particles* in, co
 int tpicb200_sort_static(const tpicb200_grid* grid, int precision, const tpicb200_particles* in,
                          tpicb200_particles* out, uint32_t* counts, uint32_t* offsets, uint32_t* invalid,
                          tpicb200_stream stream);
+
+/* S^n of a double node field (ghosts of `in` filled) into `out` with its
+ * ghosts filled: the context's energy-conserving smoothing, n passes of
+ * Face7 (alpha centre, (1-alpha)/6 faces) or Binomial27 ([1,2,1]^3/64) over
+ * the interior nodes in the field arithmetic of the precision mode. The
+ * particle field of a smoothed run is S^n(E_theta); tpicb200_cycle applies it
+ * itself. Replaces MaxwellOperator::complete_smoothing
+ * (ecsim/maxwell/maxwell_device.hpp:455-487) with node_smoothing_value
+ * (ecsim/fields/node_smoothing.hpp:24-52). Returns TPICB200_INVALID_STATE
+ * when the context has no smoothing; in and out must not alias. */
+int tpicb200_smooth(tpicb200_context* ctx, const double* in, double* out, tpicb200_stream stream);
 
 /* Zero J (node field) and the mass records. Replaces enqueue_clear_mass_matrix
  * (ecsim/mass_matrix/mass_matrix_deposition_device.hpp:107-121) and the moment clear. */

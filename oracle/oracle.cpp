@@ -382,25 +382,90 @@ struct Physics {
         inv_volume(1.0 / ((g.dx * g.dy) * g.dz)), inv{1.0 / g.dx, 1.0 / g.dy, 1.0 / g.dz} {}
 };
 
+// One energy-conserving smoothing pass at interior node (i,j,k) of a node
+// component with filled ghosts (node_smoothing_value,
+// ecsim/fields/node_smoothing.hpp:24-52): op 0 Face7, alpha*centre +
+// beta*faces with beta = (1-alpha)/6; op 1 Binomial27, (8*centre + 4*faces +
+// 2*edges + corners)/64. Each neighbour sum runs left to right in the order
+// the reference fixes; every load is promoted before any arithmetic.
+template <class C>
+C smooth_value(const Layout& L, const double* f, int i, int j, int k, int op, C alpha, C beta) {
+  auto v = [&](int a, int b, int c) { return C(f[L.node(a, b, c)]); };
+  const C face = v(i - 1, j, k) + v(i + 1, j, k) + v(i, j - 1, k) + v(i, j + 1, k) + v(i, j, k - 1) + v(i, j, k + 1);
+  if (op == 0) return alpha * v(i, j, k) + beta * face;
+  const C edge = v(i - 1, j - 1, k) + v(i + 1, j - 1, k) + v(i - 1, j + 1, k) + v(i + 1, j + 1, k) +
+                 v(i - 1, j, k - 1) + v(i + 1, j, k - 1) + v(i - 1, j, k + 1) + v(i + 1, j, k + 1) +
+                 v(i, j - 1, k - 1) + v(i, j + 1, k - 1) + v(i, j - 1, k + 1) + v(i, j + 1, k + 1);
+  const C corner = v(i - 1, j - 1, k - 1) + v(i + 1, j - 1, k - 1) + v(i - 1, j + 1, k - 1) +
+                   v(i + 1, j + 1, k - 1) + v(i - 1, j - 1, k + 1) + v(i + 1, j - 1, k + 1) +
+                   v(i - 1, j + 1, k + 1) + v(i + 1, j + 1, k + 1);
+  return (C(8) * v(i, j, k) + C(4) * face + C(2) * edge + corner) * (C(1) / C(64));
+}
+
+// S^niter of a 3-component node field in FP64 storage (complete_smoothing,
+// ecsim/maxwell/maxwell_device.hpp:455-487 on a periodic domain): the ghosts
+// are filled before every pass, each pass writes the interior nodes 0..n,
+// and the result leaves with its ghosts filled. niter = 0 copies.
+void smooth_field(const Layout& L, int niter, int op, double alpha, const double* src, double* out) {
+  std::vector<double> a(src, src + 3 * L.nodes), b(3 * L.nodes, 0.0);
+  const double beta = (1.0 - alpha) / 6.0;
+  for (int pass = 0; pass < niter; ++pass) {
+    for (int c = 0; c < 3; ++c) node_ghosts(L, a.data() + c * L.nodes, 1, 1);
+    b = a;
+    for (int c = 0; c < 3; ++c)
+      for (int k = 0; k <= L.nz; ++k)
+        for (int j = 0; j <= L.ny; ++j)
+          for (int i = 0; i <= L.nx; ++i)
+            b[c * L.nodes + L.node(i, j, k)] = smooth_value<double>(L, a.data() + c * L.nodes, i, j, k, op, alpha, beta);
+    a.swap(b);
+  }
+  for (int c = 0; c < 3; ++c) node_ghosts(L, a.data() + c * L.nodes, 1, 1);
+  std::copy(a.begin(), a.end(), out);
+}
+
 // MaxwellOperator::complete_apply with the unsmoothed full schedule and
 // combine_image, ecsim/maxwell/maxwell_device.hpp:184-212,471-484:
 // image = ((input + delta^2 * curl_C2N(curl_N2C(input))) + k * M input).
 // `in` is a node field whose ghosts this function fills.
+// With smoothing (niter > 0), complete_apply_smoothed and combine_image
+// (maxwell_device.hpp:389-432): the mass response of S^n(input), smoothed
+// n times, replaces M input.
+struct Smoothing {
+  int niter = 0, op = 0;
+  double alpha = 1.0;
+};
 template <class M>
 void maxwell_apply(const Layout& L, const Physics& ph, const M* mass, double* in, double* image,
-                   double* curl_cell, double* curl_node) {
+                   double* curl_cell, double* curl_node, const Smoothing& sm = Smoothing{}) {
   node_ghosts(L, in, 1, 1);
   node_ghosts(L, in + L.nodes, 1, 1);
   node_ghosts(L, in + 2 * L.nodes, 1, 1);
   curl_n2c(L, in, curl_cell, ph.inv);
   curl_c2n(L, curl_cell, curl_node, ph.inv);
   const double d2 = ph.delta * ph.delta;
+  std::vector<double> response;
+  if (sm.niter > 0) {
+    std::vector<double> smoothed(3 * L.nodes), mimage(3 * L.nodes, 0.0);
+    smooth_field(L, sm.niter, sm.op, sm.alpha, in, smoothed.data());
+    for (int k = 0; k <= L.nz; ++k)
+      for (int j = 0; j <= L.ny; ++j)
+        for (int i = 0; i <= L.nx; ++i) {
+          double m[3];
+          mass_apply_node(L, mass, smoothed.data(), i, j, k, ph.inv_volume, m);
+          for (int c = 0; c < 3; ++c) mimage[c * L.nodes + L.node(i, j, k)] = m[c];
+        }
+    response.resize(3 * L.nodes);
+    smooth_field(L, sm.niter, sm.op, sm.alpha, mimage.data(), response.data());
+  }
   for (int k = 0; k <= L.nz; ++k)
     for (int j = 0; j <= L.ny; ++j)
       for (int i = 0; i <= L.nx; ++i) {
         double m[3];
-        mass_apply_node(L, mass, in, i, j, k, ph.inv_volume, m);
         const long g = L.node(i, j, k);
+        if (sm.niter > 0)
+          for (int c = 0; c < 3; ++c) m[c] = response[c * L.nodes + g];
+        else
+          mass_apply_node(L, mass, in, i, j, k, ph.inv_volume, m);
         for (int c = 0; c < 3; ++c) {
           const long at = c * L.nodes + g;
           image[at] = (1.0 * in[at] + d2 * curl_node[at]) + ph.kfac * m[c];
@@ -635,15 +700,26 @@ void oracle_cell_ghosts(const oracle_grid* gp, double* cellf) { cell_ghosts(Layo
 // (classical Gram-Schmidt, Givens rotations, true-residual acceptance).
 // E, J: node fields; B: cell field with ghosts; M: double mass records with
 // ghosts; theta: node field output (the solution).
-int oracle_field_solve(const oracle_grid* gp, double dt, double th, double c, const double* E,
-                       const double* B, const double* J, const double* M, double* theta,
-                       int restart, int max_iterations, double tol, oracle_gmres_result* out) {
+// With smooth_iterations > 0 the energy-conserving smoothing of TPIC
+// (ECSimSmoothing = energy_conserving): the RHS uses S^n(J) and every apply
+// the smoothed schedule (maxwell_device.hpp:152-172,389-432).
+int oracle_field_solve_smoothed(const oracle_grid* gp, double dt, double th, double c, const double* E,
+                                const double* B, const double* J_in, const double* M, double* theta,
+                                int restart, int max_iterations, double tol, int smooth_iterations,
+                                double smooth_alpha, int smooth_operator, oracle_gmres_result* out) {
   const Grid g = to_grid(gp);
   const Layout L(g);
   const Physics ph(g, dt, th, c);
   const long N = 3 * L.interior;
+  const Smoothing sm{smooth_iterations, smooth_operator, smooth_alpha};
   std::vector<double> curl_node(3 * L.nodes, 0.0), curl_cell(3 * L.cells, 0.0), rhs(3 * L.nodes, 0.0),
-      input(3 * L.nodes, 0.0), image(3 * L.nodes, 0.0);
+      input(3 * L.nodes, 0.0), image(3 * L.nodes, 0.0), smoothed_j;
+  const double* J = J_in;
+  if (sm.niter > 0) {
+    smoothed_j.resize(3 * L.nodes);
+    smooth_field(L, sm.niter, sm.op, sm.alpha, J_in, smoothed_j.data());
+    J = smoothed_j.data();
+  }
   // RHS, maxwell_device.hpp:134-172.
   curl_c2n(L, B, curl_node.data(), ph.inv);
   for (int cc = 0; cc < 3; ++cc)
@@ -661,7 +737,7 @@ int oracle_field_solve(const oracle_grid* gp, double dt, double th, double c, co
   pack(L, rhs.data(), b.data());
   auto apply = [&](const double* vec, double* result) {
     unpack(L, vec, input.data());
-    maxwell_apply(L, ph, M, input.data(), image.data(), curl_cell.data(), curl_node.data());
+    maxwell_apply(L, ph, M, input.data(), image.data(), curl_cell.data(), curl_node.data(), sm);
     pack(L, image.data(), result);
   };
   auto dot = [&](const double* a, const double* bb) {
@@ -756,6 +832,24 @@ int oracle_field_solve(const oracle_grid* gp, double dt, double th, double c, co
   for (int cc = 0; cc < 3; ++cc) node_ghosts(L, theta + cc * L.nodes, 1, 1);
   if (out) *out = res;
   return res.converged ? 0 : 1;
+}
+
+int oracle_field_solve(const oracle_grid* gp, double dt, double th, double c, const double* E,
+                       const double* B, const double* J, const double* M, double* theta,
+                       int restart, int max_iterations, double tol, oracle_gmres_result* out) {
+  return oracle_field_solve_smoothed(gp, dt, th, c, E, B, J, M, theta, restart, max_iterations, tol, 0, 1.0, 0,
+                                     out);
+}
+
+// S^niter of a node field (FP64), ghosts filled; the particle field of a
+// smoothed run is S^n(theta) (maxwell_device.hpp:213-228).
+void oracle_smooth(const oracle_grid* gp, int niter, double alpha, int op, const double* in, double* out) {
+  smooth_field(Layout(to_grid(gp)), niter, op, alpha, in, out);
+}
+// One pass at one node, for the pin against the reference's own operator.
+double oracle_smooth_node(const oracle_grid* gp, int op, double alpha, const double* in, int i, int j, int k) {
+  const Layout L(to_grid(gp));
+  return smooth_value<double>(L, in, i, j, k, op, alpha, (1.0 - alpha) / 6.0);
 }
 
 // Field advance, ecsim/maxwell/field_update_device.hpp:25-78 and

@@ -65,6 +65,13 @@ def load():
         lib.oracle_field_solve.restype = C.c_int
         lib.oracle_field_solve.argtypes = [C.POINTER(OGrid), C.c_double, C.c_double, C.c_double, vp, vp, vp, vp,
                                            vp, C.c_int, C.c_int, C.c_double, C.POINTER(OGmres)]
+        lib.oracle_field_solve_smoothed.restype = C.c_int
+        lib.oracle_field_solve_smoothed.argtypes = [C.POINTER(OGrid), C.c_double, C.c_double, C.c_double, vp, vp,
+                                                    vp, vp, vp, C.c_int, C.c_int, C.c_double, C.c_int, C.c_double,
+                                                    C.c_int, C.POINTER(OGmres)]
+        lib.oracle_smooth.argtypes = [C.POINTER(OGrid), C.c_int, C.c_double, C.c_int, vp, vp]
+        lib.oracle_smooth_node.restype = C.c_double
+        lib.oracle_smooth_node.argtypes = [C.POINTER(OGrid), C.c_int, C.c_double, vp, C.c_int, C.c_int, C.c_int]
         lib.oracle_field_advance.argtypes = [C.POINTER(OGrid), C.c_double, C.c_double, C.c_double, vp, vp, vp,
                                              vp, vp]
         lib.oracle_field_energy.argtypes = [C.POINTER(OGrid), vp, vp, vp]
@@ -93,6 +100,9 @@ def load_reference():
         lib.ref_cic_weights_f32.argtypes = [C.c_float, C.c_float, C.c_float, vp]
         lib.ref_response_f64.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double, vp]
         lib.ref_response_f32.argtypes = [C.c_float, C.c_float, C.c_float, C.c_float, vp]
+        if hasattr(lib, "ref_smooth_node"):
+            lib.ref_smooth_node.restype = C.c_double
+            lib.ref_smooth_node.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, vp, C.c_int, C.c_int, C.c_int]
         lib.ref_pair_stencil.restype = C.c_int
         lib.ref_pair_stencil.argtypes = [C.c_int, C.c_int]
         lib.ref_stencil_offset.argtypes = [C.c_int, vp]
@@ -121,12 +131,15 @@ class OracleCycle:
 
     def __init__(self, grid, species, dt, theta=0.5, c=1.0, gmres_tol=1e-8, precision=0,
                  restart=30, max_iterations=100, e0=(0.0, 0.0, 0.0), b0=(0.0, 0.0, 0.0), e_node=None,
-                 b_cell=None):
+                 b_cell=None, smoothing=(0, 1.0, 0)):
         self.lib = load()
         self.og = OGrid(grid.nx, grid.ny, grid.nz, grid.lx / grid.nx, grid.ly / grid.ny, grid.lz / grid.nz)
         self.grid = grid
         self.dt, self.theta, self.c, self.tol = dt, theta, c, gmres_tol
         self.restart, self.max_iterations = restart, max_iterations
+        # Energy-conserving smoothing (passes, Face7 centre weight, operator
+        # 0 Face7 / 1 Binomial27); on when passes > 0 and the weight < 1.
+        self.smoothing = tuple(smoothing) if smoothing[0] > 0 and smoothing[1] < 1 else (0, 1.0, 0)
         self.precision = precision
         self.vdt = np.float64 if precision == 0 else np.float32
         self.fdt = np.float64 if precision == 0 else np.float32
@@ -195,19 +208,31 @@ class OracleCycle:
 
     def solve(self):
         res = OGmres()
-        status = self.lib.oracle_field_solve(C.byref(self.og), self.dt, self.theta, self.c, ptr(self.e), ptr(self.b),
-                                             ptr(self.j), ptr(self.m), ptr(self.theta_field), self.restart,
-                                             self.max_iterations, self.tol, C.byref(res))
+        niter, alpha, op = self.smoothing
+        status = self.lib.oracle_field_solve_smoothed(C.byref(self.og), self.dt, self.theta, self.c, ptr(self.e),
+                                                      ptr(self.b), ptr(self.j), ptr(self.m), ptr(self.theta_field),
+                                                      self.restart, self.max_iterations, self.tol, niter, alpha, op,
+                                                      C.byref(res))
         self.gmres.append(res)
         if status != 0:
             raise RuntimeError("oracle GMRES did not converge")
         return res
 
+    def particle_field(self):
+        """The field the movers gather: E_theta, or S^n(E_theta) when smoothing."""
+        niter, alpha, op = self.smoothing
+        if niter == 0:
+            return self.theta_field
+        out = np.zeros_like(self.theta_field)
+        self.lib.oracle_smooth(C.byref(self.og), niter, alpha, op, ptr(self.theta_field), ptr(out))
+        return out
+
     def move(self):
         bn = self.bnode.astype(self.fdt)
+        field = self.particle_field()
         for qom, d in self.species:
             bad = self.lib.oracle_mover(self.precision, C.byref(self.og), qom, self.dt, self.c, *self._ptrs(d),
-                                        len(d["cell"]), ptr(self.theta_field), ptr(bn))
+                                        len(d["cell"]), ptr(field), ptr(bn))
             if bad:
                 raise ValueError(f"{bad} invalid records in the mover")
 

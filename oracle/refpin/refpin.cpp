@@ -12,10 +12,12 @@
 //   node_cell_curl                 ecsim/fields/node_cell_curl.hpp:116-126
 //   cell_to_node_average           ecsim/fields/cell_to_node.hpp:19-32
 //   ParticleCellMap encode/decode  data/particles/particle_cell.hpp:34-46
+//   node_smoothing_value           ecsim/fields/node_smoothing.hpp:24-52
 #include <tpic/data/mass_matrix/mass_matrix_layout.hpp>
 #include <tpic/data/particles/particle_cell.hpp>
 #include <tpic/ecsim/fields/cell_to_node.hpp>
 #include <tpic/ecsim/fields/node_cell_curl.hpp>
+#include <tpic/ecsim/fields/node_smoothing.hpp>
 #include <tpic/ecsim/mass_matrix/mass_matrix_stencil.hpp>
 #include <tpic/ecsim/particles/cic.hpp>
 #include <tpic/ecsim/particles/particle_response.hpp>
@@ -98,6 +100,18 @@ void ref_curl_c2n(int nx, int ny, int nz, const double* cell, double ix, double 
 double ref_cell_to_node(int nx, int ny, const double* cell, int i, int j, int k) {
   const Component<lpfx::Cell> c{cell, nx + 2L, ny + 2L};
   return tpic::ecsim::cell_to_node_average<double>(c, i, j, k);
+}
+
+// One smoothing pass at node (i,j,k) of a node component with its one-node
+// halo: op 0 Face7 (centre weight alpha, faces (1 - alpha)/6), 1 Binomial27.
+double ref_smooth_node(int nx, int ny, int op, double alpha, const double* node, int i, int j, int k) {
+  using Op = tpic::config::EcsimSmoothingOperator;
+  const Component<lpfx::Node> c{node, nx + 3L, ny + 3L};
+  if (op == 0)
+    return tpic::ecsim::node_smoothing_value<Op::Face7, double>(
+        c, i, j, k, tpic::ecsim::SmoothingWeights<Op::Face7, double>{alpha, (1.0 - alpha) / 6.0});
+  return tpic::ecsim::node_smoothing_value<Op::Binomial27, double>(
+      c, i, j, k, tpic::ecsim::SmoothingWeights<Op::Binomial27, double>{});
 }
 
 // (M v) at node (i,j,k) with the reference's compact layout and apply order.

@@ -14,13 +14,14 @@ ATTRS = ("rx", "ry", "rz", "u", "v", "w", "q", "cell")
 
 class StageContext:
     def __init__(self, grid, precision=0, dt=0.15, theta=0.5, c=1.0, tol=1e-8, max_particles=1 << 20,
-                 restart=30, max_iterations=100, mass_layout=0):
+                 restart=30, max_iterations=100, mass_layout=0, smoothing=(0, 1.0, 0)):
         self.lib = _lib.load()
         self.g = grid
         self.precision = precision
         self.fdt = torch.float64 if precision == 0 else torch.float32
         self.np_fdt = np.float64 if precision == 0 else np.float32
-        opts = _lib.Options(dt, theta, c, tol, restart, max_iterations, precision, max_particles, mass_layout)
+        opts = _lib.Options(dt, theta, c, tol, restart, max_iterations, precision, max_particles, mass_layout,
+                            *smoothing)
         self.mass_layout = mass_layout
         gr = _lib.Grid(grid.nx, grid.ny, grid.nz, grid.lx, grid.ly, grid.lz)
         h = C.c_void_p()

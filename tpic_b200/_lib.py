@@ -32,7 +32,8 @@ class Grid(C.Structure):
 class Options(C.Structure):
     _fields_ = [("dt", C.c_double), ("theta", C.c_double), ("c", C.c_double), ("gmres_tol", C.c_double),
                 ("gmres_restart", C.c_int), ("gmres_max_iterations", C.c_int), ("precision", C.c_int),
-                ("max_particles", C.c_uint32), ("mass_layout", C.c_int)]
+                ("max_particles", C.c_uint32), ("mass_layout", C.c_int), ("smooth_iterations", C.c_int),
+                ("smooth_alpha", C.c_double), ("smooth_operator", C.c_int)]
 
 
 class Particles(C.Structure):
@@ -123,6 +124,7 @@ EXPORTS = {
     "tpicb200_field_advance": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                          C.c_void_p, C.c_void_p]),
     "tpicb200_magnetic_to_nodes": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tpicb200_smooth": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tpicb200_energy": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(Particles),
                                   C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_double), C.c_void_p]),
     "tpicb200_prepare": (C.c_int, [C.c_void_p, C.POINTER(State), C.c_void_p]),

@@ -30,6 +30,7 @@ struct tpicb200_context {
   int mover_written[TPICB200_MAX_SPECIES]{};
   double* reduced = nullptr;     // energy reduction results
   double* center = nullptr;      // velocity-centring partials (4 rows of energy_blocks) and 4 sums
+  double* particle_theta = nullptr;  // S^n(E_theta), the movers' field when smoothing is on
   double* pinned = nullptr;      // host mirror of `reduced` + invalid
   int energy_blocks = 0;
   cudaEvent_t events[6 + 3 * TPICB200_MAX_SPECIES]{};
@@ -159,6 +160,12 @@ int tpicb200_create(const tpicb200_grid* grid, const tpicb200_options* options, 
   if (options->mass_layout != TPICB200_MASS_LAYOUT_RECORDS &&
       options->mass_layout != TPICB200_MASS_LAYOUT_STENCIL_MAJOR)
     return fail(TPICB200_INVALID_ARGUMENT, "unknown mass layout");
+  // config/physics.cpp:65-70: 0 <= Smooth <= 1, SmoothNiter >= 0.
+  if (options->smooth_iterations < 0 || !std::isfinite(options->smooth_alpha) ||
+      (options->smooth_iterations > 0 && (options->smooth_alpha < 0 || options->smooth_alpha > 1)) ||
+      (options->smooth_operator != TPICB200_SMOOTH_FACE7 && options->smooth_operator != TPICB200_SMOOTH_BINOMIAL27))
+    return fail(TPICB200_INVALID_ARGUMENT,
+                "energy-conserving smoothing requires SmoothNiter >= 0, 0 <= Smooth <= 1 and a known operator");
   int device = 0, count = 0;
   if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
     return fail(TPICB200_BACKEND_FAILURE, "no CUDA device: the ECSIM cycle has no CPU fallback");
@@ -176,8 +183,11 @@ int tpicb200_create(const tpicb200_grid* grid, const tpicb200_options* options, 
   }
   ctx->opt = *options;
   cudaError_t e = cudaSuccess;
+  SmoothingPlan smoothing;
+  if (options->smooth_iterations > 0 && options->smooth_alpha < 1)
+    smoothing = SmoothingPlan{options->smooth_iterations, options->smooth_alpha, options->smooth_operator};
   ctx->solver = solver_create(options->precision, ctx->g, options->gmres_restart, options->dt,
-                              options->theta, options->c, &e);
+                              options->theta, options->c, smoothing, &e);
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   ctx->energy_blocks = 4 * sms;
@@ -195,6 +205,7 @@ int tpicb200_create(const tpicb200_grid* grid, const tpicb200_options* options, 
   alloc((void**)&ctx->mover_partials, size_t(kMoverPartials) * 5 * TPICB200_MAX_SPECIES * 8);
   alloc((void**)&ctx->reduced, (2 + 5 * TPICB200_MAX_SPECIES + 2) * 8);
   alloc((void**)&ctx->center, (size_t(4) * ctx->energy_blocks + 4) * 8);
+  if (smoothing.iterations > 0) alloc((void**)&ctx->particle_theta, size_t(3) * ctx->g.nodes * 8);
   alloc((void**)&ctx->moments, moment_floats(ctx->g) * (options->precision == TPICB200_PRECISION_MIXED ? 4 : 8));
   if (e == cudaSuccess) e = cudaMallocHost((void**)&ctx->pinned, (2 + 5 * TPICB200_MAX_SPECIES + 2) * 8);
   if (e == cudaSuccess) e = cudaMemset(ctx->invalid, 0, 4);
@@ -216,6 +227,7 @@ int tpicb200_destroy(tpicb200_context* ctx) {
   cudaFree(ctx->invalid);
   cudaFree(ctx->partials); cudaFree(ctx->mover_partials); cudaFree(ctx->reduced); cudaFree(ctx->moments);
   cudaFree(ctx->center);
+  cudaFree(ctx->particle_theta);
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
   for (auto& ev : ctx->events)
     if (ev) cudaEventDestroy(ev);
@@ -368,6 +380,13 @@ int tpicb200_fold_periodic(tpicb200_context* ctx, void* j, void* mass, tpicb200_
     ctx->cleared_j = ctx->cleared_mass = nullptr;
   }
   return cuda_status(launch_fold(ctx->opt.precision, ctx->g, j, mass, (cudaStream_t)stream), "fold launch failed");
+}
+
+int tpicb200_smooth(tpicb200_context* ctx, const double* in, double* out, tpicb200_stream stream) {
+  if (int s = check_ctx(ctx)) return s;
+  if (!in || !out || in == out) return fail(TPICB200_INVALID_ARGUMENT, "smoothing needs distinct in and out fields");
+  if (!ctx->particle_theta) return fail(TPICB200_INVALID_STATE, "the context has no energy-conserving smoothing");
+  return cuda_status(solver_smooth(ctx->solver, in, out, (cudaStream_t)stream), "smoothing launch failed");
 }
 
 int tpicb200_mass_apply(tpicb200_context* ctx, const void* mass, const double* in, double* out,
@@ -575,6 +594,11 @@ static int check_state(tpicb200_context* ctx, tpicb200_state* st) {
 
 // How the deposition reads a species after move_and_sort, and whether the
 // live slot flips after it.
+// The field the cycle's movers gather: S^n(E_theta) with smoothing, else E_theta.
+static const double* particle_field(const tpicb200_context* ctx, const tpicb200_state* st) {
+  return ctx->particle_theta ? ctx->particle_theta : st->e_theta;
+}
+
 struct DepositPlan {
   const tpicb200_particles* read;  // records the deposition reads
   SortedCopy copy;                 // through which ranks, and where to write them sorted
@@ -613,7 +637,7 @@ static int move_and_sort(tpicb200_context* ctx, tpicb200_state* st, int sp, uint
   const tpicb200_particles none{};
   if (!binned_sort_applies(ctx->g)) {
     if (st->ranked[sp]) return fail(TPICB200_INVALID_STATE, "ranked species on a grid without the binned sort");
-    cudaError_t e = launch_mover(p, ctx->g, qom, ctx->opt.dt, ctx->opt.c, in, nullptr, nullptr, st->e_theta,
+    cudaError_t e = launch_mover(p, ctx->g, qom, ctx->opt.dt, ctx->opt.c, in, nullptr, nullptr, particle_field(ctx, st),
                                  st->b_node, ctx->invalid, nullptr, scalars, s);
     if (e == cudaSuccess) e = cudaEventRecord(moved, s);
     if (e == cudaSuccess)
@@ -632,7 +656,7 @@ static int move_and_sort(tpicb200_context* ctx, tpicb200_state* st, int sp, uint
     // Out of place: the moved records, in the previous sorted order, go live.
     if (e == cudaSuccess)
       e = launch_mover(p, ctx->g, qom, ctx->opt.dt, ctx->opt.c, in, out, st->ranked[sp] ? st->ranks[sp] : nullptr,
-                       st->e_theta, st->b_node, ctx->invalid, &b, scalars, s);
+                       particle_field(ctx, st), st->b_node, ctx->invalid, &b, scalars, s);
     if (e == cudaSuccess) e = cudaEventRecord(moved, s);
     if (e == cudaSuccess)
       e = binned_finish(p, ctx->g, b, false, false, out, in, st->counts[sp], st->offsets[sp], ctx->cursor,
@@ -646,7 +670,7 @@ static int move_and_sort(tpicb200_context* ctx, tpicb200_state* st, int sp, uint
   }
   if (st->ranked[sp]) return fail(TPICB200_INVALID_STATE, "ranked species without a rank buffer");
   if (e == cudaSuccess)
-    e = launch_mover(p, ctx->g, qom, ctx->opt.dt, ctx->opt.c, in, nullptr, nullptr, st->e_theta, st->b_node,
+    e = launch_mover(p, ctx->g, qom, ctx->opt.dt, ctx->opt.c, in, nullptr, nullptr, particle_field(ctx, st), st->b_node,
                      ctx->invalid, &b, scalars, s);
   if (e == cudaSuccess) e = cudaEventRecord(moved, s);
   if (e == cudaSuccess)
@@ -788,6 +812,11 @@ int tpicb200_cycle(tpicb200_context* ctx, tpicb200_state* st, int ncycles, tpicb
     cudaEventRecord(ev[1], s);
     // Field advance: E^{n+1} and the next B from E_theta (the movers read
     // E_theta and the old B nodes, which the advance does not touch).
+    if (ctx->particle_theta) {
+      // The movers gather S^n(E_theta); the field advance uses E_theta.
+      const cudaError_t e = solver_smooth(ctx->solver, st->e_theta, ctx->particle_theta, s);
+      if (e != cudaSuccess) return cuda_status(e, "particle-field smoothing failed");
+    }
     if (int r = tpicb200_field_advance(ctx, st->e, st->b_cell, st->e_theta, st->b_cell_next, st->b_node_next, stream))
       return r;
     cudaEventRecord(ev[2], s);

@@ -134,9 +134,9 @@ __global__ void __launch_bounds__(256) cell_to_node_kernel(Geom g, const T* __re
 
 // rhs = ((1*E + delta*curl_C2N(B)) + (-k)*J) in Compute::Electric
 // (MaxwellOperator::complete_rhs, ecsim/maxwell/maxwell_device.hpp:152-172).
-template <class C, class T>
+template <class C, class T, class TJ>
 __global__ void __launch_bounds__(256) rhs_kernel(Geom g, C delta, C kfac, const T* __restrict__ e,
-                                                  const T* __restrict__ bcell, const T* __restrict__ j,
+                                                  const T* __restrict__ bcell, const TJ* __restrict__ j,
                                                   double* __restrict__ rhs) {
   const C inv[3] = {C(g.inv[0]), C(g.inv[1]), C(g.inv[2])};
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < g.interior;
@@ -299,14 +299,107 @@ cudaError_t launch_cell_to_node(int precision, const Geom& g, const void* cellf,
 }
 
 cudaError_t launch_rhs(int precision, const Geom& g, double delta, double kfac, const void* e,
-                       const void* bcell, const void* j, double* rhs, cudaStream_t s) {
+                       const void* bcell, const void* j, double* rhs, cudaStream_t s, bool j_double) {
   const unsigned blocks = grid_for(g.interior, 256);
   if (precision == TPICB200_PRECISION_DOUBLE)
-    rhs_kernel<double, double><<<blocks, 256, 0, s>>>(g, delta, kfac, (const double*)e, (const double*)bcell,
-                                                     (const double*)j, rhs);
+    rhs_kernel<double, double, double><<<blocks, 256, 0, s>>>(g, delta, kfac, (const double*)e,
+                                                             (const double*)bcell, (const double*)j, rhs);
+  else if (j_double)
+    rhs_kernel<float, float, double><<<blocks, 256, 0, s>>>(g, float(delta), float(kfac), (const float*)e,
+                                                           (const float*)bcell, (const double*)j, rhs);
   else
-    rhs_kernel<float, float><<<blocks, 256, 0, s>>>(g, float(delta), float(kfac), (const float*)e,
-                                                   (const float*)bcell, (const float*)j, rhs);
+    rhs_kernel<float, float, float><<<blocks, 256, 0, s>>>(g, float(delta), float(kfac), (const float*)e,
+                                                          (const float*)bcell, (const float*)j, rhs);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+// Energy-conserving smoothing, one pass (node_smoothing_kernel,
+// ecsim/fields/node_smoothing_device.hpp:17-36, with the operator of
+// ecsim/fields/node_smoothing.hpp:24-52): every interior node 0..n of the
+// three components, from a double node field with filled ghosts into a
+// double node field, in arithmetic C with each product and sum rounded on
+// its own (no contraction) in the reference's order. Op 0 Face7: alpha *
+// centre + beta * faces; op 1 Binomial27: (8 centre + 4 faces + 2 edges +
+// corners) * (1/64).
+__device__ __forceinline__ float rn_mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double rn_mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float rn_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double rn_add(double a, double b) { return __dadd_rn(a, b); }
+
+template <class C, int Op>
+__global__ void __launch_bounds__(256) smooth_kernel(Geom g, C alpha, C beta, const double* __restrict__ src,
+                                                     double* __restrict__ dst) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 3 * g.interior;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int c = int(t / g.interior);
+    int i, j, k;
+    interior_node_coordinates(g, t - c * g.interior, i, j, k);
+    const double* f = src + c * g.nodes;
+    auto v = [&](int a, int b, int d) { return C(f[g.node(a, b, d)]); };
+    const C face = rn_add(rn_add(rn_add(rn_add(rn_add(v(i - 1, j, k), v(i + 1, j, k)), v(i, j - 1, k)),
+                                        v(i, j + 1, k)), v(i, j, k - 1)), v(i, j, k + 1));
+    C value;
+    if constexpr (Op == 0) {
+      value = rn_add(rn_mul(alpha, v(i, j, k)), rn_mul(beta, face));
+    } else {
+      C edge = rn_add(v(i - 1, j - 1, k), v(i + 1, j - 1, k));
+      edge = rn_add(edge, v(i - 1, j + 1, k)); edge = rn_add(edge, v(i + 1, j + 1, k));
+      edge = rn_add(edge, v(i - 1, j, k - 1)); edge = rn_add(edge, v(i + 1, j, k - 1));
+      edge = rn_add(edge, v(i - 1, j, k + 1)); edge = rn_add(edge, v(i + 1, j, k + 1));
+      edge = rn_add(edge, v(i, j - 1, k - 1)); edge = rn_add(edge, v(i, j + 1, k - 1));
+      edge = rn_add(edge, v(i, j - 1, k + 1)); edge = rn_add(edge, v(i, j + 1, k + 1));
+      C corner = rn_add(v(i - 1, j - 1, k - 1), v(i + 1, j - 1, k - 1));
+      corner = rn_add(corner, v(i - 1, j + 1, k - 1)); corner = rn_add(corner, v(i + 1, j + 1, k - 1));
+      corner = rn_add(corner, v(i - 1, j - 1, k + 1)); corner = rn_add(corner, v(i + 1, j - 1, k + 1));
+      corner = rn_add(corner, v(i - 1, j + 1, k + 1)); corner = rn_add(corner, v(i + 1, j + 1, k + 1));
+      const C sum = rn_add(rn_add(rn_add(rn_mul(C(8), v(i, j, k)), rn_mul(C(4), face)), rn_mul(C(2), edge)), corner);
+      value = rn_mul(sum, C(1) / C(64));
+    }
+    dst[c * g.nodes + g.node(i, j, k)] = double(value);
+  }
+}
+
+// S^n(src) into out with its ghosts filled (complete_smoothing,
+// ecsim/maxwell/maxwell_device.hpp:455-487 on a periodic domain): src's
+// ghosts must be filled; the passes alternate between out and tmp so that
+// the last lands in out, with the ghosts refilled between passes. Neither
+// out nor tmp may alias src. double_arithmetic selects the pass arithmetic
+// (the reference's Arithmetic / Compute::Electric).
+cudaError_t launch_smooth(bool double_arithmetic, const Geom& g, int niter, int op, double alpha,
+                          const double* src, double* out, double* tmp, cudaStream_t s) {
+  if (niter <= 0 || src == out || src == tmp || out == tmp) return cudaErrorInvalidValue;
+  const unsigned blocks = grid_for(3 * g.interior, 256);
+  const double* from = src;
+  for (int pass = 1; pass <= niter; ++pass) {
+    double* to = (niter - pass) % 2 == 0 ? out : tmp;
+    if (double_arithmetic) {
+      const double beta = (1.0 - alpha) / 6.0;
+      if (op == 0) smooth_kernel<double, 0><<<blocks, 256, 0, s>>>(g, alpha, beta, from, to);
+      else smooth_kernel<double, 1><<<blocks, 256, 0, s>>>(g, alpha, beta, from, to);
+    } else {
+      const float a = float(alpha), beta = (1.0f - a) / 6.0f;
+      if (op == 0) smooth_kernel<float, 0><<<blocks, 256, 0, s>>>(g, a, beta, from, to);
+      else smooth_kernel<float, 1><<<blocks, 256, 0, s>>>(g, a, beta, from, to);
+    }
+    count_launches(1);
+    launch_node_ghosts(g, to, 3, s);
+    from = to;
+  }
+  return cudaGetLastError();
+}
+
+// A node field of float or double into double (every entry, ghosts included).
+__global__ void __launch_bounds__(256) widen_kernel(const float* __restrict__ in, double* __restrict__ out,
+                                                    long long n) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+    out[t] = double(in[t]);
+}
+cudaError_t launch_widen(int precision, const Geom& g, const void* in, double* out, cudaStream_t s) {
+  const long long n = 3 * g.nodes;
+  if (precision == TPICB200_PRECISION_DOUBLE)
+    return cudaMemcpyAsync(out, in, size_t(n) * 8, cudaMemcpyDeviceToDevice, s);
+  widen_kernel<<<grid_for(n, 256), 256, 0, s>>>((const float*)in, out, n);
   count_launches(1);
   return cudaGetLastError();
 }

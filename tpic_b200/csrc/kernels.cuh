@@ -145,11 +145,14 @@ cudaError_t launch_assemble_moments(int precision, const Geom& g, const void* mo
 // fields.cu
 cudaError_t launch_node_ghosts(const Geom& g, double* f, int components, cudaStream_t s,
                                bool programmatic = false);
+cudaError_t launch_smooth(bool double_arithmetic, const Geom& g, int niter, int op, double alpha,
+                          const double* src, double* out, double* tmp, cudaStream_t s);
+cudaError_t launch_widen(int precision, const Geom& g, const void* in, double* out, cudaStream_t s);
 cudaError_t launch_cell_ghosts(int precision, const Geom& g, void* f, cudaStream_t s);
 cudaError_t launch_cell_to_node(int precision, const Geom& g, const void* cellf, void* node,
                                 cudaStream_t s);
 cudaError_t launch_rhs(int precision, const Geom& g, double delta, double kfac, const void* e,
-                       const void* bcell, const void* j, double* rhs, cudaStream_t s);
+                       const void* bcell, const void* j, double* rhs, cudaStream_t s, bool j_double = false);
 cudaError_t launch_field_advance(int precision, const Geom& g, double theta_value, double faraday,
                                  void* e, const void* bcell, const double* etheta, void* bnext,
                                  uint32_t* invalid, cudaStream_t s);
@@ -166,8 +169,18 @@ cudaError_t launch_copy_node_field(const Geom& g, const void* in, int in_double,
 
 // solver.cu
 struct SolverWorkspace;
+// Energy-conserving smoothing of the field solve: passes (0: off), Face7
+// centre weight, operator (0 Face7, 1 Binomial27).
+struct SmoothingPlan {
+  int iterations = 0;
+  double alpha = 1.0;
+  int op = 0;
+};
 SolverWorkspace* solver_create(int precision, const Geom& g, int restart, double dt,
-                               double theta, double c, cudaError_t* err);
+                               double theta, double c, const SmoothingPlan& smoothing, cudaError_t* err);
+// S^n of a double node field (ghosts filled) into out, in the field
+// arithmetic of the precision mode, with the solver's scratch.
+cudaError_t solver_smooth(SolverWorkspace* w, const double* in, double* out, cudaStream_t s);
 void solver_destroy(SolverWorkspace* w);
 int solver_solve(SolverWorkspace* w, const void* e, const void* bcell, const void* j,
                  const void* mass, double* etheta, tpicb200_gmres_result* result,

@@ -120,11 +120,12 @@ constexpr int kThinTY = 8;
 // duplicate endpoint planes equal their unique node's row (same inputs, same
 // operations) and are copied by duplicate_rows_kernel. Registers are bounded
 // for four CTAs per SM in float (64) and three in double (85).
-template <class C, class M, class Out, int TX, int TY, int TZ>
+template <class C, class M, class Out, int TX, int TY, int TZ, bool kResponse = false>
 __global__ void __launch_bounds__(TX * TY * TZ, sizeof(C) == 4 ? 4 : 3) maxwell_apply_kernel(Geom g, C d2, C kfac, C inv_volume,
                                                                         const M* __restrict__ mass,
                                                                         const double* __restrict__ v,
-                                                                        Out* __restrict__ out) {
+                                                                        Out* __restrict__ out,
+                                                                        const double* __restrict__ response) {
   wait_for_predecessor();
   constexpr int VX = TX + 2, VY = TY + 2, VZ = TZ + 2;   // nodes i0-1 .. i0+TX
   constexpr int CX = TX + 1, CY = TY + 1, CZ = TZ + 1;   // cells i0-1 .. i0+TX-1
@@ -138,7 +139,7 @@ __global__ void __launch_bounds__(TX * TY * TZ, sizeof(C) == 4 ? 4 : 3) maxwell_
   // The centre block and the first stencil's forward and backward rows of
   // this thread's node are requested into L2 before the staging below, so
   // the mass stream is in flight while v and the curls are staged.
-  {
+  if constexpr (!kResponse) {
     const int pi = i0 + int(threadIdx.x % TX), pj = j0 + int((threadIdx.x / TX) % TY),
               pk = k0 + int(threadIdx.x / (TX * TY));
     if (pi < g.nx && pj < g.ny && pk < g.nz) {
@@ -207,6 +208,20 @@ __global__ void __launch_bounds__(TX * TY * TZ, sizeof(C) == 4 ? 4 : 3) maxwell_
     curl2[1] = dz(p[0]) - dx(p[2]);
     curl2[2] = dx(p[1]) - dy(p[0]);
   }
+  // With smoothing (kResponse) the mass term is the smoothed response node
+  // field S^n(M S^n v) / V, read in the apply arithmetic (combine_image,
+  // maxwell_device.hpp:420-432).
+  if constexpr (kResponse) {
+    const long long at = g.node(i, j, k);
+    const long long row = i + (long long)g.inx * (j + (long long)g.iny * k);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const C m = C(response[c * nn + at]);
+      const C value = (C(1) * vs[c][lz + 1][ly + 1][lx + 1] + d2 * C(double(curl2[c]))) + kfac * m;
+      out[c * g.interior + row] = Out(value);
+    }
+    return;
+  }
   // Mass product: centre, then forward and backward blocks per stencil,
   // untransposed (apply_mass_matrix_node, mass_matrix_stencil.hpp:119-149).
   const long long at = g.node(i, j, k), es = g.mes;
@@ -268,6 +283,24 @@ __global__ void __launch_bounds__(kThreads) duplicate_rows_kernel(Geom g, Out* _
     const int ui = i == g.nx ? 0 : i, uj = j == g.ny ? 0 : j, uk = k == g.nz ? 0 : k;
     out[c * g.interior + i + (long long)g.inx * (j + (long long)g.iny * k)] =
         out[c * g.interior + ui + (long long)g.inx * (uj + (long long)g.iny * uk)];
+  }
+}
+
+// The mass response of a node field with filled ghosts over the interior
+// nodes 0..n, in arithmetic C, stored (M v)/V in double
+// (enqueue_mass_response of the smoothed schedule, maxwell_device.hpp:413-414).
+template <class C, class M>
+__global__ void __launch_bounds__(kThreads) mass_image_kernel(Geom g, C inv_volume, const M* __restrict__ mass,
+                                                             const double* __restrict__ v, double* __restrict__ out) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < g.interior;
+       t += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    compact_coordinates(g, t, i, j, k);
+    C mv[3];
+    mass_product<C>(g, mass, v, i, j, k, mv);
+    const long long at = g.node(i, j, k);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) out[c * g.nodes + at] = double(mv[c] * inv_volume);
   }
 }
 
@@ -574,6 +607,12 @@ struct SolverWorkspace {
   double* state = nullptr;
   double* pinned = nullptr;
   ArnoldiControl* ctl = nullptr;
+  // Energy-conserving smoothing: its plan and three node fields of scratch
+  // (allocated only when it is on).
+  SmoothingPlan smoothing;
+  double* smooth_a = nullptr;
+  double* smooth_b = nullptr;
+  double* smooth_image = nullptr;
   int batch;
   size_t scalar_bytes;
   // The Arnoldi-step loop as a graph (built for one mass pointer).
@@ -595,7 +634,7 @@ struct SolverWorkspace {
 };
 
 SolverWorkspace* solver_create(int precision, const Geom& g, int restart, double dt, double theta,
-                               double c, cudaError_t* err) {
+                               double c, const SmoothingPlan& smoothing, cudaError_t* err) {
   if (3 * g.interior >= (1LL << 31)) {  // the compact-index kernels use 32-bit arithmetic
     *err = cudaErrorInvalidValue;
     return nullptr;
@@ -620,6 +659,12 @@ SolverWorkspace* solver_create(int precision, const Geom& g, int restart, double
   auto alloc = [&](void** p, size_t bytes) {
     if (e == cudaSuccess) e = cudaMalloc(p, bytes);
   };
+  w->smoothing = smoothing;
+  if (smoothing.iterations > 0) {
+    alloc((void**)&w->smooth_a, 3 * g.nodes * sizeof(double));
+    alloc((void**)&w->smooth_b, 3 * g.nodes * sizeof(double));
+    alloc((void**)&w->smooth_image, 3 * g.nodes * sizeof(double));
+  }
   alloc(&w->basis, (size_t)(restart + 1) * w->count * w->scalar_bytes);
   alloc(&w->image, (size_t)w->count * w->scalar_bytes);
   alloc((void**)&w->x, w->count * sizeof(double));
@@ -649,6 +694,7 @@ void solver_destroy(SolverWorkspace* w) {
   cudaFree(w->basis); cudaFree(w->image); cudaFree(w->x); cudaFree(w->b); cudaFree(w->r);
   cudaFree(w->ximage); cudaFree(w->input); cudaFree(w->rhs); cudaFree(w->values);
   cudaFree(w->partials); cudaFree(w->state); cudaFree(w->ctl);
+  cudaFree(w->smooth_a); cudaFree(w->smooth_b); cudaFree(w->smooth_image);
   if (w->loop_exec) cudaGraphExecDestroy(w->loop_exec);
   if (w->loop_graph) cudaGraphDestroy(w->loop_graph);
   if (w->capture) cudaStreamDestroy(w->capture);
@@ -680,18 +726,43 @@ struct Solve {
     const Geom& g = w->g;
     launch_node_ghosts(g, w->input, 3, st, true);
     const double iv = g.inv_volume;
+    // Smoothed schedule (complete_apply_smoothed, maxwell_device.hpp:389-418):
+    // S^n(v), its mass response, S^n of that, then the fused kernel combines
+    // with the curl-curl term.
+    const double* response = nullptr;
+    if (w->smoothing.iterations > 0) {
+      const SmoothingPlan& sp = w->smoothing;
+      const bool dbl = sizeof(C) == 8;
+      if (err == cudaSuccess)
+        err = launch_smooth(dbl, g, sp.iterations, sp.op, sp.alpha, w->input, w->smooth_a, w->smooth_b, st);
+      mass_image_kernel<C, Mass><<<grid_for(g.interior, kThreads), kThreads, 0, st>>>(g, C(iv), mass, w->smooth_a,
+                                                                                     w->smooth_image);
+      count_launches(1);
+      launch_node_ghosts(g, w->smooth_image, 3, st);
+      if (err == cudaSuccess)
+        err = launch_smooth(dbl, g, sp.iterations, sp.op, sp.alpha, w->smooth_image, w->smooth_a, w->smooth_b, st);
+      response = w->smooth_a;
+    }
     // The thin tile where it still gives two CTAs per SM (148 SMs).
     const long long thin_tiles = (long long)((g.nx + kTX - 1) / kTX) * ((g.ny + kThinTY - 1) / kThinTY);
-    if (g.nz == 1 && thin_tiles >= 2 * 148) {
-      const unsigned tiles = unsigned(thin_tiles);
-      launch_programmatic(maxwell_apply_kernel<C, Mass, Out, kTX, kThinTY, 1>, tiles, kTX * kThinTY, 0, st, g,
-                          C(w->delta * w->delta), C(w->kfac), C(iv), mass, (const double*)w->input, out);
-    } else {
-      const unsigned tiles =
-          unsigned(((g.nx + kTX - 1) / kTX) * ((g.ny + kTY - 1) / kTY) * ((g.nz + kTZ - 1) / kTZ));
-      launch_programmatic(maxwell_apply_kernel<C, Mass, Out, kTX, kTY, kTZ>, tiles, kTX * kTY * kTZ, 0, st, g,
-                          C(w->delta * w->delta), C(w->kfac), C(iv), mass, (const double*)w->input, out);
-    }
+    const bool thin = g.nz == 1 && thin_tiles >= 2 * 148;
+    const unsigned tiles = thin ? unsigned(thin_tiles)
+                                : unsigned(((g.nx + kTX - 1) / kTX) * ((g.ny + kTY - 1) / kTY) *
+                                           ((g.nz + kTZ - 1) / kTZ));
+    const C d2 = C(w->delta * w->delta), kf = C(w->kfac), civ = C(iv);
+    const double* in = w->input;
+    if (thin && response)
+      launch_programmatic(maxwell_apply_kernel<C, Mass, Out, kTX, kThinTY, 1, true>, tiles, kTX * kThinTY, 0, st, g,
+                          d2, kf, civ, mass, in, out, response);
+    else if (thin)
+      launch_programmatic(maxwell_apply_kernel<C, Mass, Out, kTX, kThinTY, 1>, tiles, kTX * kThinTY, 0, st, g, d2,
+                          kf, civ, mass, in, out, response);
+    else if (response)
+      launch_programmatic(maxwell_apply_kernel<C, Mass, Out, kTX, kTY, kTZ, true>, tiles, kTX * kTY * kTZ, 0, st, g,
+                          d2, kf, civ, mass, in, out, response);
+    else
+      launch_programmatic(maxwell_apply_kernel<C, Mass, Out, kTX, kTY, kTZ>, tiles, kTX * kTY * kTZ, 0, st, g, d2,
+                          kf, civ, mass, in, out, response);
     const long long dup = (long long)g.inx * g.iny + (long long)g.inx * g.nz + (long long)g.ny * g.nz;
     launch_programmatic(duplicate_rows_kernel<Out>, grid_for(3 * dup, kThreads), kThreads, 0, st, g, out);
     count_launches(2);
@@ -883,7 +954,20 @@ struct Solve {
     const bool graph = loop_ready(mass);
     // Initial guess E^n (the copy of E into theta, maxwell_device.hpp:134-147) and the RHS.
     pack_storage_kernel<Fld><<<blocks(), kThreads, 0, s>>>(g, (const Fld*)e, w->x);
-    launch_rhs(P::id, g, w->delta, w->kfac, e, bcell, j, w->rhs, s);
+    if (w->smoothing.iterations > 0) {
+      // RHS with S^n(J-hat) (complete_rhs, maxwell_device.hpp:152-172): the
+      // current widened to double with its ghosts refilled, then smoothed in
+      // the field arithmetic.
+      const SmoothingPlan& sp = w->smoothing;
+      if (err == cudaSuccess) err = launch_widen(P::id, g, j, w->smooth_image, s);
+      launch_node_ghosts(g, w->smooth_image, 3, s);
+      if (err == cudaSuccess)
+        err = launch_smooth(P::id == TPICB200_PRECISION_DOUBLE, g, sp.iterations, sp.op, sp.alpha, w->smooth_image,
+                            w->smooth_a, w->smooth_b, s);
+      launch_rhs(P::id, g, w->delta, w->kfac, e, bcell, w->smooth_a, w->rhs, s, true);
+    } else {
+      launch_rhs(P::id, g, w->delta, w->kfac, e, bcell, j, w->rhs, s);
+    }
     pack_kernel<double><<<blocks(), kThreads, 0, s>>>(g, w->rhs, w->b);
     count_launches(2);
     check();
@@ -970,6 +1054,13 @@ int solver_solve(SolverWorkspace* w, const void* e, const void* bcell, const voi
     *err = solve.err;
   }
   return status;
+}
+
+cudaError_t solver_smooth(SolverWorkspace* w, const double* in, double* out, cudaStream_t s) {
+  const SmoothingPlan& sp = w->smoothing;
+  if (sp.iterations <= 0) return cudaErrorInvalidValue;
+  return launch_smooth(w->precision == TPICB200_PRECISION_DOUBLE, w->g, sp.iterations, sp.op, sp.alpha, in, out,
+                       w->smooth_b, s);
 }
 
 cudaError_t solver_mass_apply(SolverWorkspace* w, const void* mass, const double* in, double* out,

@@ -44,6 +44,7 @@ class Simulation:
     def __init__(self, case: Case, precision: str = "double", mass_kind: str = "scalar",
                  device: int = 0, gmres_restart: int = 30, gmres_max_iterations: int = 100,
                  keep_ids: bool = False, generate_on_device: bool = False, mass_layout: str = "stencil-major",
+                 smoothing: tuple = (0, 1.0, 0),
                  generate: bool = True):
         self.case = case
         self.lib = _lib.load()
@@ -60,8 +61,12 @@ class Simulation:
         grid = _lib.Grid(g.nx, g.ny, g.nz, g.lx, g.ly, g.lz)
         self.mass_layout = {"records": _lib.MASS_LAYOUT_RECORDS,
                             "stencil-major": _lib.MASS_LAYOUT_STENCIL_MAJOR}[mass_layout]
+        # Energy-conserving smoothing: (passes, Face7 centre weight, operator
+        # 0 Face7 / 1 Binomial27); on when passes > 0 and the weight < 1.
+        self.smoothing = tuple(smoothing)
         opts = _lib.Options(case.dt, case.theta, case.c, case.gmres_tol, gmres_restart,
-                            gmres_max_iterations, self.precision, max(counts), self.mass_layout)
+                            gmres_max_iterations, self.precision, max(counts), self.mass_layout,
+                            int(smoothing[0]), float(smoothing[1]), int(smoothing[2]))
         handle = C.c_void_p()
         _lib.check(self.lib.tpicb200_create(C.byref(grid), C.byref(opts), C.byref(handle)))
         self.ctx = handle
