@@ -201,6 +201,11 @@ def run_gpu(args) -> None:
         case = workload(args.scale, 4)
     nparticles = sum(case.grid.cells * sp.ppc for sp in case.species)
     g = case.grid
+    # Energy-conserving smoothing: passes,alpha,operator (0 Face7, 1 Binomial27).
+    smoothing = (0, 1.0, 0)
+    if args.smoothing:
+        n_, a_, o_ = args.smoothing.split(",")
+        smoothing = (int(n_), float(a_), int(o_))
     if args.deck:
         ppcs = "/".join(str(sp.ppc) for sp in case.species)
         workload_name = (f"deck {Path(args.deck).name}: {D.case_name(parsed)}, {g.nx}x{g.ny}x{g.nz} cells, "
@@ -220,7 +225,7 @@ def run_gpu(args) -> None:
         the energy drift (the simulation stays open for the caller)."""
         t_gen = time.perf_counter()
         sim = Simulation(case, precision=args.precision, mass_kind=mass_kind, device=local, generate_on_device=True,
-                         gmres_max_iterations=args.gmres_max_iterations)
+                         gmres_max_iterations=args.gmres_max_iterations, smoothing=smoothing)
         gen_s = time.perf_counter() - t_gen
         sim.prepare()
         w0 = sim.energy()
@@ -295,6 +300,9 @@ def run_gpu(args) -> None:
                            "precision": args.precision, "mass_matrix": args.mass_matrix, "dt": case.dt,
                            "theta": case.theta, "gmres_tol": case.gmres_tol,
                            "gmres_max_iterations": args.gmres_max_iterations, "l2": l2_note,
+                           "smoothing": ({"passes": smoothing[0], "alpha": smoothing[1],
+                                          "operator": ("face7", "binomial27")[smoothing[2]]}
+                                         if smoothing[0] > 0 and smoothing[1] < 1 else None),
                            "parallelism": f"replicas x{world}"},
                 "energy_drift": headline["energy_drift"], "gmres_iterations": headline["gmres_iterations"],
                 "gmres_host_waits": headline["gmres_host_waits"],
@@ -482,6 +490,8 @@ def main():
     ap.add_argument("--drift-cycles", type=int, default=100, help="cycles of the energy-drift run of each form")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "double"])
     ap.add_argument("--scale", type=int, default=128, help="cells per axis of the workload")
+    ap.add_argument("--smoothing", default="",
+                    help="energy-conserving smoothing as PASSES,ALPHA,OPERATOR (0 face7, 1 binomial27); off by default")
     ap.add_argument("--gmres-max-iterations", type=int, default=100,
                     help="GMRES step limit per solve (TPIC fixes 100, config/physics.hpp:20)")
     ap.add_argument("--deck", default=None,
