@@ -202,7 +202,7 @@ def run_gpu(args) -> None:
     nparticles = sum(case.grid.cells * sp.ppc for sp in case.species)
     g = case.grid
     # Energy-conserving smoothing: passes,alpha,operator (0 Face7, 1 Binomial27).
-    smoothing = (0, 1.0, 0)
+    smoothing = tuple(case.smoothing)  # a deck's own keys, unless --smoothing is given
     if args.smoothing:
         n_, a_, o_ = args.smoothing.split(",")
         smoothing = (int(n_), float(a_), int(o_))

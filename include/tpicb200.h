@@ -381,8 +381,8 @@ int tpicb200_cycle(tpicb200_context* ctx, tpicb200_state* state, int ncycles,
  * These entry points read the keys of the periodic, unsmoothed, one-rank
  * path and the cases built here: Uniform, Weibel, TwoStream and the Harris
  * sheet family (GEMHarris, GEM, GEMnoPert, DoubleGEM, DoubleGEMnoPert,
- * plasmoidChain). Other case names, wall boundaries, smoothing and Ampere
- * currents are rejected with TPICB200_INVALID_ARGUMENT.
+ * plasmoidChain), with energy-conserving smoothing. Other case names, wall
+ * boundaries and Ampere currents are rejected with TPICB200_INVALID_ARGUMENT.
  * ------------------------------------------------------------------------ */
 #define TPICB200_CASE_NAME_MAX 32
 typedef struct {
@@ -417,6 +417,12 @@ typedef struct {
   double two_stream_phase;                /* TwoStreamSeedPhase */
   int quiet_start;                        /* QuietStart: subcell centres */
   int ignored_keys;                       /* deck keys this front end does not read */
+  /* ECSimSmoothing = energy_conserving (config/physics.cpp:65-70): SmoothNiter
+   * (default 6), Smooth (default 1) and ECSimSmoothingOperator (face7 or
+   * binomial27, as TPICB200_SMOOTH_*); smooth_iterations is 0 when off. */
+  int smooth_iterations;
+  double smooth_alpha;
+  int smooth_operator;
 } tpicb200_deck;
 
 /* Fills *out from the deck text with TPIC's defaults for absent keys

@@ -260,6 +260,32 @@ def test_deck_reader_rules():
     assert d.weibel_growth_rate == 0.0
 
 
+def test_deck_reads_energy_conserving_smoothing():
+    text = DECK_TEXT + ("ECSimSmoothing = energy_conserving\nSmooth = 0.5\nSmoothNiter = 2\n"
+                        "ECSimSmoothingOperator = binomial27\n")
+    d = D.parse(text)
+    assert (d.smooth_iterations, d.smooth_alpha, d.smooth_operator) == (2, 0.5, 1)
+    assert D.to_case(d).smoothing == (2, 0.5, 1)
+    # Defaults: six Face7 passes; Smooth = 1 (the default) leaves smoothing off.
+    d = D.parse(DECK_TEXT + "ECSimSmoothing = energy_conserving\nSmooth = 0.25\n")
+    assert (d.smooth_iterations, d.smooth_alpha, d.smooth_operator) == (6, 0.25, 0)
+    d = D.parse(DECK_TEXT + "ECSimSmoothing = energy_conserving\n")
+    assert d.smooth_iterations == 0 and D.to_case(d).smoothing == (0, 1.0, 0)
+    assert D.parse(DECK_TEXT).smooth_iterations == 0
+
+
+@pytest.mark.parametrize("extra, message", [
+    ("ECSimSmoothing = energy_conserving\nSmooth = 1.5\n", "Smooth"),
+    ("ECSimSmoothing = energy_conserving\nSmoothNiter = -1\n", "SmoothNiter"),
+    ("ECSimSmoothing = energy_conserving\nECSimSmoothingOperator = face9\n", "ECSimSmoothingOperator"),
+])
+def test_deck_smoothing_errors(extra, message):
+    with pytest.raises(_lib.TpicError) as err:
+        D.parse(DECK_TEXT + extra)
+    assert err.value.status == _lib.INVALID_ARGUMENT
+    assert message in str(err.value)
+
+
 @pytest.mark.parametrize("edit, message", [
     (lambda t: t.replace("dt = 0.125", ""), "dt"),
     (lambda t: t.replace("Case = Weibel", "Case = Whistler"), "Whistler"),

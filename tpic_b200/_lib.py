@@ -87,7 +87,8 @@ class Deck(C.Structure):
                 ("deltay_hump", C.c_double), ("kx_hump", C.c_double), ("ky_hump", C.c_double),
                 ("weibel_mode_x", C.c_int), ("weibel_amplitude", C.c_double), ("weibel_growth_rate", C.c_double),
                 ("two_stream_mode_x", C.c_int), ("two_stream_amplitude", C.c_double),
-                ("two_stream_phase", C.c_double), ("quiet_start", C.c_int), ("ignored_keys", C.c_int)]
+                ("two_stream_phase", C.c_double), ("quiet_start", C.c_int), ("ignored_keys", C.c_int),
+                ("smooth_iterations", C.c_int), ("smooth_alpha", C.c_double), ("smooth_operator", C.c_int)]
 
 
 class CheckpointInfo(C.Structure):

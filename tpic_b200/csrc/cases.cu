@@ -4,7 +4,7 @@
 // one `key = value` per line, '#' starts a comment, the last assignment of a
 // key wins, a list holds whitespace-separated values of which the first ns
 // are used, a boolean is 0, 1, true or false, and a number is read in full.
-// It reads the keys of the periodic, unsmoothed, one-rank cycle and of the
+// It reads the keys of the periodic, one-rank cycle (smoothing included) and of the
 // cases built here; it counts the other keys and ignores them.
 //
 // The cases restate TPIC's analytic startup fields and loading profiles:
@@ -395,13 +395,31 @@ extern "C" int tpicb200_deck_parse(const char* text, tpicb200_deck* out) {
     d.ncycles = cfg.required<int>("ncycles");
     d.theta = 1.0;
     cfg.read_into("th", d.theta);
-    // Smoothing: only the unsmoothed cycle is built.
+    // Energy-conserving smoothing (config/physics.cpp:65-70; on when
+    // SmoothNiter > 0 and Smooth < 1).
     const std::string smoothing = cfg.text("ECSimSmoothing");
-    if (!smoothing.empty() && smoothing != "none")
-      throw DeckError{"ECSimSmoothing = " + smoothing + " is not built here (only none)"};
-    (void)cfg.has("Smooth");
-    (void)cfg.has("SmoothNiter");
-    (void)cfg.has("ECSimSmoothingOperator");
+    if (!smoothing.empty() && smoothing != "none" && smoothing != "energy_conserving")
+      throw DeckError{"ECSimSmoothing = " + smoothing + " (none or energy_conserving)"};
+    double smooth = 1.0;
+    int smooth_niter = 6;
+    cfg.read_into("Smooth", smooth);
+    cfg.read_into("SmoothNiter", smooth_niter);
+    const std::string op = cfg.text("ECSimSmoothingOperator");
+    if (!op.empty() && op != "face7" && op != "binomial27")
+      throw DeckError{"ECSimSmoothingOperator = " + op + " (face7 or binomial27)"};
+    d.smooth_iterations = 0;
+    d.smooth_alpha = 1.0;
+    d.smooth_operator = TPICB200_SMOOTH_FACE7;
+    if (smoothing == "energy_conserving") {
+      if (!std::isfinite(smooth) || smooth < 0 || smooth > 1)
+        throw DeckError{"energy-conserving smoothing requires 0 <= Smooth <= 1"};
+      if (smooth_niter < 0) throw DeckError{"energy-conserving smoothing requires SmoothNiter >= 0"};
+      if (smooth_niter > 0 && smooth < 1) {
+        d.smooth_iterations = smooth_niter;
+        d.smooth_alpha = smooth;
+        d.smooth_operator = op == "binomial27" ? TPICB200_SMOOTH_BINOMIAL27 : TPICB200_SMOOTH_FACE7;
+      }
+    }
     d.ns = cfg.required<int>("ns");
     if (d.ns < 1 || d.ns > TPICB200_MAX_SPECIES) throw DeckError{"ns must be between 1 and 8"};
     int test_species = 0;

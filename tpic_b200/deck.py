@@ -111,7 +111,8 @@ def to_case(deck: _lib.Deck, seed: int = 0, ncycles: int | None = None) -> Case:
     """The run the deck describes, ready for Simulation (and the oracle)."""
     return Case(grid=grid_of(deck), species=species_of(deck), dt=deck.dt, theta=deck.theta, c=deck.c,
                 gmres_tol=deck.gmres_tol, ncycles=deck.ncycles if ncycles is None else ncycles,
-                fields=initial_fields(deck), seed=seed, deck=deck)
+                fields=initial_fields(deck), seed=seed, deck=deck,
+                smoothing=(deck.smooth_iterations, deck.smooth_alpha, deck.smooth_operator))
 
 
 def deck_of(case: Case) -> _lib.Deck:

@@ -201,3 +201,6 @@ class Case:
     fields: FieldInit = field(default_factory=FieldInit)
     seed: int = 0
     deck: object = None   # the tpicb200_deck it came from (tpic_b200.deck), if any
+    # Energy-conserving smoothing (passes, Face7 centre weight, operator 0
+    # Face7 / 1 Binomial27); off with 0 passes.
+    smoothing: tuple = (0, 1.0, 0)

@@ -44,7 +44,7 @@ class Simulation:
     def __init__(self, case: Case, precision: str = "double", mass_kind: str = "scalar",
                  device: int = 0, gmres_restart: int = 30, gmres_max_iterations: int = 100,
                  keep_ids: bool = False, generate_on_device: bool = False, mass_layout: str = "stencil-major",
-                 smoothing: tuple = (0, 1.0, 0),
+                 smoothing: tuple | None = None,
                  generate: bool = True):
         self.case = case
         self.lib = _lib.load()
@@ -63,7 +63,8 @@ class Simulation:
                             "stencil-major": _lib.MASS_LAYOUT_STENCIL_MAJOR}[mass_layout]
         # Energy-conserving smoothing: (passes, Face7 centre weight, operator
         # 0 Face7 / 1 Binomial27); on when passes > 0 and the weight < 1.
-        self.smoothing = tuple(smoothing)
+        smoothing = tuple(case.smoothing if smoothing is None else smoothing)
+        self.smoothing = smoothing
         opts = _lib.Options(case.dt, case.theta, case.c, case.gmres_tol, gmres_restart,
                             gmres_max_iterations, self.precision, max(counts), self.mass_layout,
                             int(smoothing[0]), float(smoothing[1]), int(smoothing[2]))
