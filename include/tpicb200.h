@@ -254,9 +254,13 @@ int tpicb200_sort_binned(tpicb200_context* ctx, const tpicb200_particles* in, co
  * allocation's implicit device synchronisation). Limits: at most
  * TPICB200_SORT_STATIC_MAX_RECORDS records on grids of at most
  * TPICB200_SORT_STATIC_MAX_BINS bins; larger inputs return
- * TPICB200_CAPACITY_EXCEEDED and enqueue nothing. The first call on each
- * device (with that device current) resolves the array's address; make that
- * call before any stream capture. Every call shares the one array: calls
+ * TPICB200_CAPACITY_EXCEEDED and enqueue nothing. The calling thread's
+ * current CUDA context is used (the current device's primary context when
+ * none is current). The first call in each context resolves the array's
+ * address in that context; make that call before any stream capture. The
+ * address is cached per context id, so a context created later (after
+ * cudaDeviceReset, or a driver context made current) resolves its own.
+ * Every call shares the one array: calls
  * that overlap in time (on other streams or host threads) race on it and
  * must be ordered on one stream. precision: TPICB200_PRECISION_* (the
  * velocity type of the records). */
@@ -274,6 +278,14 @@ int tpicb200_sort_static(const tpicb200_grid* grid, int precision, const tpicb20
  * (ecsim/fields/node_smoothing.hpp:24-52). Returns TPICB200_INVALID_STATE
  * when the context has no smoothing; in and out must not alias. */
 int tpicb200_smooth(tpicb200_context* ctx, const double* in, double* out, tpicb200_stream stream);
+
+/* The context's own invalid counter (the one entry points use when their
+ * `invalid` argument is NULL, and the one tpicb200_cycle and the solver's
+ * smoothing passes raise): *count receives its value once the work enqueued
+ * on `stream` so far has completed; clear != 0 then zeroes it (stream
+ * ordered). TPIC's callers read their `unsigned* invalid` flag the same way
+ * after the enqueued work (simulation/driver/pipeline.hpp:145-146). Host-blocking. */
+int tpicb200_read_invalid(tpicb200_context* ctx, uint32_t* count, int clear, tpicb200_stream stream);
 
 /* Zero J (node field) and the mass records. Replaces enqueue_clear_mass_matrix
  * (ecsim/mass_matrix/mass_matrix_deposition_device.hpp:107-121) and the moment clear. */

@@ -105,3 +105,30 @@ def test_smoothed_cycles_match_oracle_fp64(op):
     g = case.grid
     e_gpu, e_cpu = interior_nodes(g, sim.field("e").cpu().numpy()), interior_nodes(g, oc.e)
     assert np.abs(e_gpu - e_cpu).max() <= 3e-10 * np.abs(e_cpu).max() + 3e-12
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_smoothing_flags_a_nonfinite_value(torch_cuda, precision):
+    """A NaN reaching a smoothing pass raises the context's invalid counter,
+    as the reference's pass flags a nonfinite stored value
+    (node_smoothing_device.hpp:30-36); a finite field leaves it at zero."""
+    from gpu_helpers import StageContext
+    g = GRID
+    rng = np.random.default_rng(3)
+    f = periodic_node_field(g, rng.normal(size=(3, g.nz, g.ny, g.nx)))
+    ctx = StageContext(g, precision, smoothing=(2, 0.5, 0))
+    count = C.c_uint32(99)
+    src = ctx.field(f, np.float64)
+    out = torch_cuda.zeros_like(src)
+    assert ctx.lib.tpicb200_smooth(ctx.ctx, src.data_ptr(), out.data_ptr(), ctx.stream) == 0
+    assert ctx.lib.tpicb200_read_invalid(ctx.ctx, C.byref(count), 1, ctx.stream) == 0
+    assert count.value == 0
+    bad = f.copy()
+    nodes = (g.nx + 3) * (g.ny + 3) * (g.nz + 3)
+    bad[nodes + 3 + (g.nx + 3) * (2 + (g.ny + 3) * 2)] = np.nan  # component y, an interior node
+    src = ctx.field(bad, np.float64)
+    assert ctx.lib.tpicb200_smooth(ctx.ctx, src.data_ptr(), out.data_ptr(), ctx.stream) == 0
+    assert ctx.lib.tpicb200_read_invalid(ctx.ctx, C.byref(count), 1, ctx.stream) == 0
+    assert count.value > 0
+    assert ctx.lib.tpicb200_read_invalid(ctx.ctx, C.byref(count), 0, ctx.stream) == 0
+    assert count.value == 0

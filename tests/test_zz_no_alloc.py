@@ -71,3 +71,76 @@ def test_static_sort_rejects_oversized_inputs(torch_cuda):
                                       dummy.data_ptr(), None, None)
     assert status == _lib.CAPACITY_EXCEEDED
     assert "TPICB200_SORT_STATIC_MAX_RECORDS" in lib.tpicb200_last_error().decode()
+
+
+RESET_SCRIPT = r'''
+import ctypes as C, sys
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+from tpic_b200 import _lib
+from tpic_b200.plasma import GridSpec
+
+lib = _lib.load()
+rt = C.CDLL("libcudart.so.12")
+H2D, D2H = 1, 2
+g = GridSpec(10, 9, 8, 1.0, 1.0, 1.0)
+grid = _lib.Grid(g.nx, g.ny, g.nz, 1.0, 1.0, 1.0)
+bins = (g.nx + 4) * (g.ny + 4) * (g.nz + 4)
+
+
+def dalloc(nbytes):
+    ptr = C.c_void_p()
+    assert rt.cudaMalloc(C.byref(ptr), C.c_size_t(max(nbytes, 8))) == 0
+    return ptr
+
+
+def run(n, seed):
+    rng = np.random.default_rng(seed)
+    keys = g.encode(rng.integers(0, g.nx, n), rng.integers(0, g.ny, n), rng.integers(0, g.nz, n)).astype(np.int32)
+    host = {"rx": rng.random(n), "ry": rng.random(n), "rz": rng.random(n), "u": rng.random(n).astype(np.float32),
+            "v": rng.random(n).astype(np.float32), "w": rng.random(n).astype(np.float32), "q": rng.random(n),
+            "cell": keys}
+    src, dst = _lib.Particles(), _lib.Particles()
+    outs = {}
+    for k, a in host.items():
+        d = dalloc(a.nbytes)
+        assert rt.cudaMemcpy(d, a.ctypes.data_as(C.c_void_p), C.c_size_t(a.nbytes), H2D) == 0
+        setattr(src, k, d.value)
+        o = dalloc(a.nbytes)
+        setattr(dst, k, o.value)
+        outs[k] = o
+    src.count = n
+    counts, offsets = dalloc(4 * bins), dalloc(4 * (bins + 1))
+    status = lib.tpicb200_sort_static(C.byref(grid), 1, C.byref(src), C.byref(dst), counts, offsets, None, None)
+    assert status == 0, lib.tpicb200_last_error()
+    assert rt.cudaDeviceSynchronize() == 0
+    order = np.argsort(keys, kind="stable")
+    for k, o in outs.items():
+        got = np.empty_like(host[k])
+        assert rt.cudaMemcpy(got.ctypes.data_as(C.c_void_p), o, C.c_size_t(got.nbytes), D2H) == 0
+        assert np.array_equal(got, host[k][order]), k
+    got = np.empty(bins + 1, dtype=np.uint32)
+    assert rt.cudaMemcpy(got.ctypes.data_as(C.c_void_p), offsets, C.c_size_t(got.nbytes), D2H) == 0
+    assert np.array_equal(got, np.concatenate([[0], np.cumsum(np.bincount(keys, minlength=bins))]))
+
+
+run(70000, 5)
+assert rt.cudaDeviceReset() == 0  # ends this process's context; the next call runs in a new one
+run(50001, 6)
+print("ok")
+'''
+
+
+def test_static_sort_after_a_device_reset(torch_cuda, tmp_path):
+    """The scratch array's address is per CUDA context. After cudaDeviceReset
+    the next call runs in a new primary context and must resolve the address
+    there again rather than reuse the old one (fresh process; the buffers are
+    allocated by the test, the sort itself allocates nothing)."""
+    import subprocess
+    import sys
+    from pathlib import Path
+    script = tmp_path / "reset.py"
+    script.write_text(RESET_SCRIPT)
+    root = str(Path(__file__).resolve().parents[1])
+    done = subprocess.run([sys.executable, str(script), root], capture_output=True, text=True, timeout=300)
+    assert done.returncode == 0 and done.stdout.strip().endswith("ok"), done.stdout + done.stderr

@@ -209,6 +209,7 @@ int tpicb200_create(const tpicb200_grid* grid, const tpicb200_options* options, 
   alloc((void**)&ctx->moments, moment_floats(ctx->g) * (options->precision == TPICB200_PRECISION_MIXED ? 4 : 8));
   if (e == cudaSuccess) e = cudaMallocHost((void**)&ctx->pinned, (2 + 5 * TPICB200_MAX_SPECIES + 2) * 8);
   if (e == cudaSuccess) e = cudaMemset(ctx->invalid, 0, 4);
+  if (e == cudaSuccess && ctx->solver) solver_set_invalid(ctx->solver, ctx->invalid);
   for (auto& ev : ctx->events)
     if (e == cudaSuccess) e = cudaEventCreate(&ev);
   if (e != cudaSuccess) {
@@ -768,6 +769,15 @@ static int read_invalid(tpicb200_context* ctx, cudaStream_t s, uint32_t* value) 
   if (err == cudaSuccess) err = cudaStreamSynchronize(s);
   if (err != cudaSuccess) return cuda_status(err, "invalid-flag readback failed");
   std::memcpy(value, ctx->pinned, 4);
+  return TPICB200_SUCCESS;
+}
+
+int tpicb200_read_invalid(tpicb200_context* ctx, uint32_t* count, int clear, tpicb200_stream stream) {
+  if (int s = check_ctx(ctx)) return s;
+  if (!count) return fail(TPICB200_INVALID_ARGUMENT, "read_invalid needs an output");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (int r = read_invalid(ctx, s, count)) return r;
+  if (clear) return cuda_status(cudaMemsetAsync(ctx->invalid, 0, 4, s), "invalid-counter clear failed");
   return TPICB200_SUCCESS;
 }
 

@@ -321,7 +321,8 @@ cudaError_t launch_rhs(int precision, const Geom& g, double delta, double kfac, 
 // double node field, in arithmetic C with each product and sum rounded on
 // its own (no contraction) in the reference's order. Op 0 Face7: alpha *
 // centre + beta * faces; op 1 Binomial27: (8 centre + 4 faces + 2 edges +
-// corners) * (1/64).
+// corners) * (1/64). A nonfinite result counts in *invalid (when given), as
+// the reference's kernel flags it (node_smoothing_device.hpp:30-36).
 __device__ __forceinline__ float rn_mul(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ double rn_mul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ float rn_add(float a, float b) { return __fadd_rn(a, b); }
@@ -329,7 +330,7 @@ __device__ __forceinline__ double rn_add(double a, double b) { return __dadd_rn(
 
 template <class C, int Op>
 __global__ void __launch_bounds__(256) smooth_kernel(Geom g, C alpha, C beta, const double* __restrict__ src,
-                                                     double* __restrict__ dst) {
+                                                     double* __restrict__ dst, uint32_t* invalid) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 3 * g.interior;
        t += (long long)gridDim.x * blockDim.x) {
     const int c = int(t / g.interior);
@@ -357,6 +358,7 @@ __global__ void __launch_bounds__(256) smooth_kernel(Geom g, C alpha, C beta, co
       value = rn_mul(sum, C(1) / C(64));
     }
     dst[c * g.nodes + g.node(i, j, k)] = double(value);
+    if (invalid && !isfinite(value)) atomicAdd(invalid, 1u);
   }
 }
 
@@ -365,9 +367,10 @@ __global__ void __launch_bounds__(256) smooth_kernel(Geom g, C alpha, C beta, co
 // ghosts must be filled; the passes alternate between out and tmp so that
 // the last lands in out, with the ghosts refilled between passes. Neither
 // out nor tmp may alias src. double_arithmetic selects the pass arithmetic
-// (the reference's Arithmetic / Compute::Electric).
+// (the reference's Arithmetic / Compute::Electric). invalid (may be null)
+// counts nonfinite smoothed values.
 cudaError_t launch_smooth(bool double_arithmetic, const Geom& g, int niter, int op, double alpha,
-                          const double* src, double* out, double* tmp, cudaStream_t s) {
+                          const double* src, double* out, double* tmp, uint32_t* invalid, cudaStream_t s) {
   if (niter <= 0 || src == out || src == tmp || out == tmp) return cudaErrorInvalidValue;
   const unsigned blocks = grid_for(3 * g.interior, 256);
   const double* from = src;
@@ -375,12 +378,12 @@ cudaError_t launch_smooth(bool double_arithmetic, const Geom& g, int niter, int 
     double* to = (niter - pass) % 2 == 0 ? out : tmp;
     if (double_arithmetic) {
       const double beta = (1.0 - alpha) / 6.0;
-      if (op == 0) smooth_kernel<double, 0><<<blocks, 256, 0, s>>>(g, alpha, beta, from, to);
-      else smooth_kernel<double, 1><<<blocks, 256, 0, s>>>(g, alpha, beta, from, to);
+      if (op == 0) smooth_kernel<double, 0><<<blocks, 256, 0, s>>>(g, alpha, beta, from, to, invalid);
+      else smooth_kernel<double, 1><<<blocks, 256, 0, s>>>(g, alpha, beta, from, to, invalid);
     } else {
       const float a = float(alpha), beta = (1.0f - a) / 6.0f;
-      if (op == 0) smooth_kernel<float, 0><<<blocks, 256, 0, s>>>(g, a, beta, from, to);
-      else smooth_kernel<float, 1><<<blocks, 256, 0, s>>>(g, a, beta, from, to);
+      if (op == 0) smooth_kernel<float, 0><<<blocks, 256, 0, s>>>(g, a, beta, from, to, invalid);
+      else smooth_kernel<float, 1><<<blocks, 256, 0, s>>>(g, a, beta, from, to, invalid);
     }
     count_launches(1);
     launch_node_ghosts(g, to, 3, s);

@@ -146,7 +146,7 @@ cudaError_t launch_assemble_moments(int precision, const Geom& g, const void* mo
 cudaError_t launch_node_ghosts(const Geom& g, double* f, int components, cudaStream_t s,
                                bool programmatic = false);
 cudaError_t launch_smooth(bool double_arithmetic, const Geom& g, int niter, int op, double alpha,
-                          const double* src, double* out, double* tmp, cudaStream_t s);
+                          const double* src, double* out, double* tmp, uint32_t* invalid, cudaStream_t s);
 cudaError_t launch_widen(int precision, const Geom& g, const void* in, double* out, cudaStream_t s);
 cudaError_t launch_cell_ghosts(int precision, const Geom& g, void* f, cudaStream_t s);
 cudaError_t launch_cell_to_node(int precision, const Geom& g, const void* cellf, void* node,
@@ -182,6 +182,8 @@ SolverWorkspace* solver_create(int precision, const Geom& g, int restart, double
 // arithmetic of the precision mode, with the solver's scratch.
 cudaError_t solver_smooth(SolverWorkspace* w, const double* in, double* out, cudaStream_t s);
 void solver_destroy(SolverWorkspace* w);
+// The counter the solver's smoothing passes raise on a nonfinite value.
+void solver_set_invalid(SolverWorkspace* w, uint32_t* invalid);
 int solver_solve(SolverWorkspace* w, const void* e, const void* bcell, const void* j,
                  const void* mass, double* etheta, tpicb200_gmres_result* result,
                  int max_iterations, double tol, cudaStream_t s, cudaError_t* err);

@@ -589,6 +589,7 @@ __global__ void arnoldi_end_kernel(ArnoldiControl* ctl, const double* status, cu
 
 struct SolverWorkspace {
   int precision;
+  uint32_t* invalid = nullptr;  // the context's invalid counter (smoothing passes)
   Geom g;
   int restart;
   double dt, theta, c, delta, kfac;
@@ -734,13 +735,13 @@ struct Solve {
       const SmoothingPlan& sp = w->smoothing;
       const bool dbl = sizeof(C) == 8;
       if (err == cudaSuccess)
-        err = launch_smooth(dbl, g, sp.iterations, sp.op, sp.alpha, w->input, w->smooth_a, w->smooth_b, st);
+        err = launch_smooth(dbl, g, sp.iterations, sp.op, sp.alpha, w->input, w->smooth_a, w->smooth_b, w->invalid, st);
       mass_image_kernel<C, Mass><<<grid_for(g.interior, kThreads), kThreads, 0, st>>>(g, C(iv), mass, w->smooth_a,
                                                                                      w->smooth_image);
       count_launches(1);
       launch_node_ghosts(g, w->smooth_image, 3, st);
       if (err == cudaSuccess)
-        err = launch_smooth(dbl, g, sp.iterations, sp.op, sp.alpha, w->smooth_image, w->smooth_a, w->smooth_b, st);
+        err = launch_smooth(dbl, g, sp.iterations, sp.op, sp.alpha, w->smooth_image, w->smooth_a, w->smooth_b, w->invalid, st);
       response = w->smooth_a;
     }
     // The thin tile where it still gives two CTAs per SM (148 SMs).
@@ -963,7 +964,7 @@ struct Solve {
       launch_node_ghosts(g, w->smooth_image, 3, s);
       if (err == cudaSuccess)
         err = launch_smooth(P::id == TPICB200_PRECISION_DOUBLE, g, sp.iterations, sp.op, sp.alpha, w->smooth_image,
-                            w->smooth_a, w->smooth_b, s);
+                            w->smooth_a, w->smooth_b, w->invalid, s);
       launch_rhs(P::id, g, w->delta, w->kfac, e, bcell, w->smooth_a, w->rhs, s, true);
     } else {
       launch_rhs(P::id, g, w->delta, w->kfac, e, bcell, j, w->rhs, s);
@@ -1056,11 +1057,13 @@ int solver_solve(SolverWorkspace* w, const void* e, const void* bcell, const voi
   return status;
 }
 
+void solver_set_invalid(SolverWorkspace* w, uint32_t* invalid) { w->invalid = invalid; }
+
 cudaError_t solver_smooth(SolverWorkspace* w, const double* in, double* out, cudaStream_t s) {
   const SmoothingPlan& sp = w->smoothing;
   if (sp.iterations <= 0) return cudaErrorInvalidValue;
   return launch_smooth(w->precision == TPICB200_PRECISION_DOUBLE, w->g, sp.iterations, sp.op, sp.alpha, in, out,
-                       w->smooth_b, s);
+                       w->smooth_b, w->invalid, s);
 }
 
 cudaError_t solver_mass_apply(SolverWorkspace* w, const void* mass, const double* in, double* out,

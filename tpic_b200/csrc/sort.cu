@@ -18,6 +18,7 @@
 // test the sort's own flag) and is reported through *invalid.
 #include "kernels.cuh"
 
+#include <cuda.h>
 #include <mutex>
 
 namespace tpicb200 {
@@ -893,28 +894,74 @@ constexpr long long kStaticWords = kStaticRecords + kStaticBins + kStaticScanWor
 
 static __device__ __align__(256) uint32_t g_static_scratch[kStaticWords];
 
-constexpr int kStaticMaxDevices = 64;
+// The array's address is resolved once per CUDA context: a device's primary
+// context, a driver context a caller made current, or the primary context
+// created again after cudaDeviceReset each hold their own copy of the array.
+// A context's id (cuCtxGetId) is unique for the life of the process, so a
+// context created after another was destroyed never reuses its cached
+// address. The driver functions are fetched through the runtime, so the
+// library needs no link against the driver library.
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+constexpr int kStaticMaxContexts = 64;
 std::mutex g_static_mutex;
-uint32_t* g_static_address[kStaticMaxDevices] = {};
+struct StaticAddress {
+  unsigned long long context_id;
+  uint32_t* address;
+};
+StaticAddress g_static_address[kStaticMaxContexts] = {};
+int g_static_used = 0;
+CtxGetCurrentFn g_ctx_get_current = nullptr;
+CtxGetIdFn g_ctx_get_id = nullptr;
+
+cudaError_t current_context_id(unsigned long long* id) {
+  CUcontext ctx = nullptr;
+  if (g_ctx_get_current(&ctx) != CUDA_SUCCESS) return cudaErrorInvalidResourceHandle;
+  if (!ctx) return cudaErrorContextIsDestroyed;
+  return g_ctx_get_id(ctx, id) == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidResourceHandle;
+}
 
 }  // namespace
 
 long long sort_static_scratch_bytes() { return kStaticWords * 4; }
 
 cudaError_t sort_static_setup(uint32_t** scratch) {
-  int device = 0;
-  cudaError_t e = cudaGetDevice(&device);
-  if (e != cudaSuccess) return e;
-  if (device < 0 || device >= kStaticMaxDevices) return cudaErrorInvalidDevice;
   std::lock_guard<std::mutex> lock(g_static_mutex);
-  if (!g_static_address[device]) {
-    // Once per device, with that device current: the array's device address.
-    uint32_t* ptr = nullptr;
-    e = cudaGetSymbolAddress((void**)&ptr, g_static_scratch);
-    if (e != cudaSuccess) return e;
-    g_static_address[device] = ptr;
+  if (!g_ctx_get_current || !g_ctx_get_id) {
+    cudaDriverEntryPointQueryResult found = cudaDriverEntryPointSymbolNotFound;
+    void* fn = nullptr;
+    cudaError_t e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &found);
+    if (e != cudaSuccess || found != cudaDriverEntryPointSuccess || !fn) return e != cudaSuccess ? e : cudaErrorNotSupported;
+    g_ctx_get_current = reinterpret_cast<CtxGetCurrentFn>(fn);
+    e = cudaGetDriverEntryPoint("cuCtxGetId", &fn, cudaEnableDefault, &found);
+    if (e != cudaSuccess || found != cudaDriverEntryPointSuccess || !fn) return e != cudaSuccess ? e : cudaErrorNotSupported;
+    g_ctx_get_id = reinterpret_cast<CtxGetIdFn>(fn);
   }
-  *scratch = g_static_address[device];
+  unsigned long long id = 0;
+  cudaError_t e = current_context_id(&id);
+  uint32_t* fresh = nullptr;
+  if (e == cudaErrorContextIsDestroyed) {
+    // No context is current yet: resolving the symbol initialises the
+    // current device's primary context and makes it current.
+    e = cudaGetSymbolAddress((void**)&fresh, g_static_scratch);
+    if (e != cudaSuccess) return e;
+    e = current_context_id(&id);
+  }
+  if (e != cudaSuccess) return e;
+  for (int i = 0; i < g_static_used; ++i)
+    if (g_static_address[i].context_id == id) {
+      *scratch = g_static_address[i].address;
+      return cudaSuccess;
+    }
+  // Once per context, with that context current: the array's device address.
+  if (!fresh) {
+    e = cudaGetSymbolAddress((void**)&fresh, g_static_scratch);
+    if (e != cudaSuccess) return e;
+  }
+  // Contexts beyond the table's size replace the oldest entry.
+  const int slot = g_static_used < kStaticMaxContexts ? g_static_used++ : int(id % kStaticMaxContexts);
+  g_static_address[slot] = {id, fresh};
+  *scratch = fresh;
   return cudaSuccess;
 }
 
