@@ -220,14 +220,42 @@ def run_gpu(args) -> None:
             dist.barrier()
         torch.cuda.synchronize()
 
-    def timed_form(mass_kind, sample_clocks):
+    def bootstrap_errors(sim, reference):
+        """Max and RMS relative error of the bootstrap deposition's mass
+        entries and J-hat against the FP64 moment form's on the same state."""
+        if reference is None:
+            return {}
+        out = {}
+        for name in ("mass", "j"):
+            got = sim.field(name).double()
+            want = reference[name]
+            diff = got - want
+            out[f"{name}_rel_err_max"] = float(diff.abs().max() / want.abs().max())
+            out[f"{name}_rel_err_rms"] = float(diff.square().mean().sqrt() / want.square().mean().sqrt())
+            del got, diff
+        torch.cuda.synchronize()
+        return out
+
+    def timed_form(mass_kind, sample_clocks, precision=None, reference=None, keep=False):
         """Warm-up, the timed cycles, then more cycles up to --drift-cycles for
-        the energy drift (the simulation stays open for the caller)."""
+        the energy drift (the simulation stays open for the caller). With
+        `reference` (bootstrap mass and J of the FP64 moment form) the
+        bootstrap deposition's errors against it are measured; keep=True
+        returns this form's own bootstrap mass and J (double) for that."""
+        precision = precision or args.precision
         t_gen = time.perf_counter()
-        sim = Simulation(case, precision=args.precision, mass_kind=mass_kind, device=local, generate_on_device=True,
+        sim = Simulation(case, precision=precision, mass_kind=mass_kind, device=local, generate_on_device=True,
                          gmres_max_iterations=args.gmres_max_iterations, smoothing=smoothing)
+        if precision == "double" and args.precision == "mixed":
+            # The same state as the mixed forms: their FP32 velocities, widened.
+            for s in range(len(case.species)):
+                for k in ("u", "v", "w"):
+                    t = sim.slots[s][sim.state.current[s]][k]
+                    t.copy_(t.float().double())
         gen_s = time.perf_counter() - t_gen
         sim.prepare()
+        errors = bootstrap_errors(sim, reference)
+        own = {name: sim.field(name).double().clone() for name in ("mass", "j")} if keep else None
         w0 = sim.energy()
         total0 = w0[0] + w0[1] + sum(w0[2 + 5 * s] for s in range(len(case.species)))
         history = sim.run(args.warmup)
@@ -253,10 +281,26 @@ def run_gpu(args) -> None:
                                 for k, name in enumerate(stage_names)},
                   "gmres_iterations": float(np.mean([r.gmres_iterations for r in reports])),
                   "gmres_host_waits": float(np.mean([r.gmres_host_waits for r in reports])),
-                  "launches": int(launches), "generation_s": gen_s}
+                  "launches": int(launches), "generation_s": gen_s, **errors}
+        if keep:
+            return sim, result, clocks, own
         return sim, result, clocks
 
-    sim, headline, clocks = timed_form(args.mass_matrix, True)
+    def sweep_entry(form, precision, result):
+        keys = ("value", "ms_per_step", "energy_drift", "gmres_iterations", "mass_rel_err_max", "mass_rel_err_rms",
+                "j_rel_err_max", "j_rel_err_rms")
+        return {"mass_matrix": form, "precision": precision, **{k: result[k] for k in keys if k in result}}
+
+    # ---- the precision sweep's reference: the FP64 moment form ------------------
+    sweep, reference = [], None
+    if args.sweep and not args.deck:
+        ref_sim, ref_result, _, reference = timed_form("moments-f64", False, precision="double", keep=True)
+        ref_sim.close()
+        del ref_sim
+        sweep.append(sweep_entry("moments-f64", "double",
+                                 {**ref_result, "mass_rel_err_max": 0.0, "j_rel_err_max": 0.0}))
+
+    sim, headline, clocks = timed_form(args.mass_matrix, True, reference=reference)
     value = headline["value"]
     seconds = headline["ms_per_step"] * args.steps / 1e3
     lib = sim.lib
@@ -271,6 +315,9 @@ def run_gpu(args) -> None:
     roofline = {"kernel": dominant, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "peak_source": peak_kind,
                 "traffic": traffic, "algorithmic_bytes": dk["bytes"],
+                "algorithmic_basis": "positions 24 B + velocities 3 x 4 B + charge 8 B per particle, "
+                                     "mass assembly fused into the same pass",
+                "record_bytes": dk.get("record_bytes"),
                 "all_kernels": {k: {"ms": v["ms"], "GB/s": v["bytes"] / (v["ms"] / 1e3) / 1e9,
                                     "frac": v["bytes"] / (v["ms"] / 1e3) / 1e9 / hbm} for k, v in kernels.items()}}
 
@@ -282,11 +329,24 @@ def run_gpu(args) -> None:
     # ---- the plain FP32 CUDA-core form on the same workload -------------------------
     comparison = None
     if args.compare != "none":
-        other, plain, _ = timed_form(args.compare, False)
+        other, plain, _ = timed_form(args.compare, False, reference=reference)
         other.close()
         del other
         comparison = {"mass_matrix": args.compare, **plain,
                       "speedup": value / plain["value"]}
+    if reference is not None:
+        sweep.append(sweep_entry(args.mass_matrix, args.precision, headline))
+        if comparison is not None:
+            sweep.append(sweep_entry(args.compare, args.precision, plain))
+        for form in ("scalar", "tf32", "bf16x3"):
+            if form in (args.mass_matrix, args.compare):
+                continue
+            extra_sim, extra, _ = timed_form(form, False, reference=reference)
+            extra_sim.close()
+            del extra_sim
+            sweep.append(sweep_entry(form, args.precision, extra))
+        del reference
+        torch.cuda.empty_cache()
 
     record_bytes = 24 + 3 * (4 if args.precision == "mixed" else 8) + 8 + 4
     l2_note = ("inputs larger than L2" if nparticles * record_bytes > 126e6 else
@@ -308,7 +368,10 @@ def run_gpu(args) -> None:
                 "gmres_host_waits": headline["gmres_host_waits"],
                 "stages_ms": headline["stages_ms"], "plain_fp32_form": comparison,
                 "clocks": clocks.summary(), "e2e": e2e, "gpu_launches": headline["launches"],
-                "roofline": roofline, "generation_s": headline["generation_s"]}
+                "roofline": roofline, "cycle_roofline": cycle_roofline(headline, nparticles, g, args, hbm),
+                "generation_s": headline["generation_s"]}
+        if sweep:
+            line["sweep"] = sweep
         if not args.no_cpu_baseline and not args.deck:
             cb = cpu_oracle_rate(args.cpu_scale, 4, 2, 0)
             line["cpu_baseline"] = {"value": cb["particles"] * cb["cycles"] / cb["seconds"], "unit": UNIT,
@@ -389,9 +452,13 @@ def stage_kernel_times(sim, args, stream, repeats: int = 5) -> dict:
         return total / repeats
 
     clear = lambda: _lib.check(lib.tpicb200_clear_moments(sim.ctx, st.j, st.mass, s_))
-    out["deposit"] = {"ms": timed_after(clear, deposit),
-                      "bytes": n_total * (24 + 3 * vb + 8 + 4) + (moment_bytes if tc_form else
-                                                                  nodes * (126 + 3) * fb)}
+    # Algorithmic bytes per particle: positions, velocities and charge (the
+    # current's inputs; the mass assembly reads a subset of them in the same
+    # pass). record_bytes adds what the kernels move beyond that: the key,
+    # and the per-cell moments or the node outputs.
+    out["deposit"] = {"ms": timed_after(clear, deposit), "bytes": n_total * (24 + 3 * vb + 8),
+                      "record_bytes": n_total * (24 + 3 * vb + 8 + 4) + (moment_bytes if tc_form else
+                                                                         nodes * (126 + 3) * fb)}
     # The fold: for the tensor-core forms the moment assembly (moments read,
     # J and the mass records written) and the periodic fold.
     out["assembly"] = {"ms": timed_after(clear_and_deposit, fold),
@@ -422,13 +489,31 @@ def stage_kernel_times(sim, args, stream, repeats: int = 5) -> dict:
             p = st.slot[s][st.current[s]]
             _lib.check(lib.tpicb200_mover(sim.ctx, st.qom[s], C.byref(p), st.e_theta, st.b_node,
                                           scratch_inv.data_ptr(), s_))
-    out["mover"] = {"ms": timed(move), "bytes": n_total * ((24 + 3 * vb + 8 + 4) + (24 + 3 * vb + 4))}
+    out["mover"] = {"ms": timed(move), "bytes": n_total * 2 * (4 + 24 + 3 * vb)}
     for s in range(ns):
         for k, v in saved[s].items():
             sim.slots[s][st.current[s]][k].copy_(v)
     del saved
     torch.cuda.synchronize()
     return out
+
+
+def cycle_roofline(result: dict, particles: int, g, args, hbm: float) -> dict:
+    """Whole-cycle algorithmic bytes against the cycle time: per particle the
+    mover (key, positions, velocities read and written), the binned sort (key
+    read, record read and written) and the fused deposition (positions,
+    velocities, charge); per node the mass records per GMRES apply plus six
+    double vectors of three components, and the mass written and cleared once."""
+    vb = 4 if args.precision == "mixed" else 8
+    record = 24 + 3 * vb + 8 + 4
+    per_particle = 2 * (4 + 24 + 3 * vb) + (4 + 2 * record) + (24 + 3 * vb + 8)
+    nodes = (g.nx + 1) * (g.ny + 1) * (g.nz + 1)
+    mass_bytes = 126 * vb
+    applies = result["gmres_iterations"]
+    total = particles * per_particle + nodes * (applies * (mass_bytes + 6 * 3 * 8) + 2 * mass_bytes)
+    achieved = total / (result["ms_per_step"] / 1e3) / 1e9
+    return {"bytes_per_cycle": total, "bytes_per_particle": per_particle, "gmres_applies": applies,
+            "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm}
 
 
 def load_traffic(stage: str, particles: int):
@@ -444,10 +529,13 @@ def load_traffic(stage: str, particles: int):
 
 
 def end_to_end(sim, args, stream, barrier, nparticles, world, dist) -> dict:
-    """The metric through the public API from host buffers: every timed run
-    uploads the full state (particle records of the live slots and the
-    fields) from pinned host memory, prepares, runs the cycles and reads the
-    per-cycle energy reports back to the host."""
+    """The metric through the public API from host buffers, as one episode of
+    a fixed --e2e-cycles cycles (independent of --steps): the full state
+    (particle records of the live slots and the fields) is uploaded from
+    pinned host memory, the startup runs (tpicb200_prepare), then the cycles
+    (tpicb200_cycle), each reading its energy report back to the host. The
+    upload is charged to the episode's cycles (h2d_bytes_per_step = upload /
+    cycles); a cycle's own inputs are the previous cycle's device state."""
     import torch
     sim.materialize()
     live = []
@@ -457,7 +545,7 @@ def end_to_end(sim, args, stream, barrier, nparticles, world, dist) -> dict:
     fields = [(t, t.cpu().pin_memory()) for t in (sim.field("e"), sim.field("b_cell"))]
     h2d = sum(h.numel() * h.element_size() for d in live for _, h in d.values()) + \
         sum(h.numel() * h.element_size() for _, h in fields)
-    steps = args.steps
+    steps = args.e2e_cycles
     barrier()
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     start.record(stream)
@@ -498,6 +586,11 @@ def main():
                     help="a TPIC input deck (e.g. tpic_b200/decks/*.inp) as the workload instead of the default")
     ap.add_argument("--cpu-scale", type=int, default=24, help="cells per axis of the CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sweep", action=argparse.BooleanOptionalAction, default=True,
+                    help="also time the FP64 moment and TF32 forms and state every form's bootstrap mass and J "
+                         "error against the FP64 moment form (default on; off for decks)")
+    ap.add_argument("--e2e-cycles", type=int, default=20,
+                    help="cycles of the end-to-end episode (upload, startup, cycles, energy readback)")
     ap.add_argument("--cpu-workers", type=int, default=0, help="host processes of the reference arm (0: all cores)")
     args = ap.parse_args()
     if args.warmup < 3:

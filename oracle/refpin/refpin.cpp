@@ -13,6 +13,7 @@
 //   cell_to_node_average           ecsim/fields/cell_to_node.hpp:19-32
 //   ParticleCellMap encode/decode  data/particles/particle_cell.hpp:34-46
 //   node_smoothing_value           ecsim/fields/node_smoothing.hpp:24-52
+//   PreparedSerialParticleSort     lpfx/algorithm/particle/host/sort.hpp:180-290
 #include <tpic/data/mass_matrix/mass_matrix_layout.hpp>
 #include <tpic/data/particles/particle_cell.hpp>
 #include <tpic/ecsim/fields/cell_to_node.hpp>
@@ -21,6 +22,8 @@
 #include <tpic/ecsim/mass_matrix/mass_matrix_stencil.hpp>
 #include <tpic/ecsim/particles/cic.hpp>
 #include <tpic/ecsim/particles/particle_response.hpp>
+#include <lpfx/algorithm/particle/host/sort.hpp>
+#include <lpfx/api/particle/host_particles.hpp>
 
 #include <cstdint>
 #include <cstring>
@@ -45,9 +48,66 @@ template <class Location> struct Vector {
   template <std::size_t I> Component<Location> component() const { return c[I]; }
 };
 
+// A two-attribute host schema for the stable serial sort: the int32 cell key
+// and the record's input index, whose sorted order is the permutation.
+using SortKeyAttribute = lpfx::particle::attribute<"cell", std::int32_t>;
+using SortIndexAttribute = lpfx::particle::attribute<"source", std::uint32_t>;
+using SortSchema = lpfx::particle::schema<SortKeyAttribute, SortIndexAttribute>;
+using SortPolicy = lpfx::BasicParticleSortIndexPolicy<std::uint32_t, std::uint32_t, std::uint32_t, std::uint32_t>;
+using SortKeyAccessor = lpfx::ParticleAttributeKey<SortKeyAttribute::name_type>;
+
 }  // namespace
 
 extern "C" {
+
+// The reference's PreparedSerialParticleSort::run on `count` keys over
+// `bins` direct-cell bins: perm[dest] = source, counts and offsets of the
+// published bins. Returns the lpfx::ErrorCode value (0 = success), or -1
+// when the owners could not be built.
+int ref_serial_sort(const int32_t* keys, long count, long bins, uint32_t* perm, uint32_t* counts,
+                    uint32_t* offsets) {
+  auto made = lpfx::particle::make<SortSchema>({std::size_t(count), std::size_t(count)});
+  if (!made.has_value()) return -1;
+  auto particles = std::move(made).value();
+  {
+    auto view = particles.view();
+    auto key = view.template get<0>();
+    auto source = view.template get<1>();
+    for (long n = 0; n < count; ++n) {
+      key[n] = keys[n];
+      source[n] = std::uint32_t(n);
+    }
+  }
+  lpfx::HostMemoryBudget budget;
+  if (!budget.try_set_limit(std::size_t(1) << 40) || !budget.seal()) return -1;
+  lpfx::PreparedCellBins<std::uint32_t, std::uint32_t> prepared_bins{};
+  if (lpfx::try_prepare_cell_bins(bins, prepared_bins) != lpfx::ErrorCode::success) return -1;
+  auto made_bins = lpfx::make_host_cell_bins(budget, prepared_bins);
+  if (!made_bins.has_value()) return -1;
+  auto cell_bins = std::move(made_bins).value();
+  lpfx::PreparedSerialParticleSortWorkspace<SortPolicy> prepared_workspace{};
+  if (lpfx::try_prepare_serial_particle_sort_workspace<SortPolicy>(bins, particles.capacity(), prepared_workspace) !=
+      lpfx::ErrorCode::success)
+    return -1;
+  auto made_workspace = lpfx::make_host_serial_particle_sort_workspace(budget, prepared_workspace);
+  if (!made_workspace.has_value()) return -1;
+  auto workspace = std::move(made_workspace).value();
+  lpfx::DirectCellBinLayout<std::int32_t> layout{};
+  if (!lpfx::try_make_direct_cell_bin_layout<std::int32_t>(bins, layout)) return -1;
+  lpfx::PreparedSerialParticleSort<SortSchema, SortKeyAccessor, SortPolicy> sort{};
+  if (lpfx::try_prepare_serial_particle_sort(particles, cell_bins, workspace, layout, sort) != lpfx::ErrorCode::success)
+    return -1;
+  const lpfx::ErrorCode status = sort.run();
+  if (status != lpfx::ErrorCode::success) return int(status);
+  const auto view = std::as_const(particles).view();
+  const auto source = view.template get<1>();
+  for (long n = 0; n < count; ++n) perm[n] = source[n];
+  lpfx::CellBinsView<std::uint32_t, std::uint32_t> published{};
+  if (!cell_bins.try_completed_view(published)) return -1;
+  for (long b = 0; b < bins; ++b) counts[b] = published.counts()[b];
+  for (long b = 0; b <= bins; ++b) offsets[b] = published.offsets()[b];
+  return 0;
+}
 
 void ref_cic_weights_f64(double x, double y, double z, double* w) {
   const auto r = tpic::ecsim::make_cic_weights<double>(x, y, z);

@@ -1,0 +1,110 @@
+"""Cycle-level error of the reduced-precision forms against the FP64 oracle.
+
+The mixed-precision cycle (FP64 positions and charges, FP32 velocities, E, B,
+J and mass, FP32 mover and deposition arithmetic, FP32 Krylov basis) runs
+3 C1 cycles with each mass-assembly form: the plain FP32 CUDA-core form, the
+FP32 form with FP64 cell sums, the TF32 and the BF16x3 tensor-core forms. The
+FP64 oracle runs the same 3 cycles from the same initial state (the FP32
+velocities widened). After the cycles, E at the nodes, B at the cells and
+every particle (matched by id: its unwrapped position in cell units and its
+velocity) are compared. The bounds are the measured errors of each form with
+a margin of about 3x; the errors themselves are stated beside the bounds.
+
+These are not pinned by any reference test: the reference has no TF32 or
+BF16x3 form and no FP32-velocity storage level (precision.hpp:18-86). The
+plain FP64 cycle is held to the oracle at 1e-10 in test_gpu_cycle.py.
+"""
+from __future__ import annotations
+
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from fieldutil import interior_nodes
+from tpic_b200.plasma import generate_species
+
+pytestmark = pytest.mark.gpu
+
+# form -> bounds on (E rel. to max|E|, B - B0 rel. to max|B - B0|, position in
+# cells, velocity rel. to the species' thermal speed) after 3 C1 cycles.
+BOUNDS = {
+    "scalar": (3e-5, 3e-5, 3e-7, 3e-6),
+    "scalar-f64": (3e-5, 3e-5, 3e-7, 3e-6),
+    "tf32": (3e-3, 3e-3, 3e-6, 3e-5),
+    "bf16x3": (3e-4, 3e-4, 3e-7, 3e-6),
+}
+
+
+def unwrapped(g, d):
+    """Particle position in cell units on the periodic box, from key and fraction."""
+    key = d["cell"].astype(np.int64)
+    ex, ey = g.nx + 4, g.ny + 4
+    i, j, k = key % ex - 2, (key // ex) % ey - 2, key // (ex * ey) - 2
+    return np.stack([i + d["rx"], j + d["ry"], k + d["rz"]])
+
+
+def periodic_distance(a, b, extents):
+    d = a - b
+    for axis, n in enumerate(extents):
+        d[axis] -= n * np.round(d[axis] / n)
+    return np.abs(d).max()
+
+
+def measure(form: str, cycles: int = 3) -> dict:
+    from test_gpu_cycle import c1_case
+    from tpic_b200.simulation import Simulation
+    case = c1_case(n=16)
+    g = case.grid
+    sim = Simulation(case, precision="mixed", mass_kind=form, mass_layout="stencil-major", keep_ids=True)
+    sim.prepare()
+    sim.run(cycles)
+    arrays = []
+    for s, sp in enumerate(case.species):
+        d = generate_species(g, sp, s, seed=case.seed, velocity_dtype=np.float32)
+        for k in ("u", "v", "w"):
+            d[k] = d[k].astype(np.float64)  # the mixed run's initial velocities, exactly
+        arrays.append((sp.qom, d))
+    oc = O.OracleCycle(g, arrays, case.dt, case.theta, case.c, case.gmres_tol, 0, b0=case.fields.b0)
+    oc.prepare()
+    for _ in range(cycles):
+        oc.cycle()
+    e_gpu = interior_nodes(g, sim.field("e").cpu().numpy().astype(np.float64))
+    e_cpu = interior_nodes(g, oc.e)
+    b0 = np.repeat(np.asarray(case.fields.b0), oc.b.size // 3)
+    b_gpu = sim.field("b_cell").cpu().numpy().astype(np.float64) - b0
+    b_cpu = oc.b - b0
+    out = {"form": form, "cycles": cycles,
+           "e_rel": float(np.abs(e_gpu - e_cpu).max() / np.abs(e_cpu).max()),
+           "b_rel": float(np.abs(b_gpu - b_cpu).max() / np.abs(b_cpu).max()),
+           "position_cells": 0.0, "velocity_rel_vth": 0.0, "key_mismatches": 0}
+    for s, sp in enumerate(case.species):
+        live = {k: v.cpu().numpy() for k, v in sim.live(s).items()}
+        want = oc.species[s][1]
+        gi, wi = np.argsort(live["id"].view(np.uint64)), np.argsort(want["id"].view(np.uint64))
+        assert np.array_equal(live["id"].view(np.uint64)[gi], want["id"].view(np.uint64)[wi])
+        gl = {k: v[gi] for k, v in live.items()}
+        wl = {k: v[wi] for k, v in want.items() if not k.startswith("_")}
+        out["position_cells"] = max(out["position_cells"],
+                                    float(periodic_distance(unwrapped(g, gl), unwrapped(g, wl), (g.nx, g.ny, g.nz))))
+        dv = max(np.abs(gl[k].astype(np.float64) - wl[k]).max() for k in ("u", "v", "w"))
+        out["velocity_rel_vth"] = max(out["velocity_rel_vth"], float(dv / sp.vth[0]))
+        out["key_mismatches"] += int((gl["cell"] != wl["cell"]).sum())
+    sim.close()
+    return out
+
+
+@pytest.mark.parametrize("form", list(BOUNDS))
+def test_mixed_cycles_against_fp64_oracle(form):
+    err = measure(form)
+    path = os.environ.get("TPICB200_PARITY_LOG")
+    if path:
+        with open(path, "a") as f:
+            f.write(json.dumps(err) + "\n")
+    be, bb, bx, bv = BOUNDS[form]
+    assert err["e_rel"] <= be, err
+    assert err["b_rel"] <= bb, err
+    assert err["position_cells"] <= bx, err
+    assert err["velocity_rel_vth"] <= bv, err
