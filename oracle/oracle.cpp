@@ -23,6 +23,11 @@
 #include <limits>
 #include <vector>
 
+struct oracle_gmres_result {
+  int converged, iterations;
+  double initial_residual, residual, rhs_norm, relative_residual;
+};
+
 namespace {
 
 constexpr double kPi = 3.14159265358979323846264338327950288;
@@ -347,13 +352,22 @@ template <class T, class O> void cell_to_node(const Layout& L, const T* cellf, O
 // apply_mass_matrix_node, ecsim/mass_matrix/mass_matrix_stencil.hpp:119-149:
 // centre, then per stencil the forward neighbour with this vertex's block and
 // the backward neighbour with the neighbour vertex's block, untransposed.
+// transpose = true applies M^T: the same blocks, each 3x3 block transposed
+// (M^T has block (g, g+s) = B(g,s)^T and (g, g-s) = B(g-s,s)^T, so the
+// stencil walk is unchanged).
 template <class M>
 void mass_apply_node(const Layout& L, const M* mass, const double* in, int i, int j, int k,
-                     double row_inverse_volume, double out[3]) {
+                     double row_inverse_volume, double out[3], bool transpose = false) {
   const long nn = L.nodes;
   auto block = [&](long vertex, int s, long at, double& x, double& y, double& z) {
     const M* b = mass + vertex * 126 + s * 9;
     const double vx = in[at], vy = in[nn + at], vz = in[2 * nn + at];
+    if (transpose) {
+      x = vx * double(b[0]) + vy * double(b[3]) + vz * double(b[6]);
+      y = vx * double(b[1]) + vy * double(b[4]) + vz * double(b[7]);
+      z = vx * double(b[2]) + vy * double(b[5]) + vz * double(b[8]);
+      return;
+    }
     x = vx * double(b[0]) + vy * double(b[1]) + vz * double(b[2]);
     y = vx * double(b[3]) + vy * double(b[4]) + vz * double(b[5]);
     z = vx * double(b[6]) + vy * double(b[7]) + vz * double(b[8]);
@@ -436,7 +450,8 @@ struct Smoothing {
 };
 template <class M>
 void maxwell_apply(const Layout& L, const Physics& ph, const M* mass, double* in, double* image,
-                   double* curl_cell, double* curl_node, const Smoothing& sm = Smoothing{}) {
+                   double* curl_cell, double* curl_node, const Smoothing& sm = Smoothing{},
+                   bool transpose = false) {
   node_ghosts(L, in, 1, 1);
   node_ghosts(L, in + L.nodes, 1, 1);
   node_ghosts(L, in + 2 * L.nodes, 1, 1);
@@ -465,12 +480,112 @@ void maxwell_apply(const Layout& L, const Physics& ph, const M* mass, double* in
         if (sm.niter > 0)
           for (int c = 0; c < 3; ++c) m[c] = response[c * L.nodes + g];
         else
-          mass_apply_node(L, mass, in, i, j, k, ph.inv_volume, m);
+          mass_apply_node(L, mass, in, i, j, k, ph.inv_volume, m, transpose);
         for (int c = 0; c < 3; ++c) {
           const long at = c * L.nodes + g;
           image[at] = (1.0 * in[at] + d2 * curl_node[at]) + ph.kfac * m[c];
         }
       }
+}
+
+// Restarted GMRES from the guess x, restating Gmres::host_blocking_solve,
+// ecsim/gmres/gmres_device.hpp:355-454, with the device tails of :52-98
+// (classical Gram-Schmidt, Givens rotations, true-residual acceptance).
+// Returns -1 on a nonfinite estimate, else 0 (res.converged tells).
+template <class Apply>
+int gmres(Apply&& apply, const double* b, double* x, long N, int restart, int max_iterations, double tol,
+          oracle_gmres_result& res) {
+  std::vector<double> r(N), Ax(N), w(N);
+  std::vector<double> V((size_t)(restart + 1) * N);
+  std::vector<double> H((size_t)restart * (restart + 1)), cs(restart), sn(restart), s(restart + 1),
+      y(restart);
+  auto dot = [&](const double* a, const double* bb) {
+    double sum = 0;
+    for (long n = 0; n < N; ++n) sum += a[n] * bb[n];
+    return sum;
+  };
+  apply(x, Ax.data());
+  for (long n = 0; n < N; ++n) r[n] = b[n] - Ax[n];
+  res = oracle_gmres_result{};
+  res.residual = res.initial_residual = std::sqrt(dot(r.data(), r.data()));
+  res.rhs_norm = std::sqrt(dot(b, b));
+  const double scale = res.rhs_norm == 0 ? 1.0 : res.rhs_norm;
+  const double atol = scale * tol;
+  res.relative_residual = res.residual / scale;
+  res.converged = res.residual <= atol;
+  while (!res.converged && res.iterations < max_iterations) {
+    std::fill(H.begin(), H.end(), 0.0);
+    std::fill(cs.begin(), cs.end(), 0.0);
+    std::fill(sn.begin(), sn.end(), 0.0);
+    std::fill(s.begin(), s.end(), 0.0);
+    double rn2 = dot(r.data(), r.data());
+    double sc = rn2 > 0 ? 1.0 / std::sqrt(rn2) : 0.0;
+    for (long n = 0; n < N; ++n) V[n] = r[n] * sc;
+    s[0] = std::sqrt(rn2);
+    const int columns = std::min(restart, max_iterations - res.iterations);
+    int completed = 0;
+    bool breakdown = false;
+    for (int col = 0; col < columns; ++col) {
+      apply(&V[(size_t)col * N], w.data());
+      double* h = &H[(size_t)col * (restart + 1)];
+      std::vector<double> dots(col + 1);
+      for (int jj = 0; jj <= col; ++jj) dots[jj] = dot(&V[(size_t)jj * N], w.data());
+      double n2 = 0;
+      for (long n = 0; n < N; ++n) {
+        double val = w[n];
+        for (int jj = 0; jj <= col; ++jj) val -= dots[jj] * V[(size_t)jj * N + n];
+        w[n] = val;
+        n2 += val * val;
+      }
+      for (int jj = 0; jj <= col; ++jj) h[jj] = dots[jj];
+      // ArnoldiLeastSquaresUpdate, gmres_device.hpp:62-98.
+      const double sub = std::sqrt(n2);
+      h[col + 1] = sub;
+      for (int row = 0; row < col; ++row) {
+        const double up = h[row], lo = h[row + 1];
+        h[row] = cs[row] * up + sn[row] * lo;
+        h[row + 1] = -sn[row] * up + cs[row] * lo;
+      }
+      const double diag = h[col];
+      const double den = std::hypot(diag, sub);
+      const double cc = den != 0 ? diag / den : 1.0;
+      const double ss = den != 0 ? sub / den : 0.0;
+      cs[col] = cc;
+      sn[col] = ss;
+      h[col] = cc * diag + ss * sub;
+      h[col + 1] = 0;
+      const double up = s[col], lo = s[col + 1];
+      s[col] = cc * up + ss * lo;
+      s[col + 1] = -ss * up + cc * lo;
+      const double estimate = std::fabs(s[col + 1]);
+      const double nsc = n2 > 0 ? 1.0 / std::sqrt(n2) : 0.0;
+      for (long n = 0; n < N; ++n) V[(size_t)(col + 1) * N + n] = w[n] * nsc;
+      completed = col + 1;
+      breakdown = sub == 0;
+      if (!std::isfinite(estimate)) return -1;
+      if (estimate <= atol || breakdown) break;
+    }
+    // gmres_back_substitute_kernel, gmres_device.hpp:267-277.
+    for (int row = completed - 1; row >= 0; --row) {
+      double sum = 0;
+      for (int col = row + 1; col < completed; ++col) sum += H[(size_t)col * (restart + 1) + row] * y[col];
+      const double d = H[(size_t)row * (restart + 1) + row];
+      y[row] = d != 0 ? (s[row] - sum) / d : 0.0;
+    }
+    for (long n = 0; n < N; ++n) {
+      double val = x[n];
+      for (int col = 0; col < completed; ++col) val += y[col] * V[(size_t)col * N + n];
+      x[n] = val;
+    }
+    res.iterations += completed;
+    apply(x, Ax.data());
+    for (long n = 0; n < N; ++n) r[n] = b[n] - Ax[n];
+    res.residual = std::sqrt(dot(r.data(), r.data()));
+    res.relative_residual = res.residual / scale;
+    res.converged = res.residual <= atol;
+    if (breakdown && !res.converged) break;
+  }
+  return 0;
 }
 
 void pack(const Layout& L, const double* field, double* vec) {
@@ -499,10 +614,6 @@ struct oracle_grid {
   double dx, dy, dz;
 };
 
-struct oracle_gmres_result {
-  int converged, iterations;
-  double initial_residual, residual, rhs_norm, relative_residual;
-};
 
 static Grid to_grid(const oracle_grid* g) { return {g->nx, g->ny, g->nz, g->dx, g->dy, g->dz}; }
 
@@ -729,10 +840,7 @@ int oracle_field_solve_smoothed(const oracle_grid* gp, double dt, double th, dou
           const long at = cc * L.nodes + L.node(i, j, k);
           rhs[at] = (1.0 * E[at] + ph.delta * curl_node[at]) + (-ph.kfac) * J[at];
         }
-  std::vector<double> x(N), b(N), r(N), Ax(N), w(N);
-  std::vector<double> V((size_t)(restart + 1) * N);
-  std::vector<double> H((size_t)restart * (restart + 1)), cs(restart), sn(restart), s(restart + 1),
-      y(restart);
+  std::vector<double> x(N), b(N);
   pack(L, E, x.data());
   pack(L, rhs.data(), b.data());
   auto apply = [&](const double* vec, double* result) {
@@ -740,92 +848,8 @@ int oracle_field_solve_smoothed(const oracle_grid* gp, double dt, double th, dou
     maxwell_apply(L, ph, M, input.data(), image.data(), curl_cell.data(), curl_node.data(), sm);
     pack(L, image.data(), result);
   };
-  auto dot = [&](const double* a, const double* bb) {
-    double sum = 0;
-    for (long n = 0; n < N; ++n) sum += a[n] * bb[n];
-    return sum;
-  };
-  apply(x.data(), Ax.data());
-  for (long n = 0; n < N; ++n) r[n] = b[n] - Ax[n];
   oracle_gmres_result res{};
-  res.residual = res.initial_residual = std::sqrt(dot(r.data(), r.data()));
-  res.rhs_norm = std::sqrt(dot(b.data(), b.data()));
-  const double scale = res.rhs_norm == 0 ? 1.0 : res.rhs_norm;
-  const double atol = scale * tol;
-  res.relative_residual = res.residual / scale;
-  res.converged = res.residual <= atol;
-  while (!res.converged && res.iterations < max_iterations) {
-    std::fill(H.begin(), H.end(), 0.0);
-    std::fill(cs.begin(), cs.end(), 0.0);
-    std::fill(sn.begin(), sn.end(), 0.0);
-    std::fill(s.begin(), s.end(), 0.0);
-    double rn2 = dot(r.data(), r.data());
-    double sc = rn2 > 0 ? 1.0 / std::sqrt(rn2) : 0.0;
-    for (long n = 0; n < N; ++n) V[n] = r[n] * sc;
-    s[0] = std::sqrt(rn2);
-    const int columns = std::min(restart, max_iterations - res.iterations);
-    int completed = 0;
-    bool breakdown = false;
-    for (int col = 0; col < columns; ++col) {
-      apply(&V[(size_t)col * N], w.data());
-      double* h = &H[(size_t)col * (restart + 1)];
-      std::vector<double> dots(col + 1);
-      for (int jj = 0; jj <= col; ++jj) dots[jj] = dot(&V[(size_t)jj * N], w.data());
-      double n2 = 0;
-      for (long n = 0; n < N; ++n) {
-        double val = w[n];
-        for (int jj = 0; jj <= col; ++jj) val -= dots[jj] * V[(size_t)jj * N + n];
-        w[n] = val;
-        n2 += val * val;
-      }
-      for (int jj = 0; jj <= col; ++jj) h[jj] = dots[jj];
-      // ArnoldiLeastSquaresUpdate, gmres_device.hpp:62-98.
-      const double sub = std::sqrt(n2);
-      h[col + 1] = sub;
-      for (int row = 0; row < col; ++row) {
-        const double up = h[row], lo = h[row + 1];
-        h[row] = cs[row] * up + sn[row] * lo;
-        h[row + 1] = -sn[row] * up + cs[row] * lo;
-      }
-      const double diag = h[col];
-      const double den = std::hypot(diag, sub);
-      const double cc = den != 0 ? diag / den : 1.0;
-      const double ss = den != 0 ? sub / den : 0.0;
-      cs[col] = cc;
-      sn[col] = ss;
-      h[col] = cc * diag + ss * sub;
-      h[col + 1] = 0;
-      const double up = s[col], lo = s[col + 1];
-      s[col] = cc * up + ss * lo;
-      s[col + 1] = -ss * up + cc * lo;
-      const double estimate = std::fabs(s[col + 1]);
-      const double nsc = n2 > 0 ? 1.0 / std::sqrt(n2) : 0.0;
-      for (long n = 0; n < N; ++n) V[(size_t)(col + 1) * N + n] = w[n] * nsc;
-      completed = col + 1;
-      breakdown = sub == 0;
-      if (!std::isfinite(estimate)) return -1;
-      if (estimate <= atol || breakdown) break;
-    }
-    // gmres_back_substitute_kernel, gmres_device.hpp:267-277.
-    for (int row = completed - 1; row >= 0; --row) {
-      double sum = 0;
-      for (int col = row + 1; col < completed; ++col) sum += H[(size_t)col * (restart + 1) + row] * y[col];
-      const double d = H[(size_t)row * (restart + 1) + row];
-      y[row] = d != 0 ? (s[row] - sum) / d : 0.0;
-    }
-    for (long n = 0; n < N; ++n) {
-      double val = x[n];
-      for (int col = 0; col < completed; ++col) val += y[col] * V[(size_t)col * N + n];
-      x[n] = val;
-    }
-    res.iterations += completed;
-    apply(x.data(), Ax.data());
-    for (long n = 0; n < N; ++n) r[n] = b[n] - Ax[n];
-    res.residual = std::sqrt(dot(r.data(), r.data()));
-    res.relative_residual = res.residual / scale;
-    res.converged = res.residual <= atol;
-    if (breakdown && !res.converged) break;
-  }
+  if (gmres(apply, b.data(), x.data(), N, restart, max_iterations, tol, res) < 0) return -1;
   // The solution fills theta (interior nodes and ghosts).
   std::fill(theta, theta + 3 * L.nodes, 0.0);
   unpack(L, x.data(), theta);
@@ -922,6 +946,383 @@ void oracle_species_scalars(int precision, double qom, const void* u, const void
     s[4] += mass * vz;
   }
   std::memcpy(out, s, sizeof(s));
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Discrete adjoint of one cycle (FP64). TPIC has no adjoint; these functions
+// transpose the cycle the functions above restate, so that a gradient of a
+// final-state objective is carried back through the cycle:
+//   deposit      J_g = sum_p (q/V) W_a(x_p) (alpha_p v_p),
+//                M_ab = sum_p (beta/c) q alpha_p W_a W_b     (applied as M v)
+//   solve        A E_theta = E + delta C2N(B) - k J,  A = I + delta^2 C2N N2C + (k/V) M
+//   mover        v' = 2 alpha (v + beta E_theta(x)) - v,  x' = x + dt v' / dx
+//   advance      E' = E_theta/theta - (1-theta)/theta E,  B' = B - c dt N2C(E_theta)
+// with alpha = R(omega), omega = (beta/c) B_node(x), B_node = cell_to_node(B).
+// The adjoint of a gather at the particle positions is a scatter (then the
+// periodic fold), the adjoint of a scatter is a gather, the adjoint of the
+// solve is a solve with A^T (every 3x3 mass block transposed; the curl-curl
+// part is symmetric because C2N is the transpose of N2C on the periodic
+// grid), and N2C^T = C2N, C2N^T = N2C.
+// Adjoint node fields are gradients with respect to the unique periodic node
+// values, stored like the primal fields (duplicate endpoint nodes and ghosts
+// hold copies); scatters accumulate into a zeroed raw field that oracle_fold
+// turns into that form. Particle adjoints are indexed by record id, [3][count]
+// for positions (per axis, in cells) and velocities, [count] for charges.
+// ---------------------------------------------------------------------------
+
+namespace {
+
+struct AdjointParticle {
+  int i, j, k;
+  double f[3], v[3], w[8], dw[3][8];
+};
+
+template <int P>
+bool adjoint_load(const Layout& L, const void* rx, const void* ry, const void* rz, const void* u, const void* v,
+                  const void* w, const int32_t* key, long n, AdjointParticle& a) {
+  using Vel = typename Prec<P>::Vel;
+  if (key[n] < 0 || key[n] >= L.bins) return false;
+  L.decode(key[n], a.i, a.j, a.k);
+  if (!L.interior_cell(a.i, a.j, a.k)) return false;
+  a.f[0] = ((const double*)rx)[n];
+  a.f[1] = ((const double*)ry)[n];
+  a.f[2] = ((const double*)rz)[n];
+  a.v[0] = double(((const Vel*)u)[n]);
+  a.v[1] = double(((const Vel*)v)[n]);
+  a.v[2] = double(((const Vel*)w)[n]);
+  cic<double>(a.f[0], a.f[1], a.f[2], a.w);
+  for (int c = 0; c < 8; ++c) {
+    const double X[2] = {1 - a.f[0], a.f[0]}, Y[2] = {1 - a.f[1], a.f[1]}, Z[2] = {1 - a.f[2], a.f[2]};
+    const int bx = c & 1, by = (c >> 1) & 1, bz = (c >> 2) & 1;
+    const double sx = bx ? 1.0 : -1.0, sy = by ? 1.0 : -1.0, sz = bz ? 1.0 : -1.0;
+    a.dw[0][c] = sx * Y[by] * Z[bz];
+    a.dw[1][c] = X[bx] * sy * Z[bz];
+    a.dw[2][c] = X[bx] * Y[by] * sz;
+  }
+  return true;
+}
+
+template <class F>
+void adjoint_gather(const Layout& L, const F* field, const AdjointParticle& a, double out[3]) {
+  for (int c = 0; c < 3; ++c) {
+    double val = 0;
+    for (int b = 0; b < 8; ++b)
+      val += a.w[b] * double(field[c * L.nodes + L.node(a.i + (b & 1), a.j + ((b >> 1) & 1), a.k + ((b >> 2) & 1))]);
+    out[c] = val;
+  }
+}
+
+// sum_b dW_b/dx_axis * (field_b . g) for the three axes.
+template <class F>
+void adjoint_position_term(const Layout& L, const F* field, const AdjointParticle& a, const double g[3],
+                           double out[3]) {
+  for (int b = 0; b < 8; ++b) {
+    const long node = L.node(a.i + (b & 1), a.j + ((b >> 1) & 1), a.k + ((b >> 2) & 1));
+    double dotv = 0;
+    for (int c = 0; c < 3; ++c) dotv += double(field[c * L.nodes + node]) * g[c];
+    for (int axis = 0; axis < 3; ++axis) out[axis] += a.dw[axis][b] * dotv;
+  }
+}
+
+void adjoint_scatter(const Layout& L, double* field, const AdjointParticle& a, const double g[3]) {
+  for (int b = 0; b < 8; ++b) {
+    const long node = L.node(a.i + (b & 1), a.j + ((b >> 1) & 1), a.k + ((b >> 2) & 1));
+    for (int c = 0; c < 3; ++c) field[c * L.nodes + node] += a.w[b] * g[c];
+  }
+}
+
+// R^T g
+void transpose_apply(const double r[9], const double g[3], double out[3]) {
+  out[0] = r[0] * g[0] + r[3] * g[1] + r[6] * g[2];
+  out[1] = r[1] * g[0] + r[4] * g[1] + r[7] * g[2];
+  out[2] = r[2] * g[0] + r[5] * g[1] + r[8] * g[2];
+}
+
+// Gradient with respect to omega of sum_ij abar_ij R_ij(omega), R = (I +
+// omega omega^T + K(omega)) / (1 + |omega|^2) with K the antisymmetric part of
+// ParticleResponse (K_01 = wz, K_02 = -wy, K_12 = wx).
+void response_omega_gradient(const double om[3], const double r[9], const double ab[9], double out[3]) {
+  const double D = 1 + om[0] * om[0] + om[1] * om[1] + om[2] * om[2];
+  double ar = 0;
+  for (int e = 0; e < 9; ++e) ar += ab[e] * r[e];
+  const double kx = ab[5] - ab[7], ky = ab[6] - ab[2], kz = ab[1] - ab[3];
+  const double kk[3] = {kx, ky, kz};
+  for (int c = 0; c < 3; ++c) {
+    double sym = 0;
+    for (int e = 0; e < 3; ++e) sym += (ab[3 * c + e] + ab[3 * e + c]) * om[e];
+    out[c] = (sym + kk[c]) / D - 2 * om[c] * ar / D;
+  }
+}
+
+template <int P>
+long adjoint_mover_scatter(const Layout& L, const Grid& g, double qom, double dt, double c, const void* rx,
+                           const void* ry, const void* rz, const void* u, const void* v, const void* w,
+                           const int32_t* key, const uint64_t* id, long count, long nid, const double* xbar,
+                           const double* vbar, const double* theta, const void* bnode, double* scatter) {
+  using Fld = typename Prec<P>::Fld;
+  const double beta = qom * dt / 2, boc = beta / c;
+  const double inv[3] = {1.0 / g.dx, 1.0 / g.dy, 1.0 / g.dz};
+  long invalid = 0;
+  for (long n = 0; n < count; ++n) {
+    AdjointParticle a;
+    if (!adjoint_load<P>(L, rx, ry, rz, u, v, w, key, n, a) || id[n] >= uint64_t(nid)) { ++invalid; continue; }
+    const long pid = long(id[n]);
+    double bp[3];
+    adjoint_gather(L, (const Fld*)bnode, a, bp);
+    const Response<double> r(bp[0], bp[1], bp[2], boc);
+    double gv[3], eb[3];
+    for (int cc = 0; cc < 3; ++cc) gv[cc] = 2 * (vbar[cc * nid + pid] + dt * inv[cc] * xbar[cc * nid + pid]);
+    transpose_apply(r.a, gv, eb);
+    for (int cc = 0; cc < 3; ++cc) eb[cc] *= beta;
+    adjoint_scatter(L, scatter, a, eb);
+  }
+  return invalid;
+}
+
+template <int P>
+long adjoint_particles(const Layout& L, const Grid& g, double qom, double dt, double theta_, double c,
+                       const void* rx, const void* ry, const void* rz, const void* u, const void* v, const void* w,
+                       const double* q, const int32_t* key, const uint64_t* id, long count, long nid, double* xbar,
+                       double* vbar, double* qbar, const double* theta, const void* bnode, const double* lambda,
+                       double* bscatter) {
+  using Fld = typename Prec<P>::Fld;
+  const double beta = qom * dt / 2, boc = beta / c;
+  const double inv[3] = {1.0 / g.dx, 1.0 / g.dy, 1.0 / g.dz};
+  const double volume = (g.dx * g.dy) * g.dz, iv = 1.0 / volume;
+  const double kfac = 4 * kPi * (theta_ * dt);
+  long invalid = 0;
+  for (long n = 0; n < count; ++n) {
+    AdjointParticle a;
+    if (!adjoint_load<P>(L, rx, ry, rz, u, v, w, key, n, a) || id[n] >= uint64_t(nid)) { ++invalid; continue; }
+    const long pid = long(id[n]);
+    double bp[3], ep[3], lp[3];
+    adjoint_gather(L, (const Fld*)bnode, a, bp);
+    adjoint_gather(L, theta, a, ep);
+    adjoint_gather(L, lambda, a, lp);
+    const Response<double> r(bp[0], bp[1], bp[2], boc);
+    const double om[3] = {boc * bp[0], boc * bp[1], boc * bp[2]};
+    double xb[3], vt[3], gv[3];
+    for (int cc = 0; cc < 3; ++cc) {
+      xb[cc] = xbar[cc * nid + pid];
+      vt[cc] = vbar[cc * nid + pid] + dt * inv[cc] * xb[cc];
+      gv[cc] = 2 * vt[cc];
+    }
+    double ab[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    double vn[3], t[3];
+    // Mover: v' = 2 R (v + beta E_theta) - v, x' = x + dt v' / dx.
+    transpose_apply(r.a, gv, t);
+    double eb[3];
+    for (int cc = 0; cc < 3; ++cc) {
+      vn[cc] = -vt[cc] + t[cc];
+      eb[cc] = beta * t[cc];
+    }
+    const double uu[3] = {a.v[0] + beta * ep[0], a.v[1] + beta * ep[1], a.v[2] + beta * ep[2]};
+    for (int r0 = 0; r0 < 3; ++r0)
+      for (int c0 = 0; c0 < 3; ++c0) ab[3 * r0 + c0] += gv[r0] * uu[c0];
+    adjoint_position_term(L, theta, a, eb, xb);
+    // Current: J = sum (q/V) W (R v); its gradient is -k lambda (the RHS).
+    double h[3];
+    r.apply(a.v[0], a.v[1], a.v[2], h[0], h[1], h[2]);
+    const double jb[3] = {-kfac * lp[0], -kfac * lp[1], -kfac * lp[2]};
+    const double qv = q[n] * iv;
+    transpose_apply(r.a, jb, t);
+    for (int cc = 0; cc < 3; ++cc) vn[cc] += qv * t[cc];
+    for (int r0 = 0; r0 < 3; ++r0)
+      for (int c0 = 0; c0 < 3; ++c0) ab[3 * r0 + c0] += qv * jb[r0] * a.v[c0];
+    double qb = iv * (jb[0] * h[0] + jb[1] * h[1] + jb[2] * h[2]);
+    {
+      const double hq[3] = {-kfac * qv * h[0], -kfac * qv * h[1], -kfac * qv * h[2]};
+      adjoint_position_term(L, lambda, a, hq, xb);
+    }
+    // Mass: -(k/V) lambda^T M E_theta = -(k/V) sum_p s lambda_p^T R e_p, s = (beta/c) q.
+    const double cm = -kfac * iv, sq = boc * q[n];
+    double re[3];
+    r.apply(ep[0], ep[1], ep[2], re[0], re[1], re[2]);
+    qb += cm * boc * (lp[0] * re[0] + lp[1] * re[1] + lp[2] * re[2]);
+    for (int r0 = 0; r0 < 3; ++r0)
+      for (int c0 = 0; c0 < 3; ++c0) ab[3 * r0 + c0] += cm * sq * lp[r0] * ep[c0];
+    {
+      const double g1[3] = {cm * sq * re[0], cm * sq * re[1], cm * sq * re[2]};
+      adjoint_position_term(L, lambda, a, g1, xb);
+      double rl[3];
+      transpose_apply(r.a, lp, rl);
+      const double g2[3] = {cm * sq * rl[0], cm * sq * rl[1], cm * sq * rl[2]};
+      adjoint_position_term(L, theta, a, g2, xb);
+    }
+    // The response's dependence on B at the particle.
+    double ob[3];
+    response_omega_gradient(om, r.a, ab, ob);
+    const double bb[3] = {boc * ob[0], boc * ob[1], boc * ob[2]};
+    adjoint_scatter(L, bscatter, a, bb);
+    adjoint_position_term(L, (const Fld*)bnode, a, bb, xb);
+    for (int cc = 0; cc < 3; ++cc) {
+      xbar[cc * nid + pid] = xb[cc];
+      vbar[cc * nid + pid] = vn[cc];
+    }
+    qbar[pid] += qb;
+  }
+  return invalid;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Adjoint of the field advance: e_theta_bar = e_bar'/theta - c dt C2N(b_bar')
+// (e_bar' when theta is 1), e_bar = -(1-theta)/theta e_bar' (0 when theta is
+// 1), b_bar = b_bar'. b_bar_next needs filled ghosts; outputs are consistent
+// node fields / a cell field with ghosts.
+void oracle_adjoint_advance(const oracle_grid* gp, double dt, double th, double c, const double* e_bar_next,
+                            const double* b_bar_next, double* e_theta_bar, double* e_bar, double* b_bar) {
+  const Grid g = to_grid(gp);
+  const Layout L(g);
+  const double inv[3] = {1.0 / g.dx, 1.0 / g.dy, 1.0 / g.dz};
+  std::vector<double> curl_node(3 * L.nodes, 0.0);
+  curl_c2n(L, b_bar_next, curl_node.data(), inv);
+  const bool one = std::fabs(th - 1.0) < 1e-10;
+  for (int cc = 0; cc < 3; ++cc)
+    for (int k = 0; k <= L.nz; ++k)
+      for (int j = 0; j <= L.ny; ++j)
+        for (int i = 0; i <= L.nx; ++i) {
+          const long at = cc * L.nodes + L.node(i, j, k);
+          e_theta_bar[at] = (one ? e_bar_next[at] : e_bar_next[at] / th) + (-c * dt) * curl_node[at];
+          e_bar[at] = one ? 0.0 : (-(1.0 - th) / th) * e_bar_next[at];
+        }
+  for (int cc = 0; cc < 3; ++cc) {
+    node_ghosts(L, e_theta_bar + cc * L.nodes, 1, 1);
+    node_ghosts(L, e_bar + cc * L.nodes, 1, 1);
+  }
+  std::copy(b_bar_next, b_bar_next + 3 * L.cells, b_bar);
+  cell_ghosts(L, b_bar);
+}
+
+// Scatter of the mover's E_theta gradient (raw node field, add): per record,
+// W_a(x) beta R^T (2 (v_bar' + dt x_bar' / dx)). Returns the invalid records.
+long oracle_adjoint_mover_scatter(int precision, const oracle_grid* gp, double qom, double dt, double c,
+                                  const void* rx, const void* ry, const void* rz, const void* u, const void* v,
+                                  const void* w, const int32_t* key, const uint64_t* id, long count, long nid,
+                                  const double* xbar, const double* vbar, const double* theta, const void* bnode,
+                                  double* scatter) {
+  const Grid g = to_grid(gp);
+  const Layout L(g);
+  return precision == 0
+             ? adjoint_mover_scatter<0>(L, g, qom, dt, c, rx, ry, rz, u, v, w, key, id, count, nid, xbar, vbar,
+                                        theta, bnode, scatter)
+             : adjoint_mover_scatter<1>(L, g, qom, dt, c, rx, ry, rz, u, v, w, key, id, count, nid, xbar, vbar,
+                                        theta, bnode, scatter);
+}
+
+// Per record: the adjoints of the mover and of its current and mass
+// deposition at the cycle start, x_bar and v_bar replaced (by id), q_bar
+// accumulated, the B gradient scattered into bscatter (raw node field, add).
+long oracle_adjoint_particles(int precision, const oracle_grid* gp, double qom, double dt, double th, double c,
+                              const void* rx, const void* ry, const void* rz, const void* u, const void* v,
+                              const void* w, const double* q, const int32_t* key, const uint64_t* id, long count,
+                              long nid, double* xbar, double* vbar, double* qbar, const double* theta,
+                              const void* bnode, const double* lambda, double* bscatter) {
+  const Grid g = to_grid(gp);
+  const Layout L(g);
+  return precision == 0
+             ? adjoint_particles<0>(L, g, qom, dt, th, c, rx, ry, rz, u, v, w, q, key, id, count, nid, xbar, vbar,
+                                    qbar, theta, bnode, lambda, bscatter)
+             : adjoint_particles<1>(L, g, qom, dt, th, c, rx, ry, rz, u, v, w, q, key, id, count, nid, xbar, vbar,
+                                    qbar, theta, bnode, lambda, bscatter);
+}
+
+// The adjoint solve A^T lambda = rhs (rhs a consistent node field) by the
+// GMRES above from a zero guess; lambda gets its ghosts.
+int oracle_adjoint_solve(const oracle_grid* gp, double dt, double th, double c, const double* M, const double* rhs,
+                         double* lambda, int restart, int max_iterations, double tol, oracle_gmres_result* out) {
+  const Grid g = to_grid(gp);
+  const Layout L(g);
+  const Physics ph(g, dt, th, c);
+  const long N = 3 * L.interior;
+  std::vector<double> curl_node(3 * L.nodes, 0.0), curl_cell(3 * L.cells, 0.0), input(3 * L.nodes, 0.0),
+      image(3 * L.nodes, 0.0);
+  std::vector<double> x(N, 0.0), b(N);
+  pack(L, rhs, b.data());
+  auto apply = [&](const double* vec, double* result) {
+    unpack(L, vec, input.data());
+    maxwell_apply(L, ph, M, input.data(), image.data(), curl_cell.data(), curl_node.data(), Smoothing{}, true);
+    pack(L, image.data(), result);
+  };
+  oracle_gmres_result res{};
+  if (gmres(apply, b.data(), x.data(), N, restart, max_iterations, tol, res) < 0) return -1;
+  std::fill(lambda, lambda + 3 * L.nodes, 0.0);
+  unpack(L, x.data(), lambda);
+  for (int cc = 0; cc < 3; ++cc) node_ghosts(L, lambda + cc * L.nodes, 1, 1);
+  if (out) *out = res;
+  return res.converged ? 0 : 1;
+}
+
+// The field part after the solve: e_bar += lambda (the RHS's E term);
+// b_bar += delta N2C(lambda) (C2N^T) + cell_to_node^T(bnode_bar), with
+// bnode_bar a consistent node field; b_bar's ghosts refilled.
+void oracle_adjoint_fields(const oracle_grid* gp, double dt, double th, double c, const double* lambda,
+                           const double* bnode_bar, double* e_bar, double* b_bar) {
+  const Grid g = to_grid(gp);
+  const Layout L(g);
+  const Physics ph(g, dt, th, c);
+  for (int cc = 0; cc < 3; ++cc) {
+    for (int k = 0; k <= L.nz; ++k)
+      for (int j = 0; j <= L.ny; ++j)
+        for (int i = 0; i <= L.nx; ++i) {
+          const long at = cc * L.nodes + L.node(i, j, k);
+          e_bar[at] += lambda[at];
+        }
+    node_ghosts(L, e_bar + cc * L.nodes, 1, 1);
+  }
+  std::vector<double> curl_cell(3 * L.cells, 0.0);
+  curl_n2c(L, lambda, curl_cell.data(), ph.inv);
+  for (int cc = 0; cc < 3; ++cc)
+    for (int k = 0; k < L.nz; ++k)
+      for (int j = 0; j < L.ny; ++j)
+        for (int i = 0; i < L.nx; ++i) {
+          const long cl = cc * L.cells + L.cell(i, j, k);
+          double sum = 0;
+          // cell_to_node^T: the cell receives 1/8 of each unique node whose
+          // average reads it (nodes i..i+1 per axis, folded periodically).
+          for (int b = 0; b < 8; ++b) {
+            int ni = i + (b & 1), nj = j + ((b >> 1) & 1), nk = k + ((b >> 2) & 1);
+            if (ni == L.nx) ni = 0;
+            if (nj == L.ny) nj = 0;
+            if (nk == L.nz) nk = 0;
+            sum += bnode_bar[cc * L.nodes + L.node(ni, nj, nk)];
+          }
+          b_bar[cl] += ph.delta * curl_cell[cl] + 0.125 * sum;
+        }
+  cell_ghosts(L, b_bar);
+}
+
+// Gradient of we * W_E + wb * W_B (the energies of oracle_field_energy) with
+// respect to E at the unique nodes and B at the cells: e_bar = we V/(4 pi) E,
+// b_bar = wb V/(4 pi) B, stored as consistent fields.
+void oracle_energy_gradient(const oracle_grid* gp, double we, double wb, const double* E, const double* B,
+                            double* e_bar, double* b_bar) {
+  const Grid g = to_grid(gp);
+  const Layout L(g);
+  const double norm = ((g.dx * g.dy) * g.dz) / (4 * kPi);
+  std::fill(e_bar, e_bar + 3 * L.nodes, 0.0);
+  std::fill(b_bar, b_bar + 3 * L.cells, 0.0);
+  for (int cc = 0; cc < 3; ++cc) {
+    for (int k = 0; k < L.nz; ++k)
+      for (int j = 0; j < L.ny; ++j)
+        for (int i = 0; i < L.nx; ++i) {
+          const long n = cc * L.nodes + L.node(i, j, k), cl = cc * L.cells + L.cell(i, j, k);
+          e_bar[n] = we * norm * E[n];
+          b_bar[cl] = wb * norm * B[cl];
+        }
+    // Duplicate endpoint nodes take their unique node's value, then ghosts.
+    double* f = e_bar + cc * L.nodes;
+    for (int k = 0; k <= L.nz; ++k)
+      for (int j = 0; j <= L.ny; ++j)
+        for (int i = 0; i <= L.nx; ++i)
+          f[L.node(i, j, k)] = f[L.node(i == L.nx ? 0 : i, j == L.ny ? 0 : j, k == L.nz ? 0 : k)];
+    node_ghosts(L, f, 1, 1);
+  }
+  cell_ghosts(L, b_bar);
 }
 
 }  // extern "C"

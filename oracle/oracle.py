@@ -83,6 +83,21 @@ def load():
         lib.oracle_cic_weights_f32.argtypes = [C.c_float, C.c_float, C.c_float, vp]
         lib.oracle_response_f64.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double, vp]
         lib.oracle_response_f32.argtypes = [C.c_float, C.c_float, C.c_float, C.c_float, vp]
+        lib.oracle_adjoint_advance.argtypes = [C.POINTER(OGrid), C.c_double, C.c_double, C.c_double, vp, vp, vp, vp,
+                                               vp]
+        lib.oracle_adjoint_mover_scatter.restype = C.c_long
+        lib.oracle_adjoint_mover_scatter.argtypes = [C.c_int, C.POINTER(OGrid), C.c_double, C.c_double, C.c_double,
+                                                     vp, vp, vp, vp, vp, vp, vp, vp, C.c_long, C.c_long, vp, vp, vp,
+                                                     vp, vp]
+        lib.oracle_adjoint_particles.restype = C.c_long
+        lib.oracle_adjoint_particles.argtypes = [C.c_int, C.POINTER(OGrid), C.c_double, C.c_double, C.c_double,
+                                                 C.c_double, vp, vp, vp, vp, vp, vp, vp, vp, vp, C.c_long, C.c_long,
+                                                 vp, vp, vp, vp, vp, vp, vp]
+        lib.oracle_adjoint_solve.restype = C.c_int
+        lib.oracle_adjoint_solve.argtypes = [C.POINTER(OGrid), C.c_double, C.c_double, C.c_double, vp, vp, vp,
+                                             C.c_int, C.c_int, C.c_double, C.POINTER(OGmres)]
+        lib.oracle_adjoint_fields.argtypes = [C.POINTER(OGrid), C.c_double, C.c_double, C.c_double, vp, vp, vp, vp]
+        lib.oracle_energy_gradient.argtypes = [C.POINTER(OGrid), C.c_double, C.c_double, vp, vp, vp, vp]
         for name in ("oracle_node_count", "oracle_cell_count", "oracle_bin_count"):
             getattr(lib, name).restype = C.c_long
             getattr(lib, name).argtypes = [C.POINTER(OGrid)]
@@ -266,6 +281,106 @@ class OracleCycle:
         return self.energy()
 
 
+class OracleAdjoint:
+    """The discrete adjoint of OracleCycle's cycles in FP64 (test
+    infrastructure: the checker of the library's adjoint kernels).
+
+    `forward(n)` runs n cycles of `oc` (prepared, species carrying dense ids
+    0..count-1) and keeps a tape entry per cycle: the sorted records, E and B
+    at the cycle start and the cycle's E_theta. `backward(e_bar, b_bar)`
+    carries the gradient of an objective of the final E and B back through
+    the tape: per cycle the advance adjoint, the mover's E_theta scatter and
+    fold, the solve with A^T, the per-record adjoint (mover, current, mass),
+    the B scatter and fold, and the field adjoint. Particle adjoints are per
+    species, indexed by id: x_bar [3][count] (per axis, in cells), v_bar
+    [3][count], q_bar [count]."""
+
+    def __init__(self, oc: OracleCycle, tol: float = 1e-13, max_iterations: int = 500):
+        self.oc = oc
+        self.lib = oc.lib
+        self.tol = tol
+        self.max_iterations = max_iterations
+        self.tape = []
+        self.solves = []
+
+    def forward(self, ncycles: int):
+        oc = self.oc
+        for _ in range(ncycles):
+            snap = {"e": oc.e.copy(), "b": oc.b.copy(),
+                    "species": [(qom, {k: v.copy() for k, v in d.items()}) for qom, d in oc.species]}
+            energies = oc.cycle()
+            snap["theta"] = oc.theta_field.copy()
+            self.tape.append(snap)
+        return energies
+
+    def energy_gradient(self, we: float = 1.0, wb: float = 1.0):
+        oc = self.oc
+        e_bar, b_bar = np.zeros(3 * oc.nodes), np.zeros(3 * oc.cells)
+        self.lib.oracle_energy_gradient(C.byref(oc.og), we, wb, ptr(oc.e), ptr(oc.b), ptr(e_bar), ptr(b_bar))
+        return e_bar, b_bar
+
+    def _mass_and_bnode(self, snap):
+        oc = self.oc
+        og = C.byref(oc.og)
+        b = snap["b"].copy()
+        self.lib.oracle_cell_ghosts(og, ptr(b))
+        bnode = np.zeros(3 * oc.nodes)
+        self.lib.oracle_cell_to_node(og, ptr(b), ptr(bnode))
+        bnode = bnode.astype(oc.fdt)
+        m = np.zeros(126 * oc.nodes)
+        for qom, d in snap["species"]:
+            bad = self.lib.oracle_deposit(oc.precision, og, qom, oc.dt, oc.c, *[ptr(d[k]) for k in
+                                          ("rx", "ry", "rz", "u", "v", "w", "q", "cell")], len(d["cell"]),
+                                          ptr(bnode), None, ptr(m))
+            if bad:
+                raise ValueError(f"{bad} invalid records in the adjoint's deposition")
+        self.lib.oracle_fold(og, None, ptr(m))
+        return m.astype(oc.fdt).astype(np.float64), bnode
+
+    def backward(self, e_bar, b_bar):
+        oc = self.oc
+        og = C.byref(oc.og)
+        lib = self.lib
+        counts = [len(d["cell"]) for _, d in oc.species]
+        parts = [{"x": np.zeros(3 * n), "v": np.zeros(3 * n), "q": np.zeros(n)} for n in counts]
+        e_bar, b_bar = e_bar.copy(), b_bar.copy()
+        for snap in reversed(self.tape):
+            m, bnode = self._mass_and_bnode(snap)
+            theta = snap["theta"]
+            e_theta_bar, e_new, b_new = np.zeros(3 * oc.nodes), np.zeros(3 * oc.nodes), np.zeros(3 * oc.cells)
+            lib.oracle_adjoint_advance(og, oc.dt, oc.theta, oc.c, ptr(e_bar), ptr(b_bar), ptr(e_theta_bar),
+                                       ptr(e_new), ptr(b_new))
+            scatter = np.zeros(3 * oc.nodes)
+            for (qom, d), pa, n in zip(snap["species"], parts, counts):
+                bad = lib.oracle_adjoint_mover_scatter(oc.precision, og, qom, oc.dt, oc.c, *[ptr(d[k]) for k in
+                                                       ("rx", "ry", "rz", "u", "v", "w", "cell", "id")], n, n,
+                                                       ptr(pa["x"]), ptr(pa["v"]), ptr(theta), ptr(bnode),
+                                                       ptr(scatter))
+                if bad:
+                    raise ValueError(f"{bad} invalid records in the mover adjoint")
+            lib.oracle_fold(og, ptr(scatter), None)
+            e_theta_bar += scatter
+            lam = np.zeros(3 * oc.nodes)
+            res = OGmres()
+            status = lib.oracle_adjoint_solve(og, oc.dt, oc.theta, oc.c, ptr(m), ptr(e_theta_bar), ptr(lam),
+                                              oc.restart, self.max_iterations, self.tol, C.byref(res))
+            self.solves.append(res)
+            if status != 0:
+                raise RuntimeError("oracle adjoint GMRES did not converge")
+            bscatter = np.zeros(3 * oc.nodes)
+            for (qom, d), pa, n in zip(snap["species"], parts, counts):
+                bad = lib.oracle_adjoint_particles(oc.precision, og, qom, oc.dt, oc.theta, oc.c,
+                                                   *[ptr(d[k]) for k in ("rx", "ry", "rz", "u", "v", "w", "q", "cell",
+                                                                         "id")], n, n, ptr(pa["x"]), ptr(pa["v"]),
+                                                   ptr(pa["q"]), ptr(theta), ptr(bnode), ptr(lam), ptr(bscatter))
+                if bad:
+                    raise ValueError(f"{bad} invalid records in the particle adjoint")
+            lib.oracle_fold(og, ptr(bscatter), None)
+            lib.oracle_adjoint_fields(og, oc.dt, oc.theta, oc.c, ptr(lam), ptr(bscatter), ptr(e_new), ptr(b_new))
+            e_bar, b_bar = e_new, b_new
+        return e_bar, b_bar, parts
+
+
 def total_energy(scalars: np.ndarray, ns: int) -> float:
     return float(scalars[0] + scalars[1] + sum(scalars[2 + 5 * s] for s in range(ns)))
 
@@ -281,5 +396,5 @@ def case_species_arrays(case, precision: int, generate) -> list:
     return out
 
 
-__all__ = ["OracleCycle", "load", "load_reference", "build", "total_energy", "case_species_arrays", "OGrid", "ptr",
+__all__ = ["OracleCycle", "OracleAdjoint", "load", "load_reference", "build", "total_energy", "case_species_arrays", "OGrid", "ptr",
            "math"]
