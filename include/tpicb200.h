@@ -384,6 +384,133 @@ int tpicb200_cycle(tpicb200_context* ctx, tpicb200_state* state, int ncycles,
                    tpicb200_cycle_report* reports, tpicb200_stream stream);
 
 /* ------------------------------------------------------------------------
+ * Adjoint: reverse-mode gradients of the cycle.
+ *
+ * TPIC has no adjoint. These entry points transpose this library's forward
+ * stages so that the gradient of an objective of the state after n cycles
+ * (e.g. the final field energy) with respect to the state before them is
+ * carried back cycle by cycle, shaped like a torch.autograd.Function: a
+ * forward call saves what the backward needs (the tape), a backward call
+ * takes the gradients of a stage's outputs and returns those of its inputs.
+ * The transpose of each scatter is a gather at the particle positions (the
+ * current and mass deposition's backward), the transpose of each gather a
+ * scatter (the mover's backward), and the solve's backward is a GMRES solve
+ * with A^T (every 3x3 mass block transposed; the curl-curl part is symmetric).
+ * Gradients are FP64 in both precision modes. Smoothing is not differentiated
+ * (TPICB200_INVALID_STATE).
+ *
+ * Gradient layouts: node and cell fields of double in the field layouts
+ * above, holding the gradient with respect to the unique periodic values
+ * (duplicate endpoint nodes and ghosts hold copies); per species, indexed by
+ * record id (ids 0..count-1, as the loader assigns them): x_bar[3][count]
+ * (per axis, with respect to the position in cells), v_bar[3][count],
+ * q_bar[count].
+ * ------------------------------------------------------------------------ */
+typedef struct {
+  int ns;
+  double* e_bar;                        /* node field: d/dE */
+  double* b_bar;                        /* cell field (ghosts filled): d/dB */
+  double* x_bar[TPICB200_MAX_SPECIES];  /* [3][count] */
+  double* v_bar[TPICB200_MAX_SPECIES];  /* [3][count] */
+  double* q_bar[TPICB200_MAX_SPECIES];  /* [count]: summed over every cycle carried back */
+  uint32_t count[TPICB200_MAX_SPECIES]; /* records (ids) per species */
+  /* Scratch of tpicb200_cycle_backward: double node fields, and B at the
+   * nodes, J and the mass records in the storage types of the context. */
+  double* e_theta_bar;
+  double* lambda;
+  double* b_node_bar;
+  void* b_node;
+  void* j;
+  void* mass;
+} tpicb200_adjoint;
+
+/* What the backward of one cycle needs: the state at the cycle's start
+ * (sorted records with ids, their bins, E at the nodes and B at the cells,
+ * in the storage types) and the cycle's E_theta. Caller-owned device
+ * buffers; species[s] holds room for the species' records. */
+typedef struct {
+  int ns;
+  double qom[TPICB200_MAX_SPECIES];
+  tpicb200_particles species[TPICB200_MAX_SPECIES];
+  uint32_t* counts[TPICB200_MAX_SPECIES];
+  uint32_t* offsets[TPICB200_MAX_SPECIES];
+  void* e;
+  void* b_cell;
+  double* e_theta;
+  int mass_kind;
+} tpicb200_tape;
+
+/* One cycle of tpicb200_cycle that first saves its starting state into the
+ * tape (ranked species are materialized) and then the cycle's E_theta. The
+ * state's records need ids. Host-blocking like tpicb200_cycle. */
+int tpicb200_cycle_forward(tpicb200_context* ctx, tpicb200_state* state, tpicb200_tape* tape,
+                           tpicb200_cycle_report* report, tpicb200_stream stream);
+
+/* The backward of the cycle recorded in `tape`: on entry adj holds the
+ * gradients with respect to the state after the cycle, on return those with
+ * respect to the state at its start (q_bar accumulates). Steps: B at the
+ * nodes and the deposition of the tape's records (J and M into the adjoint's
+ * scratch, the tape's mass form), the advance's backward, the scatter of the
+ * movers' E_theta gradient, the solve with A^T (the context's GMRES tolerance
+ * and step limit; result may be NULL), the records' backward (mover, current
+ * and mass, with the B gradient scattered), and the fields' backward. The
+ * host waits for the adjoint solve as for the forward one. */
+int tpicb200_cycle_backward(tpicb200_context* ctx, tpicb200_tape* tape, tpicb200_adjoint* adj,
+                            tpicb200_gmres_result* result, tpicb200_stream stream);
+
+/* Starts a backward run: adj->e_bar and adj->b_bar receive the gradient of
+ * we * W_E + wb * W_B of the fields e (node) and b_cell (cell, storage types),
+ * the energies of tpicb200_energy (W_E over the unique nodes, W_B over the
+ * cells); the particle gradients of adj's ns species are zeroed. */
+int tpicb200_adjoint_energy(tpicb200_context* ctx, const void* e, const void* b_cell, double we, double wb,
+                            tpicb200_adjoint* adj, tpicb200_stream stream);
+
+/* Stage backwards (the transposes of the stage entry points above). Each
+ * adds into the unique values of its gradient outputs and refills their
+ * duplicates and ghosts. */
+
+/* Backward of tpicb200_field_advance: e_bar holds d/dE' on entry and d/dE
+ * (from the advance alone) on return; e_theta_bar receives
+ * e_bar'/theta - c dt C2N(b_bar'); b_bar (d/dB' = d/dB) is read. */
+int tpicb200_field_advance_backward(tpicb200_context* ctx, double* e_bar, const double* b_bar, double* e_theta_bar,
+                                    tpicb200_stream stream);
+
+/* Backward of tpicb200_mover for records p (sorted by cell for speed, with
+ * ids below nid) as they were before the move: x_bar/v_bar hold the
+ * gradients of the moved records on entry and of the records before the
+ * move on return; the gradients of E_theta and of B at the nodes are added
+ * into e_theta_bar and b_node_bar. */
+int tpicb200_mover_backward(tpicb200_context* ctx, double qom, const tpicb200_particles* p, const double* e_theta,
+                            const void* b_node, uint32_t nid, double* x_bar, double* v_bar, double* e_theta_bar,
+                            double* b_node_bar, uint32_t* invalid, tpicb200_stream stream);
+
+/* Backward of tpicb200_deposit for the objective
+ *   j_scale <j_bar, J> + mass_scale <mass_left, M mass_right>
+ * (M the mass matrix applied without its 1/V row scale; j_bar, mass_left
+ * and mass_right double node fields with ghosts, any may be NULL): the
+ * gradients are added into x_bar, v_bar, q_bar and b_node_bar. In a cycle,
+ * j_bar = mass_left = lambda, j_scale = -k, mass_right = E_theta,
+ * mass_scale = -k/V. */
+int tpicb200_deposit_backward(tpicb200_context* ctx, double qom, const tpicb200_particles* p, const void* b_node,
+                              const double* j_bar, double j_scale, const double* mass_left,
+                              const double* mass_right, double mass_scale, uint32_t nid, double* x_bar,
+                              double* v_bar, double* q_bar, double* b_node_bar, uint32_t* invalid,
+                              tpicb200_stream stream);
+
+/* Backward of tpicb200_field_solve: lambda = A^-T e_theta_bar (GMRES from a
+ * zero guess, the context's tolerance), then e_bar += lambda and
+ * b_bar += delta N2C(lambda) (the right-hand side's E and B terms); the
+ * gradients of J and M are -k lambda and -(k/V) lambda E_theta^T (pass them
+ * to tpicb200_deposit_backward). Host-blocking like the forward solve. */
+int tpicb200_field_solve_backward(tpicb200_context* ctx, const void* mass, const double* e_theta_bar, double* lambda,
+                                  double* e_bar, double* b_bar, tpicb200_gmres_result* result,
+                                  tpicb200_stream stream);
+
+/* Backward of tpicb200_magnetic_to_nodes: b_bar += cell_to_node^T(b_node_bar). */
+int tpicb200_magnetic_to_nodes_backward(tpicb200_context* ctx, const double* b_node_bar, double* b_bar,
+                                        tpicb200_stream stream);
+
+/* ------------------------------------------------------------------------
  * Input decks and analytic initial cases (host code, no device needed).
  *
  * TPIC reads a run from an input deck of `key = value` lines ('#' starts a

@@ -70,6 +70,20 @@ class CycleReport(C.Structure):
                 ("stage_ms", C.c_float * 6)]
 
 
+class Adjoint(C.Structure):
+    _fields_ = [("ns", C.c_int), ("e_bar", C.c_void_p), ("b_bar", C.c_void_p),
+                ("x_bar", C.c_void_p * MAX_SPECIES), ("v_bar", C.c_void_p * MAX_SPECIES),
+                ("q_bar", C.c_void_p * MAX_SPECIES), ("count", C.c_uint32 * MAX_SPECIES),
+                ("e_theta_bar", C.c_void_p), ("lambda_", C.c_void_p), ("b_node_bar", C.c_void_p),
+                ("b_node", C.c_void_p), ("j", C.c_void_p), ("mass", C.c_void_p)]
+
+
+class Tape(C.Structure):
+    _fields_ = [("ns", C.c_int), ("qom", C.c_double * MAX_SPECIES), ("species", Particles * MAX_SPECIES),
+                ("counts", C.c_void_p * MAX_SPECIES), ("offsets", C.c_void_p * MAX_SPECIES),
+                ("e", C.c_void_p), ("b_cell", C.c_void_p), ("e_theta", C.c_void_p), ("mass_kind", C.c_int)]
+
+
 CASE_NAME_MAX = 32
 
 
@@ -141,6 +155,22 @@ EXPORTS = {
                                         C.POINTER(Particles), C.c_void_p, C.c_void_p]),
     "tpicb200_center_velocities": (C.c_int, [C.c_void_p, C.POINTER(Deck), C.c_int, C.POINTER(Particles), C.c_void_p,
                                              C.c_void_p]),
+    "tpicb200_cycle_forward": (C.c_int, [C.c_void_p, C.POINTER(State), C.POINTER(Tape), C.POINTER(CycleReport),
+                                         C.c_void_p]),
+    "tpicb200_cycle_backward": (C.c_int, [C.c_void_p, C.POINTER(Tape), C.POINTER(Adjoint), C.POINTER(GmresResult),
+                                          C.c_void_p]),
+    "tpicb200_adjoint_energy": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_double,
+                                          C.POINTER(Adjoint), C.c_void_p]),
+    "tpicb200_field_advance_backward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tpicb200_mover_backward": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(Particles), C.c_void_p, C.c_void_p,
+                                          C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.c_void_p]),
+    "tpicb200_deposit_backward": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(Particles), C.c_void_p, C.c_void_p,
+                                            C.c_double, C.c_void_p, C.c_void_p, C.c_double, C.c_uint32, C.c_void_p,
+                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tpicb200_field_solve_backward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                C.c_void_p, C.POINTER(GmresResult), C.c_void_p]),
+    "tpicb200_magnetic_to_nodes_backward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tpicb200_checkpoint_write": (C.c_int, [C.c_void_p, C.POINTER(State), C.c_char_p, C.c_int, C.c_void_p]),
     "tpicb200_checkpoint_find": (C.c_int, [C.c_char_p, C.c_char_p, C.c_size_t]),
     "tpicb200_checkpoint_info_read": (C.c_int, [C.c_char_p, C.POINTER(CheckpointInfo)]),

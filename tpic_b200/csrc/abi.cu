@@ -899,3 +899,236 @@ int tpicb200_cycle(tpicb200_context* ctx, tpicb200_state* st, int ncycles, tpicb
 }
 
 }  // extern "C"
+
+// ---- Adjoint ----------------------------------------------------------------
+
+namespace {
+
+int check_adjoint_context(tpicb200_context* ctx) {
+  if (int s = check_ctx(ctx)) return s;
+  if (ctx->particle_theta)
+    return fail(TPICB200_INVALID_STATE, "the adjoint does not differentiate energy-conserving smoothing");
+  return TPICB200_SUCCESS;
+}
+
+int check_gradient_records(tpicb200_context* ctx, const tpicb200_particles* p, uint32_t nid, const double* x_bar,
+                           const double* v_bar) {
+  if (int r = check_particles(ctx, p)) return r;
+  if (p->count && !p->id) return fail(TPICB200_INVALID_ARGUMENT, "the adjoint needs record ids");
+  if (p->count && (!x_bar || !v_bar || nid == 0)) return fail(TPICB200_INVALID_ARGUMENT, "null record gradients");
+  return TPICB200_SUCCESS;
+}
+
+size_t field_bytes(const tpicb200_context* ctx) {
+  return ctx->opt.precision == TPICB200_PRECISION_DOUBLE ? 8 : 4;
+}
+
+cudaError_t copy_records(const tpicb200_context* ctx, const tpicb200_particles* in, tpicb200_particles* out,
+                         cudaStream_t s) {
+  const size_t n = in->count, vb = field_bytes(ctx);
+  cudaError_t e = cudaSuccess;
+  auto copy = [&](void* dst, const void* src, size_t bytes) {
+    if (e == cudaSuccess && bytes) e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, s);
+  };
+  copy(out->rx, in->rx, 8 * n);
+  copy(out->ry, in->ry, 8 * n);
+  copy(out->rz, in->rz, 8 * n);
+  copy(out->u, in->u, vb * n);
+  copy(out->v, in->v, vb * n);
+  copy(out->w, in->w, vb * n);
+  copy(out->q, in->q, 8 * n);
+  copy(out->cell, in->cell, 4 * n);
+  copy(out->id, in->id, 8 * n);
+  out->count = in->count;
+  return e;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tpicb200_cycle_forward(tpicb200_context* ctx, tpicb200_state* st, tpicb200_tape* tape,
+                           tpicb200_cycle_report* report, tpicb200_stream stream) {
+  if (int s = check_adjoint_context(ctx)) return s;
+  if (int r = check_state(ctx, st)) return r;
+  if (!tape || tape->ns != st->ns || !tape->e || !tape->b_cell || !tape->e_theta)
+    return fail(TPICB200_INVALID_ARGUMENT, "invalid tape");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (int r = tpicb200_materialize(ctx, st, stream)) return r;
+  const size_t fb = field_bytes(ctx);
+  cudaError_t e = cudaSuccess;
+  for (int sp = 0; sp < st->ns; ++sp) {
+    const tpicb200_particles* live = &st->slot[sp][st->current[sp]];
+    tpicb200_particles* out = &tape->species[sp];
+    if (live->count && (!live->id || !out->id || !out->rx || !out->ry || !out->rz || !out->u || !out->v || !out->w ||
+                        !out->q || !out->cell))
+      return fail(TPICB200_INVALID_ARGUMENT, "the tape needs every record attribute, ids included");
+    if (!tape->counts[sp] || !tape->offsets[sp]) return fail(TPICB200_INVALID_ARGUMENT, "null tape bins");
+    if (e == cudaSuccess) e = copy_records(ctx, live, out, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(tape->counts[sp], st->counts[sp], size_t(ctx->g.bins) * 4, cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(tape->offsets[sp], st->offsets[sp], size_t(ctx->g.bins + 1) * 4, cudaMemcpyDeviceToDevice,
+                          s);
+    tape->qom[sp] = st->qom[sp];
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(tape->e, st->e, 3 * size_t(ctx->g.nodes) * fb, cudaMemcpyDeviceToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(tape->b_cell, st->b_cell, 3 * size_t(ctx->g.cells) * fb, cudaMemcpyDeviceToDevice, s);
+  if (e != cudaSuccess) return cuda_status(e, "tape copy failed");
+  tape->mass_kind = st->mass_kind;
+  if (int r = tpicb200_cycle(ctx, st, 1, report, stream)) return r;
+  return cuda_status(cudaMemcpyAsync(tape->e_theta, st->e_theta, 3 * size_t(ctx->g.nodes) * 8,
+                                     cudaMemcpyDeviceToDevice, s),
+                     "tape E_theta copy failed");
+}
+
+int tpicb200_adjoint_energy(tpicb200_context* ctx, const void* e, const void* b_cell, double we, double wb,
+                            tpicb200_adjoint* adj, tpicb200_stream stream) {
+  if (int s = check_ctx(ctx)) return s;
+  if (!e || !b_cell || !adj || !adj->e_bar || !adj->b_bar || adj->ns < 0 || adj->ns > TPICB200_MAX_SPECIES)
+    return fail(TPICB200_INVALID_ARGUMENT, "invalid adjoint energy arguments");
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t err = launch_energy_gradient(ctx->opt.precision, ctx->g, we, wb, e, b_cell, adj->e_bar, adj->b_bar, s);
+  for (int sp = 0; sp < adj->ns && err == cudaSuccess; ++sp) {
+    const size_t n = adj->count[sp];
+    if (!n) continue;
+    if (!adj->x_bar[sp] || !adj->v_bar[sp] || !adj->q_bar[sp])
+      return fail(TPICB200_INVALID_ARGUMENT, "null record gradients");
+    err = cudaMemsetAsync(adj->x_bar[sp], 0, 3 * n * 8, s);
+    if (err == cudaSuccess) err = cudaMemsetAsync(adj->v_bar[sp], 0, 3 * n * 8, s);
+    if (err == cudaSuccess) err = cudaMemsetAsync(adj->q_bar[sp], 0, n * 8, s);
+  }
+  return cuda_status(err, "adjoint start failed");
+}
+
+int tpicb200_field_advance_backward(tpicb200_context* ctx, double* e_bar, const double* b_bar, double* e_theta_bar,
+                                    tpicb200_stream stream) {
+  if (int s = check_ctx(ctx)) return s;
+  if (!e_bar || !b_bar || !e_theta_bar || e_bar == e_theta_bar)
+    return fail(TPICB200_INVALID_ARGUMENT, "advance backward needs distinct gradient fields");
+  return cuda_status(launch_adjoint_advance(ctx->g, ctx->opt.theta, ctx->opt.c, ctx->opt.dt, e_bar, b_bar,
+                                            e_theta_bar, (cudaStream_t)stream),
+                     "advance backward failed");
+}
+
+int tpicb200_mover_backward(tpicb200_context* ctx, double qom, const tpicb200_particles* p, const double* e_theta,
+                            const void* b_node, uint32_t nid, double* x_bar, double* v_bar, double* e_theta_bar,
+                            double* b_node_bar, uint32_t* invalid, tpicb200_stream stream) {
+  if (int s = check_ctx(ctx)) return s;
+  if (int r = check_gradient_records(ctx, p, nid, x_bar, v_bar)) return r;
+  if (!e_theta || !b_node || !e_theta_bar || !b_node_bar)
+    return fail(TPICB200_INVALID_ARGUMENT, "mover backward needs its fields");
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t err = launch_adjoint_records(ctx->opt.precision, kAdjointMover, ctx->g, qom, ctx->opt.dt, ctx->opt.c, p,
+                                           nid, x_bar, v_bar, nullptr, e_theta, b_node, nullptr, 0.0, nullptr,
+                                           nullptr, 0.0, b_node_bar, e_theta_bar, invalid_or_own(ctx, invalid), s);
+  if (err == cudaSuccess) err = launch_node_ghosts(ctx->g, e_theta_bar, 3, s);
+  if (err == cudaSuccess) err = launch_node_ghosts(ctx->g, b_node_bar, 3, s);
+  return cuda_status(err, "mover backward failed");
+}
+
+int tpicb200_deposit_backward(tpicb200_context* ctx, double qom, const tpicb200_particles* p, const void* b_node,
+                              const double* j_bar, double j_scale, const double* mass_left,
+                              const double* mass_right, double mass_scale, uint32_t nid, double* x_bar,
+                              double* v_bar, double* q_bar, double* b_node_bar, uint32_t* invalid,
+                              tpicb200_stream stream) {
+  if (int s = check_ctx(ctx)) return s;
+  if (int r = check_gradient_records(ctx, p, nid, x_bar, v_bar)) return r;
+  if (!b_node || !b_node_bar || (p->count && !q_bar) || (mass_left && !mass_right))
+    return fail(TPICB200_INVALID_ARGUMENT, "deposit backward needs its fields");
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t err = launch_adjoint_records(ctx->opt.precision, kAdjointDeposit, ctx->g, qom, ctx->opt.dt, ctx->opt.c,
+                                           p, nid, x_bar, v_bar, q_bar, nullptr, b_node, j_bar, j_scale, mass_left,
+                                           mass_right, mass_scale, b_node_bar, nullptr, invalid_or_own(ctx, invalid),
+                                           s);
+  if (err == cudaSuccess) err = launch_node_ghosts(ctx->g, b_node_bar, 3, s);
+  return cuda_status(err, "deposit backward failed");
+}
+
+int tpicb200_field_solve_backward(tpicb200_context* ctx, const void* mass, const double* e_theta_bar, double* lambda,
+                                  double* e_bar, double* b_bar, tpicb200_gmres_result* result,
+                                  tpicb200_stream stream) {
+  if (int s = check_adjoint_context(ctx)) return s;
+  if (!mass || !e_theta_bar || !lambda || !e_bar || !b_bar || lambda == e_theta_bar)
+    return fail(TPICB200_INVALID_ARGUMENT, "solve backward needs distinct fields");
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t err = cudaSuccess;
+  tpicb200_gmres_result res{};
+  const int status = solver_solve_adjoint(ctx->solver, e_theta_bar, mass, lambda, &res,
+                                          ctx->opt.gmres_max_iterations, ctx->opt.gmres_tol, s, &err);
+  if (result) *result = res;
+  if (err != cudaSuccess) return cuda_status(err, "adjoint solve failed");
+  if (status == TPICB200_NOT_CONVERGED) return fail(status, "the adjoint GMRES did not converge");
+  if (status != TPICB200_SUCCESS) return fail(status, "the adjoint solve failed");
+  err = launch_adjoint_add_nodes(ctx->g, lambda, e_bar, s);
+  const double delta = ctx->opt.c * ctx->opt.theta * ctx->opt.dt;
+  if (err == cudaSuccess) err = launch_adjoint_cells(ctx->g, delta, lambda, nullptr, b_bar, s);
+  return cuda_status(err, "solve backward failed");
+}
+
+int tpicb200_magnetic_to_nodes_backward(tpicb200_context* ctx, const double* b_node_bar, double* b_bar,
+                                        tpicb200_stream stream) {
+  if (int s = check_ctx(ctx)) return s;
+  if (!b_node_bar || !b_bar) return fail(TPICB200_INVALID_ARGUMENT, "null gradient field");
+  return cuda_status(launch_adjoint_cells(ctx->g, 0.0, nullptr, b_node_bar, b_bar, (cudaStream_t)stream),
+                     "magnetic-to-nodes backward failed");
+}
+
+int tpicb200_cycle_backward(tpicb200_context* ctx, tpicb200_tape* tape, tpicb200_adjoint* adj,
+                            tpicb200_gmres_result* result, tpicb200_stream stream) {
+  if (int s = check_adjoint_context(ctx)) return s;
+  if (!tape || !adj || tape->ns != adj->ns || tape->ns <= 0 || tape->ns > TPICB200_MAX_SPECIES)
+    return fail(TPICB200_INVALID_ARGUMENT, "invalid tape or adjoint");
+  if (!adj->e_bar || !adj->b_bar || !adj->e_theta_bar || !adj->lambda || !adj->b_node_bar || !adj->b_node ||
+      !adj->j || !adj->mass || !tape->e || !tape->b_cell || !tape->e_theta)
+    return fail(TPICB200_INVALID_ARGUMENT, "null adjoint or tape field");
+  if (int r = check_mass_kind(ctx, tape->mass_kind)) return r;
+  for (int sp = 0; sp < tape->ns; ++sp) {
+    if (int r = check_gradient_records(ctx, &tape->species[sp], adj->count[sp], adj->x_bar[sp], adj->v_bar[sp]))
+      return r;
+    if (tape->species[sp].count && !adj->q_bar[sp]) return fail(TPICB200_INVALID_ARGUMENT, "null charge gradients");
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  const Geom& g = ctx->g;
+  const int prec = ctx->opt.precision;
+  const double dt = ctx->opt.dt, c = ctx->opt.c, kfac = 4 * 3.14159265358979323846 * (ctx->opt.theta * dt);
+  // The cycle's B at the nodes, J and M, deposited again from the tape.
+  if (int r = tpicb200_magnetic_to_nodes(ctx, tape->b_cell, adj->b_node, stream)) return r;
+  if (int r = tpicb200_clear_moments(ctx, adj->j, adj->mass, stream)) return r;
+  const tpicb200_particles* parts = tape->species;
+  const uint32_t* const* counts = tape->counts;
+  const uint32_t* const* offsets = tape->offsets;
+  if (int r = tpicb200_deposit_species(ctx, tape->ns, tape->qom, parts, counts, offsets, adj->b_node, adj->j,
+                                       adj->mass, tape->mass_kind, nullptr, stream))
+    return r;
+  if (int r = tpicb200_fold_periodic(ctx, adj->j, adj->mass, stream)) return r;
+  // Advance backward, then the movers' E_theta gradient.
+  cudaError_t err = launch_adjoint_advance(g, ctx->opt.theta, c, dt, adj->e_bar, adj->b_bar, adj->e_theta_bar, s);
+  for (int sp = 0; sp < tape->ns && err == cudaSuccess; ++sp)
+    err = launch_adjoint_theta_scatter(prec, g, tape->qom[sp], dt, c, &tape->species[sp], adj->count[sp],
+                                       adj->x_bar[sp], adj->v_bar[sp], adj->b_node, adj->e_theta_bar, ctx->invalid,
+                                       s);
+  if (err == cudaSuccess) err = launch_node_ghosts(g, adj->e_theta_bar, 3, s);
+  if (err != cudaSuccess) return cuda_status(err, "cycle backward (advance, movers) failed");
+  // The solve's backward: lambda, and its E and B terms.
+  if (int r = tpicb200_field_solve_backward(ctx, adj->mass, adj->e_theta_bar, adj->lambda, adj->e_bar, adj->b_bar,
+                                            result, stream))
+    return r;
+  // The records: mover, current and mass, with the B gradient.
+  err = cudaMemsetAsync(adj->b_node_bar, 0, 3 * size_t(g.nodes) * 8, s);
+  for (int sp = 0; sp < tape->ns && err == cudaSuccess; ++sp)
+    err = launch_adjoint_records(prec, kAdjointCycle, g, tape->qom[sp], dt, c, &tape->species[sp], adj->count[sp],
+                                 adj->x_bar[sp], adj->v_bar[sp], adj->q_bar[sp], tape->e_theta, adj->b_node,
+                                 adj->lambda, -kfac, adj->lambda, tape->e_theta, -kfac * g.inv_volume,
+                                 adj->b_node_bar, nullptr, ctx->invalid, s);
+  if (err == cudaSuccess) err = launch_node_ghosts(g, adj->b_node_bar, 3, s);
+  if (err == cudaSuccess) err = launch_adjoint_cells(g, 0.0, nullptr, adj->b_node_bar, adj->b_bar, s);
+  if (err != cudaSuccess) return cuda_status(err, "cycle backward (records) failed");
+  uint32_t bad = 0;
+  if (int r = read_invalid(ctx, s, &bad)) return r;
+  if (bad) return fail(TPICB200_INVALID_DATA, "the backward met invalid records");
+  return TPICB200_SUCCESS;
+}
+
+}  // extern "C"

@@ -167,6 +167,35 @@ cudaError_t launch_reduce_rows(const double* partials, double* out, int rows, in
 cudaError_t launch_copy_node_field(const Geom& g, const void* in, int in_double, double* out,
                                    cudaStream_t s);
 
+// adjoint.cu: the transposes of the cycle's stages (FP64 adjoint arithmetic;
+// particle adjoints indexed by record id, [3][nid] and [nid]).
+enum { kAdjointMover = 0, kAdjointDeposit = 1, kAdjointCycle = 2 };
+// Adds the mover's E_theta gradient of every record into the unique nodes of
+// etheta_bar (x_bar, v_bar: the gradients of the moved records).
+cudaError_t launch_adjoint_theta_scatter(int precision, const Geom& g, double qom, double dt, double c,
+                                         const tpicb200_particles* p, uint32_t nid, const double* xbar,
+                                         const double* vbar, const void* bnode, double* etheta_bar,
+                                         uint32_t* invalid, cudaStream_t s);
+// Record adjoint: kAdjointMover (the mover's backward, both scatters),
+// kAdjointDeposit (current and mass backward: jscale*jbar the J gradient,
+// mscale*<mleft, M mright> the mass term) or kAdjointCycle (both, the
+// E_theta scatter done before by launch_adjoint_theta_scatter). The B
+// gradient goes into the unique nodes of bnode_bar.
+cudaError_t launch_adjoint_records(int precision, int mode, const Geom& g, double qom, double dt, double c,
+                                   const tpicb200_particles* p, uint32_t nid, double* xbar, double* vbar,
+                                   double* qbar, const double* theta, const void* bnode, const double* jbar,
+                                   double jscale, const double* mleft, const double* mright, double mscale,
+                                   double* bnode_bar, double* etheta_bar, uint32_t* invalid, cudaStream_t s);
+// ebar (in place: the gradient of E' becomes that of E) and etheta_bar (out)
+// of the field advance; bbar (the gradient of B', equal to that of B) is read.
+cudaError_t launch_adjoint_advance(const Geom& g, double theta, double c, double dt, double* ebar, const double* bbar,
+                                   double* etheta_bar, cudaStream_t s);
+cudaError_t launch_adjoint_add_nodes(const Geom& g, const double* lambda, double* ebar, cudaStream_t s);
+cudaError_t launch_adjoint_cells(const Geom& g, double delta, const double* lambda, const double* bnode_bar,
+                                 double* bbar, cudaStream_t s);
+cudaError_t launch_energy_gradient(int precision, const Geom& g, double we, double wb, const void* e,
+                                   const void* bcell, double* ebar, double* bbar, cudaStream_t s);
+
 // solver.cu
 struct SolverWorkspace;
 // Energy-conserving smoothing of the field solve: passes (0: off), Face7
@@ -182,6 +211,13 @@ SolverWorkspace* solver_create(int precision, const Geom& g, int restart, double
 // arithmetic of the precision mode, with the solver's scratch.
 cudaError_t solver_smooth(SolverWorkspace* w, const double* in, double* out, cudaStream_t s);
 void solver_destroy(SolverWorkspace* w);
+// The adjoint solve A^T lambda = rhs (rhs a double node field with its
+// duplicates and ghosts filled) from a zero guess, by the same restarted
+// GMRES; lambda receives the solution with its ghosts. TPICB200_INVALID_STATE
+// with smoothing.
+int solver_solve_adjoint(SolverWorkspace* w, const double* rhs, const void* mass, double* lambda,
+                         tpicb200_gmres_result* result, int max_iterations, double tol, cudaStream_t s,
+                         cudaError_t* err);
 // The counter the solver's smoothing passes raise on a nonfinite value.
 void solver_set_invalid(SolverWorkspace* w, uint32_t* invalid);
 int solver_solve(SolverWorkspace* w, const void* e, const void* bcell, const void* j,

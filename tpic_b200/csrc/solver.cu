@@ -74,12 +74,21 @@ __device__ __forceinline__ void cell_curl(const Geom& g, const double* __restric
   out[2] = dx(s[1]) - dy(s[0]);
 }
 
-template <class C, class M>
+// One 3x3 block times (vx, vy, vz); kTranspose multiplies by the block's
+// transpose (the adjoint operator A^T keeps the stencil walk of A and
+// transposes every block).
+template <class C, class M, bool kTranspose = false>
 __device__ __forceinline__ void block_product(const M* __restrict__ b, long long es, C vx, C vy, C vz, C& x, C& y,
                                               C& z) {
-  x = vx * C(b[0]) + vy * C(b[es]) + vz * C(b[2 * es]);
-  y = vx * C(b[3 * es]) + vy * C(b[4 * es]) + vz * C(b[5 * es]);
-  z = vx * C(b[6 * es]) + vy * C(b[7 * es]) + vz * C(b[8 * es]);
+  if constexpr (kTranspose) {
+    x = vx * C(b[0]) + vy * C(b[3 * es]) + vz * C(b[6 * es]);
+    y = vx * C(b[es]) + vy * C(b[4 * es]) + vz * C(b[7 * es]);
+    z = vx * C(b[2 * es]) + vy * C(b[5 * es]) + vz * C(b[8 * es]);
+  } else {
+    x = vx * C(b[0]) + vy * C(b[es]) + vz * C(b[2 * es]);
+    y = vx * C(b[3 * es]) + vy * C(b[4 * es]) + vz * C(b[5 * es]);
+    z = vx * C(b[6 * es]) + vy * C(b[7 * es]) + vz * C(b[8 * es]);
+  }
 }
 
 // (M v)_g before the row volume scale: centre, then per stencil the forward
@@ -120,7 +129,7 @@ constexpr int kThinTY = 8;
 // duplicate endpoint planes equal their unique node's row (same inputs, same
 // operations) and are copied by duplicate_rows_kernel. Registers are bounded
 // for four CTAs per SM in float (64) and three in double (85).
-template <class C, class M, class Out, int TX, int TY, int TZ, bool kResponse = false>
+template <class C, class M, class Out, int TX, int TY, int TZ, bool kResponse = false, bool kTranspose = false>
 __global__ void __launch_bounds__(TX * TY * TZ, sizeof(C) == 4 ? 4 : 3) maxwell_apply_kernel(Geom g, C d2, C kfac, C inv_volume,
                                                                         const M* __restrict__ mass,
                                                                         const double* __restrict__ v,
@@ -227,7 +236,8 @@ __global__ void __launch_bounds__(TX * TY * TZ, sizeof(C) == 4 ? 4 : 3) maxwell_
   const long long at = g.node(i, j, k), es = g.mes;
   auto vv = [&](int c, int a, int b, int d) { return vs[c][lz + 1 + d][ly + 1 + b][lx + 1 + a]; };
   C x, y, z;
-  block_product<C>(mass + g.mass_index(at, 0), es, vv(0, 0, 0, 0), vv(1, 0, 0, 0), vv(2, 0, 0, 0), x, y, z);
+  block_product<C, M, kTranspose>(mass + g.mass_index(at, 0), es, vv(0, 0, 0, 0), vv(1, 0, 0, 0), vv(2, 0, 0, 0), x,
+                                  y, z);
 #pragma unroll
   for (int s = 1; s < 14; ++s) {
     const int ox = stencil_offset(s, 0), oy = stencil_offset(s, 1), oz = stencil_offset(s, 2);
@@ -246,11 +256,11 @@ __global__ void __launch_bounds__(TX * TY * TZ, sizeof(C) == 4 ? 4 : 3) maxwell_
       }
     }
     C bx, by, bz;
-    block_product<C>(mass + g.mass_index(at, s * 9), es, vv(0, ox, oy, oz), vv(1, ox, oy, oz), vv(2, ox, oy, oz),
-                     bx, by, bz);
+    block_product<C, M, kTranspose>(mass + g.mass_index(at, s * 9), es, vv(0, ox, oy, oz), vv(1, ox, oy, oz),
+                                    vv(2, ox, oy, oz), bx, by, bz);
     x += bx; y += by; z += bz;
-    block_product<C>(mass + g.mass_index(at - d, s * 9), es, vv(0, -ox, -oy, -oz), vv(1, -ox, -oy, -oz),
-                     vv(2, -ox, -oy, -oz), bx, by, bz);
+    block_product<C, M, kTranspose>(mass + g.mass_index(at - d, s * 9), es, vv(0, -ox, -oy, -oz),
+                                    vv(1, -ox, -oy, -oz), vv(2, -ox, -oy, -oz), bx, by, bz);
     x += bx; y += by; z += bz;
   }
   const C mv[3] = {x, y, z};
@@ -589,6 +599,7 @@ __global__ void arnoldi_end_kernel(ArnoldiControl* ctl, const double* status, cu
 
 struct SolverWorkspace {
   int precision;
+  bool transpose = false;       // applies use A^T (every mass block transposed): the adjoint solve
   uint32_t* invalid = nullptr;  // the context's invalid counter (smoothing passes)
   Geom g;
   int restart;
@@ -618,10 +629,11 @@ struct SolverWorkspace {
   size_t scalar_bytes;
   // The Arnoldi-step loop as a graph (built for one mass pointer).
   cudaStream_t capture = nullptr;
-  cudaGraph_t loop_graph = nullptr;
-  cudaGraphExec_t loop_exec = nullptr;
-  const void* loop_mass = nullptr;
-  unsigned loop_launches = 0;   // kernels of one step
+  // Index 0: the operator A; index 1: A^T (the adjoint solve).
+  cudaGraph_t loop_graph[2] = {nullptr, nullptr};
+  cudaGraphExec_t loop_exec[2] = {nullptr, nullptr};
+  const void* loop_mass[2] = {nullptr, nullptr};
+  unsigned loop_launches[2] = {0, 0};  // kernels of one step
   bool loop_unavailable = false;
   bool conditional_checked = false;
 
@@ -696,8 +708,10 @@ void solver_destroy(SolverWorkspace* w) {
   cudaFree(w->ximage); cudaFree(w->input); cudaFree(w->rhs); cudaFree(w->values);
   cudaFree(w->partials); cudaFree(w->state); cudaFree(w->ctl);
   cudaFree(w->smooth_a); cudaFree(w->smooth_b); cudaFree(w->smooth_image);
-  if (w->loop_exec) cudaGraphExecDestroy(w->loop_exec);
-  if (w->loop_graph) cudaGraphDestroy(w->loop_graph);
+  for (int t = 0; t < 2; ++t) {
+    if (w->loop_exec[t]) cudaGraphExecDestroy(w->loop_exec[t]);
+    if (w->loop_graph[t]) cudaGraphDestroy(w->loop_graph[t]);
+  }
   if (w->capture) cudaStreamDestroy(w->capture);
   if (w->pinned) cudaFreeHost(w->pinned);
   delete w;
@@ -752,7 +766,15 @@ struct Solve {
                                            ((g.nz + kTZ - 1) / kTZ));
     const C d2 = C(w->delta * w->delta), kf = C(w->kfac), civ = C(iv);
     const double* in = w->input;
-    if (thin && response)
+    if (w->transpose) {
+      // The adjoint solve (no smoothing): every mass block transposed.
+      if (thin)
+        launch_programmatic(maxwell_apply_kernel<C, Mass, Out, kTX, kThinTY, 1, false, true>, tiles, kTX * kThinTY, 0,
+                            st, g, d2, kf, civ, mass, in, out, response);
+      else
+        launch_programmatic(maxwell_apply_kernel<C, Mass, Out, kTX, kTY, kTZ, false, true>, tiles, kTX * kTY * kTZ, 0,
+                            st, g, d2, kf, civ, mass, in, out, response);
+    } else if (thin && response)
       launch_programmatic(maxwell_apply_kernel<C, Mass, Out, kTX, kThinTY, 1, true>, tiles, kTX * kThinTY, 0, st, g,
                           d2, kf, civ, mass, in, out, response);
     else if (thin)
@@ -831,11 +853,12 @@ struct Solve {
   // when conditional graphs are not available, and the host loop steps.
   bool loop_ready(const Mass* mass) {
     if (w->loop_unavailable || err != cudaSuccess) return false;
-    if (w->loop_exec && w->loop_mass == (const void*)mass) return true;
-    if (w->loop_exec) cudaGraphExecDestroy(w->loop_exec);
-    if (w->loop_graph) cudaGraphDestroy(w->loop_graph);
-    w->loop_exec = nullptr;
-    w->loop_graph = nullptr;
+    const int t = w->transpose ? 1 : 0;
+    if (w->loop_exec[t] && w->loop_mass[t] == (const void*)mass) return true;
+    if (w->loop_exec[t]) cudaGraphExecDestroy(w->loop_exec[t]);
+    if (w->loop_graph[t]) cudaGraphDestroy(w->loop_graph[t]);
+    w->loop_exec[t] = nullptr;
+    w->loop_graph[t] = nullptr;
     const char* stage = "self-test";
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -874,7 +897,7 @@ struct Solve {
       }
       const unsigned long long captured_launches = launches_so_far() - before;
       uncount_launches(captured_launches);
-      w->loop_launches = unsigned(captured_launches);
+      w->loop_launches[t] = unsigned(captured_launches);
     }
     if (ok) {
       stage = "instantiate";
@@ -890,9 +913,9 @@ struct Solve {
       w->loop_unavailable = true;
       return false;
     }
-    w->loop_graph = graph;
-    w->loop_exec = exec;
-    w->loop_mass = mass;
+    w->loop_graph[t] = graph;
+    w->loop_exec[t] = exec;
+    w->loop_mass[t] = mass;
     return true;
   }
 
@@ -945,14 +968,23 @@ struct Solve {
     return w->conditional_checked;
   }
 
+  // With rhs_in (a double node field, the adjoint solve): that right-hand
+  // side and a zero initial guess; otherwise the Maxwell RHS from e, bcell
+  // and j with the guess E^n.
   int run(const void* e, const void* bcell, const void* j, const void* mass_v, double* etheta,
-          tpicb200_gmres_result* result, int max_iterations, double tolerance) {
+          tpicb200_gmres_result* result, int max_iterations, double tolerance, const double* rhs_in = nullptr) {
     const Geom& g = w->g;
     const Mass* mass = (const Mass*)mass_v;
     const long long N = w->count;
     const int m = w->restart;
     tpicb200_gmres_result res{};
     const bool graph = loop_ready(mass);
+    if (rhs_in) {
+      if (err == cudaSuccess) err = cudaMemsetAsync(w->x, 0, size_t(N) * sizeof(double), s);
+      pack_kernel<double><<<blocks(), kThreads, 0, s>>>(g, rhs_in, w->b);
+      count_launches(1);
+      check();
+    } else {
     // Initial guess E^n (the copy of E into theta, maxwell_device.hpp:134-147) and the RHS.
     pack_storage_kernel<Fld><<<blocks(), kThreads, 0, s>>>(g, (const Fld*)e, w->x);
     if (w->smoothing.iterations > 0) {
@@ -972,6 +1004,7 @@ struct Solve {
     pack_kernel<double><<<blocks(), kThreads, 0, s>>>(g, w->rhs, w->b);
     count_launches(2);
     check();
+    }
     apply_solution(mass);
     residual_kernel<true><<<w->rblocks, kThreads, 0, s>>>(w->b, w->ximage, w->r, w->partials, N);
     count_launches(1);
@@ -1002,7 +1035,7 @@ struct Solve {
       check();
       ArnoldiControl control{};
       if (graph) {
-        if (err == cudaSuccess) err = cudaGraphLaunch(w->loop_exec, s);
+        if (err == cudaSuccess) err = cudaGraphLaunch(w->loop_exec[w->transpose ? 1 : 0], s);
       } else {
         for (int col = 0; col < columns; ++col) {
           step(mass, s, cudaGraphConditionalHandle{}, 0);
@@ -1020,7 +1053,7 @@ struct Solve {
       count_launches(1);
       reduce(1);
       if (!read_back(w->values, controls, &control)) return TPICB200_BACKEND_FAILURE;
-      if (graph) count_launches(w->loop_launches * unsigned(control.completed));
+      if (graph) count_launches(w->loop_launches[w->transpose ? 1 : 0] * unsigned(control.completed));
       if (control.stop == 2) return TPICB200_OVERFLOW;
       if (!std::isfinite(controls[0]) || controls[0] < 0) return TPICB200_OVERFLOW;
       res.iterations += control.completed;
@@ -1058,6 +1091,28 @@ int solver_solve(SolverWorkspace* w, const void* e, const void* bcell, const voi
 }
 
 void solver_set_invalid(SolverWorkspace* w, uint32_t* invalid) { w->invalid = invalid; }
+
+int solver_solve_adjoint(SolverWorkspace* w, const double* rhs, const void* mass, double* lambda,
+                         tpicb200_gmres_result* result, int max_iterations, double tol, cudaStream_t s,
+                         cudaError_t* err) {
+  if (w->smoothing.iterations > 0) {
+    *err = cudaSuccess;
+    return TPICB200_INVALID_STATE;
+  }
+  w->transpose = true;
+  int status;
+  if (w->precision == TPICB200_PRECISION_DOUBLE) {
+    Solve<PDouble> solve{w, s};
+    status = solve.run(nullptr, nullptr, nullptr, mass, lambda, result, max_iterations, tol, rhs);
+    *err = solve.err;
+  } else {
+    Solve<PMixed> solve{w, s};
+    status = solve.run(nullptr, nullptr, nullptr, mass, lambda, result, max_iterations, tol, rhs);
+    *err = solve.err;
+  }
+  w->transpose = false;
+  return status;
+}
 
 cudaError_t solver_smooth(SolverWorkspace* w, const double* in, double* out, cudaStream_t s) {
   const SmoothingPlan& sp = w->smoothing;
