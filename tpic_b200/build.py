@@ -18,6 +18,8 @@ HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 BUILD = HERE / "_build"
 LIBRARY = HERE / "libtpicb200.so"
+DRIVER = HERE / "tpicb200_run"
+DRIVER_SOURCE = HERE / "host" / "tpicb200_run.cpp"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
@@ -56,9 +58,26 @@ def build(verbose: bool = False) -> Path:
         result = subprocess.run(cmd, capture_output=True, text=True)
         if result.returncode != 0:
             raise RuntimeError(f"link failed:\n{result.stderr}")
+    build_driver()
     if verbose:
-        print(f"built {LIBRARY}")
+        print(f"built {LIBRARY} and {DRIVER}")
     return LIBRARY
+
+
+def build_driver() -> Path:
+    """The C++ host driver tpicb200_run (g++, linked against the in-tree
+    library and the CUDA runtime; no Python)."""
+    cuda = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
+    deps = [DRIVER_SOURCE, HERE.parent / "include" / "tpicb200.h", LIBRARY]
+    if DRIVER.exists() and DRIVER.stat().st_mtime >= max(d.stat().st_mtime for d in deps):
+        return DRIVER
+    cmd = ["g++", "-O2", "-std=c++17", "-Wall", "-Wextra", f"-I{cuda / 'include'}", str(DRIVER_SOURCE), "-o",
+           str(DRIVER), f"-L{HERE}", "-ltpicb200", f"-L{cuda / 'lib64'}", "-lcudart", "-Wl,-rpath,$ORIGIN",
+           f"-Wl,-rpath,{cuda / 'lib64'}"]
+    result = subprocess.run(cmd, capture_output=True, text=True)
+    if result.returncode != 0 or result.stderr.strip():
+        raise RuntimeError(f"driver build failed or warned:\n{result.stderr}")
+    return DRIVER
 
 
 if __name__ == "__main__":
