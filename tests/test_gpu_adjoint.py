@@ -9,10 +9,19 @@
 - Checkpoint-recompute equals keeping every tape.
 - Parameter gradients on shrunk two-stream (beam drift, density-seed
   amplitude) and anisotropy (T_perp/T_par) decks against central finite
-  differences of the FP64 forward run (h = 1e-4 relative), for the FP64
-  adjoint and for the mixed-precision runs the decks use (FP32 scalar mass
-  on the two-stream deck, BF16x3 tensor-core mass on the anisotropy deck):
-  within 1e-4 relative.
+  differences of the FP64 forward run, for the FP64 adjoint and for the
+  mixed-precision runs the decks use (FP32 scalar mass on the two-stream
+  deck, BF16x3 tensor-core mass on the anisotropy deck): within 1e-4
+  relative.
+
+A PIC run with CIC weights is only piecewise smooth in its parameters: the
+weights are continuous but their slopes jump where a particle's trajectory
+meets a cell face, so the final energy has kinks at the parameter values
+where that happens. The adjoint is the exact derivative of the discrete run
+at the nominal parameter; a central difference equals it only when no kink
+lies within +-h. The differences here therefore shrink h (from 1e-4 of the
+parameter by factors of 10) until the two one-sided differences agree within
+1e-3, which a kink inside the interval breaks.
 
 TPIC has no adjoint: nothing in the reference pins these; the oracle's
 adjoint is itself pinned to central differences (test_oracle_adjoint.py).
@@ -112,10 +121,13 @@ def test_checkpoint_recompute_equals_keeping_every_tape(torch_cuda):
             assert relative(a[k], b[k]) <= 1e-12, (s, k)
 
 
-@pytest.mark.parametrize("precision,mass_kind", [("double", "scalar"), ("mixed", "scalar")])
+@pytest.mark.parametrize("precision,mass_kind", [("double", "scalar"), ("mixed", "bf16x3")])
 def test_stage_backwards_compose_to_the_cycle_backward(torch_cuda, precision, mass_kind):
     """One cycle's backward through the per-stage entry points equals
-    tpicb200_cycle_backward on the same tape."""
+    tpicb200_cycle_backward on the same tape. Both deposit M again from the
+    tape, so the forms here are ones whose deposition sums in a fixed order
+    or in FP64 (the FP32 scalar form's float atomics would make the two M
+    differ at 1e-7)."""
     import torch
     from tpic_b200 import _lib
     from tpic_b200.adjoint import AdjointBuffers, TapeBuffers
@@ -207,9 +219,9 @@ def test_backward_rejects_smoothing_and_missing_ids(torch_cuda):
 
 # ---- parameter gradients on shrunk decks --------------------------------------------
 
-TWO_STREAM = ("twostream1d_1024.inp", "\nnxc = 64\nnpcelx = 32 32 32\nncycles = 40\nGMREStol = 1e-12\n")
+TWO_STREAM = ("twostream1d_1024.inp", "\nnxc = 64\nnpcelx = 32 32 32\nncycles = 10\nGMREStol = 1e-14\n")
 ANISOTROPY = ("anisotropy2d_512.inp", "\nnxc = 24\nnyc = 24\nLx = 2.4\nLy = 2.4\nnpcelx = 4 4\nnpcely = 4 4\n"
-                                      "ncycles = 40\nGMREStol = 1e-12\n")
+                                      "ncycles = 20\nGMREStol = 1e-14\n")
 
 
 def deck_text(spec, extra=""):
@@ -237,6 +249,21 @@ def deck_adjoint(text, precision, mass_kind, every, we, wb):
     return parsed, sim, run, adj
 
 
+def kink_free_difference(energy, p0, rel=1e-4, levels=6, agree=1e-3):
+    """Central difference of energy(p) at p0 with the largest h = rel |p0|
+    10^-k whose one-sided differences agree within `agree` (no kink inside
+    +-h); returns (difference, h)."""
+    l0 = energy(p0)
+    h = rel * abs(p0)
+    for _ in range(levels):
+        lp, lm = energy(p0 + h), energy(p0 - h)
+        right, left = (lp - l0) / h, (l0 - lm) / h
+        if abs(right - left) <= agree * max(abs(right), abs(left)):
+            return (lp - lm) / (2 * h), h
+        h /= 10
+    raise AssertionError(f"no kink-free step down to h = {h * 10:g}")
+
+
 @pytest.mark.parametrize("precision,mass_kind", [("double", "scalar"), ("mixed", "scalar")])
 def test_two_stream_gradients_match_central_differences(torch_cuda, precision, mass_kind):
     from tpic_b200.adjoint import contract, two_stream_tangents
@@ -247,15 +274,11 @@ def test_two_stream_gradients_match_central_differences(torch_cuda, precision, m
     grad_amp = contract(sim, adj, tangents["amplitude"])
     sim.close()
     u0, a = parsed.species[0].drift[0], parsed.two_stream_amplitude
-    hu, ha = 1e-4 * abs(u0), 1e-4 * abs(a)
-    fd_drift = (final_energy(deck_text(TWO_STREAM, f"\nu0 = {u0 + hu!r} {-(u0 + hu)!r} 0.0\n"), "double", "scalar",
-                             (0, 1)) -
-                final_energy(deck_text(TWO_STREAM, f"\nu0 = {u0 - hu!r} {-(u0 - hu)!r} 0.0\n"), "double", "scalar",
-                             (0, 1))) / (2 * hu)
-    fd_amp = (final_energy(deck_text(TWO_STREAM, f"\nTwoStreamSeedDensityAmplitude = {a + ha!r}\n"), "double", "scalar",
-                           (0, 1)) -
-              final_energy(deck_text(TWO_STREAM, f"\nTwoStreamSeedDensityAmplitude = {a - ha!r}\n"), "double",
-                           "scalar", (0, 1))) / (2 * ha)
+    fd_drift, _ = kink_free_difference(
+        lambda u: final_energy(deck_text(TWO_STREAM, f"\nu0 = {u!r} {-u!r} 0.0\n"), "double", "scalar", (0, 1)), u0)
+    fd_amp, _ = kink_free_difference(
+        lambda x: final_energy(deck_text(TWO_STREAM, f"\nTwoStreamSeedDensityAmplitude = {x!r}\n"), "double",
+                               "scalar", (0, 1)), a)
     assert abs(grad_drift - fd_drift) <= 1e-4 * abs(fd_drift), (grad_drift, fd_drift)
     assert abs(grad_amp - fd_amp) <= 1e-4 * abs(fd_amp), (grad_amp, fd_amp)
 
@@ -269,11 +292,10 @@ def test_anisotropy_gradient_matches_central_differences(torch_cuda, precision, 
     ratio = (vperp / vpar) ** 2
     grad = contract(sim, adj, anisotropy_tangent(run, 0, 0, ratio))
     sim.close()
-    h = 1e-4 * ratio
 
     def energy(r):
         v = vpar * math.sqrt(r)
         return final_energy(deck_text(ANISOTROPY, f"\nvth = {v!r} 0.003\nwth = {v!r} 0.003\n"), "double",
                             "moments-f64", (1,))
-    fd = (energy(ratio + h) - energy(ratio - h)) / (2 * h)
+    fd, _ = kink_free_difference(energy, ratio)
     assert abs(grad - fd) <= 1e-4 * abs(fd), (grad, fd)
