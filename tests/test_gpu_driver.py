@@ -2,7 +2,7 @@
 by `python -m tpic_b200 --run` gives the same diagnostics.csv (both load the
 records on the device from the same seed and run the same cycles through the
 C ABI), and a driver run restarted from its checkpoint continues the
-straight run bit for bit."""
+straight run (bit for bit after the restart)."""
 from __future__ import annotations
 
 import subprocess
@@ -17,6 +17,10 @@ from tpic_b200 import build as B
 pytestmark = pytest.mark.gpu
 ROOT = Path(__file__).resolve().parents[1]
 C1 = ROOT / "tpic_b200" / "decks" / "uniform3d_16.inp"
+# The row at a restart's checkpoint cycle comes from tpicb200_energy over the
+# restored records (its own summation order); the movers' scalars give the
+# straight run's row, so that row agrees to rounding and every other row bit
+# for bit.
 
 
 def rows(path: Path) -> np.ndarray:
@@ -53,4 +57,8 @@ def test_driver_restart_continues_the_run(tmp_path):
     driver(*base, "--cycles", "6", "--restart", "--output", str(restarted), cwd=tmp_path)
     text = (restarted / "diagnostics.csv").read_text()
     assert "# restart at cycle 4" in text
-    assert np.array_equal(rows(straight / "diagnostics.csv"), rows(restarted / "diagnostics.csv"))
+    a, b = rows(straight / "diagnostics.csv"), rows(restarted / "diagnostics.csv")
+    assert a.shape == b.shape == (7, 21)
+    other = np.arange(7) != 4
+    assert np.array_equal(a[other], b[other])
+    assert np.allclose(a[4], b[4], rtol=1e-12, atol=1e-300)
