@@ -163,6 +163,103 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_adjoint(args) -> None:
+    """Gradient of a deck's final-state objective by the adjoint (the deck's
+    precision and mass form, checkpoints every --checkpoint-every cycles)
+    against central differences of the FP64 forward run: at h = 1e-4 of the
+    parameter, and at the largest h = 1e-4 |p| 10^-k (k <= 6) whose one-sided
+    differences agree within 1e-3 (no cell-crossing kink inside +-h), if any.
+    Two-stream decks: d(W_E + W_B)/d(beam drift) and d/d(density-seed
+    amplitude); anisotropy decks (Uniform with a bi-Maxwellian species):
+    d(W_B)/d(T_perp/T_par) of species 0 about x."""
+    import torch
+    from tpic_b200 import deck as D
+    from tpic_b200.adjoint import AdjointRun, anisotropy_tangent, contract, two_stream_tangents
+    from tpic_b200.simulation import Simulation
+    if not args.deck:
+        raise SystemExit("--adjoint needs --deck")
+    text = Path(args.deck).read_text()
+    parsed = D.parse(text)
+    case = D.to_case(parsed)
+    name = D.case_name(parsed)
+    ncycles = parsed.ncycles
+    nparticles = sum(case.grid.cells * sp.ppc for sp in case.species)
+    torch.cuda.set_device(0)
+    sim = Simulation(case, precision=args.precision, mass_kind=args.mass_matrix, keep_ids=True,
+                     generate_on_device=True, gmres_max_iterations=args.gmres_max_iterations)
+    sim.prepare()
+    run = AdjointRun(sim, every=args.checkpoint_every)
+    t0 = time.perf_counter()
+    run.forward(ncycles)
+    if name == "TwoStream":
+        we, wb, objective = 1.0, 1.0, "W_E + W_B"
+    else:
+        we, wb, objective = 0.0, 1.0, "W_B"
+    adj = run.backward(we, wb)
+    torch.cuda.synchronize()
+    total_s = time.perf_counter() - t0
+    params = {}
+    if name == "TwoStream":
+        tangents = two_stream_tangents(run, parsed)
+        params["drift"] = (contract(sim, adj, tangents["drift"]), parsed.species[0].drift[0])
+        params["amplitude"] = (contract(sim, adj, tangents["amplitude"]), parsed.two_stream_amplitude)
+    else:
+        vpar, vperp = parsed.species[0].vth[0], parsed.species[0].vth[1]
+        ratio = (vperp / vpar) ** 2
+        params["anisotropy"] = (contract(sim, adj, anisotropy_tangent(run, 0, 0, ratio)), ratio)
+    stats = run.stats
+    sim.close()
+    del sim, run, adj
+    torch.cuda.empty_cache()
+
+    def energy(param: str, value: float) -> float:
+        if param == "drift":
+            extra = f"\nu0 = {value!r} {-value!r} 0.0\n"
+        elif param == "amplitude":
+            extra = f"\nTwoStreamSeedDensityAmplitude = {value!r}\n"
+        else:
+            v = parsed.species[0].vth[0] * math.sqrt(value)
+            extra = f"\nvth = {v!r} {parsed.species[1].vth[1]!r}\nwth = {v!r} {parsed.species[1].vth[2]!r}\n"
+        dk = D.parse(text + extra + "\nGMREStol = 1e-12\n")
+        fd_sim = Simulation(D.to_case(dk), precision="double", mass_kind="moments-f64", generate_on_device=True,
+                            gmres_max_iterations=max(args.gmres_max_iterations, 500))
+        fd_sim.prepare()
+        r = fd_sim.run(ncycles)[-1]
+        fd_sim.close()
+        return we * r.field_energy[0] + wb * r.field_energy[1]
+
+    gradients = {}
+    for param, (grad, p0) in params.items():
+        l0 = energy(param, p0)
+        h = 1e-4 * abs(p0)
+        lp, lm = energy(param, p0 + h), energy(param, p0 - h)
+        fd4 = (lp - lm) / (2 * h)
+        entry = {"adjoint": grad, "fd_h1e-4": fd4, "rel_err_h1e-4": abs(grad - fd4) / abs(fd4),
+                 "one_sided_h1e-4": [(l0 - lm) / h, (lp - l0) / h]}
+        kink_free = None
+        for _ in range(6):
+            right, left = (lp - l0) / h, (l0 - lm) / h
+            if abs(right - left) <= 1e-3 * max(abs(right), abs(left)):
+                kink_free = {"h_rel": h / abs(p0), "fd": (lp - lm) / (2 * h),
+                             "rel_err": abs(grad - (lp - lm) / (2 * h)) / abs((lp - lm) / (2 * h))}
+                break
+            h /= 10
+            lp, lm = energy(param, p0 + h), energy(param, p0 - h)
+        entry["kink_free"] = kink_free
+        gradients[param] = entry
+    line = {"metric": "adjoint gradient of the final field energy: forward + recompute + backward", "value": total_s,
+            "unit": "s", "higher_is_better": False, "impl": "tpic_b200", "n_gpus": 1,
+            "config": {"workload": f"deck {Path(args.deck).name}: {name}", "particles": nparticles,
+                       "cycles": ncycles, "precision": args.precision, "mass_matrix": args.mass_matrix,
+                       "checkpoint_every": args.checkpoint_every, "objective": objective},
+            "forward_s": stats.forward_s, "recompute_s": stats.recompute_s, "backward_s": stats.backward_s,
+            "backward_over_forward": (stats.recompute_s + stats.backward_s) / stats.forward_s,
+            "checkpoints": stats.checkpoints, "tapes": stats.tapes, "tape_bytes": stats.device_bytes,
+            "adjoint_gmres_iterations_mean": float(np.mean(stats.adjoint_iterations)),
+            "gradients": gradients}
+    print(json.dumps(line), flush=True)
+
+
 def max_over_ranks(seconds: float, dist, device) -> float:
     """The slowest rank's time (every rank takes part; a no-op on one rank)."""
     if dist is None:
@@ -589,6 +686,10 @@ def main():
     ap.add_argument("--sweep", action=argparse.BooleanOptionalAction, default=True,
                     help="also time the FP64 moment and TF32 forms and state every form's bootstrap mass and J "
                          "error against the FP64 moment form (default on; off for decks)")
+    ap.add_argument("--adjoint", action="store_true",
+                    help="with --deck (two-stream or anisotropy): gradients by the adjoint with checkpoint-recompute, "
+                         "against central differences of the FP64 forward run, and the backward/forward time ratio")
+    ap.add_argument("--checkpoint-every", type=int, default=20, help="adjoint checkpoint interval (cycles)")
     ap.add_argument("--e2e-cycles", type=int, default=20,
                     help="cycles of the end-to-end episode (upload, startup, cycles, energy readback)")
     ap.add_argument("--cpu-workers", type=int, default=0, help="host processes of the reference arm (0: all cores)")
@@ -597,6 +698,8 @@ def main():
         ap.error("at least 3 warm-up steps")
     if args.impl == "reference":
         run_reference(args)
+    elif args.adjoint:
+        run_adjoint(args)
     else:
         run_gpu(args)
 
