@@ -166,12 +166,14 @@ def run_reference(args) -> None:
 def run_adjoint(args) -> None:
     """Gradient of a deck's final-state objective by the adjoint (the deck's
     precision and mass form, checkpoints every --checkpoint-every cycles)
-    against central differences of the FP64 forward run: at h = 1e-4 of the
+    against central differences of the FP64 forward run, over one or more
+    horizons (--horizons, default the deck's ncycles): at h = 1e-4 of the
     parameter, and at the largest h = 1e-4 |p| 10^-k (k <= 6) whose one-sided
     differences agree within 1e-3 (no cell-crossing kink inside +-h), if any.
     Two-stream decks: d(W_E + W_B)/d(beam drift) and d/d(density-seed
     amplitude); anisotropy decks (Uniform with a bi-Maxwellian species):
-    d(W_B)/d(T_perp/T_par) of species 0 about x."""
+    d(W_B)/d(T_perp/T_par) of species 0 about x. With --adjoint-fp64 the FP64
+    adjoint (FP64 moment form) runs beside the deck's precision."""
     import torch
     from tpic_b200 import deck as D
     from tpic_b200.adjoint import AdjointRun, anisotropy_tangent, contract, two_stream_tangents
@@ -180,39 +182,48 @@ def run_adjoint(args) -> None:
         raise SystemExit("--adjoint needs --deck")
     text = Path(args.deck).read_text()
     parsed = D.parse(text)
-    case = D.to_case(parsed)
     name = D.case_name(parsed)
-    ncycles = parsed.ncycles
+    horizons = [int(h) for h in args.horizons.split(",")] if args.horizons else [parsed.ncycles]
+    case = D.to_case(parsed)
     nparticles = sum(case.grid.cells * sp.ppc for sp in case.species)
     torch.cuda.set_device(0)
-    sim = Simulation(case, precision=args.precision, mass_kind=args.mass_matrix, keep_ids=True,
-                     generate_on_device=True, gmres_max_iterations=args.gmres_max_iterations)
-    sim.prepare()
-    run = AdjointRun(sim, every=args.checkpoint_every)
-    t0 = time.perf_counter()
-    run.forward(ncycles)
     if name == "TwoStream":
         we, wb, objective = 1.0, 1.0, "W_E + W_B"
     else:
         we, wb, objective = 0.0, 1.0, "W_B"
-    adj = run.backward(we, wb)
-    torch.cuda.synchronize()
-    total_s = time.perf_counter() - t0
-    params = {}
-    if name == "TwoStream":
-        tangents = two_stream_tangents(run, parsed)
-        params["drift"] = (contract(sim, adj, tangents["drift"]), parsed.species[0].drift[0])
-        params["amplitude"] = (contract(sim, adj, tangents["amplitude"]), parsed.two_stream_amplitude)
-    else:
-        vpar, vperp = parsed.species[0].vth[0], parsed.species[0].vth[1]
-        ratio = (vperp / vpar) ** 2
-        params["anisotropy"] = (contract(sim, adj, anisotropy_tangent(run, 0, 0, ratio)), ratio)
-    stats = run.stats
-    sim.close()
-    del sim, run, adj
-    torch.cuda.empty_cache()
 
-    def energy(param: str, value: float) -> float:
+    def adjoint(ncycles: int, precision: str, mass_matrix: str):
+        sim = Simulation(case, precision=precision, mass_kind=mass_matrix, keep_ids=True, generate_on_device=True,
+                         gmres_max_iterations=args.gmres_max_iterations)
+        sim.prepare()
+        run = AdjointRun(sim, every=args.checkpoint_every)
+        t0 = time.perf_counter()
+        run.forward(ncycles)
+        adj = run.backward(we, wb)
+        torch.cuda.synchronize()
+        total_s = time.perf_counter() - t0
+        grads = {}
+        if name == "TwoStream":
+            tangents = two_stream_tangents(run, parsed)
+            grads["drift"] = contract(sim, adj, tangents["drift"])
+            grads["amplitude"] = contract(sim, adj, tangents["amplitude"])
+        else:
+            vpar, vperp = parsed.species[0].vth[0], parsed.species[0].vth[1]
+            grads["anisotropy"] = contract(sim, adj, anisotropy_tangent(run, 0, 0, (vperp / vpar) ** 2))
+        stats = run.stats
+        sim.close()
+        del sim, run, adj
+        torch.cuda.empty_cache()
+        return grads, stats, total_s
+
+    def param_value(param: str) -> float:
+        if param == "drift":
+            return parsed.species[0].drift[0]
+        if param == "amplitude":
+            return parsed.two_stream_amplitude
+        return (parsed.species[0].vth[1] / parsed.species[0].vth[0]) ** 2
+
+    def energy(param: str, value: float, ncycles: int) -> float:
         if param == "drift":
             extra = f"\nu0 = {value!r} {-value!r} 0.0\n"
         elif param == "amplitude":
@@ -228,35 +239,46 @@ def run_adjoint(args) -> None:
         fd_sim.close()
         return we * r.field_energy[0] + wb * r.field_energy[1]
 
-    gradients = {}
-    for param, (grad, p0) in params.items():
-        l0 = energy(param, p0)
-        h = 1e-4 * abs(p0)
-        lp, lm = energy(param, p0 + h), energy(param, p0 - h)
-        fd4 = (lp - lm) / (2 * h)
-        entry = {"adjoint": grad, "fd_h1e-4": fd4, "rel_err_h1e-4": abs(grad - fd4) / abs(fd4),
+    results = []
+    for ncycles in horizons:
+        grads, stats, total_s = adjoint(ncycles, args.precision, args.mass_matrix)
+        entry = {"cycles": ncycles, "seconds": total_s, "forward_s": stats.forward_s,
+                 "recompute_s": stats.recompute_s, "backward_s": stats.backward_s,
+                 "backward_over_forward": (stats.recompute_s + stats.backward_s) / stats.forward_s,
+                 "checkpoints": stats.checkpoints, "tapes": stats.tapes, "tape_bytes": stats.device_bytes,
+                 "adjoint_gmres_iterations_mean": float(np.mean(stats.adjoint_iterations)), "gradients": {}}
+        fp64 = adjoint(ncycles, "double", "moments-f64")[0] if args.adjoint_fp64 else None
+        for param, grad in grads.items():
+            p0 = param_value(param)
+            l0 = energy(param, p0, ncycles)
+            h = 1e-4 * abs(p0)
+            lp, lm = energy(param, p0 + h, ncycles), energy(param, p0 - h, ncycles)
+            fd4 = (lp - lm) / (2 * h)
+            g = {"adjoint": grad, "fd_h1e-4": fd4, "rel_err_h1e-4": abs(grad - fd4) / abs(fd4),
                  "one_sided_h1e-4": [(l0 - lm) / h, (lp - l0) / h]}
-        kink_free = None
-        for _ in range(6):
-            right, left = (lp - l0) / h, (l0 - lm) / h
-            if abs(right - left) <= 1e-3 * max(abs(right), abs(left)):
-                kink_free = {"h_rel": h / abs(p0), "fd": (lp - lm) / (2 * h),
-                             "rel_err": abs(grad - (lp - lm) / (2 * h)) / abs((lp - lm) / (2 * h))}
-                break
-            h /= 10
-            lp, lm = energy(param, p0 + h), energy(param, p0 - h)
-        entry["kink_free"] = kink_free
-        gradients[param] = entry
-    line = {"metric": "adjoint gradient of the final field energy: forward + recompute + backward", "value": total_s,
-            "unit": "s", "higher_is_better": False, "impl": "tpic_b200", "n_gpus": 1,
+            if fp64 is not None:
+                g["adjoint_fp64"] = fp64[param]
+                g["rel_diff_fp64_adjoint"] = abs(grad - fp64[param]) / abs(fp64[param])
+            kink_free = None
+            for _ in range(6):
+                right, left = (lp - l0) / h, (l0 - lm) / h
+                if abs(right - left) <= 1e-3 * max(abs(right), abs(left)):
+                    fd = (lp - lm) / (2 * h)
+                    kink_free = {"h_rel": h / abs(p0), "fd": fd, "rel_err": abs(grad - fd) / abs(fd)}
+                    break
+                h /= 10
+                lp, lm = energy(param, p0 + h, ncycles), energy(param, p0 - h, ncycles)
+            g["kink_free"] = kink_free
+            entry["gradients"][param] = g
+        results.append(entry)
+        print(json.dumps({"horizon": entry}), flush=True)
+    line = {"metric": "adjoint gradient of the final field energy: forward + recompute + backward",
+            "value": results[-1]["seconds"], "unit": "s", "higher_is_better": False, "impl": "tpic_b200",
+            "n_gpus": 1,
             "config": {"workload": f"deck {Path(args.deck).name}: {name}", "particles": nparticles,
-                       "cycles": ncycles, "precision": args.precision, "mass_matrix": args.mass_matrix,
+                       "precision": args.precision, "mass_matrix": args.mass_matrix,
                        "checkpoint_every": args.checkpoint_every, "objective": objective},
-            "forward_s": stats.forward_s, "recompute_s": stats.recompute_s, "backward_s": stats.backward_s,
-            "backward_over_forward": (stats.recompute_s + stats.backward_s) / stats.forward_s,
-            "checkpoints": stats.checkpoints, "tapes": stats.tapes, "tape_bytes": stats.device_bytes,
-            "adjoint_gmres_iterations_mean": float(np.mean(stats.adjoint_iterations)),
-            "gradients": gradients}
+            "horizons": results}
     print(json.dumps(line), flush=True)
 
 
@@ -690,6 +712,8 @@ def main():
                     help="with --deck (two-stream or anisotropy): gradients by the adjoint with checkpoint-recompute, "
                          "against central differences of the FP64 forward run, and the backward/forward time ratio")
     ap.add_argument("--checkpoint-every", type=int, default=20, help="adjoint checkpoint interval (cycles)")
+    ap.add_argument("--horizons", default="", help="adjoint: comma-separated cycle counts (default: the deck's)")
+    ap.add_argument("--adjoint-fp64", action="store_true", help="adjoint: also the FP64 adjoint at each horizon")
     ap.add_argument("--e2e-cycles", type=int, default=20,
                     help="cycles of the end-to-end episode (upload, startup, cycles, energy readback)")
     ap.add_argument("--cpu-workers", type=int, default=0, help="host processes of the reference arm (0: all cores)")
