@@ -287,6 +287,15 @@ int tpicb200_smooth(tpicb200_context* ctx, const double* in, double* out, tpicb2
  * after the enqueued work (simulation/driver/pipeline.hpp:145-146). Host-blocking. */
 int tpicb200_read_invalid(tpicb200_context* ctx, uint32_t* count, int clear, tpicb200_stream stream);
 
+/* Bound of the device-side waits of the BF16X3 tensor-core deposition (the
+ * wait for a chunk's MMAs and for the issuer's published decision): polls
+ * before a wait gives up, 0 restoring the default of 4,194,304. A wait that
+ * gives up makes its CTA leave the chunk loop, wait (with the default bound)
+ * for the MMAs it has in flight and free its tensor memory; the deposition
+ * then adds 1 << 20 to the invalid counter and tpicb200_cycle returns
+ * TPICB200_INVALID_DATA. A small bound serves to test that path. */
+int tpicb200_set_wait_limit(tpicb200_context* ctx, uint32_t polls);
+
 /* Zero J (node field) and the mass records. Replaces enqueue_clear_mass_matrix
  * (ecsim/mass_matrix/mass_matrix_deposition_device.hpp:107-121) and the moment clear. */
 int tpicb200_clear_moments(tpicb200_context* ctx, void* j, void* mass, tpicb200_stream stream);

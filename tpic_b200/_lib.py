@@ -141,6 +141,7 @@ EXPORTS = {
     "tpicb200_magnetic_to_nodes": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tpicb200_smooth": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tpicb200_read_invalid": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint32), C.c_int, C.c_void_p]),
+    "tpicb200_set_wait_limit": (C.c_int, [C.c_void_p, C.c_uint32]),
     "tpicb200_energy": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(Particles),
                                   C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_double), C.c_void_p]),
     "tpicb200_prepare": (C.c_int, [C.c_void_p, C.POINTER(State), C.c_void_p]),

@@ -40,6 +40,7 @@ struct tpicb200_context {
   // else has deposited into since: the assembly may store instead of add.
   const void* cleared_j = nullptr;
   const void* cleared_mass = nullptr;
+  uint32_t wait_polls = 0;  // tensor-core stream kernel wait bound (0: the default)
 };
 
 namespace {
@@ -100,7 +101,7 @@ cudaError_t launch_moments(tpicb200_context* ctx, int kind, int ns, const double
     return launch_deposit_moments_f64(ctx->g, ns, qom, ctx->opt.dt, ctx->opt.c, parts, counts, offsets, b_node,
                                       (double*)ctx->moments, accumulate, invalid, copies, s);
   return launch_deposit_tc(kind, ctx->g, ns, qom, ctx->opt.dt, ctx->opt.c, parts, counts, offsets, b_node,
-                           (float*)ctx->moments, accumulate, invalid, copies, s);
+                           (float*)ctx->moments, accumulate, invalid, copies, s, ctx->wait_polls);
 }
 
 }  // namespace
@@ -769,6 +770,12 @@ static int read_invalid(tpicb200_context* ctx, cudaStream_t s, uint32_t* value) 
   if (err == cudaSuccess) err = cudaStreamSynchronize(s);
   if (err != cudaSuccess) return cuda_status(err, "invalid-flag readback failed");
   std::memcpy(value, ctx->pinned, 4);
+  return TPICB200_SUCCESS;
+}
+
+int tpicb200_set_wait_limit(tpicb200_context* ctx, uint32_t polls) {
+  if (int s = check_ctx(ctx)) return s;
+  ctx->wait_polls = polls;
   return TPICB200_SUCCESS;
 }
 

@@ -128,10 +128,14 @@ cudaError_t launch_fold(int precision, const Geom& g, void* j, void* mass, cudaS
 size_t moment_floats(const Geom& g);
 // Tensor-core deposition of `ns` species (fused two per launch) into the
 // per-cell moments; `accumulate` adds to moments already present.
+// wait_polls bounds the BF16X3 stream kernel's chunk-loop waits (0: the
+// default kDefaultWaitPolls); a wait that gives up sets bit 20 of *invalid.
+constexpr uint32_t kDefaultWaitPolls = 1u << 22;
 cudaError_t launch_deposit_tc(int mass_kind, const Geom& g, int ns, const double* qom, double dt, double c,
                               const tpicb200_particles* const* p, const uint32_t* const* counts,
                               const uint32_t* const* offsets, const void* bnode, float* moments, int accumulate,
-                              uint32_t* invalid, const SortedCopy* const* copies, cudaStream_t s);
+                              uint32_t* invalid, const SortedCopy* const* copies, cudaStream_t s,
+                              uint32_t wait_polls = 0);
 // FP64 CUDA-core form of the same moments (double precision; double moments).
 cudaError_t launch_deposit_moments_f64(const Geom& g, int ns, const double* qom, double dt, double c,
                                        const tpicb200_particles* const* p, const uint32_t* const* counts,

@@ -116,6 +116,7 @@ struct TcParams {
   TcSpecies sp[kFuse];
   int ns;
   float inv_volume;
+  uint32_t wait_polls;  // polls of the stream kernel's chunk-loop waits before they give up
 };
 
 template <bool Bf16> struct __align__(128) TcShared {
@@ -959,7 +960,6 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
   StreamInfo i1 = ia;
   StreamInfo ip{0, 0u};  // the previous chunk, whose cells are flushed next
   bool bad = false;
-  uint32_t last_arrived = 0xFFFFFFFFu;  // the last chunk this warp arrived for
   const int kofs = (lane >> 3) * 128 + (lane & 7) * 16;  // lane's K row in a 512-byte core group
   for (uint32_t j = 0;; ++j) {
     const StreamRec r0 = r1;
@@ -1045,7 +1045,7 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
     // The MMAs of chunk j - 1 have completed: flush the cells that ended in
     // it; a warp without chunks learns whether any warp of the CTA has one.
     if (j > 0) {
-      const bool done = tc::mbar_wait(&sh.mma_bar, (j - 1) & 1u);
+      const bool done = tc::mbar_wait(&sh.mma_bar, (j - 1) & 1u, tp.wait_polls);
       if (__any_sync(0xffffffffu, !done)) {
         bad = true;
         break;
@@ -1056,7 +1056,7 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
         // The issuer of chunk j - 1 published whether any warp has chunk j.
         uint32_t d = 0;
         bool seen = false;
-        for (uint32_t i = 0; i < (1u << 22) && !seen; ++i) {
+        for (uint32_t i = 0; i < tp.wait_polls && !seen; ++i) {
           d = tc::ld_acquire(&sh.decision);
           seen = (d >> 1) == ((j - 1) & 0x7FFFFFFFu);
         }
@@ -1126,15 +1126,24 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
         tc::commit(&sh.mma_bar);
       }
     }
-    last_arrived = j;
     ip = i0;
   }
 
   tc::cp_async_wait_all();
   if (bad && lane == 0) atomicAdd(invalid, 1u << 20);
-  // After a failed wait the MMAs of the last chunk may still be in flight:
-  // wait for them (bounded) before the tensor memory is freed.
-  if (bad && lane == 0 && last_arrived != 0xFFFFFFFFu) tc::mbar_wait(&sh.mma_bar, last_arrived & 1u);
+  // Every warp has left the chunk loop, so no chunk is issued after this
+  // barrier. The issuer publishes a chunk's index before issuing its MMAs:
+  // the last published chunk is the last issued one. After a failed wait its
+  // MMAs may still be in flight; one thread waits for them (with the default
+  // bound, whatever tp.wait_polls is) before the tensor memory is freed. On
+  // the normal path that chunk has completed and the wait returns at once.
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  if (threadIdx.x == 0) {
+    const uint32_t d = tc::ld_acquire(&sh.decision);
+    if (d != 0xFFFFFFFEu) tc::mbar_wait(&sh.mma_bar, (d >> 1) & 1u);
+  }
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
@@ -1152,7 +1161,8 @@ size_t moment_floats(const Geom& g) { return size_t(kMoments) * size_t(moment_st
 cudaError_t launch_deposit_tc(int mass_kind, const Geom& g, int ns, const double* qom, double dt, double c,
                               const tpicb200_particles* const* p, const uint32_t* const* counts,
                               const uint32_t* const* offsets, const void* bnode, float* moments, int accumulate,
-                              uint32_t* invalid, const SortedCopy* const* copies, cudaStream_t s) {
+                              uint32_t* invalid, const SortedCopy* const* copies, cudaStream_t s,
+                              uint32_t wait_polls) {
   if (mass_kind != TPICB200_MASS_TF32 && mass_kind != TPICB200_MASS_BF16X3) return cudaErrorNotSupported;
   if (!moments || ns < 1) return cudaErrorInvalidValue;
   int device = 0, sms = 148;
@@ -1187,6 +1197,7 @@ cudaError_t launch_deposit_tc(int mass_kind, const Geom& g, int ns, const double
     TcParams tp{};
     tp.ns = std::min(kFuse, ns - first);
     tp.inv_volume = float(g.inv_volume);
+    tp.wait_polls = wait_polls ? wait_polls : kDefaultWaitPolls;
     for (int i = 0; i < tp.ns; ++i) {
       const tpicb200_particles* sp = p[first + i];
       const SortedCopy* cp = copies ? copies[first + i] : nullptr;
