@@ -194,7 +194,7 @@ def run_adjoint(args) -> None:
 
     def adjoint(ncycles: int, precision: str, mass_matrix: str):
         sim = Simulation(case, precision=precision, mass_kind=mass_matrix, keep_ids=True, generate_on_device=True,
-                         gmres_max_iterations=args.gmres_max_iterations)
+                         gmres_max_iterations=args.gmres_max_iterations, mass_layout=args.mass_layout)
         sim.prepare()
         run = AdjointRun(sim, every=args.checkpoint_every)
         t0 = time.perf_counter()
@@ -276,7 +276,7 @@ def run_adjoint(args) -> None:
             "value": results[-1]["seconds"], "unit": "s", "higher_is_better": False, "impl": "tpic_b200",
             "n_gpus": 1,
             "config": {"workload": f"deck {Path(args.deck).name}: {name}", "particles": nparticles,
-                       "precision": args.precision, "mass_matrix": args.mass_matrix,
+                       "precision": args.precision, "mass_matrix": args.mass_matrix, "mass_layout": args.mass_layout,
                        "checkpoint_every": args.checkpoint_every, "objective": objective},
             "horizons": results}
     print(json.dumps(line), flush=True)
@@ -364,7 +364,8 @@ def run_gpu(args) -> None:
         precision = precision or args.precision
         t_gen = time.perf_counter()
         sim = Simulation(case, precision=precision, mass_kind=mass_kind, device=local, generate_on_device=True,
-                         gmres_max_iterations=args.gmres_max_iterations, smoothing=smoothing)
+                         gmres_max_iterations=args.gmres_max_iterations, smoothing=smoothing,
+                         mass_layout=args.mass_layout)
         if precision == "double" and args.precision == "mixed":
             # The same state as the mixed forms: their FP32 velocities, widened.
             for s in range(len(case.species)):
@@ -476,7 +477,7 @@ def run_gpu(args) -> None:
                 "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32" if args.precision == "mixed" else "f64", "data": "synthetic",
                 "config": {"workload": workload_name, "particles": nparticles,
-                           "precision": args.precision, "mass_matrix": args.mass_matrix, "dt": case.dt,
+                           "precision": args.precision, "mass_matrix": args.mass_matrix, "mass_layout": args.mass_layout, "dt": case.dt,
                            "theta": case.theta, "gmres_tol": case.gmres_tol,
                            "gmres_max_iterations": args.gmres_max_iterations, "l2": l2_note,
                            "smoothing": ({"passes": smoothing[0], "alpha": smoothing[1],
@@ -696,6 +697,8 @@ def main():
                     help="second form timed on the same workload (default: the plain FP32 CUDA-core form)")
     ap.add_argument("--drift-cycles", type=int, default=100, help="cycles of the energy-drift run of each form")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "double"])
+    ap.add_argument("--mass-layout", default="tiled", choices=["records", "stencil-major", "tiled"],
+                    help="mass buffer layout (tiled: 16-byte rows, the operator apply stages them by TMA)")
     ap.add_argument("--scale", type=int, default=128, help="cells per axis of the workload")
     ap.add_argument("--smoothing", default="",
                     help="energy-conserving smoothing as PASSES,ALPHA,OPERATOR (0 face7, 1 binomial27); off by default")

@@ -85,7 +85,14 @@ enum { TPICB200_PRECISION_DOUBLE = 0, TPICB200_PRECISION_MIXED = 1 };
  * k = 9*stencil + component of vertex v at k*node_count + v, so a warp
  * applying the matrix to 32 consecutive nodes reads each entry with one
  * coalesced 128-byte request. */
-enum { TPICB200_MASS_LAYOUT_RECORDS = 0, TPICB200_MASS_LAYOUT_STENCIL_MAJOR = 1 };
+enum { TPICB200_MASS_LAYOUT_RECORDS = 0, TPICB200_MASS_LAYOUT_STENCIL_MAJOR = 1, TPICB200_MASS_LAYOUT_TILED = 2 };
+/* TILED is STENCIL_MAJOR with each x row of a plane padded from nx+3 to a
+ * multiple of 4 vertices: entry k of vertex (i, j, k3) at
+ * k*plane + (i+1) + mx*((j+1) + (ny+3)*(k3+1)), mx = (nx+3) rounded up to a
+ * multiple of 4, plane = mx*(ny+3)*(nz+3). Every row then starts on a 16-byte
+ * boundary, so the field solve reads the mass with tensor-memory-access box
+ * copies. The padding is never read or written. A mass buffer holds
+ * tpicb200_layout.mass_count scalars in every layout. */
 
 /* Mass-matrix assembly forms, the extended `--mass-matrix` selection
  * (TPIC: scalar | matrix-core, config/numerics_options.hpp:31-47). */
@@ -138,6 +145,7 @@ typedef struct {
   size_t field_scalar_bytes; /* sizeof E/B/J scalars: 8 (DOUBLE) or 4 (MIXED) */
   size_t mass_scalar_bytes;  /* sizeof mass scalars */
   size_t velocity_scalar_bytes;
+  int64_t mass_count;        /* scalars of a mass buffer in the context's layout */
 } tpicb200_layout;
 
 typedef struct {

@@ -115,23 +115,36 @@ class StageContext:
                                                  self.invalid.data_ptr(), self.stream))
         return dst, counts, offsets
 
+    def _tiled_shape(self):
+        g = self.g
+        mx = (g.nx + 3 + 3) // 4 * 4
+        return (126, g.nz + 3, g.ny + 3, mx)
+
     def records(self, m) -> np.ndarray:
         """Mass coefficients of a device buffer in TPIC's record order (float64)."""
         a = m.cpu().numpy().astype(np.float64)
         if self.mass_layout == 1:
             a = np.ascontiguousarray(a.reshape(126, -1).T).ravel()
+        elif self.mass_layout == 2:
+            t = a.reshape(self._tiled_shape())[..., :self.g.nx + 3]
+            a = np.ascontiguousarray(t.reshape(126, -1).T).ravel()
         return a
 
     def mass_from_records(self, rec: np.ndarray):
         a = rec.astype(self.np_fdt)
         if self.mass_layout == 1:
             a = np.ascontiguousarray(a.reshape(-1, 126).T).ravel()
+        elif self.mass_layout == 2:
+            g = self.g
+            t = np.zeros(self._tiled_shape(), dtype=self.np_fdt)
+            t[..., :g.nx + 3] = a.reshape(-1, 126).T.reshape(126, g.nz + 3, g.ny + 3, g.nx + 3)
+            a = t.ravel()
         return torch.from_numpy(a).cuda()
 
     def moments(self):
         nodes = self.layout.node_count
         j = torch.zeros(3 * nodes, dtype=self.fdt, device="cuda")
-        m = torch.zeros(126 * nodes, dtype=self.fdt, device="cuda")
+        m = torch.zeros(self.layout.mass_count, dtype=self.fdt, device="cuda")
         return j, m
 
     def deposit(self, qom, parts: dict, n: int, bnode, j, m, counts=None, offsets=None, kind=0):

@@ -37,7 +37,8 @@ def run_both(case, precision, cycles, mass_kind="scalar", mass_layout="records")
 
 
 @pytest.mark.parametrize("mass_layout,mass_kind", [("records", "scalar"), ("stencil-major", "scalar"),
-                                                   ("records", "moments-f64"), ("stencil-major", "moments-f64")])
+                                                   ("records", "moments-f64"), ("stencil-major", "moments-f64"),
+                                                   ("tiled", "scalar"), ("tiled", "moments-f64")])
 def test_c1_cycle_matches_oracle_fp64(mass_layout, mass_kind):
     case = c1_case(n=16)
     sim, reports, oc, energies = run_both(case, 0, 3, mass_kind=mass_kind, mass_layout=mass_layout)

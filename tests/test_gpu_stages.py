@@ -151,7 +151,7 @@ def assert_moments(g, jg, mg, jw, mw, rel):
 
 @pytest.mark.parametrize("precision,kind,sorted_bins,layout", [
     (0, 0, True, 0), (0, 0, False, 0), (1, 0, True, 0), (1, 0, False, 0), (1, 1, True, 0), (0, 1, True, 0),
-    (0, 0, True, 1), (1, 0, False, 1), (1, 0, True, 1)])
+    (0, 0, True, 1), (1, 0, False, 1), (1, 0, True, 1), (0, 0, True, 2), (1, 0, False, 2)])
 def test_deposit_matches_oracle(torch_cuda, precision, kind, sorted_bins, layout):
     g = GRID
     rng = np.random.default_rng(21)
@@ -194,7 +194,7 @@ def test_reference_mass_fixture(torch_cuda, precision, kind):
     assert np.abs(gi - wi).max() <= rel * np.abs(wi).max() + 1e-15
 
 
-@pytest.mark.parametrize("layout", [0, 1])
+@pytest.mark.parametrize("layout", [0, 1, 2])
 def test_mass_apply_matches_oracle(torch_cuda, layout):
     g = GRID
     rng = np.random.default_rng(2)
@@ -230,7 +230,7 @@ def prepared_oracle(g, precision, seed=1):
     return oc
 
 
-@pytest.mark.parametrize("layout", [0, 1])
+@pytest.mark.parametrize("layout", [0, 1, 2])
 def test_field_solve_matches_oracle(torch_cuda, layout):
     g = GRID
     oc = prepared_oracle(g, 0)
@@ -360,7 +360,7 @@ def test_tc_exact_inputs(torch_cuda, kind, nx):
 
 
 @pytest.mark.parametrize("kind,rel,layout,nx", [(2, 3e-3, 0, 6), (3, 1e-4, 0, 6), (2, 3e-3, 1, 6), (3, 1e-4, 1, 6),
-                                                 (3, 1e-4, 1, 8), (2, 3e-3, 0, 8)])
+                                                 (3, 1e-4, 1, 8), (2, 3e-3, 0, 8), (3, 1e-4, 2, 6)])
 def test_tc_mass_matches_oracle(torch_cuda, kind, rel, layout, nx):
     g = GRID if nx == GRID.nx else GridSpec(nx, GRID.ny, GRID.nz, GRID.lx * nx / GRID.nx, GRID.ly, GRID.lz)
     rng = np.random.default_rng(23)
@@ -385,7 +385,7 @@ def test_tc_mass_matches_oracle(torch_cuda, kind, rel, layout, nx):
     assert err <= rel, err
 
 
-@pytest.mark.parametrize("layout,nx", [(0, 6), (1, 6), (1, 8), (0, 8)])
+@pytest.mark.parametrize("layout,nx", [(0, 6), (1, 6), (1, 8), (0, 8), (2, 6), (2, 8)])
 def test_fp64_moments_match_oracle(torch_cuda, layout, nx):
     """The FP64 moment form (double precision): J-hat and the mass records
     equal the oracle's scalar deposition to the rounding of the regrouped

@@ -15,7 +15,7 @@ SUCCESS, INVALID_ARGUMENT, INVALID_STATE, OVERFLOW, BACKEND_FAILURE = 0, 1, 2, 3
 NOT_CONVERGED, CAPACITY_EXCEEDED, INVALID_DATA = 5, 6, 7
 PRECISION_DOUBLE, PRECISION_MIXED = 0, 1
 MASS_SCALAR, MASS_SCALAR_F64, MASS_TF32, MASS_BF16X3, MASS_MOMENTS_F64 = 0, 1, 2, 3, 4
-MASS_LAYOUT_RECORDS, MASS_LAYOUT_STENCIL_MAJOR = 0, 1
+MASS_LAYOUT_RECORDS, MASS_LAYOUT_STENCIL_MAJOR, MASS_LAYOUT_TILED = 0, 1, 2
 MAX_SPECIES = 8
 
 MASS_KINDS = {"scalar": MASS_SCALAR, "scalar-f64": MASS_SCALAR_F64, "fp64": MASS_SCALAR_F64,
@@ -45,7 +45,8 @@ class Particles(C.Structure):
 class Layout(C.Structure):
     _fields_ = [("node_count", C.c_int64), ("cell_count", C.c_int64), ("bin_count", C.c_int64),
                 ("interior_nodes", C.c_int64), ("field_scalar_bytes", C.c_size_t),
-                ("mass_scalar_bytes", C.c_size_t), ("velocity_scalar_bytes", C.c_size_t)]
+                ("mass_scalar_bytes", C.c_size_t), ("velocity_scalar_bytes", C.c_size_t),
+                ("mass_count", C.c_int64)]
 
 
 class GmresResult(C.Structure):

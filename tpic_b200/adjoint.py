@@ -103,7 +103,7 @@ class AdjointBuffers:
         self.b_node_bar = torch.zeros(3 * nodes, dtype=f64, device=dev)
         self.b_node = torch.zeros(3 * nodes, dtype=sim.fdt, device=dev)
         self.j = torch.zeros(3 * nodes, dtype=sim.fdt, device=dev)
-        self.mass = torch.zeros(126 * nodes, dtype=sim.fdt, device=dev)
+        self.mass = torch.zeros(sim.layout.mass_count, dtype=sim.fdt, device=dev)
         a = self.struct
         a.e_bar, a.b_bar = _ptr(self.e_bar), _ptr(self.b_bar)
         a.e_theta_bar, a.lambda_, a.b_node_bar = _ptr(self.e_theta_bar), _ptr(self.lam), _ptr(self.b_node_bar)

@@ -130,6 +130,8 @@ Geom make_geom(const tpicb200_grid& grid) {
   g.inv_volume = 1.0 / g.volume;
   g.mvs = 126;
   g.mes = 1;
+  g.MX = g.NX;
+  g.mnodes = g.nodes;
   g.run_len = kRunCells;
   while (g.run_len > 1 && (long long)((g.nx + g.run_len - 1) / g.run_len) * g.ny * g.nz < kRunTarget) g.run_len >>= 1;
   return g;
@@ -159,7 +161,8 @@ int tpicb200_create(const tpicb200_grid* grid, const tpicb200_options* options, 
   if (options->precision != TPICB200_PRECISION_DOUBLE && options->precision != TPICB200_PRECISION_MIXED)
     return fail(TPICB200_INVALID_ARGUMENT, "unknown precision mode");
   if (options->mass_layout != TPICB200_MASS_LAYOUT_RECORDS &&
-      options->mass_layout != TPICB200_MASS_LAYOUT_STENCIL_MAJOR)
+      options->mass_layout != TPICB200_MASS_LAYOUT_STENCIL_MAJOR &&
+      options->mass_layout != TPICB200_MASS_LAYOUT_TILED)
     return fail(TPICB200_INVALID_ARGUMENT, "unknown mass layout");
   // config/physics.cpp:65-70: 0 <= Smooth <= 1, SmoothNiter >= 0.
   if (options->smooth_iterations < 0 || !std::isfinite(options->smooth_alpha) ||
@@ -181,6 +184,11 @@ int tpicb200_create(const tpicb200_grid* grid, const tpicb200_options* options, 
   if (options->mass_layout == TPICB200_MASS_LAYOUT_STENCIL_MAJOR) {
     ctx->g.mvs = 1;
     ctx->g.mes = ctx->g.nodes;
+  } else if (options->mass_layout == TPICB200_MASS_LAYOUT_TILED) {
+    ctx->g.MX = (ctx->g.NX + 3) & ~3;
+    ctx->g.mnodes = (long long)ctx->g.MX * ctx->g.NY * ctx->g.NZ;
+    ctx->g.mvs = 1;
+    ctx->g.mes = ctx->g.mnodes;
   }
   ctx->opt = *options;
   cudaError_t e = cudaSuccess;
@@ -247,6 +255,7 @@ int tpicb200_get_layout(const tpicb200_context* ctx, tpicb200_layout* out) {
   out->field_scalar_bytes = dbl ? 8 : 4;
   out->mass_scalar_bytes = dbl ? 8 : 4;
   out->velocity_scalar_bytes = dbl ? 8 : 4;
+  out->mass_count = 126 * ctx->g.mnodes;
   return TPICB200_SUCCESS;
 }
 
@@ -335,7 +344,7 @@ int tpicb200_clear_moments(tpicb200_context* ctx, void* j, void* mass, tpicb200_
   ctx->cleared_j = j && mass ? j : nullptr;
   ctx->cleared_mass = j && mass ? mass : nullptr;
   if (j) e = cudaMemsetAsync(j, 0, 3 * size_t(ctx->g.nodes) * fb, (cudaStream_t)stream);
-  if (mass && e == cudaSuccess) e = cudaMemsetAsync(mass, 0, 126 * size_t(ctx->g.nodes) * fb, (cudaStream_t)stream);
+  if (mass && e == cudaSuccess) e = cudaMemsetAsync(mass, 0, 126 * size_t(ctx->g.mnodes) * fb, (cudaStream_t)stream);
   return cuda_status(e, "moment clear failed");
 }
 

@@ -26,8 +26,13 @@ struct Geom {
   double volume;       // (dx*dy)*dz
   double inv_volume;   // 1/volume
   // Mass storage: entry k = 9*stencil + component of vertex v lives at
-  // v*mvs + k*mes: (126, 1) for TPIC's records, (1, nodes) stencil-major.
+  // v*mvs + k*mes: (126, 1) for TPIC's records, (1, mnodes) stencil-major.
+  // A mass vertex is mass_vertex(i, j, k): the node index, except in the
+  // tiled layout, whose x pitch MX pads the n + 3 nodes of a row to a
+  // multiple of 4 (16-byte rows for the tensor-memory-access copies).
   long long mvs, mes;
+  int MX;             // mass x pitch: NX, or NX rounded up to a multiple of 4 (tiled)
+  long long mnodes;   // vertices of one mass entry plane: MX*NY*NZ
   // Cells per run of the run mover and the binned sort (a power of two,
   // 1..kRunCells): a warp walks one run's records, so small grids use
   // shorter runs to keep enough warps in flight.
@@ -35,6 +40,13 @@ struct Geom {
 
   __host__ __device__ __forceinline__ long long mass_index(long long vertex, int k) const {
     return vertex * mvs + (long long)k * mes;
+  }
+  __host__ __device__ __forceinline__ long long mass_vertex(int i, int j, int k) const {
+    return (long long)(i + 1) + (long long)MX * ((j + 1) + (long long)NY * (k + 1));
+  }
+  // Mass-vertex offset of a stencil (dx, dy, dz).
+  __host__ __device__ __forceinline__ long long mass_offset(int dx, int dy, int dz) const {
+    return (long long)dx + (long long)MX * (dy + (long long)NY * dz);
   }
 
   __host__ __device__ __forceinline__ long long node(int i, int j, int k) const {

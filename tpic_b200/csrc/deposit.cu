@@ -41,6 +41,9 @@ struct DepositParams {
 __device__ __forceinline__ long long wrapped_node(const Geom& g, int i, int j, int k) {
   return g.node(i == g.nx ? 0 : i, j == g.ny ? 0 : j, k == g.nz ? 0 : k);
 }
+__device__ __forceinline__ long long wrapped_mass_vertex(const Geom& g, int i, int j, int k) {
+  return g.mass_vertex(i == g.nx ? 0 : i, j == g.ny ? 0 : j, k == g.nz ? 0 : k);
+}
 
 // ---------------------------------------------------------------------------
 // Unsorted per-record deposition.
@@ -126,7 +129,11 @@ __global__ void __launch_bounds__(128) unsorted_deposit_kernel(Geom g, DepositPa
 #pragma unroll
           for (int e = 0; e < 9; ++e) {
             const Mass amount = Mass(as[e] * pw);
-            if (amount != Mass(0)) atomicAdd(M + g.mass_index(nodes[a], s * 9 + e), amount);
+            if (amount != Mass(0))
+              atomicAdd(M + g.mass_index(wrapped_mass_vertex(g, ci + (a & 1), cj + ((a >> 1) & 1),
+                                                             ck + ((a >> 2) & 1)),
+                                         s * 9 + e),
+                        amount);
           }
         }
     }
@@ -323,8 +330,8 @@ __global__ void __launch_bounds__(128) sorted_deposit_kernel(Geom g, DepositPara
       }
     }
     if (M) {
-      const long long vertex = wrapped_node(g, ci + (corner_a & 1), cj + ((corner_a >> 1) & 1),
-                                            ck + ((corner_a >> 2) & 1));
+      const long long vertex = wrapped_mass_vertex(g, ci + (corner_a & 1), cj + ((corner_a >> 1) & 1),
+                                                   ck + ((corner_a >> 2) & 1));
 #pragma unroll
       for (int slot = 0; slot < 2; ++slot) {
         if (stencil[slot] < 0) continue;
@@ -365,7 +372,8 @@ __global__ void __launch_bounds__(256) fold_mass_rows_kernel(Geom g, T* __restri
   for (uint32_t sv = blockIdx.x * blockDim.x + threadIdx.x; sv < shell; sv += gridDim.x * blockDim.x) {
     int i, j, k;
     shell_coordinates32(g, sv, i, j, k);
-    const long long to = g.node(i, j, k), from = g.node(wrap_index(i, g.nx), wrap_index(j, g.ny), wrap_index(k, g.nz));
+    const long long to = g.mass_vertex(i, j, k),
+                    from = g.mass_vertex(wrap_index(i, g.nx), wrap_index(j, g.ny), wrap_index(k, g.nz));
 #pragma unroll 6
     for (int e = 0; e < 126; ++e) m[g.mass_index(to, e)] = m[g.mass_index(from, e)];
   }
@@ -384,8 +392,8 @@ __global__ void __launch_bounds__(256) fold_mass_kernel(Geom g, T* __restrict__ 
     else { e = t / shell; sv = t - e * shell; }
     int i, j, k;
     shell_coordinates(g, sv, i, j, k);
-    m[g.mass_index(g.node(i, j, k), int(e))] =
-        m[g.mass_index(g.node(wrap_index(i, g.nx), wrap_index(j, g.ny), wrap_index(k, g.nz)), int(e))];
+    m[g.mass_index(g.mass_vertex(i, j, k), int(e))] =
+        m[g.mass_index(g.mass_vertex(wrap_index(i, g.nx), wrap_index(j, g.ny), wrap_index(k, g.nz)), int(e))];
   }
 }
 

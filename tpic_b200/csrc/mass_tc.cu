@@ -1258,7 +1258,7 @@ __host__ __device__ constexpr StencilPairs make_stencil_pairs() {
 // was deposited); otherwise they are added.
 template <class T, int S>
 __device__ __forceinline__ void assemble_stencil(const Geom& g, const long long (&cell)[8], long long node,
-                                                 const T* __restrict__ mom,
+                                                 long long mvertex, const T* __restrict__ mom,
                                                  T* __restrict__ J, T* __restrict__ M, int overwrite) {
   constexpr StencilPairs pairs = make_stencil_pairs();
   if constexpr (S < 14) {
@@ -1275,7 +1275,7 @@ __device__ __forceinline__ void assemble_stencil(const Geom& g, const long long 
     }
 #pragma unroll
     for (int e = 0; e < 9; ++e) {
-      T* dst = M + g.mass_index(node, S * 9 + e);
+      T* dst = M + g.mass_index(mvertex, S * 9 + e);
       *dst = overwrite ? sum[e] : *dst + sum[e];
     }
   } else {
@@ -1309,23 +1309,23 @@ __global__ void __launch_bounds__(128) assemble_moments_kernel(Geom g, const T* 
 #pragma unroll
   for (int a = 0; a < 8; ++a)
     cell[a] = ((a & 1) ? i1 : i) + (long long)nx * (((a & 2) ? j1 : j) + (long long)ny * ((a & 4) ? k1 : k));
-  const long long node = g.node(i, j, k);
+  const long long node = g.node(i, j, k), mvertex = g.mass_vertex(i, j, k);
   switch (stencil) {
-    case 0: assemble_stencil<T, 0>(g, cell, node, mom, J, M, overwrite); break;
-    case 1: assemble_stencil<T, 1>(g, cell, node, mom, J, M, overwrite); break;
-    case 2: assemble_stencil<T, 2>(g, cell, node, mom, J, M, overwrite); break;
-    case 3: assemble_stencil<T, 3>(g, cell, node, mom, J, M, overwrite); break;
-    case 4: assemble_stencil<T, 4>(g, cell, node, mom, J, M, overwrite); break;
-    case 5: assemble_stencil<T, 5>(g, cell, node, mom, J, M, overwrite); break;
-    case 6: assemble_stencil<T, 6>(g, cell, node, mom, J, M, overwrite); break;
-    case 7: assemble_stencil<T, 7>(g, cell, node, mom, J, M, overwrite); break;
-    case 8: assemble_stencil<T, 8>(g, cell, node, mom, J, M, overwrite); break;
-    case 9: assemble_stencil<T, 9>(g, cell, node, mom, J, M, overwrite); break;
-    case 10: assemble_stencil<T, 10>(g, cell, node, mom, J, M, overwrite); break;
-    case 11: assemble_stencil<T, 11>(g, cell, node, mom, J, M, overwrite); break;
-    case 12: assemble_stencil<T, 12>(g, cell, node, mom, J, M, overwrite); break;
-    case 13: assemble_stencil<T, 13>(g, cell, node, mom, J, M, overwrite); break;
-    default: assemble_stencil<T, 14>(g, cell, node, mom, J, M, overwrite); break;
+    case 0: assemble_stencil<T, 0>(g, cell, node, mvertex, mom, J, M, overwrite); break;
+    case 1: assemble_stencil<T, 1>(g, cell, node, mvertex, mom, J, M, overwrite); break;
+    case 2: assemble_stencil<T, 2>(g, cell, node, mvertex, mom, J, M, overwrite); break;
+    case 3: assemble_stencil<T, 3>(g, cell, node, mvertex, mom, J, M, overwrite); break;
+    case 4: assemble_stencil<T, 4>(g, cell, node, mvertex, mom, J, M, overwrite); break;
+    case 5: assemble_stencil<T, 5>(g, cell, node, mvertex, mom, J, M, overwrite); break;
+    case 6: assemble_stencil<T, 6>(g, cell, node, mvertex, mom, J, M, overwrite); break;
+    case 7: assemble_stencil<T, 7>(g, cell, node, mvertex, mom, J, M, overwrite); break;
+    case 8: assemble_stencil<T, 8>(g, cell, node, mvertex, mom, J, M, overwrite); break;
+    case 9: assemble_stencil<T, 9>(g, cell, node, mvertex, mom, J, M, overwrite); break;
+    case 10: assemble_stencil<T, 10>(g, cell, node, mvertex, mom, J, M, overwrite); break;
+    case 11: assemble_stencil<T, 11>(g, cell, node, mvertex, mom, J, M, overwrite); break;
+    case 12: assemble_stencil<T, 12>(g, cell, node, mvertex, mom, J, M, overwrite); break;
+    case 13: assemble_stencil<T, 13>(g, cell, node, mvertex, mom, J, M, overwrite); break;
+    default: assemble_stencil<T, 14>(g, cell, node, mvertex, mom, J, M, overwrite); break;
   }
 }
 
@@ -1390,7 +1390,7 @@ __device__ __forceinline__ void assemble_quad(const Geom& g, int m, int j, int k
     const long long node = g.node(4 * m + n, j, k);
 #pragma unroll
     for (int e = 0; e < kSums; ++e) {
-      T* dst = S < 14 ? M + g.mass_index(node, S * 9 + e) : J + e * g.nodes + node;
+      T* dst = S < 14 ? M + g.mass_index(g.mass_vertex(4 * m + n, j, k), S * 9 + e) : J + e * g.nodes + node;
       *dst = overwrite ? sum[e][n] : *dst + sum[e][n];
     }
   }

@@ -19,8 +19,12 @@
 // order, and stores the image straight into the compact Krylov vector: the
 // M records (504 B/node FP32, 1008 B/node FP64) are the only HBM stream.
 #include "kernels.cuh"
+#include "tcgen05.cuh"
+
+#include <cuda.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -99,18 +103,19 @@ template <class C, class M>
 __device__ __forceinline__ void mass_product(const Geom& g, const M* __restrict__ mass,
                                              const double* __restrict__ v, int i, int j, int k, C out[3]) {
   const long long nn = g.nodes;
-  const long long at = g.node(i, j, k);
+  const long long at = g.node(i, j, k), mat = g.mass_vertex(i, j, k);
   C x, y, z;
   const long long es = g.mes;
-  block_product<C>(mass + g.mass_index(at, 0), es, C(v[at]), C(v[nn + at]), C(v[2 * nn + at]), x, y, z);
+  block_product<C>(mass + g.mass_index(mat, 0), es, C(v[at]), C(v[nn + at]), C(v[2 * nn + at]), x, y, z);
 #pragma unroll
   for (int s = 1; s < 14; ++s) {
     const long long d = stencil_offset(s, 0) + (long long)g.NX * (stencil_offset(s, 1) + (long long)g.NY * stencil_offset(s, 2));
+    const long long md = g.mass_offset(stencil_offset(s, 0), stencil_offset(s, 1), stencil_offset(s, 2));
     C bx, by, bz;
     const long long f = at + d, b = at - d;
-    block_product<C>(mass + g.mass_index(at, s * 9), es, C(v[f]), C(v[nn + f]), C(v[2 * nn + f]), bx, by, bz);
+    block_product<C>(mass + g.mass_index(mat, s * 9), es, C(v[f]), C(v[nn + f]), C(v[2 * nn + f]), bx, by, bz);
     x += bx; y += by; z += bz;
-    block_product<C>(mass + g.mass_index(b, s * 9), es, C(v[b]), C(v[nn + b]), C(v[2 * nn + b]), bx, by, bz);
+    block_product<C>(mass + g.mass_index(mat - md, s * 9), es, C(v[b]), C(v[nn + b]), C(v[2 * nn + b]), bx, by, bz);
     x += bx; y += by; z += bz;
   }
   out[0] = x; out[1] = y; out[2] = z;
@@ -152,8 +157,8 @@ __global__ void __launch_bounds__(TX * TY * TZ, sizeof(C) == 4 ? 4 : 3) maxwell_
     const int pi = i0 + int(threadIdx.x % TX), pj = j0 + int((threadIdx.x / TX) % TY),
               pk = k0 + int(threadIdx.x / (TX * TY));
     if (pi < g.nx && pj < g.ny && pk < g.nz) {
-      const long long pat = g.node(pi, pj, pk);
-      const long long d1 = stencil_offset(1, 0) + (long long)g.NX * (stencil_offset(1, 1) + (long long)g.NY * stencil_offset(1, 2));
+      const long long pat = g.mass_vertex(pi, pj, pk);
+      const long long d1 = g.mass_offset(stencil_offset(1, 0), stencil_offset(1, 1), stencil_offset(1, 2));
 #pragma unroll
       for (int e = 0; e < 9; ++e) {
         prefetch_l2(mass + g.mass_index(pat, e));
@@ -233,7 +238,7 @@ __global__ void __launch_bounds__(TX * TY * TZ, sizeof(C) == 4 ? 4 : 3) maxwell_
   }
   // Mass product: centre, then forward and backward blocks per stencil,
   // untransposed (apply_mass_matrix_node, mass_matrix_stencil.hpp:119-149).
-  const long long at = g.node(i, j, k), es = g.mes;
+  const long long at = g.mass_vertex(i, j, k), es = g.mes;
   auto vv = [&](int c, int a, int b, int d) { return vs[c][lz + 1 + d][ly + 1 + b][lx + 1 + a]; };
   C x, y, z;
   block_product<C, M, kTranspose>(mass + g.mass_index(at, 0), es, vv(0, 0, 0, 0), vv(1, 0, 0, 0), vv(2, 0, 0, 0), x,
@@ -241,14 +246,14 @@ __global__ void __launch_bounds__(TX * TY * TZ, sizeof(C) == 4 ? 4 : 3) maxwell_
 #pragma unroll
   for (int s = 1; s < 14; ++s) {
     const int ox = stencil_offset(s, 0), oy = stencil_offset(s, 1), oz = stencil_offset(s, 2);
-    const long long d = ox + (long long)g.NX * (oy + (long long)g.NY * oz);
+    const long long d = g.mass_offset(ox, oy, oz);
     // The next stencil's forward and backward rows are requested into L2
     // while this one is applied: the loads of a block then wait for L2, not
     // for HBM (the kernel is bound by memory latency; prefetches hold no
     // registers).
     if (s + 1 < 14) {
       const int sn = s + 1;
-      const long long dn = stencil_offset(sn, 0) + (long long)g.NX * (stencil_offset(sn, 1) + (long long)g.NY * stencil_offset(sn, 2));
+      const long long dn = g.mass_offset(stencil_offset(sn, 0), stencil_offset(sn, 1), stencil_offset(sn, 2));
 #pragma unroll
       for (int e = 0; e < 9; ++e) {
         prefetch_l2(mass + g.mass_index(at, sn * 9 + e));
@@ -269,6 +274,185 @@ __global__ void __launch_bounds__(TX * TY * TZ, sizeof(C) == 4 ? 4 : 3) maxwell_
   for (int c = 0; c < 3; ++c) {
     // The mass image is narrowed to the solver storage (double) before the
     // combination reads it back (maxwell_device.hpp:424-429,471-484).
+    const C m = C(double(mv[c] * inv_volume));
+    const C value = (C(1) * vv(c, 0, 0, 0) + d2 * C(double(curl2[c]))) + kfac * m;
+    out[c * g.interior + row] = Out(value);
+  }
+}
+
+// A(v) with the mass rows staged by tensor-memory-access (TMA) copies, for
+// mass buffers whose rows start on 16-byte boundaries (the tiled layout).
+// Per stencil s = (ox, oy, oz) one 4-D box of the mass tensor (x, y, z,
+// entry) holds the stencil's 9 entries over the tile plus a one-node halo
+// on the side of -s: x elements i0 .. i0+35 (nodes i0-1 .. i0+34; element
+// i0 is 16-byte aligned), y nodes j0 - max(oy,0) .. + TY, z likewise. The
+// forward block of a node (at the node) and its backward block (at the
+// node - s) are both in that box. The boxes stream through S stages with one
+// mbarrier each; one thread issues the copies (after the kernel's
+// predecessor has completed), every thread waits (bounded) for a stage's
+// copy, and the stage is refilled with stencil s + S after a CTA barrier. The
+// input v and the cell curls are staged as in maxwell_apply_kernel, and every
+// sum runs in the same order, so the result equals it bit for bit. A copy
+// that does not arrive within the bound adds 1 << 21 to *invalid; the CTA
+// then waits (bounded) for its copies in flight and returns.
+constexpr int kBoxX = 36;
+
+template <int TY, int TZ, class M> struct TmaBox {
+  static constexpr int X = kBoxX, Y = TY + 1, Z = TZ + 1;
+  static constexpr int entry = X * Y * Z;              // elements of one entry's box
+  static constexpr int elems = 9 * entry;              // one stencil's box
+  static constexpr int bytes = elems * int(sizeof(M));
+  static constexpr int stage = (bytes + 1023) / 1024 * 1024;  // 1024-byte aligned stages
+};
+
+template <class C, class M, int TX, int TY, int TZ, int S>
+struct TmaApplyShared {
+  static constexpr int VX = TX + 2, VY = TY + 2, VZ = TZ + 2;
+  static constexpr int CX = TX + 1, CY = TY + 1, CZ = TZ + 1;
+  static constexpr int stages = S * TmaBox<TY, TZ, M>::stage;
+  static constexpr int bars = stages;                              // S mbarriers
+  static constexpr int vs = (bars + S * 8 + 15) / 16 * 16;         // C [3][VZ][VY][VX]
+  static constexpr int cs = vs + 3 * VZ * VY * VX * int(sizeof(C));  // C [3][CZ][CY][CX]
+  static constexpr int total = cs + 3 * CZ * CY * CX * int(sizeof(C));
+};
+
+template <class C, class M, class Out, int TX, int TY, int TZ, int S, bool kTranspose>
+__global__ void __launch_bounds__(TX * TY * TZ, sizeof(C) == 4 ? 3 : 2)
+    maxwell_apply_tma_kernel(const __grid_constant__ CUtensorMap map, Geom g, C d2, C kfac, C inv_volume,
+                             const double* __restrict__ v, Out* __restrict__ out, uint32_t* invalid) {
+  using Box = TmaBox<TY, TZ, M>;
+  using L = TmaApplyShared<C, M, TX, TY, TZ, S>;
+  constexpr int VX = L::VX, VY = L::VY, VZ = L::VZ, CX = L::CX, CY = L::CY, CZ = L::CZ;
+  extern __shared__ __align__(1024) uint8_t tma_smem[];
+  uint64_t* bars = reinterpret_cast<uint64_t*>(tma_smem + L::bars);
+  auto vs = reinterpret_cast<C (*)[VZ][VY][VX]>(tma_smem + L::vs);
+  auto cs = reinterpret_cast<C (*)[CZ][CY][CX]>(tma_smem + L::cs);
+  const C inv[3] = {C(g.inv[0]), C(g.inv[1]), C(g.inv[2])};
+  const int tiles_x = (g.nx + TX - 1) / TX, tiles_y = (g.ny + TY - 1) / TY;
+  const int tx = blockIdx.x % tiles_x, ty = (blockIdx.x / tiles_x) % tiles_y, tz = blockIdx.x / (tiles_x * tiles_y);
+  const int i0 = tx * TX, j0 = ty * TY, k0 = tz * TZ;
+  const long long nn = g.nodes;
+  auto issue = [&](int s) {
+    const int oy = stencil_offset(s, 1), oz = stencil_offset(s, 2);
+    uint64_t* bar = &bars[s % S];
+    tc::mbar_arrive_expect_tx(bar, uint32_t(Box::bytes));
+    tc::tma_load_4d(tma_smem + (s % S) * Box::stage, &map, i0, j0 + 1 - (oy > 0 ? oy : 0), k0 + 1 - (oz > 0 ? oz : 0),
+                    9 * s, bar);
+  };
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int b = 0; b < S; ++b) tc::mbar_init(&bars[b], 1);
+    tc::fence_mbar_init();
+  }
+  __syncthreads();
+  wait_for_predecessor();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int s = 0; s < S; ++s) issue(s);
+  }
+  // Stage v over nodes [i0-1, i0+TX] x [j0-1, j0+TY] x [k0-1, k0+TZ]; nodes
+  // beyond n+1 (partial tiles) are never read by a live node and load 0.
+  for (int t = threadIdx.x; t < 3 * VZ * VY * VX; t += blockDim.x) {
+    const int c = t / (VZ * VY * VX), r = t % (VZ * VY * VX);
+    const int lx = r % VX, ly = (r / VX) % VY, lz = r / (VX * VY);
+    const int i = i0 - 1 + lx, j = j0 - 1 + ly, k = k0 - 1 + lz;
+    C val = C(0);
+    if (i <= g.nx + 1 && j <= g.ny + 1 && k <= g.nz + 1) val = C(v[c * nn + g.node(i, j, k)]);
+    vs[c][lz][ly][lx] = val;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < CZ * CY * CX; t += blockDim.x) {
+    const int lx = t % CX, ly = (t / CX) % CY, lz = t / (CX * CY);
+    C q[3][8];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      q[c][0] = vs[c][lz][ly][lx];         q[c][1] = vs[c][lz][ly][lx + 1];
+      q[c][2] = vs[c][lz][ly + 1][lx];     q[c][3] = vs[c][lz + 1][ly][lx];
+      q[c][4] = vs[c][lz][ly + 1][lx + 1]; q[c][5] = vs[c][lz + 1][ly][lx + 1];
+      q[c][6] = vs[c][lz + 1][ly + 1][lx]; q[c][7] = vs[c][lz + 1][ly + 1][lx + 1];
+    }
+    auto dx = [&](const C* p) { return C(0.25) * inv[0] * (p[1] - p[0] + (p[5] - p[3]) + (p[4] - p[2]) + (p[7] - p[6])); };
+    auto dy = [&](const C* p) { return C(0.25) * inv[1] * (p[2] - p[0] + (p[6] - p[3]) + (p[4] - p[1]) + (p[7] - p[5])); };
+    auto dz = [&](const C* p) { return C(0.25) * inv[2] * (p[3] - p[0] + (p[5] - p[1]) + (p[6] - p[2]) + (p[7] - p[4])); };
+    cs[0][lz][ly][lx] = C(double(dy(q[2]) - dz(q[1])));
+    cs[1][lz][ly][lx] = C(double(dz(q[0]) - dx(q[2])));
+    cs[2][lz][ly][lx] = C(double(dx(q[1]) - dy(q[0])));
+  }
+  __syncthreads();
+  const int lx = threadIdx.x % TX, ly = (threadIdx.x / TX) % TY, lz = threadIdx.x / (TX * TY);
+  const int i = i0 + lx, j = j0 + ly, k = k0 + lz;
+  const bool live = i < g.nx && j < g.ny && k < g.nz;
+  C curl2[3] = {C(0), C(0), C(0)};
+  if (live) {
+    C p[3][8];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      p[c][0] = cs[c][lz + 1][ly + 1][lx + 1]; p[c][1] = cs[c][lz + 1][ly + 1][lx];
+      p[c][2] = cs[c][lz + 1][ly][lx + 1];     p[c][3] = cs[c][lz][ly + 1][lx + 1];
+      p[c][4] = cs[c][lz + 1][ly][lx];         p[c][5] = cs[c][lz][ly + 1][lx];
+      p[c][6] = cs[c][lz][ly][lx + 1];         p[c][7] = cs[c][lz][ly][lx];
+    }
+    auto dx = [&](const C* q) { return C(0.25) * inv[0] * (q[0] - q[1] + (q[3] - q[5]) + (q[2] - q[4]) + (q[6] - q[7])); };
+    auto dy = [&](const C* q) { return C(0.25) * inv[1] * (q[0] - q[2] + (q[3] - q[6]) + (q[1] - q[4]) + (q[5] - q[7])); };
+    auto dz = [&](const C* q) { return C(0.25) * inv[2] * (q[0] - q[3] + (q[1] - q[5]) + (q[2] - q[6]) + (q[4] - q[7])); };
+    curl2[0] = dy(p[2]) - dz(p[1]);
+    curl2[1] = dz(p[0]) - dx(p[2]);
+    curl2[2] = dx(p[1]) - dy(p[0]);
+  }
+  auto vv = [&](int c, int a, int b, int d) { return vs[c][lz + 1 + d][ly + 1 + b][lx + 1 + a]; };
+  C x = C(0), y = C(0), z = C(0);
+  bool failed = false;
+  int consumed = 0;
+  // Unrolled (the stencil offsets fold into constants); `failed` is uniform
+  // over the CTA, so the barriers below are reached by every thread.
+#pragma unroll
+  for (int s = 0; s < 14; ++s) {
+    if (failed) continue;
+    const bool ok = tc::mbar_wait(&bars[s % S], uint32_t((s / S) & 1));
+    if (__syncthreads_or(!ok)) {
+      failed = true;
+      continue;
+    }
+    consumed = s + 1;
+    if (live) {
+      const M* box = reinterpret_cast<const M*>(tma_smem + (s % S) * Box::stage);
+      const int ox = stencil_offset(s, 0), oy = stencil_offset(s, 1), oz = stencil_offset(s, 2);
+      const int my = oy > 0 ? oy : 0, mz = oz > 0 ? oz : 0;
+      const int fwd = (lx + 1) + Box::X * ((ly + my) + Box::Y * (lz + mz));
+      if (s == 0) {
+        block_product<C, M, kTranspose>(box + fwd, Box::entry, vv(0, 0, 0, 0), vv(1, 0, 0, 0), vv(2, 0, 0, 0), x, y, z);
+      } else {
+        const int bwd = (lx + 1 - ox) + Box::X * ((ly - oy + my) + Box::Y * (lz - oz + mz));
+        C bx, by, bz;
+        block_product<C, M, kTranspose>(box + fwd, Box::entry, vv(0, ox, oy, oz), vv(1, ox, oy, oz),
+                                        vv(2, ox, oy, oz), bx, by, bz);
+        x += bx; y += by; z += bz;
+        block_product<C, M, kTranspose>(box + bwd, Box::entry, vv(0, -ox, -oy, -oz), vv(1, -ox, -oy, -oz),
+                                        vv(2, -ox, -oy, -oz), bx, by, bz);
+        x += bx; y += by; z += bz;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && s + S < 14) {
+      tc::fence_proxy_async_smem();
+      issue(s + S);
+    }
+  }
+  if (failed) {
+    // Copies issued but not consumed may still land: wait for them (bounded)
+    // before the CTA's shared memory is released.
+    if (threadIdx.x == 0) {
+      if (invalid) atomicAdd(invalid, 1u << 21);
+      for (int s = consumed; s < 14 && s < consumed + S; ++s) tc::mbar_wait(&bars[s % S], uint32_t((s / S) & 1));
+    }
+    __syncthreads();
+    return;
+  }
+  if (!live) return;
+  const C mv[3] = {x, y, z};
+  const long long row = i + (long long)g.inx * (j + (long long)g.iny * k);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
     const C m = C(double(mv[c] * inv_volume));
     const C value = (C(1) * vv(c, 0, 0, 0) + d2 * C(double(curl2[c]))) + kfac * m;
     out[c * g.interior + row] = Out(value);
@@ -636,6 +820,16 @@ struct SolverWorkspace {
   unsigned loop_launches[2] = {0, 0};  // kernels of one step
   bool loop_unavailable = false;
   bool conditional_checked = false;
+  // Tensor maps of mass buffers for the TMA-staged apply, per mass pointer
+  // and tile shape (0: 32x4x2, 1: thin 32x8x1); built on first use.
+  struct MassMap {
+    CUtensorMap map;
+    const void* mass = nullptr;
+    int tile = -1;
+    bool usable = false;
+  };
+  MassMap maps[4];
+  int next_map = 0;
 
   double* hessenberg() { return state; }
   double* cosine() { return state + (size_t)restart * (restart + 1); }
@@ -719,6 +913,84 @@ void solver_destroy(SolverWorkspace* w) {
 
 namespace {
 
+using TensorMapEncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                          const cuuint64_t*, const cuuint32_t*, const cuuint32_t*,
+                                          CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                          CUtensorMapFloatOOBfill);
+
+TensorMapEncodeTiled tensor_map_encoder() {
+  static std::atomic<TensorMapEncodeTiled> fn{nullptr};
+  TensorMapEncodeTiled f = fn.load();
+  if (f) return f;
+  void* p = nullptr;
+  cudaDriverEntryPointQueryResult found;
+  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &found) != cudaSuccess ||
+      found != cudaDriverEntryPointSuccess || !p) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  f = reinterpret_cast<TensorMapEncodeTiled>(p);
+  fn.store(f);
+  return f;
+}
+
+// The tensor map of a mass buffer as a 4-D tensor (x pitch MX, y NY, z NZ,
+// 126 entries) with the apply's box {36, TY+1, TZ+1, 9}, or nullptr when the
+// buffer does not meet the copies' alignment rules (vertex stride 1, the
+// base, the row pitch and the entry-plane stride multiples of 16 bytes):
+// those buffers take maxwell_apply_kernel.
+template <class M>
+const CUtensorMap* mass_tensor_map(SolverWorkspace* w, const M* mass, bool thin) {
+  const Geom& g = w->g;
+  const int tile = thin ? 1 : 0;
+  for (auto& m : w->maps)
+    if (m.mass == mass && m.tile == tile) return m.usable ? &m.map : nullptr;
+  auto& m = w->maps[w->next_map];
+  w->next_map = (w->next_map + 1) % 4;
+  m.mass = mass;
+  m.tile = tile;
+  m.usable = false;
+  const size_t es = sizeof(M);
+  if (g.mvs != 1 || (reinterpret_cast<uintptr_t>(mass) % 16) != 0 || ((size_t)g.MX * es) % 16 != 0 ||
+      ((size_t)g.mes * es) % 16 != 0 || (size_t)g.mes < (size_t)g.mnodes)
+    return nullptr;
+  TensorMapEncodeTiled encode = tensor_map_encoder();
+  if (!encode) return nullptr;
+  const cuuint64_t dims[4] = {cuuint64_t(g.MX), cuuint64_t(g.NY), cuuint64_t(g.NZ), 126};
+  const cuuint64_t strides[3] = {cuuint64_t(g.MX) * es, cuuint64_t(g.MX) * g.NY * es, cuuint64_t(g.mes) * es};
+  const cuuint32_t box[4] = {cuuint32_t(kBoxX), cuuint32_t((thin ? kThinTY : kTY) + 1), cuuint32_t((thin ? 1 : kTZ) + 1),
+                             9};
+  const cuuint32_t unit[4] = {1, 1, 1, 1};
+  const CUresult r = encode(&m.map, es == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
+                            const_cast<M*>(mass), dims, strides, box, unit, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  m.usable = r == CUDA_SUCCESS;
+  return m.usable ? &m.map : nullptr;
+}
+
+// Launches the TMA-staged apply; the kernel's dynamic shared memory limit is
+// raised once per device.
+template <class C, class M, class Out, int TY, int TZ, bool kTranspose>
+cudaError_t launch_apply_tma(const CUtensorMap& map, unsigned tiles, cudaStream_t st, const Geom& g, C d2, C kf,
+                             C civ, const double* in, Out* out, uint32_t* invalid) {
+  constexpr int S = sizeof(M) == 4 ? 3 : 2;
+  constexpr int bytes = TmaApplyShared<C, M, kTX, TY, TZ, S>::total;
+  static_assert(bytes <= 227 * 1024, "apply tile exceeds shared memory");
+  auto kernel = maxwell_apply_tma_kernel<C, M, Out, kTX, TY, TZ, S, kTranspose>;
+  static std::atomic<uint64_t> ready{0};
+  int device = 0;
+  cudaError_t e = cudaGetDevice(&device);
+  if (e != cudaSuccess) return e;
+  const uint64_t bit = device < 64 ? 1ull << device : 0;
+  if (!bit || !(ready.load() & bit)) {
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+    ready.fetch_or(bit);
+  }
+  return launch_programmatic(kernel, tiles, kTX * TY * TZ, bytes, st, map, g, d2, kf, civ, in, out, invalid);
+}
+
 template <class P>
 struct Solve {
   using S = typename P::EC;     // Krylov basis and Arnoldi arithmetic
@@ -766,7 +1038,19 @@ struct Solve {
                                            ((g.nz + kTZ - 1) / kTZ));
     const C d2 = C(w->delta * w->delta), kf = C(w->kfac), civ = C(iv);
     const double* in = w->input;
-    if (w->transpose) {
+    const CUtensorMap* map = response ? nullptr : mass_tensor_map(w, mass, thin);
+    if (map) {
+      cudaError_t e;
+      if (w->transpose && thin)
+        e = launch_apply_tma<C, Mass, Out, kThinTY, 1, true>(*map, tiles, st, g, d2, kf, civ, in, out, w->invalid);
+      else if (w->transpose)
+        e = launch_apply_tma<C, Mass, Out, kTY, kTZ, true>(*map, tiles, st, g, d2, kf, civ, in, out, w->invalid);
+      else if (thin)
+        e = launch_apply_tma<C, Mass, Out, kThinTY, 1, false>(*map, tiles, st, g, d2, kf, civ, in, out, w->invalid);
+      else
+        e = launch_apply_tma<C, Mass, Out, kTY, kTZ, false>(*map, tiles, st, g, d2, kf, civ, in, out, w->invalid);
+      if (err == cudaSuccess) err = e;
+    } else if (w->transpose) {
       // The adjoint solve (no smoothing): every mass block transposed.
       if (thin)
         launch_programmatic(maxwell_apply_kernel<C, Mass, Out, kTX, kThinTY, 1, false, true>, tiles, kTX * kThinTY, 0,

@@ -265,7 +265,7 @@ int main(int argc, char** argv) {
   st.b_node = dev.alloc(3 * lay.node_count * fb);
   st.b_node_next = dev.alloc(3 * lay.node_count * fb);
   st.j = dev.alloc(3 * lay.node_count * fb);
-  st.mass = dev.alloc(126 * lay.node_count * lay.mass_scalar_bytes);
+  st.mass = dev.alloc(size_t(lay.mass_count) * lay.mass_scalar_bytes);
   st.e_theta = (double*)dev.alloc(3 * lay.node_count * 8);
   st.mass_kind = kind;
   for (int s = 0; s < deck.ns; ++s) {

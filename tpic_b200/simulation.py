@@ -60,7 +60,8 @@ class Simulation:
             raise ValueError("too many species")
         grid = _lib.Grid(g.nx, g.ny, g.nz, g.lx, g.ly, g.lz)
         self.mass_layout = {"records": _lib.MASS_LAYOUT_RECORDS,
-                            "stencil-major": _lib.MASS_LAYOUT_STENCIL_MAJOR}[mass_layout]
+                            "stencil-major": _lib.MASS_LAYOUT_STENCIL_MAJOR,
+                            "tiled": _lib.MASS_LAYOUT_TILED}[mass_layout]
         # Energy-conserving smoothing: (passes, Face7 centre weight, operator
         # 0 Face7 / 1 Binomial27); on when passes > 0 and the weight < 1.
         smoothing = tuple(case.smoothing if smoothing is None else smoothing)
@@ -82,7 +83,7 @@ class Simulation:
         self.b_node = torch.zeros(3 * nodes, dtype=self.fdt, device=dev)
         self.b_node_next = torch.zeros(3 * nodes, dtype=self.fdt, device=dev)
         self.j = torch.zeros(3 * nodes, dtype=self.fdt, device=dev)
-        self.mass = torch.zeros(126 * nodes, dtype=self.fdt, device=dev)
+        self.mass = torch.zeros(layout.mass_count, dtype=self.fdt, device=dev)
         self.e_theta = torch.zeros(3 * nodes, dtype=torch.float64, device=dev)
         for k in range(3):
             self.e[k * nodes:(k + 1) * nodes] = case.fields.e0[k]
