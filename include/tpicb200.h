@@ -295,14 +295,29 @@ int tpicb200_smooth(tpicb200_context* ctx, const double* in, double* out, tpicb2
  * after the enqueued work (simulation/driver/pipeline.hpp:145-146). Host-blocking. */
 int tpicb200_read_invalid(tpicb200_context* ctx, uint32_t* count, int clear, tpicb200_stream stream);
 
-/* Bound of the device-side waits of the BF16X3 tensor-core deposition (the
- * wait for a chunk's MMAs and for the issuer's published decision): polls
- * before a wait gives up, 0 restoring the default of 4,194,304. A wait that
- * gives up makes its CTA leave the chunk loop, wait (with the default bound)
- * for the MMAs it has in flight and free its tensor memory; the deposition
- * then adds 1 << 20 to the invalid counter and tpicb200_cycle returns
- * TPICB200_INVALID_DATA. A small bound serves to test that path. */
+/* Bound of the device-side waits: polls before a wait gives up, 0 restoring
+ * the default of 4,194,304.
+ * - The BF16X3 tensor-core deposition (the wait for a chunk's MMAs and for
+ *   the issuer's published decision): a wait that gives up makes its CTA
+ *   leave the chunk loop, wait (with the default bound) for the MMAs it has
+ *   in flight and free its tensor memory; the deposition adds 1 << 20 to the
+ *   invalid counter.
+ * - The operator apply that stages mass boxes by TMA (mass buffers with
+ *   16-byte rows: the tiled layout): a wait for a box that gives up makes
+ *   its CTA wait (with the default bound) for its copies in flight and
+ *   return without writing its rows; the apply adds 1 << 21 to the invalid
+ *   counter.
+ * tpicb200_cycle then returns TPICB200_INVALID_DATA. */
 int tpicb200_set_wait_limit(tpicb200_context* ctx, uint32_t polls);
+
+/* Test of the bounded waits (tpicb200_set_wait_limit) without a fault: with
+ * site TPICB200_STALL_DEPOSIT the tensor-core deposition's wait for the MMAs
+ * of chunk index - 1 (index >= 1), with TPICB200_STALL_APPLY the TMA apply's
+ * wait for the mass box of stencil `index` (0..13) waits instead on an
+ * mbarrier that nothing arrives on, so it gives up at its bound and takes
+ * the recovery path above. TPICB200_STALL_NONE turns it off. */
+enum { TPICB200_STALL_NONE = 0, TPICB200_STALL_DEPOSIT = 1, TPICB200_STALL_APPLY = 2 };
+int tpicb200_inject_stall(tpicb200_context* ctx, int site, uint32_t index);
 
 /* Zero J (node field) and the mass records. Replaces enqueue_clear_mass_matrix
  * (ecsim/mass_matrix/mass_matrix_deposition_device.hpp:107-121) and the moment clear. */

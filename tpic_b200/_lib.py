@@ -16,6 +16,7 @@ NOT_CONVERGED, CAPACITY_EXCEEDED, INVALID_DATA = 5, 6, 7
 PRECISION_DOUBLE, PRECISION_MIXED = 0, 1
 MASS_SCALAR, MASS_SCALAR_F64, MASS_TF32, MASS_BF16X3, MASS_MOMENTS_F64 = 0, 1, 2, 3, 4
 MASS_LAYOUT_RECORDS, MASS_LAYOUT_STENCIL_MAJOR, MASS_LAYOUT_TILED = 0, 1, 2
+STALL_NONE, STALL_DEPOSIT, STALL_APPLY = 0, 1, 2
 MAX_SPECIES = 8
 
 MASS_KINDS = {"scalar": MASS_SCALAR, "scalar-f64": MASS_SCALAR_F64, "fp64": MASS_SCALAR_F64,
@@ -143,6 +144,7 @@ EXPORTS = {
     "tpicb200_smooth": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tpicb200_read_invalid": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint32), C.c_int, C.c_void_p]),
     "tpicb200_set_wait_limit": (C.c_int, [C.c_void_p, C.c_uint32]),
+    "tpicb200_inject_stall": (C.c_int, [C.c_void_p, C.c_int, C.c_uint32]),
     "tpicb200_energy": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(Particles),
                                   C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_double), C.c_void_p]),
     "tpicb200_prepare": (C.c_int, [C.c_void_p, C.POINTER(State), C.c_void_p]),

@@ -40,7 +40,9 @@ struct tpicb200_context {
   // else has deposited into since: the assembly may store instead of add.
   const void* cleared_j = nullptr;
   const void* cleared_mass = nullptr;
-  uint32_t wait_polls = 0;  // tensor-core stream kernel wait bound (0: the default)
+  uint32_t wait_polls = 0;  // device wait bound of the stream kernel and the TMA apply (0: the default)
+  int stall_site = TPICB200_STALL_NONE;  // tpicb200_inject_stall
+  uint32_t stall_index = 0;
 };
 
 namespace {
@@ -101,7 +103,8 @@ cudaError_t launch_moments(tpicb200_context* ctx, int kind, int ns, const double
     return launch_deposit_moments_f64(ctx->g, ns, qom, ctx->opt.dt, ctx->opt.c, parts, counts, offsets, b_node,
                                       (double*)ctx->moments, accumulate, invalid, copies, s);
   return launch_deposit_tc(kind, ctx->g, ns, qom, ctx->opt.dt, ctx->opt.c, parts, counts, offsets, b_node,
-                           (float*)ctx->moments, accumulate, invalid, copies, s, ctx->wait_polls);
+                           (float*)ctx->moments, accumulate, invalid, copies, s, ctx->wait_polls,
+                           ctx->stall_site == TPICB200_STALL_DEPOSIT ? ctx->stall_index : 0u);
 }
 
 }  // namespace
@@ -785,6 +788,25 @@ static int read_invalid(tpicb200_context* ctx, cudaStream_t s, uint32_t* value) 
 int tpicb200_set_wait_limit(tpicb200_context* ctx, uint32_t polls) {
   if (int s = check_ctx(ctx)) return s;
   ctx->wait_polls = polls;
+  if (ctx->solver)
+    solver_set_waits(ctx->solver, polls, ctx->stall_site == TPICB200_STALL_APPLY ? int(ctx->stall_index) : -1);
+  return TPICB200_SUCCESS;
+}
+
+int tpicb200_inject_stall(tpicb200_context* ctx, int site, uint32_t index) {
+  if (int s = check_ctx(ctx)) return s;
+  if (site == TPICB200_STALL_NONE) {
+    index = 0;
+  } else if (site == TPICB200_STALL_DEPOSIT) {
+    if (index < 1) return fail(TPICB200_INVALID_ARGUMENT, "the deposition stall index is a chunk >= 1");
+  } else if (site == TPICB200_STALL_APPLY) {
+    if (index > 13) return fail(TPICB200_INVALID_ARGUMENT, "the apply stall index is a stencil 0..13");
+  } else {
+    return fail(TPICB200_INVALID_ARGUMENT, "unknown stall site");
+  }
+  ctx->stall_site = site;
+  ctx->stall_index = index;
+  if (ctx->solver) solver_set_waits(ctx->solver, ctx->wait_polls, site == TPICB200_STALL_APPLY ? int(index) : -1);
   return TPICB200_SUCCESS;
 }
 

@@ -130,12 +130,14 @@ size_t moment_floats(const Geom& g);
 // per-cell moments; `accumulate` adds to moments already present.
 // wait_polls bounds the BF16X3 stream kernel's chunk-loop waits (0: the
 // default kDefaultWaitPolls); a wait that gives up sets bit 20 of *invalid.
+// stall_chunk >= 1 makes the wait for the MMAs of chunk stall_chunk - 1 wait
+// on an mbarrier that nothing arrives on instead (a test of the bound).
 constexpr uint32_t kDefaultWaitPolls = 1u << 22;
 cudaError_t launch_deposit_tc(int mass_kind, const Geom& g, int ns, const double* qom, double dt, double c,
                               const tpicb200_particles* const* p, const uint32_t* const* counts,
                               const uint32_t* const* offsets, const void* bnode, float* moments, int accumulate,
                               uint32_t* invalid, const SortedCopy* const* copies, cudaStream_t s,
-                              uint32_t wait_polls = 0);
+                              uint32_t wait_polls = 0, uint32_t stall_chunk = 0);
 // FP64 CUDA-core form of the same moments (double precision; double moments).
 cudaError_t launch_deposit_moments_f64(const Geom& g, int ns, const double* qom, double dt, double c,
                                        const tpicb200_particles* const* p, const uint32_t* const* counts,
@@ -224,6 +226,10 @@ int solver_solve_adjoint(SolverWorkspace* w, const double* rhs, const void* mass
                          cudaError_t* err);
 // The counter the solver's smoothing passes raise on a nonfinite value.
 void solver_set_invalid(SolverWorkspace* w, uint32_t* invalid);
+// Bound of the TMA apply's copy waits (0: kDefaultWaitPolls); stall_stencil
+// in 0..13 makes the wait for that stencil's box wait on an mbarrier that
+// nothing arrives on (a test of the bound), -1 none.
+void solver_set_waits(SolverWorkspace* w, uint32_t polls, int stall_stencil);
 int solver_solve(SolverWorkspace* w, const void* e, const void* bcell, const void* j,
                  const void* mass, double* etheta, tpicb200_gmres_result* result,
                  int max_iterations, double tol, cudaStream_t s, cudaError_t* err);

@@ -117,6 +117,7 @@ struct TcParams {
   int ns;
   float inv_volume;
   uint32_t wait_polls;  // polls of the stream kernel's chunk-loop waits before they give up
+  uint32_t stall_chunk; // nonzero: the wait for chunk stall_chunk - 1 targets `never` (a test of the waits)
 };
 
 template <bool Bf16> struct __align__(128) TcShared {
@@ -640,6 +641,7 @@ struct __align__(16) StreamShared {
   uint32_t arrived[2];  // arrivals of the chunks of each parity (monotonic)
   uint32_t decision;    // (chunk << 1) | (some warp has a chunk after it)
   uint64_t mma_bar;     // the MMAs of a chunk have completed
+  uint64_t never;       // an mbarrier that nothing arrives on (TcParams::stall_chunk)
   uint32_t tmem_base;
 };
 
@@ -682,6 +684,7 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
   }
   if (threadIdx.x == 0) {
     tc::mbar_init(&sh.mma_bar, 1);
+    tc::mbar_init(&sh.never, 1);
     tc::fence_mbar_init();
     sh.more[0] = sh.more[1] = 0u;
     sh.arrived[0] = sh.arrived[1] = 0u;
@@ -1045,7 +1048,8 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
     // The MMAs of chunk j - 1 have completed: flush the cells that ended in
     // it; a warp without chunks learns whether any warp of the CTA has one.
     if (j > 0) {
-      const bool done = tc::mbar_wait(&sh.mma_bar, (j - 1) & 1u, tp.wait_polls);
+      const bool stall = j == tp.stall_chunk;
+      const bool done = tc::mbar_wait(stall ? &sh.never : &sh.mma_bar, stall ? 0u : (j - 1) & 1u, tp.wait_polls);
       if (__any_sync(0xffffffffu, !done)) {
         bad = true;
         break;
@@ -1162,7 +1166,7 @@ cudaError_t launch_deposit_tc(int mass_kind, const Geom& g, int ns, const double
                               const tpicb200_particles* const* p, const uint32_t* const* counts,
                               const uint32_t* const* offsets, const void* bnode, float* moments, int accumulate,
                               uint32_t* invalid, const SortedCopy* const* copies, cudaStream_t s,
-                              uint32_t wait_polls) {
+                              uint32_t wait_polls, uint32_t stall_chunk) {
   if (mass_kind != TPICB200_MASS_TF32 && mass_kind != TPICB200_MASS_BF16X3) return cudaErrorNotSupported;
   if (!moments || ns < 1) return cudaErrorInvalidValue;
   int device = 0, sms = 148;
@@ -1198,6 +1202,7 @@ cudaError_t launch_deposit_tc(int mass_kind, const Geom& g, int ns, const double
     tp.ns = std::min(kFuse, ns - first);
     tp.inv_volume = float(g.inv_volume);
     tp.wait_polls = wait_polls ? wait_polls : kDefaultWaitPolls;
+    tp.stall_chunk = stall_chunk;
     for (int i = 0; i < tp.ns; ++i) {
       const tpicb200_particles* sp = p[first + i];
       const SortedCopy* cp = copies ? copies[first + i] : nullptr;

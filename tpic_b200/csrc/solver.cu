@@ -35,7 +35,11 @@ namespace tpicb200 {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kDotTile = 4;
+constexpr int kDotTile = 8;
+// Krylov basis columns start kColumnAlign elements apart (vector loads).
+constexpr long long kColumnAlign = 64;
+// Largest GMRES restart the context accepts.
+constexpr int kMaxRestart = 1024;
 
 // Device-side state of one restart cycle's Arnoldi steps.
 struct ArnoldiControl {
@@ -293,8 +297,9 @@ __global__ void __launch_bounds__(TX * TY * TZ, sizeof(C) == 4 ? 4 : 3) maxwell_
 // copy, and the stage is refilled with stencil s + S after a CTA barrier. The
 // input v and the cell curls are staged as in maxwell_apply_kernel, and every
 // sum runs in the same order, so the result equals it bit for bit. A copy
-// that does not arrive within the bound adds 1 << 21 to *invalid; the CTA
-// then waits (bounded) for its copies in flight and returns.
+// that does not arrive within `polls` polls adds 1 << 21 to *invalid; the
+// CTA then waits (with the default bound) for its copies in flight and
+// returns without writing its rows.
 constexpr int kBoxX = 36;
 
 template <int TY, int TZ, class M> struct TmaBox {
@@ -310,21 +315,22 @@ struct TmaApplyShared {
   static constexpr int VX = TX + 2, VY = TY + 2, VZ = TZ + 2;
   static constexpr int CX = TX + 1, CY = TY + 1, CZ = TZ + 1;
   static constexpr int stages = S * TmaBox<TY, TZ, M>::stage;
-  static constexpr int bars = stages;                              // S mbarriers
-  static constexpr int vs = (bars + S * 8 + 15) / 16 * 16;         // C [3][VZ][VY][VX]
+  static constexpr int bars = stages;                              // S + 1 mbarriers
+  static constexpr int vs = (bars + (S + 1) * 8 + 15) / 16 * 16;   // C [3][VZ][VY][VX]
   static constexpr int cs = vs + 3 * VZ * VY * VX * int(sizeof(C));  // C [3][CZ][CY][CX]
   static constexpr int total = cs + 3 * CZ * CY * CX * int(sizeof(C));
 };
 
 template <class C, class M, class Out, int TX, int TY, int TZ, int S, bool kTranspose>
-__global__ void __launch_bounds__(TX * TY * TZ, sizeof(C) == 4 ? 3 : 2)
+__global__ void __launch_bounds__(TX * TY * TZ, sizeof(C) == 4 ? 4 : 2)
     maxwell_apply_tma_kernel(const __grid_constant__ CUtensorMap map, Geom g, C d2, C kfac, C inv_volume,
-                             const double* __restrict__ v, Out* __restrict__ out, uint32_t* invalid) {
+                             const double* __restrict__ v, Out* __restrict__ out, uint32_t* invalid,
+                             uint32_t polls, int stall) {
   using Box = TmaBox<TY, TZ, M>;
   using L = TmaApplyShared<C, M, TX, TY, TZ, S>;
   constexpr int VX = L::VX, VY = L::VY, VZ = L::VZ, CX = L::CX, CY = L::CY, CZ = L::CZ;
   extern __shared__ __align__(1024) uint8_t tma_smem[];
-  uint64_t* bars = reinterpret_cast<uint64_t*>(tma_smem + L::bars);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(tma_smem + L::bars);  // S stage barriers, then `never`
   auto vs = reinterpret_cast<C (*)[VZ][VY][VX]>(tma_smem + L::vs);
   auto cs = reinterpret_cast<C (*)[CZ][CY][CX]>(tma_smem + L::cs);
   const C inv[3] = {C(g.inv[0]), C(g.inv[1]), C(g.inv[2])};
@@ -341,7 +347,7 @@ __global__ void __launch_bounds__(TX * TY * TZ, sizeof(C) == 4 ? 3 : 2)
   };
   if (threadIdx.x == 0) {
 #pragma unroll
-    for (int b = 0; b < S; ++b) tc::mbar_init(&bars[b], 1);
+    for (int b = 0; b <= S; ++b) tc::mbar_init(&bars[b], 1);
     tc::fence_mbar_init();
   }
   __syncthreads();
@@ -408,7 +414,10 @@ __global__ void __launch_bounds__(TX * TY * TZ, sizeof(C) == 4 ? 3 : 2)
 #pragma unroll
   for (int s = 0; s < 14; ++s) {
     if (failed) continue;
-    const bool ok = tc::mbar_wait(&bars[s % S], uint32_t((s / S) & 1));
+    // stall == s (a test of the bound) waits on bars[S], which nothing
+    // arrives on.
+    const bool ok = s == stall ? tc::mbar_wait(&bars[S], 0u, polls)
+                               : tc::mbar_wait(&bars[s % S], uint32_t((s / S) & 1), polls);
     if (__syncthreads_or(!ok)) {
       failed = true;
       continue;
@@ -439,11 +448,12 @@ __global__ void __launch_bounds__(TX * TY * TZ, sizeof(C) == 4 ? 3 : 2)
     }
   }
   if (failed) {
-    // Copies issued but not consumed may still land: wait for them (bounded)
-    // before the CTA's shared memory is released.
+    // Copies issued but not consumed may still land: wait for them (with the
+    // default bound) before the CTA's shared memory is released.
     if (threadIdx.x == 0) {
       if (invalid) atomicAdd(invalid, 1u << 21);
-      for (int s = consumed; s < 14 && s < consumed + S; ++s) tc::mbar_wait(&bars[s % S], uint32_t((s / S) & 1));
+      for (int s = consumed; s < 14 && s < consumed + S; ++s)
+        tc::mbar_wait(&bars[s % S], uint32_t((s / S) & 1), kDefaultWaitPolls);
     }
     __syncthreads();
     return;
@@ -549,27 +559,67 @@ __global__ void __launch_bounds__(kThreads) pack_storage_kernel(Geom g, const T*
   }
 }
 
-// Dots of `image` with basis columns [first, first+4) per block row,
+// Four consecutive elements of a basis column or of the image (16-byte
+// aligned: columns are kColumnAlign elements apart), widened to double.
+struct Quad {
+  double v[4];
+};
+__device__ __forceinline__ Quad load_quad(const float* p) {
+  const float4 q = *reinterpret_cast<const float4*>(p);
+  return Quad{{q.x, q.y, q.z, q.w}};
+}
+__device__ __forceinline__ Quad load_quad(const double* p) {
+  const double2 a = reinterpret_cast<const double2*>(p)[0], b = reinterpret_cast<const double2*>(p)[1];
+  return Quad{{a.x, a.y, b.x, b.y}};
+}
+__device__ __forceinline__ void store_quad(float* p, const float (&v)[4]) {
+  *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void store_quad(double* p, const double (&v)[4]) {
+  reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+  reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+}
+
+// Dots of `image` with basis columns [first, first + kDotTile) per block row,
 // block partials per column (gmres_dot_batch_kernel, gmres_device.hpp:163-192).
+// Each thread takes four consecutive elements at a time (one 16-byte load per
+// column); the `count % 4` tail elements go to the first threads. Columns
+// are `ld` elements apart.
 template <class S>
 __global__ void __launch_bounds__(kThreads) dot_batch_kernel(const S* __restrict__ basis, const S* __restrict__ image,
                                                              double* __restrict__ partials, long long count,
-                                                             const ArnoldiControl* __restrict__ ctl) {
+                                                             long long ld, const ArnoldiControl* __restrict__ ctl) {
   wait_for_predecessor();
   __shared__ double scratch[kDotTile][kThreads / 32];
   const int columns = ctl->col + 1;
+  const long long quads = count >> 2, stride = (long long)gridDim.x * blockDim.x;
+  const long long start = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   for (int first = blockIdx.y * kDotTile; first < columns; first += gridDim.y * kDotTile) {
-    double sum[kDotTile] = {0, 0, 0, 0};
-    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < count;
-         n += (long long)gridDim.x * blockDim.x) {
-      const double value = double(image[n]);
+    const int tile = min(kDotTile, columns - first);
+    const S* col = basis + (long long)first * ld;
+    double sum[kDotTile];
+#pragma unroll
+    for (int r = 0; r < kDotTile; ++r) sum[r] = 0.0;
+    for (long long q = start; q < quads; q += stride) {
+      const Quad x = load_quad(image + 4 * q);
 #pragma unroll
       for (int r = 0; r < kDotTile; ++r)
-        if (first + r < columns) sum[r] += double(basis[(long long)(first + r) * count + n]) * value;
+        if (r < tile) {
+          const Quad b = load_quad(col + r * ld + 4 * q);
+#pragma unroll
+          for (int e = 0; e < 4; ++e) sum[r] += b.v[e] * x.v[e];
+        }
+    }
+    const long long tail = 4 * quads + start;
+    if (tail < count) {
+      const double value = double(image[tail]);
+#pragma unroll
+      for (int r = 0; r < kDotTile; ++r)
+        if (r < tile) sum[r] += double(col[r * ld + tail]) * value;
     }
 #pragma unroll
     for (int r = 0; r < kDotTile; ++r)
-      if (first + r < columns) {
+      if (r < tile) {
         const double total = block_sum<kThreads>(sum[r], scratch[r]);
         if (threadIdx.x == 0) partials[(long long)(first + r) * gridDim.x + blockIdx.x] = total;
       }
@@ -604,26 +654,61 @@ __global__ void __launch_bounds__(kThreads) residual_kernel(const double* __rest
 // Classical Gram-Schmidt with the reduced dots, squared-norm partials of the
 // stored result; block 0 copies the dots into the Hessenberg column
 // (gmres_orthogonalize_squared_norm_kernel, gmres_device.hpp:243-263).
+// Every element subtracts the columns in order 0, 1, ...; a thread takes four
+// consecutive elements at a time (16-byte loads, the columns' loads issued
+// four at once), the `count % 4` tail elements go to the first threads.
 template <class S>
 __global__ void __launch_bounds__(kThreads) orthogonalize_kernel(const S* __restrict__ basis, const double* __restrict__ dots,
                                                                  S* __restrict__ image, double* __restrict__ hessenberg,
                                                                  int leading, double* __restrict__ partials,
-                                                                 long long count, const ArnoldiControl* __restrict__ ctl) {
+                                                                 long long count, long long ld,
+                                                                 const ArnoldiControl* __restrict__ ctl) {
   wait_for_predecessor();
   __shared__ double scratch[kThreads / 32];
+  __shared__ double h[kMaxRestart + 1];
   const int columns = ctl->col + 1;
+  for (int c = threadIdx.x; c < columns; c += blockDim.x) h[c] = dots[c];
+  __syncthreads();
   double* column = hessenberg + (long long)ctl->col * leading;
   double norm2 = 0;
-  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < count;
-       n += (long long)gridDim.x * blockDim.x) {
-    double value = double(image[n]);
-    for (int c = 0; c < columns; ++c) value -= dots[c] * double(basis[(long long)c * count + n]);
+  const long long quads = count >> 2, stride = (long long)gridDim.x * blockDim.x;
+  const long long start = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  for (long long q = start; q < quads; q += stride) {
+    const Quad x = load_quad(image + 4 * q);
+    double value[4] = {x.v[0], x.v[1], x.v[2], x.v[3]};
+    int c = 0;
+    for (; c + 4 <= columns; c += 4) {
+      Quad b[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) b[r] = load_quad(basis + (long long)(c + r) * ld + 4 * q);
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) value[e] -= h[c + r] * b[r].v[e];
+    }
+    for (; c < columns; ++c) {
+      const Quad b = load_quad(basis + (long long)c * ld + 4 * q);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) value[e] -= h[c] * b.v[e];
+    }
+    S stored[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      stored[e] = S(value[e]);
+      norm2 += double(stored[e]) * double(stored[e]);
+    }
+    store_quad(image + 4 * q, stored);
+  }
+  const long long tail = 4 * quads + start;
+  if (tail < count) {
+    double value = double(image[tail]);
+    for (int c = 0; c < columns; ++c) value -= h[c] * double(basis[(long long)c * ld + tail]);
     const S stored = S(value);
-    image[n] = stored;
+    image[tail] = stored;
     norm2 += double(stored) * double(stored);
   }
   if (blockIdx.x == 0 && threadIdx.x == 0)
-    for (int row = 0; row < columns; ++row) column[row] = dots[row];
+    for (int row = 0; row < columns; ++row) column[row] = h[row];
   const double total = block_sum<kThreads>(norm2, scratch);
   if (threadIdx.x == 0) partials[blockIdx.x] = total;
 }
@@ -718,12 +803,13 @@ template <class S>
 __global__ void __launch_bounds__(kThreads) update_solution_kernel(const S* __restrict__ basis,
                                                                    const double* __restrict__ coefficients,
                                                                    double* __restrict__ x, long long count,
+                                                                   long long ld,
                                                                    const ArnoldiControl* __restrict__ ctl) {
   const int columns = ctl->completed;
   for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < count;
        n += (long long)gridDim.x * blockDim.x) {
     double value = x[n];
-    for (int c = 0; c < columns; ++c) value += coefficients[c] * double(basis[(long long)c * count + n]);
+    for (int c = 0; c < columns; ++c) value += coefficients[c] * double(basis[(long long)c * ld + n]);
     x[n] = value;
   }
 }
@@ -784,13 +870,16 @@ __global__ void arnoldi_end_kernel(ArnoldiControl* ctl, const double* status, cu
 struct SolverWorkspace {
   int precision;
   bool transpose = false;       // applies use A^T (every mass block transposed): the adjoint solve
-  uint32_t* invalid = nullptr;  // the context's invalid counter (smoothing passes)
+  uint32_t* invalid = nullptr;  // the context's invalid counter (smoothing passes, TMA apply waits)
+  uint32_t wait_polls = 0;      // TMA apply wait bound (0: kDefaultWaitPolls)
+  int stall_stencil = -1;       // a test of that bound: the stencil whose wait targets no copy
   Geom g;
   int restart;
   double dt, theta, c, delta, kfac;
   long long count;  // 3 * interior
+  long long ld;     // basis column stride: count rounded up to kColumnAlign
   unsigned rblocks;
-  void* basis = nullptr;   // (restart+1) * count Scalar
+  void* basis = nullptr;   // (restart+1) columns of count Scalar, ld apart
   void* image = nullptr;   // count Scalar
   double* x = nullptr;
   double* b = nullptr;
@@ -837,7 +926,7 @@ struct SolverWorkspace {
   double* ls_rhs() { return sine() + restart; }
   double* coefficients() { return ls_rhs() + restart + 1; }
   double* status() { return coefficients() + restart; }
-  template <class S> S* basis_col(int c) { return (S*)basis + (size_t)c * count; }
+  template <class S> S* basis_col(int c) { return (S*)basis + (size_t)c * ld; }
 };
 
 SolverWorkspace* solver_create(int precision, const Geom& g, int restart, double dt, double theta,
@@ -856,6 +945,7 @@ SolverWorkspace* solver_create(int precision, const Geom& g, int restart, double
   w->delta = c * theta * dt;
   w->kfac = 4 * 3.14159265358979323846 * (theta * dt);
   w->count = 3 * g.interior;
+  w->ld = (w->count + kColumnAlign - 1) / kColumnAlign * kColumnAlign;
   int device = 0, sms = 148;
   cudaGetDevice(&device);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -872,7 +962,7 @@ SolverWorkspace* solver_create(int precision, const Geom& g, int restart, double
     alloc((void**)&w->smooth_b, 3 * g.nodes * sizeof(double));
     alloc((void**)&w->smooth_image, 3 * g.nodes * sizeof(double));
   }
-  alloc(&w->basis, (size_t)(restart + 1) * w->count * w->scalar_bytes);
+  alloc(&w->basis, (size_t)(restart + 1) * w->ld * w->scalar_bytes);
   alloc(&w->image, (size_t)w->count * w->scalar_bytes);
   alloc((void**)&w->x, w->count * sizeof(double));
   alloc((void**)&w->b, w->count * sizeof(double));
@@ -973,8 +1063,10 @@ const CUtensorMap* mass_tensor_map(SolverWorkspace* w, const M* mass, bool thin)
 // raised once per device.
 template <class C, class M, class Out, int TY, int TZ, bool kTranspose>
 cudaError_t launch_apply_tma(const CUtensorMap& map, unsigned tiles, cudaStream_t st, const Geom& g, C d2, C kf,
-                             C civ, const double* in, Out* out, uint32_t* invalid) {
-  constexpr int S = sizeof(M) == 4 ? 3 : 2;
+                             C civ, const double* in, Out* out, uint32_t* invalid, uint32_t polls, int stall) {
+  // Two stages: four CTAs per SM in the float apply (three in the mixed
+  // residual apply); three stages gave three (two) and a slower solve.
+  constexpr int S = 2;
   constexpr int bytes = TmaApplyShared<C, M, kTX, TY, TZ, S>::total;
   static_assert(bytes <= 227 * 1024, "apply tile exceeds shared memory");
   auto kernel = maxwell_apply_tma_kernel<C, M, Out, kTX, TY, TZ, S, kTranspose>;
@@ -988,7 +1080,8 @@ cudaError_t launch_apply_tma(const CUtensorMap& map, unsigned tiles, cudaStream_
     if (e != cudaSuccess) return e;
     ready.fetch_or(bit);
   }
-  return launch_programmatic(kernel, tiles, kTX * TY * TZ, bytes, st, map, g, d2, kf, civ, in, out, invalid);
+  return launch_programmatic(kernel, tiles, kTX * TY * TZ, bytes, st, map, g, d2, kf, civ, in, out, invalid,
+                             polls ? polls : kDefaultWaitPolls, stall);
 }
 
 template <class P>
@@ -1040,15 +1133,21 @@ struct Solve {
     const double* in = w->input;
     const CUtensorMap* map = response ? nullptr : mass_tensor_map(w, mass, thin);
     if (map) {
+      const uint32_t polls = w->wait_polls;
+      const int stall = w->stall_stencil;
       cudaError_t e;
       if (w->transpose && thin)
-        e = launch_apply_tma<C, Mass, Out, kThinTY, 1, true>(*map, tiles, st, g, d2, kf, civ, in, out, w->invalid);
+        e = launch_apply_tma<C, Mass, Out, kThinTY, 1, true>(*map, tiles, st, g, d2, kf, civ, in, out, w->invalid,
+                                                             polls, stall);
       else if (w->transpose)
-        e = launch_apply_tma<C, Mass, Out, kTY, kTZ, true>(*map, tiles, st, g, d2, kf, civ, in, out, w->invalid);
+        e = launch_apply_tma<C, Mass, Out, kTY, kTZ, true>(*map, tiles, st, g, d2, kf, civ, in, out, w->invalid,
+                                                           polls, stall);
       else if (thin)
-        e = launch_apply_tma<C, Mass, Out, kThinTY, 1, false>(*map, tiles, st, g, d2, kf, civ, in, out, w->invalid);
+        e = launch_apply_tma<C, Mass, Out, kThinTY, 1, false>(*map, tiles, st, g, d2, kf, civ, in, out, w->invalid,
+                                                              polls, stall);
       else
-        e = launch_apply_tma<C, Mass, Out, kTY, kTZ, false>(*map, tiles, st, g, d2, kf, civ, in, out, w->invalid);
+        e = launch_apply_tma<C, Mass, Out, kTY, kTZ, false>(*map, tiles, st, g, d2, kf, civ, in, out, w->invalid,
+                                                            polls, stall);
       if (err == cudaSuccess) err = e;
     } else if (w->transpose) {
       // The adjoint solve (no smoothing): every mass block transposed.
@@ -1113,15 +1212,15 @@ struct Solve {
     apply<S, S>(mass, image, st);
     const dim3 grid(w->rblocks, (m + kDotTile - 1) / kDotTile);
     launch_programmatic(dot_batch_kernel<S>, grid, kThreads, 0, st, (const S*)basis, (const S*)image, w->partials, N,
-                        (const ArnoldiControl*)w->ctl);
+                        w->ld, (const ArnoldiControl*)w->ctl);
     launch_programmatic(reduce_columns_kernel, unsigned(m), 256, 0, st, (const double*)w->partials, w->values,
                         int(w->rblocks), (const ArnoldiControl*)w->ctl);
     launch_programmatic(orthogonalize_kernel<S>, w->rblocks, kThreads, 0, st, (const S*)basis,
-                        (const double*)w->values, image, w->hessenberg(), m + 1, w->partials, N,
+                        (const double*)w->values, image, w->hessenberg(), m + 1, w->partials, N, w->ld,
                         (const ArnoldiControl*)w->ctl);
     launch_reduce_rows(w->partials, w->values, w->batch, w->rblocks, w->rblocks, 1, st, true);
     launch_programmatic(normalize_kernel<S, S>, w->rblocks, kThreads, 0, st, g, (const S*)image,
-                        (const double*)w->values, basis, N, w->input,
+                        (const double*)w->values, basis, w->ld, w->input,
                         ArnoldiTail{w->hessenberg(), w->cosine(), w->sine(), w->ls_rhs(), w->status(), 0, m + 1},
                         (const ArnoldiControl*)w->ctl);
     launch_programmatic(arnoldi_end_kernel, 1u, 1u, 0, st, w->ctl, (const double*)w->status(), handle, conditional);
@@ -1309,7 +1408,7 @@ struct Solve {
       cudaMemsetAsync(w->state, 0, ((size_t)m * (m + 1) + 4 * m + 3) * sizeof(double), s);
       // values[0] holds |r|^2 of the residual just formed.
       normalize_kernel<double, S><<<w->rblocks, kThreads, 0, s>>>(
-          g, w->r, w->values, w->template basis_col<S>(0), N, w->input,
+          g, w->r, w->values, w->template basis_col<S>(0), w->ld, w->input,
           ArnoldiTail{nullptr, nullptr, nullptr, w->ls_rhs(), nullptr, -1, 0}, nullptr);
       const int columns = std::min(m, max_iterations - res.iterations);
       const double cycle_tolerance =
@@ -1329,7 +1428,8 @@ struct Solve {
       }
       back_substitute_kernel<<<1, 1, 0, s>>>(w->hessenberg(), w->ls_rhs(), w->coefficients(), m + 1, w->ctl);
       update_solution_kernel<S><<<grid_for(N, kThreads), kThreads, 0, s>>>(w->template basis_col<S>(0),
-                                                                          w->coefficients(), w->x, N, w->ctl);
+                                                                          w->coefficients(), w->x, N, w->ld,
+                                                                          w->ctl);
       count_launches(2);
       check();
       apply_solution(mass);
@@ -1375,6 +1475,14 @@ int solver_solve(SolverWorkspace* w, const void* e, const void* bcell, const voi
 }
 
 void solver_set_invalid(SolverWorkspace* w, uint32_t* invalid) { w->invalid = invalid; }
+
+void solver_set_waits(SolverWorkspace* w, uint32_t polls, int stall_stencil) {
+  if (polls == w->wait_polls && stall_stencil == w->stall_stencil) return;
+  w->wait_polls = polls;
+  w->stall_stencil = stall_stencil;
+  // The step graphs hold the apply's arguments: capture them again.
+  for (int t = 0; t < 2; ++t) w->loop_mass[t] = nullptr;
+}
 
 int solver_solve_adjoint(SolverWorkspace* w, const double* rhs, const void* mass, double* lambda,
                          tpicb200_gmres_result* result, int max_iterations, double tol, cudaStream_t s,
