@@ -585,47 +585,43 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_deposit_kernel(Geom g, TcP
 // Each warp owns a sequence of batches of four consecutive cells (batches
 // gw, gw + W, gw + 2W, ... for global warp gw of W) and walks a batch's
 // records as one stream - cell by cell, species 0 before species 1 in a
-// cell - 32 per chunk (one per lane), without padding between cells: a chunk
-// may hold the tail of one cell and the head of the next nonempty cell. The
-// warp's quadrant of D therefore holds two accumulator blocks that alternate
-// between consecutive nonempty cells (the cell's parity), and a cell is
-// flushed - read from tensor memory, then zeroed - once the MMAs of its last
-// chunk have completed and before the warp's next chunk is issued. A chunk
-// ends early where it would reach a third nonempty cell. Every batch starts a
-// new chunk, so a cell's summation order depends only on its batch's counts:
-// the moments are reproducible.
+// cell - in chunks of up to 32 records (one per lane). A chunk never crosses
+// the end of a (cell, species) range, so its cell and species are the same
+// for every lane: the species' record arrays are addressed without per-lane
+// selection, and the warp's quadrant of D holds one accumulator block, which
+// is flushed - read from tensor memory, then zeroed - once the MMAs of the
+// cell's last chunk have completed and before the warp's next chunk is
+// written. Every batch starts a new chunk, so a cell's summation order
+// depends only on its batch's counts: the moments are reproducible.
 //
 // The four warps of a CTA share every MMA (M = 128 = four quadrants of 32
 // monomial rows; rows 27..31 of a quadrant stay zero):
 //   A (shared memory, MN-major, 128 x 32, BF16 hi and lo): row 32w + t,
 //     column k holds m_t of warp w's lane-k record;
-//   B (shared memory, MN-major, 32 x 96, BF16 hi and lo): columns 24w..24w+23
-//     belong to warp w: parity 0 uses columns 0..7 and 8..11 of them, parity 1
-//     columns 16..23 and 12..15; a lane writes its 12 values (s alpha, j) in
-//     its parity's block and zeros in the other;
-//   D (tensor memory, 128 x 96 FP32): D[32w + t][24w + 16p + c] = G[t][c]
-//     (c < 8) and D[32w + t][24w + 8 + 4p + c] = (G[t][8], H[t][0..2]).
+//   B (shared memory, MN-major, 32 x 64, BF16 hi and lo): columns
+//     16w..16w+11 hold the 12 values (s alpha, j) of warp w's lane-k record
+//     in row k, columns 16w+12..16w+15 stay zero;
+//   D (tensor memory, 128 x 64 FP32): D[32w + t][16w + c] = G[t][c] (c < 9)
+//     and H[t][c - 9] (9 <= c < 12); the off-diagonal blocks are never read.
 // Both operands are single-buffered: a warp writes chunk j's A and B after the
 // MMAs of chunk j - 1 have completed, which it waits for anyway to flush the
-// cells that ended in chunk j - 1. The warps build the A rows of their own
+// cell that ended in chunk j - 1. The warps build the A rows of their own
 // records directly (27 products per lane), with no transposition. The last
 // warp to finish writing a chunk's operands (an acquire-release counter per
 // chunk parity) issues its MMAs, so no warp waits for the others.
 //
-// Records are fetched in a three-stage software pipeline per warp: the walk
-// of chunk j + 2 issues the rank loads, chunk j + 1's record loads are in
-// flight, chunk j is computed. A warp that has run out of batches keeps
+// Records are fetched in a software pipeline per warp: the walk of chunk
+// j + 3 copies the ranks (cp.async), chunk j + 1's record loads are in
+// flight while chunk j is computed. A warp that has run out of batches keeps
 // arriving with no data while any warp of its CTA still has chunks (each
 // warp publishes, per chunk, whether it has another; the issuer publishes
 // the CTA's answer), and the CTA's warps leave the loop together.
 constexpr int kBatch = 4;                  // cells per batch
-constexpr int kStreamN = 96;               // B columns: 4 quadrants x 2 parities x 12
-constexpr uint32_t kStreamTmemCols = 128;  // D uses 96 of them
+constexpr int kStreamN = 64;               // B columns: 4 quadrants x 16 (12 used)
+constexpr uint32_t kStreamTmemCols = 64;
 constexpr int kMetaSlots = 3;              // batches of chunks j .. j + 2
 
 struct StreamMeta {
-  uint32_t split[kBatch];   // stream position of the cell's first species-1 record
-  uint32_t off[kBatch][2];  // sorted position - stream position, species 0 / 1
   int32_t bin[kBatch];
   float bpoly[kBatch][24];
 };
@@ -646,12 +642,13 @@ struct __align__(16) StreamShared {
 };
 
 // Per-lane record of a chunk: rank (record index in the read slot), sorted
-// position, flags (1 present, 2 second species, slot << 2, parity << 4).
+// position, flags (1 present).
 struct StreamLane {
   uint32_t idx, pos, flags;
 };
 // Warp-uniform chunk description: batch and bits (ended cells 0-3,
-// nonempty cells 4-7, parities 8-11, valid 13, metadata slot 14-15).
+// nonempty cells 4-7, species 12, valid 13, metadata slot 14-15, cell slot
+// 16-17).
 struct StreamInfo {
   int bid;
   uint32_t bits;
@@ -694,13 +691,13 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
   __syncthreads();
   tc::fence_after_sync();
   const uint32_t tmem = sh.tmem_base;
-  // This warp's 24 accumulator columns, in its own 32 lanes.
-  const uint32_t dq = tmem + (uint32_t(32 * warp) << 16) + 24u * warp;
+  // This warp's 12 accumulator columns, in its own 32 lanes.
+  const uint32_t dq = tmem + (uint32_t(32 * warp) << 16) + 16u * warp;
   {
     const uint32_t z[8] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
+    const uint32_t z4[4] = {0u, 0u, 0u, 0u};
     tc::tmem_st8(dq, z);
-    tc::tmem_st8(dq + 8, z);
-    tc::tmem_st8(dq + 16, z);
+    tc::tmem_st4(dq + 8, z4);
     tc::tmem_wait_st();
   }
   constexpr uint32_t idesc = tc::instr_desc(1u, 128, kStreamN, 1u, 1u);
@@ -732,14 +729,16 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
     return r;
   };
   // The walk: a warp-uniform cursor over this warp's batches. Per batch,
-  // the cumulative record starts of its cells (start of slot s = b[s],
-  // b[0] = 0, b[4] = total), the nonempty cells and their parities.
+  // the eight (cell, species) ranges of its stream: lane r < 8 holds the
+  // stream end of range r = 2 slot + species and its sorted-array offset
+  // minus its stream start; cb1, cb2, cb3, ctot are the cell ends.
   int cbid = blockIdx.x * kCells + warp;  // current batch
   int cslot = 0;                          // its metadata slot
+  uint32_t rend = 0, roff = 0;
   uint32_t cb1 = 0, cb2 = 0, cb3 = 0, ctot = 0;
-  uint32_t cbits = 0;  // nonempty | parity << 4 of the batch
-  uint32_t cbase = 0;  // stream position of the next chunk
-  uint32_t cdone = 0;  // cells of the batch already ended
+  uint32_t cnonempty = 0;  // nonempty cells of the batch
+  uint32_t cbase = 0;      // stream position of the next chunk
+  uint32_t cdone = 0;      // cells of the batch already ended
   bool cend = cbid >= batches, cnext = false;
   // Writes a batch's metadata into its slot and sets the cursor's batch
   // state: counts and offsets, bins and the trilinear B of each cell as a
@@ -748,27 +747,26 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
   auto enter_batch = [&](const MetaRegs& r) {
     StreamMeta& m = sh.meta[warp][cslot];
     float* tmp = sh.scratch[warp];
-    const uint32_t n = r.c0 + r.c1;
-    uint32_t incl = n;  // inclusive scan over lanes 0..3
+    const int cell_slot = (lane >> 1) & 3;
+    const uint32_t c0 = __shfl_sync(0xffffffffu, r.c0, cell_slot), c1 = __shfl_sync(0xffffffffu, r.c1, cell_slot);
+    const uint32_t f0 = __shfl_sync(0xffffffffu, r.f0, cell_slot), f1 = __shfl_sync(0xffffffffu, r.f1, cell_slot);
+    const uint32_t n = lane < 2 * kBatch ? ((lane & 1) ? c1 : c0) : 0u;
+    uint32_t incl = n;  // inclusive scan over the ranges
 #pragma unroll
-    for (int o = 1; o < kBatch; o <<= 1) {
+    for (int o = 1; o < 2 * kBatch; o <<= 1) {
       const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-      if ((lane & 3) >= o) incl += t;
+      if (lane >= o) incl += t;
     }
-    const uint32_t start = incl - n;
-    if (lane < kBatch) {
-      m.split[lane] = start + r.c0;
-      m.off[lane][0] = r.f0 - start;
-      m.off[lane][1] = r.f1 - (start + r.c0);
-      m.bin[lane] = r.bin;
-    }
+    rend = incl;
+    roff = ((lane & 1) ? f1 : f0) - (incl - n);
+    if (lane < kBatch) m.bin[lane] = r.bin;
 #pragma unroll
     for (int i = 0; i < 3; ++i) tmp[(lane & 3) * 24 + (lane >> 2) + 8 * i] = r.corner[i];
-    cb1 = __shfl_sync(0xffffffffu, incl, 0);
-    cb2 = __shfl_sync(0xffffffffu, incl, 1);
-    cb3 = __shfl_sync(0xffffffffu, incl, 2);
-    ctot = __shfl_sync(0xffffffffu, incl, 3);
-    const uint32_t nonempty = __ballot_sync(0xffffffffu, lane < kBatch && n > 0u) & 0xFu;
+    cb1 = __shfl_sync(0xffffffffu, incl, 1);
+    cb2 = __shfl_sync(0xffffffffu, incl, 3);
+    cb3 = __shfl_sync(0xffffffffu, incl, 5);
+    ctot = __shfl_sync(0xffffffffu, incl, 7);
+    cnonempty = __ballot_sync(0xffffffffu, lane < kBatch && r.c0 + r.c1 > 0u) & 0xFu;
     __syncwarp();
     if (lane < 3 * kBatch) {
       const int s = lane / 3, c = lane - 3 * s;
@@ -786,10 +784,6 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
       cp[7] = ((bc[7] - bc[6]) - (bc[5] - bc[4])) - ((bc[3] - bc[2]) - (bc[1] - bc[0]));
     }
     __syncwarp();
-    uint32_t parity = 0;
-#pragma unroll
-    for (int s = 0; s < kBatch; ++s) parity |= (uint32_t(__popc(nonempty & ((1u << s) - 1u))) & 1u) << s;
-    cbits = nonempty | (parity << 4);
     cbase = 0;
     cdone = 0;
   };
@@ -813,58 +807,46 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
       }
     }
     if (cend) return;
-    // The chunk [cbase, end): at most 32 records, and no record of a third
-    // nonempty cell: end <= the second cell boundary above cbase.
-    uint32_t first = ctot, second = ctot;
-    first = cb3 > cbase ? cb3 : first;
-    first = cb2 > cbase ? cb2 : first;
-    first = cb1 > cbase ? cb1 : first;
-    second = cb3 > first ? cb3 : second;
-    second = cb2 > first ? cb2 : second;
-    second = cb1 > first ? cb1 : second;
-    const uint32_t end = min(cbase + 32u, second);
+    // The chunk [cbase, end): at most 32 records of the first range that
+    // ends above cbase (empty ranges end at or below it).
+    const uint32_t above = __ballot_sync(0xffffffffu, lane < 2 * kBatch && rend > cbase);
+    // A batch without records has no range: its one chunk is empty.
+    const int range = above ? __ffs(above) - 1 : 0;
+    const uint32_t range_end = __shfl_sync(0xffffffffu, rend, range);
+    const uint32_t offset = __shfl_sync(0xffffffffu, roff, range);
+    const uint32_t end = above ? min(cbase + 32u, range_end) : cbase;
     // Cells ending in this chunk (empty cells at or below `end` included).
     uint32_t ended = (cb1 <= end ? 1u : 0u) | (cb2 <= end ? 2u : 0u) | (cb3 <= end ? 4u : 0u) |
                      (ctot <= end ? 8u : 0u);
     ended &= ~cdone;
     cdone |= ended;
     const bool last = end >= ctot;
+    const uint32_t second = uint32_t(range & 1);
     I.bid = cbid;
-    I.bits = ended | ((cbits & 0xFFu) << 4) | (1u << 13) | (uint32_t(cslot) << 14);
+    I.bits = ended | (cnonempty << 4) | (second << 12) | (1u << 13) | (uint32_t(cslot) << 14) |
+             (uint32_t(range >> 1) << 16);
     const uint32_t p = cbase + lane;
     if (p < end) {
-      const int slot = (p >= cb1 ? 1 : 0) + (p >= cb2 ? 1 : 0) + (p >= cb3 ? 1 : 0);
-      const StreamMeta& m = sh.meta[warp][cslot];
-      const uint32_t s1 = p >= m.split[slot] ? 1u : 0u;
-      L.pos = p + m.off[slot][s1];
-      const uint32_t* perm = s1 ? tp.sp[1].perm : tp.sp[0].perm;
+      L.pos = p + offset;
+      const uint32_t* perm = second ? tp.sp[1].perm : tp.sp[0].perm;
       uint32_t* dst = &sh.rank[warp][chunk & 3u][lane];
       if (perm)
         tc::cp_async4(dst, perm + L.pos);
       else
         *dst = L.pos;
-      L.flags = 1u | (s1 << 1) | (uint32_t(slot) << 2) | (((cbits >> (4 + slot)) & 1u) << 4);
+      L.flags = 1u;
     }
     if (last)
       cnext = true;
     else
       cbase = end;
   };
-  // The record index of a walked chunk (its rank copy has completed) and an
-  // L2 prefetch of the record, one chunk before its loads are issued.
-  auto prefetch_rec = [&](StreamLane& L, uint32_t chunk) {
-    L.idx = sh.rank[warp][chunk & 3u][lane];
-    if (L.flags & 1u) {
-      const TcSpecies& sp = (L.flags & 2u) ? tp.sp[1] : tp.sp[0];
-      const uint32_t n = L.idx;
-      prefetch_l2(sp.rx + n); prefetch_l2(sp.ry + n); prefetch_l2(sp.rz + n); prefetch_l2(sp.q + n);
-      prefetch_l2(sp.u + n); prefetch_l2(sp.v + n); prefetch_l2(sp.w + n); prefetch_l2(sp.key + n);
-    }
-  };
-  auto load_rec = [&](const StreamLane& L) {
+  // The record index of a walked chunk (its rank copy has completed).
+  auto take_rank = [&](StreamLane& L, uint32_t chunk) { L.idx = sh.rank[warp][chunk & 3u][lane]; };
+  // The record of a lane; the species is the chunk's (one branch per warp).
+  auto load_rec = [&](const StreamLane& L, const StreamInfo& I) {
     StreamRec r{0.0, 0.0, 0.0, 0.0, 0.0f, 0.0f, 0.0f, -1, L.pos, L.flags};
-    if (L.flags & 1u) {
-      const TcSpecies& sp = (L.flags & 2u) ? tp.sp[1] : tp.sp[0];
+    auto from = [&](const TcSpecies& sp) {
       const uint32_t n = L.idx;
       r.fx = sp.rx[n];
       r.fy = sp.ry[n];
@@ -874,6 +856,12 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
       r.v = sp.v[n];
       r.w = sp.w[n];
       r.key = sp.key[n];
+    };
+    if (L.flags & 1u) {
+      if ((I.bits >> 12) & 1u)
+        from(tp.sp[1]);
+      else
+        from(tp.sp[0]);
     }
     return r;
   };
@@ -882,22 +870,21 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
   auto flush = [&](const StreamInfo& I) {
     const uint32_t ended = I.bits & 0xFu;
     if (!((I.bits >> 13) & 1u) || ended == 0u) return;
-    const uint32_t nonempty = (I.bits >> 4) & 0xFu, parity = (I.bits >> 8) & 0xFu;
+    const uint32_t nonempty = (I.bits >> 4) & 0xFu;
     float* hs = sh.scratch[warp];
 #pragma unroll 1
     for (int s = 0; s < kBatch; ++s) {
       if (!((ended >> s) & 1u)) continue;
       float* st = sh.stage[warp][s];
       if ((nonempty >> s) & 1u) {
-        const uint32_t p = (parity >> s) & 1u;
         uint32_t g8[8], g4[4];
-        tc::tmem_ld8(dq + 16u * p, g8);
-        tc::tmem_ld4(dq + 8u + 4u * p, g4);
+        tc::tmem_ld8(dq, g8);
+        tc::tmem_ld4(dq + 8u, g4);
         tc::tmem_wait_ld();
         const uint32_t z8[8] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
         const uint32_t z4[4] = {0u, 0u, 0u, 0u};
-        tc::tmem_st8(dq + 16u * p, z8);
-        tc::tmem_st4(dq + 8u + 4u * p, z4);
+        tc::tmem_st8(dq, z8);
+        tc::tmem_st4(dq + 8u, z4);
         if (lane < 27) {
 #pragma unroll
           for (int e = 0; e < 8; ++e) st[lane * 9 + e] = __uint_as_float(g8[e]);
@@ -944,8 +931,8 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
     }
   };
 
-  // Per-warp pipeline: chunk j + 3 walked (ranks copying), j + 2
-  // prefetched into L2, j + 1 loaded into registers, j computed.
+  // Per-warp pipeline: chunk j + 3 walked (ranks copying), j + 2's ranks
+  // read, j + 1 loaded into registers, j computed.
   StreamLane la, lb, lc;
   StreamInfo ia, ib, ic;
   // One cp.async group per walked chunk (empty when no rank is copied).
@@ -956,10 +943,10 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
   walk(lc, ic, 2u);
   tc::cp_async_commit();
   tc::cp_async_wait_group<2>();
-  prefetch_rec(la, 0u);
+  take_rank(la, 0u);
   tc::cp_async_wait_group<1>();
-  prefetch_rec(lb, 1u);
-  StreamRec r1 = load_rec(la);
+  take_rank(lb, 1u);
+  StreamRec r1 = load_rec(la, ia);
   StreamInfo i1 = ia;
   StreamInfo ip{0, 0u};  // the previous chunk, whose cells are flushed next
   bool bad = false;
@@ -967,14 +954,14 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
   for (uint32_t j = 0;; ++j) {
     const StreamRec r0 = r1;
     const StreamInfo i0 = i1;
-    r1 = load_rec(lb);
+    r1 = load_rec(lb, ib);
     i1 = ib;
     StreamLane ld;
     StreamInfo id;
     walk(ld, id, j + 3u);
     tc::cp_async_commit();
     tc::cp_async_wait_group<1>();
-    prefetch_rec(lc, j + 2u);
+    take_rank(lc, j + 2u);
     lb = lc;
     ib = ic;
     lc = ld;
@@ -989,11 +976,9 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
     for (int c = 0; c < 3; ++c) X[c] = 0.0f;
 #pragma unroll
     for (int c = 0; c < 9; ++c) YZ[c] = 0.0f;
-    uint32_t par = 0;
     if (have && (r0.flags & 1u)) {
-      const int slot = (r0.flags >> 2) & 3;
-      par = (r0.flags >> 4) & 1u;
-      const bool second = r0.flags & 2u;
+      const int slot = int(i0.bits >> 16) & 3;
+      const bool second = (i0.bits >> 12) & 1u;
       const TcSpecies& sp = second ? tp.sp[1] : tp.sp[0];
       if (sp.orx) {
         const uint32_t o = r0.pos;
@@ -1072,7 +1057,7 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
       }
     }
     if (have) {
-      // B: 12 values in the parity's block, zeros in the other.
+      // B: the 12 values in columns 16w..16w+11, zeros in 16w+12..16w+15.
       uint32_t bh[6], bl[6];
 #pragma unroll
       for (int e = 0; e < 6; ++e) split_pair(make_float2(bv[2 * e], bv[2 * e + 1]), bh[e], bl[e]);
@@ -1080,10 +1065,8 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
       for (int h = 0; h < 2; ++h) {
         const uint32_t* w = h ? bl : bh;
         uint8_t* base = sh.b[h] + kofs;
-        *reinterpret_cast<uint4*>(base + (3 * warp + 2 * par) * 512) = make_uint4(w[0], w[1], w[2], w[3]);
-        *reinterpret_cast<uint4*>(base + (3 * warp + 2 - 2 * par) * 512) = make_uint4(0u, 0u, 0u, 0u);
-        *reinterpret_cast<uint4*>(base + (3 * warp + 1) * 512) =
-            par ? make_uint4(0u, 0u, w[4], w[5]) : make_uint4(w[4], w[5], 0u, 0u);
+        *reinterpret_cast<uint4*>(base + (2 * warp) * 512) = make_uint4(w[0], w[1], w[2], w[3]);
+        *reinterpret_cast<uint4*>(base + (2 * warp + 1) * 512) = make_uint4(w[4], w[5], 0u, 0u);
       }
       // A: the 27 monomials m_t = X[t % 3] YZ[t / 3] of this lane's record.
       uint32_t ah[16], al[16];
