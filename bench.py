@@ -685,6 +685,51 @@ def end_to_end(sim, args, stream, barrier, nparticles, world, dist) -> dict:
             "seconds": seconds, "cycles": len(reports)}
 
 
+def run_solve(args) -> None:
+    """Field solves alone: the workload's bootstrap state (deposited mass and
+    J, startup E and B) solved --steps times after --warmup untimed solves,
+    timed with CUDA events on the context's stream. One JSON line with ms per
+    solve and the GMRES iterations. With TPICB200_STEP_GRAPH=0 in the
+    environment the Arnoldi steps are launched one by one (for a kernel
+    profiler's launch list)."""
+    import ctypes as C
+    import torch
+    from tpic_b200 import _lib
+    from tpic_b200.simulation import Simulation
+    case = workload(args.scale)
+    torch.cuda.set_device(0)
+    sim = Simulation(case, precision=args.precision, mass_kind=args.mass_matrix, generate_on_device=True,
+                     gmres_max_iterations=args.gmres_max_iterations, mass_layout=args.mass_layout)
+    sim.prepare()
+    st = sim.state
+    stream = C.c_void_p(sim.stream.cuda_stream)
+    e_theta = torch.zeros(3 * sim.layout.node_count, dtype=torch.float64, device=sim.device)
+    res = _lib.GmresResult()
+
+    def solve():
+        _lib.check(sim.lib.tpicb200_field_solve(sim.ctx, st.e, st.b_cell, st.j, st.mass, e_theta.data_ptr(),
+                                                C.byref(res), stream))
+
+    for _ in range(args.warmup):
+        solve()
+    torch.cuda.synchronize()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(sim.stream)
+    for _ in range(args.steps):
+        solve()
+    stop.record(sim.stream)
+    torch.cuda.synchronize()
+    ms = start.elapsed_time(stop) / args.steps
+    print(json.dumps({"metric": "field solve time", "value": ms, "unit": "ms", "steps": args.steps,
+                      "warmup": args.warmup, "gmres_iterations": res.iterations, "host_waits": res.host_waits,
+                      "relative_residual": res.relative_residual,
+                      "config": {"workload": f"bootstrap state of the {args.scale}^3-cell uniform plasma",
+                                 "precision": args.precision, "mass_matrix": args.mass_matrix,
+                                 "mass_layout": args.mass_layout,
+                                 "step_graph": os.environ.get("TPICB200_STEP_GRAPH", "1") != "0"}}))
+    sim.close()
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -720,6 +765,8 @@ def main():
     ap.add_argument("--e2e-cycles", type=int, default=20,
                     help="cycles of the end-to-end episode (upload, startup, cycles, energy readback)")
     ap.add_argument("--cpu-workers", type=int, default=0, help="host processes of the reference arm (0: all cores)")
+    ap.add_argument("--solve", action="store_true",
+                    help="time field solves alone on the workload's bootstrap state (ms per solve)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("at least 3 warm-up steps")
@@ -727,6 +774,8 @@ def main():
         run_reference(args)
     elif args.adjoint:
         run_adjoint(args)
+    elif args.solve:
+        run_solve(args)
     else:
         run_gpu(args)
 

@@ -370,8 +370,12 @@ int tpicb200_mass_apply(tpicb200_context* ctx, const void* mass, const double* i
 /* Field solve: rhs = E + delta curl_C2N(B) - k J; GMRES(restart) on
  * A(v) = v + delta^2 curl_C2N curl_N2C v + k M v / V from the guess E; writes
  * E_theta (interior nodes and ghosts) when converged. Host-blocking like
- * Gmres::host_blocking_solve (ecsim/gmres/gmres_device.hpp:353-454):
- * two scalars are read back per Arnoldi step. b_cell needs filled ghosts. */
+ * Gmres::host_blocking_solve (ecsim/gmres/gmres_device.hpp:353-454), which
+ * reads two scalars back per Arnoldi step; here the steps of a restart cycle
+ * run as one CUDA graph (a WHILE node) and the host waits once per restart
+ * cycle plus once for the initial residual. With the environment variable
+ * TPICB200_STEP_GRAPH=0 when the context is created, the host steps the loop
+ * (one wait per step). b_cell needs filled ghosts. */
 int tpicb200_field_solve(tpicb200_context* ctx, const void* e, const void* b_cell, const void* j,
                          const void* mass, double* e_theta, tpicb200_gmres_result* result,
                          tpicb200_stream stream);

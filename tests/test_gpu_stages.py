@@ -415,6 +415,41 @@ def test_fp64_moments_match_oracle(torch_cuda, layout, nx):
 
 
 @pytest.mark.parametrize("kind", [2, 3])
+def test_tc_mass_sparse_batches(torch_cuda, kind):
+    """Records in scattered cells only (every 13th cell), so many batches of
+    four cells are empty and a warp's stream runs through one-chunk batches:
+    the per-batch metadata of a chunk must survive the walk three chunks
+    ahead into later batches. The moments equal the oracle's and no record
+    is flagged."""
+    # More batches than the launch has warps (4 x 148 CTAs x 4 warps), so each
+    # warp walks several batches.
+    g = GridSpec(64, 64, 16, 6.4, 6.4, 1.6)
+    rng = np.random.default_rng(41)
+    d = species_arrays(g, 1, vth=(0.2, 0.1, 0.3), npcel=(2, 2, 2))
+    ex, ey = g.nx + 4, g.ny + 4
+    key = d["cell"].astype(np.int64)
+    i, j, k = key % ex - 2, (key // ex) % ey - 2, key // (ex * ey) - 2
+    keep = ((i + g.nx * (j + g.ny * k)) % 13) == 0
+    d = {name: np.ascontiguousarray(v[keep]) for name, v in d.items()}
+    n = len(d["cell"])
+    assert 0 < n < 60000
+    ctx = make_ctx(g, 1, dt=0.2, max_particles=n, mass_layout=1)
+    bnode = periodic_node_field(g, smooth_random_unique(g, rng, 0.9)).astype(np.float32)
+    parts = ctx.upload_particles(d)
+    parts, counts, offsets = ctx.sort(parts, n)
+    j_, m = ctx.moments()
+    ctx.deposit(-4.0, parts, n, ctx.field(bnode), j_, m, counts, offsets, kind=kind)
+    ctx.fold(j_, m)
+    jw, mw, bad = oracle_moments(g, 1, -4.0, 0.2, d, bnode)
+    assert bad == 0 and ctx.invalid_count() == 0
+    rel = 3e-3 if kind == 2 else 1e-4
+    jw_i, jg_i = interior_nodes(g, jw), interior_nodes(g, j_.cpu().numpy().astype(np.float64))
+    assert np.abs(jg_i - jw_i).max() <= rel * np.abs(jw_i).max() + 1e-15
+    mw_i, mg_i = interior_records(g, mw), interior_records(g, ctx.records(m))
+    assert np.abs(mg_i - mw_i).max() <= rel * np.abs(mw_i).max()
+
+
+@pytest.mark.parametrize("kind", [2, 3])
 def test_tc_moments_accumulate_two_species(torch_cuda, kind):
     """Two species deposited with the tensor-core forms before one fold: the
     second species adds to the cell moments of the first (compare with the

@@ -619,7 +619,7 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_deposit_kernel(Geom g, TcP
 constexpr int kBatch = 4;                  // cells per batch
 constexpr int kStreamN = 64;               // B columns: 4 quadrants x 16 (12 used)
 constexpr uint32_t kStreamTmemCols = 64;
-constexpr int kMetaSlots = 3;              // batches of chunks j .. j + 2
+constexpr int kMetaSlots = 4;              // batches of chunks j .. j + 3 (the walk of j + 3 precedes chunk j)
 
 struct StreamMeta {
   int32_t bin[kBatch];

@@ -27,6 +27,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <limits>
 #include <vector>
@@ -951,6 +952,9 @@ SolverWorkspace* solver_create(int precision, const Geom& g, int restart, double
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   w->rblocks = unsigned(std::min<long long>((w->count + kThreads - 1) / kThreads, 4LL * sms));
   w->batch = std::max(restart, 2);
+  // TPICB200_STEP_GRAPH=0 keeps the host-stepped Arnoldi loop (one launch per
+  // kernel, which a kernel profiler lists one by one).
+  if (const char* v = std::getenv("TPICB200_STEP_GRAPH")) w->loop_unavailable = std::strcmp(v, "0") == 0;
   w->scalar_bytes = precision == TPICB200_PRECISION_DOUBLE ? 8 : 4;
   cudaError_t e = cudaSuccess;
   auto alloc = [&](void** p, size_t bytes) {
