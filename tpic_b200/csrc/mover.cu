@@ -29,6 +29,7 @@
 #include "kernels.cuh"
 
 #include <climits>
+#include <type_traits>
 
 namespace tpicb200 {
 namespace {
@@ -149,12 +150,46 @@ struct SharedFields {
   }
 };
 
+// FP32 corner values staged in shared memory as component pairs for a run:
+// pair 0 = (Bx, By), 1 = (Bz, Ex), 2 = (Ey, Ez), layout [pair][z][y][x].
+struct SharedPairFields {
+  const float2* s;  // 3 x 2 x 2 x kRunNodes pairs
+  int x;            // cell offset in the run
+  __device__ __forceinline__ float2 operator()(int pair, int a) const {
+    return s[((pair * 2 + ((a >> 2) & 1)) * 2 + ((a >> 1) & 1)) * kRunNodes + x + (a & 1)];
+  }
+};
+
 template <class C, class F>
 __device__ __forceinline__ C gather8(const F& field, int which, int c, const C w[8]) {
   C value = 0;
 #pragma unroll
   for (int a = 0; a < 8; ++a) value += w[a] * field(which, c, a);
   return value;
+}
+
+// B and E_theta at the record: sum over corners a = 0..7 of w[a] * corner
+// value, each product and sum rounded on its own.
+template <class C, class F>
+__device__ __forceinline__ void gather_fields(const F& field, const C w[8], C (&b)[3], C (&e)[3]) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) b[c] = gather8<C>(field, 0, c, w);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) e[c] = gather8<C>(field, 1, c, w);
+}
+// The same sums, two components per packed FP32 multiply and add (each
+// element rounded on its own, so the results equal the scalar sums).
+__device__ __forceinline__ void gather_fields(const SharedPairFields& field, const float w[8], float (&b)[3],
+                                              float (&e)[3]) {
+  float2 sum[3] = {make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f)};
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    const float2 weight = make_float2(w[a], w[a]);
+#pragma unroll
+    for (int p = 0; p < 3; ++p) sum[p] = __fadd2_rn(sum[p], __fmul2_rn(weight, field(p, a)));
+  }
+  b[0] = sum[0].x; b[1] = sum[0].y; b[2] = sum[1].x;
+  e[0] = sum[1].y; e[1] = sum[2].x; e[2] = sum[2].y;
 }
 
 // The push of record n, whose valid interior cell (ci, cj, ck) was decoded
@@ -171,12 +206,10 @@ __device__ __forceinline__ int push(const Geom& g, const MoverParams<P>& mp, con
   using Vel = typename P::Vel;
   C wt[8];
   cic_weights<C>(C(fx), C(fy), C(fz), wt);
-  const C bx = gather8<C>(field, 0, 0, wt);
-  const C by = gather8<C>(field, 0, 1, wt);
-  const C bz = gather8<C>(field, 0, 2, wt);
-  const C ex = gather8<C>(field, 1, 0, wt);
-  const C ey = gather8<C>(field, 1, 1, wt);
-  const C ez = gather8<C>(field, 1, 2, wt);
+  C bf[3], ef[3];
+  gather_fields(field, wt, bf, ef);
+  const C bx = bf[0], by = bf[1], bz = bf[2];
+  const C ex = ef[0], ey = ef[1], ez = ef[2];
   const Response<C> rs(bx, by, bz, mp.beta_over_c);
   const C uu = C(r.u[n]), vv = C(r.v[n]), ww = C(r.w[n]);
   C hx, hy, hz, ax, ay, az;
@@ -320,7 +353,7 @@ __global__ void __launch_bounds__(kRunWarps * 32, 2 * TPICB200_MOVER_MIN_BLOCKS)
   using C = typename P::VC;
   using Pos = typename P::Pos;
   constexpr int kStaged = 2 * 3 * 2 * 2 * kRunNodes;
-  __shared__ C fields[kRunWarps][kStaged];
+  __shared__ __align__(8) C fields[kRunWarps][kStaged];
   __shared__ uint32_t starts[kRunWarps][kRunCells];
   __shared__ double scratch[kRunWarps];
   __shared__ double lane_sums[kRunWarps][5][32];
@@ -349,13 +382,31 @@ __global__ void __launch_bounds__(kRunWarps * 32, 2 * TPICB200_MOVER_MIN_BLOCKS)
     st[lane] = off;
     const uint32_t begin = __shfl_sync(0xffffffffu, off, 0);
     const uint32_t end = min(__shfl_sync(0xffffffffu, stop, len - 1), count);
-    // Stage the run's nodes: x in [i0, i0 + len], y in {j, j+1}, z in {k, k+1}.
+    // Stage the run's nodes: x in [i0, i0 + len], y in {j, j+1}, z in {k, k+1};
+    // in FP32 as component pairs (SharedPairFields).
     const int nodes_x = len + 1;
-    for (int t = lane; t < 24 * nodes_x; t += 32) {
-      const int x = t % nodes_x, rest = t / nodes_x;  // rest = ((which*3 + c)*2 + z)*2 + y
-      const int y = rest & 1, z = (rest >> 1) & 1, c = (rest >> 2) % 3, which = (rest >> 2) / 3;
-      const long long at = c * g.nodes + g.node(i0 + x, j + y, k + z);
-      sf[rest * kRunNodes + x] = which ? C(__ldg(theta + at)) : C(__ldg(bnode + at));
+    if constexpr (std::is_same_v<C, float>) {
+      float2* sp = reinterpret_cast<float2*>(sf);
+      for (int t = lane; t < 12 * nodes_x; t += 32) {
+        const int x = t % nodes_x, rest = t / nodes_x;  // rest = (pair*2 + z)*2 + y
+        const int y = rest & 1, z = (rest >> 1) & 1, pair = rest >> 2;
+        const long long at = g.node(i0 + x, j + y, k + z);
+        // Component q = 2 pair + h of (Bx, By, Bz, Ex, Ey, Ez).
+        float v[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int q = 2 * pair + h;
+          v[h] = q < 3 ? float(__ldg(bnode + q * g.nodes + at)) : float(__ldg(theta + (q - 3) * g.nodes + at));
+        }
+        sp[rest * kRunNodes + x] = make_float2(v[0], v[1]);
+      }
+    } else {
+      for (int t = lane; t < 24 * nodes_x; t += 32) {
+        const int x = t % nodes_x, rest = t / nodes_x;  // rest = ((which*3 + c)*2 + z)*2 + y
+        const int y = rest & 1, z = (rest >> 1) & 1, c = (rest >> 2) % 3, which = (rest >> 2) / 3;
+        const long long at = c * g.nodes + g.node(i0 + x, j + y, k + z);
+        sf[rest * kRunNodes + x] = which ? C(__ldg(theta + at)) : C(__ldg(bnode + at));
+      }
     }
     __syncwarp();
     const Records<P>& r = io.in;
@@ -382,9 +433,14 @@ __global__ void __launch_bounds__(kRunWarps * 32, 2 * TPICB200_MOVER_MIN_BLOCKS)
         // A record in its bin's cell needs no key decode.
         const bool home = k0 == g.encode(ci, cj, ck);
         if (home ? fields_ok<P>(charge, fx, fy, fz) : record_ok<P>(g, k0, charge, fx, fy, fz, ci, cj, ck)) {
-          if (home)
-            d = push<P, true>(g, mp, io, n, p, ci, cj, ck, fx, fy, fz, charge, SharedFields<C>{sf, c}, invalid,
-                              acc);
+          if (home) {
+            if constexpr (std::is_same_v<C, float>)
+              d = push<P, true>(g, mp, io, n, p, ci, cj, ck, fx, fy, fz, charge,
+                                SharedPairFields{reinterpret_cast<const float2*>(sf), c}, invalid, acc);
+            else
+              d = push<P, true>(g, mp, io, n, p, ci, cj, ck, fx, fy, fz, charge, SharedFields<C>{sf, c}, invalid,
+                                acc);
+          }
           else
             d = push<P, true>(g, mp, io, n, p, ci, cj, ck, fx, fy, fz, charge,
                               global_fields<P>(g, theta, bnode, ci, cj, ck), invalid, acc);
