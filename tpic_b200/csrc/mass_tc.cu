@@ -611,7 +611,8 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_deposit_kernel(Geom g, TcP
 // chunk parity) issues its MMAs, so no warp waits for the others.
 //
 // Records are fetched in a software pipeline per warp: the walk of chunk
-// j + 3 copies the ranks (cp.async), chunk j + 1's record loads are in
+// j + 3 copies the ranks (cp.async), chunk j + 2's records are requested
+// into L2 (when read through ranks), chunk j + 1's record loads are in
 // flight while chunk j is computed. A warp that has run out of batches keeps
 // arriving with no data while any warp of its CTA still has chunks (each
 // warp publishes, per chunk, whether it has another; the issuer publishes
@@ -841,8 +842,24 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
     else
       cbase = end;
   };
-  // The record index of a walked chunk (its rank copy has completed).
-  auto take_rank = [&](StreamLane& L, uint32_t chunk) { L.idx = sh.rank[warp][chunk & 3u][lane]; };
+  // The record index of a walked chunk (its rank copy has completed). Records
+  // read through ranks are gathered: they are requested into L2 one chunk
+  // before their loads are issued.
+  auto take_rank = [&](StreamLane& L, const StreamInfo& I, uint32_t chunk) {
+    L.idx = sh.rank[warp][chunk & 3u][lane];
+    auto prefetch = [&](const TcSpecies& sp) {
+      if (!sp.perm) return;
+      const uint32_t n = L.idx;
+      prefetch_l2(sp.rx + n); prefetch_l2(sp.ry + n); prefetch_l2(sp.rz + n); prefetch_l2(sp.q + n);
+      prefetch_l2(sp.u + n); prefetch_l2(sp.v + n); prefetch_l2(sp.w + n); prefetch_l2(sp.key + n);
+    };
+    if (L.flags & 1u) {
+      if ((I.bits >> 12) & 1u)
+        prefetch(tp.sp[1]);
+      else
+        prefetch(tp.sp[0]);
+    }
+  };
   // The record of a lane; the species is the chunk's (one branch per warp).
   auto load_rec = [&](const StreamLane& L, const StreamInfo& I) {
     StreamRec r{0.0, 0.0, 0.0, 0.0, 0.0f, 0.0f, 0.0f, -1, L.pos, L.flags};
@@ -932,7 +949,8 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
   };
 
   // Per-warp pipeline: chunk j + 3 walked (ranks copying), j + 2's ranks
-  // read, j + 1 loaded into registers, j computed.
+  // read (its records requested into L2), j + 1 loaded into registers, j
+  // computed.
   StreamLane la, lb, lc;
   StreamInfo ia, ib, ic;
   // One cp.async group per walked chunk (empty when no rank is copied).
@@ -943,9 +961,9 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
   walk(lc, ic, 2u);
   tc::cp_async_commit();
   tc::cp_async_wait_group<2>();
-  take_rank(la, 0u);
+  take_rank(la, ia, 0u);
   tc::cp_async_wait_group<1>();
-  take_rank(lb, 1u);
+  take_rank(lb, ib, 1u);
   StreamRec r1 = load_rec(la, ia);
   StreamInfo i1 = ia;
   StreamInfo ip{0, 0u};  // the previous chunk, whose cells are flushed next
@@ -961,7 +979,7 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
     walk(ld, id, j + 3u);
     tc::cp_async_commit();
     tc::cp_async_wait_group<1>();
-    take_rank(lc, j + 2u);
+    take_rank(lc, ic, j + 2u);
     lb = lc;
     ib = ic;
     lc = ld;
