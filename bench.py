@@ -730,6 +730,35 @@ def run_solve(args) -> None:
     sim.close()
 
 
+def run_peaks(args) -> None:
+    """Dense FP32 peaks the roofline of the FP32 CUDA-core and TF32 forms
+    divides by: cuBLAS SGEMM with TF32 off (FP32 SIMT FMA) and with TF32 on
+    (tensor cores), 8192^3, timed with CUDA events after warm-up. One JSON
+    line of TFLOP/s."""
+    import torch
+    torch.cuda.set_device(0)
+    n = 8192
+    a = torch.randn(n, n, device="cuda")
+    b = torch.randn(n, n, device="cuda")
+    out = {}
+    for name, tf32 in (("fp32_simt_tflops", False), ("tf32_tflops", True)):
+        torch.backends.cuda.matmul.allow_tf32 = tf32
+        for _ in range(3):
+            torch.matmul(a, b)
+        torch.cuda.synchronize()
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 10 if tf32 else 3
+        start.record()
+        for _ in range(reps):
+            torch.matmul(a, b)
+        stop.record()
+        torch.cuda.synchronize()
+        out[name] = 2.0 * n ** 3 * reps / (start.elapsed_time(stop) * 1e-3) / 1e12
+    torch.backends.cuda.matmul.allow_tf32 = False
+    print(json.dumps({"metric": "dense FP32 peaks", **out, "unit": "TFLOP/s", "size": n,
+                      "method": "cuBLAS SGEMM via torch.matmul, TF32 off and on"}))
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -765,6 +794,7 @@ def main():
     ap.add_argument("--e2e-cycles", type=int, default=20,
                     help="cycles of the end-to-end episode (upload, startup, cycles, energy readback)")
     ap.add_argument("--cpu-workers", type=int, default=0, help="host processes of the reference arm (0: all cores)")
+    ap.add_argument("--peaks", action="store_true", help="measure the FP32 SIMT and TF32 GEMM peaks (cuBLAS)")
     ap.add_argument("--solve", action="store_true",
                     help="time field solves alone on the workload's bootstrap state (ms per solve)")
     args = ap.parse_args()
@@ -776,6 +806,8 @@ def main():
         run_adjoint(args)
     elif args.solve:
         run_solve(args)
+    elif args.peaks:
+        run_peaks(args)
     else:
         run_gpu(args)
 
