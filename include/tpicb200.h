@@ -719,6 +719,57 @@ int tpicb200_checkpoint_info_read(const char* path, tpicb200_checkpoint_info* in
 int tpicb200_checkpoint_read(tpicb200_context* ctx, tpicb200_state* state, const char* path,
                              tpicb200_checkpoint_info* info, tpicb200_stream stream);
 
+/* ------------------------------------------------------------------------
+ * Snapshot output (TPIC's output channels, docs/user/output.md; the VTK
+ * engine of src/io/vtk_field_engine.cpp and src/io/vtk_particle_engine.cpp).
+ * ---------------------------------------------------------------------- */
+
+/* Output moments of one species (diagnostics/output_moment_deposition_device.hpp:30-107),
+ * FP64, ADDED into the caller's arrays at the nx*ny*nz unique nodes (x fastest, each
+ * component a separate array of that size, components outer): rho = 4 pi sum(q W)/V
+ * (the snapshot's rho), J = sum(q v W)/V (3 components) and the raw second moment
+ * P_ij = sum((q/qom) v_i v_j W)/V (6 components: xx, xy, xz, yy, yz, zz). Any of the
+ * three may be NULL. V is the cell volume, the dual volume of every node of a
+ * periodic grid. Records with an invalid key, a fraction outside [0, 1) or a
+ * nonfinite amount add nothing and raise the context's invalid counter. */
+int tpicb200_output_moments(tpicb200_context* ctx, double qom, const tpicb200_particles* p, double* rho, double* j,
+                            double* pressure, tpicb200_stream stream);
+
+/* A species' records in output form on the device: position = (cell + fraction)
+ * * spacing (3 per record, interleaved), velocity widened to FP64 (3 per record),
+ * charge. A record with an invalid key, a fraction outside [0, 1) or a nonfinite
+ * velocity or charge raises the context's invalid counter (TPIC refuses to
+ * write such a snapshot). */
+int tpicb200_output_particles(tpicb200_context* ctx, const tpicb200_particles* p, double* position, double* velocity,
+                              double* charge, tpicb200_stream stream);
+
+/* Writes one Float64 field array as VTK XML ImageData (host only): `values` holds
+ * the (nx+1)(ny+1)(nz+1) nodes of the grid, end nodes included, x fastest, the
+ * `components` values of a node interleaved. FieldData: TimeValue = time, cycle,
+ * final_state and the strings state ("final" or "pre_solve"), precision_profile
+ * and precision_roles. overwrite = 0 refuses an existing file
+ * (TPICB200_BACKEND_FAILURE with the path in tpicb200_last_error()). The file name
+ * is the caller's; TPIC names it <array>_tNNNNNN.vti. */
+int tpicb200_vtk_write_field(const char* path, const char* name, int components, const tpicb200_grid* grid,
+                             const double* values, int cycle, double time, int final_state, const char* profile,
+                             const char* roles, int overwrite);
+
+typedef struct {
+  uint64_t count;
+  const double* position;  /* 3 * count, global coordinates */
+  const double* velocity;  /* 3 * count */
+  const double* charge;    /* count */
+  const uint64_t* id;      /* count */
+  uint64_t species;        /* species index written for every record */
+} tpicb200_vtk_species;
+
+/* Writes a particle snapshot under `directory` (host only): the PolyData piece
+ * particles_tNNNNNN_r000000.vtp (the species one after another: point data
+ * velocity, charge, id, species; points = positions; one vertex per point) and
+ * its PPolyData manifest particles_tNNNNNN.pvtp. */
+int tpicb200_vtk_write_particles(const char* directory, int cycle, double time, int final_state, const char* profile,
+                                 const char* roles, int ns, const tpicb200_vtk_species* species, int overwrite);
+
 #ifdef __cplusplus
 }
 #endif

@@ -398,3 +398,37 @@ def case_species_arrays(case, precision: int, generate) -> list:
 
 __all__ = ["OracleCycle", "OracleAdjoint", "load", "load_reference", "build", "total_energy", "case_species_arrays", "OGrid", "ptr",
            "math"]
+
+
+def output_moments(grid, d: dict, qom: float, precision: int = 0):
+    """Output moments of one species at the nx*ny*nz unique nodes (FP64),
+    restating deposit_output_moments_kernel
+    (diagnostics/output_moment_deposition_device.hpp:30-107) with the
+    shared-node sum of a periodic grid: per record the amounts q/V, q/V v and
+    (q/V)(1/qom) v_i v_j times the CIC weights of its cell corners
+    ((wx*wy)*wz, ecsim/particles/cic.hpp:24-36). Returns (4 pi rho, J[3],
+    P[6] as xx, xy, xz, yy, yz, zz), each (components, nz, ny, nx)."""
+    g = grid
+    vol = (g.lx / g.nx) * (g.ly / g.ny) * (g.lz / g.nz)
+    ex, ey = g.nx + 4, g.ny + 4
+    key = d["cell"].astype(np.int64)
+    ci, cj, ck = key % ex - 2, (key // ex) % ey - 2, key // (ex * ey) - 2
+    fx, fy, fz = (np.asarray(d[k], dtype=np.float64) for k in ("rx", "ry", "rz"))
+    u, v, w = (np.asarray(d[k]).astype(np.float64) for k in ("u", "v", "w"))
+    charge = np.asarray(d["q"], dtype=np.float64) * (1.0 / vol)
+    mass = charge * (1.0 / qom)
+    amounts = [charge * (4.0 * np.pi)] + [charge * u, charge * v, charge * w] + \
+              [mass * u * u, mass * u * v, mass * u * w, mass * v * v, mass * v * w, mass * w * w]
+    out = np.zeros((10, g.nz, g.ny, g.nx))
+    cx, cy, cz = 1.0 - fx, 1.0 - fy, 1.0 - fz
+    for a in range(8):
+        wx = fx if a & 1 else cx
+        wy = fy if a & 2 else cy
+        wz = fz if a & 4 else cz
+        wt = (wx * wy) * wz
+        i = (ci + (a & 1)) % g.nx
+        j = (cj + ((a >> 1) & 1)) % g.ny
+        k = (ck + ((a >> 2) & 1)) % g.nz
+        for c in range(10):
+            np.add.at(out[c], (k, j, i), amounts[c] * wt)
+    return out[0:1], out[1:4], out[4:10]

@@ -59,12 +59,13 @@ def periodic_distance(a, b, extents):
     return np.abs(d).max()
 
 
-def measure(form: str, cycles: int = 3) -> dict:
+def measure(form: str, cycles: int = 3, smoothing=(0, 1.0, 0), mass_layout="stencil-major") -> dict:
     from test_gpu_cycle import c1_case
     from tpic_b200.simulation import Simulation
     case = c1_case(n=16)
     g = case.grid
-    sim = Simulation(case, precision="mixed", mass_kind=form, mass_layout="stencil-major", keep_ids=True)
+    sim = Simulation(case, precision="mixed", mass_kind=form, mass_layout=mass_layout, keep_ids=True,
+                     smoothing=smoothing)
     sim.prepare()
     sim.run(cycles)
     arrays = []
@@ -73,7 +74,8 @@ def measure(form: str, cycles: int = 3) -> dict:
         for k in ("u", "v", "w"):
             d[k] = d[k].astype(np.float64)  # the mixed run's initial velocities, exactly
         arrays.append((sp.qom, d))
-    oc = O.OracleCycle(g, arrays, case.dt, case.theta, case.c, case.gmres_tol, 0, b0=case.fields.b0)
+    oc = O.OracleCycle(g, arrays, case.dt, case.theta, case.c, case.gmres_tol, 0, b0=case.fields.b0,
+                       smoothing=smoothing)
     oc.prepare()
     for _ in range(cycles):
         oc.cycle()
@@ -114,3 +116,19 @@ def test_mixed_cycles_against_fp64_oracle(form):
     assert err["b_rel"] <= bb, err
     assert err["position_cells"] <= bx, err
     assert err["velocity_rel_vth"] <= bv, err
+
+
+@pytest.mark.parametrize("form,op", [("bf16x3", 0), ("bf16x3", 1), ("tf32", 0)])
+def test_smoothed_mixed_cycles_against_fp64_oracle(form, op):
+    """Energy-conserving smoothing (two passes, Face7 alpha 0.5 or Binomial27)
+    in the mixed-precision cycle with a tensor-core form and the tiled mass
+    layout: the smoothed particle field reaches the run mover's staged
+    nodes and the smoothed current the right-hand side. Against the
+    smoothed FP64 oracle, within twice the unsmoothed form's bounds."""
+    err = measure(form, smoothing=(2, 0.5, op), mass_layout="tiled")
+    be, bb, bx, bv = (2 * b for b in BOUNDS[form])
+    assert err["e_rel"] <= be, err
+    assert err["b_rel"] <= bb, err
+    assert err["position_cells"] <= bx, err
+    assert err["velocity_rel_vth"] <= bv, err
+

@@ -113,6 +113,12 @@ class CheckpointInfo(C.Structure):
                 ("count", C.c_uint32 * MAX_SPECIES), ("has_id", C.c_int * MAX_SPECIES)]
 
 
+
+class VtkSpecies(C.Structure):
+    _fields_ = [("count", C.c_uint64), ("position", C.c_void_p), ("velocity", C.c_void_p), ("charge", C.c_void_p),
+                ("id", C.c_void_p), ("species", C.c_uint64)]
+
+
 EXPORTS = {
     "tpicb200_version": (C.c_char_p, []),
     "tpicb200_last_error": (C.c_char_p, []),
@@ -180,6 +186,14 @@ EXPORTS = {
     "tpicb200_checkpoint_info_read": (C.c_int, [C.c_char_p, C.POINTER(CheckpointInfo)]),
     "tpicb200_checkpoint_read": (C.c_int, [C.c_void_p, C.POINTER(State), C.c_char_p, C.POINTER(CheckpointInfo),
                                            C.c_void_p]),
+    "tpicb200_output_moments": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(Particles), C.c_void_p, C.c_void_p,
+                                          C.c_void_p, C.c_void_p]),
+    "tpicb200_output_particles": (C.c_int, [C.c_void_p, C.POINTER(Particles), C.c_void_p, C.c_void_p, C.c_void_p,
+                                            C.c_void_p]),
+    "tpicb200_vtk_write_field": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.POINTER(Grid), C.c_void_p, C.c_int,
+                                           C.c_double, C.c_int, C.c_char_p, C.c_char_p, C.c_int]),
+    "tpicb200_vtk_write_particles": (C.c_int, [C.c_char_p, C.c_int, C.c_double, C.c_int, C.c_char_p, C.c_char_p,
+                                               C.c_int, C.POINTER(VtkSpecies), C.c_int]),
 }
 
 _lib = None

@@ -740,6 +740,7 @@ namespace tpicb200 {
 const Geom& context_geom(const tpicb200_context* ctx) { return ctx->g; }
 const tpicb200_options& context_options(const tpicb200_context* ctx) { return ctx->opt; }
 const tpicb200_grid& context_grid(const tpicb200_context* ctx) { return ctx->grid; }
+uint32_t* context_invalid(tpicb200_context* ctx) { return ctx->invalid; }
 int context_check_state(tpicb200_context* ctx, tpicb200_state* st) {
   if (int s = check_ctx(ctx)) return s;
   return check_state(ctx, st);

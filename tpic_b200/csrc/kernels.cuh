@@ -23,6 +23,7 @@ const Geom& context_geom(const tpicb200_context* ctx);
 const tpicb200_options& context_options(const tpicb200_context* ctx);
 const tpicb200_grid& context_grid(const tpicb200_context* ctx);
 int context_check_state(tpicb200_context* ctx, tpicb200_state* st);
+uint32_t* context_invalid(tpicb200_context* ctx);
 
 // mover.cu
 struct BinnedScratch;

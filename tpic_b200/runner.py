@@ -84,12 +84,20 @@ def parse_args(argv=None):
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--gmres-max-iterations", type=int, default=100)
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--field-output-cycle", type=int, default=None,
+                    help="FieldOutputCycle (default: the deck's, else 100; <= 0: no field snapshots)")
+    ap.add_argument("--particles-output-cycle", type=int, default=None,
+                    help="ParticlesOutputCycle (default: the deck's, else 0: no particle snapshots)")
+    ap.add_argument("--save-dir", default=None, help="SaveDirName of the snapshots, under --output (default: the "
+                                                     "deck's, else data)")
     return ap.parse_args(argv)
 
 
 def run(args) -> int:
     from .simulation import Simulation
-    deck = D.load(args.run)
+    from .output import OutputPlan, write_fields, write_particles
+    text = Path(args.run).read_text()
+    deck = D.parse(text)
     case = D.to_case(deck, seed=args.seed)
     last = deck.ncycles if args.cycles is None else args.cycles
     form = resolve_form(args.mass_matrix, args.precision)
@@ -97,8 +105,12 @@ def run(args) -> int:
     out.mkdir(parents=True, exist_ok=True)
     ckpt_dir = out / args.restart_dir
     csv_path = out / "diagnostics.csv"
+    plan = OutputPlan.from_deck(text, out, field_cycle=args.field_output_cycle,
+                                particles_cycle=args.particles_output_cycle)
+    if args.save_dir is not None:
+        plan.save_dir = out / args.save_dir
     kw = dict(precision=args.precision, mass_kind=form, device=args.device,
-              gmres_max_iterations=args.gmres_max_iterations)
+              gmres_max_iterations=args.gmres_max_iterations, keep_ids=plan.particles_cycle > 0)
     ns = len(case.species)
     if args.restart:
         sim = Simulation.restart(case, ckpt_dir, **kw)
@@ -137,14 +149,26 @@ def run(args) -> int:
         total = field[0] + field[1] + sum(sp[0] for sp in species)
         print(f"cycle {sim.cycle:6d}  total energy {total:.10e}  change {total - initial:+.3e}", flush=True)
 
+    def snapshots() -> None:
+        final = sim.cycle == last
+        fields_due, particles_due = plan.due(sim.cycle, final)
+        if fields_due:
+            write_fields(sim, plan, sim.cycle, final)
+        if particles_due:
+            write_particles(sim, plan, sim.cycle, final)
+
     if (cadence and sim.cycle % cadence == 0) or sim.cycle == last:
         record(sim.cycle == last)
+    snapshots()
     while sim.cycle < last:
         stops = [last]
         if cadence:
             stops.append((sim.cycle // cadence + 1) * cadence)
         if ckpt:
             stops.append((sim.cycle // ckpt + 1) * ckpt)
+        for channel in (plan.field_cycle, plan.particles_cycle):
+            if channel > 0:
+                stops.append((sim.cycle // channel + 1) * channel)
         n = min(stops) - sim.cycle
         reports = sim.run(n)
         r = reports[-1]
@@ -153,6 +177,7 @@ def run(args) -> int:
             sim.checkpoint(ckpt_dir)
         if sim.cycle == last or (cadence and sim.cycle % cadence == 0):
             record(sim.cycle == last)
+        snapshots()
         if not all(math.isfinite(x) for x in field):
             raise SystemExit("nonfinite field energy")
     sim.close()
