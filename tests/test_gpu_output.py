@@ -65,7 +65,7 @@ def test_runner_writes_snapshots(torch_cuda, tmp_path):
     """A shrunk two-stream deck for 2 cycles with fields every cycle and
     particles every 2: E, B, rho and J files at cycles 0, 1, 2 and particle
     snapshots at 0 and 2; the final E file equals the run's E, the particle
-    file holds every record once with the deck's charge."""
+    file holds every record once."""
     import torch
     from tpic_b200 import deck as D
     from tpic_b200.runner import main
@@ -102,7 +102,8 @@ def test_runner_writes_snapshots(torch_cuda, tmp_path):
     root, parr, _ = read(data / "particles_t000002_r000000.vtp")
     count = sum(case.grid.cells * sp.ppc for sp in case.species)
     assert int(root.find("PolyData/Piece").get("NumberOfPoints")) == count
-    assert len(np.unique(parr["id"])) == count
+    # Ids count within a species: (species, id) names a record.
+    assert len(np.unique(parr["species"].astype(np.uint64) * np.uint64(1 << 40) + parr["id"])) == count
     lo = np.zeros(3)
     hi = np.array([g.lx, g.ly, g.lz])
     assert np.all(parr["position"] >= lo) and np.all(parr["position"] < hi)

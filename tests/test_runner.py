@@ -46,7 +46,10 @@ def test_deck_run_with_checkpoints_and_restart(tmp_path):
     assert [r[2] for r in rows] == ["pre_solve"] * 4 + ["final"]
     assert float(rows[0][7]) == 0.0
     assert abs(float(rows[-1][7])) <= 1e-5 * float(rows[0][6])
-    assert sorted(p.name for p in (out / "data").iterdir()) == ["checkpoint_t000004_n000001"]
+    names = sorted(p.name for p in (out / "data").iterdir())
+    assert [n for n in names if n.startswith("checkpoint")] == ["checkpoint_t000004_n000001"]
+    # Field snapshots (FieldOutputCycle defaults to 100): the first and the final state.
+    assert "E_t000000.vti" in names and "E_t000004.vti" in names and "B_t000004.vti" in names
     # Continue to cycle 6 from the checkpoint of cycle 4.
     assert runner.main(["--run", str(deck), "--output", str(out), "--restart", "--cycles", "6"]) == 0
     text = (out / "diagnostics.csv").read_text()
