@@ -1302,7 +1302,7 @@ __global__ void __launch_bounds__(128) assemble_moments_kernel(Geom g, const T* 
                                                                int overwrite) {
   const int nx = g.nx, ny = g.ny;
   const long long unique = (long long)nx * ny * g.nz;
-  // The stencil is the fast block index (see assemble_quads_kernel).
+  // The stencil is the fast block index (see assemble_warp_quads_kernel).
   const int stencil = int(blockIdx.x % 15);
   const long long v = (blockIdx.x / 15) * (long long)blockDim.x + threadIdx.x;
   if (v >= unique) return;
@@ -1353,87 +1353,116 @@ __device__ __forceinline__ void load_quad(const double* p, double (&v)[4]) {
   v[0] = x.x; v[1] = x.y; v[2] = y.x; v[3] = y.y;
 }
 
+// The moment assembly when nx is a multiple of 4: a warp takes eight consecutive
+// quads (32 nodes) of one node row and one stencil; lane l works on quad
+// l / 4 and on the entries e = l % 4, l % 4 + 4 (and 8 for l % 4 = 0), so
+// the four lanes of a quad read four consecutive 16-byte moment words and a
+// warp's load touches eight 64-byte runs instead of 32 scattered words.
+// Every (node, entry) sum adds the pairs' moments in increasing corner
+// order, the quad's lower neighbour group supplying the corner-1 cells of
+// its first node. The sums are staged in
+// shared memory and stored by node (32 consecutive nodes per entry).
 template <class T, int S>
-__device__ __forceinline__ void assemble_quad(const Geom& g, int m, int j, int k, const T* __restrict__ mom,
-                                              T* __restrict__ J, T* __restrict__ M, int overwrite) {
+__device__ __forceinline__ void assemble_warp_quads(const Geom& g, int m0, int j, int k, const T* __restrict__ mom,
+                                                    T* __restrict__ J, T* __restrict__ M, int overwrite,
+                                                    T (*stage)[32]) {
   constexpr StencilPairs pairs = make_stencil_pairs();
-  constexpr int kSums = S < 14 ? 9 : 3;
+  constexpr int kEntries = S < 14 ? 9 : 3;
+  const int lane = threadIdx.x & 31, sub = lane & 3;
   const int ny = g.ny, nz = g.nz, qx = g.nx >> 2;
+  const int m = m0 + (lane >> 2);
+  const bool live = m < qx;
   const int j1 = j > 0 ? j - 1 : ny - 1, k1 = k > 0 ? k - 1 : nz - 1;
   const int mp = m > 0 ? m - 1 : qx - 1;
-  T sum[kSums][4];
+  T sum[3][4];
 #pragma unroll
-  for (int e = 0; e < kSums; ++e)
+  for (int r = 0; r < 3; ++r)
 #pragma unroll
-    for (int n = 0; n < 4; ++n) sum[e][n] = T(0);
+    for (int n = 0; n < 4; ++n) sum[r][n] = T(0);
+  if (live) {
 #pragma unroll
-  for (int a = 0; a < 8; ++a) {
-    const long long row = (long long)((a & 2) ? j1 : j) + (long long)ny * ((a & 4) ? k1 : k);
-    const long long own = row * qx + m, prev = row * qx + mp;
-    auto add = [&](int q, int e) {
-      T v[4];
-      load_quad(mom + (own * kMoments + q) * 4, v);
-      if (a & 1) {
-        const T p3 = __ldg(mom + (prev * kMoments + q) * 4 + 3);
-        sum[e][0] += p3; sum[e][1] += v[0]; sum[e][2] += v[1]; sum[e][3] += v[2];
-      } else {
-        sum[e][0] += v[0]; sum[e][1] += v[1]; sum[e][2] += v[2]; sum[e][3] += v[3];
+    for (int a = 0; a < 8; ++a) {
+      const long long row = (long long)((a & 2) ? j1 : j) + (long long)ny * ((a & 4) ? k1 : k);
+      const long long own = row * qx + m, prev = row * qx + mp;
+      auto add = [&](int q, int r) {
+        T v[4];
+        load_quad(mom + (own * kMoments + q) * 4, v);
+        if (a & 1) {
+          const T p3 = __ldg(mom + (prev * kMoments + q) * 4 + 3);
+          sum[r][0] += p3; sum[r][1] += v[0]; sum[r][2] += v[1]; sum[r][3] += v[2];
+        } else {
+          sum[r][0] += v[0]; sum[r][1] += v[1]; sum[r][2] += v[2]; sum[r][3] += v[3];
+        }
+      };
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        const int e = sub + 4 * r;
+        if (e >= kEntries) continue;
+        if constexpr (S < 14) {
+#pragma unroll
+          for (int pp = 0; pp < 8; ++pp)
+            if (pp < pairs.count[S] && pairs.corner[S][pp] == a) add(pairs.monomial[S][pp] * 9 + e, r);
+        } else {
+          add(kMassMoments + a * 3 + e, r);
+        }
       }
-    };
-    if constexpr (S < 14) {
-#pragma unroll
-      for (int p = 0; p < 8; ++p)
-        if (p < pairs.count[S] && pairs.corner[S][p] == a)
-#pragma unroll
-          for (int e = 0; e < 9; ++e) add(pairs.monomial[S][p] * 9 + e, e);
-    } else {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) add(kMassMoments + a * 3 + c, c);
     }
   }
 #pragma unroll
-  for (int n = 0; n < 4; ++n) {
-    const long long node = g.node(4 * m + n, j, k);
+  for (int r = 0; r < 3; ++r) {
+    const int e = sub + 4 * r;
+    if (e < kEntries)
 #pragma unroll
-    for (int e = 0; e < kSums; ++e) {
-      T* dst = S < 14 ? M + g.mass_index(g.mass_vertex(4 * m + n, j, k), S * 9 + e) : J + e * g.nodes + node;
-      *dst = overwrite ? sum[e][n] : *dst + sum[e][n];
+      for (int n = 0; n < 4; ++n) stage[e][4 * (lane >> 2) + n] = sum[r][n];
+  }
+  __syncwarp();
+  const int i = 4 * m0 + lane;
+  if (i < g.nx) {
+    const long long node = g.node(i, j, k);
+#pragma unroll
+    for (int e = 0; e < kEntries; ++e) {
+      T* dst = S < 14 ? M + g.mass_index(g.mass_vertex(i, j, k), S * 9 + e) : J + e * g.nodes + node;
+      *dst = overwrite ? stage[e][lane] : *dst + stage[e][lane];
     }
   }
 }
 
 template <class T>
-__global__ void __launch_bounds__(128) assemble_quads_kernel(Geom g, const T* __restrict__ mom,
-                                                             T* __restrict__ J, T* __restrict__ M,
-                                                             int overwrite) {
-  const int qx = g.nx >> 2, ny = g.ny;
-  const long long quads = (long long)qx * ny * g.nz;
+__global__ void __launch_bounds__(128) assemble_warp_quads_kernel(Geom g, const T* __restrict__ mom,
+                                                                  T* __restrict__ J, T* __restrict__ M,
+                                                                  int overwrite) {
+  __shared__ T stage[4][9][32];
+  const int warp = threadIdx.x >> 5;
+  const int qx = g.nx >> 2, tiles = (qx + 7) / 8;
+  const long long rows = (long long)g.ny * g.nz;
   // The stencil is the fast block index, so that the 15 blocks of the same
   // nodes run together and share the cell moments in L2.
   const int stencil = int(blockIdx.x % 15);
-  const long long v = (blockIdx.x / 15) * (long long)blockDim.x + threadIdx.x;
-  if (v >= quads) return;
-  const int m = int(v % qx);
-  const long long r = v / qx;
-  const int j = int(r % ny), k = int(r / ny);
+  const long long t = (blockIdx.x / 15) * 4LL + warp;
+  if (t >= rows * tiles) return;
+  const long long row = t / tiles;
+  const int m0 = int(t - row * tiles) * 8;
+  const int j = int(row % g.ny), k = int(row / g.ny);
+  T (*st)[32] = stage[warp];
   switch (stencil) {
-    case 0: assemble_quad<T, 0>(g, m, j, k, mom, J, M, overwrite); break;
-    case 1: assemble_quad<T, 1>(g, m, j, k, mom, J, M, overwrite); break;
-    case 2: assemble_quad<T, 2>(g, m, j, k, mom, J, M, overwrite); break;
-    case 3: assemble_quad<T, 3>(g, m, j, k, mom, J, M, overwrite); break;
-    case 4: assemble_quad<T, 4>(g, m, j, k, mom, J, M, overwrite); break;
-    case 5: assemble_quad<T, 5>(g, m, j, k, mom, J, M, overwrite); break;
-    case 6: assemble_quad<T, 6>(g, m, j, k, mom, J, M, overwrite); break;
-    case 7: assemble_quad<T, 7>(g, m, j, k, mom, J, M, overwrite); break;
-    case 8: assemble_quad<T, 8>(g, m, j, k, mom, J, M, overwrite); break;
-    case 9: assemble_quad<T, 9>(g, m, j, k, mom, J, M, overwrite); break;
-    case 10: assemble_quad<T, 10>(g, m, j, k, mom, J, M, overwrite); break;
-    case 11: assemble_quad<T, 11>(g, m, j, k, mom, J, M, overwrite); break;
-    case 12: assemble_quad<T, 12>(g, m, j, k, mom, J, M, overwrite); break;
-    case 13: assemble_quad<T, 13>(g, m, j, k, mom, J, M, overwrite); break;
-    default: assemble_quad<T, 14>(g, m, j, k, mom, J, M, overwrite); break;
+    case 0: assemble_warp_quads<T, 0>(g, m0, j, k, mom, J, M, overwrite, st); break;
+    case 1: assemble_warp_quads<T, 1>(g, m0, j, k, mom, J, M, overwrite, st); break;
+    case 2: assemble_warp_quads<T, 2>(g, m0, j, k, mom, J, M, overwrite, st); break;
+    case 3: assemble_warp_quads<T, 3>(g, m0, j, k, mom, J, M, overwrite, st); break;
+    case 4: assemble_warp_quads<T, 4>(g, m0, j, k, mom, J, M, overwrite, st); break;
+    case 5: assemble_warp_quads<T, 5>(g, m0, j, k, mom, J, M, overwrite, st); break;
+    case 6: assemble_warp_quads<T, 6>(g, m0, j, k, mom, J, M, overwrite, st); break;
+    case 7: assemble_warp_quads<T, 7>(g, m0, j, k, mom, J, M, overwrite, st); break;
+    case 8: assemble_warp_quads<T, 8>(g, m0, j, k, mom, J, M, overwrite, st); break;
+    case 9: assemble_warp_quads<T, 9>(g, m0, j, k, mom, J, M, overwrite, st); break;
+    case 10: assemble_warp_quads<T, 10>(g, m0, j, k, mom, J, M, overwrite, st); break;
+    case 11: assemble_warp_quads<T, 11>(g, m0, j, k, mom, J, M, overwrite, st); break;
+    case 12: assemble_warp_quads<T, 12>(g, m0, j, k, mom, J, M, overwrite, st); break;
+    case 13: assemble_warp_quads<T, 13>(g, m0, j, k, mom, J, M, overwrite, st); break;
+    default: assemble_warp_quads<T, 14>(g, m0, j, k, mom, J, M, overwrite, st); break;
   }
 }
+
 
 
 // ---------------------------------------------------------------------------
@@ -1628,19 +1657,22 @@ __global__ void __launch_bounds__(kF64Warps * 32) moments_f64_kernel(Geom g, F64
 cudaError_t launch_assemble_moments(int precision, const Geom& g, const void* moments, void* j, void* mass,
                                     int overwrite, cudaStream_t s) {
   const long long unique = (long long)g.nx * g.ny * g.nz;
-  const long long items = g.nx % 4 == 0 ? unique / 4 : unique;
+  // nx a multiple of 4: warps of eight quads (4 warps a block); otherwise one
+  // node per thread.
+  const long long warp_tiles = (long long)g.ny * g.nz * (((g.nx >> 2) + 7) / 8);
+  const long long items = g.nx % 4 == 0 ? warp_tiles * 32 : unique;
   const long long blocks = (items + 127) / 128 * 15;
   if (blocks > 0x7FFFFFFFLL) return cudaErrorInvalidValue;
   if (precision == TPICB200_PRECISION_DOUBLE) {
     if (g.nx % 4 == 0)
-      assemble_quads_kernel<double><<<unsigned(blocks), 128, 0, s>>>(g, (const double*)moments, (double*)j,
-                                                                    (double*)mass, overwrite);
+      assemble_warp_quads_kernel<double><<<unsigned(blocks), 128, 0, s>>>(g, (const double*)moments, (double*)j,
+                                                                         (double*)mass, overwrite);
     else
       assemble_moments_kernel<double><<<unsigned(blocks), 128, 0, s>>>(g, (const double*)moments, (double*)j,
                                                                       (double*)mass, overwrite);
   } else if (g.nx % 4 == 0) {
-    assemble_quads_kernel<float><<<unsigned(blocks), 128, 0, s>>>(g, (const float*)moments, (float*)j,
-                                                                 (float*)mass, overwrite);
+    assemble_warp_quads_kernel<float><<<unsigned(blocks), 128, 0, s>>>(g, (const float*)moments, (float*)j,
+                                                                      (float*)mass, overwrite);
   } else {
     assemble_moments_kernel<float><<<unsigned(blocks), 128, 0, s>>>(g, (const float*)moments, (float*)j,
                                                                    (float*)mass, overwrite);
