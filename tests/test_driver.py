@@ -37,3 +37,54 @@ def test_bad_command_lines(driver, tmp_path):
     bad.write_text("Case = Whistler\n")
     done = subprocess.run([driver, "--run", str(bad), "--dry-run"], capture_output=True, text=True, timeout=60)
     assert done.returncode == 1 and "deck" in done.stderr
+
+
+TAGS = [("", ""), ("B", ""), ("", "rho+rho0"), ("E", "J_tot+PXX1+PZZ+rho5"), ("E+B", "PXY+PXY_tot+J1+J0"),
+        ("", "rho007")]
+
+
+@pytest.mark.parametrize("field_tag,moments_tag", TAGS)
+def test_snapshot_selection_matches_the_runner(driver, tmp_path, field_tag, moments_tag):
+    """The driver's reading of FieldOutputTag / MomentsOutputTag (printed by
+    --dry-run) selects the runner's arrays in the runner's order."""
+    from tpic_b200.output import select_arrays
+    deck = tmp_path / "tagged.inp"
+    keys = "FieldOutputCycle = 5\nParticlesOutputCycle = 3\nSaveDirName = snaps # comment\n"
+    if field_tag:
+        keys += f"FieldOutputTag = {field_tag}\n"
+    if moments_tag:
+        keys += f"MomentsOutputTag = {moments_tag}\n"
+    deck.write_text(DECKS[0].read_text() + keys)
+    done = subprocess.run([driver, "--run", str(deck), "--dry-run", "--output", str(tmp_path)], capture_output=True,
+                          text=True, timeout=60)
+    assert done.returncode == 0, done.stderr
+    line = [x for x in done.stdout.splitlines() if x.startswith("snapshots under")][0]
+    ns = int(done.stdout.split(" species")[0].rsplit(" ", 1)[1])
+    fields, moments = select_arrays(field_tag, moments_tag, ns)
+    listed = line.split("(", 1)[1].split(")", 1)[0].split()
+    assert listed == fields + [m[0] for m in moments]
+    assert f"under {tmp_path}/snaps:" in line and "fields every 5 cycles" in line
+    assert line.endswith("particles every 3 cycles")
+    over = subprocess.run([driver, "--run", str(deck), "--dry-run", "--field-output-cycle", "0",
+                           "--particles-output-cycle", "7", "--save-dir", "x"], capture_output=True, text=True,
+                          timeout=60)
+    assert over.returncode == 0, over.stderr
+    assert "under ./x:" in over.stdout and "fields every 0 cycles" in over.stdout
+    assert "particles every 7 cycles" in over.stdout
+
+
+@pytest.mark.parametrize("keys", ["FieldOutputTag = EB\n", "FieldOutputTag = B+\n", "FieldOutputTag = Gauss\n",
+                                  "MomentsOutputTag = rhoJ\n", "MomentsOutputTag = rho-1\n",
+                                  "MomentsOutputTag = PXX_totally\n", "MomentsOutputTag = rho++J\n",
+                                  "MomentsOutputTag = rho2147483648\n", "WriteMethod = hdf5\n",
+                                  "FieldWriteMethod = csv\n"])
+def test_bad_snapshot_keys(driver, tmp_path, keys):
+    deck = tmp_path / "bad.inp"
+    deck.write_text(DECKS[0].read_text() + keys)
+    done = subprocess.run([driver, "--run", str(deck), "--dry-run"], capture_output=True, text=True, timeout=60)
+    assert done.returncode == 1, (keys, done.stdout, done.stderr)
+    assert "Tag" in done.stderr or "Method" in done.stderr
+    ok = tmp_path / "off.inp"
+    ok.write_text(DECKS[0].read_text() + "WriteMethod = hdf5\nFieldOutputCycle = 0\n")
+    done = subprocess.run([driver, "--run", str(ok), "--dry-run"], capture_output=True, text=True, timeout=60)
+    assert done.returncode == 0, done.stderr

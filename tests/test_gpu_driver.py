@@ -62,3 +62,43 @@ def test_driver_restart_continues_the_run(tmp_path):
     other = np.arange(7) != 4
     assert np.array_equal(a[other], b[other])
     assert np.allclose(a[4], b[4], rtol=1e-12, atol=1e-300)
+
+
+def test_driver_snapshots_match_the_python_runner(tmp_path):
+    """Field snapshots every cycle and particle snapshots every 2 cycles of the
+    shrunk C1 deck, written by the driver and by the runner: the same files;
+    E, B and the records (matched by species and id) bit for bit, the
+    moments (device atomics, any summation order) to rounding."""
+    from vtkread import field_data, read
+    B.build()
+    a, b = tmp_path / "cpp", tmp_path / "py"
+    args = ["--run", str(C1), "--cycles", "3", "--field-output-cycle", "1", "--particles-output-cycle", "2"]
+    driver(*args, "--output", str(a), cwd=tmp_path)
+    done = subprocess.run([sys.executable, "-m", "tpic_b200", *args, "--output", str(b)], capture_output=True,
+                          text=True, timeout=600, cwd=ROOT)
+    assert done.returncode == 0, done.stdout + done.stderr
+    names = sorted(p.name for p in (a / "data").iterdir())
+    assert names == sorted(p.name for p in (b / "data").iterdir())
+    for cycle in (0, 1, 2, 3):
+        assert f"rho_1_t{cycle:06d}.vti" in names
+    assert "particles_t000002.pvtp" in names and "particles_t000003_r000000.vtp" in names
+    assert "particles_t000001.pvtp" not in names
+    for name in names:
+        if name.endswith(".pvtp"):
+            assert (a / "data" / name).read_bytes() == (b / "data" / name).read_bytes()
+            continue
+        ra, xa, _ = read(a / "data" / name)
+        rb, xb, _ = read(b / "data" / name)
+        assert field_data(ra) == field_data(rb), name
+        if name.endswith(".vtp"):
+            order = [np.lexsort((x["id"], x["species"])) for x in (xa, xb)]
+            for key in ("position", "velocity", "charge", "id", "species"):
+                assert np.array_equal(xa[key][order[0]], xb[key][order[1]]), (name, key)
+            assert np.array_equal(xa["connectivity"], xb["connectivity"])
+            continue
+        (key,) = xa.keys()
+        if key in ("E", "B"):
+            assert np.array_equal(xa[key], xb[key]), name
+        else:
+            scale = max(np.abs(xb[key]).max(), 1e-300)
+            assert np.abs(xa[key] - xb[key]).max() <= 1e-12 * scale, name

@@ -3,7 +3,8 @@
 //   tpicb200_run --run deck.inp [--mass-matrix matrix-core|scalar|scalar-f64|tf32|bf16x3|moments-f64]
 //                [--precision mixed|double] [--restart] [--output DIR] [--cycles N]
 //                [--diagnostics-cycle K] [--restart-cycle R] [--restart-dir NAME] [--seed S]
-//                [--gmres-max-iterations M] [--device D] [--dry-run]
+//                [--gmres-max-iterations M] [--device D] [--field-output-cycle F]
+//                [--particles-output-cycle P] [--save-dir NAME] [--dry-run]
 //
 // The command line of TPIC's one-rank run (`tpic --run deck.inp --mass-matrix
 // scalar|matrix-core [--restart]`, src/app/main.cpp:60-127), as a C++ host
@@ -17,6 +18,12 @@
 // at the final state, and checkpoints every --restart-cycle cycles under
 // --output/--restart-dir; --restart continues from the newest complete
 // checkpoint and the diagnostics file after a `# restart at cycle N` line.
+// Snapshots follow TPIC's output channels (docs/user/output.md): every
+// FieldOutputCycle cycles one `<array>_tNNNNNN.vti` per array selected by
+// FieldOutputTag / MomentsOutputTag, every ParticlesOutputCycle cycles
+// `particles_tNNNNNN.pvtp` with its piece, both also at the final state, under
+// --output/SaveDirName (deck keys; the --field-output-cycle,
+// --particles-output-cycle and --save-dir options override them).
 // `matrix-core` (TPIC's tensor-core form) selects BF16x3 in mixed precision
 // and the FP64 moment form in double. --dry-run parses the deck and prints
 // the run's sizes without touching a device.
@@ -29,6 +36,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <map>
 #include <sstream>
 #include <string>
 #include <sys/stat.h>
@@ -44,6 +52,10 @@ struct Args {
   long long cycles = -1;
   int diagnostics_cycle = 1, restart_cycle = 0, gmres_max_iterations = 100, device = 0;
   unsigned long long seed = 0;
+  // Snapshot overrides of the deck's keys (unset: the deck's value).
+  bool has_field_cycle = false, has_particles_cycle = false, has_save_dir = false;
+  int field_cycle = 0, particles_cycle = 0;
+  std::string save_dir;
 };
 
 [[noreturn]] void usage(const char* why) {
@@ -52,7 +64,8 @@ struct Args {
                "usage: tpicb200_run --run deck.inp [--mass-matrix matrix-core|scalar|scalar-f64|tf32|bf16x3|"
                "moments-f64] [--precision mixed|double] [--restart] [--output DIR] [--cycles N] "
                "[--diagnostics-cycle K] [--restart-cycle R] [--restart-dir NAME] [--seed S] "
-               "[--gmres-max-iterations M] [--device D] [--dry-run]\n");
+               "[--gmres-max-iterations M] [--device D] [--field-output-cycle F] [--particles-output-cycle P] "
+               "[--save-dir NAME] [--dry-run]\n");
   std::exit(2);
 }
 
@@ -77,6 +90,16 @@ Args parse_args(int argc, char** argv) {
     else if (k == "--gmres-max-iterations") a.gmres_max_iterations = std::atoi(value(i).c_str());
     else if (k == "--device") a.device = std::atoi(value(i).c_str());
     else if (k == "--seed") a.seed = std::strtoull(value(i).c_str(), nullptr, 10);
+    else if (k == "--field-output-cycle") {
+      a.has_field_cycle = true;
+      a.field_cycle = std::atoi(value(i).c_str());
+    } else if (k == "--particles-output-cycle") {
+      a.has_particles_cycle = true;
+      a.particles_cycle = std::atoi(value(i).c_str());
+    } else if (k == "--save-dir") {
+      a.has_save_dir = true;
+      a.save_dir = value(i);
+    }
     else if (k == "--help" || k == "-h") usage("help");
     else usage(("unknown option " + k).c_str());
   }
@@ -93,6 +116,11 @@ int mass_kind(const std::string& form, bool dbl) {
   if (form == "bf16x3") return TPICB200_MASS_BF16X3;
   if (form == "moments-f64") return TPICB200_MASS_MOMENTS_F64;
   usage(("unknown --mass-matrix " + form).c_str());
+}
+
+[[noreturn]] void fail(const std::string& why) {
+  std::fprintf(stderr, "tpicb200_run: %s\n", why.c_str());
+  std::exit(1);
 }
 
 void check(int status, const char* what) {
@@ -205,6 +233,308 @@ bool file_exists(const std::string& path) {
   return ::stat(path.c_str(), &st) == 0;
 }
 
+// mkdir -p: every missing directory of the path.
+void make_dirs(const std::string& path) {
+  for (size_t at = path.find('/', 1); ; at = path.find('/', at + 1)) {
+    const std::string part = path.substr(0, at);
+    if (!part.empty() && ::mkdir(part.c_str(), 0755) != 0 && !file_exists(part))
+      fail("cannot create " + part);
+    if (at == std::string::npos) break;
+  }
+}
+
+// key -> value of a deck text: the last assignment of a key wins, `#` starts
+// a comment (the reading of TPIC's key = value decks).
+std::map<std::string, std::string> deck_keys(const std::string& text) {
+  std::map<std::string, std::string> keys;
+  auto trim = [](std::string v) {
+    const char* ws = " \t\r\n\f\v";
+    const size_t a = v.find_first_not_of(ws);
+    if (a == std::string::npos) return std::string();
+    return v.substr(a, v.find_last_not_of(ws) - a + 1);
+  };
+  std::stringstream in(text);
+  std::string line;
+  while (std::getline(in, line)) {
+    line = line.substr(0, line.find('#'));
+    const size_t eq = line.find('=');
+    if (eq == std::string::npos) continue;
+    keys[trim(line.substr(0, eq))] = trim(line.substr(eq + 1));
+  }
+  return keys;
+}
+
+// The output moments TPIC names: charge density, current and the six
+// pressure components (quantity index 2..7).
+const char* const kMoments[8] = {"rho", "J", "PXX", "PXY", "PXZ", "PYY", "PYZ", "PZZ"};
+
+struct MomentArray {
+  std::string name;
+  int quantity;  // index into kMoments
+  int species;   // -1: the sum over species
+};
+
+// The snapshot channels of a run: cadences, directory and selected arrays.
+struct OutputPlan {
+  std::string save_dir;
+  int field_cycle = 100, particles_cycle = 0;
+  bool e = false, b = false;
+  std::vector<MomentArray> moments;
+  bool fields_due(long long cycle, bool final) const {
+    return field_cycle > 0 && (final || cycle % field_cycle == 0);
+  }
+  bool particles_due(long long cycle, bool final) const {
+    return particles_cycle > 0 && (final || cycle % particles_cycle == 0);
+  }
+};
+
+std::vector<std::string> tag_tokens(const std::string& tag, const char* key) {
+  std::vector<std::string> out;
+  if (tag.empty()) return out;
+  size_t start = 0;
+  while (true) {
+    const size_t plus = tag.find('+', start);
+    const std::string t = tag.substr(start, plus == std::string::npos ? std::string::npos : plus - start);
+    if (t.empty() || t.find_first_of(" \t\r\n\f\v") != std::string::npos)
+      fail(std::string(key) + ": empty or spaced token in '" + tag + "'");
+    out.push_back(t);
+    if (plus == std::string::npos) break;
+    start = plus + 1;
+  }
+  return out;
+}
+
+// The plan from the deck's keys and the command line: the write methods
+// (only the VTK engine is built; ADIOS2 and HDF5 are refused where their
+// channel is on) and TPIC's array selection of FieldOutputTag and
+// MomentsOutputTag. Both tags empty select E, B, rho, J and rho_s, J_s of
+// every species. A moment token is a quantity with no suffix (every
+// species), `_tot` (the sum) or a species index (ignored beyond the run's
+// species); totals come first, then the species in index order, per
+// quantity in TPIC's order.
+OutputPlan output_plan(const std::string& text, const Args& args, int ns) {
+  const std::map<std::string, std::string> k = deck_keys(text);
+  auto get = [&](const char* key, const std::string& fallback) {
+    const auto it = k.find(key);
+    return it == k.end() ? fallback : it->second;
+  };
+  OutputPlan plan;
+  plan.save_dir = args.output + "/" + (args.has_save_dir ? args.save_dir : get("SaveDirName", "data"));
+  plan.field_cycle = args.has_field_cycle ? args.field_cycle : std::atoi(get("FieldOutputCycle", "100").c_str());
+  plan.particles_cycle =
+      args.has_particles_cycle ? args.particles_cycle : std::atoi(get("ParticlesOutputCycle", "0").c_str());
+  const std::string method = get("WriteMethod", "");
+  const std::pair<const char*, int> channels[2] = {{"FieldWriteMethod", plan.field_cycle},
+                                                   {"ParticlesWriteMethod", plan.particles_cycle}};
+  for (const auto& [key, cadence] : channels) {
+    std::string m = get(key, "");
+    if (m.empty()) m = method;
+    if (m == "vtk" || m == "pvtk" || m == "default" || m.empty()) continue;
+    if (m == "adios2" || m == "bp" || m == "bp5" || m == "hdf5" || m == "h5") {
+      if (cadence > 0) fail(std::string(key) + "=" + m + ": only the VTK engine is built");
+      continue;
+    }
+    fail(std::string(key) + ": unknown write method '" + m + "'");
+  }
+  const std::vector<std::string> ftok = tag_tokens(get("FieldOutputTag", ""), "FieldOutputTag");
+  const std::vector<std::string> mtok = tag_tokens(get("MomentsOutputTag", ""), "MomentsOutputTag");
+  if (ftok.empty() && mtok.empty()) {
+    plan.e = plan.b = true;
+    for (int q = 0; q < 2; ++q) plan.moments.push_back({kMoments[q], q, -1});
+    for (int q = 0; q < 2; ++q)
+      for (int s = 0; s < ns; ++s) plan.moments.push_back({std::string(kMoments[q]) + "_" + std::to_string(s), q, s});
+    return plan;
+  }
+  for (const std::string& t : ftok) {
+    if (t == "E") plan.e = true;
+    else if (t == "B") plan.b = true;
+    else if (t == "Gauss") fail("FieldOutputTag: the Gauss-law residual array is not built");
+    else fail("FieldOutputTag: unknown token '" + t + "'");
+  }
+  bool total[8] = {}, bare[8] = {};
+  std::vector<bool> indexed(8 * size_t(ns), false);
+  for (const std::string& t : mtok) {
+    int q = -1;
+    for (int c = 0; c < 8 && q < 0; ++c)
+      if (t.compare(0, std::strlen(kMoments[c]), kMoments[c]) == 0) q = c;
+    if (q < 0) fail("MomentsOutputTag: unknown token '" + t + "'");
+    const std::string suffix = t.substr(std::strlen(kMoments[q]));
+    if (suffix.empty()) {
+      bare[q] = true;
+    } else if (suffix == "_tot") {
+      total[q] = true;
+    } else {
+      if (suffix.find_first_not_of("0123456789") != std::string::npos)
+        fail("MomentsOutputTag: unknown token '" + t + "'");
+      const size_t digits = suffix.find_first_not_of('0');
+      const std::string value = digits == std::string::npos ? "0" : suffix.substr(digits);
+      if (value.size() > 10 || std::strtoull(value.c_str(), nullptr, 10) >= (1ull << 31))
+        fail("MomentsOutputTag: index out of range in '" + t + "'");
+      const long long index = std::atoll(value.c_str());
+      if (index < ns) indexed[8 * size_t(index) + q] = true;
+    }
+  }
+  for (int q = 0; q < 8; ++q) {
+    if (total[q]) plan.moments.push_back({kMoments[q], q, -1});
+    bool any = false;
+    for (int s = 0; s < ns; ++s) any = any || indexed[8 * size_t(s) + q];
+    for (int s = 0; s < ns; ++s)
+      if (indexed[8 * size_t(s) + q] || (bare[q] && !any))
+        plan.moments.push_back({std::string(kMoments[q]) + "_" + std::to_string(s), q, s});
+  }
+  return plan;
+}
+
+// The precision profile name and roles written into every snapshot.
+std::pair<std::string, std::string> precision_strings(bool dbl) {
+  if (dbl)
+    return {"double/double",
+            "storage: position=float64 velocity=float64 weight=float64 E=float64 B=float64 J=float64 "
+            "mass=float64 cell=int32 ID=uint64; compute: position=float64 velocity=float64 E=float64 "
+            "B=float64 J=float64 mass=float64 solver-reduction=float64 reduction=float64 "
+            "output-moment-accumulation=float64"};
+  return {"mixed/mixed",
+          "storage: position=float64 velocity=float32 weight=float64 E=float32 B=float32 J=float32 "
+          "mass=float32 cell=int32 ID=uint64; compute: position=float64 velocity=float32 E=float32 "
+          "B=float32 J=float32 mass=float32 solver-reduction=float64 reduction=float64 "
+          "output-moment-accumulation=float64"};
+}
+
+std::string tagged(const std::string& dir, const std::string& name, long long cycle, const char* ext) {
+  char num[32];
+  std::snprintf(num, sizeof(num), "_t%06lld", cycle);
+  return dir + "/" + name + num + ext;
+}
+
+// One node field of the state (3 components over the stored extent, nodes
+// -1..n+1 per axis, FP32 or FP64) as the snapshot's nodes 0..n per axis,
+// x fastest, components interleaved, FP64.
+std::vector<double> snapshot_nodes(const void* field, const tpicb200_grid& g, bool dbl, cudaStream_t stream) {
+  const size_t ex = g.nx + 3, ey = g.ny + 3, ez = g.nz + 3, plane = ex * ey * ez;
+  std::vector<double> all(3 * plane);
+  if (dbl) {
+    cuda(cudaMemcpyAsync(all.data(), field, all.size() * 8, cudaMemcpyDeviceToHost, stream), "field read");
+    cuda(cudaStreamSynchronize(stream), "field read");
+  } else {
+    std::vector<float> f(3 * plane);
+    cuda(cudaMemcpyAsync(f.data(), field, f.size() * 4, cudaMemcpyDeviceToHost, stream), "field read");
+    cuda(cudaStreamSynchronize(stream), "field read");
+    std::copy(f.begin(), f.end(), all.begin());
+  }
+  const size_t nx = g.nx + 1, ny = g.ny + 1, nz = g.nz + 1;
+  std::vector<double> out(3 * nx * ny * nz);
+  for (size_t k = 0; k < nz; ++k)
+    for (size_t j = 0; j < ny; ++j)
+      for (size_t i = 0; i < nx; ++i)
+        for (size_t c = 0; c < 3; ++c)
+          out[3 * (i + nx * (j + ny * k)) + c] = all[c * plane + (i + 1) + ex * ((j + 1) + ey * (k + 1))];
+  return out;
+}
+
+// Unique-node values (components planes of nz*ny*nx, x fastest) onto the
+// snapshot's node grid with the periodic end nodes, components interleaved.
+std::vector<double> wrap_unique(const double* u, int components, size_t stride, const tpicb200_grid& g) {
+  const size_t nx = g.nx + 1, ny = g.ny + 1, nz = g.nz + 1;
+  std::vector<double> out(size_t(components) * nx * ny * nz);
+  for (size_t k = 0; k < nz; ++k)
+    for (size_t j = 0; j < ny; ++j)
+      for (size_t i = 0; i < nx; ++i) {
+        const size_t src = i % g.nx + size_t(g.nx) * (j % g.ny + size_t(g.ny) * (k % g.nz));
+        for (int c = 0; c < components; ++c)
+          out[size_t(components) * (i + nx * (j + ny * k)) + c] = u[c * stride + src];
+      }
+  return out;
+}
+
+// The field snapshot of the state at `cycle` (the records materialized):
+// E and B at the nodes and the selected output moments, one .vti per array.
+void write_fields(tpicb200_context* ctx, const tpicb200_state& st, const tpicb200_grid& g, const OutputPlan& plan,
+                  int ns, bool dbl, long long cycle, double time, bool final, cudaStream_t stream) {
+  const auto [profile, roles] = precision_strings(dbl);
+  auto put = [&](const std::string& name, const std::vector<double>& values, int components) {
+    check(tpicb200_vtk_write_field(tagged(plan.save_dir, name, cycle, ".vti").c_str(), name.c_str(), components, &g,
+                                   values.data(), int(cycle), time, final ? 1 : 0, profile.c_str(), roles.c_str(),
+                                   1),
+          "field snapshot");
+  };
+  if (plan.e) put("E", snapshot_nodes(st.e, g, dbl, stream), 3);
+  if (plan.b) put("B", snapshot_nodes(st.b_node, g, dbl, stream), 3);
+  if (plan.moments.empty()) return;
+  // kind 0 rho (1 component), 1 J (3), 2 the pressure tensor (6); per[kind]
+  // holds every species' moments and, last, their sum.
+  const size_t unique = size_t(g.nx) * g.ny * g.nz;
+  const int comps[3] = {1, 3, 6};
+  bool needed[3] = {};
+  for (const MomentArray& m : plan.moments) needed[m.quantity < 2 ? m.quantity : 2] = true;
+  std::vector<double> per[3];
+  double* buf = nullptr;
+  cuda(cudaMalloc((void**)&buf, 6 * unique * 8), "moment buffer");
+  for (int kind = 0; kind < 3; ++kind) {
+    if (!needed[kind]) continue;
+    const size_t n = comps[kind] * unique;
+    per[kind].assign((ns + 1) * n, 0.0);
+    for (int s = 0; s < ns; ++s) {
+      const tpicb200_particles part = st.slot[s][st.current[s]];
+      double* args[3] = {nullptr, nullptr, nullptr};
+      args[kind] = buf;
+      cuda(cudaMemsetAsync(buf, 0, n * 8, stream), "moment buffer");
+      check(tpicb200_output_moments(ctx, st.qom[s], &part, args[0], args[1], args[2], stream), "output moments");
+      cuda(cudaMemcpyAsync(per[kind].data() + s * n, buf, n * 8, cudaMemcpyDeviceToHost, stream), "moment read");
+    }
+    cuda(cudaStreamSynchronize(stream), "moment read");
+    double* sum = per[kind].data() + ns * n;
+    for (int s = 0; s < ns; ++s)
+      for (size_t i = 0; i < n; ++i) sum[i] += per[kind][s * n + i];
+  }
+  cudaFree(buf);
+  uint32_t bad = 0;
+  check(tpicb200_read_invalid(ctx, &bad, 0, stream), "invalid-counter read");
+  if (bad) fail("output moments: invalid records in the snapshot state");
+  for (const MomentArray& m : plan.moments) {
+    const int kind = m.quantity < 2 ? m.quantity : 2;
+    const size_t n = comps[kind] * unique;
+    const double* base = per[kind].data() + (m.species < 0 ? ns : m.species) * n;
+    if (kind == 2) put(m.name, wrap_unique(base + (m.quantity - 2) * unique, 1, unique, g), 1);
+    else put(m.name, wrap_unique(base, comps[kind], unique, g), comps[kind]);
+  }
+}
+
+// The particle snapshot of the state at `cycle` (the records materialized,
+// their ids kept): positions, velocities, charges and ids of every species.
+void write_particles(tpicb200_context* ctx, const tpicb200_state& st, const OutputPlan& plan, int ns, bool dbl,
+                     long long cycle, double time, bool final, cudaStream_t stream) {
+  const auto [profile, roles] = precision_strings(dbl);
+  std::vector<std::vector<double>> pos(ns), vel(ns), chg(ns);
+  std::vector<std::vector<uint64_t>> ids(ns);
+  std::vector<tpicb200_vtk_species> species(std::max(ns, 1));
+  for (int s = 0; s < ns; ++s) {
+    const tpicb200_particles part = st.slot[s][st.current[s]];
+    const size_t n = part.count;
+    pos[s].resize(3 * std::max<size_t>(n, 1));
+    vel[s].resize(3 * std::max<size_t>(n, 1));
+    chg[s].resize(std::max<size_t>(n, 1));
+    ids[s].resize(std::max<size_t>(n, 1));
+    if (n) {
+      double* d = nullptr;
+      cuda(cudaMalloc((void**)&d, 7 * n * 8), "particle buffer");
+      check(tpicb200_output_particles(ctx, &part, d, d + 3 * n, d + 6 * n, stream), "output particles");
+      cuda(cudaMemcpyAsync(pos[s].data(), d, 3 * n * 8, cudaMemcpyDeviceToHost, stream), "particle read");
+      cuda(cudaMemcpyAsync(vel[s].data(), d + 3 * n, 3 * n * 8, cudaMemcpyDeviceToHost, stream), "particle read");
+      cuda(cudaMemcpyAsync(chg[s].data(), d + 6 * n, n * 8, cudaMemcpyDeviceToHost, stream), "particle read");
+      cuda(cudaMemcpyAsync(ids[s].data(), part.id, n * 8, cudaMemcpyDeviceToHost, stream), "particle read");
+      cuda(cudaStreamSynchronize(stream), "particle read");
+      cudaFree(d);
+    }
+    species[s] = tpicb200_vtk_species{n, pos[s].data(), vel[s].data(), chg[s].data(), ids[s].data(), uint64_t(s)};
+  }
+  uint32_t bad = 0;
+  check(tpicb200_read_invalid(ctx, &bad, 0, stream), "invalid-counter read");
+  if (bad) fail("particle output: invalid records in the snapshot state");
+  check(tpicb200_vtk_write_particles(plan.save_dir.c_str(), int(cycle), time, final ? 1 : 0, profile.c_str(),
+                                     roles.c_str(), ns, species.data(), 1),
+        "particle snapshot");
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -228,11 +558,24 @@ int main(int argc, char** argv) {
     count[s] = uint32_t(cells * ppc);
     largest = std::max(largest, count[s]);
   }
+  const OutputPlan plan = output_plan(text.str(), args, deck.ns);
   if (args.dry_run) {
     std::printf("deck %s: case %s, %dx%dx%d cells, %d species", args.deck.c_str(), deck.case_name, grid.nx, grid.ny,
                 grid.nz, deck.ns);
     for (int s = 0; s < deck.ns; ++s) std::printf(" %s%u", s ? "+" : " ", count[s]);
     std::printf(" records, %lld cycles, mass form %d, %s precision\n", last, kind, args.precision.c_str());
+    std::printf("snapshots under %s: fields every %d cycles (", plan.save_dir.c_str(), plan.field_cycle);
+    const char* sep = "";
+    for (const char* f : {"E", "B"})
+      if ((f[0] == 'E' && plan.e) || (f[0] == 'B' && plan.b)) {
+        std::printf("%s%s", sep, f);
+        sep = " ";
+      }
+    for (const MomentArray& m : plan.moments) {
+      std::printf("%s%s", sep, m.name.c_str());
+      sep = " ";
+    }
+    std::printf("), particles every %d cycles\n", plan.particles_cycle);
     return 0;
   }
 
@@ -382,12 +725,24 @@ int main(int argc, char** argv) {
     std::printf("cycle %6lld  total energy %.10e  change %+.3e\n", cycle, t, t - initial);
     std::fflush(stdout);
   };
+  auto snapshots = [&] {
+    const bool final = cycle == last;
+    const bool fields = plan.fields_due(cycle, final), particles = plan.particles_due(cycle, final);
+    if (!fields && !particles) return;
+    make_dirs(plan.save_dir);
+    check(tpicb200_materialize(ctx, &st, s_), "materialize");
+    if (fields) write_fields(ctx, st, grid, plan, deck.ns, dbl, cycle, double(cycle) * deck.dt, final, stream);
+    if (particles) write_particles(ctx, st, plan, deck.ns, dbl, cycle, double(cycle) * deck.dt, final, stream);
+  };
   if ((cadence && cycle % cadence == 0) || cycle == last) record(cycle == last);
+  snapshots();
   std::vector<tpicb200_cycle_report> reports;
   while (cycle < last) {
     long long stop = last;
     if (cadence) stop = std::min(stop, (cycle / cadence + 1) * cadence);
     if (every) stop = std::min(stop, (cycle / every + 1) * every);
+    for (const int channel : {plan.field_cycle, plan.particles_cycle})
+      if (channel > 0) stop = std::min(stop, (cycle / channel + 1) * channel);
     const int n = int(stop - cycle);
     reports.assign(n, tpicb200_cycle_report{});
     check(tpicb200_cycle(ctx, &st, n, reports.data(), s_), "cycle");
@@ -400,6 +755,7 @@ int main(int argc, char** argv) {
     if (every && (cycle % every == 0 || cycle == last))
       check(tpicb200_checkpoint_write(ctx, &st, ckpt_dir.c_str(), int(cycle), s_), "checkpoint write");
     if (cycle == last || (cadence && cycle % cadence == 0)) record(cycle == last);
+    snapshots();
     if (!std::isfinite(field[0]) || !std::isfinite(field[1])) {
       std::fprintf(stderr, "tpicb200_run: nonfinite field energy\n");
       return 1;
