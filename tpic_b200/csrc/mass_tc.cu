@@ -28,7 +28,7 @@
 // tcgen05.mma.kind::tf32 (K = 8) issued by one thread; A and B are
 // double-buffered so the next chunk is produced while the tensor core
 // consumes the previous one (tcgen05.commit -> mbarrier, bounded waits).
-// Operands are rounded to nearest (cvt.rna.tf32, bf16 RN split) so the
+// Operands are rounded to nearest (TF32 ties away, bf16 RN split) so the
 // rounding is unbiased; accumulation is FP32. The epilogue reads G and H with
 // tcgen05.ld, forms the 8x3 corner currents and stores the cell's moments
 // (27x9 + 8x3 values; each group of four consecutive cells has one

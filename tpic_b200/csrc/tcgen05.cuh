@@ -169,11 +169,14 @@ __host__ __device__ constexpr uint32_t instr_desc(uint32_t ab_format, uint32_t m
          ((m >> 4) << 24);
 }
 
-__device__ __forceinline__ uint32_t to_tf32(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return r;
-}
+// x rounded to TF32 (10 explicit mantissa bits), to nearest with ties away
+// from zero: half a TF32 unit (bit 12) is added to the magnitude bits and the
+// 13 low bits are cleared; a carry into the exponent is the correct rounding
+// up to the next binade. For finite |x| below the largest TF32 value this is
+// the rounding of cvt.rna.tf32.f32 in two integer instructions; the callers
+// pass finite operands only (a record with a non-finite value contributes
+// zeros).
+__device__ __forceinline__ uint32_t to_tf32(float x) { return (__float_as_uint(x) + 0x1000u) & 0xFFFFE000u; }
 
 }  // namespace tc
 }  // namespace tpicb200
