@@ -644,19 +644,10 @@ __global__ void __launch_bounds__(256) binned_bases_kernel(Geom g, const uint32_
   }
 }
 
-// Rank of each live lane among the live lanes of its slot and the slot's
-// lane mask: one ballot per distinct slot value in the warp (a chunk of
-// sorted records holds few).
+// The lane mask of a live lane's slot: the live lanes with the same slot
+// value (one match instruction; a lane that is not live matches only itself).
 __device__ __forceinline__ unsigned slot_group(int slot, bool live) {
-  unsigned rem = __ballot_sync(0xffffffffu, live), group = 0;
-  while (rem) {
-    const int leader = __ffs(rem) - 1;
-    const int s = __shfl_sync(0xffffffffu, slot, leader);
-    const unsigned m = __ballot_sync(0xffffffffu, live && slot == s);
-    if (live && slot == s) group = m;
-    rem &= ~m;
-  }
-  return group;
+  return __match_any_sync(0xffffffffu, live ? slot : -1 - int(threadIdx.x & 31));
 }
 
 // Output position of every record: perm[position] = record. The record goes
