@@ -586,13 +586,15 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_deposit_kernel(Geom g, TcP
 // gw, gw + W, gw + 2W, ... for global warp gw of W) and walks a batch's
 // records as one stream - cell by cell, species 0 before species 1 in a
 // cell - in chunks of up to 32 records (one per lane). A chunk never crosses
-// the end of a (cell, species) range, so its cell and species are the same
-// for every lane: the species' record arrays are addressed without per-lane
-// selection, and the warp's quadrant of D holds one accumulator block, which
-// is flushed - read from tensor memory, then zeroed - once the MMAs of the
-// cell's last chunk have completed and before the warp's next chunk is
-// written. Every batch starts a new chunk, so a cell's summation order
-// depends only on its batch's counts: the moments are reproducible.
+// the end of a cell, so its cell is the same for every lane and the warp's
+// quadrant of D holds one accumulator block, which is flushed - read from
+// tensor memory, then zeroed - once the MMAs of the cell's last chunk have
+// completed and before the warp's next chunk is written. A chunk may cross
+// from the cell's species-0 records to its species-1 records (each lane
+// reads its own species' arrays): a cell of c0 + c1 records takes
+// ceil((c0 + c1) / 32) chunks, not ceil(c0 / 32) + ceil(c1 / 32). Every batch
+// starts a new chunk, so a cell's summation order depends only on its
+// batch's counts: the moments are reproducible.
 //
 // The four warps of a CTA share every MMA (M = 128 = four quadrants of 32
 // monomial rows; rows 27..31 of a quadrant stay zero):
@@ -643,13 +645,12 @@ struct __align__(16) StreamShared {
 };
 
 // Per-lane record of a chunk: rank (record index in the read slot), sorted
-// position, flags (1 present).
+// position, flags (bit 0 present, bit 1 species 1).
 struct StreamLane {
   uint32_t idx, pos, flags;
 };
 // Warp-uniform chunk description: batch and bits (ended cells 0-3,
-// nonempty cells 4-7, species 12, valid 13, metadata slot 14-15, cell slot
-// 16-17).
+// nonempty cells 4-7, valid 13, metadata slot 14-15, cell slot 16-17).
 struct StreamInfo {
   int bid;
   uint32_t bits;
@@ -808,25 +809,28 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
       }
     }
     if (cend) return;
-    // The chunk [cbase, end): at most 32 records of the first range that
-    // ends above cbase (empty ranges end at or below it).
+    // The chunk [cbase, end): at most 32 records of the cell of the first
+    // range that ends above cbase (empty ranges end at or below it); the
+    // chunk may hold the end of the cell's species-0 range and the start of
+    // its species-1 range.
     const uint32_t above = __ballot_sync(0xffffffffu, lane < 2 * kBatch && rend > cbase);
     // A batch without records has no range: its one chunk is empty.
-    const int range = above ? __ffs(above) - 1 : 0;
-    const uint32_t range_end = __shfl_sync(0xffffffffu, rend, range);
-    const uint32_t offset = __shfl_sync(0xffffffffu, roff, range);
-    const uint32_t end = above ? min(cbase + 32u, range_end) : cbase;
+    const int cell_slot = above ? (__ffs(above) - 1) >> 1 : 0;
+    const uint32_t first_end = __shfl_sync(0xffffffffu, rend, 2 * cell_slot);
+    const uint32_t cell_end = __shfl_sync(0xffffffffu, rend, 2 * cell_slot + 1);
+    const uint32_t end = above ? min(cbase + 32u, cell_end) : cbase;
+    // Each lane's range (species) and its sorted-array offset.
+    const uint32_t p = cbase + lane;
+    const uint32_t second = p >= first_end ? 1u : 0u;
+    const uint32_t offset = __shfl_sync(0xffffffffu, roff, 2 * cell_slot + int(second));
     // Cells ending in this chunk (empty cells at or below `end` included).
     uint32_t ended = (cb1 <= end ? 1u : 0u) | (cb2 <= end ? 2u : 0u) | (cb3 <= end ? 4u : 0u) |
                      (ctot <= end ? 8u : 0u);
     ended &= ~cdone;
     cdone |= ended;
     const bool last = end >= ctot;
-    const uint32_t second = uint32_t(range & 1);
     I.bid = cbid;
-    I.bits = ended | (cnonempty << 4) | (second << 12) | (1u << 13) | (uint32_t(cslot) << 14) |
-             (uint32_t(range >> 1) << 16);
-    const uint32_t p = cbase + lane;
+    I.bits = ended | (cnonempty << 4) | (1u << 13) | (uint32_t(cslot) << 14) | (uint32_t(cell_slot) << 16);
     if (p < end) {
       L.pos = p + offset;
       const uint32_t* perm = second ? tp.sp[1].perm : tp.sp[0].perm;
@@ -835,7 +839,7 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
         tc::cp_async4(dst, perm + L.pos);
       else
         *dst = L.pos;
-      L.flags = 1u;
+      L.flags = 1u | (second << 1);
     }
     if (last)
       cnext = true;
@@ -854,14 +858,14 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
       prefetch_l2(sp.u + n); prefetch_l2(sp.v + n); prefetch_l2(sp.w + n); prefetch_l2(sp.key + n);
     };
     if (L.flags & 1u) {
-      if ((I.bits >> 12) & 1u)
+      if (L.flags & 2u)
         prefetch(tp.sp[1]);
       else
         prefetch(tp.sp[0]);
     }
   };
-  // The record of a lane; the species is the chunk's (one branch per warp).
-  auto load_rec = [&](const StreamLane& L, const StreamInfo& I) {
+  // The record of a lane (its species: bit 1 of its flags).
+  auto load_rec = [&](const StreamLane& L) {
     StreamRec r{0.0, 0.0, 0.0, 0.0, 0.0f, 0.0f, 0.0f, -1, L.pos, L.flags};
     auto from = [&](const TcSpecies& sp) {
       const uint32_t n = L.idx;
@@ -875,7 +879,7 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
       r.key = sp.key[n];
     };
     if (L.flags & 1u) {
-      if ((I.bits >> 12) & 1u)
+      if (L.flags & 2u)
         from(tp.sp[1]);
       else
         from(tp.sp[0]);
@@ -964,7 +968,7 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
   take_rank(la, ia, 0u);
   tc::cp_async_wait_group<1>();
   take_rank(lb, ib, 1u);
-  StreamRec r1 = load_rec(la, ia);
+  StreamRec r1 = load_rec(la);
   StreamInfo i1 = ia;
   StreamInfo ip{0, 0u};  // the previous chunk, whose cells are flushed next
   bool bad = false;
@@ -972,7 +976,7 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
   for (uint32_t j = 0;; ++j) {
     const StreamRec r0 = r1;
     const StreamInfo i0 = i1;
-    r1 = load_rec(lb, ib);
+    r1 = load_rec(lb);
     i1 = ib;
     StreamLane ld;
     StreamInfo id;
@@ -996,8 +1000,7 @@ __global__ void __launch_bounds__(128, kCtasPerSm) tc_stream_kernel(Geom g, TcPa
     for (int c = 0; c < 9; ++c) YZ[c] = 0.0f;
     if (have && (r0.flags & 1u)) {
       const int slot = int(i0.bits >> 16) & 3;
-      const bool second = (i0.bits >> 12) & 1u;
-      const TcSpecies& sp = second ? tp.sp[1] : tp.sp[0];
+      const TcSpecies& sp = (r0.flags & 2u) ? tp.sp[1] : tp.sp[0];
       if (sp.orx) {
         const uint32_t o = r0.pos;
         sp.orx[o] = r0.fx; sp.ory[o] = r0.fy; sp.orz[o] = r0.fz;
