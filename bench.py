@@ -435,8 +435,7 @@ def run_gpu(args) -> None:
     roofline = {"kernel": dominant, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "peak_source": peak_kind,
                 "traffic": traffic, "algorithmic_bytes": dk["bytes"],
-                "algorithmic_basis": "positions 24 B + velocities 3 x 4 B + charge 8 B per particle, "
-                                     "mass assembly fused into the same pass",
+                "algorithmic_basis": dk["basis"],
                 "record_bytes": dk.get("record_bytes"),
                 "all_kernels": {k: {"ms": v["ms"], "GB/s": v["bytes"] / (v["ms"] / 1e3) / 1e9,
                                     "frac": v["bytes"] / (v["ms"] / 1e3) / 1e9 / hbm} for k, v in kernels.items()}}
@@ -577,12 +576,16 @@ def stage_kernel_times(sim, args, stream, repeats: int = 5) -> dict:
     # pass). record_bytes adds what the kernels move beyond that: the key,
     # and the per-cell moments or the node outputs.
     out["deposit"] = {"ms": timed_after(clear, deposit), "bytes": n_total * (24 + 3 * vb + 8),
+                      "basis": f"positions 24 B + velocities 3 x {vb} B + charge 8 B per particle, mass assembly "
+                               "fused into the same pass",
                       "record_bytes": n_total * (24 + 3 * vb + 8 + 4) + (moment_bytes if tc_form else
                                                                          nodes * (126 + 3) * fb)}
     # The fold: for the tensor-core forms the moment assembly (moments read,
     # J and the mass records written) and the periodic fold.
     out["assembly"] = {"ms": timed_after(clear_and_deposit, fold),
-                       "bytes": (moment_bytes if tc_form else 0) + nodes * (126 + 3) * fb}
+                       "bytes": (moment_bytes if tc_form else 0) + nodes * (126 + 3) * fb,
+                       "basis": ("per-cell moments read, " if tc_form else "") +
+                                f"126 mass entries + 3 current components x {fb} B per node written"}
 
     # Sort of all species as the cycle runs it (the binned sort of records
     # grouped by the live bins; ping-pong into the idle slot and back).
@@ -593,7 +596,8 @@ def stage_kernel_times(sim, args, stream, repeats: int = 5) -> dict:
                                                 C.byref(st.slot[s][1 - cur]), st.counts[s], st.offsets[s],
                                                 scratch_inv.data_ptr(), s_))
             st.current[s] = 1 - cur
-    out["sort"] = {"ms": timed(sort_once), "bytes": n_total * (4 + 2 * (24 + 3 * vb + 8 + 4))}
+    out["sort"] = {"ms": timed(sort_once), "bytes": n_total * (4 + 2 * (24 + 3 * vb + 8 + 4)),
+                   "basis": f"key 4 B read, record ({24 + 3 * vb + 12} B) read and written per particle"}
     # Make sure the live slot is the sorted one with valid bins (an even number of sorts ran).
     if (repeats + 1) % 2:
         sort_once()
@@ -609,7 +613,8 @@ def stage_kernel_times(sim, args, stream, repeats: int = 5) -> dict:
             p = st.slot[s][st.current[s]]
             _lib.check(lib.tpicb200_mover(sim.ctx, st.qom[s], C.byref(p), st.e_theta, st.b_node,
                                           scratch_inv.data_ptr(), s_))
-    out["mover"] = {"ms": timed(move), "bytes": n_total * 2 * (4 + 24 + 3 * vb)}
+    out["mover"] = {"ms": timed(move), "bytes": n_total * 2 * (4 + 24 + 3 * vb),
+                    "basis": f"key 4 B, positions 24 B, velocities 3 x {vb} B read and written per particle"}
     for s in range(ns):
         for k, v in saved[s].items():
             sim.slots[s][st.current[s]][k].copy_(v)
