@@ -479,3 +479,57 @@ def test_tc_moments_accumulate_two_species(torch_cuda, kind):
     assert np.abs(interior_nodes(g, jg) - interior_nodes(g, jw)).max() <= rel * np.abs(interior_nodes(g, jw)).max()
     mi = interior_records(g, mw)
     assert np.abs(interior_records(g, mg) - mi).max() <= rel * np.abs(mi).max()
+
+
+@pytest.mark.parametrize("kind", [2, 3])
+def test_tc_fused_species_ragged_cells(torch_cuda, kind):
+    """Both species in one tensor-core pass over ragged cells: per cell each
+    species keeps 0 %, 30 %, 70 % or all of 64 records by a cell pattern, so
+    cells hold only species 0, only species 1, neither, or both with counts
+    that cross 32-record chunk boundaries anywhere (a chunk may run from the
+    cell's species-0 records into its species-1 records). The moments equal
+    the oracle's sum of both species."""
+    g = GridSpec(24, 20, 16, 2.4, 2.0, 1.6)
+    rng = np.random.default_rng(53)
+    keep_fraction = (0.0, 0.3, 0.7, 1.0)
+    species = []
+    for s, (qom, seed, vth) in enumerate(((-4.0, 11, (0.2, 0.1, 0.3)), (1.0, 12, (0.02, 0.01, 0.03)))):
+        d = species_arrays(g, 1, seed=seed, vth=vth, npcel=(4, 4, 4), qom=qom)
+        key = d["cell"].astype(np.int64)
+        ex, ey = g.nx + 4, g.ny + 4
+        i, j, k = key % ex - 2, (key // ex) % ey - 2, key // (ex * ey) - 2
+        pattern = (i + 3 * j + 7 * k + s) % 4
+        keep = rng.random(len(key)) < np.take(keep_fraction, pattern)
+        species.append((qom, {name: np.ascontiguousarray(v[keep]) for name, v in d.items()}))
+    counts_per_cell = [np.bincount(d["cell"], minlength=(g.nx + 4) * (g.ny + 4) * (g.nz + 4)) for _, d in species]
+    both = (counts_per_cell[0] > 0) & (counts_per_cell[1] > 0)
+    assert both.any() and ((counts_per_cell[0] > 0) & ~both).any() and ((counts_per_cell[1] > 0) & ~both).any()
+    assert (counts_per_cell[0][both] % 32 != 0).any()
+    nmax = max(len(d["cell"]) for _, d in species)
+    ctx = make_ctx(g, 1, dt=0.2, max_particles=nmax, mass_layout=1)
+    bnode = periodic_node_field(g, smooth_random_unique(g, rng, 0.9)).astype(np.float32)
+    bn = ctx.field(bnode)
+    j, m = ctx.moments()
+    sorted_species, structs, jw, mw = [], [], 0.0, 0.0
+    for qom, d in species:
+        n = len(d["cell"])
+        parts, counts, offsets = ctx.sort(ctx.upload_particles(d), n)
+        sorted_species.append((parts, counts, offsets))
+        structs.append(ctx.struct(parts, n))
+        js, ms, bad = oracle_moments(g, 1, qom, 0.2, d, bnode)
+        assert bad == 0
+        jw, mw = jw + js, mw + ms
+    qoms = (C.c_double * 2)(*[qom for qom, _ in species])
+    parts_arr = (_lib.Particles * 2)(*structs)
+    counts_arr = (C.c_void_p * 2)(*[c.data_ptr() for _, c, _ in sorted_species])
+    offsets_arr = (C.c_void_p * 2)(*[o.data_ptr() for _, _, o in sorted_species])
+    _lib.check(ctx.lib.tpicb200_deposit_species(ctx.ctx, 2, qoms, parts_arr, counts_arr, offsets_arr, bn.data_ptr(),
+                                                j.data_ptr(), m.data_ptr(), kind, ctx.invalid.data_ptr(),
+                                                ctx.stream))
+    ctx.fold(j, m)
+    assert ctx.invalid_count() == 0
+    jg, mg = j.cpu().numpy().astype(np.float64), ctx.records(m)
+    rel = 3e-3 if kind == 2 else 1e-4
+    assert np.abs(interior_nodes(g, jg) - interior_nodes(g, jw)).max() <= rel * np.abs(interior_nodes(g, jw)).max()
+    mi = interior_records(g, mw)
+    assert np.abs(interior_records(g, mg) - mi).max() <= rel * np.abs(mi).max()
