@@ -481,19 +481,21 @@ def test_tc_moments_accumulate_two_species(torch_cuda, kind):
     assert np.abs(interior_records(g, mg) - mi).max() <= rel * np.abs(mi).max()
 
 
-@pytest.mark.parametrize("kind", [2, 3])
-def test_tc_fused_species_ragged_cells(torch_cuda, kind):
+@pytest.mark.parametrize("kind,nspecies", [(2, 2), (3, 2), (2, 3), (3, 3)])
+def test_tc_fused_species_ragged_cells(torch_cuda, kind, nspecies):
     """Both species in one tensor-core pass over ragged cells: per cell each
     species keeps 0 %, 30 %, 70 % or all of 64 records by a cell pattern, so
     cells hold only species 0, only species 1, neither, or both with counts
     that cross 32-record chunk boundaries anywhere (a chunk may run from the
     cell's species-0 records into its species-1 records). The moments equal
-    the oracle's sum of both species."""
+    the oracle's sum of both species. With three species the call runs two
+    passes (species 0 and 1, then species 2 added into the same moments)."""
     g = GridSpec(24, 20, 16, 2.4, 2.0, 1.6)
     rng = np.random.default_rng(53)
     keep_fraction = (0.0, 0.3, 0.7, 1.0)
     species = []
-    for s, (qom, seed, vth) in enumerate(((-4.0, 11, (0.2, 0.1, 0.3)), (1.0, 12, (0.02, 0.01, 0.03)))):
+    params = ((-4.0, 11, (0.2, 0.1, 0.3)), (1.0, 12, (0.02, 0.01, 0.03)), (-1.0, 13, (0.1, 0.1, 0.1)))
+    for s, (qom, seed, vth) in enumerate(params[:nspecies]):
         d = species_arrays(g, 1, seed=seed, vth=vth, npcel=(4, 4, 4), qom=qom)
         key = d["cell"].astype(np.int64)
         ex, ey = g.nx + 4, g.ny + 4
@@ -519,13 +521,13 @@ def test_tc_fused_species_ragged_cells(torch_cuda, kind):
         js, ms, bad = oracle_moments(g, 1, qom, 0.2, d, bnode)
         assert bad == 0
         jw, mw = jw + js, mw + ms
-    qoms = (C.c_double * 2)(*[qom for qom, _ in species])
-    parts_arr = (_lib.Particles * 2)(*structs)
-    counts_arr = (C.c_void_p * 2)(*[c.data_ptr() for _, c, _ in sorted_species])
-    offsets_arr = (C.c_void_p * 2)(*[o.data_ptr() for _, _, o in sorted_species])
-    _lib.check(ctx.lib.tpicb200_deposit_species(ctx.ctx, 2, qoms, parts_arr, counts_arr, offsets_arr, bn.data_ptr(),
-                                                j.data_ptr(), m.data_ptr(), kind, ctx.invalid.data_ptr(),
-                                                ctx.stream))
+    qoms = (C.c_double * nspecies)(*[qom for qom, _ in species])
+    parts_arr = (_lib.Particles * nspecies)(*structs)
+    counts_arr = (C.c_void_p * nspecies)(*[c.data_ptr() for _, c, _ in sorted_species])
+    offsets_arr = (C.c_void_p * nspecies)(*[o.data_ptr() for _, _, o in sorted_species])
+    _lib.check(ctx.lib.tpicb200_deposit_species(ctx.ctx, nspecies, qoms, parts_arr, counts_arr, offsets_arr,
+                                                bn.data_ptr(), j.data_ptr(), m.data_ptr(), kind,
+                                                ctx.invalid.data_ptr(), ctx.stream))
     ctx.fold(j, m)
     assert ctx.invalid_count() == 0
     jg, mg = j.cpu().numpy().astype(np.float64), ctx.records(m)
