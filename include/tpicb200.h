@@ -754,6 +754,13 @@ int tpicb200_vtk_write_field(const char* path, const char* name, int components,
                              const double* values, int cycle, double time, int final_state, const char* profile,
                              const char* roles, int overwrite);
 
+/* Writes one Float64 cell array (nx ny nz values, x fastest) as VTK XML
+ * ImageData CellData over the same node extent and FieldData as
+ * tpicb200_vtk_write_field (host only): TPIC's Gauss snapshot array. */
+int tpicb200_vtk_write_cells(const char* path, const char* name, const tpicb200_grid* grid, const double* values,
+                             int cycle, double time, int final_state, const char* profile, const char* roles,
+                             int overwrite);
+
 typedef struct {
   uint64_t count;
   const double* position;  /* 3 * count, global coordinates */
@@ -769,6 +776,39 @@ typedef struct {
  * its PPolyData manifest particles_tNNNNNN.pvtp. */
 int tpicb200_vtk_write_particles(const char* directory, int cycle, double time, int final_state, const char* profile,
                                  const char* roles, int ns, const tpicb200_vtk_species* species, int overwrite);
+
+/* ------------------------------------------------------------------------
+ * Gauss-law residual (TPIC's DiagnosticGaussCycle and FieldOutputTag Gauss;
+ * diagnostics/gauss_residual_device.hpp, docs/developer/gauss_diagnostic.md).
+ *
+ * A sample begun at state n holds per cell s = divC(E^n)/2 - c, where divC is
+ * the solver's node-to-cell divergence and c is 4 pi times the 8-node mean of
+ * the charge density rho = sum(q W)/V of the state's records (the positions
+ * x^{n+1/2}), smoothed like the solver's current when the context smooths;
+ * finishing it at state n+1 gives r = s + divC(E^{n+1})/2, the residual at
+ * time (n + 1/2) dt. Cell arrays (stash, first, residual) are caller-owned
+ * FP64 device buffers of nx ny nz cells, x fastest; sums is a device double[4]
+ * in gauss.csv's column order: sum of r^2, of (r - r_first)^2, of r^2 over
+ * wall cells (0: a periodic grid has none), of c^2. The root mean squares are
+ * sqrt(sum / (nx ny nz)). Stream-ordered; the sums of the same inputs are
+ * reproducible (fixed-order reductions).
+ * ------------------------------------------------------------------------ */
+
+/* The field part of a sample (gauss_field_partials_kernel): with finish,
+ * r = stash + divC(E)/2 into residual, sums[0..2], and first = r when
+ * set_first (the run's first finished sample; its drift sum is 0); with
+ * begin, stash = divC(E)/2, after the finish has read it (one call serves a
+ * state that finishes a sample and begins the next). */
+int tpicb200_gauss_field(tpicb200_context* ctx, const void* e, double* stash, double* first, double* residual,
+                         int begin, int finish, int set_first, double* sums, tpicb200_stream stream);
+
+/* The charge part of a begun sample (gauss_charge_partials_kernel): rho of
+ * the ns species' records, the context's smoothing in FP64 arithmetic when it
+ * has one, c per cell, stash -= c and sums[3] = sum of c^2. A record with an
+ * invalid key, a fraction outside [0, 1) or a nonfinite charge raises the
+ * context's invalid counter. */
+int tpicb200_gauss_charge(tpicb200_context* ctx, int ns, const tpicb200_particles* species, double* stash,
+                          double* sums, tpicb200_stream stream);
 
 #ifdef __cplusplus
 }

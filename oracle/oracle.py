@@ -432,3 +432,68 @@ def output_moments(grid, d: dict, qom: float, precision: int = 0):
         for c in range(10):
             np.add.at(out[c], (k, j, i), amounts[c] * wt)
     return out[0:1], out[1:4], out[4:10]
+
+
+def _node_samples(grid, f: np.ndarray):
+    """The eight corner samples of every cell from a halo-layout node field
+    component (nz+3, ny+3, nx+3): base, x, y, z, xy, xz, yz, xyz
+    (load_node_cell_samples, ecsim/fields/node_cell_curl.hpp:84-98)."""
+    g = grid
+
+    def at(a, b, d):
+        return f[1 + d:1 + d + g.nz, 1 + b:1 + b + g.ny, 1 + a:1 + a + g.nx]
+    return [at(0, 0, 0), at(1, 0, 0), at(0, 1, 0), at(0, 0, 1), at(1, 1, 0), at(1, 0, 1), at(0, 1, 1), at(1, 1, 1)]
+
+
+def gauss_half_divergence(grid, e: np.ndarray) -> np.ndarray:
+    """divC(E)/2 per cell in FP64 (nz, ny, nx), restating node_cell_divergence
+    (ecsim/fields/node_cell_curl.hpp:129-141) with NodeCellSamples::derivative's
+    edge differences in their order (:63-80) and the residual's 0.5 factor
+    (diagnostics/gauss_residual_device.hpp:46-47). `e` is the node field in
+    the library's halo layout, (3, nz+3, ny+3, nx+3) (float storage widened)."""
+    g = grid
+    e = np.asarray(e, dtype=np.float64).reshape(3, g.nz + 3, g.ny + 3, g.nx + 3)
+    inv = (1.0 / (g.lx / g.nx), 1.0 / (g.ly / g.ny), 1.0 / (g.lz / g.nz))
+    q = _node_samples(g, e[0])
+    dx = 0.25 * inv[0] * ((((q[1] - q[0]) + (q[5] - q[3])) + (q[4] - q[2])) + (q[7] - q[6]))
+    q = _node_samples(g, e[1])
+    dy = 0.25 * inv[1] * ((((q[2] - q[0]) + (q[6] - q[3])) + (q[4] - q[1])) + (q[7] - q[5]))
+    q = _node_samples(g, e[2])
+    dz = 0.25 * inv[2] * ((((q[3] - q[0]) + (q[5] - q[1])) + (q[6] - q[2])) + (q[7] - q[4]))
+    return 0.5 * ((dx + dy) + dz)
+
+
+def gauss_cell_charge(grid, species: list, smoothing=(0, 1.0, 0)) -> np.ndarray:
+    """c per cell in FP64 (nz, ny, nx): 4 pi times the 8-node mean of the
+    charge density rho = sum(q W)/V of every species' records (the rho of
+    output_moments before its 4 pi), after `smoothing` = (passes, alpha,
+    operator) passes of the oracle's smoothing (gauss_residual_device.hpp:82-99,
+    the complete_charge steps of docs/developer/gauss_diagnostic.md)."""
+    g = grid
+    vol = (g.lx / g.nx) * (g.ly / g.ny) * (g.lz / g.nz)
+    ex, ey = g.nx + 4, g.ny + 4
+    rho = np.zeros((g.nz, g.ny, g.nx))
+    for d in species:
+        key = d["cell"].astype(np.int64)
+        ci, cj, ck = key % ex - 2, (key // ex) % ey - 2, key // (ex * ey) - 2
+        fx, fy, fz = (np.asarray(d[k], dtype=np.float64) for k in ("rx", "ry", "rz"))
+        charge = np.asarray(d["q"], dtype=np.float64) * (1.0 / vol)
+        cx, cy, cz = 1.0 - fx, 1.0 - fy, 1.0 - fz
+        for a in range(8):
+            wt = ((fx if a & 1 else cx) * (fy if a & 2 else cy)) * (fz if a & 4 else cz)
+            np.add.at(rho, ((ck + ((a >> 2) & 1)) % g.nz, (cj + ((a >> 1) & 1)) % g.ny, (ci + (a & 1)) % g.nx),
+                      charge * wt)
+    # The node field with its periodic ghosts and end nodes, component 0.
+    k = (np.arange(g.nz + 3) - 1) % g.nz
+    j = (np.arange(g.ny + 3) - 1) % g.ny
+    i = (np.arange(g.nx + 3) - 1) % g.nx
+    field = np.zeros((3, g.nz + 3, g.ny + 3, g.nx + 3))
+    field[0] = rho[k][:, j][:, :, i]
+    passes, alpha, op = smoothing
+    if passes > 0:
+        out = np.zeros_like(field)
+        grid_struct = OGrid(g.nx, g.ny, g.nz, g.lx / g.nx, g.ly / g.ny, g.lz / g.nz)
+        load().oracle_smooth(C.byref(grid_struct), int(passes), float(alpha), int(op), ptr(field), ptr(out))
+        field = out
+    q = _node_samples(g, field[0])
+    return np.pi / 2 * (((((((q[0] + q[1]) + q[2]) + q[4]) + q[3]) + q[5]) + q[6]) + q[7])

@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 from tpic_b200 import _lib
-from tpic_b200.output import OutputPlan, deck_keys, select_arrays
+from tpic_b200.output import GaussSample, GaussWriter, OutputPlan, csv_number, deck_keys, select_arrays
 from vtkread import field_data, read
 
 
@@ -84,8 +84,8 @@ def test_default_and_tagged_selection():
         with pytest.raises(ValueError):
             select_arrays(bad if bad in ("EB", "none", "B+") else "", bad if bad not in ("EB", "none", "B+") else "",
                           2)
-    with pytest.raises(ValueError):
-        select_arrays("Gauss", "", 1)
+    fields, moments = select_arrays("Gauss+E", "", 1)
+    assert fields == ["Gauss", "E"] and moments == []
 
 
 def test_plan_from_deck(tmp_path):
@@ -102,3 +102,60 @@ def test_plan_from_deck(tmp_path):
         OutputPlan.from_deck("FieldWriteMethod = csv\n", tmp_path)
     plan = OutputPlan.from_deck("", tmp_path, field_cycle=2, particles_cycle=3)
     assert (plan.field_cycle, plan.particles_cycle, plan.save_dir) == (2, 3, tmp_path / "data")
+
+
+def test_cell_file_round_trip(tmp_path):
+    """The Gauss array: Float64 CellData over the node extent, nx*ny*nz values."""
+    lib = _lib.load()
+    grid = _lib.Grid(4, 3, 2, 2.0, 1.5, 0.5)
+    values = np.random.default_rng(5).normal(size=(2, 3, 4))
+    path = tmp_path / "Gauss_t000004.vti"
+    _lib.check(lib.tpicb200_vtk_write_cells(str(path).encode(), b"Gauss", C.byref(grid),
+                                            np.ascontiguousarray(values).ctypes.data, 4, 0.5, 0, b"mixed/mixed",
+                                            b"roles", 1))
+    root, arrays, _ = read(path)
+    piece = root.find("ImageData/Piece")
+    assert piece.find("CellData/DataArray").get("Name") == "Gauss"
+    assert len(piece.find("PointData")) == 0
+    assert root.find("ImageData").get("WholeExtent") == "0 4 0 3 0 2"
+    assert np.array_equal(arrays["Gauss"], values.ravel())
+    assert field_data(root)["cycle"] == 4
+
+
+def test_gauss_cadence():
+    """PreparedOutput::should_sample_gauss (src/config/output.cpp): multiples of
+    DiagnosticGaussCycle below the last cycle, and with the Gauss array one
+    cycle before every field snapshot and before the final state."""
+    plan = OutputPlan.from_deck("DiagnosticGaussCycle = 3\nFieldOutputCycle = 0\n", "/tmp")
+    assert plan.gauss_enabled() and not plan.output_gauss
+    assert [n for n in range(12) if plan.gauss_begins(n, 10)] == [0, 3, 6, 9]
+    assert plan.next_gauss_begin(3, 10) == 6 and plan.next_gauss_begin(9, 10) is None
+    plan = OutputPlan.from_deck("FieldOutputCycle = 4\nFieldOutputTag = E+Gauss\n", "/tmp")
+    assert plan.output_gauss and plan.gauss_cycle == 0
+    assert [n for n in range(12) if plan.gauss_begins(n, 10)] == [3, 7, 9]
+    # Gauss has no effect without a field channel.
+    plan = OutputPlan.from_deck("FieldOutputCycle = 0\nFieldOutputTag = Gauss\n", "/tmp")
+    assert not plan.gauss_enabled()
+    plan = OutputPlan.from_deck("DiagnosticGaussCycle = 1\n", "/tmp")
+    assert [n for n in range(6) if plan.gauss_begins(n, 5)] == [0, 1, 2, 3, 4]
+
+
+def test_gauss_csv(tmp_path):
+    """gauss.csv: precision lines, TPIC's column definitions and header, rows of
+    17-significant-digit numbers; a restart keeps the rows below its cycle."""
+    path = tmp_path / "data" / "gauss.csv"
+    w = GaussWriter(path, "mixed/mixed", "roles")
+    for n in (0, 2, 4):
+        w.write(GaussSample(n, (n + 0.5) * 0.15, (1e-3 * (n + 1), 0.0 if n == 0 else 1e-5 * n, 0.0, 0.1)))
+    text = path.read_text()
+    lines = text.splitlines()
+    assert lines[0] == "# precision_profile = mixed/mixed" and lines[1] == "# precision_roles = roles"
+    assert "cycle,time,residual_rms,drift_rms,wall_residual_rms,charge_rms" in lines
+    rows = [line for line in lines if line and line[0].isdigit()]
+    assert rows[1].split(",")[:2] == ["2", csv_number(2.5 * 0.15)]
+    assert [float(v) for v in rows[2].split(",")[2:]] == [5e-3, 4e-5, 0.0, 0.1]
+    assert csv_number(0.1) == "0.10000000000000001"
+    GaussWriter(path, "mixed/mixed", "roles", restart_cycle=2)
+    rows = [line for line in path.read_text().splitlines() if line and line[0].isdigit()]
+    assert [r.split(",")[0] for r in rows] == ["0"]
+    assert path.read_text().splitlines()[-1].startswith("# restart at cycle 2: precision_profile = mixed/mixed")

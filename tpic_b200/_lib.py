@@ -194,6 +194,12 @@ EXPORTS = {
                                            C.c_double, C.c_int, C.c_char_p, C.c_char_p, C.c_int]),
     "tpicb200_vtk_write_particles": (C.c_int, [C.c_char_p, C.c_int, C.c_double, C.c_int, C.c_char_p, C.c_char_p,
                                                C.c_int, C.POINTER(VtkSpecies), C.c_int]),
+    "tpicb200_vtk_write_cells": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(Grid), C.c_void_p, C.c_int, C.c_double,
+                                           C.c_int, C.c_char_p, C.c_char_p, C.c_int]),
+    "tpicb200_gauss_field": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
+                                       C.c_int, C.c_void_p, C.c_void_p]),
+    "tpicb200_gauss_charge": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(Particles), C.c_void_p, C.c_void_p,
+                                        C.c_void_p]),
 }
 
 _lib = None

@@ -26,7 +26,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relax
           "-Xptxas", "-warn-spills"]
 PER_FILE = {"mover.cu": ["-fmad=false"], "load.cu": ["-fmad=false"]}
 SOURCES = ["abi.cu", "mover.cu", "sort.cu", "deposit.cu", "fields.cu", "solver.cu", "mass_tc.cu", "cases.cu",
-           "load.cu", "checkpoint.cu", "adjoint.cu", "output.cu"]
+           "load.cu", "checkpoint.cu", "adjoint.cu", "output.cu", "gauss.cu"]
 
 
 def nvcc() -> str:

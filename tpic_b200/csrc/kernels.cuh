@@ -152,6 +152,12 @@ cudaError_t launch_assemble_moments(int precision, const Geom& g, const void* mo
 // fields.cu
 cudaError_t launch_node_ghosts(const Geom& g, double* f, int components, cudaStream_t s,
                                bool programmatic = false);
+// The output moments of one species (output.cu): rho scaled by rho_scale and,
+// where their buffers are given, J and the raw second moments, FP64 atomics
+// at the unique nodes.
+cudaError_t launch_output_moments(int precision, const Geom& g, const tpicb200_particles& p, double qom,
+                                  double rho_scale, double* rho, double* j, double* pressure, uint32_t* invalid,
+                                  cudaStream_t s);
 cudaError_t launch_smooth(bool double_arithmetic, const Geom& g, int niter, int op, double alpha,
                           const double* src, double* out, double* tmp, uint32_t* invalid, cudaStream_t s);
 cudaError_t launch_widen(int precision, const Geom& g, const void* in, double* out, cudaStream_t s);

@@ -34,11 +34,15 @@ namespace {
 
 constexpr double kFourPi = 4.0 * 3.14159265358979323846;
 
+// The output moments of one species (rho scaled by rho_scale: 4 pi for the
+// snapshot, 1 for the Gauss-law charge). A record's amounts are checked only
+// where they are requested: rho always, J and P when their buffers are given
+// (a velocity enters only those).
 template <class V>
 __global__ void __launch_bounds__(256) output_moments_kernel(Geom g, tpicb200_particles p, double inverse_volume,
-                                                           double inverse_qom, double* __restrict__ rho,
-                                                           double* __restrict__ j, double* __restrict__ pressure,
-                                                           uint32_t* invalid) {
+                                                           double inverse_qom, double rho_scale,
+                                                           double* __restrict__ rho, double* __restrict__ j,
+                                                           double* __restrict__ pressure, uint32_t* invalid) {
   const long long unique = (long long)g.nx * g.ny * g.nz;
   const V* u = (const V*)p.u;
   const V* v = (const V*)p.v;
@@ -60,7 +64,7 @@ __global__ void __launch_bounds__(256) output_moments_kernel(Geom g, tpicb200_pa
     const double charge = p.q[n] * inverse_volume;
     const double vx = double(u[n]), vy = double(v[n]), vz = double(w[n]);
     double amount[10];
-    amount[0] = charge * kFourPi;
+    amount[0] = charge * rho_scale;
     amount[1] = charge * vx;
     amount[2] = charge * vy;
     amount[3] = charge * vz;
@@ -71,9 +75,11 @@ __global__ void __launch_bounds__(256) output_moments_kernel(Geom g, tpicb200_pa
     amount[7] = mass * vy * vy;
     amount[8] = mass * vy * vz;
     amount[9] = mass * vz * vz;
-    bool finite = true;
+    bool finite = isfinite(amount[0]);
 #pragma unroll
-    for (int c = 0; c < 10; ++c) finite = finite && isfinite(amount[c]);
+    for (int c = 1; c < 4; ++c) finite = finite && (!j || isfinite(amount[c]));
+#pragma unroll
+    for (int c = 4; c < 10; ++c) finite = finite && (!pressure || isfinite(amount[c]));
     if (!finite) {
       atomicAdd(invalid, 1u);
       continue;
@@ -216,6 +222,64 @@ int launch_status(const char* what) {
 }
 
 }  // namespace
+
+cudaError_t launch_output_moments(int precision, const Geom& g, const tpicb200_particles& p, double qom,
+                                  double rho_scale, double* rho, double* j, double* pressure, uint32_t* invalid,
+                                  cudaStream_t s) {
+  if (p.count == 0) return cudaSuccess;
+  const unsigned blocks = grid_for(p.count, 256, 148u * 16u);
+  if (precision == TPICB200_PRECISION_DOUBLE)
+    output_moments_kernel<double><<<blocks, 256, 0, s>>>(g, p, g.inv_volume, 1.0 / qom, rho_scale, rho, j, pressure,
+                                                         invalid);
+  else
+    output_moments_kernel<float><<<blocks, 256, 0, s>>>(g, p, g.inv_volume, 1.0 / qom, rho_scale, rho, j, pressure,
+                                                        invalid);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+namespace {
+
+// One Float64 array of the node grid (PointData, (nx+1)(ny+1)(nz+1) tuples)
+// or of its cells (CellData, nx ny nz tuples) as VTK XML ImageData.
+int write_image(bool cells, const char* path, const char* name, int components, const tpicb200_grid* grid,
+                const double* values, int cycle, double time, int final_state, const char* profile, const char* roles,
+                int overwrite) {
+  if (!path || !name || !grid || !values || components < 1)
+    return report_error(TPICB200_INVALID_ARGUMENT, "vtk field: null argument or no components");
+  if (grid->nx < 1 || grid->ny < 1 || grid->nz < 1) return report_error(TPICB200_INVALID_ARGUMENT, "vtk field: empty grid");
+  const std::string extent = "0 " + std::to_string(grid->nx) + " 0 " + std::to_string(grid->ny) + " 0 " +
+                             std::to_string(grid->nz);
+  std::string xml;
+  file_open(xml, "ImageData");
+  xml += "  <ImageData WholeExtent=\"" + extent + "\" Origin=\"0 0 0\" Spacing=\"" + number(grid->lx / grid->nx) +
+         " " + number(grid->ly / grid->ny) + " " + number(grid->lz / grid->nz) + "\">\n";
+  field_data(xml, cycle, time, final_state, profile, roles);
+  xml += "    <Piece Extent=\"" + extent + "\">\n";
+  if (cells) {
+    xml += "      <PointData/>\n      <CellData>\n";
+    data_array(xml, "Float64", name, components, 0);
+    xml += "      </CellData>\n";
+  } else {
+    xml += "      <PointData>\n";
+    data_array(xml, "Float64", name, components, 0);
+    xml += "      </PointData>\n      <CellData/>\n";
+  }
+  xml += "    </Piece>\n  </ImageData>\n";
+  xml += kAppendedOpen;
+  const int extra = cells ? 0 : 1;
+  const uint64_t points = uint64_t(grid->nx + extra) * uint64_t(grid->ny + extra) * uint64_t(grid->nz + extra);
+  const uint64_t bytes = points * uint64_t(components) * sizeof(double);
+  File f(path, overwrite);
+  f.text(xml);
+  f.value(bytes);
+  f.write(values, bytes);
+  f.text(kAppendedClose);
+  if (!f.close()) return file_error(path);
+  return TPICB200_SUCCESS;
+}
+
+}  // namespace
 }  // namespace tpicb200
 
 using namespace tpicb200;
@@ -229,17 +293,11 @@ int tpicb200_output_moments(tpicb200_context* ctx, double qom, const tpicb200_pa
   if (!std::isfinite(qom) || qom == 0)
     return report_error(TPICB200_INVALID_ARGUMENT, "output moments need a finite nonzero q/m");
   if (p->count == 0 || (!rho && !j && !pressure)) return TPICB200_SUCCESS;
-  const Geom& g = context_geom(ctx);
-  cudaStream_t s = (cudaStream_t)stream;
-  const unsigned blocks = grid_for(p->count, 256, 148u * 16u);
-  if (context_options(ctx).precision == TPICB200_PRECISION_DOUBLE)
-    output_moments_kernel<double><<<blocks, 256, 0, s>>>(g, *p, g.inv_volume, 1.0 / qom, rho, j, pressure,
-                                                         context_invalid(ctx));
-  else
-    output_moments_kernel<float><<<blocks, 256, 0, s>>>(g, *p, g.inv_volume, 1.0 / qom, rho, j, pressure,
-                                                        context_invalid(ctx));
-  count_launches(1);
-  return launch_status("output moments launch failed");
+  const cudaError_t e = launch_output_moments(context_options(ctx).precision, context_geom(ctx), *p, qom, kFourPi, rho,
+                                              j, pressure, context_invalid(ctx), (cudaStream_t)stream);
+  if (e != cudaSuccess)
+    return report_error(TPICB200_BACKEND_FAILURE, std::string("output moments launch failed: ") + cudaGetErrorString(e));
+  return TPICB200_SUCCESS;
 }
 
 int tpicb200_output_particles(tpicb200_context* ctx, const tpicb200_particles* p, double* position, double* velocity,
@@ -261,29 +319,13 @@ int tpicb200_output_particles(tpicb200_context* ctx, const tpicb200_particles* p
 int tpicb200_vtk_write_field(const char* path, const char* name, int components, const tpicb200_grid* grid,
                              const double* values, int cycle, double time, int final_state, const char* profile,
                              const char* roles, int overwrite) {
-  if (!path || !name || !grid || !values || components < 1)
-    return report_error(TPICB200_INVALID_ARGUMENT, "vtk field: null argument or no components");
-  if (grid->nx < 1 || grid->ny < 1 || grid->nz < 1) return report_error(TPICB200_INVALID_ARGUMENT, "vtk field: empty grid");
-  const std::string extent = "0 " + std::to_string(grid->nx) + " 0 " + std::to_string(grid->ny) + " 0 " +
-                             std::to_string(grid->nz);
-  std::string xml;
-  file_open(xml, "ImageData");
-  xml += "  <ImageData WholeExtent=\"" + extent + "\" Origin=\"0 0 0\" Spacing=\"" + number(grid->lx / grid->nx) +
-         " " + number(grid->ly / grid->ny) + " " + number(grid->lz / grid->nz) + "\">\n";
-  field_data(xml, cycle, time, final_state, profile, roles);
-  xml += "    <Piece Extent=\"" + extent + "\">\n      <PointData>\n";
-  data_array(xml, "Float64", name, components, 0);
-  xml += "      </PointData>\n      <CellData/>\n    </Piece>\n  </ImageData>\n";
-  xml += kAppendedOpen;
-  const uint64_t points = uint64_t(grid->nx + 1) * uint64_t(grid->ny + 1) * uint64_t(grid->nz + 1);
-  const uint64_t bytes = points * uint64_t(components) * sizeof(double);
-  File f(path, overwrite);
-  f.text(xml);
-  f.value(bytes);
-  f.write(values, bytes);
-  f.text(kAppendedClose);
-  if (!f.close()) return file_error(path);
-  return TPICB200_SUCCESS;
+  return write_image(false, path, name, components, grid, values, cycle, time, final_state, profile, roles, overwrite);
+}
+
+int tpicb200_vtk_write_cells(const char* path, const char* name, const tpicb200_grid* grid, const double* values,
+                             int cycle, double time, int final_state, const char* profile, const char* roles,
+                             int overwrite) {
+  return write_image(true, path, name, 1, grid, values, cycle, time, final_state, profile, roles, overwrite);
 }
 
 int tpicb200_vtk_write_particles(const char* directory, int cycle, double time, int final_state, const char* profile,

@@ -19,6 +19,7 @@ HDF5 engines of TPIC are optional there too and are refused here.
 from __future__ import annotations
 
 import ctypes as C
+import math
 import re
 from dataclasses import dataclass, field
 from pathlib import Path
@@ -58,6 +59,7 @@ class OutputPlan:
     field_method: str = ""
     particles_method: str = ""
     overwrite: bool = True
+    gauss_cycle: int = 0
     written: list = field(default_factory=list)
 
     @classmethod
@@ -69,7 +71,8 @@ class OutputPlan:
                    particles_cycle=int(k.get("ParticlesOutputCycle", 0)),
                    field_tag=k.get("FieldOutputTag", ""), moments_tag=k.get("MomentsOutputTag", ""),
                    field_method=k.get("FieldWriteMethod", "") or method,
-                   particles_method=k.get("ParticlesWriteMethod", "") or method)
+                   particles_method=k.get("ParticlesWriteMethod", "") or method,
+                   gauss_cycle=int(k.get("DiagnosticGaussCycle", 0)))
         for name, value in override.items():
             if value is not None:
                 setattr(plan, name, value)
@@ -91,6 +94,32 @@ class OutputPlan:
         f = self.field_cycle > 0 and (final or cycle % self.field_cycle == 0)
         p = self.particles_cycle > 0 and (final or cycle % self.particles_cycle == 0)
         return f, p
+
+    @property
+    def output_gauss(self) -> bool:
+        """The FieldOutputTag token Gauss, effective with a field channel."""
+        return self.field_cycle > 0 and "Gauss" in _tokens(self.field_tag, "FieldOutputTag")
+
+    def gauss_enabled(self) -> bool:
+        return self.gauss_cycle > 0 or self.output_gauss
+
+    def next_gauss_begin(self, cycle: int, last: int) -> int | None:
+        """The first cycle after `cycle` at which a sample begins, if any."""
+        for m in range(cycle + 1, last):
+            if self.gauss_begins(m, last):
+                return m
+        return None
+
+    def gauss_begins(self, cycle: int, last: int) -> bool:
+        """A Gauss-law sample begins at cycle n < last when n is a multiple of
+        DiagnosticGaussCycle, or, with the Gauss array selected, when n + 1 is
+        a field snapshot cycle or the final state (PreparedOutput::
+        should_sample_gauss, src/config/output.cpp)."""
+        if cycle >= last:
+            return False
+        if self.gauss_cycle > 0 and cycle % self.gauss_cycle == 0:
+            return True
+        return self.output_gauss and ((cycle + 1) % self.field_cycle == 0 or cycle + 1 == last)
 
 
 def _tokens(tag: str, key: str) -> list[str]:
@@ -116,8 +145,6 @@ def select_arrays(field_tag: str, moments_tag: str, ns: int):
     for t in ftok:
         if t not in ("B", "E", "Gauss"):
             raise ValueError(f"FieldOutputTag: unknown token {t!r}")
-        if t == "Gauss":
-            raise ValueError("FieldOutputTag: the Gauss-law residual array is not built")
         if t not in fields:
             fields.append(t)
     totals, indexed, bare = [], {}, []
@@ -185,8 +212,10 @@ def _grid(sim) -> _lib.Grid:
     return _lib.Grid(g.nx, g.ny, g.nz, g.lx, g.ly, g.lz)
 
 
-def write_fields(sim, plan: OutputPlan, cycle: int, final: bool) -> list[Path]:
-    """The field snapshot of the simulation's current state at `cycle`."""
+def write_fields(sim, plan: OutputPlan, cycle: int, final: bool, gauss: "GaussSampler | None" = None) -> list[Path]:
+    """The field snapshot of the simulation's current state at `cycle`; with
+    the Gauss array selected, the residual of the sample that finished at
+    `cycle` as cell data (absent when none did)."""
     lib = sim.lib
     g = sim.case.grid
     ns = len(sim.case.species)
@@ -207,6 +236,13 @@ def write_fields(sim, plan: OutputPlan, cycle: int, final: bool) -> list[Path]:
         written.append(path)
 
     sim.materialize()
+    if "Gauss" in fields and gauss is not None and gauss.finished is not None and gauss.finished + 1 == cycle:
+        path = plan.save_dir / f"Gauss_t{cycle:06d}.vti"
+        values = np.ascontiguousarray(gauss.residual_cells(), dtype=np.float64)
+        _lib.check(lib.tpicb200_vtk_write_cells(str(path).encode(), b"Gauss", C.byref(_grid(sim)), values.ctypes.data,
+                                                cycle, time, int(final), profile.encode(), roles.encode(),
+                                                int(plan.overwrite)))
+        written.append(path)
     if "E" in fields:
         put("E", _nodes(sim, "e"), 3)
     if "B" in fields:
@@ -284,3 +320,130 @@ def write_particles(sim, plan: OutputPlan, cycle: int, final: bool) -> Path:
     path = plan.save_dir / f"particles_t{cycle:06d}.pvtp"
     plan.written.append(path)
     return path
+
+
+GAUSS_HEADER = (
+    "# TPIC Gauss-law residual v1\n"
+    "# A sample begins at cycle n and finishes at n + 1: per cell r = (divC(E^n) + divC(E^{n+1}))/2 - c, where divC is\n"
+    "# the solver's node-to-cell divergence and c = 4*pi times the eight-node mean of the charge density of the particles\n"
+    "# at x^{n+1/2} (dual-volume scaled, zero on PEC wall nodes, smoothed like the solver's current). time = (n + 1/2)*dt.\n"
+    "# Root mean squares over the global cells: residual_rms of r; drift_rms of r minus the first finished sample of the\n"
+    "# run (a restart starts a new baseline); wall_residual_rms of r over the cells touching a physical wall (0 without\n"
+    "# walls); charge_rms of c.\n"
+    "cycle,time,residual_rms,drift_rms,wall_residual_rms,charge_rms\n")
+
+
+def csv_number(value: float) -> str:
+    """A double as TPIC's CSV rows print it: general format, 17 significant
+    digits (io::detail::CsvBuffer::append, src/io/diagnostics_writer.cpp:31-34)."""
+    return format(value, ".17g")
+
+
+@dataclass
+class GaussSample:
+    cycle: int             # the begin cycle n
+    time: float            # (n + 1/2) dt
+    rms: tuple             # residual, drift, wall, charge
+
+    def row(self) -> str:
+        return ",".join([str(self.cycle), csv_number(self.time)] + [csv_number(v) for v in self.rms])
+
+
+class GaussSampler:
+    """The Gauss-law residual samples of a Simulation
+    (diagnostics/gauss_residual_device.hpp, docs/developer/gauss_diagnostic.md):
+    begin(n) at state n stores divC(E^n)/2 - c per cell, finish() at state
+    n + 1 adds divC(E^{n+1})/2 and returns the sample's root mean squares;
+    `residual` holds r of the last finished sample. The cell buffers are FP64
+    device tensors of the nx*ny*nz cells; the kernels are the library's
+    (tpicb200_gauss_field, tpicb200_gauss_charge)."""
+
+    def __init__(self, sim):
+        g = sim.case.grid
+        self.sim = sim
+        self.cells = g.nx * g.ny * g.nz
+        mk = lambda: torch.zeros(self.cells, dtype=torch.float64, device=sim.device)
+        self.stash, self.first, self.residual = mk(), mk(), mk()
+        self.sums = torch.zeros(4, dtype=torch.float64, device=sim.device)
+        self.begun = None        # the begin cycle of the open sample
+        self.first_set = False
+        self.finished = None     # the begin cycle of the last finished sample
+
+    def _species(self):
+        sim = self.sim
+        st = sim.state
+        ns = st.ns
+        sim.materialize()
+        return ns, (_lib.Particles * max(ns, 1))(*[st.slot[s][st.current[s]] for s in range(ns)])
+
+    def step(self, cycle: int, begin: bool) -> GaussSample | None:
+        """At state `cycle`: finish the open sample (begun at cycle - 1), then
+        begin a new one when `begin`; returns the finished sample, if any."""
+        sim = self.sim
+        lib = sim.lib
+        stream = C.c_void_p(sim.stream.cuda_stream)
+        finish = self.begun is not None
+        if finish and self.begun != cycle - 1:
+            raise RuntimeError("a Gauss sample finishes at the cycle after its begin")
+        if not finish and not begin:
+            return None
+        e = sim.state.e
+        _lib.check(lib.tpicb200_gauss_field(sim.ctx, e, self.stash.data_ptr(), self.first.data_ptr(),
+                                            self.residual.data_ptr(), int(begin), int(finish),
+                                            int(finish and not self.first_set), self.sums.data_ptr(), stream))
+        sample = None
+        if finish:
+            sim.stream.synchronize()
+            s = self.sums.cpu().numpy()
+            rms = (math.sqrt(s[0] / self.cells), math.sqrt(s[1] / self.cells), 0.0)
+            # The charge sum was taken at the begin.
+            rms = rms + (math.sqrt(self.charge_sum / self.cells),)
+            if not all(math.isfinite(v) for v in rms):
+                raise ValueError("Gauss residual: nonfinite sample")
+            sample = GaussSample(self.begun, (self.begun + 0.5) * sim.case.dt, rms)
+            self.first_set = True
+            self.finished = self.begun
+            self.begun = None
+        if begin:
+            ns, species = self._species()
+            _lib.check(lib.tpicb200_gauss_charge(sim.ctx, ns, species, self.stash.data_ptr(), self.sums.data_ptr(),
+                                                 stream))
+            sim.stream.synchronize()
+            count = C.c_uint32(0)
+            _lib.check(lib.tpicb200_read_invalid(sim.ctx, C.byref(count), 0, stream))
+            if count.value:
+                raise ValueError("Gauss residual: invalid records in the sampled state")
+            self.charge_sum = float(self.sums[3].item())
+            self.begun = cycle
+        return sample
+
+    def residual_cells(self) -> np.ndarray:
+        """r of the last finished sample as a host array of the nx*ny*nz cells."""
+        return self.residual.cpu().numpy()
+
+
+class GaussWriter:
+    """gauss.csv under SaveDirName (io::GaussWriter, src/io/diagnostics_writer.cpp:215-232):
+    the precision header, the column definitions and one row per finished sample;
+    a restart keeps the rows below its cycle and adds a restart line."""
+
+    def __init__(self, path: Path, profile: str, roles: str, restart_cycle: int | None = None):
+        self.path = Path(path)
+        self.path.parent.mkdir(parents=True, exist_ok=True)
+        head = f"# precision_profile = {profile}\n# precision_roles = {roles}\n" + GAUSS_HEADER
+        if restart_cycle is None or not self.path.exists():
+            self.path.write_text(head if restart_cycle is None else
+                                 head + f"# restart at cycle {restart_cycle}: precision_profile = {profile}, "
+                                        f"precision_roles = {roles}\n")
+            return
+        kept = []
+        for line in self.path.read_text().splitlines():
+            if line and line[0].isdigit() and int(line.split(",")[0]) >= restart_cycle:
+                continue
+            kept.append(line)
+        kept.append(f"# restart at cycle {restart_cycle}: precision_profile = {profile}, precision_roles = {roles}")
+        self.path.write_text("\n".join(kept) + "\n")
+
+    def write(self, sample: GaussSample) -> None:
+        with open(self.path, "a") as f:
+            f.write(sample.row() + "\n")

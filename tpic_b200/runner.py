@@ -90,12 +90,14 @@ def parse_args(argv=None):
                     help="ParticlesOutputCycle (default: the deck's, else 0: no particle snapshots)")
     ap.add_argument("--save-dir", default=None, help="SaveDirName of the snapshots, under --output (default: the "
                                                      "deck's, else data)")
+    ap.add_argument("--gauss-cycle", type=int, default=None,
+                    help="DiagnosticGaussCycle (default: the deck's, else 0: no Gauss-law samples)")
     return ap.parse_args(argv)
 
 
 def run(args) -> int:
     from .simulation import Simulation
-    from .output import OutputPlan, write_fields, write_particles
+    from .output import GaussSampler, GaussWriter, OutputPlan, precision_strings, write_fields, write_particles
     text = Path(args.run).read_text()
     deck = D.parse(text)
     case = D.to_case(deck, seed=args.seed)
@@ -106,7 +108,7 @@ def run(args) -> int:
     ckpt_dir = out / args.restart_dir
     csv_path = out / "diagnostics.csv"
     plan = OutputPlan.from_deck(text, out, field_cycle=args.field_output_cycle,
-                                particles_cycle=args.particles_output_cycle)
+                                particles_cycle=args.particles_output_cycle, gauss_cycle=args.gauss_cycle)
     if args.save_dir is not None:
         plan.save_dir = out / args.save_dir
     kw = dict(precision=args.precision, mass_kind=form, device=args.device,
@@ -141,6 +143,12 @@ def run(args) -> int:
         initial = field[0] + field[1] + sum(sp[0] for sp in species)
     cadence = args.diagnostics_cycle if args.diagnostics_cycle > 0 else 0
     ckpt = args.restart_cycle if args.restart_cycle > 0 else 0
+    gauss = gauss_writer = None
+    if plan.gauss_enabled():
+        gauss = GaussSampler(sim)
+        profile, roles = precision_strings(sim)
+        gauss_writer = GaussWriter(plan.save_dir / "gauss.csv", profile, roles,
+                                   restart_cycle=sim.cycle if args.restart else None)
 
     def record(final: bool) -> None:
         line = row(sim.cycle, case.dt, final, field, species, initial)
@@ -149,16 +157,27 @@ def run(args) -> int:
         total = field[0] + field[1] + sum(sp[0] for sp in species)
         print(f"cycle {sim.cycle:6d}  total energy {total:.10e}  change {total - initial:+.3e}", flush=True)
 
+    def gauss_step() -> None:
+        if gauss is None:
+            return
+        sample = gauss.step(sim.cycle, plan.gauss_begins(sim.cycle, last))
+        if sample is not None:
+            gauss_writer.write(sample)
+            r, d, w, c = sample.rms
+            print(f"  Gauss residual: cycle {sample.cycle} t = {sample.time:e}  rms = {r:e}  drift = {d:e}  "
+                  f"wall = {w:e}  charge = {c:e}", flush=True)
+
     def snapshots() -> None:
         final = sim.cycle == last
         fields_due, particles_due = plan.due(sim.cycle, final)
         if fields_due:
-            write_fields(sim, plan, sim.cycle, final)
+            write_fields(sim, plan, sim.cycle, final, gauss)
         if particles_due:
             write_particles(sim, plan, sim.cycle, final)
 
     if (cadence and sim.cycle % cadence == 0) or sim.cycle == last:
         record(sim.cycle == last)
+    gauss_step()
     snapshots()
     while sim.cycle < last:
         stops = [last]
@@ -169,6 +188,12 @@ def run(args) -> int:
         for channel in (plan.field_cycle, plan.particles_cycle):
             if channel > 0:
                 stops.append((sim.cycle // channel + 1) * channel)
+        if gauss is not None:
+            if gauss.begun is not None:
+                stops.append(gauss.begun + 1)
+            nxt = plan.next_gauss_begin(sim.cycle, last)
+            if nxt is not None:
+                stops.append(nxt)
         n = min(stops) - sim.cycle
         reports = sim.run(n)
         r = reports[-1]
@@ -177,6 +202,7 @@ def run(args) -> int:
             sim.checkpoint(ckpt_dir)
         if sim.cycle == last or (cadence and sim.cycle % cadence == 0):
             record(sim.cycle == last)
+        gauss_step()
         snapshots()
         if not all(math.isfinite(x) for x in field):
             raise SystemExit("nonfinite field energy")
