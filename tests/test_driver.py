@@ -40,7 +40,7 @@ def test_bad_command_lines(driver, tmp_path):
 
 
 TAGS = [("", ""), ("B", ""), ("", "rho+rho0"), ("E", "J_tot+PXX1+PZZ+rho5"), ("E+B", "PXY+PXY_tot+J1+J0"),
-        ("", "rho007")]
+        ("", "rho007"), ("Gauss+B+E", "rho")]
 
 
 @pytest.mark.parametrize("field_tag,moments_tag", TAGS)
@@ -73,7 +73,7 @@ def test_snapshot_selection_matches_the_runner(driver, tmp_path, field_tag, mome
     assert "particles every 7 cycles" in over.stdout
 
 
-@pytest.mark.parametrize("keys", ["FieldOutputTag = EB\n", "FieldOutputTag = B+\n", "FieldOutputTag = Gauss\n",
+@pytest.mark.parametrize("keys", ["FieldOutputTag = EB\n", "FieldOutputTag = B+\n", "FieldOutputTag = Gauss+Q\n",
                                   "MomentsOutputTag = rhoJ\n", "MomentsOutputTag = rho-1\n",
                                   "MomentsOutputTag = PXX_totally\n", "MomentsOutputTag = rho++J\n",
                                   "MomentsOutputTag = rho2147483648\n", "WriteMethod = hdf5\n",
@@ -88,3 +88,17 @@ def test_bad_snapshot_keys(driver, tmp_path, keys):
     ok.write_text(DECKS[0].read_text() + "WriteMethod = hdf5\nFieldOutputCycle = 0\n")
     done = subprocess.run([driver, "--run", str(ok), "--dry-run"], capture_output=True, text=True, timeout=60)
     assert done.returncode == 0, done.stderr
+
+
+def test_gauss_cadence_of_the_driver(driver, tmp_path):
+    """--dry-run prints the Gauss-law cadence: DiagnosticGaussCycle (or
+    --gauss-cycle) and, with the Gauss array on a field channel, the samples
+    before each field snapshot."""
+    deck = tmp_path / "g.inp"
+    deck.write_text(DECKS[0].read_text() + "DiagnosticGaussCycle = 4\nFieldOutputCycle = 5\nFieldOutputTag = E+Gauss\n")
+    done = subprocess.run([driver, "--run", str(deck), "--dry-run"], capture_output=True, text=True, timeout=60)
+    assert done.returncode == 0, done.stderr
+    assert "Gauss-law samples every 4 cycles and before each field snapshot" in done.stdout
+    done = subprocess.run([driver, "--run", str(deck), "--dry-run", "--gauss-cycle", "0", "--field-output-cycle", "0"],
+                          capture_output=True, text=True, timeout=60)
+    assert "Gauss-law samples every 0 cycles\n" in done.stdout

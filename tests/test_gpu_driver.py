@@ -119,3 +119,36 @@ def test_driver_snapshots_match_the_python_runner(tmp_path):
         else:
             scale = max(np.abs(xb[key]).max(), 1e-300)
             assert np.abs(xa[key] - xb[key]).max() <= 1e-12 * scale, name
+
+
+def test_driver_gauss_rows_match_the_python_runner(tmp_path):
+    """A shrunk C1 deck with Gauss-law samples every cycle and the Gauss array
+    on the field snapshots, run by the driver and by the runner: the same
+    gauss.csv cycles and times, the root mean squares and the Gauss arrays
+    to rounding (the charge is summed with FP64 atomics)."""
+    from vtkread import read
+    B.build()
+    deck = tmp_path / "gauss.inp"
+    deck.write_text(C1.read_text() + "\nDiagnosticGaussCycle = 1\nFieldOutputCycle = 2\nFieldOutputTag = E+Gauss\n")
+    a, b = tmp_path / "cpp", tmp_path / "py"
+    args = ["--run", str(deck), "--cycles", "3"]
+    driver(*args, "--output", str(a), cwd=tmp_path)
+    done = subprocess.run([sys.executable, "-m", "tpic_b200", *args, "--output", str(b)], capture_output=True,
+                          text=True, timeout=600, cwd=ROOT)
+    assert done.returncode == 0, done.stdout + done.stderr
+
+    def gauss_rows(path):
+        lines = (path / "data" / "gauss.csv").read_text().splitlines()
+        return lines[:2], np.array([[float(v) for v in line.split(",")] for line in lines if line and line[0].isdigit()])
+
+    head_a, x = gauss_rows(a)
+    head_b, y = gauss_rows(b)
+    assert head_a == head_b
+    assert x.shape == y.shape == (3, 6)
+    assert np.array_equal(x[:, :2], y[:, :2])
+    assert np.allclose(x[:, 2:], y[:, 2:], rtol=1e-10, atol=0)
+    for cycle in (2, 3):
+        ga = read(a / "data" / f"Gauss_t{cycle:06d}.vti")[1]["Gauss"]
+        gb = read(b / "data" / f"Gauss_t{cycle:06d}.vti")[1]["Gauss"]
+        assert np.abs(ga - gb).max() <= 1e-12 * np.abs(gb).max()
+    assert not (a / "data" / "Gauss_t000000.vti").exists()

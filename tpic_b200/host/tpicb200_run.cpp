@@ -4,7 +4,7 @@
 //                [--precision mixed|double] [--restart] [--output DIR] [--cycles N]
 //                [--diagnostics-cycle K] [--restart-cycle R] [--restart-dir NAME] [--seed S]
 //                [--gmres-max-iterations M] [--device D] [--field-output-cycle F]
-//                [--particles-output-cycle P] [--save-dir NAME] [--dry-run]
+//                [--particles-output-cycle P] [--save-dir NAME] [--gauss-cycle K] [--dry-run]
 //
 // The command line of TPIC's one-rank run (`tpic --run deck.inp --mass-matrix
 // scalar|matrix-core [--restart]`, src/app/main.cpp:60-127), as a C++ host
@@ -53,8 +53,8 @@ struct Args {
   int diagnostics_cycle = 1, restart_cycle = 0, gmres_max_iterations = 100, device = 0;
   unsigned long long seed = 0;
   // Snapshot overrides of the deck's keys (unset: the deck's value).
-  bool has_field_cycle = false, has_particles_cycle = false, has_save_dir = false;
-  int field_cycle = 0, particles_cycle = 0;
+  bool has_field_cycle = false, has_particles_cycle = false, has_save_dir = false, has_gauss_cycle = false;
+  int field_cycle = 0, particles_cycle = 0, gauss_cycle = 0;
   std::string save_dir;
 };
 
@@ -65,7 +65,7 @@ struct Args {
                "moments-f64] [--precision mixed|double] [--restart] [--output DIR] [--cycles N] "
                "[--diagnostics-cycle K] [--restart-cycle R] [--restart-dir NAME] [--seed S] "
                "[--gmres-max-iterations M] [--device D] [--field-output-cycle F] [--particles-output-cycle P] "
-               "[--save-dir NAME] [--dry-run]\n");
+               "[--save-dir NAME] [--gauss-cycle K] [--dry-run]\n");
   std::exit(2);
 }
 
@@ -99,6 +99,9 @@ Args parse_args(int argc, char** argv) {
     } else if (k == "--save-dir") {
       a.has_save_dir = true;
       a.save_dir = value(i);
+    } else if (k == "--gauss-cycle") {
+      a.has_gauss_cycle = true;
+      a.gauss_cycle = std::atoi(value(i).c_str());
     }
     else if (k == "--help" || k == "-h") usage("help");
     else usage(("unknown option " + k).c_str());
@@ -278,13 +281,32 @@ struct MomentArray {
 struct OutputPlan {
   std::string save_dir;
   int field_cycle = 100, particles_cycle = 0;
-  bool e = false, b = false;
+  int gauss_cycle = 0;                 // DiagnosticGaussCycle
+  bool e = false, b = false, gauss = false;
+  std::vector<std::string> fields;     // the field arrays in tag order
   std::vector<MomentArray> moments;
   bool fields_due(long long cycle, bool final) const {
     return field_cycle > 0 && (final || cycle % field_cycle == 0);
   }
   bool particles_due(long long cycle, bool final) const {
     return particles_cycle > 0 && (final || cycle % particles_cycle == 0);
+  }
+  // The Gauss array selected, with a field channel to write it.
+  bool output_gauss() const { return gauss && field_cycle > 0; }
+  bool gauss_enabled() const { return gauss_cycle > 0 || output_gauss(); }
+  // A Gauss-law sample begins at cycle n < last at the multiples of
+  // DiagnosticGaussCycle and, with the Gauss array, one cycle before every
+  // field snapshot and before the final state (PreparedOutput::
+  // should_sample_gauss, src/config/output.cpp).
+  bool gauss_begins(long long n, long long last) const {
+    if (n >= last) return false;
+    if (gauss_cycle > 0 && n % gauss_cycle == 0) return true;
+    return output_gauss() && ((n + 1) % field_cycle == 0 || n + 1 == last);
+  }
+  long long next_gauss_begin(long long n, long long last) const {
+    for (long long m = n + 1; m < last; ++m)
+      if (gauss_begins(m, last)) return m;
+    return -1;
   }
 };
 
@@ -323,6 +345,7 @@ OutputPlan output_plan(const std::string& text, const Args& args, int ns) {
   plan.field_cycle = args.has_field_cycle ? args.field_cycle : std::atoi(get("FieldOutputCycle", "100").c_str());
   plan.particles_cycle =
       args.has_particles_cycle ? args.particles_cycle : std::atoi(get("ParticlesOutputCycle", "0").c_str());
+  plan.gauss_cycle = args.has_gauss_cycle ? args.gauss_cycle : std::atoi(get("DiagnosticGaussCycle", "0").c_str());
   const std::string method = get("WriteMethod", "");
   const std::pair<const char*, int> channels[2] = {{"FieldWriteMethod", plan.field_cycle},
                                                    {"ParticlesWriteMethod", plan.particles_cycle}};
@@ -340,6 +363,7 @@ OutputPlan output_plan(const std::string& text, const Args& args, int ns) {
   const std::vector<std::string> mtok = tag_tokens(get("MomentsOutputTag", ""), "MomentsOutputTag");
   if (ftok.empty() && mtok.empty()) {
     plan.e = plan.b = true;
+    plan.fields = {"E", "B"};
     for (int q = 0; q < 2; ++q) plan.moments.push_back({kMoments[q], q, -1});
     for (int q = 0; q < 2; ++q)
       for (int s = 0; s < ns; ++s) plan.moments.push_back({std::string(kMoments[q]) + "_" + std::to_string(s), q, s});
@@ -348,8 +372,9 @@ OutputPlan output_plan(const std::string& text, const Args& args, int ns) {
   for (const std::string& t : ftok) {
     if (t == "E") plan.e = true;
     else if (t == "B") plan.b = true;
-    else if (t == "Gauss") fail("FieldOutputTag: the Gauss-law residual array is not built");
+    else if (t == "Gauss") plan.gauss = true;
     else fail("FieldOutputTag: unknown token '" + t + "'");
+    if (std::find(plan.fields.begin(), plan.fields.end(), t) == plan.fields.end()) plan.fields.push_back(t);
   }
   bool total[8] = {}, bare[8] = {};
   std::vector<bool> indexed(8 * size_t(ns), false);
@@ -446,11 +471,75 @@ std::vector<double> wrap_unique(const double* u, int components, size_t stride, 
   return out;
 }
 
+// The Gauss-law samples of a run (docs/developer/gauss_diagnostic.md): the
+// cell buffers on the device (tpicb200_gauss_field / _charge) and gauss.csv.
+struct GaussRun {
+  bool on = false;
+  double *stash = nullptr, *first = nullptr, *residual = nullptr, *sums = nullptr;
+  long long cells = 0;
+  long long begun = -1, finished = -1;  // begin cycle of the open / last finished sample
+  bool first_set = false;
+  double charge_sum = 0.0;
+  std::string csv;
+};
+
+const char* kGaussHeader =
+    "# TPIC Gauss-law residual v1\n"
+    "# A sample begins at cycle n and finishes at n + 1: per cell r = (divC(E^n) + divC(E^{n+1}))/2 - c, where divC is\n"
+    "# the solver's node-to-cell divergence and c = 4*pi times the eight-node mean of the charge density of the particles\n"
+    "# at x^{n+1/2} (dual-volume scaled, zero on PEC wall nodes, smoothed like the solver's current). time = (n + 1/2)*dt.\n"
+    "# Root mean squares over the global cells: residual_rms of r; drift_rms of r minus the first finished sample of the\n"
+    "# run (a restart starts a new baseline); wall_residual_rms of r over the cells touching a physical wall (0 without\n"
+    "# walls); charge_rms of c.\n"
+    "cycle,time,residual_rms,drift_rms,wall_residual_rms,charge_rms\n";
+
+// A double as TPIC's CSV rows print it: 17 significant digits, general format.
+std::string csv_number(double v) {
+  char buf[40];
+  std::snprintf(buf, sizeof(buf), "%.17g", v);
+  return buf;
+}
+
+// gauss.csv: the precision lines and the header; a restart keeps the rows
+// below its cycle and adds its restart line.
+void open_gauss_csv(const std::string& path, bool dbl, long long restart_cycle) {
+  const auto [profile, roles] = precision_strings(dbl);
+  const std::string head = "# precision_profile = " + profile + "\n# precision_roles = " + roles + "\n" + kGaussHeader;
+  std::vector<std::string> kept;
+  if (restart_cycle >= 0 && file_exists(path)) {
+    std::ifstream old(path);
+    std::string line;
+    while (std::getline(old, line)) {
+      if (!line.empty() && std::isdigit((unsigned char)line[0]) && std::atoll(line.c_str()) >= restart_cycle) continue;
+      kept.push_back(line);
+    }
+  } else {
+    std::stringstream h(head);
+    std::string line;
+    while (std::getline(h, line)) kept.push_back(line);
+  }
+  if (restart_cycle >= 0)
+    kept.push_back("# restart at cycle " + std::to_string(restart_cycle) + ": precision_profile = " + profile +
+                   ", precision_roles = " + roles);
+  std::ofstream f(path);
+  for (const std::string& line : kept) f << line << "\n";
+}
+
 // The field snapshot of the state at `cycle` (the records materialized):
 // E and B at the nodes and the selected output moments, one .vti per array.
 void write_fields(tpicb200_context* ctx, const tpicb200_state& st, const tpicb200_grid& g, const OutputPlan& plan,
-                  int ns, bool dbl, long long cycle, double time, bool final, cudaStream_t stream) {
+                  int ns, bool dbl, long long cycle, double time, bool final, const GaussRun& gauss,
+                  cudaStream_t stream) {
   const auto [profile, roles] = precision_strings(dbl);
+  // The Gauss array: r of the sample that finished at this cycle, as cell data.
+  if (plan.output_gauss() && gauss.on && gauss.finished >= 0 && gauss.finished + 1 == cycle) {
+    std::vector<double> r(gauss.cells);
+    cuda(cudaMemcpyAsync(r.data(), gauss.residual, r.size() * 8, cudaMemcpyDeviceToHost, stream), "Gauss read");
+    cuda(cudaStreamSynchronize(stream), "Gauss read");
+    check(tpicb200_vtk_write_cells(tagged(plan.save_dir, "Gauss", cycle, ".vti").c_str(), "Gauss", &g, r.data(),
+                                   int(cycle), time, final ? 1 : 0, profile.c_str(), roles.c_str(), 1),
+          "Gauss snapshot");
+  }
   auto put = [&](const std::string& name, const std::vector<double>& values, int components) {
     check(tpicb200_vtk_write_field(tagged(plan.save_dir, name, cycle, ".vti").c_str(), name.c_str(), components, &g,
                                    values.data(), int(cycle), time, final ? 1 : 0, profile.c_str(), roles.c_str(),
@@ -566,16 +655,17 @@ int main(int argc, char** argv) {
     std::printf(" records, %lld cycles, mass form %d, %s precision\n", last, kind, args.precision.c_str());
     std::printf("snapshots under %s: fields every %d cycles (", plan.save_dir.c_str(), plan.field_cycle);
     const char* sep = "";
-    for (const char* f : {"E", "B"})
-      if ((f[0] == 'E' && plan.e) || (f[0] == 'B' && plan.b)) {
-        std::printf("%s%s", sep, f);
-        sep = " ";
-      }
+    for (const std::string& f : plan.fields) {
+      std::printf("%s%s", sep, f.c_str());
+      sep = " ";
+    }
     for (const MomentArray& m : plan.moments) {
       std::printf("%s%s", sep, m.name.c_str());
       sep = " ";
     }
     std::printf("), particles every %d cycles\n", plan.particles_cycle);
+    std::printf("Gauss-law samples every %d cycles%s\n", plan.gauss_cycle,
+                plan.output_gauss() ? " and before each field snapshot" : "");
     return 0;
   }
 
@@ -690,6 +780,18 @@ int main(int argc, char** argv) {
     f << kHeader << columns(deck.ns) << "\n";
   }
   if (last < cycle) usage("the run's last cycle lies before the checkpoint cycle");
+  GaussRun gauss;
+  if (plan.gauss_enabled()) {
+    gauss.on = true;
+    gauss.cells = cells;
+    gauss.stash = (double*)dev.alloc(8 * cells);
+    gauss.first = (double*)dev.alloc(8 * cells);
+    gauss.residual = (double*)dev.alloc(8 * cells);
+    gauss.sums = (double*)dev.alloc(8 * 4);
+    make_dirs(plan.save_dir);
+    gauss.csv = plan.save_dir + "/gauss.csv";
+    open_gauss_csv(gauss.csv, dbl, args.restart ? cycle : -1);
+  }
   check(tpicb200_prepare(ctx, &st, s_), "startup");
   {
     uint32_t bad = 0;
@@ -725,16 +827,59 @@ int main(int argc, char** argv) {
     std::printf("cycle %6lld  total energy %.10e  change %+.3e\n", cycle, t, t - initial);
     std::fflush(stdout);
   };
+  // At state `cycle`: finish the open sample, then begin one when due.
+  auto gauss_step = [&] {
+    if (!gauss.on) return;
+    const bool begin = plan.gauss_begins(cycle, last), finish = gauss.begun >= 0;
+    if (!begin && !finish) return;
+    check(tpicb200_gauss_field(ctx, st.e, gauss.stash, gauss.first, gauss.residual, begin ? 1 : 0, finish ? 1 : 0,
+                               finish && !gauss.first_set ? 1 : 0, gauss.sums, s_),
+          "Gauss field");
+    if (finish) {
+      double sums[4];
+      cuda(cudaMemcpyAsync(sums, gauss.sums, sizeof(sums), cudaMemcpyDeviceToHost, stream), "Gauss sums");
+      cuda(cudaStreamSynchronize(stream), "Gauss sums");
+      const double n = double(gauss.cells);
+      const double rms[4] = {std::sqrt(sums[0] / n), std::sqrt(sums[1] / n), 0.0, std::sqrt(gauss.charge_sum / n)};
+      for (double v : rms)
+        if (!std::isfinite(v)) fail("Gauss residual: nonfinite sample");
+      const double t = (double(gauss.begun) + 0.5) * deck.dt;
+      std::ofstream f(gauss.csv, std::ios::app);
+      f << gauss.begun << "," << csv_number(t);
+      for (double v : rms) f << "," << csv_number(v);
+      f << "\n";
+      std::printf("  Gauss residual: cycle %lld t = %e  rms = %e  drift = %e  wall = %e  charge = %e\n",
+                  gauss.begun, t, rms[0], rms[1], rms[2], rms[3]);
+      std::fflush(stdout);
+      gauss.first_set = true;
+      gauss.finished = gauss.begun;
+      gauss.begun = -1;
+    }
+    if (begin) {
+      check(tpicb200_materialize(ctx, &st, s_), "materialize");
+      tpicb200_particles live[TPICB200_MAX_SPECIES];
+      for (int s = 0; s < deck.ns; ++s) live[s] = st.slot[s][st.current[s]];
+      check(tpicb200_gauss_charge(ctx, deck.ns, live, gauss.stash, gauss.sums, s_), "Gauss charge");
+      uint32_t bad = 0;
+      check(tpicb200_read_invalid(ctx, &bad, 0, s_), "invalid-counter read");
+      if (bad) fail("Gauss residual: invalid records in the sampled state");
+      cuda(cudaMemcpyAsync(&gauss.charge_sum, gauss.sums + 3, 8, cudaMemcpyDeviceToHost, stream), "Gauss sums");
+      cuda(cudaStreamSynchronize(stream), "Gauss sums");
+      gauss.begun = cycle;
+    }
+  };
   auto snapshots = [&] {
     const bool final = cycle == last;
     const bool fields = plan.fields_due(cycle, final), particles = plan.particles_due(cycle, final);
     if (!fields && !particles) return;
     make_dirs(plan.save_dir);
     check(tpicb200_materialize(ctx, &st, s_), "materialize");
-    if (fields) write_fields(ctx, st, grid, plan, deck.ns, dbl, cycle, double(cycle) * deck.dt, final, stream);
+    if (fields)
+      write_fields(ctx, st, grid, plan, deck.ns, dbl, cycle, double(cycle) * deck.dt, final, gauss, stream);
     if (particles) write_particles(ctx, st, plan, deck.ns, dbl, cycle, double(cycle) * deck.dt, final, stream);
   };
   if ((cadence && cycle % cadence == 0) || cycle == last) record(cycle == last);
+  gauss_step();
   snapshots();
   std::vector<tpicb200_cycle_report> reports;
   while (cycle < last) {
@@ -743,6 +888,11 @@ int main(int argc, char** argv) {
     if (every) stop = std::min(stop, (cycle / every + 1) * every);
     for (const int channel : {plan.field_cycle, plan.particles_cycle})
       if (channel > 0) stop = std::min(stop, (cycle / channel + 1) * channel);
+    if (gauss.on) {
+      if (gauss.begun >= 0) stop = std::min(stop, gauss.begun + 1);
+      const long long next = plan.next_gauss_begin(cycle, last);
+      if (next >= 0) stop = std::min(stop, next);
+    }
     const int n = int(stop - cycle);
     reports.assign(n, tpicb200_cycle_report{});
     check(tpicb200_cycle(ctx, &st, n, reports.data(), s_), "cycle");
@@ -755,6 +905,7 @@ int main(int argc, char** argv) {
     if (every && (cycle % every == 0 || cycle == last))
       check(tpicb200_checkpoint_write(ctx, &st, ckpt_dir.c_str(), int(cycle), s_), "checkpoint write");
     if (cycle == last || (cadence && cycle % cadence == 0)) record(cycle == last);
+    gauss_step();
     snapshots();
     if (!std::isfinite(field[0]) || !std::isfinite(field[1])) {
       std::fprintf(stderr, "tpicb200_run: nonfinite field energy\n");
