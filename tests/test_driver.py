@@ -102,3 +102,20 @@ def test_gauss_cadence_of_the_driver(driver, tmp_path):
     done = subprocess.run([driver, "--run", str(deck), "--dry-run", "--gauss-cycle", "0", "--field-output-cycle", "0"],
                           capture_output=True, text=True, timeout=60)
     assert "Gauss-law samples every 0 cycles\n" in done.stdout
+
+
+def test_diagnostics_and_checkpoint_keys(driver, tmp_path):
+    """DiagnosticsOutputCycle defaults to FieldOutputCycle, RestartOutputCycle to
+    0 and RestartDirName to data; the options override the keys."""
+    deck = tmp_path / "k.inp"
+    deck.write_text(DECKS[0].read_text() + "FieldOutputCycle = 7\n")
+    done = subprocess.run([driver, "--run", str(deck), "--dry-run", "--output", "o"], capture_output=True, text=True,
+                          timeout=60)
+    assert "diagnostics.csv rows every 7 cycles, checkpoints every 0 cycles under o/data" in done.stdout
+    deck.write_text(DECKS[0].read_text() + "DiagnosticsOutputCycle = 3\nRestartOutputCycle = 5\nRestartDirName = ck\n")
+    done = subprocess.run([driver, "--run", str(deck), "--dry-run", "--output", "o"], capture_output=True, text=True,
+                          timeout=60)
+    assert "diagnostics.csv rows every 3 cycles, checkpoints every 5 cycles under o/ck" in done.stdout
+    done = subprocess.run([driver, "--run", str(deck), "--dry-run", "--output", "o", "--diagnostics-cycle", "1",
+                           "--restart-cycle", "2", "--restart-dir", "r"], capture_output=True, text=True, timeout=60)
+    assert "diagnostics.csv rows every 1 cycles, checkpoints every 2 cycles under o/r" in done.stdout

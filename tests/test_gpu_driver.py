@@ -43,12 +43,15 @@ def driver(*argv, cwd):
 def test_driver_matches_the_python_runner(tmp_path, form, precision):
     B.build()
     a, b = tmp_path / "cpp", tmp_path / "py"
-    args = ["--run", str(C1), "--mass-matrix", form, "--precision", precision, "--cycles", "4"]
+    args = ["--run", str(C1), "--mass-matrix", form, "--precision", precision, "--cycles", "4",
+            "--diagnostics-cycle", "1"]
     driver(*args, "--output", str(a), cwd=tmp_path)
     done = subprocess.run([sys.executable, "-m", "tpic_b200", *args, "--output", str(b)], capture_output=True,
                           text=True, timeout=600, cwd=ROOT)
     assert done.returncode == 0, done.stdout + done.stderr
-    x, y = rows(a / "diagnostics.csv"), rows(b / "diagnostics.csv")
+    x, y = rows(a / "data" / "diagnostics.csv"), rows(b / "data" / "diagnostics.csv")
+    assert (a / "data" / "diagnostics.csv").read_text().splitlines()[:2] == \
+        (b / "data" / "diagnostics.csv").read_text().splitlines()[:2]
     assert x.shape == y.shape == (5, 11 + 2 * 5)
     assert np.array_equal(x, y)
 
@@ -56,13 +59,13 @@ def test_driver_matches_the_python_runner(tmp_path, form, precision):
 def test_driver_restart_continues_the_run(tmp_path):
     B.build()
     straight, restarted = tmp_path / "straight", tmp_path / "restarted"
-    base = ["--run", str(C1), "--mass-matrix", "matrix-core"]
+    base = ["--run", str(C1), "--mass-matrix", "matrix-core", "--diagnostics-cycle", "1"]
     driver(*base, "--cycles", "6", "--output", str(straight), cwd=tmp_path)
     driver(*base, "--cycles", "4", "--restart-cycle", "2", "--output", str(restarted), cwd=tmp_path)
     driver(*base, "--cycles", "6", "--restart", "--output", str(restarted), cwd=tmp_path)
-    text = (restarted / "diagnostics.csv").read_text()
-    assert "# restart at cycle 4" in text
-    a, b = rows(straight / "diagnostics.csv"), rows(restarted / "diagnostics.csv")
+    text = (restarted / "data" / "diagnostics.csv").read_text()
+    assert "# restart at cycle 4: precision_profile = mixed/mixed" in text
+    a, b = rows(straight / "data" / "diagnostics.csv"), rows(restarted / "data" / "diagnostics.csv")
     assert a.shape == b.shape == (7, 21)
     other = np.arange(7) != 4
     assert np.array_equal(a[other], b[other])
@@ -101,6 +104,8 @@ def test_driver_snapshots_match_the_python_runner(tmp_path):
     assert "particles_t000002.pvtp" in names and "particles_t000003_r000000.vtp" in names
     assert "particles_t000001.pvtp" not in names
     for name in names:
+        if name.endswith(".csv"):
+            continue
         if name.endswith(".pvtp"):
             assert (a / "data" / name).read_bytes() == (b / "data" / name).read_bytes()
             continue

@@ -40,19 +40,22 @@ def test_deck_run_with_checkpoints_and_restart(tmp_path):
     deck.write_text((DECKS / "harris2d_256x128.inp").read_text() +
                     "\nnxc = 16\nnyc = 16\nLx = 4.0\nLy = 4.0\nnpcelx = 2 2 2 2\nnpcely = 2 2 2 2\nncycles = 4\n")
     out = tmp_path / "out"
-    assert runner.main(["--run", str(deck), "--output", str(out), "--restart-cycle", "2"]) == 0
-    rows = [l.split(",") for l in (out / "diagnostics.csv").read_text().splitlines() if l[:1].isdigit()]
+    assert runner.main(["--run", str(deck), "--output", str(out), "--restart-cycle", "2",
+                        "--diagnostics-cycle", "1"]) == 0
+    rows = [l.split(",") for l in (out / "data" / "diagnostics.csv").read_text().splitlines() if l[:1].isdigit()]
     assert [r[0] for r in rows] == ["0", "1", "2", "3", "4"]
     assert [r[2] for r in rows] == ["pre_solve"] * 4 + ["final"]
     assert float(rows[0][7]) == 0.0
     assert abs(float(rows[-1][7])) <= 1e-5 * float(rows[0][6])
     names = sorted(p.name for p in (out / "data").iterdir())
     assert [n for n in names if n.startswith("checkpoint")] == ["checkpoint_t000004_n000001"]
+    assert "diagnostics.csv" in names
     # Field snapshots (FieldOutputCycle defaults to 100): the first and the final state.
     assert "E_t000000.vti" in names and "E_t000004.vti" in names and "B_t000004.vti" in names
     # Continue to cycle 6 from the checkpoint of cycle 4.
-    assert runner.main(["--run", str(deck), "--output", str(out), "--restart", "--cycles", "6"]) == 0
-    text = (out / "diagnostics.csv").read_text()
+    assert runner.main(["--run", str(deck), "--output", str(out), "--restart", "--cycles", "6",
+                        "--diagnostics-cycle", "1"]) == 0
+    text = (out / "data" / "diagnostics.csv").read_text()
     assert "# restart at cycle 4" in text
     rows = [l.split(",") for l in text.splitlines() if l[:1].isdigit()]
     assert [r[0] for r in rows] == ["0", "1", "2", "3", "4", "5", "6"]

@@ -13,17 +13,21 @@
 // are sampled on the host from the case (tpicb200_case_fields), the species
 // are loaded and centred on the device (tpicb200_load_species,
 // tpicb200_center_velocities), and the cycles run through tpicb200_cycle.
-// It writes TPIC's diagnostics.csv rows (docs/user/output.md; columns of
-// src/io/diagnostics_writer.cpp:60-62) every --diagnostics-cycle cycles and
-// at the final state, and checkpoints every --restart-cycle cycles under
-// --output/--restart-dir; --restart continues from the newest complete
-// checkpoint and the diagnostics file after a `# restart at cycle N` line.
-// Snapshots follow TPIC's output channels (docs/user/output.md): every
-// FieldOutputCycle cycles one `<array>_tNNNNNN.vti` per array selected by
-// FieldOutputTag / MomentsOutputTag, every ParticlesOutputCycle cycles
-// `particles_tNNNNNN.pvtp` with its piece, both also at the final state, under
-// --output/SaveDirName (deck keys; the --field-output-cycle,
-// --particles-output-cycle and --save-dir options override them).
+// Output follows TPIC's channels and deck keys (docs/user/output.md,
+// docs/user/input_keys.md), each key overridden by its option:
+// - diagnostics.csv in SaveDirName (precision lines, then the columns of
+//   src/io/diagnostics_writer.cpp:60-62): a row every DiagnosticsOutputCycle
+//   cycles (default FieldOutputCycle; <= 0: no file) and at the final state;
+// - checkpoints every RestartOutputCycle cycles (default 0) under
+//   RestartDirName (default data); --restart continues from the newest
+//   complete checkpoint and the diagnostics file after a
+//   `# restart at cycle N: ...` line;
+// - snapshots every FieldOutputCycle cycles (one `<array>_tNNNNNN.vti` per
+//   array selected by FieldOutputTag / MomentsOutputTag) and every
+//   ParticlesOutputCycle cycles (`particles_tNNNNNN.pvtp` with its piece),
+//   both also at the final state, under SaveDirName (default data);
+// - Gauss-law samples every DiagnosticGaussCycle cycles and, with the Gauss
+//   array, before every field snapshot: gauss.csv rows and the Gauss array.
 // `matrix-core` (TPIC's tensor-core form) selects BF16x3 in mixed precision
 // and the FP64 moment form in double. --dry-run parses the deck and prints
 // the run's sizes without touching a device.
@@ -47,10 +51,12 @@
 namespace {
 
 struct Args {
-  std::string deck, form = "matrix-core", precision = "mixed", output = ".", restart_dir = "data";
+  std::string deck, form = "matrix-core", precision = "mixed", output = ".", restart_dir;
   bool restart = false, dry_run = false;
   long long cycles = -1;
-  int diagnostics_cycle = 1, restart_cycle = 0, gmres_max_iterations = 100, device = 0;
+  // Unset (has_* false): the deck's DiagnosticsOutputCycle, RestartOutputCycle, RestartDirName.
+  bool has_diagnostics_cycle = false, has_restart_cycle = false, has_restart_dir = false;
+  int diagnostics_cycle = 0, restart_cycle = 0, gmres_max_iterations = 100, device = 0;
   unsigned long long seed = 0;
   // Snapshot overrides of the deck's keys (unset: the deck's value).
   bool has_field_cycle = false, has_particles_cycle = false, has_save_dir = false, has_gauss_cycle = false;
@@ -83,10 +89,18 @@ Args parse_args(int argc, char** argv) {
     else if (k == "--restart") a.restart = true;
     else if (k == "--dry-run") a.dry_run = true;
     else if (k == "--output") a.output = value(i);
-    else if (k == "--restart-dir") a.restart_dir = value(i);
+    else if (k == "--restart-dir") {
+      a.has_restart_dir = true;
+      a.restart_dir = value(i);
+    }
     else if (k == "--cycles") a.cycles = std::atoll(value(i).c_str());
-    else if (k == "--diagnostics-cycle") a.diagnostics_cycle = std::atoi(value(i).c_str());
-    else if (k == "--restart-cycle") a.restart_cycle = std::atoi(value(i).c_str());
+    else if (k == "--diagnostics-cycle") {
+      a.has_diagnostics_cycle = true;
+      a.diagnostics_cycle = std::atoi(value(i).c_str());
+    } else if (k == "--restart-cycle") {
+      a.has_restart_cycle = true;
+      a.restart_cycle = std::atoi(value(i).c_str());
+    }
     else if (k == "--gmres-max-iterations") a.gmres_max_iterations = std::atoi(value(i).c_str());
     else if (k == "--device") a.device = std::atoi(value(i).c_str());
     else if (k == "--seed") a.seed = std::strtoull(value(i).c_str(), nullptr, 10);
@@ -282,6 +296,9 @@ struct OutputPlan {
   std::string save_dir;
   int field_cycle = 100, particles_cycle = 0;
   int gauss_cycle = 0;                 // DiagnosticGaussCycle
+  int diagnostics_cycle = 100;         // DiagnosticsOutputCycle (default FieldOutputCycle; <= 0: no file)
+  int restart_cycle = 0;               // RestartOutputCycle
+  std::string restart_dir = "data";    // RestartDirName
   bool e = false, b = false, gauss = false;
   std::vector<std::string> fields;     // the field arrays in tag order
   std::vector<MomentArray> moments;
@@ -341,11 +358,20 @@ OutputPlan output_plan(const std::string& text, const Args& args, int ns) {
     return it == k.end() ? fallback : it->second;
   };
   OutputPlan plan;
-  plan.save_dir = args.output + "/" + (args.has_save_dir ? args.save_dir : get("SaveDirName", "data"));
+  std::string save = args.has_save_dir ? args.save_dir : get("SaveDirName", "data");
+  if (save.empty()) save = "data";
+  plan.save_dir = args.output + "/" + save;
   plan.field_cycle = args.has_field_cycle ? args.field_cycle : std::atoi(get("FieldOutputCycle", "100").c_str());
   plan.particles_cycle =
       args.has_particles_cycle ? args.particles_cycle : std::atoi(get("ParticlesOutputCycle", "0").c_str());
   plan.gauss_cycle = args.has_gauss_cycle ? args.gauss_cycle : std::atoi(get("DiagnosticGaussCycle", "0").c_str());
+  plan.diagnostics_cycle = args.has_diagnostics_cycle
+                               ? args.diagnostics_cycle
+                               : std::atoi(get("DiagnosticsOutputCycle", std::to_string(plan.field_cycle)).c_str());
+  plan.restart_cycle =
+      args.has_restart_cycle ? args.restart_cycle : std::atoi(get("RestartOutputCycle", "0").c_str());
+  plan.restart_dir = args.has_restart_dir ? args.restart_dir : get("RestartDirName", "data");
+  if (plan.restart_dir.empty()) plan.restart_dir = "data";
   const std::string method = get("WriteMethod", "");
   const std::pair<const char*, int> channels[2] = {{"FieldWriteMethod", plan.field_cycle},
                                                    {"ParticlesWriteMethod", plan.particles_cycle}};
@@ -666,6 +692,8 @@ int main(int argc, char** argv) {
     std::printf("), particles every %d cycles\n", plan.particles_cycle);
     std::printf("Gauss-law samples every %d cycles%s\n", plan.gauss_cycle,
                 plan.output_gauss() ? " and before each field snapshot" : "");
+    std::printf("diagnostics.csv rows every %d cycles, checkpoints every %d cycles under %s/%s\n",
+                plan.diagnostics_cycle, plan.restart_cycle, args.output.c_str(), plan.restart_dir.c_str());
     return 0;
   }
 
@@ -728,8 +756,13 @@ int main(int argc, char** argv) {
 
   const std::string out = args.output;
   ::mkdir(out.c_str(), 0755);
-  const std::string ckpt_dir = out + "/" + args.restart_dir;
-  const std::string csv = out + "/diagnostics.csv";
+  const std::string ckpt_dir = out + "/" + plan.restart_dir;
+  make_dirs(plan.save_dir);
+  const std::string csv = plan.save_dir + "/diagnostics.csv";
+  const bool diagnostics = plan.diagnostics_cycle > 0;
+  const auto [profile, roles] = precision_strings(dbl);
+  const std::string head = "# precision_profile = " + profile + "\n# precision_roles = " + roles + "\n" + kHeader +
+                           columns(deck.ns);
   long long cycle = 0;
   double initial = NAN;
   if (args.restart) {
@@ -744,7 +777,8 @@ int main(int argc, char** argv) {
     // The restarted run replaces the rows from its checkpoint cycle on and
     // keeps the first state's total energy as the reference of the change.
     std::vector<std::string> kept;
-    if (file_exists(csv)) {
+    if (!diagnostics) {
+    } else if (file_exists(csv)) {
       std::ifstream old(csv);
       std::string line;
       while (std::getline(old, line)) {
@@ -761,13 +795,16 @@ int main(int argc, char** argv) {
         kept.push_back(line);
       }
     } else {
-      std::stringstream h(std::string(kHeader) + columns(deck.ns));
+      std::stringstream h(head);
       std::string line;
       while (std::getline(h, line)) kept.push_back(line);
     }
-    kept.push_back("# restart at cycle " + std::to_string(cycle));
-    std::ofstream f(csv);
-    for (const std::string& line : kept) f << line << "\n";
+    if (diagnostics) {
+      kept.push_back("# restart at cycle " + std::to_string(cycle) + ": precision_profile = " + profile +
+                     ", precision_roles = " + roles);
+      std::ofstream f(csv);
+      for (const std::string& line : kept) f << line << "\n";
+    }
   } else {
     upload(st.e, sample_field(deck, true), !dbl);
     upload(st.b_cell, sample_field(deck, false), !dbl);
@@ -776,8 +813,10 @@ int main(int argc, char** argv) {
       if (deck.species[s].center_velocity)
         check(tpicb200_center_velocities(ctx, &deck, s, &st.slot[s][0], nullptr, s_), "velocity centring");
     }
-    std::ofstream f(csv);
-    f << kHeader << columns(deck.ns) << "\n";
+    if (diagnostics) {
+      std::ofstream f(csv);
+      f << head << "\n";
+    }
   }
   if (last < cycle) usage("the run's last cycle lies before the checkpoint cycle");
   GaussRun gauss;
@@ -818,11 +857,13 @@ int main(int argc, char** argv) {
     return t;
   };
   if (std::isnan(initial)) initial = total_of();
-  const int cadence = args.diagnostics_cycle > 0 ? args.diagnostics_cycle : 0;
-  const int every = args.restart_cycle > 0 ? args.restart_cycle : 0;
+  const int cadence = diagnostics ? plan.diagnostics_cycle : 0;
+  const int every = plan.restart_cycle > 0 ? plan.restart_cycle : 0;
   auto record = [&](bool final) {
-    std::ofstream f(csv, std::ios::app);
-    f << row(cycle, deck.dt, final, field, species, deck.ns, initial) << "\n";
+    if (diagnostics) {
+      std::ofstream f(csv, std::ios::app);
+      f << row(cycle, deck.dt, final, field, species, deck.ns, initial) << "\n";
+    }
     const double t = total_of();
     std::printf("cycle %6lld  total energy %.10e  change %+.3e\n", cycle, t, t - initial);
     std::fflush(stdout);

@@ -7,9 +7,13 @@ TPIC's `diagnostics.csv` (docs/user/output.md, "diagnostics.csv": cycle, time,
 state, electric, magnetic, kinetic and total energy, the change of the total
 energy from the run's first state, charge and momentum, then per species
 kinetic energy, charge and momentum) every `DiagnosticsOutputCycle` cycles and
-at the final state, and checkpoints every `RestartOutputCycle` cycles under
-`RestartDirName`. `--restart` continues from the newest complete checkpoint,
-and the diagnostics file continues after a `# restart at cycle N` line.
+at the final state, in `SaveDirName` after the precision lines, and checkpoints
+every `RestartOutputCycle` cycles under `RestartDirName` (deck keys with TPIC's
+defaults, docs/user/input_keys.md: DiagnosticsOutputCycle = FieldOutputCycle,
+RestartOutputCycle = 0, both directories `data`; a nonpositive diagnostics
+cadence disables the file; the command-line options override the keys).
+`--restart` continues from the newest complete checkpoint, and the diagnostics
+file continues after a `# restart at cycle N` line.
 """
 from __future__ import annotations
 
@@ -78,9 +82,11 @@ def parse_args(argv=None):
     ap.add_argument("--restart", action="store_true", help="continue from the newest complete checkpoint")
     ap.add_argument("--output", default=".", help="directory of diagnostics.csv and RestartDirName")
     ap.add_argument("--cycles", type=int, default=None, help="last cycle of the run (default: the deck's ncycles)")
-    ap.add_argument("--diagnostics-cycle", type=int, default=1, help="DiagnosticsOutputCycle (<= 0: final row only)")
-    ap.add_argument("--restart-cycle", type=int, default=0, help="RestartOutputCycle (<= 0: no checkpoints)")
-    ap.add_argument("--restart-dir", default="data", help="RestartDirName, under --output")
+    ap.add_argument("--diagnostics-cycle", type=int, default=None,
+                    help="DiagnosticsOutputCycle (default: the deck's, else FieldOutputCycle; <= 0: no file)")
+    ap.add_argument("--restart-cycle", type=int, default=None,
+                    help="RestartOutputCycle (default: the deck's, else 0: no checkpoints)")
+    ap.add_argument("--restart-dir", default=None, help="RestartDirName, under --output (default: the deck's, else data)")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--gmres-max-iterations", type=int, default=100)
     ap.add_argument("--device", type=int, default=0)
@@ -97,7 +103,8 @@ def parse_args(argv=None):
 
 def run(args) -> int:
     from .simulation import Simulation
-    from .output import GaussSampler, GaussWriter, OutputPlan, precision_strings, write_fields, write_particles
+    from .output import (GaussSampler, GaussWriter, OutputPlan, deck_keys, precision_strings, write_fields,
+                         write_particles)
     text = Path(args.run).read_text()
     deck = D.parse(text)
     case = D.to_case(deck, seed=args.seed)
@@ -105,18 +112,32 @@ def run(args) -> int:
     form = resolve_form(args.mass_matrix, args.precision)
     out = Path(args.output)
     out.mkdir(parents=True, exist_ok=True)
-    ckpt_dir = out / args.restart_dir
-    csv_path = out / "diagnostics.csv"
     plan = OutputPlan.from_deck(text, out, field_cycle=args.field_output_cycle,
                                 particles_cycle=args.particles_output_cycle, gauss_cycle=args.gauss_cycle)
     if args.save_dir is not None:
         plan.save_dir = out / args.save_dir
+    keys = deck_keys(text)
+    ckpt_dir = out / (args.restart_dir if args.restart_dir is not None else (keys.get("RestartDirName", "") or "data"))
+    plan.save_dir.mkdir(parents=True, exist_ok=True)
+    csv_path = plan.save_dir / "diagnostics.csv"
+    diagnostics_cycle = (args.diagnostics_cycle if args.diagnostics_cycle is not None else
+                         int(keys.get("DiagnosticsOutputCycle", plan.field_cycle)))
+    restart_cycle = (args.restart_cycle if args.restart_cycle is not None else
+                     int(keys.get("RestartOutputCycle", 0)))
     kw = dict(precision=args.precision, mass_kind=form, device=args.device,
               gmres_max_iterations=args.gmres_max_iterations, keep_ids=plan.particles_cycle > 0)
     ns = len(case.species)
+    diagnostics = diagnostics_cycle > 0
     if args.restart:
         sim = Simulation.restart(case, ckpt_dir, **kw)
         initial = first_total(csv_path)
+    else:
+        sim = Simulation(case, generate_on_device=True, **kw)
+        sim.prepare()
+        initial = None
+    profile, roles = precision_strings(sim)
+    head = f"# precision_profile = {profile}\n# precision_roles = {roles}\n" + HEADER + columns(ns)
+    if diagnostics and args.restart:
         # The restarted run replaces the rows from its checkpoint cycle on.
         kept = []
         if csv_path.exists():
@@ -125,15 +146,11 @@ def run(args) -> int:
                     continue
                 kept.append(line)
         else:
-            kept = (HEADER + columns(ns)).splitlines()
-        kept.append(f"# restart at cycle {sim.cycle}")
+            kept = head.splitlines()
+        kept.append(f"# restart at cycle {sim.cycle}: precision_profile = {profile}, precision_roles = {roles}")
         csv_path.write_text("\n".join(kept) + "\n")
-    else:
-        sim = Simulation(case, generate_on_device=True, **kw)
-        sim.prepare()
-        initial = None
-        with open(csv_path, "w") as f:
-            f.write(HEADER + columns(ns) + "\n")
+    elif diagnostics:
+        csv_path.write_text(head + "\n")
     if last < sim.cycle:
         raise SystemExit(f"the run's last cycle {last} lies before the checkpoint cycle {sim.cycle}")
     w = sim.energy()
@@ -141,19 +158,18 @@ def run(args) -> int:
     species = tuple(tuple(w[2 + 5 * s:7 + 5 * s]) for s in range(ns))
     if initial is None:
         initial = field[0] + field[1] + sum(sp[0] for sp in species)
-    cadence = args.diagnostics_cycle if args.diagnostics_cycle > 0 else 0
-    ckpt = args.restart_cycle if args.restart_cycle > 0 else 0
+    cadence = diagnostics_cycle if diagnostics else 0
+    ckpt = restart_cycle if restart_cycle > 0 else 0
     gauss = gauss_writer = None
     if plan.gauss_enabled():
         gauss = GaussSampler(sim)
-        profile, roles = precision_strings(sim)
         gauss_writer = GaussWriter(plan.save_dir / "gauss.csv", profile, roles,
                                    restart_cycle=sim.cycle if args.restart else None)
 
     def record(final: bool) -> None:
-        line = row(sim.cycle, case.dt, final, field, species, initial)
-        with open(csv_path, "a") as f:
-            f.write(line + "\n")
+        if diagnostics:
+            with open(csv_path, "a") as f:
+                f.write(row(sim.cycle, case.dt, final, field, species, initial) + "\n")
         total = field[0] + field[1] + sum(sp[0] for sp in species)
         print(f"cycle {sim.cycle:6d}  total energy {total:.10e}  change {total - initial:+.3e}", flush=True)
 
