@@ -1,6 +1,6 @@
 """The C++ host driver tpicb200_run (tpic_b200/host/tpicb200_run.cpp), on the
 host: it builds against include/tpicb200.h and the library, parses every
-shipped deck (--dry-run needs no device), and rejects bad command lines."""
+shipped deck (--check-input needs no device), and rejects bad command lines."""
 from __future__ import annotations
 
 import subprocess
@@ -21,21 +21,29 @@ def driver():
 
 @pytest.mark.parametrize("deck", DECKS, ids=[d.name for d in DECKS])
 def test_dry_run_of_every_shipped_deck(driver, deck):
-    done = subprocess.run([driver, "--run", str(deck), "--dry-run"], capture_output=True, text=True, timeout=60)
+    done = subprocess.run([driver, "--check-input", str(deck)], capture_output=True, text=True, timeout=60)
     assert done.returncode == 0, done.stderr
     assert "cells" in done.stdout and "records" in done.stdout
 
 
 def test_bad_command_lines(driver, tmp_path):
     deck = str(DECKS[0])
-    for argv in ([], ["--run"], ["--run", deck, "--mass-matrix", "nope", "--dry-run"],
-                 ["--run", deck, "--precision", "half"], ["--run", str(tmp_path / "absent.inp")], ["--bogus"]):
+    # TPIC's exit code of an invalid command line or input is 1.
+    for argv in ([], ["--run"], ["--check-input", deck, "--mass-matrix", "nope"], ["--run", "--check-input", deck],
+                 ["--run", deck, deck], ["--run", deck, "--precision", "half"], ["--check-input", deck, "--restart"],
+                 ["--run", deck, "--order", "random"], ["--run", str(tmp_path / "absent.inp")], ["--bogus"]):
         done = subprocess.run([driver, *argv], capture_output=True, text=True, timeout=60)
-        assert done.returncode == 2, (argv, done.stdout, done.stderr)
+        assert done.returncode == 1, (argv, done.stdout, done.stderr)
         assert "usage" in done.stderr
+    done = subprocess.run([driver, "--help"], capture_output=True, text=True, timeout=60)
+    assert done.returncode == 0 and "--check-input|--initialize|--run" in done.stdout
+    # --dry-run is --check-input; --order takes TPIC's three values; the form defaults to scalar.
+    for argv in (["--dry-run", deck], ["--check-input", deck, "--order", "full"], [deck, "--check-input"]):
+        done = subprocess.run([driver, *argv], capture_output=True, text=True, timeout=60)
+        assert done.returncode == 0 and "mass form 0" in done.stdout, (argv, done.stderr)
     bad = tmp_path / "bad.inp"
     bad.write_text("Case = Whistler\n")
-    done = subprocess.run([driver, "--run", str(bad), "--dry-run"], capture_output=True, text=True, timeout=60)
+    done = subprocess.run([driver, "--check-input", str(bad)], capture_output=True, text=True, timeout=60)
     assert done.returncode == 1 and "deck" in done.stderr
 
 
@@ -55,7 +63,7 @@ def test_snapshot_selection_matches_the_runner(driver, tmp_path, field_tag, mome
     if moments_tag:
         keys += f"MomentsOutputTag = {moments_tag}\n"
     deck.write_text(DECKS[0].read_text() + keys)
-    done = subprocess.run([driver, "--run", str(deck), "--dry-run", "--output", str(tmp_path)], capture_output=True,
+    done = subprocess.run([driver, "--check-input", str(deck), "--output", str(tmp_path)], capture_output=True,
                           text=True, timeout=60)
     assert done.returncode == 0, done.stderr
     line = [x for x in done.stdout.splitlines() if x.startswith("snapshots under")][0]
@@ -65,7 +73,7 @@ def test_snapshot_selection_matches_the_runner(driver, tmp_path, field_tag, mome
     assert listed == fields + [m[0] for m in moments]
     assert f"under {tmp_path}/snaps:" in line and "fields every 5 cycles" in line
     assert line.endswith("particles every 3 cycles")
-    over = subprocess.run([driver, "--run", str(deck), "--dry-run", "--field-output-cycle", "0",
+    over = subprocess.run([driver, "--check-input", str(deck), "--field-output-cycle", "0",
                            "--particles-output-cycle", "7", "--save-dir", "x"], capture_output=True, text=True,
                           timeout=60)
     assert over.returncode == 0, over.stderr
@@ -81,12 +89,12 @@ def test_snapshot_selection_matches_the_runner(driver, tmp_path, field_tag, mome
 def test_bad_snapshot_keys(driver, tmp_path, keys):
     deck = tmp_path / "bad.inp"
     deck.write_text(DECKS[0].read_text() + keys)
-    done = subprocess.run([driver, "--run", str(deck), "--dry-run"], capture_output=True, text=True, timeout=60)
+    done = subprocess.run([driver, "--check-input", str(deck)], capture_output=True, text=True, timeout=60)
     assert done.returncode == 1, (keys, done.stdout, done.stderr)
     assert "Tag" in done.stderr or "Method" in done.stderr
     ok = tmp_path / "off.inp"
     ok.write_text(DECKS[0].read_text() + "WriteMethod = hdf5\nFieldOutputCycle = 0\n")
-    done = subprocess.run([driver, "--run", str(ok), "--dry-run"], capture_output=True, text=True, timeout=60)
+    done = subprocess.run([driver, "--check-input", str(ok)], capture_output=True, text=True, timeout=60)
     assert done.returncode == 0, done.stderr
 
 
@@ -96,10 +104,10 @@ def test_gauss_cadence_of_the_driver(driver, tmp_path):
     before each field snapshot."""
     deck = tmp_path / "g.inp"
     deck.write_text(DECKS[0].read_text() + "DiagnosticGaussCycle = 4\nFieldOutputCycle = 5\nFieldOutputTag = E+Gauss\n")
-    done = subprocess.run([driver, "--run", str(deck), "--dry-run"], capture_output=True, text=True, timeout=60)
+    done = subprocess.run([driver, "--check-input", str(deck)], capture_output=True, text=True, timeout=60)
     assert done.returncode == 0, done.stderr
     assert "Gauss-law samples every 4 cycles and before each field snapshot" in done.stdout
-    done = subprocess.run([driver, "--run", str(deck), "--dry-run", "--gauss-cycle", "0", "--field-output-cycle", "0"],
+    done = subprocess.run([driver, "--check-input", str(deck), "--gauss-cycle", "0", "--field-output-cycle", "0"],
                           capture_output=True, text=True, timeout=60)
     assert "Gauss-law samples every 0 cycles\n" in done.stdout
 
@@ -109,13 +117,13 @@ def test_diagnostics_and_checkpoint_keys(driver, tmp_path):
     0 and RestartDirName to data; the options override the keys."""
     deck = tmp_path / "k.inp"
     deck.write_text(DECKS[0].read_text() + "FieldOutputCycle = 7\n")
-    done = subprocess.run([driver, "--run", str(deck), "--dry-run", "--output", "o"], capture_output=True, text=True,
+    done = subprocess.run([driver, "--check-input", str(deck), "--output", "o"], capture_output=True, text=True,
                           timeout=60)
     assert "diagnostics.csv rows every 7 cycles, checkpoints every 0 cycles under o/data" in done.stdout
     deck.write_text(DECKS[0].read_text() + "DiagnosticsOutputCycle = 3\nRestartOutputCycle = 5\nRestartDirName = ck\n")
-    done = subprocess.run([driver, "--run", str(deck), "--dry-run", "--output", "o"], capture_output=True, text=True,
+    done = subprocess.run([driver, "--check-input", str(deck), "--output", "o"], capture_output=True, text=True,
                           timeout=60)
     assert "diagnostics.csv rows every 3 cycles, checkpoints every 5 cycles under o/ck" in done.stdout
-    done = subprocess.run([driver, "--run", str(deck), "--dry-run", "--output", "o", "--diagnostics-cycle", "1",
+    done = subprocess.run([driver, "--check-input", str(deck), "--output", "o", "--diagnostics-cycle", "1",
                            "--restart-cycle", "2", "--restart-dir", "r"], capture_output=True, text=True, timeout=60)
     assert "diagnostics.csv rows every 1 cycles, checkpoints every 2 cycles under o/r" in done.stdout

@@ -92,7 +92,8 @@ def test_driver_snapshots_match_the_python_runner(tmp_path):
     from vtkread import field_data, read
     B.build()
     a, b = tmp_path / "cpp", tmp_path / "py"
-    args = ["--run", str(C1), "--cycles", "3", "--field-output-cycle", "1", "--particles-output-cycle", "2"]
+    args = ["--run", str(C1), "--mass-matrix", "matrix-core", "--cycles", "3", "--field-output-cycle", "1",
+            "--particles-output-cycle", "2"]
     driver(*args, "--output", str(a), cwd=tmp_path)
     done = subprocess.run([sys.executable, "-m", "tpic_b200", *args, "--output", str(b)], capture_output=True,
                           text=True, timeout=600, cwd=ROOT)
@@ -136,7 +137,7 @@ def test_driver_gauss_rows_match_the_python_runner(tmp_path):
     deck = tmp_path / "gauss.inp"
     deck.write_text(C1.read_text() + "\nDiagnosticGaussCycle = 1\nFieldOutputCycle = 2\nFieldOutputTag = E+Gauss\n")
     a, b = tmp_path / "cpp", tmp_path / "py"
-    args = ["--run", str(deck), "--cycles", "3"]
+    args = ["--run", str(deck), "--mass-matrix", "matrix-core", "--cycles", "3"]
     driver(*args, "--output", str(a), cwd=tmp_path)
     done = subprocess.run([sys.executable, "-m", "tpic_b200", *args, "--output", str(b)], capture_output=True,
                           text=True, timeout=600, cwd=ROOT)
@@ -157,3 +158,20 @@ def test_driver_gauss_rows_match_the_python_runner(tmp_path):
         gb = read(b / "data" / f"Gauss_t{cycle:06d}.vti")[1]["Gauss"]
         assert np.abs(ga - gb).max() <= 1e-12 * np.abs(gb).max()
     assert not (a / "data" / "Gauss_t000000.vti").exists()
+
+
+def test_initialize_writes_nothing_and_fresh_runs_refuse_existing_files(tmp_path):
+    """--initialize completes the startup and writes no output; a fresh --run
+    refuses an existing diagnostics.csv unless --overwrite-output, and a
+    restart replaces its outputs (TPIC's --overwrite-output rule)."""
+    B.build()
+    out = tmp_path / "o"
+    done = driver("--initialize", str(C1), "--output", str(out), cwd=tmp_path)
+    assert "initialized" in done.stdout and not out.exists()
+    base = ["--run", str(C1), "--cycles", "1", "--diagnostics-cycle", "1", "--output", str(out)]
+    driver(*base, cwd=tmp_path)
+    again = subprocess.run([str(B.DRIVER), *base], capture_output=True, text=True, timeout=600, cwd=tmp_path)
+    assert again.returncode == 1 and "--overwrite-output" in again.stderr
+    driver(*base, "--overwrite-output", cwd=tmp_path)
+    rows = [line for line in (out / "data" / "diagnostics.csv").read_text().splitlines() if line[:1].isdigit()]
+    assert [r.split(",")[0] for r in rows] == ["0", "1"]

@@ -31,7 +31,21 @@ def test_mass_matrix_names():
     assert runner.resolve_form("matrix-core", "double") == "moments-f64"
     assert runner.resolve_form("tf32", "mixed") == "tf32"
     args = runner.parse_args(["--run", "x.inp", "--mass-matrix", "scalar", "--restart"])
-    assert args.mass_matrix == "scalar" and args.restart and args.precision == "mixed"
+    assert args.mass_matrix == "scalar" and args.restart and args.precision == "mixed" and args.input == "x.inp"
+    # TPIC's command line: one of three commands and one input, scalar by default, exit code 1 otherwise.
+    assert runner.parse_args(["x.inp", "--run"]).mass_matrix == "scalar"
+    for argv in (["x.inp"], ["--run", "--check-input", "x.inp"], ["--check-input", "x.inp", "--restart"],
+                 ["--run", "x.inp", "--order", "random"]):
+        with pytest.raises(SystemExit) as e:
+            runner.parse_args(argv)
+        assert e.value.code == 1
+
+
+def test_check_input_writes_nothing(tmp_path, capsys):
+    out = tmp_path / "o"
+    assert runner.main(["--check-input", str(DECKS / "uniform3d_16.inp"), "--output", str(out)]) == 0
+    assert "16x16x16 cells, 2 species, 3 cycles, mass form scalar" in capsys.readouterr().out
+    assert not out.exists()
 
 
 @pytest.mark.gpu

@@ -51,8 +51,9 @@
 namespace {
 
 struct Args {
-  std::string deck, form = "matrix-core", precision = "mixed", output = ".", restart_dir;
-  bool restart = false, dry_run = false;
+  std::string deck, form = "scalar", precision = "mixed", output = ".", restart_dir, order = "partial";
+  std::string mode;  // check, initialize or run
+  bool restart = false, overwrite = false;
   long long cycles = -1;
   // Unset (has_* false): the deck's DiagnosticsOutputCycle, RestartOutputCycle, RestartDirName.
   bool has_diagnostics_cycle = false, has_restart_cycle = false, has_restart_dir = false;
@@ -64,30 +65,44 @@ struct Args {
   std::string save_dir;
 };
 
+const char* kUsage =
+    "usage: tpicb200_run --check-input|--initialize|--run deck.inp [--mass-matrix scalar|matrix-core|scalar-f64|"
+    "tf32|bf16x3|moments-f64] [--precision mixed|double] [--order full|partial|unsorted] [--overwrite-output] "
+    "[--restart] [--output DIR] [--cycles N] [--diagnostics-cycle K] [--restart-cycle R] [--restart-dir NAME] "
+    "[--seed S] [--gmres-max-iterations M] [--device D] [--field-output-cycle F] [--particles-output-cycle P] "
+    "[--save-dir NAME] [--gauss-cycle K]\n";
+
+// An invalid command line or input: exit code 1, as TPIC's.
 [[noreturn]] void usage(const char* why) {
   std::fprintf(stderr, "tpicb200_run: %s\n", why);
-  std::fprintf(stderr,
-               "usage: tpicb200_run --run deck.inp [--mass-matrix matrix-core|scalar|scalar-f64|tf32|bf16x3|"
-               "moments-f64] [--precision mixed|double] [--restart] [--output DIR] [--cycles N] "
-               "[--diagnostics-cycle K] [--restart-cycle R] [--restart-dir NAME] [--seed S] "
-               "[--gmres-max-iterations M] [--device D] [--field-output-cycle F] [--particles-output-cycle P] "
-               "[--save-dir NAME] [--gauss-cycle K] [--dry-run]\n");
-  std::exit(2);
+  std::fputs(kUsage, stderr);
+  std::exit(1);
 }
 
+// TPIC's command line (src/app/main.cpp:60-120): exactly one of --check-input,
+// --initialize or --run and one input file (--dry-run is --check-input); the
+// options of this driver follow.
 Args parse_args(int argc, char** argv) {
   Args a;
   auto value = [&](int& i) -> std::string {
     if (i + 1 >= argc) usage((std::string("missing value of ") + argv[i]).c_str());
     return argv[++i];
   };
+  int modes = 0;
   for (int i = 1; i < argc; ++i) {
     const std::string k = argv[i];
-    if (k == "--run") a.deck = value(i);
+    if (k == "--help" || k == "-h") {
+      std::fputs(kUsage, stdout);
+      std::exit(0);
+    }
+    if (k == "--check-input" || k == "--dry-run") { a.mode = "check"; ++modes; }
+    else if (k == "--initialize") { a.mode = "initialize"; ++modes; }
+    else if (k == "--run") { a.mode = "run"; ++modes; }
     else if (k == "--mass-matrix") a.form = value(i);
     else if (k == "--precision") a.precision = value(i);
+    else if (k == "--order") a.order = value(i);
+    else if (k == "--overwrite-output") a.overwrite = true;
     else if (k == "--restart") a.restart = true;
-    else if (k == "--dry-run") a.dry_run = true;
     else if (k == "--output") a.output = value(i);
     else if (k == "--restart-dir") {
       a.has_restart_dir = true;
@@ -117,11 +132,17 @@ Args parse_args(int argc, char** argv) {
       a.has_gauss_cycle = true;
       a.gauss_cycle = std::atoi(value(i).c_str());
     }
-    else if (k == "--help" || k == "-h") usage("help");
-    else usage(("unknown option " + k).c_str());
+    else if (!k.empty() && k[0] == '-') usage(("unknown option " + k).c_str());
+    else if (!a.deck.empty()) usage("expected exactly one input file");
+    else a.deck = k;
   }
-  if (a.deck.empty()) usage("--run DECK is required");
+  if (modes != 1 || a.deck.empty()) usage("give exactly one of --check-input, --initialize or --run and one input file");
+  if (a.restart && a.mode == "check") usage("--restart is only valid with --run or --initialize");
   if (a.precision != "mixed" && a.precision != "double") usage("--precision is mixed or double");
+  // Records are kept sorted by cell every cycle whatever the order: TPIC's
+  // three orders differ in its kernels' access patterns, not in the results.
+  if (a.order != "full" && a.order != "partial" && a.order != "unsorted")
+    usage("--order must be full, partial or unsorted");
   return a;
 }
 
@@ -299,6 +320,7 @@ struct OutputPlan {
   int diagnostics_cycle = 100;         // DiagnosticsOutputCycle (default FieldOutputCycle; <= 0: no file)
   int restart_cycle = 0;               // RestartOutputCycle
   std::string restart_dir = "data";    // RestartDirName
+  bool overwrite = false;              // replace existing output files (--overwrite-output, or a restart)
   bool e = false, b = false, gauss = false;
   std::vector<std::string> fields;     // the field arrays in tag order
   std::vector<MomentArray> moments;
@@ -372,6 +394,7 @@ OutputPlan output_plan(const std::string& text, const Args& args, int ns) {
       args.has_restart_cycle ? args.restart_cycle : std::atoi(get("RestartOutputCycle", "0").c_str());
   plan.restart_dir = args.has_restart_dir ? args.restart_dir : get("RestartDirName", "data");
   if (plan.restart_dir.empty()) plan.restart_dir = "data";
+  plan.overwrite = args.overwrite || args.restart;
   const std::string method = get("WriteMethod", "");
   const std::pair<const char*, int> channels[2] = {{"FieldWriteMethod", plan.field_cycle},
                                                    {"ParticlesWriteMethod", plan.particles_cycle}};
@@ -563,13 +586,14 @@ void write_fields(tpicb200_context* ctx, const tpicb200_state& st, const tpicb20
     cuda(cudaMemcpyAsync(r.data(), gauss.residual, r.size() * 8, cudaMemcpyDeviceToHost, stream), "Gauss read");
     cuda(cudaStreamSynchronize(stream), "Gauss read");
     check(tpicb200_vtk_write_cells(tagged(plan.save_dir, "Gauss", cycle, ".vti").c_str(), "Gauss", &g, r.data(),
-                                   int(cycle), time, final ? 1 : 0, profile.c_str(), roles.c_str(), 1),
+                                   int(cycle), time, final ? 1 : 0, profile.c_str(), roles.c_str(),
+                                   plan.overwrite ? 1 : 0),
           "Gauss snapshot");
   }
   auto put = [&](const std::string& name, const std::vector<double>& values, int components) {
     check(tpicb200_vtk_write_field(tagged(plan.save_dir, name, cycle, ".vti").c_str(), name.c_str(), components, &g,
                                    values.data(), int(cycle), time, final ? 1 : 0, profile.c_str(), roles.c_str(),
-                                   1),
+                                   plan.overwrite ? 1 : 0),
           "field snapshot");
   };
   if (plan.e) put("E", snapshot_nodes(st.e, g, dbl, stream), 3);
@@ -646,7 +670,7 @@ void write_particles(tpicb200_context* ctx, const tpicb200_state& st, const Outp
   check(tpicb200_read_invalid(ctx, &bad, 0, stream), "invalid-counter read");
   if (bad) fail("particle output: invalid records in the snapshot state");
   check(tpicb200_vtk_write_particles(plan.save_dir.c_str(), int(cycle), time, final ? 1 : 0, profile.c_str(),
-                                     roles.c_str(), ns, species.data(), 1),
+                                     roles.c_str(), ns, species.data(), plan.overwrite ? 1 : 0),
         "particle snapshot");
 }
 
@@ -674,7 +698,7 @@ int main(int argc, char** argv) {
     largest = std::max(largest, count[s]);
   }
   const OutputPlan plan = output_plan(text.str(), args, deck.ns);
-  if (args.dry_run) {
+  if (args.mode == "check") {
     std::printf("deck %s: case %s, %dx%dx%d cells, %d species", args.deck.c_str(), deck.case_name, grid.nx, grid.ny,
                 grid.nz, deck.ns);
     for (int s = 0; s < deck.ns; ++s) std::printf(" %s%u", s ? "+" : " ", count[s]);
@@ -755,9 +779,11 @@ int main(int argc, char** argv) {
   const tpicb200_stream s_ = (tpicb200_stream)stream;
 
   const std::string out = args.output;
-  ::mkdir(out.c_str(), 0755);
+  if (args.mode == "run") ::mkdir(out.c_str(), 0755);
   const std::string ckpt_dir = out + "/" + plan.restart_dir;
-  make_dirs(plan.save_dir);
+  // --initialize completes the startup and writes no output.
+  const bool advance = args.mode == "run";
+  if (advance) make_dirs(plan.save_dir);
   const std::string csv = plan.save_dir + "/diagnostics.csv";
   const bool diagnostics = plan.diagnostics_cycle > 0;
   const auto [profile, roles] = precision_strings(dbl);
@@ -799,7 +825,7 @@ int main(int argc, char** argv) {
       std::string line;
       while (std::getline(h, line)) kept.push_back(line);
     }
-    if (diagnostics) {
+    if (diagnostics && advance) {
       kept.push_back("# restart at cycle " + std::to_string(cycle) + ": precision_profile = " + profile +
                      ", precision_roles = " + roles);
       std::ofstream f(csv);
@@ -813,14 +839,19 @@ int main(int argc, char** argv) {
       if (deck.species[s].center_velocity)
         check(tpicb200_center_velocities(ctx, &deck, s, &st.slot[s][0], nullptr, s_), "velocity centring");
     }
-    if (diagnostics) {
-      std::ofstream f(csv);
-      f << head << "\n";
-    }
   }
   if (last < cycle) usage("the run's last cycle lies before the checkpoint cycle");
+  // A fresh run refuses output files that exist unless --overwrite-output.
+  if (advance && !args.restart && !plan.overwrite)
+    for (const std::string& path : {csv, plan.save_dir + "/gauss.csv"})
+      if (file_exists(path) && (path == csv ? diagnostics : plan.gauss_enabled()))
+        fail(path + " exists (--overwrite-output replaces it)");
+  if (advance && !args.restart && diagnostics) {
+    std::ofstream f(csv);
+    f << head << "\n";
+  }
   GaussRun gauss;
-  if (plan.gauss_enabled()) {
+  if (advance && plan.gauss_enabled()) {
     gauss.on = true;
     gauss.cells = cells;
     gauss.stash = (double*)dev.alloc(8 * cells);
@@ -839,6 +870,12 @@ int main(int argc, char** argv) {
       std::fprintf(stderr, "tpicb200_run: %u nonfinite records at startup\n", bad);
       return 1;
     }
+  }
+  if (!advance) {
+    std::printf("initialized: cycle %lld, %d species, context ready\n", cycle, deck.ns);
+    cudaStreamDestroy(stream);
+    check(tpicb200_destroy(ctx), "context release");
+    return 0;
   }
   double field[2], species[TPICB200_MAX_SPECIES][5];
   {

@@ -74,11 +74,29 @@ def resolve_form(form: str, precision: str) -> str:
     return form
 
 
+class _Parser(argparse.ArgumentParser):
+    """An invalid command line exits with code 1, as TPIC's."""
+
+    def error(self, message):
+        self.print_usage(sys.stderr)
+        self.exit(1, f"{self.prog}: error: {message}\n")
+
+
 def parse_args(argv=None):
-    ap = argparse.ArgumentParser(prog="python -m tpic_b200", description="Run a TPIC input deck on one B200.")
-    ap.add_argument("--run", required=True, metavar="DECK", help="TPIC input deck (.inp)")
-    ap.add_argument("--mass-matrix", default="matrix-core", choices=FORMS)
+    ap = _Parser(prog="python -m tpic_b200", description="Run a TPIC input deck on one B200.")
+    # TPIC's command line (src/app/main.cpp:60-120): exactly one of the three
+    # commands and one input file.
+    mode = ap.add_mutually_exclusive_group(required=True)
+    mode.add_argument("--check-input", action="store_true", help="parse and check the deck, no device, no output")
+    mode.add_argument("--initialize", action="store_true", help="complete the startup and exit before the cycles")
+    mode.add_argument("--run", action="store_true", help="advance the deck's cycles")
+    ap.add_argument("input", metavar="DECK", help="TPIC input deck (.inp)")
+    ap.add_argument("--mass-matrix", default="scalar", choices=FORMS)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "double"])
+    ap.add_argument("--order", default="partial", choices=["full", "partial", "unsorted"],
+                    help="accepted for TPIC's command line: the records are sorted by cell every cycle")
+    ap.add_argument("--overwrite-output", action="store_true",
+                    help="replace output files that exist (a fresh run refuses them otherwise)")
     ap.add_argument("--restart", action="store_true", help="continue from the newest complete checkpoint")
     ap.add_argument("--output", default=".", help="directory of diagnostics.csv and RestartDirName")
     ap.add_argument("--cycles", type=int, default=None, help="last cycle of the run (default: the deck's ncycles)")
@@ -98,27 +116,35 @@ def parse_args(argv=None):
                                                      "deck's, else data)")
     ap.add_argument("--gauss-cycle", type=int, default=None,
                     help="DiagnosticGaussCycle (default: the deck's, else 0: no Gauss-law samples)")
-    return ap.parse_args(argv)
+    args = ap.parse_args(argv)
+    if args.restart and args.check_input:
+        ap.error("--restart is only valid with --run or --initialize")
+    return args
 
 
 def run(args) -> int:
     from .simulation import Simulation
-    from .output import (GaussSampler, GaussWriter, OutputPlan, deck_keys, precision_strings, write_fields,
-                         write_particles)
-    text = Path(args.run).read_text()
+    from .output import (GaussSampler, GaussWriter, OutputPlan, deck_keys, precision_strings, select_arrays,
+                         write_fields, write_particles)
+    text = Path(args.input).read_text()
     deck = D.parse(text)
     case = D.to_case(deck, seed=args.seed)
     last = deck.ncycles if args.cycles is None else args.cycles
     form = resolve_form(args.mass_matrix, args.precision)
     out = Path(args.output)
-    out.mkdir(parents=True, exist_ok=True)
     plan = OutputPlan.from_deck(text, out, field_cycle=args.field_output_cycle,
                                 particles_cycle=args.particles_output_cycle, gauss_cycle=args.gauss_cycle)
     if args.save_dir is not None:
         plan.save_dir = out / args.save_dir
+    select_arrays(plan.field_tag, plan.moments_tag, len(case.species))  # the tags are checked before any work
+    plan.overwrite = args.overwrite_output or args.restart
     keys = deck_keys(text)
     ckpt_dir = out / (args.restart_dir if args.restart_dir is not None else (keys.get("RestartDirName", "") or "data"))
-    plan.save_dir.mkdir(parents=True, exist_ok=True)
+    if args.check_input:
+        g = case.grid
+        print(f"deck {args.input}: {g.nx}x{g.ny}x{g.nz} cells, {len(case.species)} species, "
+              f"{last} cycles, mass form {form}, {args.precision} precision; output under {plan.save_dir}")
+        return 0
     csv_path = plan.save_dir / "diagnostics.csv"
     diagnostics_cycle = (args.diagnostics_cycle if args.diagnostics_cycle is not None else
                          int(keys.get("DiagnosticsOutputCycle", plan.field_cycle)))
@@ -135,6 +161,17 @@ def run(args) -> int:
         sim = Simulation(case, generate_on_device=True, **kw)
         sim.prepare()
         initial = None
+    if args.initialize:
+        # The startup is complete; --initialize writes no output.
+        print(f"initialized: cycle {sim.cycle}, {len(case.species)} species, context ready")
+        sim.close()
+        return 0
+    out.mkdir(parents=True, exist_ok=True)
+    plan.save_dir.mkdir(parents=True, exist_ok=True)
+    if not args.restart and not plan.overwrite:
+        for path, used in ((csv_path, diagnostics), (plan.save_dir / "gauss.csv", plan.gauss_enabled())):
+            if used and path.exists():
+                raise SystemExit(f"{path} exists (--overwrite-output replaces it)")
     profile, roles = precision_strings(sim)
     head = f"# precision_profile = {profile}\n# precision_roles = {roles}\n" + HEADER + columns(ns)
     if diagnostics and args.restart:
