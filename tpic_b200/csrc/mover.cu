@@ -344,9 +344,17 @@ __global__ void __launch_bounds__(256, TPICB200_MOVER_MIN_BLOCKS) mover_kernel(G
 // (old_counts, old_offsets), which validate_bins has checked (the kernel
 // returns at once when they do not tile the records).
 constexpr int kRunWarps = 4;
+// Resident blocks of the run mover: eight (64 registers) in the mixed form;
+// five (96 registers) in FP64, which spills at 64 registers (the FP64 move
+// stage of the 128^3-cell, 268M-record workload: 16.5 ms with eight blocks,
+// 14.4 with seven, 13.0 with six, 12.7 with five).
+template <class P>
+constexpr int run_mover_blocks() {
+  return std::is_same_v<P, PDouble> ? 5 : 2 * TPICB200_MOVER_MIN_BLOCKS;
+}
 
 template <class P>
-__global__ void __launch_bounds__(kRunWarps * 32, 2 * TPICB200_MOVER_MIN_BLOCKS) run_mover_kernel(Geom g,
+__global__ void __launch_bounds__(kRunWarps * 32, run_mover_blocks<P>()) run_mover_kernel(Geom g,
     MoverParams<P> mp, MoveIo<P> io, uint32_t count, const double* __restrict__ theta,
     const typename P::Fld* __restrict__ bnode, const uint32_t* __restrict__ old_counts,
     const uint32_t* __restrict__ old_offsets, uint32_t* __restrict__ invalid, MoveCodes mc, MoverScalars sc) {
