@@ -344,13 +344,15 @@ __global__ void __launch_bounds__(256, TPICB200_MOVER_MIN_BLOCKS) mover_kernel(G
 // (old_counts, old_offsets), which validate_bins has checked (the kernel
 // returns at once when they do not tile the records).
 constexpr int kRunWarps = 4;
-// Resident blocks of the run mover: eight (64 registers) in the mixed form;
-// five (96 registers) in FP64, which spills at 64 registers (the FP64 move
-// stage of the 128^3-cell, 268M-record workload: 16.5 ms with eight blocks,
-// 14.4 with seven, 13.0 with six, 12.7 with five).
+// Resident blocks of the run mover: eight (64 registers) in the mixed form,
+// six (80 registers, no spills) in FP64, which spills at 64. The grid is one
+// wave of them. FP64 move stage of the 128^3-cell, 268M-record workload with
+// one-wave grids: 11.3 ms at four blocks, 11.3 at five, 10.3 at six, 11.5 at
+// seven (16.5 ms at eight blocks with the spills); mixed: 7.53 ms at eight,
+// 7.85 at seven, 8.14 at six.
 template <class P>
 constexpr int run_mover_blocks() {
-  return std::is_same_v<P, PDouble> ? 5 : 2 * TPICB200_MOVER_MIN_BLOCKS;
+  return std::is_same_v<P, PDouble> ? 6 : 2 * TPICB200_MOVER_MIN_BLOCKS;
 }
 
 template <class P>
@@ -511,7 +513,8 @@ cudaError_t launch(const Geom& g, double qom, double dt, double c, tpicb200_part
   MoveCodes mc{binned->code, binned->transfer, &binned->state->fallback, &binned->state->bins_bad,
                (long long)g.nx * g.ny * g.nz};
   const long long runs = run_count(g);
-  const unsigned run_blocks = grid_for(runs * 32, kRunWarps * 32, 148u * 8u);
+  // One wave of resident blocks (148 SMs); each warp strides over the runs.
+  const unsigned run_blocks = grid_for(runs * 32, kRunWarps * 32, 148u * unsigned(run_mover_blocks<P>()));
   run_mover_kernel<P><<<run_blocks, kRunWarps * 32, 0, s>>>(g, mp, io, p->count, theta, bn, binned->old_counts,
                                                             binned->old_offsets, invalid, mc, sc);
   sc.offset = int(run_blocks);
