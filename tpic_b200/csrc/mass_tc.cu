@@ -1469,22 +1469,25 @@ __global__ void __launch_bounds__(128) assemble_warp_quads_kernel(Geom g, const 
 
 
 // ---------------------------------------------------------------------------
-// FP64 CUDA-core form of the moment deposition (double precision).
+// FP64 form of the moment deposition (double precision).
 //
 // The same per-cell moments as the tensor-core forms, G[t][e] = sum_p m_pt
-// (s_p alpha_p[e]) and H[t][c] = sum_p m_pt j_p[c], accumulated in FP64 on
-// the CUDA cores: a warp per cell; per chunk of 32 records each lane forms
-// one record's B gather, response, s alpha and j (12 values) and its 27
-// pair-weight products m_t = (X_tx Y_ty) Z_tz into shared memory; then lane
-// 3b + q (b < 9, q < 3) adds, for every record of the chunk, the products of
-// m_t for t = 3b .. 3b+2 and entries 4q .. 4q+3 of the 12 into a 3 x 4 block
-// of registers (7 shared loads per 12 fused multiply-adds). The flush stores
-// G and the corner currents J_a[c] = sum_b H[t(a,b)][c] into the double
-// moment records, which the assembly adds into J and the mass records as for
-// the tensor-core forms. Per record this is 27 x 12 fused multiply-adds,
-// where the reference's scalar and matrix-core kernels form the 64
-// corner-pair products of 9 entries (mass_matrix_scalar_device.hpp:25-97,
-// mass_matrix_mma_device.hpp:58-150).
+// (s_p alpha_p[e]) and H[t][c] = sum_p m_pt j_p[c], accumulated in FP64: a
+// warp per cell; per chunk of 32 records each lane forms one record's B
+// gather, response, s alpha and j (12 values) and its 27 pair-weight products
+// m_t = (X_tx Y_ty) Z_tz into shared memory; then the warp contracts the
+// chunk on the FP64 tensor cores (mma.sync m8n8k4: D[t][e] += sum_k m[k][t]
+// src[k][e], t in four tiles of 8 rows (27 used), e in two of 8 columns (12
+// used), four records per step). The contraction on the CUDA cores (a 3 x 4
+// register block per lane, 7 shared loads per 12 fused multiply-adds) was
+// bound by the shared-memory pipe (93 % of its wavefronts at 64^3); the
+// fragments need 6 shared loads per 4 records and lane (128^3-cell workload:
+// the FP64 deposit stage 20.0 -> 16.1 ms). The flush stores G and the corner
+// currents J_a[c] = sum_b H[t(a,b)][c] into the double moment records, which
+// the assembly adds into J and the mass records as for the tensor-core forms.
+// Per record this is 27 x 12 multiply-adds, where the reference's scalar and
+// matrix-core kernels form the 64 corner-pair products of 9 entries
+// (mass_matrix_scalar_device.hpp:25-97, mass_matrix_mma_device.hpp:58-150).
 struct F64Species {
   const double* rx;
   const double* ry;
@@ -1514,6 +1517,14 @@ struct F64Params {
   double inv_volume;
 };
 
+// D (8 x 8) += A (8 x 4) B (4 x 8) in FP64 on the tensor cores. Per lane:
+// A[lane >> 2][lane & 3], B[lane & 3][lane >> 2], D[lane >> 2][2 (lane & 3) + i].
+__device__ __forceinline__ void dmma_884(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
 constexpr int kF64Warps = 4;
 // Row pitches with an odd number of 8-byte words past a multiple of 32 banks
 // keep the lanes' row stores spread over the banks.
@@ -1535,7 +1546,7 @@ __global__ void __launch_bounds__(kF64Warps * 32) moments_f64_kernel(Geom g, F64
   F64Warp& S = shared[warp];
   const int nx = g.nx, ny = g.ny;
   const long long cells = (long long)nx * ny * g.nz, nn = g.nodes;
-  const int t0 = 3 * (lane / 3), e0 = 4 * (lane % 3);  // this lane's block (lane < 27)
+  const int kk = lane & 3, rr = lane >> 2;  // fragment coordinates
   uint32_t bad = 0;
   for (long long cell = (long long)blockIdx.x * kF64Warps + warp; cell < cells;
        cell += (long long)gridDim.x * kF64Warps) {
@@ -1546,11 +1557,12 @@ __global__ void __launch_bounds__(kF64Warps * 32) moments_f64_kernel(Geom g, F64
       S.bc[lane] = bnode[c * nn + g.node(ci + (a & 1), cj + ((a >> 1) & 1), ck + ((a >> 2) & 1))];
     }
     __syncwarp();
-    double acc[3][4];
+    // D tiles (t: 4 x 8 rows, entry: 2 x 8 columns) of this lane.
+    double acc[4][2][2];
 #pragma unroll
-    for (int i = 0; i < 3; ++i)
+    for (int i = 0; i < 4; ++i)
 #pragma unroll
-      for (int e = 0; e < 4; ++e) acc[i][e] = 0.0;
+      for (int e = 0; e < 2; ++e) acc[i][e][0] = acc[i][e][1] = 0.0;
     for (int si = 0; si < fp.ns; ++si) {
       const F64Species& sp = fp.sp[si];
       const uint32_t begin = sp.offsets[key], n = sp.counts[key];
@@ -1611,35 +1623,37 @@ __global__ void __launch_bounds__(kF64Warps * 32) moments_f64_kernel(Geom g, F64
           }
         }
         __syncwarp();
-        if (lane < 27) {
-          for (uint32_t k = 0; k < m; ++k) {
-            const double* mk = S.m[k] + t0;
-            const double* sk = S.src[k] + e0;
-            const double mv[3] = {mk[0], mk[1], mk[2]};
-            const double sv[4] = {sk[0], sk[1], sk[2], sk[3]};
+        for (uint32_t k0 = 0; k0 < m; k0 += 4) {
+          const uint32_t k = k0 + kk;
+          const bool in = k < m;
+          double av[4], bv[2];
 #pragma unroll
-            for (int i = 0; i < 3; ++i)
+          for (int i = 0; i < 4; ++i) av[i] = in && 8 * i + rr < 27 ? S.m[k][8 * i + rr] : 0.0;
 #pragma unroll
-              for (int e = 0; e < 4; ++e) acc[i][e] += mv[i] * sv[e];
-          }
+          for (int e = 0; e < 2; ++e) bv[e] = in && 8 * e + rr < 12 ? S.src[k][8 * e + rr] : 0.0;
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) dmma_884(acc[i][e], av[i], bv[e]);
         }
         __syncwarp();
       }
     }
-    if (lane < 27) {
 #pragma unroll
-      for (int i = 0; i < 3; ++i)
+    for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const int t = t0 + i, entry = e0 + e;
+      for (int e = 0; e < 2; ++e)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int t = 8 * i + rr, entry = 8 * e + 2 * kk + h;
+          if (t >= 27 || entry >= 12) continue;
           if (entry < 9) {
             double* dst = mom + moment_index(cell, t * 9 + entry);
-            *dst = accumulate ? *dst + acc[i][e] : acc[i][e];
+            *dst = accumulate ? *dst + acc[i][e][h] : acc[i][e][h];
           } else {
-            S.hs[t][entry - 9] = acc[i][e];
+            S.hs[t][entry - 9] = acc[i][e][h];
           }
         }
-    }
     __syncwarp();
     if (lane < 24) {
       const int a = lane / 3, c = lane % 3;
