@@ -1526,14 +1526,16 @@ __device__ __forceinline__ void dmma_884(double (&d)[2], double a, double b) {
 }
 
 constexpr int kF64Warps = 4;
-// Row pitches with an odd number of 8-byte words past a multiple of 32 banks
-// keep the lanes' row stores spread over the banks.
-constexpr int kF64MPitch = 29;
-constexpr int kF64SPitch = 13;
+// The products and values are stored by (t or entry, record), 36 records a
+// row: a lane's stores of its record fall in consecutive words, and the 16
+// lanes of a half-warp fragment load (4 rows x 4 records) hit 16 different
+// bank pairs. With record-major rows of 29 and 13 words the fragment loads
+// met 2-way conflicts (C3 FP64 deposit stage 16.2 ms, 15.7 ms with these rows).
+constexpr int kF64Pitch = 36;
 struct F64Warp {
   double bc[24];                 // B at the cell's corners, [c][a]
-  double m[32][kF64MPitch];      // per record: the 27 pair-weight products
-  double src[32][kF64SPitch];    // per record: s alpha[9], j[3]
+  double m[27][kF64Pitch];       // [t][record]: the 27 pair-weight products
+  double src[12][kF64Pitch];     // [entry][record]: s alpha[9], j[3]
   double hs[27][3];              // H of the cell at the flush
 };
 
@@ -1578,8 +1580,6 @@ __global__ void __launch_bounds__(kF64Warps * 32) moments_f64_kernel(Geom g, F64
             sp.orx[pos] = fx; sp.ory[pos] = fy; sp.orz[pos] = fz;
             sp.ou[pos] = u; sp.ov[pos] = v; sp.ow[pos] = w; sp.oq[pos] = q; sp.okey[pos] = k0;
           }
-          double* mt = S.m[lane];
-          double* src = S.src[lane];
           bool ok = k0 == key && fx >= 0 && fx < 1 && fy >= 0 && fy < 1 && fz >= 0 && fz < 1;
           if (ok) {
             double wt[8];
@@ -1597,10 +1597,15 @@ __global__ void __launch_bounds__(kF64Warps * 32) moments_f64_kernel(Geom g, F64
             double hx, hy, hz;
             resp.apply(u, v, w, hx, hy, hz);
             const double qv = q * fp.inv_volume;
+            double sv[12];
 #pragma unroll
-            for (int e = 0; e < 9; ++e) src[e] = resp.a[e] * scale;
-            src[9] = qv * hx; src[10] = qv * hy; src[11] = qv * hz;
-            for (int e = 0; e < 12; ++e) ok = ok && isfinite(src[e]);
+            for (int e = 0; e < 9; ++e) sv[e] = resp.a[e] * scale;
+            sv[9] = qv * hx; sv[10] = qv * hy; sv[11] = qv * hz;
+#pragma unroll
+            for (int e = 0; e < 12; ++e) {
+              ok = ok && isfinite(sv[e]);
+              S.src[e][lane] = sv[e];
+            }
             const double cx = 1.0 - fx, cy = 1.0 - fy, cz = 1.0 - fz;
             const double px[3] = {cx * cx, cx * fx, fx * fx};
             const double py[3] = {cy * cy, cy * fy, fy * fy};
@@ -1611,15 +1616,15 @@ __global__ void __launch_bounds__(kF64Warps * 32) moments_f64_kernel(Geom g, F64
               for (int tx = 0; tx < 3; ++tx) {
                 const double pxy = px[tx] * py[ty];
 #pragma unroll
-                for (int tz = 0; tz < 3; ++tz) mt[tx + 3 * ty + 9 * tz] = pxy * pz[tz];
+                for (int tz = 0; tz < 3; ++tz) S.m[tx + 3 * ty + 9 * tz][lane] = pxy * pz[tz];
               }
           }
           if (!ok) {
             ++bad;
 #pragma unroll
-            for (int e = 0; e < 12; ++e) src[e] = 0.0;
+            for (int e = 0; e < 12; ++e) S.src[e][lane] = 0.0;
 #pragma unroll
-            for (int t = 0; t < 27; ++t) mt[t] = 0.0;
+            for (int t = 0; t < 27; ++t) S.m[t][lane] = 0.0;
           }
         }
         __syncwarp();
@@ -1628,9 +1633,9 @@ __global__ void __launch_bounds__(kF64Warps * 32) moments_f64_kernel(Geom g, F64
           const bool in = k < m;
           double av[4], bv[2];
 #pragma unroll
-          for (int i = 0; i < 4; ++i) av[i] = in && 8 * i + rr < 27 ? S.m[k][8 * i + rr] : 0.0;
+          for (int i = 0; i < 4; ++i) av[i] = in && 8 * i + rr < 27 ? S.m[8 * i + rr][k] : 0.0;
 #pragma unroll
-          for (int e = 0; e < 2; ++e) bv[e] = in && 8 * e + rr < 12 ? S.src[k][8 * e + rr] : 0.0;
+          for (int e = 0; e < 2; ++e) bv[e] = in && 8 * e + rr < 12 ? S.src[8 * e + rr][k] : 0.0;
 #pragma unroll
           for (int i = 0; i < 4; ++i)
 #pragma unroll
