@@ -350,32 +350,40 @@ __global__ void __launch_bounds__(128) sorted_deposit_kernel(Geom g, DepositPara
 // ---------------------------------------------------------------------------
 // Fold: duplicates (index n) and ghosts (-1, n+1) take their unique node's
 // value. Only the shell of non-unique vertices is visited.
+// Component blockIdx.y; the shell index in 32-bit arithmetic (launch_fold
+// checks that the shell holds fewer than 2^31 vertices).
 template <class T>
 __global__ void __launch_bounds__(256) fold_field_kernel(Geom g, T* __restrict__ f) {
-  const long long shell = shell_count(g), total = 3 * shell;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-       t += (long long)gridDim.x * blockDim.x) {
-    const long long c = t / shell;
+  const uint32_t shell = uint32_t(shell_count(g));
+  T* fc = f + (long long)blockIdx.y * g.nodes;
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < shell; t += gridDim.x * blockDim.x) {
     int i, j, k;
-    shell_coordinates(g, t - c * shell, i, j, k);
-    f[c * g.nodes + g.node(i, j, k)] =
-        f[c * g.nodes + g.node(wrap_index(i, g.nx), wrap_index(j, g.ny), wrap_index(k, g.nz))];
+    shell_coordinates32(g, t, i, j, k);
+    fc[g.node(i, j, k)] = fc[g.node(wrap_index(i, g.nx), wrap_index(j, g.ny), wrap_index(k, g.nz))];
   }
 }
 
-// Stencil-major layout: one thread per shell vertex copies its 126 entries
-// (each entry a coalesced row across the warp's vertices); the vertex is
-// decoded once (32-bit arithmetic: a shell holds far fewer than 2^31 vertices).
+// Stencil-major and tiled layouts: a thread copies kFoldEntries entries
+// (group blockIdx.y of the 126) of one shell vertex, each entry a coalesced
+// row across the warp's vertices; the vertex is decoded once (32-bit
+// arithmetic, checked by launch_fold). One thread per vertex and all 126
+// entries took 342 us at 512 x 512 x 1, where the ghost planes hold three
+// times the interior vertices.
+constexpr int kFoldEntries = 9;
 template <class T>
 __global__ void __launch_bounds__(256) fold_mass_rows_kernel(Geom g, T* __restrict__ m) {
   const uint32_t shell = uint32_t(shell_count(g));
+  const int e0 = int(blockIdx.y) * kFoldEntries;
   for (uint32_t sv = blockIdx.x * blockDim.x + threadIdx.x; sv < shell; sv += gridDim.x * blockDim.x) {
     int i, j, k;
     shell_coordinates32(g, sv, i, j, k);
     const long long to = g.mass_vertex(i, j, k),
                     from = g.mass_vertex(wrap_index(i, g.nx), wrap_index(j, g.ny), wrap_index(k, g.nz));
-#pragma unroll 6
-    for (int e = 0; e < 126; ++e) m[g.mass_index(to, e)] = m[g.mass_index(from, e)];
+    T v[kFoldEntries];
+#pragma unroll
+    for (int e = 0; e < kFoldEntries; ++e) v[e] = m[g.mass_index(from, e0 + e)];
+#pragma unroll
+    for (int e = 0; e < kFoldEntries; ++e) m[g.mass_index(to, e0 + e)] = v[e];
   }
 }
 
@@ -456,15 +464,16 @@ cudaError_t launch_copy_ids(const tpicb200_particles* in, const SortedCopy* copy
 }
 
 cudaError_t launch_fold(int precision, const Geom& g, void* j, void* mass, cudaStream_t s) {
+  if (shell_count(g) >= (1LL << 31)) return cudaErrorInvalidValue;
   if (j) {
-    const unsigned blocks = grid_for(3 * shell_count(g), 256, 148u * 8u);
+    const dim3 blocks(grid_for(shell_count(g), 256), 3);
     if (precision == TPICB200_PRECISION_DOUBLE) fold_field_kernel<double><<<blocks, 256, 0, s>>>(g, (double*)j);
     else fold_field_kernel<float><<<blocks, 256, 0, s>>>(g, (float*)j);
     count_launches(1);
   }
   if (mass) {
     if (g.mes != 1) {
-      const unsigned blocks = grid_for(shell_count(g), 256, 148u * 8u);
+      const dim3 blocks(grid_for(shell_count(g), 256), 126 / kFoldEntries);
       if (precision == TPICB200_PRECISION_DOUBLE) fold_mass_rows_kernel<double><<<blocks, 256, 0, s>>>(g, (double*)mass);
       else fold_mass_rows_kernel<float><<<blocks, 256, 0, s>>>(g, (float*)mass);
     } else {

@@ -7,17 +7,20 @@
 namespace tpicb200 {
 namespace {
 
+// Ghost nodes take their periodic images; component blockIdx.y. The shell
+// index is decoded in 32-bit arithmetic (launch_node_ghosts checks that the
+// shell holds fewer than 2^31 nodes): on a grid one cell thick the ghost
+// planes hold three times the interior, and 64-bit division per node took
+// 23 us per fill at 512 x 512 x 1.
 template <class T>
-__global__ void __launch_bounds__(256) node_fill_kernel(Geom g, T* __restrict__ f, int components) {
+__global__ void __launch_bounds__(256) node_fill_kernel(Geom g, T* __restrict__ f) {
   wait_for_predecessor();
-  const long long shell = shell_count(g), total = shell * components;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-       t += (long long)gridDim.x * blockDim.x) {
-    const long long c = t / shell;
+  const uint32_t shell = uint32_t(shell_count(g));
+  T* fc = f + (long long)blockIdx.y * g.nodes;
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < shell; t += gridDim.x * blockDim.x) {
     int i, j, k;
-    shell_coordinates(g, t - c * shell, i, j, k);
-    f[c * g.nodes + g.node(i, j, k)] =
-        f[c * g.nodes + g.node(wrap_index(i, g.nx), wrap_index(j, g.ny), wrap_index(k, g.nz))];
+    shell_coordinates32(g, t, i, j, k);
+    fc[g.node(i, j, k)] = fc[g.node(wrap_index(i, g.nx), wrap_index(j, g.ny), wrap_index(k, g.nz))];
   }
 }
 
@@ -212,10 +215,11 @@ __global__ void __launch_bounds__(256) copy_node_kernel(long long total, const T
 }  // namespace
 
 cudaError_t launch_node_ghosts(const Geom& g, double* f, int components, cudaStream_t s, bool programmatic) {
-  const unsigned blocks = grid_for(shell_count(g) * components, 256);
+  if (shell_count(g) >= (1LL << 31)) return cudaErrorInvalidValue;
+  const dim3 blocks(grid_for(shell_count(g), 256), unsigned(components));
   count_launches(1);
-  if (programmatic) return launch_programmatic(node_fill_kernel<double>, blocks, 256, 0, s, g, f, components);
-  node_fill_kernel<double><<<blocks, 256, 0, s>>>(g, f, components);
+  if (programmatic) return launch_programmatic(node_fill_kernel<double>, blocks, 256, 0, s, g, f);
+  node_fill_kernel<double><<<blocks, 256, 0, s>>>(g, f);
   return cudaGetLastError();
 }
 
@@ -232,10 +236,10 @@ cudaError_t launch_cell_to_node(int precision, const Geom& g, const void* cellf,
   const unsigned blocks = grid_for(3 * g.interior, 256);
   if (precision == TPICB200_PRECISION_DOUBLE) {
     cell_to_node_kernel<double, double><<<blocks, 256, 0, s>>>(g, (const double*)cellf, (double*)node);
-    node_fill_kernel<double><<<grid_for(3 * shell_count(g), 256), 256, 0, s>>>(g, (double*)node, 3);
+    node_fill_kernel<double><<<dim3(grid_for(shell_count(g), 256), 3), 256, 0, s>>>(g, (double*)node);
   } else {
     cell_to_node_kernel<float, float><<<blocks, 256, 0, s>>>(g, (const float*)cellf, (float*)node);
-    node_fill_kernel<float><<<grid_for(3 * shell_count(g), 256), 256, 0, s>>>(g, (float*)node, 3);
+    node_fill_kernel<float><<<dim3(grid_for(shell_count(g), 256), 3), 256, 0, s>>>(g, (float*)node);
   }
   count_launches(2);
   return cudaGetLastError();
