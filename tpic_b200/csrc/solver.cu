@@ -303,32 +303,37 @@ __global__ void __launch_bounds__(TX * TY * TZ, sizeof(C) == 4 ? 4 : 3) maxwell_
 // returns without writing its rows.
 constexpr int kBoxX = 36;
 
-template <int TY, int TZ, class M> struct TmaBox {
-  static constexpr int X = kBoxX, Y = TY + 1, Z = TZ + 1;
+// Flat: a grid one cell thick along z (thin tiles). Every block a node of
+// plane 0 needs is then in plane 0: the planes -1 and 1 are the fold's copies
+// of it, so the box holds that plane alone and the products are unchanged bit
+// for bit, with half the mass bytes read.
+template <int TY, int TZ, class M, bool Flat = false> struct TmaBox {
+  static constexpr int X = kBoxX, Y = TY + 1, Z = Flat ? 1 : TZ + 1;
   static constexpr int entry = X * Y * Z;              // elements of one entry's box
   static constexpr int elems = 9 * entry;              // one stencil's box
   static constexpr int bytes = elems * int(sizeof(M));
   static constexpr int stage = (bytes + 1023) / 1024 * 1024;  // 1024-byte aligned stages
 };
 
-template <class C, class M, int TX, int TY, int TZ, int S>
+template <class C, class M, int TX, int TY, int TZ, int S, bool Flat = false>
 struct TmaApplyShared {
   static constexpr int VX = TX + 2, VY = TY + 2, VZ = TZ + 2;
   static constexpr int CX = TX + 1, CY = TY + 1, CZ = TZ + 1;
-  static constexpr int stages = S * TmaBox<TY, TZ, M>::stage;
+  static constexpr int stages = S * TmaBox<TY, TZ, M, Flat>::stage;
   static constexpr int bars = stages;                              // S + 1 mbarriers
   static constexpr int vs = (bars + (S + 1) * 8 + 15) / 16 * 16;   // C [3][VZ][VY][VX]
   static constexpr int cs = vs + 3 * VZ * VY * VX * int(sizeof(C));  // C [3][CZ][CY][CX]
   static constexpr int total = cs + 3 * CZ * CY * CX * int(sizeof(C));
 };
 
-template <class C, class M, class Out, int TX, int TY, int TZ, int S, bool kTranspose>
+template <class C, class M, class Out, int TX, int TY, int TZ, int S, bool kTranspose, bool kFlat>
 __global__ void __launch_bounds__(TX * TY * TZ, sizeof(C) == 4 ? 4 : 2)
     maxwell_apply_tma_kernel(const __grid_constant__ CUtensorMap map, Geom g, C d2, C kfac, C inv_volume,
                              const double* __restrict__ v, Out* __restrict__ out, uint32_t* invalid,
                              uint32_t polls, int stall) {
-  using Box = TmaBox<TY, TZ, M>;
-  using L = TmaApplyShared<C, M, TX, TY, TZ, S>;
+  static_assert(!kFlat || TZ == 1, "flat boxes hold one z plane");
+  using Box = TmaBox<TY, TZ, M, kFlat>;
+  using L = TmaApplyShared<C, M, TX, TY, TZ, S, kFlat>;
   constexpr int VX = L::VX, VY = L::VY, VZ = L::VZ, CX = L::CX, CY = L::CY, CZ = L::CZ;
   extern __shared__ __align__(1024) uint8_t tma_smem[];
   uint64_t* bars = reinterpret_cast<uint64_t*>(tma_smem + L::bars);  // S stage barriers, then `never`
@@ -343,8 +348,8 @@ __global__ void __launch_bounds__(TX * TY * TZ, sizeof(C) == 4 ? 4 : 2)
     const int oy = stencil_offset(s, 1), oz = stencil_offset(s, 2);
     uint64_t* bar = &bars[s % S];
     tc::mbar_arrive_expect_tx(bar, uint32_t(Box::bytes));
-    tc::tma_load_4d(tma_smem + (s % S) * Box::stage, &map, i0, j0 + 1 - (oy > 0 ? oy : 0), k0 + 1 - (oz > 0 ? oz : 0),
-                    9 * s, bar);
+    tc::tma_load_4d(tma_smem + (s % S) * Box::stage, &map, i0, j0 + 1 - (oy > 0 ? oy : 0),
+                    kFlat ? k0 + 1 : k0 + 1 - (oz > 0 ? oz : 0), 9 * s, bar);
   };
   if (threadIdx.x == 0) {
 #pragma unroll
@@ -428,11 +433,11 @@ __global__ void __launch_bounds__(TX * TY * TZ, sizeof(C) == 4 ? 4 : 2)
       const M* box = reinterpret_cast<const M*>(tma_smem + (s % S) * Box::stage);
       const int ox = stencil_offset(s, 0), oy = stencil_offset(s, 1), oz = stencil_offset(s, 2);
       const int my = oy > 0 ? oy : 0, mz = oz > 0 ? oz : 0;
-      const int fwd = (lx + 1) + Box::X * ((ly + my) + Box::Y * (lz + mz));
+      const int fwd = (lx + 1) + Box::X * ((ly + my) + Box::Y * (kFlat ? 0 : lz + mz));
       if (s == 0) {
         block_product<C, M, kTranspose>(box + fwd, Box::entry, vv(0, 0, 0, 0), vv(1, 0, 0, 0), vv(2, 0, 0, 0), x, y, z);
       } else {
-        const int bwd = (lx + 1 - ox) + Box::X * ((ly - oy + my) + Box::Y * (lz - oz + mz));
+        const int bwd = (lx + 1 - ox) + Box::X * ((ly - oy + my) + Box::Y * (kFlat ? 0 : lz - oz + mz));
         C bx, by, bz;
         block_product<C, M, kTranspose>(box + fwd, Box::entry, vv(0, ox, oy, oz), vv(1, ox, oy, oz),
                                         vv(2, ox, oy, oz), bx, by, bz);
@@ -1036,6 +1041,7 @@ TensorMapEncodeTiled tensor_map_encoder() {
 template <class M>
 const CUtensorMap* mass_tensor_map(SolverWorkspace* w, const M* mass, bool thin) {
   const Geom& g = w->g;
+  const bool flat = thin;  // thin tiles are on grids one cell thick along z
   const int tile = thin ? 1 : 0;
   for (auto& m : w->maps)
     if (m.mass == mass && m.tile == tile) return m.usable ? &m.map : nullptr;
@@ -1052,8 +1058,8 @@ const CUtensorMap* mass_tensor_map(SolverWorkspace* w, const M* mass, bool thin)
   if (!encode) return nullptr;
   const cuuint64_t dims[4] = {cuuint64_t(g.MX), cuuint64_t(g.NY), cuuint64_t(g.NZ), 126};
   const cuuint64_t strides[3] = {cuuint64_t(g.MX) * es, cuuint64_t(g.MX) * g.NY * es, cuuint64_t(g.mes) * es};
-  const cuuint32_t box[4] = {cuuint32_t(kBoxX), cuuint32_t((thin ? kThinTY : kTY) + 1), cuuint32_t((thin ? 1 : kTZ) + 1),
-                             9};
+  const cuuint32_t box[4] = {cuuint32_t(kBoxX), cuuint32_t((thin ? kThinTY : kTY) + 1),
+                             cuuint32_t(flat ? 1 : kTZ + 1), 9};
   const cuuint32_t unit[4] = {1, 1, 1, 1};
   const CUresult r = encode(&m.map, es == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
                             const_cast<M*>(mass), dims, strides, box, unit, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -1065,15 +1071,15 @@ const CUtensorMap* mass_tensor_map(SolverWorkspace* w, const M* mass, bool thin)
 
 // Launches the TMA-staged apply; the kernel's dynamic shared memory limit is
 // raised once per device.
-template <class C, class M, class Out, int TY, int TZ, bool kTranspose>
+template <class C, class M, class Out, int TY, int TZ, bool kTranspose, bool kFlat = false>
 cudaError_t launch_apply_tma(const CUtensorMap& map, unsigned tiles, cudaStream_t st, const Geom& g, C d2, C kf,
                              C civ, const double* in, Out* out, uint32_t* invalid, uint32_t polls, int stall) {
   // Two stages: four CTAs per SM in the float apply (three in the mixed
   // residual apply); three stages gave three (two) and a slower solve.
   constexpr int S = 2;
-  constexpr int bytes = TmaApplyShared<C, M, kTX, TY, TZ, S>::total;
+  constexpr int bytes = TmaApplyShared<C, M, kTX, TY, TZ, S, kFlat>::total;
   static_assert(bytes <= 227 * 1024, "apply tile exceeds shared memory");
-  auto kernel = maxwell_apply_tma_kernel<C, M, Out, kTX, TY, TZ, S, kTranspose>;
+  auto kernel = maxwell_apply_tma_kernel<C, M, Out, kTX, TY, TZ, S, kTranspose, kFlat>;
   static std::atomic<uint64_t> ready{0};
   int device = 0;
   cudaError_t e = cudaGetDevice(&device);
@@ -1140,15 +1146,16 @@ struct Solve {
       const uint32_t polls = w->wait_polls;
       const int stall = w->stall_stencil;
       cudaError_t e;
+      // Thin tiles are on grids one cell thick along z: flat boxes.
       if (w->transpose && thin)
-        e = launch_apply_tma<C, Mass, Out, kThinTY, 1, true>(*map, tiles, st, g, d2, kf, civ, in, out, w->invalid,
-                                                             polls, stall);
+        e = launch_apply_tma<C, Mass, Out, kThinTY, 1, true, true>(*map, tiles, st, g, d2, kf, civ, in, out,
+                                                                   w->invalid, polls, stall);
       else if (w->transpose)
         e = launch_apply_tma<C, Mass, Out, kTY, kTZ, true>(*map, tiles, st, g, d2, kf, civ, in, out, w->invalid,
                                                            polls, stall);
       else if (thin)
-        e = launch_apply_tma<C, Mass, Out, kThinTY, 1, false>(*map, tiles, st, g, d2, kf, civ, in, out, w->invalid,
-                                                              polls, stall);
+        e = launch_apply_tma<C, Mass, Out, kThinTY, 1, false, true>(*map, tiles, st, g, d2, kf, civ, in, out,
+                                                                    w->invalid, polls, stall);
       else
         e = launch_apply_tma<C, Mass, Out, kTY, kTZ, false>(*map, tiles, st, g, d2, kf, civ, in, out, w->invalid,
                                                             polls, stall);
